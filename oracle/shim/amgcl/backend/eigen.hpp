@@ -1,0 +1,3 @@
+// amgcl/backend/eigen.hpp -- oracle API shim (test infrastructure); see shim_amgcl.hpp.
+#pragma once
+#include "../../shim_amgcl.hpp"
