@@ -1,0 +1,350 @@
+"""Benchmark: DOF-updates/s and Poisson ms/step of the FR time step on one B200.
+
+Workload (default): the backward-facing step with ~15,000 jittered quads (14,625
+elements, h = 1/15, +/-0.15h interior jitter, seed 2), K = P+1 = 5 (365,625 DOF),
+Re = 400, RK4 at CFL 0.5, parabolic pulsatile inlet -- synthetic mesh of the stated
+shape (no dataset is involved). Each rank is an independent replica (the path has no
+data-path collective); `value` sums DOF updates over ranks and divides by the slowest
+rank's device time.
+
+The headline precision is mixed (FP32 FR residual + FP32 BiCGSTAB inside FP64 iterative
+refinement, FP64 RK accumulation); the FP64 plain path is timed on the same workload and
+reported under "fp64", with the relative L2 vorticity difference between the two after
+the same steps.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ho-cxx_b200"))
+
+METRIC = "DOF-updates/s + Poisson ms/step, mixed vs FP64 on one B200 at stated L2 error"
+UNIT = "DOF-updates/s"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default="bfs")
+    ap.add_argument("--knod", type=int, default=5)
+    ap.add_argument("--cpu-stages", type=int, default=1, help="RK stages timed for the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier and max-reduce of host floats across replicas (gloo; nothing GPU-side)."""
+
+    def __init__(self, world):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as td
+
+            td.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.td = td
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+def make_workload(tmp, case, knod, steps):
+    from ho2d import meshgen
+
+    return meshgen.make_case(case, tmp, knod=knod, steps=steps)
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.path = None
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = max(smax, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(inp, stages):
+    """The reference's own CPU step (oracle/_ref: src/HO_2D.cpp + src/Mesh.cpp built against
+    the oracle's Eigen/AMGCL API shim), single thread, timed over `stages` RK stages of
+    the same workload; DOF-updates/s = DOF / (4 * seconds per stage)."""
+    if not os.path.exists(REF_BIN):
+        return None
+    r = subprocess.run([REF_BIN, inp, os.path.join(os.path.dirname(inp), "refout"), "--time-stages", str(stages)],
+                       capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return None
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    per_stage = d["seconds"] / d["stages"]
+    value = d["dof"] / (4.0 * per_stage)
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{d['stages']} RK4 stage(s) of the same mesh (DOF {d['dof']}), reference setup excluded; "
+                      f"Poisson solve {d['poisson_seconds']:.1f} s of {d['seconds']:.1f} s "
+                      f"({d['poisson_iterations']} shim BiCGSTAB iterations, tol 1e-15, maxiter 150; "
+                      f"shim solver, not AMGCL 1.4.0)",
+            "poisson_ms_per_step": 4.0 * d["poisson_seconds"] / d["stages"] * 1e3,
+            "cpu": _cpu_model(), "nproc": os.cpu_count()}
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = make_workload(tmp, args.case, args.knod, 1)
+        if not os.path.exists(REF_BIN):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ho2d_ref was not built"}))
+            return
+        vals = []
+        for _ in range(max(1, args.steps)):
+            cb = cpu_baseline(inp, args.cpu_stages)
+            if cb is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+                return
+            vals.append(cb["value"])
+        value = statistics.median(vals)
+        dof = None
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": workload_name(args), "dof": dof},
+                "cpu_baseline": dict(cb, value=value),
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+
+
+def workload_name(args):
+    if args.case == "bfs":
+        return (f"backward-facing step, 14,625 jittered quads (+/-0.15h, seed 2), K={args.knod}, Re=400, RK4, "
+                f"CFL-0.5 dt, pulsatile parabolic inlet")
+    return f"{args.case}, K={args.knod}"
+
+
+def pinned_like(n):
+    """float64 host buffer in page-locked memory (cudaMallocHost of the runtime libho2d uses)."""
+    import ctypes
+
+    import numpy as np
+
+    from ho2d import capi
+
+    capi.load()
+    rt = ctypes.CDLL("libcudart.so.12")
+    p = ctypes.c_void_p()
+    if rt.cudaMallocHost(ctypes.byref(p), ctypes.c_size_t(n * 8)) != 0:
+        return np.zeros(n)
+    buf = (ctypes.c_double * n).from_address(p.value)
+    return np.frombuffer(buf, dtype=np.float64)
+
+
+def run_ours(args, rank, world, local, phys):
+    dist = Dist(world)
+    import numpy as np
+
+    import ho2d
+
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = make_workload(tmp, args.case, args.knod, args.steps)
+        solvers = {}
+        for prec in ("mixed", "fp64"):
+            s = ho2d.HO_2D()
+            s.read_input_file(inp)
+            s.set_precision(ho2d.MIXED if prec == "mixed" else ho2d.FP64)
+            s.setup()
+            solvers[prec] = s
+        s0 = solvers["mixed"]
+        n_dof = s0.N_el * s0.Knod * s0.Knod
+        results = {}
+        clocks = None
+        for prec in ("mixed", "fp64"):
+            s = solvers[prec]
+            s.solve_advection_diffusion(args.warmup)
+            dist.barrier()
+            sampler = ClockSampler(phys) if prec == "mixed" else None
+            l0 = s.launch_count()
+            tot_ms, pois_ms = s.time_steps(args.steps)
+            launches = s.launch_count() - l0
+            if sampler:
+                clocks = sampler.stop()
+            dist.barrier()
+            tmax = dist.max(tot_ms)
+            pmax = dist.max(pois_ms)
+            spmv_ms, spmv_bytes = s.profile_spmv(30)
+            results[prec] = {"ms_per_step": tmax / args.steps, "poisson_ms_per_step": pmax / args.steps,
+                             "value": dist.sum(n_dof * args.steps) / (tmax / 1e3), "launches": launches,
+                             "spmv_ms": spmv_ms, "spmv_bytes": spmv_bytes, "iters": s.poisson_stats()[0]}
+        w_mixed = solvers["mixed"].get_vorticity()
+        w_fp64 = solvers["fp64"].get_vorticity()
+        l2 = float(np.linalg.norm(w_mixed - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
+        # end to end through the public API with host buffers: H2D of the step's input
+        # vorticity from pinned memory, the step, D2H of the resulting vorticity
+        s = solvers["mixed"]
+        host_in = pinned_like(n_dof)
+        host_in[:] = w_mixed.ravel()
+        host_out = pinned_like(n_dof)
+        e2e_steps = max(3, args.steps // 2)
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            s.set_vorticity(host_in)
+            s.solve_advection_diffusion(1)
+            s._check(s._lib.ho2d_get_vort(s._h, n_dof, ho2d.capi.dptr(host_out)))
+            host_in[:] = host_out
+        e2e_s = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.sum(n_dof * e2e_steps) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n_dof * 8,
+               "d2h_bytes_per_step": n_dof * 8}
+        peak, peak_kind = measured_peaks()
+        m = results["mixed"]
+        achieved = m["spmv_bytes"] / (m["spmv_ms"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": "k_spmv_v (Poisson block SpMV, FP32, inner Krylov)",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_kind": peak_kind, "traffic": None,
+                    "launch_ms": m["spmv_ms"], "algorithmic_bytes_per_launch": m["spmv_bytes"]}
+        f = results["fp64"]
+        roofline_fp64 = {"kernel": "k_spmv_v (FP64)", "achieved": f["spmv_bytes"] / (f["spmv_ms"] * 1e-3) / 1e9,
+                         "launch_ms": f["spmv_ms"], "algorithmic_bytes_per_launch": f["spmv_bytes"]}
+        roofline_fp64["frac"] = roofline_fp64["achieved"] / peak
+        cb = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline(inp, args.cpu_stages)
+        if rank == 0:
+            line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+                    "data": "synthetic (seeded mesh of the stated shape)",
+                    "config": {"workload": workload_name(args), "dof": n_dof, "n_el": s0.N_el,
+                               "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 "
+                               "(Poisson operator alone > 126 MB), no flush",
+                               "poisson_tol": 1e-12},
+                    "poisson_ms_per_step": m["poisson_ms_per_step"],
+                    "poisson_iterations_last_solve": m["iters"],
+                    "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"],
+                             "poisson_ms_per_step": f["poisson_ms_per_step"], "roofline": roofline_fp64,
+                             "poisson_iterations_last_solve": f["iters"]},
+                    "mixed_over_fp64": m["value"] / f["value"],
+                    "l2_rel_vorticity_mixed_vs_fp64": l2,
+                    "l2_after_steps": args.warmup + args.steps,
+                    "clocks": clocks, "e2e": e2e, "gpu_launches": m["launches"], "roofline": roofline,
+                    "cpu_baseline": cb}
+            print(json.dumps(line))
+    dist.close()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    # one GPU per rank: each replica sees only its own device
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    devs = [d for d in visible.split(",") if d.strip()] if visible else None
+    phys = devs[local % len(devs)] if devs else str(local)
+    os.environ["CUDA_VISIBLE_DEVICES"] = phys
+    run_ours(args, rank, world, local, phys)
+
+
+if __name__ == "__main__":
+    main()

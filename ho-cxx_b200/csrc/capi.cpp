@@ -1,0 +1,214 @@
+// capi.cpp -- the extern "C" boundary declared in include/ho2d.h. Every entry point
+// catches exceptions and turns them into status codes plus a per-handle message.
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "../../include/ho2d.h"
+#include "solver.hpp"
+
+struct ho2d_solver {
+    ho2d::Solver s;
+    std::string err;
+};
+
+namespace {
+
+int finish(ho2d_solver* h, const ho2d::Error& e) {
+    h->err = e.code ? e.msg : std::string();
+    return e.code;
+}
+
+template <typename F>
+int guarded(ho2d_solver* h, F&& f) {
+    if (!h) return HO2D_ERR_ARG;
+    try {
+        return finish(h, f());
+    } catch (const std::bad_alloc&) {
+        h->err = "host out of memory";
+        return HO2D_ERR_ARG;
+    } catch (const std::exception& ex) {
+        h->err = ex.what();
+        return HO2D_ERR_ARG;
+    } catch (...) {
+        h->err = "unknown exception";
+        return HO2D_ERR_ARG;
+    }
+}
+
+ho2d::Error check_len(const ho2d_solver* h, int32_t len, size_t expect, const void* buf) {
+    if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};
+    if (!buf) return {HO2D_ERR_ARG, "null buffer"};
+    if (len < 0 || (size_t)len != expect)
+        return {HO2D_ERR_ARG, "buffer length " + std::to_string(len) + " != expected " + std::to_string(expect)};
+    return {0, ""};
+}
+
+size_t nvol(const ho2d_solver* h) { return (size_t)h->s.n_el() * h->s.knod() * h->s.knod(); }
+size_t nbnd(const ho2d_solver* h) { return (size_t)h->s.n_eb() * h->s.knod(); }
+
+}  // namespace
+
+extern "C" {
+
+int ho2d_create(ho2d_solver** handle) {
+    if (!handle) return HO2D_ERR_ARG;
+    try {
+        *handle = new ho2d_solver();
+    } catch (...) {
+        *handle = nullptr;
+        return HO2D_ERR_ARG;
+    }
+    return HO2D_OK;
+}
+
+int ho2d_destroy(ho2d_solver* handle) {
+    if (!handle) return HO2D_ERR_ARG;
+    delete handle;
+    return HO2D_OK;
+}
+
+int ho2d_read_input(ho2d_solver* h, const char* path) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!path) return {HO2D_ERR_ARG, "null path"};
+        return h->s.read_input(path);
+    });
+}
+
+int ho2d_setup(ho2d_solver* h) {
+    return guarded(h, [&]() { return h->s.setup(); });
+}
+
+int ho2d_solve(ho2d_solver* h) {
+    return guarded(h, [&]() { return h->s.solve(); });
+}
+
+int ho2d_step(ho2d_solver* h, int32_t nsteps) {
+    return guarded(h, [&]() { return h->s.step(nsteps); });
+}
+
+int ho2d_stage(ho2d_solver* h, double coeff) {
+    return guarded(h, [&]() { return h->s.stage(coeff); });
+}
+
+int ho2d_solveto(ho2d_solver* h, double outerdt, int32_t numstep, int32_t integtype, double reyn) {
+    return guarded(h, [&]() { return h->s.solveto(outerdt, numstep, integtype, reyn); });
+}
+
+int ho2d_get_sizes(ho2d_solver* h, int32_t* n_el, int32_t* knod, int32_t* n_edges_boundary, int32_t* lnod) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};
+        if (n_el) *n_el = h->s.n_el();
+        if (knod) *knod = h->s.knod();
+        if (n_edges_boundary) *n_edges_boundary = h->s.n_eb();
+        if (lnod) *lnod = h->s.lnod();
+        return {0, ""};
+    });
+}
+
+int ho2d_get_vort(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.get_volume(HO2D_FIELD_VORTICITY, buf);
+    });
+}
+
+int ho2d_set_vort(ho2d_solver* h, int32_t len, const double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.set_vorticity(buf);
+    });
+}
+
+int ho2d_get_psi(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.get_volume(HO2D_FIELD_STREAMFUNCTION, buf);
+    });
+}
+
+int ho2d_get_vel(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, 2 * nvol(h), buf);
+        return e.code ? e : h->s.get_velocity(buf);
+    });
+}
+
+int ho2d_get_field(ho2d_solver* h, int32_t which, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.get_volume(which, buf);
+    });
+}
+
+int ho2d_get_boundary(ho2d_solver* h, int32_t which, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nbnd(h), buf);
+        return e.code ? e : h->s.get_boundary(which, buf);
+    });
+}
+
+int ho2d_set_boundary(ho2d_solver* h, int32_t which, int32_t len, const double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nbnd(h), buf);
+        return e.code ? e : h->s.set_boundary(which, buf);
+    });
+}
+
+int ho2d_get_solution_points(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, 2 * nvol(h), buf);
+        return e.code ? e : h->s.get_solution_points(buf);
+    });
+}
+
+int ho2d_set_precision(ho2d_solver* h, int32_t mode) {
+    return guarded(h, [&]() { return h->s.set_precision(mode); });
+}
+
+int ho2d_set_poisson_tolerance(ho2d_solver* h, double rel_tol, int32_t max_iter) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!(rel_tol > 0.0) || max_iter <= 0) return {HO2D_ERR_ARG, "tolerance and iteration cap must be positive"};
+        h->s.set_poisson_tolerance(rel_tol, max_iter);
+        return {0, ""};
+    });
+}
+
+int ho2d_poisson_stats(ho2d_solver* h, int32_t* iterations, double* rel_residual) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (iterations) *iterations = h->s.last_poisson_iterations();
+        if (rel_residual) *rel_residual = h->s.last_poisson_residual();
+        return {0, ""};
+    });
+}
+
+int ho2d_get_time(ho2d_solver* h, double* time, double* dt) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (time) *time = h->s.time();
+        if (dt) *dt = h->s.dt();
+        return {0, ""};
+    });
+}
+
+int ho2d_time_steps(ho2d_solver* h, int32_t nsteps, double* total_ms, double* poisson_ms) {
+    return guarded(h, [&]() { return h->s.time_steps(nsteps, total_ms, poisson_ms); });
+}
+
+int ho2d_profile_spmv(ho2d_solver* h, int32_t reps, double* avg_ms, double* bytes_per_launch) {
+    return guarded(h, [&]() { return h->s.profile_spmv(reps, avg_ms, bytes_per_launch); });
+}
+
+int ho2d_last_launch_count(ho2d_solver* h, int64_t* launches) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (launches) *launches = h->s.launches();
+        return {0, ""};
+    });
+}
+
+const char* ho2d_last_error(ho2d_solver* h) {
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+}  // extern "C"

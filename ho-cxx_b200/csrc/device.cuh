@@ -1,0 +1,72 @@
+// device.cuh -- device-side data structures shared by the FR and Krylov kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ho2d {
+
+constexpr int kDirichlet = 0, kNeumann = 1;
+
+// Threads: K^2 per element (one per solution point), EPB elements per CTA.
+template <int K>
+struct Shape {
+    static constexpr int K2 = K * K;
+    static constexpr int EPB = (256 / K2) > 64 ? 64 : ((256 / K2) > 0 ? (256 / K2) : 1);
+    static constexpr int THREADS = ((EPB * K2 + 31) / 32) * 32;  // whole warps; tail threads idle
+    static constexpr int NF = 4 * K;  // face points per element
+};
+
+// 1-D bases, passed by value (kernel parameter space); T is the arithmetic type.
+template <typename T>
+struct DevBases {
+    T D[64];     // D[k*K+m] = l_k'(x_m)
+    T sbb[16];   // [k*2+lr] l_k(-1), l_k(+1)
+    T sbgb[16];  // [k*2+lr] l_k'(-1), l_k'(+1)
+    T R[16];     // [k*2+lr] Radau values (left, right)
+    T gR[16];    // [k*2+lr] Radau derivatives
+    T gp[2];     // g'(-1), g'(+1)
+};
+
+// Everything an FR kernel reads. Pointers are device pointers; volume arrays are
+// [N][K][K], face arrays [N][4][K] (ijp order), boundary arrays [N_eb][K].
+template <typename T>
+struct FrGeom {
+    int N, n_eb;
+    const int* face_nb;     // [N*4] neighbour element (>= 0) or -(edge + 1) on the boundary
+    const int* face_nijp;   // [N*4] neighbour's face ijp across this face
+    const T* xxi;           // volume metrics
+    const T* xeta;
+    const T* yxi;
+    const T* yeta;
+    const T* J;
+    const T* fA;            // face metrics g.g (normal), g1.g2, face Jacobian, |g|
+    const T* fB;
+    const T* fJ;
+    const T* fAn;
+    const int* be_group;    // [N_eb]
+    const int* sw_p;        // [N_eb]
+    const int* sw_d;        // [N_eb]
+    const int* noslip;      // [n_groups]
+};
+
+// Boundary-edge arrays, always double (they carry the 1/(dt Re^-1) wall flux).
+struct BcArrays {
+    double* bc_p;
+    double* bc_nv;
+    double* bc_pv;
+    double* bc_d;
+    double* bc_w;
+    double* vjump;
+    double* bc_adv;
+};
+
+// Scalars of one Krylov solve, resident on the device.
+struct KrylovScalars {
+    double rho, rho_old, alpha, omega, beta;
+    double bnorm2, rnorm2, snorm2, eps2;
+    int it, done, breakdown, s_exit, zero_rhs, pad;
+};
+
+}  // namespace ho2d

@@ -1,0 +1,653 @@
+// fr_kernels.cu -- flux-reconstruction kernels of one explicit stage (sm_100a).
+//
+// Mapping: K^2 threads per element (one per solution point), EPB elements per CTA;
+// an element's volume block is staged in shared memory, face work (4K points) is spread
+// over the element's threads. Neighbour data come from per-element face-trace buffers
+// ([el][ijp][k]) written by the previous kernel, so every kernel reads each array once.
+//
+//   trace_kernel      psi -> psi face values / normal derivatives
+//   velocity_kernel   common psi, corrected grad psi, u = dpsi/dy, v = -dpsi/dx
+//                     (src/HO_2D.cpp:3174-3366) + velocity_jump / BC_normal_vel side
+//                     outputs + no-slip diffusion BC (2647-2664) + the omega and
+//                     contravariant-flux face traces the residual kernel needs
+//   residual_kernel   Re^-1 Lap(omega) (2666-2927) + BC_vorticity + BC_advection
+//                     (2219-2243) + -div(u omega), type 1 (2245-2437) or type 2
+//                     (2439-2645) + k = dt (adv + diff) (1833-1836) + the RK update
+//                     of solve_advection_diffusion (1465-1531)
+//   poisson_rhs_kernel  b = -omega J - sum boundary_source . BC_Poisson (1881-1900)
+//   bc_update_kernel  time-dependent BC refresh and h-direction flip (1979-2217)
+#include <cmath>
+
+#include "device.cuh"
+#include "fr_launch.hpp"
+
+namespace ho2d {
+
+namespace {
+
+template <int K>
+__device__ __forceinline__ int bf_index(int side, int k) {
+    return (side / 2) * (K - 2 * k - 1) + k;
+}
+
+__device__ __forceinline__ int side_of_ijp(int ijp) {
+    // ijp 0 W, 1 E, 2 S, 3 N -> element side (S=0, E=1, N=2, W=3)
+    return ijp == 0 ? 3 : (ijp == 1 ? 1 : (ijp == 2 ? 0 : 2));
+}
+
+// Face values (basis at -1/+1) and normal derivatives of a K x K block in shared memory.
+template <int K, typename T>
+__device__ __forceinline__ void face_trace(const T* f, const DevBases<T>& b, int o, T& val, T& der) {
+    const int ijp = o / K, k = o % K;
+    const int lr = ijp & 1;
+    T v = T(0), g = T(0);
+    if (ijp < 2) {
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            v += f[k * K + m] * b.sbb[m * 2 + lr];
+            g += f[k * K + m] * b.sbgb[m * 2 + lr];
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            v += f[m * K + k] * b.sbb[m * 2 + lr];
+            g += f[m * K + k] * b.sbgb[m * 2 + lr];
+        }
+    }
+    val = v;
+    der = g;
+}
+
+template <int K, typename T>
+__device__ __forceinline__ T face_value(const T* f, const DevBases<T>& b, int o) {
+    const int ijp = o / K, k = o % K;
+    const int lr = ijp & 1;
+    T v = T(0);
+    if (ijp < 2) {
+#pragma unroll
+        for (int m = 0; m < K; ++m) v += f[k * K + m] * b.sbb[m * 2 + lr];
+    } else {
+#pragma unroll
+        for (int m = 0; m < K; ++m) v += f[m * K + k] * b.sbb[m * 2 + lr];
+    }
+    return v;
+}
+
+// Common value (s_com) and common normal flux (s_cg) on the 4 faces of one element,
+// Huynh's method 2 with g = g_DG: calc_internal_comm_vals_meth2 and
+// calc_boundary_comm_vals_meth2 (src/HO_2D.cpp:2833-2927), the face-flux average of
+// 2739-2743, for boundary values `bcv` with switches `sw`. `neu_sign` multiplies the
+// Neumann values by the h-direction sign (the psi case, src/HO_2D.cpp:3259-3262).
+// Must be called by all threads of the CTA (contains __syncthreads).
+template <int K, typename T>
+__device__ void face_common(bool active, int el, int ij, const FrGeom<T>& g, const DevBases<T>& b,
+                            const T* __restrict__ tv_glob, const T* __restrict__ tg_glob, const T* s_tv,
+                            const T* s_tg, T* s_com, T* s_cg, const int* __restrict__ sw,
+                            const double* __restrict__ bcv, bool neu_sign) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    // (1) common values of interior and Dirichlet faces
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K;
+            const int nb = g.face_nb[el * 4 + ijp];
+            T com;
+            if (nb >= 0) {
+                const int nijp = g.face_nijp[el * 4 + ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                const int jn = rev ? K - 1 - k : k;
+                com = T(0.5) * (s_tv[o] + tv_glob[(nb * 4 + nijp) * K + jn]);
+            } else {
+                const int e = -nb - 1;
+                com = sw[e] == kDirichlet ? T(bcv[e * K + bf_index<K>(side_of_ijp(ijp), k)]) : T(0);
+            }
+            s_com[o] = com;
+        }
+    }
+    __syncthreads();
+    // (2) Neumann faces: solve the K x K system for the common value (one thread per face)
+    for (int ijp = ij; active && ijp < 4; ijp += K2) {
+        const int nb = g.face_nb[el * 4 + ijp];
+        if (nb < 0 && sw[-nb - 1] == kNeumann) {
+            const int e = -nb - 1, side = side_of_ijp(ijp), lr = ijp & 1;
+            const T sgn = neu_sign ? T(2 * (ijp % 2) - 1) : T(1);
+            T M[K][K], r[K], x[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int q = (el * 4 + ijp) * K + k;
+                const T cg = sgn * T(bcv[e * K + bf_index<K>(side, k)]) * g.fAn[q];
+                s_cg[ijp * K + k] = cg;
+                r[k] = g.fJ[q] * cg - g.fA[q] * (s_tg[ijp * K + k] - s_tv[ijp * K + k] * b.gp[lr]);
+#pragma unroll
+                for (int i = 0; i < K; ++i) M[k][i] = -g.fB[q] * b.D[i * K + k];
+                M[k][k] += g.fA[q] * b.gp[lr];
+            }
+            // Gauss elimination without pivoting (src/MathHelpers.hpp:53-74)
+#pragma unroll
+            for (int c = 0; c < K - 1; ++c) {
+#pragma unroll
+                for (int i = c + 1; i < K; ++i) {
+                    const T f = M[i][c] / M[c][c];
+                    r[i] -= f * r[c];
+#pragma unroll
+                    for (int j = c + 1; j < K; ++j) M[i][j] -= f * M[c][j];
+                }
+            }
+#pragma unroll
+            for (int i = K - 1; i >= 0; --i) {
+                T s = T(0);
+#pragma unroll
+                for (int j = i + 1; j < K; ++j) s += M[i][j] * x[j];
+                x[i] = (r[i] - s) / M[i][i];
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) s_com[ijp * K + k] = x[k];
+        }
+    }
+    __syncthreads();
+    // (3) corrected normal fluxes; interior faces average with the neighbour's flux
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            const int nb = g.face_nb[el * 4 + ijp];
+            if (nb < 0 && sw[-nb - 1] == kNeumann) continue;
+            const int q = (el * 4 + ijp) * K + k;
+            const T com = s_com[o];
+            T cross = T(0);
+#pragma unroll
+            for (int m = 0; m < K; ++m) cross += s_com[ijp * K + m] * b.D[m * K + k];
+            const T dv = s_tg[o] + (com - s_tv[o]) * b.gp[lr];
+            const T fl = (dv * g.fA[q] - cross * g.fB[q]) / g.fJ[q];
+            if (nb < 0) {
+                s_cg[o] = fl;
+            } else {
+                const int nijp = g.face_nijp[el * 4 + ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                const int jn = rev ? K - 1 - k : k;
+                const int nq = (nb * 4 + nijp) * K + jn;
+                T crn = T(0);
+#pragma unroll
+                for (int m = 0; m < K; ++m) crn += s_com[ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
+                const T dvn = tg_glob[nq] + (com - tv_glob[nq]) * b.gp[nijp & 1];
+                const T fln = (dvn * g.fA[nq] - crn * g.fB[nq]) / g.fJ[nq];
+                const T sign = T(2 * ((ijp + nijp) % 2) - 1);
+                s_cg[o] = T(0.5) * (fl + sign * fln);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// f~, g~ at the solution points (src/HO_2D.cpp:2775-2792) and their face corrections
+// fB/gB (2795-2803) in s_fb[ijp][k]. Needs s_f, s_tv, s_com, s_cg. Collective.
+template <int K, typename T>
+__device__ void contravariant_gradient(bool active, int el, int ij, const FrGeom<T>& g, const DevBases<T>& b,
+                                       const T* s_f, const T* s_tv, const T* s_com, const T* s_cg, T* s_a,
+                                       T* s_b, T* s_fb, T& ft, T& gt) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    const int j = ij / K, i = ij % K;
+    if (active) {
+        T dx = T(0), de = T(0);
+#pragma unroll
+        for (int d = 0; d < K; ++d) {
+            dx += s_f[j * K + d] * b.D[d * K + i];
+            de += s_f[d * K + i] * b.D[d * K + j];
+        }
+        dx += (s_com[0 * K + j] - s_tv[0 * K + j]) * b.gR[i * 2 + 0];
+        dx += (s_com[1 * K + j] - s_tv[1 * K + j]) * b.gR[i * 2 + 1];
+        de += (s_com[2 * K + i] - s_tv[2 * K + i]) * b.gR[j * 2 + 0];
+        de += (s_com[3 * K + i] - s_tv[3 * K + i]) * b.gR[j * 2 + 1];
+        const int p = el * K2 + ij;
+        const T xx = g.xxi[p], xe = g.xeta[p], yx = g.yxi[p], ye = g.yeta[p], J = g.J[p];
+        ft = (dx * (xe * xe + ye * ye) - de * (xx * xe + yx * ye)) / J;
+        gt = (de * (xx * xx + yx * yx) - dx * (xx * xe + yx * ye)) / J;
+        s_a[ij] = ft;
+        s_b[ij] = gt;
+    }
+    __syncthreads();
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            T v = s_cg[o];
+            if (ijp < 2) {
+#pragma unroll
+                for (int d = 0; d < K; ++d) v -= s_a[k * K + d] * b.sbb[d * 2 + lr];
+            } else {
+#pragma unroll
+                for (int d = 0; d < K; ++d) v -= s_b[d * K + k] * b.sbb[d * 2 + lr];
+            }
+            s_fb[o] = v;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------------
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) trace_kernel(int N, const T* __restrict__ f, T* __restrict__ tv,
+                                                                   T* __restrict__ tg, DevBases<T> b) {
+    using S = Shape<K>;
+    __shared__ T s_f[S::EPB][S::K2];
+    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
+    const int el = blockIdx.x * S::EPB + le;
+    const bool active = le < S::EPB && el < N;
+    if (active) s_f[le][ij] = f[el * S::K2 + ij];
+    __syncthreads();
+    if (active) {
+        for (int o = ij; o < S::NF; o += S::K2) {
+            T v, d;
+            face_trace<K, T>(s_f[le], b, o, v, d);
+            tv[el * S::NF + o] = v;
+            tg[el * S::NF + o] = d;
+        }
+    }
+}
+
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g, DevBases<T> b, BcArrays bc,
+                                                                      VelocityArgs<T> a) {
+    using S = Shape<K>;
+    constexpr int K2 = S::K2, NF = S::NF, EPB = S::EPB;
+    __shared__ T s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2], s_w[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
+    __shared__ T s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF];
+    const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
+    const int el = blockIdx.x * EPB + le;
+    const bool active = le < EPB && el < g.N;
+    const int lei = active ? le : 0;
+    if (active) {
+        s_f[le][ij] = a.psi[el * K2 + ij];
+        s_w[le][ij] = a.w[el * K2 + ij];
+    }
+    __syncthreads();
+    if (active)
+        for (int o = ij; o < NF; o += K2) face_trace<K, T>(s_f[le], b, o, s_tv[le][o], s_tg[le][o]);
+    __syncthreads();
+    face_common<K, T>(active, el, ij, g, b, a.psi_tv, a.psi_tg, s_tv[lei], s_tg[lei], s_com[lei], s_cg[lei], g.sw_p,
+                      bc.bc_p, true);
+    // boundary side outputs: velocity_jump / BC_normal_vel, then the no-slip diffusion BC
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K;
+            const int nb = g.face_nb[el * 4 + ijp];
+            if (nb >= 0) continue;
+            const int e = -nb - 1;
+            const int be = e * K + bf_index<K>(side_of_ijp(ijp), k);
+            const int q = (el * 4 + ijp) * K + k;
+            double vj = bc.vjump[be];
+            if (g.sw_p[e] == kDirichlet) {
+                vj = double(s_cg[le][o]) / double(g.fAn[q]);
+            } else {
+                const T vsign = T(1 - 2 * (ijp / 2));
+                T nv = T(0);
+#pragma unroll
+                for (int d = 0; d < K; ++d) nv += vsign * s_com[le][ijp * K + d] * b.D[d * K + k];
+                bc.bc_nv[be] = double(nv / g.fAn[q]);
+            }
+            if (g.noslip[g.be_group[e]]) {
+                vj += double(2 * (ijp % 2) - 1) * bc.bc_pv[be];
+                bc.bc_d[be] = vj / (a.dt * a.re_inv);
+            }
+            bc.vjump[be] = vj;
+        }
+    }
+    T ft = T(0), gt = T(0);
+    contravariant_gradient<K, T>(active, el, ij, g, b, s_f[lei], s_tv[lei], s_com[lei], s_cg[lei], s_a[lei],
+                                 s_b[lei], s_fb[lei], ft, gt);
+    if (active) {
+        const int j = ij / K, i = ij % K, p = el * K2 + ij;
+        const T tx = ft + s_fb[le][0 * K + j] * b.R[i * 2 + 0] + s_fb[le][1 * K + j] * b.R[i * 2 + 1];
+        const T ty = gt + s_fb[le][2 * K + i] * b.R[j * 2 + 0] + s_fb[le][3 * K + i] * b.R[j * 2 + 1];
+        const T xx = g.xxi[p], xe = g.xeta[p], yx = g.yxi[p], ye = g.yeta[p], J = g.J[p];
+        const T dpdx = (tx * xx + ty * xe) / J;
+        const T dpdy = (tx * yx + ty * ye) / J;
+        const T u = dpdy, v = -dpdx;
+        a.u[p] = u;
+        a.v[p] = v;
+        s_ux[le][ij] = u * ye - v * xe;   // contravariant volumetric fluxes J u.grad(xi), J u.grad(eta)
+        s_uy[le][ij] = -u * yx + v * xx;
+    }
+    __syncthreads();
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K;
+            T wv, wg;
+            face_trace<K, T>(s_w[le], b, o, wv, wg);
+            a.w_tv[el * NF + o] = wv;
+            a.w_tg[el * NF + o] = wg;
+            a.U_t[el * NF + o] = face_value<K, T>(ijp < 2 ? s_ux[le] : s_uy[le], b, o);
+        }
+    }
+}
+
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) residual_kernel(FrGeom<T> g, DevBases<T> b, BcArrays bc,
+                                                                      ResidualArgs<T> a) {
+    using S = Shape<K>;
+    constexpr int K2 = S::K2, NF = S::NF, EPB = S::EPB;
+    __shared__ T s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
+    __shared__ T s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF], s_ut[EPB][NF],
+        s_up[EPB][NF];
+    const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
+    const int el = blockIdx.x * EPB + le;
+    const bool active = le < EPB && el < g.N;
+    const int lei = active ? le : 0;
+    const int j = ij / K, i = ij % K, p = el * K2 + ij;
+    T xx = T(0), xe = T(0), yx = T(0), ye = T(0), J = T(1), w = T(0);
+    if (active) {
+        w = a.w[p];
+        s_f[le][ij] = w;
+        xx = g.xxi[p]; xe = g.xeta[p]; yx = g.yxi[p]; ye = g.yeta[p]; J = g.J[p];
+        const T u = a.u[p], v = a.v[p];
+        s_ux[le][ij] = u * ye - v * xe;
+        s_uy[le][ij] = -u * yx + v * xx;
+    }
+    __syncthreads();
+    if (active)
+        for (int o = ij; o < NF; o += K2) {
+            face_trace<K, T>(s_f[le], b, o, s_tv[le][o], s_tg[le][o]);
+            s_ut[le][o] = face_value<K, T>((o / K) < 2 ? s_ux[le] : s_uy[le], b, o);
+        }
+    __syncthreads();
+    // ---- diffusion
+    face_common<K, T>(active, el, ij, g, b, a.w_tv, a.w_tg, s_tv[lei], s_tg[lei], s_com[lei], s_cg[lei], g.sw_d,
+                      bc.bc_d, false);
+    // BC_vorticity (src/HO_2D.cpp:2726-2727) and BC_advection (2219-2243) on boundary faces
+    if (active) {
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K;
+            const int nb = g.face_nb[el * 4 + ijp];
+            if (nb >= 0) continue;
+            const int e = -nb - 1;
+            const int be = e * K + bf_index<K>(side_of_ijp(ijp), k);
+            const double wb = double(s_com[le][o]);
+            bc.bc_w[be] = wb;
+            const double adv = wb * bc.bc_nv[be] * double(g.fAn[(el * 4 + ijp) * K + k]);
+            bc.bc_adv[be] = adv;
+            s_up[le][o] = T(adv);
+        }
+    }
+    T ft = T(0), gt = T(0);
+    contravariant_gradient<K, T>(active, el, ij, g, b, s_f[lei], s_tv[lei], s_com[lei], s_cg[lei], s_a[lei],
+                                 s_b[lei], s_fb[lei], ft, gt);
+    T diff = T(0);
+    if (active) {
+        T lap = T(0);
+#pragma unroll
+        for (int d = 0; d < K; ++d) lap += s_a[le][j * K + d] * b.D[d * K + i];
+        lap += s_fb[le][0 * K + j] * b.gR[i * 2 + 0] + s_fb[le][1 * K + j] * b.gR[i * 2 + 1];
+#pragma unroll
+        for (int d = 0; d < K; ++d) lap += s_b[le][d * K + i] * b.D[d * K + j];
+        lap += s_fb[le][2 * K + i] * b.gR[j * 2 + 0] + s_fb[le][3 * K + i] * b.gR[j * 2 + 1];
+        diff = lap * (T(a.re_inv) / J);
+    }
+    __syncthreads();  // s_a / s_b are reused below
+    // ---- advection
+    if (a.adv_type == 2) {
+        // continuous volumetric flux: common flux on faces, Radau-corrected inside
+        if (active)
+            for (int o = ij; o < NF; o += K2) {
+                const int ijp = o / K, k = o % K;
+                const int nb = g.face_nb[el * 4 + ijp];
+                T cvf;
+                if (nb >= 0) {
+                    const int nijp = g.face_nijp[el * 4 + ijp];
+                    const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                    const int jn = rev ? K - 1 - k : k;
+                    const T sign = T(2 * ((ijp + nijp) % 2) - 1);
+                    cvf = T(0.5) * (s_ut[le][o] + sign * a.U_t[(nb * 4 + nijp) * K + jn]);
+                    const T t = T(ijp % 2);
+                    const T wn = a.w_tv[(nb * 4 + nijp) * K + jn];
+                    s_up[le][o] = cvf > T(0) ? cvf * (t * s_tv[le][o] + (T(1) - t) * wn)
+                                             : cvf * ((T(1) - t) * s_tv[le][o] + t * wn);
+                } else {
+                    const int e = -nb - 1;
+                    cvf = T(bc.bc_nv[e * K + bf_index<K>(side_of_ijp(ijp), k)]) * g.fAn[(el * 4 + ijp) * K + k];
+                }
+                s_com[le][o] = cvf;  // reuse: common volumetric flux
+            }
+        __syncthreads();
+        if (active) {
+            const T cx = s_ux[le][ij] + (s_com[le][0 * K + j] - s_ut[le][0 * K + j]) * b.R[i * 2 + 0] +
+                         (s_com[le][1 * K + j] - s_ut[le][1 * K + j]) * b.R[i * 2 + 1];
+            const T cy = s_uy[le][ij] + (s_com[le][2 * K + i] - s_ut[le][2 * K + i]) * b.R[j * 2 + 0] +
+                         (s_com[le][3 * K + i] - s_ut[le][3 * K + i]) * b.R[j * 2 + 1];
+            s_a[le][ij] = cx * w;
+            s_b[le][ij] = cy * w;
+        }
+    } else {
+        if (active) {
+            s_a[le][ij] = s_ux[le][ij] * w;
+            s_b[le][ij] = s_uy[le][ij] * w;
+            for (int o = ij; o < NF; o += K2) {
+                const int ijp = o / K, k = o % K;
+                const int nb = g.face_nb[el * 4 + ijp];
+                if (nb < 0) continue;
+                const int nijp = g.face_nijp[el * 4 + ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                const int jn = rev ? K - 1 - k : k;
+                const int nq = (nb * 4 + nijp) * K + jn;
+                const T sign = T(2 * ((ijp + nijp) % 2) - 1);
+                const T wl = s_tv[le][o], wr = a.w_tv[nq];
+                const T fl = s_ut[le][o] * wl, fr = a.U_t[nq] * wr;
+                T up = T(0.5) * (fl + sign * fr);
+                const T dw = wl - wr;
+                if (fabs(double(dw)) > 1e-4) {  // upwind switch evaluated in double (src/HO_2D.cpp:2370)
+                    const T av = (fl - sign * fr) / dw;
+                    up += T(0.5) * T((ijp & 1) ? 1 : -1) * fabs(av) * dw;
+                }
+                s_up[le][o] = up;
+            }
+        }
+    }
+    __syncthreads();
+    if (active)
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            T v = s_up[le][o];
+            if (ijp < 2) {
+#pragma unroll
+                for (int m = 0; m < K; ++m) v -= s_a[le][k * K + m] * b.sbb[m * 2 + lr];
+            } else {
+#pragma unroll
+                for (int m = 0; m < K; ++m) v -= s_b[le][m * K + k] * b.sbb[m * 2 + lr];
+            }
+            s_fb[le][o] = v;
+        }
+    __syncthreads();
+    if (!active) return;
+    T dv = T(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) dv += s_a[le][j * K + d] * b.D[d * K + i];
+#pragma unroll
+    for (int d = 0; d < K; ++d) dv += s_b[le][d * K + i] * b.D[d * K + j];
+    dv += s_fb[le][0 * K + j] * b.gR[i * 2 + 0] + s_fb[le][1 * K + j] * b.gR[i * 2 + 1];
+    dv += s_fb[le][2 * K + i] * b.gR[j * 2 + 0] + s_fb[le][3 * K + i] * b.gR[j * 2 + 1];
+    const T adv = -dv / J;
+    const T kk = T(a.dt) * (adv + diff);
+    if (a.rhs_diff) a.rhs_diff[p] = diff;
+    if (a.rhs_adv) a.rhs_adv[p] = adv;
+    if (a.k_out) a.k_out[p] = kk;
+    // ---- RK stage update (src/HO_2D.cpp:1465-1531), FP64 accumulation
+    const double k = double(kk);
+    if (a.ti_type == 0) return;  // stage only: no update
+    double om = a.omega[p];
+    if (a.ti_type == 1) {
+        om += k;
+        a.omega[p] = om;
+        if (a.w_next) a.w_next[p] = T(om);
+    } else if (a.ti_type == 2) {
+        if (a.stage == 0) {
+            a.acc[p] = k;
+            a.w_next[p] = T(om + 1.0 * k);
+        } else {
+            om += 0.5 * (a.acc[p] + k);
+            a.omega[p] = om;
+            if (a.w_next) a.w_next[p] = T(om);
+        }
+    } else {
+        if (a.stage == 0) {
+            a.acc[p] = k;
+            a.w_next[p] = T(om + 0.5 * k);
+        } else if (a.stage == 1) {
+            a.acc[p] = a.acc[p] + 2.0 * k;
+            a.w_next[p] = T(om + 0.5 * k);
+        } else if (a.stage == 2) {
+            a.acc[p] = a.acc[p] + 2.0 * k;
+            a.w_next[p] = T(om + 1.0 * k);
+        } else {
+            om += (a.acc[p] + k) / 6.0;
+            a.omega[p] = om;
+            if (a.w_next) a.w_next[p] = T(om);
+        }
+    }
+}
+
+// b = -omega J - sum over the element's boundary edges of boundary_source . BC_Poisson,
+// edges taken in increasing index like the reference's loop.
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) poisson_rhs_kernel(int N, const int* __restrict__ face_nb,
+                                                                         const T* __restrict__ w,
+                                                                         const T* __restrict__ J,
+                                                                         const double* __restrict__ bsrc,
+                                                                         const double* __restrict__ bc_p,
+                                                                         double* __restrict__ rhs) {
+    using S = Shape<K>;
+    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
+    const int el = blockIdx.x * S::EPB + le;
+    if (le >= S::EPB || el >= N) return;
+    const int p = el * S::K2 + ij;
+    double r = -double(w[p]) * double(J[p]);
+    int es[4], ne = 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const int nb = face_nb[el * 4 + f];
+        if (nb < 0) es[ne++] = -nb - 1;
+    }
+    for (int x = 1; x < ne; ++x)
+        for (int y = x; y > 0 && es[y - 1] > es[y]; --y) {
+            const int t = es[y];
+            es[y] = es[y - 1];
+            es[y - 1] = t;
+        }
+    for (int x = 0; x < ne; ++x) {
+        const int e = es[x];
+        const double* s = bsrc + ((size_t)e * S::K2 + ij) * K;
+        double acc = r;
+#pragma unroll
+        for (int al = 0; al < K; ++al) acc -= s[al] * bc_p[e * K + al];
+        r = acc;
+    }
+    rhs[p] = r;
+}
+
+// Time-dependent BC refresh (problem types 2 and 3) and the flip of normal velocities
+// and Neumann vorticity BCs into the local h direction, one thread per edge point.
+__global__ void bc_update_kernel(int n_eb, int K, int ptype, double tc, double y_min, double y_max,
+                                 const int* __restrict__ role, const int* __restrict__ be_ijp,
+                                 const int* __restrict__ sw_d, const double* __restrict__ edge_y, BcArrays bc) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n_eb * K) return;
+    const int e = idx / K;
+    const int r = role[e];
+    const double y = edge_y[idx];
+    if (ptype == 2) {
+        const double h2 = (y_max - y_min) * (y_max - y_min);
+        if (r == 1) {
+            bc.bc_p[idx] = tc * ((y - y_min) * (y - y_min)) * (3.0 * y_max - y_min - 2.0 * y) / h2;
+            bc.bc_d[idx] = tc * 6.0 * (2.0 * y - y_min - y_max) / h2;
+            bc.bc_nv[idx] = tc * 6.0 * (y - y_min) * (y - y_max) / h2;
+        } else if (r == 2) {
+            bc.bc_p[idx] = tc * (y_max - y_min);
+        }
+    } else if (ptype == 3) {
+        if (r == 1) {
+            bc.bc_p[idx] = tc * (y - y_min);
+            bc.bc_nv[idx] = -tc;
+        } else if (r == 2) {
+            bc.bc_p[idx] = tc * (y_max - y_min);
+            bc.bc_d[idx] = 0.0;
+            bc.bc_pv[idx] = -tc;
+        } else if (r == 3) {
+            bc.bc_pv[idx] = tc;
+        } else if (r == 4) {
+            bc.bc_p[idx] = tc * 0.5 * (y_max - y_min);
+        }
+    }
+    const double sign = 2.0 * (be_ijp[e] % 2) - 1.0;
+    bc.bc_nv[idx] *= sign;
+    if (sw_d[e] == kNeumann) bc.bc_d[idx] *= sign;
+}
+
+// ----------------------------------------------------------------------------------
+// launchers
+
+#define HO2D_DISPATCH_K(K, CALL)                          \
+    switch (K) {                                          \
+        case 1: { constexpr int KK = 1; CALL; } break;     \
+        case 2: { constexpr int KK = 2; CALL; } break;     \
+        case 3: { constexpr int KK = 3; CALL; } break;     \
+        case 4: { constexpr int KK = 4; CALL; } break;     \
+        case 5: { constexpr int KK = 5; CALL; } break;     \
+        case 6: { constexpr int KK = 6; CALL; } break;     \
+        case 7: { constexpr int KK = 7; CALL; } break;     \
+        case 8: { constexpr int KK = 8; CALL; } break;     \
+        default: return cudaErrorInvalidValue;            \
+    }
+
+template <int K>
+static unsigned grid_for(int N) {
+    return (unsigned)((N + Shape<K>::EPB - 1) / Shape<K>::EPB);
+}
+
+template <typename T>
+cudaError_t launch_trace(int K, int N, const T* f, T* tv, T* tg, const DevBases<T>& b, cudaStream_t s) {
+    HO2D_DISPATCH_K(K, (trace_kernel<KK, T><<<grid_for<KK>(N), Shape<KK>::THREADS, 0, s>>>(N, f, tv, tg, b)));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_velocity(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
+                            const VelocityArgs<T>& a, cudaStream_t s) {
+    HO2D_DISPATCH_K(K, (velocity_kernel<KK, T><<<grid_for<KK>(g.N), Shape<KK>::THREADS, 0, s>>>(g, b, bc, a)));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_residual(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
+                            const ResidualArgs<T>& a, cudaStream_t s) {
+    HO2D_DISPATCH_K(K, (residual_kernel<KK, T><<<grid_for<KK>(g.N), Shape<KK>::THREADS, 0, s>>>(g, b, bc, a)));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_poisson_rhs(int K, int N, const int* face_nb, const T* w, const T* J, const double* bsrc,
+                               const double* bc_p, double* rhs, cudaStream_t s) {
+    HO2D_DISPATCH_K(K, (poisson_rhs_kernel<KK, T><<<grid_for<KK>(N), Shape<KK>::THREADS, 0, s>>>(
+                           N, face_nb, w, J, bsrc, bc_p, rhs)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bc_update(int n_eb, int K, int ptype, double tc, double y_min, double y_max, const int* role,
+                             const int* be_ijp, const int* sw_d, const double* edge_y, const BcArrays& bc,
+                             cudaStream_t s) {
+    const int n = n_eb * K;
+    if (n == 0) return cudaSuccess;
+    bc_update_kernel<<<(n + 127) / 128, 128, 0, s>>>(n_eb, K, ptype, tc, y_min, y_max, role, be_ijp, sw_d, edge_y,
+                                                     bc);
+    return cudaGetLastError();
+}
+
+#define HO2D_INSTANTIATE_FR(T)                                                                                     \
+    template cudaError_t launch_trace<T>(int, int, const T*, T*, T*, const DevBases<T>&, cudaStream_t);            \
+    template cudaError_t launch_velocity<T>(int, const FrGeom<T>&, const DevBases<T>&, const BcArrays&,           \
+                                            const VelocityArgs<T>&, cudaStream_t);                                 \
+    template cudaError_t launch_residual<T>(int, const FrGeom<T>&, const DevBases<T>&, const BcArrays&,           \
+                                            const ResidualArgs<T>&, cudaStream_t);                                 \
+    template cudaError_t launch_poisson_rhs<T>(int, int, const int*, const T*, const T*, const double*,           \
+                                               const double*, double*, cudaStream_t);
+
+HO2D_INSTANTIATE_FR(double)
+HO2D_INSTANTIATE_FR(float)
+
+}  // namespace ho2d

@@ -1,0 +1,117 @@
+// host.hpp -- host-side setup of the B200 HO-CXX solver: input.dat, Gmsh mesh, bases,
+// metrics, boundary conditions and the Poisson operator in block form.
+//
+// Layouts (all flat, row-major):
+//   volume fields      [el][j][i]            (j = eta index, i = xi index)
+//   face traces        [el][ijp][k]          ijp 0 = W (xi=-1), 1 = E, 2 = S (eta=-1), 3 = N
+//   boundary arrays    [edge][k]             edge in boundary-edge (file) order
+//   Poisson blocks     [el][slot][rs][ij]    slot 0 = element itself, 1..4 = face ijp 0..3;
+//                      stored transposed (column rs outer) so that consecutive threads
+//                      (one per output row ij) read consecutive addresses.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ho2d {
+
+constexpr int kMaxK = 8;
+constexpr int DIRICHLET = 0, NEUMANN = 1;
+// element sides (counter-clockwise from the bottom, src/Mesh.hpp:114-119)
+constexpr int SOUTH = 0, EAST = 1, NORTH = 2, WEST = 3;
+// ijp -> element side and back (src/MathHelpers.hpp:23-24)
+constexpr int kI2F[4] = {WEST, EAST, SOUTH, NORTH};
+constexpr int kF2I[4] = {2, 1, 3, 0};
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+// Positional input.dat fields (src/HO_2D.cpp:213-317).
+struct Input {
+    int nel_i = 0, nel_j = 0;
+    int knod = 2;
+    int lnod_in = 1;
+    std::string mesh_file;
+    std::string base_dir;
+    int occ = 0;
+    double reyn_inv = 0.001;
+    double dx_ratio = 1.0, fac = 0.0;
+    int huynh = 2;
+    int ti_type = 4;
+    int adv_type = 1;
+    int problem_type = 1;
+    int num_steps = 0;
+    double dt = 0.001;
+    int dump_freq = 1000;
+    int fast = 0;
+    int lhs_type = 3;
+    std::string sample_file;
+};
+
+// Mesh after reading and processing; element sides in SENW order.
+struct Mesh {
+    int n_el = 0, lnod = 2, n_eb = 0;
+    std::vector<double> node_xy;               // [n_nodes][2]
+    std::vector<std::vector<int>> elem_nodes;  // Gmsh node slots per element
+    std::vector<std::vector<int>> edge_nodes;  // boundary edges first (file order), element CCW orientation
+    std::vector<std::string> group_names;
+    std::vector<std::vector<int>> group_edges;
+    std::vector<int> nbr, nbr_side, bidx;      // [n_el][4] by side; -1 where absent
+    std::vector<int> be_el, be_side, be_group; // [n_eb]
+};
+
+// 1-D bases on the K Gauss-Legendre solution points and the L equispaced geometry nodes.
+struct Bases {
+    int K = 0, L = 0;
+    std::vector<double> xs, w;          // [K]
+    std::vector<double> sbb, sbgb;      // [K][2]  l_k(-1), l_k(+1) and derivatives
+    std::vector<double> D;              // [K][K]  D[k][m] = l_k'(x_m)
+    std::vector<double> R, gR;          // [K][2]  Radau g_L/g_R values and derivatives
+    std::vector<double> gsb, gsgb;      // [L][K]  geometry basis (and derivative) at the sps
+    std::vector<double> gbb, gbgb;      // [L][2]  geometry basis (and derivative) at -1, +1
+    double gp[2] = {0.0, 0.0};          // g'(-1), g'(+1) of g_DG
+};
+
+struct Metrics {
+    std::vector<double> xxi, xeta, yxi, yeta, J;  // [N][K][K]
+    std::vector<double> G;                        // [N][K][K][2][2]  (g_r . g_s) / J
+    std::vector<double> GB;                       // [N][2][2][K][2]
+    std::vector<double> fA, fB, fJ, fAn;          // [N][4][K]
+};
+
+struct BoundaryConditions {
+    std::vector<int> sw_p, sw_d;                   // [N_eb] DIRICHLET / NEUMANN
+    std::vector<int> noslip;                       // [n_groups]
+    std::vector<double> bc_p, bc_nv, bc_pv, bc_d;  // [N_eb][K]
+    std::vector<double> edge_y;                    // [N_eb][K] y at the edge's solution points
+    std::vector<int> role;                         // [N_eb] time-dependent role (see BcRole)
+    double y_min = 0.0, y_max = 0.0;
+};
+
+// Per-edge role in the time-dependent BC refresh of src/HO_2D.cpp:1979-2217.
+enum BcRole { ROLE_NONE = 0, ROLE_INLET = 1, ROLE_TOP = 2, ROLE_BOTTOM = 3, ROLE_OBJECT = 4 };
+
+// Poisson operator: 5 K^2 x K^2 blocks per element (transposed) and the boundary source.
+struct PoissonOperator {
+    int K2 = 0;
+    std::vector<double> blocks;   // [N][5][K2][K2] (rs outer, ij inner)
+    std::vector<int> block_col;   // [N][5] column element (-1 = empty slot)
+    std::vector<double> bsrc;     // [N_eb][K2][K]
+    std::vector<double> dinv;     // [N][K2][K2] inverse of the diagonal block (rs outer)
+    int64_t nnz = 0;              // entries surviving the |a| > 1e-14 filter
+};
+
+Error read_input(const std::string& path, Input& in);
+Error read_msh(const std::string& path, int occ, Mesh& mesh);
+Error make_bases(int K, int L, Bases& B);
+void make_metrics(const Mesh& mesh, const Bases& B, Metrics& M);
+Error setup_bcs(const Input& in, const Mesh& mesh, const Bases& B, BoundaryConditions& bc);
+void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
+                      PoissonOperator& op);
+int tensor2fem(int i, int j, int lnod_in);
+int tensor2fem_1d(int i, int lnod_in);
+
+}  // namespace ho2d

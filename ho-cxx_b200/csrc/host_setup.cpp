@@ -1,0 +1,539 @@
+// host_setup.cpp -- bases, metrics, boundary conditions and the block Poisson operator.
+//
+// bases ............ src/HO_2D.cpp:486-673 (Gauss-Legendre by Newton iteration on the
+//                    Legendre three-term recurrence, so any K <= 8 works; the reference's
+//                    closed forms stop at K = 5)
+// metrics .......... src/HO_2D.cpp:1240-1388
+// BCs .............. src/HO_2D.cpp:675-1238 (problem types 1, 2, 3)
+// Poisson operator . src/HO_2D.cpp:1533-1804 with the |a| > 1e-14 filter of 3023-3062.
+//   The element-interior and face couplings are linear in the metric terms G and GB, so
+//   they are evaluated from small precomputed coefficient lists (one entry per
+//   (row, column, metric slot)) instead of the reference's nested loops; Neumann faces
+//   add the inverse of the K x K face system.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "host.hpp"
+
+namespace ho2d {
+
+namespace {
+
+double legendre(int n, double x) {
+    if (n == 0) return 1.0;
+    double p0 = 1.0, p1 = x;
+    for (int i = 2; i <= n; ++i) {
+        const double p2 = ((2.0 * i - 1.0) * x * p1 - (i - 1.0) * p0) / i;
+        p0 = p1;
+        p1 = p2;
+    }
+    return p1;
+}
+
+// Lagrange basis of `nodes` evaluated at x: values V[k], derivatives Dv[k].
+void lagrange_at(const std::vector<double>& nodes, double x, double* V, double* Dv) {
+    const int n = (int)nodes.size();
+    for (int k = 0; k < n; ++k) {
+        double den = 1.0, val = 1.0, der = 0.0;
+        for (int j = 0; j < n; ++j) {
+            if (j == k) continue;
+            den *= nodes[k] - nodes[j];
+            val *= x - nodes[j];
+            double term = 1.0;
+            for (int i = 0; i < n; ++i)
+                if (i != k && i != j) term *= x - nodes[i];
+            der += term;
+        }
+        V[k] = val / den;
+        Dv[k] = der / den;
+    }
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting of an n x n row-major matrix.
+bool invert(int n, std::vector<double>& a) {
+    std::vector<double> inv((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)p * n + k])) p = i;
+        if (a[(size_t)p * n + k] == 0.0) return false;
+        if (p != k)
+            for (int j = 0; j < n; ++j) {
+                std::swap(a[(size_t)k * n + j], a[(size_t)p * n + j]);
+                std::swap(inv[(size_t)k * n + j], inv[(size_t)p * n + j]);
+            }
+        const double d = 1.0 / a[(size_t)k * n + k];
+        for (int j = 0; j < n; ++j) {
+            a[(size_t)k * n + j] *= d;
+            inv[(size_t)k * n + j] *= d;
+        }
+        for (int i = 0; i < n; ++i) {
+            if (i == k) continue;
+            const double l = a[(size_t)i * n + k];
+            if (l == 0.0) continue;
+            for (int j = 0; j < n; ++j) {
+                a[(size_t)i * n + j] -= l * a[(size_t)k * n + j];
+                inv[(size_t)i * n + j] -= l * inv[(size_t)k * n + j];
+            }
+        }
+    }
+    a.swap(inv);
+    return true;
+}
+
+}  // namespace
+
+Error make_bases(int K, int L, Bases& B) {
+    if (K < 1 || K > kMaxK) return {4, "Knod out of range"};
+    if (L < 2 || L > 4) return {4, "Lnod must be 2, 3 or 4"};
+    B.K = K;
+    B.L = L;
+    B.xs.assign(K, 0.0);
+    B.w.assign(K, 0.0);
+    // Gauss-Legendre nodes: Newton on P_K from the Chebyshev-like initial guess
+    for (int i = 0; i < K; ++i) {
+        double x = std::cos(M_PI * (i + 0.75) / (K + 0.5));
+        double dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            const double p = legendre(K, x), pm = legendre(K - 1, x);
+            dp = K * (x * p - pm) / (x * x - 1.0);
+            const double dx = p / dp;
+            x -= dx;
+            if (std::fabs(dx) < 1e-16) break;
+        }
+        const double p = legendre(K, x), pm = legendre(K - 1, x);
+        dp = K * (x * p - pm) / (x * x - 1.0);
+        B.xs[K - 1 - i] = x;
+        B.w[K - 1 - i] = 2.0 / ((1.0 - x * x) * dp * dp);
+    }
+    if (K == 1) { B.xs[0] = 0.0; B.w[0] = 2.0; }
+    if (K % 2 == 1) B.xs[K / 2] = 0.0;
+    for (int i = 0; i < K / 2; ++i) {  // exact symmetry
+        const double a = 0.5 * (B.xs[K - 1 - i] - B.xs[i]);
+        B.xs[i] = -a;
+        B.xs[K - 1 - i] = a;
+        const double w = 0.5 * (B.w[i] + B.w[K - 1 - i]);
+        B.w[i] = B.w[K - 1 - i] = w;
+    }
+    std::vector<double> gx(L);
+    for (int i = 0; i < L; ++i) gx[i] = -1.0 + 2.0 * i / (L - 1);
+    std::vector<double> V(std::max(K, L)), Dv(std::max(K, L));
+    B.sbb.assign(K * 2, 0.0);
+    B.sbgb.assign(K * 2, 0.0);
+    for (int lr = 0; lr < 2; ++lr) {
+        lagrange_at(B.xs, lr ? 1.0 : -1.0, V.data(), Dv.data());
+        for (int k = 0; k < K; ++k) { B.sbb[k * 2 + lr] = V[k]; B.sbgb[k * 2 + lr] = Dv[k]; }
+    }
+    B.D.assign(K * K, 0.0);
+    for (int m = 0; m < K; ++m) {
+        lagrange_at(B.xs, B.xs[m], V.data(), Dv.data());
+        for (int k = 0; k < K; ++k) B.D[k * K + m] = Dv[k];
+    }
+    B.gsb.assign(L * K, 0.0);
+    B.gsgb.assign(L * K, 0.0);
+    for (int m = 0; m < K; ++m) {
+        lagrange_at(gx, B.xs[m], V.data(), Dv.data());
+        for (int k = 0; k < L; ++k) { B.gsb[k * K + m] = V[k]; B.gsgb[k * K + m] = Dv[k]; }
+    }
+    B.gbb.assign(L * 2, 0.0);
+    B.gbgb.assign(L * 2, 0.0);
+    for (int lr = 0; lr < 2; ++lr) {
+        lagrange_at(gx, lr ? 1.0 : -1.0, V.data(), Dv.data());
+        for (int k = 0; k < L; ++k) { B.gbb[k * 2 + lr] = V[k]; B.gbgb[k * 2 + lr] = Dv[k]; }
+    }
+    B.R.assign(K * 2, 0.0);
+    B.gR.assign(K * 2, 0.0);
+    if (K == 1) {
+        B.R[0] = B.R[1] = 0.5;
+        B.gR[0] = -0.5;
+        B.gR[1] = 0.5;
+    } else {
+        // right Radau R_K(x) = (-1)^K/2 (P_K - P_{K-1}); the left one is its mirror
+        const double sg = (K % 2 == 0) ? 1.0 : -1.0;
+        const double c = 0.5 * sg, cd = 0.5 * K * sg;
+        for (int i = 0; i < K; ++i) {
+            const double x = B.xs[i];
+            B.R[i * 2 + 0] = c * (legendre(K, x) - legendre(K - 1, x));
+            B.R[i * 2 + 1] = c * (legendre(K, -x) - legendre(K - 1, -x));
+            B.gR[i * 2 + 0] = cd * (legendre(K, x) + legendre(K - 1, x)) / (1.0 + x);
+            B.gR[i * 2 + 1] = -cd * (legendre(K, -x) + legendre(K - 1, -x)) / (1.0 - x);
+        }
+    }
+    B.gp[0] = -0.5 * K * (K + 1.0);
+    B.gp[1] = 0.5 * K * (K + 1.0);
+    return {0, ""};
+}
+
+void make_metrics(const Mesh& mesh, const Bases& B, Metrics& M) {
+    const int N = mesh.n_el, K = B.K, L = B.L, lin = L - 1;
+    const size_t nv = (size_t)N * K * K;
+    M.xxi.assign(nv, 0.0); M.xeta.assign(nv, 0.0); M.yxi.assign(nv, 0.0); M.yeta.assign(nv, 0.0);
+    M.J.assign(nv, 0.0);
+    M.G.assign(nv * 4, 0.0);
+    M.GB.assign((size_t)N * 4 * K * 2, 0.0);
+    M.fA.assign((size_t)N * 4 * K, 0.0); M.fB = M.fA; M.fJ = M.fA; M.fAn = M.fA;
+#pragma omp parallel for schedule(static)
+    for (int el = 0; el < N; ++el) {
+        double X[4][4], Y[4][4];
+        for (int j = 0; j < L; ++j)
+            for (int i = 0; i < L; ++i) {
+                const int nd = mesh.elem_nodes[el][tensor2fem(i, j, lin)];
+                X[j][i] = mesh.node_xy[2 * nd];
+                Y[j][i] = mesh.node_xy[2 * nd + 1];
+            }
+        for (int j = 0; j < K; ++j)
+            for (int i = 0; i < K; ++i) {
+                double xx = 0, yx = 0, xe = 0, ye = 0;
+                for (int n = 0; n < L; ++n)
+                    for (int m = 0; m < L; ++m) {
+                        const double a = B.gsgb[m * K + i] * B.gsb[n * K + j];
+                        const double b = B.gsgb[n * K + j] * B.gsb[m * K + i];
+                        xx += a * X[n][m]; yx += a * Y[n][m];
+                        xe += b * X[n][m]; ye += b * Y[n][m];
+                    }
+                const size_t p = ((size_t)el * K + j) * K + i;
+                M.xxi[p] = xx; M.yxi[p] = yx; M.xeta[p] = xe; M.yeta[p] = ye;
+                const double J = xx * ye - xe * yx;
+                M.J[p] = J;
+                const double g[2][2] = {{-xe, ye}, {xx, -yx}};
+                for (int r = 0; r < 2; ++r)
+                    for (int s = 0; s < 2; ++s)
+                        M.G[p * 4 + r * 2 + s] = (g[r][0] * g[s][0] + g[r][1] * g[s][1]) / J;
+            }
+        for (int ijp = 0; ijp < 4; ++ijp) {
+            const int d = ijp / 2, t = ijp % 2;
+            for (int k = 0; k < K; ++k) {
+                double xx = 0, yx = 0, xe = 0, ye = 0;
+                for (int j = 0; j < L; ++j)
+                    for (int i = 0; i < L; ++i) {
+                        double a, b;  // weights of d/dxi and d/deta
+                        if (d == 0) {
+                            a = B.gbgb[i * 2 + t] * B.gsb[j * K + k];
+                            b = B.gbb[i * 2 + t] * B.gsgb[j * K + k];
+                        } else {
+                            a = B.gbb[j * 2 + t] * B.gsgb[i * K + k];
+                            b = B.gbgb[j * 2 + t] * B.gsb[i * K + k];
+                        }
+                        xx += a * X[j][i]; yx += a * Y[j][i];
+                        xe += b * X[j][i]; ye += b * Y[j][i];
+                    }
+                const size_t q = ((size_t)el * 4 + ijp) * K + k;
+                const double fJ = xx * ye - xe * yx;
+                M.fJ[q] = fJ;
+                M.fA[q] = d == 0 ? xe * xe + ye * ye : xx * xx + yx * yx;
+                M.fB[q] = xx * xe + yx * ye;
+                M.fAn[q] = std::sqrt(M.fA[q]);
+                const double g[2][2] = {{-xe, ye}, {xx, -yx}};
+                for (int r = 0; r < 2; ++r)
+                    M.GB[((((size_t)el * 2 + d) * 2 + t) * K + k) * 2 + r] =
+                        (g[d][0] * g[r][0] + g[d][1] * g[r][1]) / fJ;
+            }
+        }
+    }
+}
+
+namespace {
+
+std::vector<double> edge_y(const Mesh& m, const Bases& B, int e) {
+    std::vector<double> y(B.K, 0.0);
+    const int lin = m.lnod - 1;
+    for (int k = 0; k < B.K; ++k)
+        for (int j = 0; j < m.lnod; ++j) y[k] += B.gsb[j * B.K + k] * m.node_xy[2 * m.edge_nodes[e][tensor2fem_1d(j, lin)] + 1];
+    return y;
+}
+
+}  // namespace
+
+Error setup_bcs(const Input& in, const Mesh& m, const Bases& B, BoundaryConditions& bc) {
+    const int K = B.K, neb = m.n_eb, ng = (int)m.group_names.size();
+    bc.sw_p.assign(neb, DIRICHLET);
+    bc.sw_d.assign(neb, DIRICHLET);
+    bc.noslip.assign(ng, 0);
+    bc.bc_p.assign((size_t)neb * K, 0.0);
+    bc.bc_nv = bc.bc_p; bc.bc_pv = bc.bc_p; bc.bc_d = bc.bc_p;
+    bc.edge_y.assign((size_t)neb * K, 0.0);
+    bc.role.assign(neb, ROLE_NONE);
+    for (int e = 0; e < neb; ++e) {
+        const auto y = edge_y(m, B, e);
+        std::copy(y.begin(), y.end(), bc.edge_y.begin() + (size_t)e * K);
+    }
+    auto fill = [&](std::vector<double>& a, int e, double v) { std::fill_n(a.begin() + (size_t)e * K, K, v); };
+    const int pt = in.problem_type;
+    if (pt == 1) {  // lid-driven cavity (src/HO_2D.cpp:700-727)
+        std::fill(bc.noslip.begin(), bc.noslip.end(), 1);
+        std::fill(bc.sw_p.begin(), bc.sw_p.end(), DIRICHLET);
+        std::fill(bc.sw_d.begin(), bc.sw_d.end(), NEUMANN);
+        for (int g = 0; g < ng; ++g)
+            if (m.group_names[g] == "top")
+                for (int e : m.group_edges[g]) fill(bc.bc_pv, e, -1.0);
+    } else {  // backward-facing step (729-817) and flow over an object (819-906)
+        bool have_inlet = false;
+        for (int g = 0; g < ng; ++g) {
+            if (m.group_names[g] != "inlet" || m.group_edges[g].empty()) continue;
+            have_inlet = true;
+            const int n0 = m.edge_nodes[m.group_edges[g][0]][0];
+            bc.y_min = bc.y_max = m.node_xy[2 * n0 + 1];
+            for (int e : m.group_edges[g])
+                for (int c = 0; c < 2; ++c) {
+                    const double y = m.node_xy[2 * m.edge_nodes[e][c] + 1];
+                    bc.y_min = std::min(bc.y_min, y);
+                    bc.y_max = std::max(bc.y_max, y);
+                }
+        }
+        (void)have_inlet;
+        const double ymin = bc.y_min, ymax = bc.y_max, h2 = (ymax - ymin) * (ymax - ymin);
+        for (int g = 0; g < ng; ++g) {
+            const std::string& nm = m.group_names[g];
+            for (int e : m.group_edges[g]) {
+                const double* y = &bc.edge_y[(size_t)e * K];
+                if (nm == "inlet") {
+                    bc.sw_d[e] = DIRICHLET;
+                    bc.sw_p[e] = DIRICHLET;
+                    bc.role[e] = ROLE_INLET;
+                    for (int k = 0; k < K; ++k) {
+                        const size_t q = (size_t)e * K + k;
+                        if (pt == 2) {
+                            bc.bc_p[q] = (y[k] - ymin) * (y[k] - ymin) * (3.0 * ymax - ymin - 2.0 * y[k]) / h2;
+                            bc.bc_d[q] = 6.0 * (2.0 * y[k] - ymin - ymax) / h2;
+                            bc.bc_nv[q] = 6.0 * (y[k] - ymin) * (y[k] - ymax) / h2;
+                        } else {
+                            bc.bc_p[q] = y[k] - ymin;
+                            bc.bc_d[q] = 0.0;
+                            bc.bc_nv[q] = -1.0;
+                        }
+                    }
+                } else if (nm == "outlet") {
+                    bc.sw_d[e] = NEUMANN;
+                    bc.sw_p[e] = NEUMANN;
+                    fill(bc.bc_d, e, 0.0);
+                    fill(bc.bc_p, e, 0.0);
+                } else if (nm == "top" || nm == "bottom") {
+                    bc.sw_p[e] = DIRICHLET;
+                    bc.sw_d[e] = NEUMANN;
+                    bc.role[e] = nm == "top" ? ROLE_TOP : ROLE_BOTTOM;
+                    fill(bc.bc_p, e, nm == "top" ? ymax - ymin : 0.0);
+                    fill(bc.bc_nv, e, 0.0);
+                    fill(bc.bc_pv, e, pt == 2 ? 0.0 : (nm == "top" ? -1.0 : 1.0));
+                } else if (nm == "object" && pt == 3) {
+                    bc.sw_p[e] = DIRICHLET;
+                    bc.sw_d[e] = NEUMANN;
+                    bc.role[e] = ROLE_OBJECT;
+                    fill(bc.bc_p, e, 0.5 * (ymax - ymin));
+                    fill(bc.bc_nv, e, 0.0);
+                    fill(bc.bc_pv, e, 0.0);
+                }
+            }
+            if (nm == "inlet" || nm == "outlet") bc.noslip[g] = 0;
+            else if (nm == "top" || nm == "bottom") bc.noslip[g] = pt == 2 ? 1 : 0;
+            else if (nm == "object" && pt == 3) bc.noslip[g] = 1;
+        }
+    }
+    // outward normal values into the local h direction (src/HO_2D.cpp:1228-1237)
+    for (int e = 0; e < neb; ++e) {
+        const int ijp = kF2I[m.be_side[e]];
+        const double sign = 2.0 * (ijp % 2) - 1.0;
+        for (int k = 0; k < K; ++k) {
+            bc.bc_nv[(size_t)e * K + k] *= sign;
+            if (bc.sw_d[e] == NEUMANN) bc.bc_d[(size_t)e * K + k] *= sign;
+        }
+    }
+    return {0, ""};
+}
+
+namespace {
+
+struct Entry {
+    int row, g;
+    double c;
+};
+
+// Element-interior coupling: Lc[ij][rs] += c * G[el][b][a][r][d] (src/HO_2D.cpp:1567-1596).
+std::vector<Entry> volume_entries(const Bases& B) {
+    const int K = B.K, K2 = K * K;
+    std::vector<Entry> out;
+    for (int j = 0; j < K; ++j)
+        for (int i = 0; i < K; ++i)
+            for (int m = 0; m < K; ++m)
+                for (int r = 0; r < 2; ++r) {
+                    const int a = m * (1 - r) + i * r, b = m * r + j * (1 - r);
+                    const int cr = j * r + i * (1 - r);
+                    const double tmp3 = B.sbb[m * 2] * B.gR[cr * 2] + B.sbb[m * 2 + 1] * B.gR[cr * 2 + 1];
+                    const double sn = B.D[m * K + i * (1 - r) + j * r];
+                    for (int d = 0; d < 2; ++d) {
+                        const int t1 = a * (1 - d) + b * d;
+                        for (int p = 0; p < K; ++p) {
+                            const int rs = (p * d + b * (1 - d)) * K + (p * (1 - d) + a * d);
+                            const double tmp2 = 0.5 * (B.sbb[p * 2] * B.gR[t1 * 2] + B.sbb[p * 2 + 1] * B.gR[t1 * 2 + 1]);
+                            const double c = sn * (B.D[p * K + t1] - tmp2) + tmp3 * (-B.D[p * K + t1] + tmp2);
+                            out.push_back({(j * K + i) * K2 + rs, ((b * K + a) * 2 + r) * 2 + d, c});
+                        }
+                    }
+                }
+    return out;
+}
+
+// Face weights W[ij][q] = sum c * G[el][b][a][r][d] for face (d, t) (src/HO_2D.cpp:1614-1637).
+std::vector<Entry> face_entries(const Bases& B, int d, int t) {
+    const int K = B.K;
+    std::vector<Entry> out;
+    for (int j = 0; j < K; ++j)
+        for (int i = 0; i < K; ++i)
+            for (int m = 0; m < K; ++m)
+                for (int r = 0; r < 2; ++r) {
+                    const int a = m * (1 - r) + i * r, b = m * r + j * (1 - r);
+                    const int q = a * d + b * (1 - d);
+                    const int cr = j * r + i * (1 - r);
+                    const double sn = B.D[m * K + i * (1 - r) + j * r];
+                    const double ngr = B.gR[(a * (1 - d) + b * d) * 2 + t];
+                    const double tmp2 = B.sbb[m * 2] * B.gR[cr * 2] + B.sbb[m * 2 + 1] * B.gR[cr * 2 + 1];
+                    out.push_back({(j * K + i) * K + q, ((b * K + a) * 2 + r) * 2 + d, (sn - tmp2) * ngr});
+                }
+    return out;
+}
+
+inline int rs_of(int p, int q, int d, int K) { return (p * d + q * (1 - d)) * K + (p * (1 - d) + q * d); }
+inline int bf_of(int side, int k, int K) { return (side / 2) * (K - 2 * k - 1) + k; }
+
+}  // namespace
+
+void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
+                      PoissonOperator& op) {
+    const int N = mesh.n_el, K = B.K, K2 = K * K, K4 = K2 * K2;
+    op.K2 = K2;
+    op.blocks.assign((size_t)N * 5 * K4, 0.0);
+    op.block_col.assign((size_t)N * 5, -1);
+    op.bsrc.assign((size_t)mesh.n_eb * K2 * K, 0.0);
+    op.dinv.assign((size_t)N * K4, 0.0);
+    const std::vector<Entry> vol = volume_entries(B);
+    std::vector<Entry> fw[2][2];
+    for (int d = 0; d < 2; ++d)
+        for (int t = 0; t < 2; ++t) fw[d][t] = face_entries(B, d, t);
+    const double* gp = B.gp;
+    int64_t nnz = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nnz)
+    for (int el = 0; el < N; ++el) {
+        std::vector<double> Lc(K4, 0.0), Ln(4 * (size_t)K4, 0.0), W(K2 * K), WN(K2 * K), Nm(K * K);
+        const double* G = &M.G[(size_t)el * K2 * 4];
+        for (const Entry& e : vol) Lc[e.row] += e.c * G[e.g];
+        for (int ijp = 0; ijp < 4; ++ijp) {
+            const int d = ijp / 2, t = ijp % 2, side = kI2F[ijp];
+            std::fill(W.begin(), W.end(), 0.0);
+            for (const Entry& e : fw[d][t]) W[e.row] += e.c * G[e.g];
+            const double* GBe = &M.GB[(((size_t)el * 2 + d) * 2 + t) * K * 2];
+            const int eb = mesh.bidx[(size_t)el * 4 + side];
+            if (eb >= 0) {
+                double* bs = &op.bsrc[(size_t)eb * K2 * K];
+                for (int ij = 0; ij < K2; ++ij)
+                    for (int q = 0; q < K; ++q)
+                        for (int p = 0; p < K; ++p) Lc[ij * K2 + rs_of(p, q, d, K)] -= 0.5 * W[ij * K + q] * B.sbb[p * 2 + t];
+                if (bc.sw_p[eb] == DIRICHLET) {
+                    for (int ij = 0; ij < K2; ++ij) {
+                        const int j = ij / K, i = ij % K;
+                        for (int q = 0; q < K; ++q) bs[ij * K + bf_of(side, q, K)] += W[ij * K + q];
+                        const int alpha = i * d + j * (1 - d);
+                        const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
+                        const double A = GBe[alpha * 2 + d], Bc = GBe[alpha * 2 + 1 - d];
+                        for (int mm = 0; mm < K; ++mm)
+                            Lc[ij * K2 + rs_of(mm, alpha, d, K)] += A * (B.sbgb[mm * 2 + t] - gp[t] * B.sbb[mm * 2 + t]) * ngr;
+                        bs[ij * K + bf_of(side, alpha, K)] += A * gp[t] * ngr;
+                        for (int mm = 0; mm < K; ++mm) bs[ij * K + bf_of(side, mm, K)] += Bc * B.D[mm * K + alpha] * ngr;
+                    }
+                } else {  // Neumann face (src/HO_2D.cpp:1660-1714)
+                    for (int r = 0; r < K; ++r) {
+                        for (int c = 0; c < K; ++c) Nm[r * K + c] = -GBe[r * 2 + 1 - d] * B.D[c * K + r];
+                        Nm[r * K + r] += -GBe[r * 2 + d] * gp[t];
+                    }
+                    invert(K, Nm);
+                    const double sign = t ? 1.0 : -1.0;
+                    double s[kMaxK];
+                    for (int p = 0; p < K; ++p) s[p] = std::sqrt(GBe[p * 2 + d] * M.fJ[((size_t)el * 4 + ijp) * K + p]);
+                    for (int ij = 0; ij < K2; ++ij)
+                        for (int c = 0; c < K; ++c) {
+                            double acc = 0.0;
+                            for (int q = 0; q < K; ++q) acc += W[ij * K + q] * Nm[q * K + c];
+                            WN[ij * K + c] = acc;
+                        }
+                    for (int ij = 0; ij < K2; ++ij) {
+                        const int j = ij / K, i = ij % K;
+                        const int alpha = i * d + j * (1 - d);
+                        const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
+                        bs[ij * K + bf_of(side, alpha, K)] += sign * ngr * s[alpha];
+                        for (int p = 0; p < K; ++p) {
+                            bs[ij * K + bf_of(side, p, K)] -= sign * WN[ij * K + p] * s[p];
+                            const double tmp4 = B.sbgb[p * 2 + t] - gp[t] * B.sbb[p * 2 + t];
+                            for (int c = 0; c < K; ++c)
+                                Lc[ij * K2 + rs_of(p, c, d, K)] += WN[ij * K + c] * tmp4 * GBe[c * 2 + d];
+                        }
+                    }
+                }
+            } else {  // interior face (src/HO_2D.cpp:1716-1792)
+                const int eln = mesh.nbr[(size_t)el * 4 + side];
+                const int ijpm = kF2I[mesh.nbr_side[(size_t)el * 4 + side]];
+                const int dn = ijpm / 2, tn = ijpm % 2;
+                const int rev = (d + t + dn + tn + 1) % 2;
+                double* L = &Ln[(size_t)ijp * K4];
+                for (int ij = 0; ij < K2; ++ij)
+                    for (int q = 0; q < K; ++q) {
+                        const int Mq = rev * (K - 2 * q - 1) + q;
+                        for (int p = 0; p < K; ++p) L[ij * K2 + rs_of(p, Mq, dn, K)] += 0.5 * W[ij * K + q] * B.sbb[p * 2 + tn];
+                    }
+                const double* GBn = &M.GB[(((size_t)eln * 2 + dn) * 2 + tn) * K * 2];
+                const double sign = (t == tn) ? -1.0 : 1.0;
+                for (int ij = 0; ij < K2; ++ij) {
+                    const int j = ij / K, i = ij % K;
+                    const int alpha = i * d + j * (1 - d);
+                    const int Ma = rev * (K - 2 * alpha - 1) + alpha;
+                    const double A = GBe[alpha * 2 + d], Bc = GBe[alpha * 2 + 1 - d];
+                    const double An = GBn[Ma * 2 + dn], Bn = GBn[Ma * 2 + 1 - dn];
+                    const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
+                    for (int mm = 0; mm < K; ++mm) {
+                        const int Mm = rev * (K - 2 * mm - 1) + mm;
+                        Lc[ij * K2 + rs_of(mm, alpha, d, K)] +=
+                            (0.5 * A * B.sbgb[mm * 2 + t] - 0.25 * gp[t] * A * B.sbb[mm * 2 + t] +
+                             0.25 * sign * gp[tn] * An * B.sbb[mm * 2 + t]) * ngr;
+                        L[ij * K2 + rs_of(mm, Ma, dn, K)] +=
+                            (0.5 * sign * An * B.sbgb[mm * 2 + tn] - 0.25 * sign * gp[tn] * An * B.sbb[mm * 2 + tn] +
+                             0.25 * gp[t] * A * B.sbb[mm * 2 + tn]) * ngr;
+                        const double coeff = 0.25 * (Bc * B.D[mm * K + alpha] + sign * Bn * B.D[Mm * K + Ma]) * ngr;
+                        for (int p = 0; p < K; ++p) {
+                            Lc[ij * K2 + rs_of(p, mm, d, K)] += coeff * B.sbb[p * 2 + t];
+                            L[ij * K2 + rs_of(p, Mm, dn, K)] += coeff * B.sbb[p * 2 + tn];
+                        }
+                    }
+                }
+                op.block_col[(size_t)el * 5 + 1 + ijp] = eln;
+            }
+        }
+        op.block_col[(size_t)el * 5] = el;
+        // filter and store transposed: blocks[el][slot][rs][ij]
+        auto store = [&](const double* src, int slot) {
+            double* dst = &op.blocks[((size_t)el * 5 + slot) * K4];
+            int64_t cnt = 0;
+            for (int ij = 0; ij < K2; ++ij)
+                for (int rs = 0; rs < K2; ++rs) {
+                    double v = src[ij * K2 + rs];
+                    if (!(std::fabs(v) > 1e-14)) v = 0.0;
+                    else ++cnt;
+                    dst[rs * K2 + ij] = v;
+                }
+            return cnt;
+        };
+        nnz += store(Lc.data(), 0);
+        for (int ijp = 0; ijp < 4; ++ijp)
+            if (op.block_col[(size_t)el * 5 + 1 + ijp] >= 0) nnz += store(&Ln[(size_t)ijp * K4], 1 + ijp);
+        // inverse of the filtered diagonal block, stored transposed like the blocks
+        std::vector<double> Dm(K4);
+        const double* blk = &op.blocks[((size_t)el * 5) * K4];
+        for (int ij = 0; ij < K2; ++ij)
+            for (int rs = 0; rs < K2; ++rs) Dm[ij * K2 + rs] = blk[rs * K2 + ij];
+        invert(K2, Dm);
+        double* di = &op.dinv[(size_t)el * K4];
+        for (int ij = 0; ij < K2; ++ij)
+            for (int rs = 0; rs < K2; ++rs) di[rs * K2 + ij] = Dm[ij * K2 + rs];
+    }
+    op.nnz = nnz;
+}
+
+}  // namespace ho2d

@@ -1,0 +1,654 @@
+// solver.cu -- device state and the stage / step / Poisson drivers.
+//
+// One stage (src/HO_2D.cpp:1806-1839) on the device:
+//   bc_update      update_BCs(t + c dt)                     (1979-2217)
+//   poisson_rhs    RHS of solve_Poisson                    (1881-1900)
+//   Krylov solve   replaces (*AMGCL_solver)(RHS, x)         (1960), warm start = last psi
+//   trace + velocity   calc_velocity_vector_from_streamfunction + update_diffusion_BC
+//   residual       calc_RHS_diffusion + update_advection_BC + calc_RHS_advection[_continuous]
+//                  + k = dt (adv + diff) + the RK combination of solve_advection_diffusion
+// Nothing crosses PCIe inside a step except the Krylov convergence flag polled by the host.
+#include <cmath>
+#include <cstring>
+
+#include "device.cuh"
+#include "fr_launch.hpp"
+#include "solver.hpp"
+
+namespace ho2d {
+
+cudaError_t DeviceBuffer::alloc(size_t bytes) {
+    reset();
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p_, bytes);
+    if (e == cudaSuccess) n_ = bytes;
+    else p_ = nullptr;
+    return e;
+}
+
+void DeviceBuffer::reset() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+}
+
+struct DeviceState {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+    // connectivity and boundary tables
+    DeviceBuffer face_nb, face_nijp, be_group, sw_p, sw_d, noslip, role, be_ijp;
+    DevBases<double> b64;
+    DevBases<float> b32;
+    // metrics: xxi, xeta, yxi, yeta, J, fA, fB, fJ, fAn
+    DeviceBuffer m64[9], m32[9];
+    bool have32 = false;
+    // boundary arrays (double)
+    DeviceBuffer bc_p, bc_nv, bc_pv, bc_d, bc_w, vjump, bc_adv, edge_y, bsrc;
+    // fields
+    DeviceBuffer omega, acc, psi64, rhs, rres;
+    DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
+    // Poisson operator and Krylov workspace
+    DeviceBuffer A64, dinv64, bcol, A32, dinv32;
+    DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
+    DeviceBuffer partials, counter, scalars;
+    KrylovScalars* h_sc = nullptr;
+
+    ~DeviceState() {
+        if (h_sc) cudaFreeHost(h_sc);
+        for (cudaEvent_t e : {ev0, ev1, evp0, evp1})
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <typename T>
+DevBases<T> make_dev_bases(const Bases& B) {
+    DevBases<T> d;
+    std::memset(&d, 0, sizeof(d));
+    for (int i = 0; i < B.K * B.K; ++i) d.D[i] = T(B.D[i]);
+    for (int i = 0; i < B.K * 2; ++i) {
+        d.sbb[i] = T(B.sbb[i]);
+        d.sbgb[i] = T(B.sbgb[i]);
+        d.R[i] = T(B.R[i]);
+        d.gR[i] = T(B.gR[i]);
+    }
+    d.gp[0] = T(B.gp[0]);
+    d.gp[1] = T(B.gp[1]);
+    return d;
+}
+
+template <typename T>
+cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& h) {
+    cudaError_t e = buf.alloc(h.size() * sizeof(T));
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpy(buf.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <typename T>
+cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
+    std::vector<T> c(h.begin(), h.end());
+    return upload(buf, c);
+}
+
+}  // namespace
+
+Solver::Solver() : d_(new DeviceState) {}
+Solver::~Solver() = default;
+
+Error Solver::cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return {0, ""};
+    return {5, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+#define HO2D_TRY(expr)                 \
+    do {                               \
+        Error _e = (expr);             \
+        if (_e.code) return _e;        \
+    } while (0)
+#define HO2D_CUDA(call, what) HO2D_TRY(cuda((call), what))
+
+Error Solver::read_input(const std::string& path) {
+    Input in;
+    Error e = ho2d::read_input(path, in);
+    if (e.code) return e;
+    in_ = in;
+    input_done_ = true;
+    setup_done_ = false;
+    return {0, ""};
+}
+
+Error Solver::setup() {
+    if (!input_done_) return {1, "ho2d_setup called before ho2d_read_input"};
+    std::string mesh_path = in_.mesh_file;
+    if (!mesh_path.empty() && mesh_path[0] != '/') mesh_path = in_.base_dir + "/" + mesh_path;
+    mesh_ = Mesh();
+    HO2D_TRY(read_msh(mesh_path, in_.occ, mesh_));
+    HO2D_TRY(make_bases(in_.knod, mesh_.lnod, B_));
+    make_metrics(mesh_, B_, M_);
+    for (double j : M_.J)
+        if (!(j > 0.0)) return {3, "non-positive element Jacobian: check the element orientation"};
+    HO2D_TRY(setup_bcs(in_, mesh_, B_, bc_));
+    assemble_poisson(mesh_, B_, M_, bc_, op_);
+
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
+    if (!d.stream) HO2D_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* e : {&d.ev0, &d.ev1, &d.evp0, &d.evp1})
+        if (!*e) HO2D_CUDA(cudaEventCreate(e), "cudaEventCreate");
+    if (!d.h_sc) HO2D_CUDA(cudaMallocHost(&d.h_sc, sizeof(KrylovScalars)), "cudaMallocHost");
+
+    const int N = mesh_.n_el, K = in_.knod, K2 = K * K, neb = mesh_.n_eb;
+    const size_t nv = (size_t)N * K2, nf = (size_t)N * 4 * K;
+    // connectivity in ijp order
+    std::vector<int> fnb((size_t)N * 4), fnijp((size_t)N * 4), beijp(neb);
+    for (int el = 0; el < N; ++el)
+        for (int ijp = 0; ijp < 4; ++ijp) {
+            const int side = kI2F[ijp];
+            const int nb = mesh_.nbr[(size_t)el * 4 + side];
+            if (nb >= 0) {
+                fnb[(size_t)el * 4 + ijp] = nb;
+                fnijp[(size_t)el * 4 + ijp] = kF2I[mesh_.nbr_side[(size_t)el * 4 + side]];
+            } else {
+                fnb[(size_t)el * 4 + ijp] = -(mesh_.bidx[(size_t)el * 4 + side] + 1);
+                fnijp[(size_t)el * 4 + ijp] = -1;
+            }
+        }
+    for (int e = 0; e < neb; ++e) beijp[e] = kF2I[mesh_.be_side[e]];
+    HO2D_CUDA(upload(d.face_nb, fnb), "upload");
+    HO2D_CUDA(upload(d.face_nijp, fnijp), "upload");
+    HO2D_CUDA(upload(d.be_group, mesh_.be_group), "upload");
+    HO2D_CUDA(upload(d.sw_p, bc_.sw_p), "upload");
+    HO2D_CUDA(upload(d.sw_d, bc_.sw_d), "upload");
+    HO2D_CUDA(upload(d.noslip, bc_.noslip.empty() ? std::vector<int>{0} : bc_.noslip), "upload");
+    HO2D_CUDA(upload(d.role, bc_.role), "upload");
+    HO2D_CUDA(upload(d.be_ijp, beijp), "upload");
+    d.b64 = make_dev_bases<double>(B_);
+    d.b32 = make_dev_bases<float>(B_);
+    const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
+    for (int i = 0; i < 9; ++i) HO2D_CUDA(upload(d.m64[i], *mets[i]), "upload metrics");
+    d.have32 = false;
+    HO2D_CUDA(upload(d.bc_p, bc_.bc_p), "upload");
+    HO2D_CUDA(upload(d.bc_nv, bc_.bc_nv), "upload");
+    HO2D_CUDA(upload(d.bc_pv, bc_.bc_pv), "upload");
+    HO2D_CUDA(upload(d.bc_d, bc_.bc_d), "upload");
+    HO2D_CUDA(upload(d.edge_y, bc_.edge_y), "upload");
+    HO2D_CUDA(upload(d.bsrc, op_.bsrc), "upload");
+    const std::vector<double> zb((size_t)neb * K, 0.0);
+    HO2D_CUDA(upload(d.bc_w, zb), "upload");
+    HO2D_CUDA(upload(d.vjump, zb), "upload");
+    HO2D_CUDA(upload(d.bc_adv, zb), "upload");
+    // fields (typed fields sized for double so either precision fits)
+    const std::vector<double> zv(nv, 0.0);
+    for (DeviceBuffer* b : {&d.omega, &d.acc, &d.psi64, &d.rhs, &d.rres, &d.w_stage, &d.psiT, &d.u, &d.v, &d.rhs_diff,
+                            &d.rhs_adv, &d.kout})
+        HO2D_CUDA(upload(*b, zv), "alloc fields");
+    const std::vector<double> zf(nf, 0.0);
+    for (DeviceBuffer* b : {&d.psi_tv, &d.psi_tg, &d.w_tv, &d.w_tg, &d.U_t}) HO2D_CUDA(upload(*b, zf), "alloc traces");
+    // Poisson operator
+    HO2D_CUDA(upload(d.A64, op_.blocks), "upload Poisson blocks");
+    HO2D_CUDA(upload(d.dinv64, op_.dinv), "upload block-Jacobi");
+    HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
+    d.A32.reset();
+    d.dinv32.reset();
+    for (auto& b : d.kv) HO2D_CUDA(upload(b, zv), "alloc Krylov");
+    const int mb = krylov_max_blocks(K, N);
+    HO2D_CUDA(upload(d.partials, std::vector<double>((size_t)4 * mb, 0.0)), "alloc partials");
+    HO2D_CUDA(upload(d.counter, std::vector<unsigned>(1, 0u)), "alloc counter");
+    HO2D_CUDA(d.scalars.alloc(sizeof(KrylovScalars)), "alloc scalars");
+    HO2D_CUDA(cudaMemset(d.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
+    time_ = 0.0;
+    setup_done_ = true;
+    if (mixed_) HO2D_TRY(upload_precision_arrays());
+    HO2D_CUDA(cudaDeviceSynchronize(), "setup");
+    return {0, ""};
+}
+
+Error Solver::upload_precision_arrays() {
+    DeviceState& d = *d_;
+    if (d.have32) return {0, ""};
+    const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
+    for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
+    HO2D_CUDA(upload_as<float>(d.A32, op_.blocks), "upload fp32 blocks");
+    HO2D_CUDA(upload_as<float>(d.dinv32, op_.dinv), "upload fp32 block-Jacobi");
+    d.have32 = true;
+    return {0, ""};
+}
+
+Error Solver::set_precision(int mode) {
+    if (mode != 0 && mode != 1) return {1, "precision must be HO2D_FP64 (0) or HO2D_MIXED (1)"};
+    const bool was = mixed_;
+    mixed_ = mode == 1;
+    if (setup_done_ && mixed_ != was) {
+        if (mixed_) HO2D_TRY(upload_precision_arrays());
+        // re-derive the stage input in the new precision from the FP64 vorticity
+        DeviceState& d = *d_;
+        const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+        if (mixed_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
+        else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    }
+    return {0, ""};
+}
+
+// ------------------------------------------------------------------ Poisson
+Error Solver::poisson_solve() {
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t nv = (size_t)N * K * K;
+    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
+    if (timing_) HO2D_CUDA(cudaEventRecord(d.evp0, d.stream), "event");
+    auto poll = [&]() -> Error {
+        HO2D_CUDA(cudaMemcpyAsync(d.h_sc, d.scalars.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream),
+                  "poll");
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "poll");
+        return {0, ""};
+    };
+    // runs BiCGSTAB to completion on (A, v); returns iterations
+    auto run = [&](auto A, auto v, double tol, int& iters) -> Error {
+        HO2D_CUDA(krylov_init(A, v, rs, tol, d.stream), "krylov init");
+        launches_ += 2;
+        HO2D_TRY(poll());
+        int chunk = std::max(1, prev_iters_ - 1);
+        while (!d.h_sc->done) {
+            for (int c = 0; c < chunk; ++c) {
+                HO2D_CUDA(krylov_iteration(A, v, rs, max_iter_, d.stream), "krylov iteration");
+                launches_ += 6;
+            }
+            HO2D_TRY(poll());
+            chunk = 2;
+        }
+        iters = d.h_sc->it;
+        return {0, ""};
+    };
+    last_iters_ = 0;
+    if (!mixed_) {
+        BsrOp<double> A{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
+        BicgVectors<double> v{d.psi64.as<double>(), d.kv[0].as<double>(), d.kv[1].as<double>(), d.kv[2].as<double>(),
+                              d.kv[3].as<double>(), d.kv[4].as<double>(), d.kv[5].as<double>(), d.kv[6].as<double>(),
+                              d.kv[7].as<double>(), d.rhs.as<double>()};
+        int it = 0;
+        HO2D_TRY(run(A, v, tol_, it));
+        last_iters_ = it;
+        last_res_ = d.h_sc->bnorm2 > 0 ? std::sqrt(d.h_sc->rnorm2 / d.h_sc->bnorm2) : 0.0;
+    } else {
+        // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator
+        BsrOp<double> A64{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
+        BsrOp<float> A32{N, K, d.A32.as<float>(), d.bcol.as<int>(), d.dinv32.as<float>()};
+        BicgVectors<float> v{d.kv[8].as<float>(), d.kv[0].as<float>(), d.kv[1].as<float>(), d.kv[2].as<float>(),
+                             d.kv[3].as<float>(), d.kv[4].as<float>(), d.kv[5].as<float>(), d.kv[6].as<float>(),
+                             d.kv[7].as<float>(), d.kv[9].as<float>()};
+        for (int sweep = 0; sweep < 20; ++sweep) {
+            HO2D_CUDA(residual_fp64(A64, d.rhs.as<double>(), d.psi64.as<double>(), d.rres.as<double>(), rs, d.stream),
+                      "fp64 residual");
+            launches_ += 1;
+            HO2D_TRY(poll());
+            const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
+            last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
+            if (bn == 0.0) {
+                HO2D_CUDA(cudaMemsetAsync(d.psi64.get(), 0, nv * 8, d.stream), "memset");
+                last_res_ = 0.0;
+                break;
+            }
+            if (!(rn == rn)) break;  // NaN: reported by the caller
+            if (rn <= tol_ * tol_ * bn || last_iters_ >= max_iter_) break;
+            HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
+            HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
+            launches_ += 1;
+            int it = 0;
+            HO2D_TRY(run(A32, v, 1e-5, it));
+            last_iters_ += it;
+            HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
+            launches_ += 1;
+        }
+    }
+    prev_iters_ = std::max(1, mixed_ ? last_iters_ / 2 : last_iters_);
+    if (timing_) {
+        HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");
+        HO2D_CUDA(cudaEventSynchronize(d.evp1), "event");
+        float ms = 0.f;
+        HO2D_CUDA(cudaEventElapsedTime(&ms, d.evp0, d.evp1), "event");
+        poisson_ms_acc_ += ms;
+    }
+    if (!(last_res_ == last_res_)) return {7, "non-finite values in the Poisson solve (vorticity blew up)"};
+    return {0, ""};
+}
+
+// ------------------------------------------------------------------ stages
+template <typename T>
+static FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
+    DeviceBuffer* mm = f32 ? d.m32 : d.m64;
+    FrGeom<T> g;
+    g.N = m.n_el;
+    g.n_eb = m.n_eb;
+    g.face_nb = d.face_nb.as<int>();
+    g.face_nijp = d.face_nijp.as<int>();
+    g.xxi = mm[0].as<T>();
+    g.xeta = mm[1].as<T>();
+    g.yxi = mm[2].as<T>();
+    g.yeta = mm[3].as<T>();
+    g.J = mm[4].as<T>();
+    g.fA = mm[5].as<T>();
+    g.fB = mm[6].as<T>();
+    g.fJ = mm[7].as<T>();
+    g.fAn = mm[8].as<T>();
+    g.be_group = d.be_group.as<int>();
+    g.sw_p = d.sw_p.as<int>();
+    g.sw_d = d.sw_d.as<int>();
+    g.noslip = d.noslip.as<int>();
+    return g;
+}
+
+template <typename T>
+Error Solver::stage_t(double coeff, int rk_stage, bool update) {
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t nv = (size_t)N * K * K;
+    const bool f32 = sizeof(T) == 4;
+    const DevBases<T>& b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
+    const FrGeom<T> g = geom_of<T>(d, mesh_, f32);
+    BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
+                d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
+    const double t = time_ + coeff * in_.dt;
+    const double tc = 2.0 * std::fabs(std::sin(M_PI / 40.0 * t));
+    HO2D_CUDA(launch_bc_update(mesh_.n_eb, K, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
+                               d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, d.stream),
+              "bc_update");
+    HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
+                                    d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
+              "poisson_rhs");
+    launches_ += 2;
+    HO2D_TRY(poisson_solve());
+    const T* psi = f32 ? d.psiT.as<T>() : reinterpret_cast<const T*>(d.psi64.get());
+    if (f32) {
+        HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), nv, d.stream), "d2f");
+        launches_ += 1;
+    }
+    HO2D_CUDA(launch_trace<T>(K, N, psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), b, d.stream), "trace");
+    VelocityArgs<T> va{psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), d.w_stage.as<T>(), d.u.as<T>(), d.v.as<T>(),
+                       d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
+    HO2D_CUDA(launch_velocity<T>(K, g, b, bc, va, d.stream), "velocity");
+    ResidualArgs<T> ra;
+    ra.w = d.w_stage.as<T>();
+    ra.u = d.u.as<T>();
+    ra.v = d.v.as<T>();
+    ra.w_tv = d.w_tv.as<T>();
+    ra.w_tg = d.w_tg.as<T>();
+    ra.U_t = d.U_t.as<T>();
+    ra.dt = in_.dt;
+    ra.re_inv = in_.reyn_inv;
+    ra.adv_type = in_.adv_type;
+    ra.ti_type = update ? in_.ti_type : 0;
+    ra.stage = rk_stage;
+    ra.omega = d.omega.as<double>();
+    ra.acc = d.acc.as<double>();
+    ra.w_next = update ? d.w_stage.as<T>() : nullptr;
+    ra.rhs_diff = update ? nullptr : d.rhs_diff.as<T>();
+    ra.rhs_adv = update ? nullptr : d.rhs_adv.as<T>();
+    ra.k_out = update ? nullptr : d.kout.as<T>();
+    HO2D_CUDA(launch_residual<T>(K, g, b, bc, ra, d.stream), "residual");
+    launches_ += 3;
+    return {0, ""};
+}
+
+template <typename T>
+Error Solver::velocity_only_t() {
+    // update_BCs(t) + solve_Poisson(vorticity) + velocity, as at dump steps (src/HO_2D.cpp:1411-1416)
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t nv = (size_t)N * K * K;
+    const bool f32 = sizeof(T) == 4;
+    const DevBases<T>& b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
+    const FrGeom<T> g = geom_of<T>(d, mesh_, f32);
+    BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
+                d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
+    const double tc = 2.0 * std::fabs(std::sin(M_PI / 40.0 * time_));
+    HO2D_CUDA(launch_bc_update(mesh_.n_eb, K, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
+                               d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, d.stream),
+              "bc_update");
+    HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
+                                    d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
+              "poisson_rhs");
+    HO2D_TRY(poisson_solve());
+    const T* psi = f32 ? d.psiT.as<T>() : reinterpret_cast<const T*>(d.psi64.get());
+    if (f32) HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), nv, d.stream), "d2f");
+    HO2D_CUDA(launch_trace<T>(K, N, psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), b, d.stream), "trace");
+    VelocityArgs<T> va{psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), d.w_stage.as<T>(), d.u.as<T>(), d.v.as<T>(),
+                       d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
+    HO2D_CUDA(launch_velocity<T>(K, g, b, bc, va, d.stream), "velocity");
+    launches_ += 4 + (f32 ? 1 : 0);
+    return {0, ""};
+}
+
+Error Solver::stage_impl(double coeff, int rk_stage, bool update) {
+    return mixed_ ? stage_t<float>(coeff, rk_stage, update) : stage_t<double>(coeff, rk_stage, update);
+}
+
+Error Solver::step(int nsteps) {
+    if (!setup_done_) return {1, "ho2d_step called before ho2d_setup"};
+    if (nsteps < 0) return {1, "nsteps must be non-negative"};
+    HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
+    static const double c4[4] = {0.0, 0.5, 0.5, 1.0};
+    static const double c2[2] = {0.0, 1.0};
+    const int ns = in_.ti_type == 4 ? 4 : (in_.ti_type == 2 ? 2 : 1);
+    const double* c = in_.ti_type == 4 ? c4 : c2;
+    for (int i = 0; i < nsteps; ++i) {
+        for (int s = 0; s < ns; ++s) HO2D_TRY(stage_impl(c[s], s, true));
+        time_ += in_.dt;
+    }
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "step");
+    HO2D_CUDA(cudaGetLastError(), "step");
+    return {0, ""};
+}
+
+Error Solver::stage(double coeff) {
+    if (!setup_done_) return {1, "ho2d_stage called before ho2d_setup"};
+    HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
+    HO2D_TRY(stage_impl(coeff, 0, false));
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "stage");
+    return {0, ""};
+}
+
+Error Solver::solve() {
+    if (!setup_done_) return {1, "ho2d_solve called before ho2d_setup"};
+    HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
+    const int nt = in_.num_steps, df = std::max(1, in_.dump_freq);
+    for (int ti = 0; ti < nt; ++ti) {
+        if (ti % df == 0) HO2D_TRY(mixed_ ? velocity_only_t<float>() : velocity_only_t<double>());
+        HO2D_TRY(step(1));
+    }
+    if (nt % df == 0) HO2D_TRY(mixed_ ? velocity_only_t<float>() : velocity_only_t<double>());
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "solve");
+    return {0, ""};
+}
+
+Error Solver::solveto(double outerdt, int numstep, int integtype, double reyn) {
+    // src/HO_2D.cpp:4194-4233 for the non-hybrid problem types
+    if (!setup_done_) return {1, "ho2d_solveto called before ho2d_setup"};
+    if (numstep <= 0 || !(outerdt > 0.0)) return {1, "solveto needs numstep > 0 and outerdt > 0"};
+    if (integtype != 1 && integtype != 2 && integtype != 4) return {4, "integtype must be 1, 2 or 4"};
+    in_.dt = outerdt / numstep;
+    in_.ti_type = integtype;
+    in_.reyn_inv = reyn > 1e-3 ? 1.0 / reyn : -1.0;
+    return step(numstep);
+}
+
+Error Solver::time_steps(int nsteps, double* total_ms, double* poisson_ms) {
+    if (!setup_done_) return {1, "ho2d_time_steps called before ho2d_setup"};
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    timing_ = true;
+    poisson_ms_acc_ = 0.0;
+    HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+    Error e = step(nsteps);
+    timing_ = false;
+    HO2D_TRY(e);
+    HO2D_CUDA(cudaEventRecord(d.ev1, d.stream), "event");
+    HO2D_CUDA(cudaEventSynchronize(d.ev1), "event");
+    float ms = 0.f;
+    HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
+    if (total_ms) *total_ms = ms;
+    if (poisson_ms) *poisson_ms = poisson_ms_acc_;
+    return {0, ""};
+}
+
+// Average duration of the Poisson SpMV kernel (the solver's own k_spmv_v) over `reps`
+// launches between CUDA events on the handle's stream, and its algorithmic bytes per
+// launch: every stored block entry once, x and rhat once per element row, v written once,
+// the block-column table once.
+Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
+    if (!setup_done_) return {1, "not set up"};
+    if (reps <= 0) return {1, "reps must be positive"};
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t K2 = (size_t)K * K;
+    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
+    size_t nblocks = 0;
+    for (int c : op_.block_col) nblocks += c >= 0;
+    const size_t w = mixed_ ? 4 : 8;
+    if (bytes) *bytes = double(nblocks * K2 * K2 * w + 3 * (size_t)N * K2 * w + op_.block_col.size() * 4);
+    HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+    if (!mixed_) {
+        BsrOp<double> A{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
+        BicgVectors<double> v{d.psi64.as<double>(), d.kv[0].as<double>(), d.kv[1].as<double>(), d.kv[2].as<double>(),
+                              d.kv[3].as<double>(), d.kv[4].as<double>(), d.kv[5].as<double>(), d.kv[6].as<double>(),
+                              d.kv[7].as<double>(), d.rhs.as<double>()};
+        HO2D_CUDA(krylov_spmv_only(A, v, rs, reps, d.stream), "spmv");
+    } else {
+        BsrOp<float> A{N, K, d.A32.as<float>(), d.bcol.as<int>(), d.dinv32.as<float>()};
+        BicgVectors<float> v{d.kv[8].as<float>(), d.kv[0].as<float>(), d.kv[1].as<float>(), d.kv[2].as<float>(),
+                             d.kv[3].as<float>(), d.kv[4].as<float>(), d.kv[5].as<float>(), d.kv[6].as<float>(),
+                             d.kv[7].as<float>(), d.kv[9].as<float>()};
+        HO2D_CUDA(krylov_spmv_only(A, v, rs, reps, d.stream), "spmv");
+    }
+    HO2D_CUDA(cudaEventRecord(d.ev1, d.stream), "event");
+    HO2D_CUDA(cudaEventSynchronize(d.ev1), "event");
+    float ms = 0.f;
+    HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
+    if (avg_ms) *avg_ms = ms / reps;
+    return {0, ""};
+}
+
+// ------------------------------------------------------------------ data access
+Error Solver::get_volume(int which, double* out) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    const void* src = nullptr;
+    bool typed = false;
+    switch (which) {
+        case 0: src = d.omega.get(); break;
+        case 1: src = d.psi64.get(); break;
+        case 2: src = d.rhs_diff.get(); typed = true; break;
+        case 3: src = d.rhs_adv.get(); typed = true; break;
+        case 4: src = d.kout.get(); typed = true; break;
+        case 5:
+            std::copy(M_.J.begin(), M_.J.end(), out);
+            return {0, ""};
+        default: return {1, "unknown field"};
+    }
+    if (typed && mixed_) {
+        std::vector<float> tmp(nv);
+        HO2D_CUDA(cudaMemcpy(tmp.data(), src, nv * 4, cudaMemcpyDeviceToHost), "copy");
+        std::copy(tmp.begin(), tmp.end(), out);
+    } else {
+        HO2D_CUDA(cudaMemcpy(out, src, nv * 8, cudaMemcpyDeviceToHost), "copy");
+    }
+    return {0, ""};
+}
+
+Error Solver::get_velocity(double* out) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    std::vector<double> u(nv), v(nv);
+    if (mixed_) {
+        std::vector<float> uf(nv), vf(nv);
+        HO2D_CUDA(cudaMemcpy(uf.data(), d.u.get(), nv * 4, cudaMemcpyDeviceToHost), "copy");
+        HO2D_CUDA(cudaMemcpy(vf.data(), d.v.get(), nv * 4, cudaMemcpyDeviceToHost), "copy");
+        std::copy(uf.begin(), uf.end(), u.begin());
+        std::copy(vf.begin(), vf.end(), v.begin());
+    } else {
+        HO2D_CUDA(cudaMemcpy(u.data(), d.u.get(), nv * 8, cudaMemcpyDeviceToHost), "copy");
+        HO2D_CUDA(cudaMemcpy(v.data(), d.v.get(), nv * 8, cudaMemcpyDeviceToHost), "copy");
+    }
+    for (size_t i = 0; i < nv; ++i) {
+        out[2 * i] = u[i];
+        out[2 * i + 1] = v[i];
+    }
+    return {0, ""};
+}
+
+Error Solver::set_vorticity(const double* in) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    for (size_t i = 0; i < nv; ++i)
+        if (!std::isfinite(in[i])) return {7, "non-finite value in the vorticity passed in"};
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    HO2D_CUDA(cudaMemcpy(d.omega.get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
+    if (mixed_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
+    else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    return {0, ""};
+}
+
+static DeviceBuffer* boundary_buffer(DeviceState& d, int which) {
+    switch (which) {
+        case 0: return &d.bc_p;
+        case 1: return &d.bc_nv;
+        case 2: return &d.bc_pv;
+        case 3: return &d.bc_d;
+        case 4: return &d.bc_w;
+        case 5: return &d.vjump;
+        case 6: return &d.bc_adv;
+        default: return nullptr;
+    }
+}
+
+Error Solver::get_boundary(int which, double* out) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceBuffer* b = boundary_buffer(*d_, which);
+    if (!b) return {1, "unknown boundary array"};
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "sync");
+    HO2D_CUDA(cudaMemcpy(out, b->get(), (size_t)mesh_.n_eb * in_.knod * 8, cudaMemcpyDeviceToHost), "copy");
+    return {0, ""};
+}
+
+Error Solver::set_boundary(int which, const double* in) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceBuffer* b = boundary_buffer(*d_, which);
+    if (!b) return {1, "unknown boundary array"};
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "sync");
+    HO2D_CUDA(cudaMemcpy(b->get(), in, (size_t)mesh_.n_eb * in_.knod * 8, cudaMemcpyHostToDevice), "copy");
+    return {0, ""};
+}
+
+Error Solver::get_solution_points(double* out) {
+    if (!setup_done_) return {1, "not set up"};
+    const int N = mesh_.n_el, K = in_.knod, L = mesh_.lnod;
+    for (int el = 0; el < N; ++el)
+        for (int j = 0; j < K; ++j)
+            for (int i = 0; i < K; ++i) {
+                double x = 0.0, y = 0.0;
+                for (int ly = 0; ly < L; ++ly)
+                    for (int lx = 0; lx < L; ++lx) {
+                        const int nd = mesh_.elem_nodes[el][tensor2fem(lx, ly, L - 1)];
+                        const double wgt = B_.gsb[ly * K + j] * B_.gsb[lx * K + i];
+                        x += wgt * mesh_.node_xy[2 * nd];
+                        y += wgt * mesh_.node_xy[2 * nd + 1];
+                    }
+                const size_t p = ((size_t)el * K + j) * K + i;
+                out[2 * p] = x;
+                out[2 * p + 1] = y;
+            }
+    return {0, ""};
+}
+
+}  // namespace ho2d

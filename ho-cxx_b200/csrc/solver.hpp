@@ -1,0 +1,104 @@
+// solver.hpp -- one solver instance: host setup tables plus everything resident on the GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+
+namespace ho2d {
+
+// Owning device allocation.
+class DeviceBuffer {
+  public:
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { reset(); }
+    cudaError_t alloc(size_t bytes);
+    void reset();
+    void* get() const { return p_; }
+    size_t bytes() const { return n_; }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p_); }
+
+  private:
+    void* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+struct DeviceState;  // defined in solver.cu
+
+class Solver {
+  public:
+    Solver();
+    ~Solver();
+
+    Error read_input(const std::string& path);
+    Error setup();
+    Error step(int nsteps);
+    Error stage(double coeff);
+    Error solve();
+    Error solveto(double outerdt, int numstep, int integtype, double reyn);
+    Error set_precision(int mode);
+    Error time_steps(int nsteps, double* total_ms, double* poisson_ms);
+    Error profile_spmv(int reps, double* avg_ms, double* bytes);
+
+    Error get_volume(int which, double* out);  // [N][K][K]
+    Error get_velocity(double* out);           // [N][K][K][2]
+    Error set_vorticity(const double* in);
+    Error get_boundary(int which, double* out);
+    Error set_boundary(int which, const double* in);
+    Error get_solution_points(double* out);
+
+    bool is_setup() const { return setup_done_; }
+    const Input& input() const { return in_; }
+    int n_el() const { return mesh_.n_el; }
+    int knod() const { return in_.knod; }
+    int n_eb() const { return mesh_.n_eb; }
+    int lnod() const { return mesh_.lnod; }
+    double time() const { return time_; }
+    double dt() const { return in_.dt; }
+    int precision() const { return mixed_ ? 1 : 0; }
+    int last_poisson_iterations() const { return last_iters_; }
+    double last_poisson_residual() const { return last_res_; }
+    int64_t launches() const { return launches_; }
+    void set_poisson_tolerance(double tol, int max_iter) {
+        tol_ = tol;
+        max_iter_ = max_iter;
+    }
+
+  private:
+    Error stage_impl(double coeff, int rk_stage, bool update);
+    Error poisson_solve();
+    template <typename T>
+    Error stage_t(double coeff, int rk_stage, bool update);
+    template <typename T>
+    Error velocity_only_t();
+    Error upload_precision_arrays();
+    Error cuda(cudaError_t e, const char* what);
+
+    Input in_;
+    Mesh mesh_;
+    Bases B_;
+    Metrics M_;
+    BoundaryConditions bc_;
+    PoissonOperator op_;
+    bool input_done_ = false, setup_done_ = false;
+    bool mixed_ = false;
+    double time_ = 0.0;
+    double tol_ = 1e-12;
+    int max_iter_ = 500;
+    int last_iters_ = 0, prev_iters_ = 8;
+    double last_res_ = 0.0;
+    int64_t launches_ = 0;
+    bool timing_ = false;
+    double poisson_ms_acc_ = 0.0;
+    std::unique_ptr<DeviceState> d_;
+};
+
+}  // namespace ho2d

@@ -1,0 +1,166 @@
+"""B200-native HO-CXX vorticity-streamfunction flux-reconstruction solver.
+
+``HO_2D`` mirrors the member functions of the reference's ``HO_2D`` class
+(src/HO_2D.hpp:219-290) on top of the C ABI in ``include/ho2d.h``; the whole time step
+runs in the CUDA library ``ho2d/_lib/libho2d.so``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import FP64, MIXED, HO2DError  # noqa: F401
+
+
+class HO_2D:
+    """One solver instance (one mesh), like the reference's ``HO_2D``.
+
+    Errors raise :class:`HO2DError` with the C ABI's status code where the reference
+    calls ``exit()`` or returns a non-zero char.
+    """
+
+    def __init__(self):
+        self._lib = capi.load()
+        h = ctypes.c_void_p()
+        self._check(self._lib.ho2d_create(ctypes.byref(h)), handle=None)
+        self._h = h
+        self._setup = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.ho2d_destroy(h)
+            self._h = None
+
+    close = __del__
+
+    def _check(self, code: int, handle="self"):
+        if code != capi.HO2D_OK:
+            msg = self._lib.ho2d_last_error(self._h if handle == "self" else None) or b""
+            raise HO2DError(code, msg.decode(errors="replace"))
+
+    # -- setup sequence of src/main.cpp:44-75
+    def read_input_file(self, path: str) -> int:
+        self._check(self._lib.ho2d_read_input(self._h, str(path).encode()))
+        return 0
+
+    def setup(self) -> None:
+        if not self._setup:
+            self._check(self._lib.ho2d_setup(self._h))
+            self._setup = True
+            n, k, neb, lnod = (ctypes.c_int32() for _ in range(4))
+            self._check(self._lib.ho2d_get_sizes(self._h, ctypes.byref(n), ctypes.byref(k), ctypes.byref(neb),
+                                                 ctypes.byref(lnod)))
+            self.N_el, self.Knod, self.N_edges_boundary, self.Lnod = n.value, k.value, neb.value, lnod.value
+
+    # the reference's individual setup calls all map onto the one device setup
+    def setup_mesh(self) -> int:
+        self.setup()
+        return 0
+
+    allocate_arrays = setup_mesh
+    setup_sps_gps = setup_mesh
+    form_bases = setup_mesh
+    form_metrics = setup_mesh
+    setup_IC_BC_SRC = setup_mesh
+    form_Laplace_operator_matrix = setup_mesh
+
+    # -- time stepping
+    def solve_vorticity_streamfunction(self) -> int:
+        self._check(self._lib.ho2d_solve(self._h))
+        return 0
+
+    def solve_advection_diffusion(self, nsteps: int = 1) -> int:
+        self._check(self._lib.ho2d_step(self._h, int(nsteps)))
+        return 0
+
+    def Euler_time_integrate(self, coeff: float) -> np.ndarray:
+        """One stage on the current vorticity; returns k = dt (advective + diffusive)."""
+        self._check(self._lib.ho2d_stage(self._h, float(coeff)))
+        return self.get_field(capi.FIELD_STAGE_K)
+
+    def solveto_d(self, outerdt: float, numstep: int, integtype: int, reyn: float, region: int = 0) -> None:
+        self._check(self._lib.ho2d_solveto(self._h, float(outerdt), int(numstep), int(integtype), float(reyn)))
+
+    # -- data exchange
+    def _vol(self, comps=1):
+        return np.zeros((self.N_el, self.Knod, self.Knod) + ((comps,) if comps > 1 else ()), dtype=np.float64)
+
+    def getallvorts_d(self) -> np.ndarray:
+        out = self._vol()
+        self._check(self._lib.ho2d_get_vort(self._h, out.size, capi.dptr(out)))
+        return out
+
+    get_vorticity = getallvorts_d
+
+    def setsolnvort_d(self, vort) -> None:
+        a = np.ascontiguousarray(vort, dtype=np.float64)
+        self._check(self._lib.ho2d_set_vort(self._h, a.size, capi.dptr(a)))
+
+    set_vorticity = setsolnvort_d
+
+    def get_streamfunction(self) -> np.ndarray:
+        out = self._vol()
+        self._check(self._lib.ho2d_get_psi(self._h, out.size, capi.dptr(out)))
+        return out
+
+    def get_velocity(self) -> np.ndarray:
+        out = self._vol(2)
+        self._check(self._lib.ho2d_get_vel(self._h, out.size, capi.dptr(out)))
+        return out
+
+    def get_field(self, which: int) -> np.ndarray:
+        out = self._vol()
+        self._check(self._lib.ho2d_get_field(self._h, int(which), out.size, capi.dptr(out)))
+        return out
+
+    def get_boundary(self, which: int) -> np.ndarray:
+        out = np.zeros((self.N_edges_boundary, self.Knod))
+        self._check(self._lib.ho2d_get_boundary(self._h, int(which), out.size, capi.dptr(out)))
+        return out
+
+    def set_boundary(self, which: int, values) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self._lib.ho2d_set_boundary(self._h, int(which), a.size, capi.dptr(a)))
+
+    def getsolnpts_d(self) -> np.ndarray:
+        out = self._vol(2)
+        self._check(self._lib.ho2d_get_solution_points(self._h, out.size, capi.dptr(out)))
+        return out
+
+    # -- controls and statistics
+    def set_precision(self, mode: int) -> None:
+        self._check(self._lib.ho2d_set_precision(self._h, int(mode)))
+
+    def set_poisson_tolerance(self, rel_tol: float, max_iter: int) -> None:
+        self._check(self._lib.ho2d_set_poisson_tolerance(self._h, float(rel_tol), int(max_iter)))
+
+    def poisson_stats(self):
+        it, res = ctypes.c_int32(), ctypes.c_double()
+        self._check(self._lib.ho2d_poisson_stats(self._h, ctypes.byref(it), ctypes.byref(res)))
+        return it.value, res.value
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.ho2d_get_time(self._h, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def time_steps(self, nsteps: int):
+        """Advance nsteps and return (total device ms, Poisson device ms) from CUDA events."""
+        tot, pois = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.ho2d_time_steps(self._h, int(nsteps), ctypes.byref(tot), ctypes.byref(pois)))
+        return tot.value, pois.value
+
+    def profile_spmv(self, reps: int = 20):
+        """(average ms per launch, algorithmic bytes per launch) of the Poisson SpMV kernel."""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.ho2d_profile_spmv(self._h, int(reps), ctypes.byref(ms), ctypes.byref(by)))
+        return ms.value, by.value
+
+    def launch_count(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self._lib.ho2d_last_launch_count(self._h, ctypes.byref(n)))
+        return n.value

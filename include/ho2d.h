@@ -1,0 +1,134 @@
+/*
+ * ho2d.h -- C ABI of the B200-native HO-CXX vorticity-streamfunction FR solver.
+ *
+ * One opaque handle drives one mesh, like one instance of the reference's HO_2D class
+ * (src/HO_2D.hpp:69-291). Every entry point returns an int status (0 = success, as the
+ * reference's char/int returns at src/main.cpp:49-59); no C++ exception crosses this
+ * boundary. Buffers are caller-owned (int32 length, double* data) pairs in the
+ * reference's ordering: volume fields [el][j][i] with el in .msh file order, boundary
+ * arrays [edge][k] in boundary-edge order (src/HO_2D.cpp:4148-4250 use the same pairs).
+ * Calls are synchronous at return and not thread-safe on one handle. Every handle owns
+ * one CUDA stream on the device that is current when ho2d_setup runs.
+ */
+#ifndef HO2D_H
+#define HO2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ho2d_solver ho2d_solver;
+
+enum ho2d_status {
+    HO2D_OK = 0,
+    HO2D_ERR_ARG = 1,            /* null handle/buffer, wrong length, call out of order */
+    HO2D_ERR_IO = 2,             /* input.dat or .msh cannot be opened (reference: exit(1)) */
+    HO2D_ERR_MESH = 3,           /* malformed mesh, unsupported element type (reference: returns 2/3) */
+    HO2D_ERR_UNSUPPORTED = 4,    /* Knod, Lnod, scheme or problem type outside what is implemented */
+    HO2D_ERR_CUDA = 5,           /* a CUDA runtime error; ho2d_last_error has the text */
+    HO2D_ERR_NOT_CONVERGED = 6,  /* Poisson solve hit its iteration cap above tolerance */
+    HO2D_ERR_NONFINITE = 7       /* NaN/Inf detected in the vorticity */
+};
+
+enum ho2d_precision {
+    HO2D_FP64 = 0,  /* every device array and operation in double precision */
+    HO2D_MIXED = 1  /* FP32 FR residual and Krylov, FP64 refinement residual and RK accumulation */
+};
+
+/* which boundary-edge array [N_eb][Knod] ho2d_get_boundary / ho2d_set_boundary address */
+enum ho2d_boundary_array {
+    HO2D_BC_POISSON = 0,        /* BC_Poisson: psi or d(psi)/dn */
+    HO2D_BC_NORMAL_VEL = 1,     /* BC_normal_vel (local h direction) */
+    HO2D_BC_PARL_VEL = 2,       /* BC_parl_vel (counter-clockwise tangential velocity) */
+    HO2D_BC_DIFFUSION = 3,      /* BC_diffusion: vorticity or its normal derivative */
+    HO2D_BC_VORTICITY = 4,      /* BC_vorticity: common vorticity on the boundary */
+    HO2D_BC_VELOCITY_JUMP = 5,  /* velocity_jump: d(psi)/dn on Dirichlet-psi edges */
+    HO2D_BC_ADVECTION = 6       /* BC_advection */
+};
+
+/* which volume array [N_el][Knod][Knod] ho2d_get_field addresses */
+enum ho2d_field {
+    HO2D_FIELD_VORTICITY = 0,
+    HO2D_FIELD_STREAMFUNCTION = 1,
+    HO2D_FIELD_RHS_DIFFUSIVE = 2,  /* Re^-1 Laplacian(omega) of the last stage */
+    HO2D_FIELD_RHS_ADVECTIVE = 3,  /* -div(u omega) of the last stage */
+    HO2D_FIELD_STAGE_K = 4,        /* k = dt (advective + diffusive) of the last stage */
+    HO2D_FIELD_JACOBIAN = 5        /* vol_jac at the solution points */
+};
+
+/* Replaces HO_2D::HO_2D() (src/HO_2D.hpp:184-198). */
+int ho2d_create(ho2d_solver** handle);
+/* Replaces HO_2D::~HO_2D / release_memory (src/HO_2D.cpp:125-211); frees device memory. */
+int ho2d_destroy(ho2d_solver* handle);
+/* Replaces HO_2D::read_input_file (src/HO_2D.cpp:213-317); the mesh path in the file is
+ * resolved relative to the directory of `path`. */
+int ho2d_read_input(ho2d_solver* handle, const char* path);
+/* Replaces the setup sequence of src/main.cpp:49-75: setup_mesh, allocate_arrays,
+ * setup_sps_gps, form_bases, form_metrics, setup_IC_BC_SRC, form_Laplace_operator_matrix
+ * (src/HO_2D.cpp:476-1804, 3011-3086). Uploads everything to the current CUDA device. */
+int ho2d_setup(ho2d_solver* handle);
+/* Replaces HO_2D::solve_vorticity_streamfunction (src/HO_2D.cpp:1390-1463) for
+ * num_time_steps steps from the initial vorticity, including the extra Poisson solve and
+ * velocity recovery at every dump step; VTK files are not written. */
+int ho2d_solve(ho2d_solver* handle);
+/* Replaces nsteps calls of HO_2D::solve_advection_diffusion (src/HO_2D.cpp:1465-1531),
+ * advancing the solver time by dt after each. */
+int ho2d_step(ho2d_solver* handle, int32_t nsteps);
+/* Replaces one HO_2D::Euler_time_integrate(vorticity, k, coeff) (src/HO_2D.cpp:1806-1839)
+ * on the current vorticity, without advancing time; results via ho2d_get_field. */
+int ho2d_stage(ho2d_solver* handle, double coeff);
+/* Replaces HO_2D::solveto_d (src/HO_2D.cpp:4194-4233) for the non-hybrid problem types:
+ * dt = outerdt / numstep, integrator `integtype`, Re = reyn, numstep steps. */
+int ho2d_solveto(ho2d_solver* handle, double outerdt, int32_t numstep, int32_t integtype, double reyn);
+
+/* Sizes after ho2d_setup: elements, Knod, boundary edges, geometry nodes per edge. */
+int ho2d_get_sizes(ho2d_solver* handle, int32_t* n_el, int32_t* knod, int32_t* n_edges_boundary,
+                   int32_t* lnod);
+/* Vorticity in/out (like setsolnvort_d / getallvorts_d, src/HO_2D.cpp:4148-4250);
+ * len = N_el*Knod*Knod. ho2d_set_vort also sets the initial vorticity used by ho2d_solve. */
+int ho2d_get_vort(ho2d_solver* handle, int32_t len, double* buf);
+int ho2d_set_vort(ho2d_solver* handle, int32_t len, const double* buf);
+/* Stream function, len = N_el*Knod*Knod. */
+int ho2d_get_psi(ho2d_solver* handle, int32_t len, double* buf);
+/* Cartesian velocity [el][j][i][u,v] (velocity_cart), len = 2*N_el*Knod*Knod. */
+int ho2d_get_vel(ho2d_solver* handle, int32_t len, double* buf);
+/* Any volume array of enum ho2d_field, len = N_el*Knod*Knod. */
+int ho2d_get_field(ho2d_solver* handle, int32_t which, int32_t len, double* buf);
+/* Boundary-edge arrays of enum ho2d_boundary_array, len = N_eb*Knod. Setting
+ * HO2D_BC_PARL_VEL replaces a lid/wall velocity profile (the reference's BC_parl_vel). */
+int ho2d_get_boundary(ho2d_solver* handle, int32_t which, int32_t len, double* buf);
+int ho2d_set_boundary(ho2d_solver* handle, int32_t which, int32_t len, const double* buf);
+/* Solution-point coordinates [el][j][i][x,y] (like getsolnpts_d, src/HO_2D.cpp:3946-3980),
+ * len = 2*N_el*Knod*Knod. */
+int ho2d_get_solution_points(ho2d_solver* handle, int32_t len, double* buf);
+
+/* HO2D_FP64 (default) or HO2D_MIXED; may be called before or after ho2d_setup. */
+int ho2d_set_precision(ho2d_solver* handle, int32_t mode);
+/* Poisson solve controls: relative tolerance on ||b - A psi|| / ||b|| (default 1e-12)
+ * and iteration cap (default 500). */
+int ho2d_set_poisson_tolerance(ho2d_solver* handle, double rel_tol, int32_t max_iter);
+/* Statistics of the last Poisson solve: Krylov iterations (inner iterations summed over
+ * refinement sweeps) and final relative residual. */
+int ho2d_poisson_stats(ho2d_solver* handle, int32_t* iterations, double* rel_residual);
+/* Current solver time and time-step size. */
+int ho2d_get_time(ho2d_solver* handle, double* time, double* dt);
+/* Runs nsteps time steps and reports device time between CUDA events recorded on the
+ * handle's stream around them: total milliseconds and the part spent in Poisson solves. */
+int ho2d_time_steps(ho2d_solver* handle, int32_t nsteps, double* total_ms, double* poisson_ms);
+/* Runs the Poisson solver's block-SpMV kernel `reps` times back to back (on the current
+ * Krylov vectors, in the active precision) between CUDA events on the handle's stream;
+ * returns the average launch duration and the algorithmic bytes one launch must move. */
+int ho2d_profile_spmv(ho2d_solver* handle, int32_t reps, double* avg_ms, double* bytes_per_launch);
+/* Total number of kernel launches this handle has issued since it was created. */
+int ho2d_last_launch_count(ho2d_solver* handle, int64_t* launches);
+/* Text of the last error on this handle ("" if none). The pointer stays valid until the
+ * next call on the handle. */
+const char* ho2d_last_error(ho2d_solver* handle);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HO2D_H */

@@ -23,6 +23,8 @@
 //   --steps N              run N time steps, dumping vorticity/psi every --every steps
 //   --every M              dump period for --steps (default N)
 //   --time N               time N steps (no dumps) and print a JSON line
+//   --time-stages N        time N RK stages (Euler_time_integrate on the current vorticity,
+//                          coefficients cycling 0, .5, .5, 1) and print a JSON line
 //   --verbose              keep the reference's stdout
 #include "HO_2D.hpp"
 
@@ -104,7 +106,7 @@ int main(int argc, char** argv) {
     std::string input = argv[1], outdir = argv[2];
     bool do_setup = false, verbose = false, do_stage = false;
     double stage_coeff = 0.0, dt_override = -1.0;
-    long nsteps = 0, every = 0, ntime = 0;
+    long nsteps = 0, every = 0, ntime = 0, nstages = 0;
     std::string init_vort, lid;
     for (int i = 3; i < argc; ++i) {
         std::string a = argv[i];
@@ -117,6 +119,7 @@ int main(int argc, char** argv) {
         else if (a == "--steps" && i + 1 < argc) nsteps = std::atol(argv[++i]);
         else if (a == "--every" && i + 1 < argc) every = std::atol(argv[++i]);
         else if (a == "--time" && i + 1 < argc) ntime = std::atol(argv[++i]);
+        else if (a == "--time-stages" && i + 1 < argc) nstages = std::atol(argv[++i]);
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     mkdir(outdir.c_str(), 0755);
@@ -283,6 +286,18 @@ int main(int argc, char** argv) {
         std::printf("{\"steps\": %ld, \"seconds\": %.6f, \"poisson_seconds\": %.6f, \"poisson_iterations\": %ld, "
                     "\"setup_seconds\": %.6f, \"N_el\": %zu, \"Knod\": %zu, \"dof\": %zu}\n",
                     ntime, sec, amgcl::shim_solve_seconds(), amgcl::shim_solve_iterations(), setup_s, N, K, N * K * K);
+    }
+    if (nstages > 0) {
+        static const double c4[4] = {0.0, 0.5, 0.5, 1.0};
+        amgcl::shim_solve_seconds() = 0.0;
+        amgcl::shim_solve_iterations() = 0;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (long s = 0; s < nstages; ++s) ho.Euler_time_integrate(ho.vorticity, ho.k1, c4[s % 4]);
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::cout.rdbuf(saved);
+        std::printf("{\"stages\": %ld, \"seconds\": %.6f, \"poisson_seconds\": %.6f, \"poisson_iterations\": %ld, "
+                    "\"setup_seconds\": %.6f, \"N_el\": %zu, \"Knod\": %zu, \"dof\": %zu}\n",
+                    nstages, sec, amgcl::shim_solve_seconds(), amgcl::shim_solve_iterations(), setup_s, N, K, N * K * K);
     }
     std::cout.rdbuf(saved);
     return 0;
