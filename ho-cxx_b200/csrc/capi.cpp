@@ -1,5 +1,6 @@
 // capi.cpp -- the extern "C" boundary declared in include/ho2d.h. Every entry point
 // catches exceptions and turns them into status codes plus a per-handle message.
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -191,12 +192,29 @@ int ho2d_get_time(ho2d_solver* h, double* time, double* dt) {
     });
 }
 
+int ho2d_set_time(ho2d_solver* h, double time) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!std::isfinite(time)) return {HO2D_ERR_ARG, "time must be finite"};
+        h->s.set_time(time);
+        return {0, ""};
+    });
+}
+
 int ho2d_time_steps(ho2d_solver* h, int32_t nsteps, double* total_ms, double* poisson_ms) {
     return guarded(h, [&]() { return h->s.time_steps(nsteps, total_ms, poisson_ms); });
 }
 
 int ho2d_profile_spmv(ho2d_solver* h, int32_t reps, double* avg_ms, double* bytes_per_launch) {
     return guarded(h, [&]() { return h->s.profile_spmv(reps, avg_ms, bytes_per_launch); });
+}
+
+int ho2d_apply_poisson(ho2d_solver* h, int32_t len, const double* x, double* y) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), x);
+        if (e.code) return e;
+        if (!y) return {HO2D_ERR_ARG, "null output buffer"};
+        return h->s.apply_poisson(x, y);
+    });
 }
 
 int ho2d_last_launch_count(ho2d_solver* h, int64_t* launches) {

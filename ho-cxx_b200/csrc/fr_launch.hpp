@@ -57,19 +57,24 @@ cudaError_t launch_bc_update(int n_eb, int K, int ptype, double tc, double y_min
                              cudaStream_t s);
 
 // ---- Krylov (krylov.cu)
-// Block-sparse operator: 5 K^2 x K^2 blocks per element row, transposed ([rs][ij]).
-template <typename TM>
-struct BsrOp {
-    int N, K;
-    const TM* blocks;  // [N][5][K2][K2]
-    const int* col;    // [N][5]
-    const TM* dinv;    // [N][K2][K2] inverse diagonal block (transposed), block-Jacobi
+// Matrix-free FR Laplacian (the Poisson operator) plus the preconditioner's element data.
+template <typename T>
+struct MfOp {
+    int K;
+    FrGeom<T> g;            // metrics, connectivity, Poisson BC switches (g.sw_p)
+    DevBases<T> b;
+    const double* zero_bc;  // [N_eb * K] zeros: homogeneous boundary values
+    const T* dinv;          // [N][K2][K2] inverse diagonal blocks, transposed ([rs][ij])
+    const T* rowsum;        // [N][5][K2] row sums of the 5 blocks of each element row
+    const int* bcol;        // [N][5] element of each block (slot 0 = self, 1 + ijp = neighbours)
 };
 
 template <typename T>
 struct BicgVectors {
     T *x, *r, *rhat, *p, *v, *s, *t, *ph, *sh;
     const T* b;
+    T *tv, *tg;    // face traces of the operand of the next operator application (ph or sh)
+    T *xtv, *xtg;  // face traces of x (initial residual)
 };
 
 struct ReduceScratch {
@@ -78,25 +83,58 @@ struct ReduceScratch {
     KrylovScalars* sc;   // device scalars
 };
 
-template <typename T, typename TM>
-cudaError_t krylov_init(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+// scalar CSR matrix on the device
+template <typename T>
+struct DevCsr {
+    int n;
+    const int* ptr;
+    const int* col;
+    const T* val;
+};
+
+// one coarse level of the two-level preconditioner (level 0 = one value per element)
+template <typename T>
+struct CoarseLevel {
+    int n;
+    DevCsr<T> A, P, R;  // P, R unused on the coarsest level
+    const T* m;         // SPAI-0 weights
+    T *f, *u, *t, *u2;  // right-hand side, iterate, residual, smoothed iterate
+    T* out;             // where this level's cycle leaves its result (u2, or u when coarsest)
+};
+
+constexpr int kMaxLevels = 24;
+
+// preconditioner: nlev == 0 -> block-Jacobi; otherwise the two-level V(0,1) cycle
+template <typename T>
+struct Precond {
+    int nlev = 0;
+    double omega = 1.0;  // weight of the block-Jacobi smoothing step
+    CoarseLevel<T> lev[kMaxLevels];
+    const T* dense_inv = nullptr;  // inverse of the coarsest operator
+};
+
+template <typename T>
+cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
                         cudaStream_t s);
-template <typename T, typename TM>
-cudaError_t krylov_iteration(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
-                             cudaStream_t s);
-// `reps` back-to-back launches of the solver's SpMV kernel (v = A ph, fused (rhat, v))
-template <typename T, typename TM>
-cudaError_t krylov_spmv_only(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, int reps,
-                             cudaStream_t s);
-// y = b - A x in FP64 (x in T64 = double); fused ||y||^2, ||b||^2 -> sc->rnorm2, sc->bnorm2
-template <typename TM>
-cudaError_t residual_fp64(const BsrOp<TM>& A, const double* b, const double* x, double* r, const ReduceScratch& rs,
-                          cudaStream_t s);
+template <typename T>
+cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                             const Precond<T>& pc, cudaStream_t s);
+template <typename T>
+int krylov_launches_per_iteration(const Precond<T>& pc);
+// r = b - A x with ||r||^2 -> sc->rnorm2, ||b||^2 -> sc->bnorm2 (traces of x into xtv/xtg)
+template <typename T>
+cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
+                        const ReduceScratch& rs, cudaStream_t s);
+// y = A x (traces of x into xtv/xtg first)
+template <typename T>
+cudaError_t mf_apply_op(const MfOp<T>& op, const T* x, T* xtv, T* xtg, T* y, cudaStream_t s);
+// `reps` launches of the operator kernel alone on x whose traces are already in xtv/xtg
+template <typename T>
+cudaError_t mf_apply_only(const MfOp<T>& op, const T* x, const T* xtv, const T* xtg, T* y, int reps, cudaStream_t s);
 int krylov_max_blocks(int K, int N);
 
 // elementwise helpers
 cudaError_t launch_copy_d2f(const double* a, float* b, size_t n, cudaStream_t s);
-cudaError_t launch_copy_f2d(const float* a, double* b, size_t n, cudaStream_t s);
 cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s);  // x += e
 
 }  // namespace ho2d

@@ -101,6 +101,7 @@ struct PoissonOperator {
     std::vector<int> block_col;   // [N][5] column element (-1 = empty slot)
     std::vector<double> bsrc;     // [N_eb][K2][K]
     std::vector<double> dinv;     // [N][K2][K2] inverse of the diagonal block (rs outer)
+    std::vector<double> rowsum;   // [N][5][K2] sum over rs of each block row
     int64_t nnz = 0;              // entries surviving the |a| > 1e-14 filter
 };
 

@@ -1,0 +1,33 @@
+// host_amg.hpp -- P0 coarse operator and its smoothed-aggregation hierarchy (host setup).
+#pragma once
+
+#include <vector>
+
+#include "host.hpp"
+
+namespace ho2d {
+
+constexpr int kDenseMax = 384;  // the coarsest level is inverted densely below this size
+
+struct Csr {
+    int n = 0, m = 0;
+    std::vector<int> ptr, col;
+    std::vector<double> val;
+};
+
+struct AmgLevel {
+    Csr A, P, R;            // P, R empty on the coarsest level
+    std::vector<double> m;  // SPAI-0 smoother weights
+};
+
+struct CoarseHierarchy {
+    std::vector<AmgLevel> levels;  // levels[0] is the P0 (one value per element) operator
+    int n_dense = 0;
+    std::vector<double> dense_inv;  // row-major inverse of the coarsest operator
+};
+
+// A1 = P^T A P for P = element indicator: the sum of each K^2 x K^2 block.
+Csr p0_coarse_operator(const PoissonOperator& op, int N);
+Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H);
+
+}  // namespace ho2d

@@ -1,19 +1,27 @@
-// krylov.cu -- block-sparse Poisson operator and BiCGSTAB on the device (sm_100a).
+// krylov.cu -- matrix-free FR Poisson operator and preconditioned BiCGSTAB (sm_100a).
 //
-// The assembled FR Laplacian has, per element row, the element's own K^2 x K^2 block and
-// up to four neighbour blocks (src/HO_2D.cpp:1533-1804). It is stored as 5 dense blocks
-// per element, transposed ([rs][ij]) so that the K^2 threads of an element (one per
-// output row) read consecutive addresses: the matrix streams from HBM once per product
-// and the x entries of a column block are warp-broadcast loads.
+// Operator. The reference assembles the FR Laplacian into a CSR matrix with up to
+// 5 K^4 entries per element (src/HO_2D.cpp:1533-1804, 3011-3062) and hands it to AMGCL.
+// That matrix is exactly the method-2 FR Laplacian of calc_RHS_diffusion applied with
+// homogeneous Poisson boundary values, so here A x is evaluated matrix-free from face
+// traces (lap_element in fr_device.cuh): per DOF it reads x, 5 volume metrics and a
+// share of the face data instead of 5 K^2 matrix entries. Every kernel that produces
+// a vector the operator is applied to next also writes that vector's face traces, so
+// one operator application is one launch.
 //
-// The solver replaces AMGCL's BiCGSTAB (src/HO_2D.hpp:53-54, src/HO_2D.cpp:1960) with a
-// right-preconditioned BiCGSTAB (van der Vorst 1992) preconditioned by the inverse
-// diagonal (element) blocks. All scalars stay on the device; each kernel fuses its
-// vector update with the dot products the next step needs, reduced deterministically
-// (per-CTA partials, the last CTA to finish sums them in a fixed order). A `done` flag
-// makes the remaining launches of an enqueued batch return immediately, so the host only
-// polls for convergence every few iterations.
+// Solver. Right-preconditioned BiCGSTAB (van der Vorst 1992) replacing AMGCL's BiCGSTAB
+// (src/HO_2D.hpp:53-54, src/HO_2D.cpp:1960). Preconditioner, two-level V(0,1):
+//   coarse:  e = P A1^{-1} P^T f, P = element-wise constants, A1 = P^T A P, A1^{-1}
+//            approximated by one smoothed-aggregation V-cycle (host_amg.cpp);
+//   smooth:  z = e + w D^{-1} (f - A e), D = the K^2 x K^2 diagonal blocks of A; A e is
+//            cheap because e is element-wise constant (A e = sum_s rowsum_s e_s).
+// With HO2D_PRECOND=bj the preconditioner is z = D^{-1} f (block-Jacobi).
+// Scalars stay on the device; every vector update fuses the dot products the next step
+// needs, reduced deterministically (per-CTA partials summed in a fixed order by the last
+// CTA to finish); a `done` flag turns the rest of an enqueued batch into no-ops, so the
+// host only polls for convergence every few iterations.
 #include "device.cuh"
+#include "fr_device.cuh"
 #include "fr_launch.hpp"
 
 namespace ho2d {
@@ -75,49 +83,77 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     return true;
 }
 
-template <int K, typename T, typename TM>
-__device__ __forceinline__ T bsr_row(const BsrOp<TM>& A, const T* __restrict__ x, int el, int ij) {
-    constexpr int K2 = K * K;
-    T acc = T(0);
-    const TM* blk = A.blocks + (size_t)el * 5 * K2 * K2 + ij;
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-        const int c = A.col[el * 5 + s];
-        if (c < 0) continue;
-        const T* xc = x + (size_t)c * K2;
-        const TM* bs = blk + (size_t)s * K2 * K2;
-#pragma unroll
-        for (int rs = 0; rs < K2; ++rs) acc += T(__ldg(bs + rs * K2)) * __ldg(xc + rs);
+// Shared-memory working set of one CTA (EPB elements).
+template <int K, typename T>
+struct MfShared {
+    static constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
+    T x[EPB][K2], a[EPB][K2], b[EPB][K2];
+    T tv[EPB][NF], tg[EPB][NF], com[EPB][NF], cg[EPB][NF], fb[EPB][NF];
+};
+
+// y = A x at (el, ij); x's own traces are recomputed, the neighbours' come from tv/tg.
+// Collective. Leaves x of the element in sm.x.
+template <int K, typename T>
+__device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
+                      MfShared<K, T>& sm, bool active, int le, int el, int ij) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    const int lei = active ? le : 0;
+    if (active) sm.x[le][ij] = x[el * K2 + ij];
+    __syncthreads();
+    if (active)
+        for (int o = ij; o < NF; o += K2) face_trace<K, T>(sm.x[le], op.b, o, sm.tv[le][o], sm.tg[le][o]);
+    __syncthreads();
+    return lap_element<K, T>(active, el, ij, op.g, op.b, tv, tg, sm.x[lei], sm.tv[lei], sm.tg[lei], sm.com[lei],
+                             sm.cg[lei], sm.a[lei], sm.b[lei], sm.fb[lei], op.g.sw_p, op.zero_bc);
+}
+
+// face traces of an element vector held in shared memory
+template <int K, typename T>
+__device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, T* tv, T* tg, bool active, int el,
+                                            int ij) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    if (!active) return;
+    for (int o = ij; o < NF; o += K2) {
+        T v, d;
+        face_trace<K, T>(sy, b, o, v, d);
+        tv[el * NF + o] = v;
+        tg[el * NF + o] = d;
     }
+}
+
+// z = Dinv y for one element, y in shared memory (Dinv stored [rs][ij])
+template <int K, typename T>
+__device__ __forceinline__ T block_apply(const T* __restrict__ dinv, const T* sy, int el, int ij) {
+    constexpr int K2 = K * K;
+    const T* d = dinv + (size_t)el * K2 * K2 + ij;
+    T acc = T(0);
+#pragma unroll
+    for (int rs = 0; rs < K2; ++rs) acc += __ldg(d + rs * K2) * sy[rs];
     return acc;
 }
 
-// z[el] = Dinv[el] y[el] with y staged in shared memory
-template <int K, typename T, typename TM>
-__device__ __forceinline__ T block_apply(const TM* __restrict__ dinv, const T* sy, int el, int ij) {
-    constexpr int K2 = K * K;
-    const TM* d = dinv + (size_t)el * K2 * K2 + ij;
-    T acc = T(0);
-#pragma unroll
-    for (int rs = 0; rs < K2; ++rs) acc += T(__ldg(d + rs * K2)) * sy[rs];
-    return acc;
+__device__ __forceinline__ bool pc_skip(const KrylovScalars* sc, int mode) {
+    return sc->done || (mode == 1 && sc->s_exit);
 }
 
 }  // namespace
 
-// r = b - A x, rhat = r; ||r||^2, ||b||^2
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_init(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs,
-                                                             double tol) {
+// ---------------------------------------------------------------- fine-level kernels
+// r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
+                                                                double tol) {
     using S = Shape<K>;
+    __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
+    const T y = mf_apply<K, T>(op, v.x, v.xtv, v.xtg, sm, active, le, el, ij);
     double part[2] = {0.0, 0.0};
     if (active) {
         const int p = el * S::K2 + ij;
         const T bb = v.b[p];
-        const T r = bb - bsr_row<K, T, TM>(A, v.x, el, ij);
+        const T r = bb - y;
         v.r[p] = r;
         v.rhat[p] = r;
         part[0] = double(r) * double(r);
@@ -140,7 +176,6 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_init(BsrOp<TM> A, BicgVec
     }
 }
 
-// zero right-hand side: x = 0 (the reference's solver returns the zero vector)
 template <typename T>
 __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
     if (!sc->zero_rhs) return;
@@ -148,16 +183,18 @@ __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
     if (i < n) x[i] = T(0);
 }
 
-// p = r + beta (p - omega v) (p = r on the first iteration); ph = M^{-1} p
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_p_update(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs) {
+// p = r + beta (p - omega v) (= r on the first iteration); then either ph = D^{-1} p with
+// its traces (block-Jacobi) or the element sums of p (two-level: coarse right-hand side)
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
+                                                                   T* rc) {
     using S = Shape<K>;
     const KrylovScalars* sc = rs.sc;
     if (sc->done) return;
-    __shared__ T sp[S::EPB][S::K2];
+    __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
     const int p = el * S::K2 + ij;
     if (active) {
         T pv;
@@ -171,22 +208,72 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_p_update(BsrOp<TM> A, Bic
         sp[le][ij] = pv;
     }
     __syncthreads();
-    if (active) v.ph[p] = block_apply<K, T, TM>(A.dinv, sp[le], el, ij);
+    if (rc) {
+        if (active && ij == 0) {
+            T sum = T(0);
+#pragma unroll
+            for (int q = 0; q < S::K2; ++q) sum += sp[le][q];
+            rc[el] = sum;
+        }
+        return;
+    }
+    if (active) {
+        const T z = block_apply<K, T>(op.dinv, sp[le], el, ij);
+        v.ph[p] = z;
+        sz[le][ij] = z;
+    }
+    __syncthreads();
+    emit_traces<K, T>(sz[active ? le : 0], op.b, v.tv, v.tg, active, el, ij);
+}
+
+// two-level smoothing step: z = e + w D^{-1} (f - A e), e = P ec element-wise constant;
+// writes z and its face traces
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const T* __restrict__ f,
+                                                                const T* __restrict__ ec, T* __restrict__ z,
+                                                                T* __restrict__ tv, T* __restrict__ tg, double w,
+                                                                const KrylovScalars* sc, int mode) {
+    using S = Shape<K>;
+    constexpr int K2 = S::K2;
+    if (pc_skip(sc, mode)) return;
+    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2];
+    const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
+    const int el = blockIdx.x * S::EPB + le;
+    const bool active = le < S::EPB && el < op.g.N;
+    const int p = el * K2 + ij;
+    if (active) {
+        T ae = T(0);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const int c = op.bcol[el * 5 + s];
+            if (c >= 0) ae += op.rowsum[((size_t)el * 5 + s) * K2 + ij] * ec[c];
+        }
+        sr[le][ij] = f[p] - ae;
+    }
+    __syncthreads();
+    if (active) {
+        const T zz = ec[el] + T(w) * block_apply<K, T>(op.dinv, sr[le], el, ij);
+        z[p] = zz;
+        sz[le][ij] = zz;
+    }
+    __syncthreads();
+    emit_traces<K, T>(sz[active ? le : 0], op.b, tv, tg, active, el, ij);
 }
 
 // v = A ph; alpha = rho / (rhat, v)
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_spmv_v(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs) {
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
     if (sc->done) return;
+    __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
+    const T y = mf_apply<K, T>(op, v.ph, v.tv, v.tg, sm, active, le, el, ij);
     double part[1] = {0.0};
     if (active) {
         const int p = el * S::K2 + ij;
-        const T y = bsr_row<K, T, TM>(A, v.ph, el, ij);
         v.v[p] = y;
         part[0] = double(v.rhat[p]) * double(y);
     }
@@ -201,16 +288,17 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_spmv_v(BsrOp<TM> A, BicgV
     }
 }
 
-// s = r - alpha v; ||s||^2; sh = M^{-1} s
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_s_update(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs) {
+// s = r - alpha v; ||s||^2; then sh = D^{-1} s with traces, or the element sums of s
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_supdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
+                                                                   T* rc) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
     if (sc->done) return;
-    __shared__ T sp[S::EPB][S::K2];
+    __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
     const int p = el * S::K2 + ij;
     double part[1] = {0.0};
     if (active) {
@@ -220,7 +308,22 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_s_update(BsrOp<TM> A, Bic
         part[0] = double(s) * double(s);
     }
     __syncthreads();
-    if (active) v.sh[p] = block_apply<K, T, TM>(A.dinv, sp[le], el, ij);
+    if (rc) {
+        if (active && ij == 0) {
+            T sum = T(0);
+#pragma unroll
+            for (int q = 0; q < S::K2; ++q) sum += sp[le][q];
+            rc[el] = sum;
+        }
+    } else {
+        if (active) {
+            const T z = block_apply<K, T>(op.dinv, sp[le], el, ij);
+            v.sh[p] = z;
+            sz[le][ij] = z;
+        }
+        __syncthreads();
+        emit_traces<K, T>(sz[active ? le : 0], op.b, v.tv, v.tg, active, el, ij);
+    }
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         sc->snorm2 = out[0];
@@ -229,18 +332,19 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_s_update(BsrOp<TM> A, Bic
 }
 
 // t = A sh; omega = (t, s) / (t, t)
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_spmv_t(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs) {
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
     if (sc->done || sc->s_exit) return;
+    __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
+    const T y = mf_apply<K, T>(op, v.sh, v.tv, v.tg, sm, active, le, el, ij);
     double part[2] = {0.0, 0.0};
     if (active) {
         const int p = el * S::K2 + ij;
-        const T y = bsr_row<K, T, TM>(A, v.sh, el, ij);
         v.t[p] = y;
         part[0] = double(y) * double(v.s[p]);
         part[1] = double(y) * double(y);
@@ -251,21 +355,20 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_spmv_t(BsrOp<TM> A, BicgV
 }
 
 // x += alpha ph + omega sh; r = s - omega t; ||r||^2, (rhat, r); convergence test
-template <int K, typename T, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(BsrOp<TM> A, BicgVectors<T> v, ReduceScratch rs,
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
                                                                   int max_iter) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
     if (sc->done) return;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < N;
     const int p = el * S::K2 + ij;
     const double alpha = sc->alpha;
     if (sc->s_exit) {  // ||s|| already below tolerance: x += alpha ph and stop
         if (active) v.x[p] += T(alpha) * v.ph[p];
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            // every CTA read s_exit before any could observe done: done is only read at kernel entry
             sc->rnorm2 = sc->snorm2;
             sc->it += 1;
         }
@@ -290,27 +393,30 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(BsrOp<TM> A, Bi
     }
 }
 
-// marks the solve finished after an s-exit iteration (separate launch: all CTAs of
-// k_xr_update have read s_exit before this runs)
+// ends the solve after an s-exit iteration (a separate launch: every CTA of k_xr_update
+// has read s_exit before done changes)
 __global__ void k_finish_s_exit(KrylovScalars* sc) {
     if (!sc->done && sc->s_exit) sc->done = 1;
 }
 
-// r = b - A x in FP64; ||r||^2 -> rnorm2, ||b||^2 -> bnorm2
-template <int K, typename TM>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_residual64(BsrOp<TM> A, const double* __restrict__ b,
-                                                                   const double* __restrict__ x, double* r,
-                                                                   ReduceScratch rs) {
+// r = b - A x (FP64 refinement residual); ||r||^2 -> rnorm2, ||b||^2 -> bnorm2
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_residual(MfOp<T> op, const double* __restrict__ b,
+                                                                    const T* __restrict__ x, const T* __restrict__ xtv,
+                                                                    const T* __restrict__ xtg, double* __restrict__ r,
+                                                                    ReduceScratch rs) {
     using S = Shape<K>;
+    __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < A.N;
+    const bool active = le < S::EPB && el < op.g.N;
+    const T y = mf_apply<K, T>(op, x, xtv, xtg, sm, active, le, el, ij);
     double part[2] = {0.0, 0.0};
     if (active) {
         const int p = el * S::K2 + ij;
-        const double y = b[p] - bsr_row<K, double, TM>(A, x, el, ij);
-        r[p] = y;
-        part[0] = y * y;
+        const double rr = b[p] - double(y);
+        r[p] = rr;
+        part[0] = rr * rr;
         part[1] = b[p] * b[p];
     }
     double out[2];
@@ -320,13 +426,82 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_residual64(BsrOp<TM> A, c
     }
 }
 
+// y = A x (operator only)
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_apply(MfOp<T> op, const T* __restrict__ x,
+                                                                 const T* __restrict__ xtv, const T* __restrict__ xtg,
+                                                                 T* __restrict__ y) {
+    using S = Shape<K>;
+    __shared__ MfShared<K, T> sm;
+    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
+    const int el = blockIdx.x * S::EPB + le;
+    const bool active = le < S::EPB && el < op.g.N;
+    const T yy = mf_apply<K, T>(op, x, xtv, xtg, sm, active, le, el, ij);
+    if (active) y[el * S::K2 + ij] = yy;
+}
+
+// ---------------------------------------------------------------- coarse levels (scalar CSR)
+template <typename T>
+__device__ __forceinline__ T csr_row(const DevCsr<T>& A, const T* __restrict__ x, int i) {
+    T acc = T(0);
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) acc += A.val[k] * x[A.col[k]];
+    return acc;
+}
+
+template <typename T>
+__global__ void k_c_smooth0(int n, const T* __restrict__ m, const T* __restrict__ f, T* __restrict__ u,
+                            const KrylovScalars* sc, int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) u[i] = m[i] * f[i];
+}
+
+template <typename T>
+__global__ void k_c_residual(DevCsr<T> A, const T* __restrict__ f, const T* __restrict__ u, T* __restrict__ t,
+                             const KrylovScalars* sc, int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < A.n) t[i] = f[i] - csr_row<T>(A, u, i);
+}
+
+template <typename T>
+__global__ void k_c_spmv(DevCsr<T> M, const T* __restrict__ x, T* __restrict__ y, const KrylovScalars* sc,
+                         int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M.n) y[i] = csr_row<T>(M, x, i);
+}
+
+template <typename T>
+__global__ void k_c_prolong_add(DevCsr<T> P, const T* __restrict__ uc, T* __restrict__ u, const KrylovScalars* sc,
+                                int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.n) u[i] += csr_row<T>(P, uc, i);
+}
+
+template <typename T>
+__global__ void k_c_smooth(DevCsr<T> A, const T* __restrict__ m, const T* __restrict__ f, const T* __restrict__ u,
+                           T* __restrict__ u2, const KrylovScalars* sc, int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < A.n) u2[i] = u[i] + m[i] * (f[i] - csr_row<T>(A, u, i));
+}
+
+template <typename T>
+__global__ void k_c_dense(int n, const T* __restrict__ inv, const T* __restrict__ f, T* __restrict__ u,
+                          const KrylovScalars* sc, int mode) {
+    if (pc_skip(sc, mode)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T acc = T(0);
+    for (int j = 0; j < n; ++j) acc += inv[(size_t)i * n + j] * f[j];
+    u[i] = acc;
+}
+
 __global__ void k_d2f(const double* a, float* b, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
-}
-__global__ void k_f2d(const float* a, double* b, size_t n) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = (double)a[i];
 }
 __global__ void k_axpy_f2d(const float* e, double* x, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -358,56 +533,95 @@ int krylov_max_blocks(int K, int N) {
     return (N + epb - 1) / epb;
 }
 
-template <typename T, typename TM>
-cudaError_t krylov_init(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+template <typename T>
+cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
                         cudaStream_t s) {
-    HO2D_KSWITCH(A.K, (k_init<KK, T, TM><<<kgrid<KK>(A.N), Shape<KK>::THREADS, 0, s>>>(A, v, rs, tol)));
-    const size_t n = (size_t)A.N * A.K * A.K;
+    const int N = op.g.N;
+    cudaError_t e = launch_trace<T>(op.K, N, v.x, v.xtv, v.xtg, op.b, s);
+    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v, rs, tol)));
+    const size_t n = (size_t)N * op.K * op.K;
     k_zero_if<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v.x, n, rs.sc);
     return cudaGetLastError();
 }
 
-template <int K, typename T, typename TM>
-static void iteration_impl(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
-                           cudaStream_t s) {
-    const unsigned g = kgrid<K>(A.N);
-    constexpr int th = Shape<K>::THREADS;
-    k_p_update<K, T, TM><<<g, th, 0, s>>>(A, v, rs);
-    k_spmv_v<K, T, TM><<<g, th, 0, s>>>(A, v, rs);
-    k_s_update<K, T, TM><<<g, th, 0, s>>>(A, v, rs);
-    k_spmv_t<K, T, TM><<<g, th, 0, s>>>(A, v, rs);
-    k_xr_update<K, T, TM><<<g, th, 0, s>>>(A, v, rs, max_iter);
+template <typename T>
+static void coarse_cycle(const Precond<T>& pc, int l, const KrylovScalars* sc, int mode, cudaStream_t s) {
+    const CoarseLevel<T>& L = pc.lev[l];
+    const unsigned g = (unsigned)((L.n + 127) / 128);
+    if (l == pc.nlev - 1) {
+        k_c_dense<T><<<g, 128, 0, s>>>(L.n, pc.dense_inv, L.f, L.u, sc, mode);
+        return;
+    }
+    const CoarseLevel<T>& C = pc.lev[l + 1];
+    k_c_smooth0<T><<<g, 128, 0, s>>>(L.n, L.m, L.f, L.u, sc, mode);
+    k_c_residual<T><<<g, 128, 0, s>>>(L.A, L.f, L.u, L.t, sc, mode);
+    k_c_spmv<T><<<(unsigned)((C.n + 127) / 128), 128, 0, s>>>(L.R, L.t, C.f, sc, mode);
+    coarse_cycle(pc, l + 1, sc, mode, s);
+    k_c_prolong_add<T><<<g, 128, 0, s>>>(L.P, C.out, L.u, sc, mode);
+    k_c_smooth<T><<<g, 128, 0, s>>>(L.A, L.m, L.f, L.u, L.u2, sc, mode);
 }
 
-template <typename T, typename TM>
-cudaError_t krylov_iteration(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
-                             cudaStream_t s) {
-    HO2D_KSWITCH(A.K, (iteration_impl<KK, T, TM>(A, v, rs, max_iter, s)));
+template <int K, typename T>
+static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                           const Precond<T>& pc, cudaStream_t s) {
+    const int N = op.g.N;
+    const unsigned g = kgrid<K>(N);
+    constexpr int th = Shape<K>::THREADS;
+    const bool mg = pc.nlev > 0;
+    T* rc = mg ? pc.lev[0].f : nullptr;
+    k_mf_pupdate<K, T><<<g, th, 0, s>>>(op, v, rs, rc);
+    if (mg) {
+        coarse_cycle(pc, 0, rs.sc, 0, s);
+        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.p, pc.lev[0].out, v.ph, v.tv, v.tg, pc.omega, rs.sc, 0);
+    }
+    k_mf_v<K, T><<<g, th, 0, s>>>(op, v, rs);
+    k_mf_supdate<K, T><<<g, th, 0, s>>>(op, v, rs, rc);
+    if (mg) {
+        coarse_cycle(pc, 0, rs.sc, 1, s);
+        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.s, pc.lev[0].out, v.sh, v.tv, v.tg, pc.omega, rs.sc, 1);
+    }
+    k_mf_t<K, T><<<g, th, 0, s>>>(op, v, rs);
+    k_xr_update<K, T><<<g, th, 0, s>>>(N, v, rs, max_iter);
+}
+
+template <typename T>
+int krylov_launches_per_iteration(const Precond<T>& pc) {
+    if (pc.nlev == 0) return 6;
+    const int coarse = 5 * (pc.nlev - 1) + 1;
+    return 6 + 2 * (coarse + 1);
+}
+
+template <typename T>
+cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                             const Precond<T>& pc, cudaStream_t s) {
+    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, s)));
     k_finish_s_exit<<<1, 1, 0, s>>>(rs.sc);
     return cudaGetLastError();
 }
 
-template <int K, typename T, typename TM>
-__global__ void k_reset_done(KrylovScalars* sc) {
-    sc->done = 0;
-    sc->s_exit = 0;
-    sc->rho = 1.0;
-}
-
-template <typename T, typename TM>
-cudaError_t krylov_spmv_only(const BsrOp<TM>& A, const BicgVectors<T>& v, const ReduceScratch& rs, int reps,
-                             cudaStream_t s) {
-    k_reset_done<1, T, TM><<<1, 1, 0, s>>>(rs.sc);
-    for (int r = 0; r < reps; ++r) {
-        HO2D_KSWITCH(A.K, (k_spmv_v<KK, T, TM><<<kgrid<KK>(A.N), Shape<KK>::THREADS, 0, s>>>(A, v, rs)));
-    }
+template <typename T>
+cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
+                        const ReduceScratch& rs, cudaStream_t s) {
+    cudaError_t e = launch_trace<T>(op.K, op.g.N, x, xtv, xtg, op.b, s);
+    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
+                                                                                                  rs)));
     return cudaGetLastError();
 }
 
-template <typename TM>
-cudaError_t residual_fp64(const BsrOp<TM>& A, const double* b, const double* x, double* r, const ReduceScratch& rs,
-                          cudaStream_t s) {
-    HO2D_KSWITCH(A.K, (k_residual64<KK, TM><<<kgrid<KK>(A.N), Shape<KK>::THREADS, 0, s>>>(A, b, x, r, rs)));
+template <typename T>
+cudaError_t mf_apply_op(const MfOp<T>& op, const T* x, T* xtv, T* xtg, T* y, cudaStream_t s) {
+    cudaError_t e = launch_trace<T>(op.K, op.g.N, x, xtv, xtg, op.b, s);
+    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t mf_apply_only(const MfOp<T>& op, const T* x, const T* xtv, const T* xtg, T* y, int reps, cudaStream_t s) {
+    for (int r = 0; r < reps; ++r)
+        HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
     return cudaGetLastError();
 }
 
@@ -415,28 +629,23 @@ cudaError_t launch_copy_d2f(const double* a, float* b, size_t n, cudaStream_t s)
     if (n) k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, n);
     return cudaGetLastError();
 }
-cudaError_t launch_copy_f2d(const float* a, double* b, size_t n, cudaStream_t s) {
-    if (n) k_f2d<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, n);
-    return cudaGetLastError();
-}
 cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s) {
     if (n) k_axpy_f2d<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(e, x, n);
     return cudaGetLastError();
 }
 
-template cudaError_t krylov_init<double, double>(const BsrOp<double>&, const BicgVectors<double>&,
-                                                 const ReduceScratch&, double, cudaStream_t);
-template cudaError_t krylov_iteration<double, double>(const BsrOp<double>&, const BicgVectors<double>&,
-                                                      const ReduceScratch&, int, cudaStream_t);
-template cudaError_t krylov_init<float, float>(const BsrOp<float>&, const BicgVectors<float>&, const ReduceScratch&,
-                                               double, cudaStream_t);
-template cudaError_t krylov_iteration<float, float>(const BsrOp<float>&, const BicgVectors<float>&,
-                                                    const ReduceScratch&, int, cudaStream_t);
-template cudaError_t krylov_spmv_only<double, double>(const BsrOp<double>&, const BicgVectors<double>&,
-                                                      const ReduceScratch&, int, cudaStream_t);
-template cudaError_t krylov_spmv_only<float, float>(const BsrOp<float>&, const BicgVectors<float>&,
-                                                    const ReduceScratch&, int, cudaStream_t);
-template cudaError_t residual_fp64<double>(const BsrOp<double>&, const double*, const double*, double*,
-                                           const ReduceScratch&, cudaStream_t);
+#define HO2D_INSTANTIATE_KRYLOV(T)                                                                                \
+    template cudaError_t krylov_init<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, double,     \
+                                        cudaStream_t);                                                            \
+    template cudaError_t krylov_iteration<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, int,    \
+                                             const Precond<T>&, cudaStream_t);                                    \
+    template int krylov_launches_per_iteration<T>(const Precond<T>&);                                             \
+    template cudaError_t mf_residual<T>(const MfOp<T>&, const double*, const T*, T*, T*, double*,                 \
+                                        const ReduceScratch&, cudaStream_t);                                      \
+    template cudaError_t mf_apply_op<T>(const MfOp<T>&, const T*, T*, T*, T*, cudaStream_t);                      \
+    template cudaError_t mf_apply_only<T>(const MfOp<T>&, const T*, const T*, const T*, T*, int, cudaStream_t);
+
+HO2D_INSTANTIATE_KRYLOV(double)
+HO2D_INSTANTIATE_KRYLOV(float)
 
 }  // namespace ho2d

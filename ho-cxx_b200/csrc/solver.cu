@@ -9,10 +9,15 @@
 //                  + k = dt (adv + diff) + the RK combination of solve_advection_diffusion
 // Nothing crosses PCIe inside a step except the Krylov convergence flag polled by the host.
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <type_traits>
 
 #include "device.cuh"
 #include "fr_launch.hpp"
+#include "host_amg.hpp"
 #include "solver.hpp"
 
 namespace ho2d {
@@ -49,10 +54,25 @@ struct DeviceState {
     DeviceBuffer omega, acc, psi64, rhs, rres;
     DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
     // Poisson operator and Krylov workspace
-    DeviceBuffer A64, dinv64, bcol, A32, dinv32;
+    // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
+    DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol, zero_bc;
     DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
+    DeviceBuffer ktv, ktg, kxtv, kxtg;  // face traces of the Krylov operand and of x
     DeviceBuffer partials, counter, scalars;
     KrylovScalars* h_sc = nullptr;
+    // two-level preconditioner: fine scratch, coarse hierarchy (per level: A, P, R CSR
+    // with FP64 and FP32 values, SPAI-0 weights, work vectors)
+    struct CsrBufs {
+        DeviceBuffer ptr, col, v64, v32;
+    };
+    struct LevelBufs {
+        CsrBufs A, P, R;
+        DeviceBuffer m64, m32, f, u, t, u2;
+    };
+    std::vector<std::unique_ptr<LevelBufs>> lev;
+    DeviceBuffer dense64, dense32;
+    Precond<double> pc64;
+    Precond<float> pc32;
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
@@ -93,9 +113,25 @@ cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
     return upload(buf, c);
 }
 
+cudaError_t upload_csr(DeviceState::CsrBufs& b, const Csr& A) {
+    cudaError_t e;
+    if ((e = upload(b.ptr, A.ptr.empty() ? std::vector<int>{0} : A.ptr)) != cudaSuccess) return e;
+    if ((e = upload(b.col, A.col.empty() ? std::vector<int>{0} : A.col)) != cudaSuccess) return e;
+    if ((e = upload(b.v64, A.val.empty() ? std::vector<double>{0.0} : A.val)) != cudaSuccess) return e;
+    return upload_as<float>(b.v32, A.val.empty() ? std::vector<double>{0.0} : A.val);
+}
+
+template <typename TM>
+DevCsr<TM> view(const DeviceState::CsrBufs& b, int n, bool f32) {
+    return DevCsr<TM>{n, b.ptr.as<int>(), b.col.as<int>(), f32 ? (const TM*)b.v32.get() : (const TM*)b.v64.get()};
+}
+
 }  // namespace
 
-Solver::Solver() : d_(new DeviceState) {}
+Solver::Solver() : d_(new DeviceState) {
+    const char* v = std::getenv("HO2D_VERBOSE");
+    verbose_ = v && v[0] && v[0] != '0';
+}
 Solver::~Solver() = default;
 
 Error Solver::cuda(cudaError_t e, const char* what) {
@@ -188,11 +224,21 @@ Error Solver::setup() {
     const std::vector<double> zf(nf, 0.0);
     for (DeviceBuffer* b : {&d.psi_tv, &d.psi_tg, &d.w_tv, &d.w_tg, &d.U_t}) HO2D_CUDA(upload(*b, zf), "alloc traces");
     // Poisson operator
-    HO2D_CUDA(upload(d.A64, op_.blocks), "upload Poisson blocks");
+    // row sums of every block (the two-level smoother's A e for element-wise constant e)
+    op_.rowsum.assign((size_t)N * 5 * K2, 0.0);
+    for (size_t eb = 0; eb < (size_t)N * 5; ++eb) {
+        const double* blk = &op_.blocks[eb * K2 * K2];
+        for (int rs = 0; rs < K2; ++rs)
+            for (int ij = 0; ij < K2; ++ij) op_.rowsum[eb * K2 + ij] += blk[rs * K2 + ij];
+    }
     HO2D_CUDA(upload(d.dinv64, op_.dinv), "upload block-Jacobi");
+    HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
-    d.A32.reset();
+    HO2D_CUDA(upload(d.zero_bc, std::vector<double>(std::max<size_t>(1, (size_t)neb * K), 0.0)), "alloc");
+    for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
+    d.rowsum32.reset();
+    HO2D_TRY(setup_preconditioner());
     for (auto& b : d.kv) HO2D_CUDA(upload(b, zv), "alloc Krylov");
     const int mb = krylov_max_blocks(K, N);
     HO2D_CUDA(upload(d.partials, std::vector<double>((size_t)4 * mb, 0.0)), "alloc partials");
@@ -206,13 +252,73 @@ Error Solver::setup() {
     return {0, ""};
 }
 
+// Builds the P0 coarse hierarchy on the host and the device views of both precisions.
+// HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight.
+Error Solver::setup_preconditioner() {
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el;
+    d.pc64 = Precond<double>();
+    d.pc32 = Precond<float>();
+    d.lev.clear();
+    const char* mode = std::getenv("HO2D_PRECOND");
+    if (mode && std::string(mode) == "bj") return {0, ""};
+    const char* om = std::getenv("HO2D_MG_OMEGA");
+    const double omega = om ? std::atof(om) : 1.0;
+    CoarseHierarchy H;
+    HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H));
+    if ((int)H.levels.size() > kMaxLevels) return {4, "coarse hierarchy too deep"};
+    const int nl = (int)H.levels.size();
+    for (int l = 0; l < nl; ++l) {
+        const AmgLevel& L = H.levels[l];
+        auto b = std::unique_ptr<DeviceState::LevelBufs>(new DeviceState::LevelBufs);
+        HO2D_CUDA(upload_csr(b->A, L.A), "upload coarse A");
+        HO2D_CUDA(upload_csr(b->P, L.P), "upload coarse P");
+        HO2D_CUDA(upload_csr(b->R, L.R), "upload coarse R");
+        HO2D_CUDA(upload(b->m64, L.m), "upload smoother");
+        HO2D_CUDA(upload_as<float>(b->m32, L.m), "upload smoother");
+        const std::vector<double> z(std::max(1, L.A.n), 0.0);
+        for (DeviceBuffer* v : {&b->f, &b->u, &b->t, &b->u2}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
+        d.lev.push_back(std::move(b));
+    }
+    HO2D_CUDA(upload(d.dense64, H.dense_inv), "upload dense");
+    HO2D_CUDA(upload_as<float>(d.dense32, H.dense_inv), "upload dense");
+    auto fill = [&](auto& pc, bool f32) {
+        using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense_inv)>::type>::type;
+        using TM = T;
+        pc.nlev = nl;
+        pc.omega = omega;
+        pc.dense_inv = f32 ? (const TM*)d.dense32.get() : (const TM*)d.dense64.get();
+        for (int l = 0; l < nl; ++l) {
+            const AmgLevel& L = H.levels[l];
+            auto& b = *d.lev[l];
+            auto& c = pc.lev[l];
+            c.n = L.A.n;
+            c.A = view<TM>(b.A, L.A.n, f32);
+            c.P = view<TM>(b.P, L.P.n, f32);
+            c.R = view<TM>(b.R, L.R.n, f32);
+            c.m = f32 ? (const TM*)b.m32.get() : (const TM*)b.m64.get();
+            c.f = b.f.as<T>();
+            c.u = b.u.as<T>();
+            c.t = b.t.as<T>();
+            c.u2 = b.u2.as<T>();
+            c.out = (l == nl - 1) ? c.u : c.u2;
+        }
+    };
+    fill(d.pc64, false);
+    fill(d.pc32, true);
+    coarse_levels_ = nl;
+    coarse_sizes_.clear();
+    for (const auto& L : H.levels) coarse_sizes_.push_back(L.A.n);
+    return {0, ""};
+}
+
 Error Solver::upload_precision_arrays() {
     DeviceState& d = *d_;
     if (d.have32) return {0, ""};
     const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
     for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
-    HO2D_CUDA(upload_as<float>(d.A32, op_.blocks), "upload fp32 blocks");
     HO2D_CUDA(upload_as<float>(d.dinv32, op_.dinv), "upload fp32 block-Jacobi");
+    HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
     d.have32 = true;
     return {0, ""};
 }
@@ -233,90 +339,6 @@ Error Solver::set_precision(int mode) {
     return {0, ""};
 }
 
-// ------------------------------------------------------------------ Poisson
-Error Solver::poisson_solve() {
-    DeviceState& d = *d_;
-    const int N = mesh_.n_el, K = in_.knod;
-    const size_t nv = (size_t)N * K * K;
-    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
-    if (timing_) HO2D_CUDA(cudaEventRecord(d.evp0, d.stream), "event");
-    auto poll = [&]() -> Error {
-        HO2D_CUDA(cudaMemcpyAsync(d.h_sc, d.scalars.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream),
-                  "poll");
-        HO2D_CUDA(cudaStreamSynchronize(d.stream), "poll");
-        return {0, ""};
-    };
-    // runs BiCGSTAB to completion on (A, v); returns iterations
-    auto run = [&](auto A, auto v, double tol, int& iters) -> Error {
-        HO2D_CUDA(krylov_init(A, v, rs, tol, d.stream), "krylov init");
-        launches_ += 2;
-        HO2D_TRY(poll());
-        int chunk = std::max(1, prev_iters_ - 1);
-        while (!d.h_sc->done) {
-            for (int c = 0; c < chunk; ++c) {
-                HO2D_CUDA(krylov_iteration(A, v, rs, max_iter_, d.stream), "krylov iteration");
-                launches_ += 6;
-            }
-            HO2D_TRY(poll());
-            chunk = 2;
-        }
-        iters = d.h_sc->it;
-        return {0, ""};
-    };
-    last_iters_ = 0;
-    if (!mixed_) {
-        BsrOp<double> A{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
-        BicgVectors<double> v{d.psi64.as<double>(), d.kv[0].as<double>(), d.kv[1].as<double>(), d.kv[2].as<double>(),
-                              d.kv[3].as<double>(), d.kv[4].as<double>(), d.kv[5].as<double>(), d.kv[6].as<double>(),
-                              d.kv[7].as<double>(), d.rhs.as<double>()};
-        int it = 0;
-        HO2D_TRY(run(A, v, tol_, it));
-        last_iters_ = it;
-        last_res_ = d.h_sc->bnorm2 > 0 ? std::sqrt(d.h_sc->rnorm2 / d.h_sc->bnorm2) : 0.0;
-    } else {
-        // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator
-        BsrOp<double> A64{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
-        BsrOp<float> A32{N, K, d.A32.as<float>(), d.bcol.as<int>(), d.dinv32.as<float>()};
-        BicgVectors<float> v{d.kv[8].as<float>(), d.kv[0].as<float>(), d.kv[1].as<float>(), d.kv[2].as<float>(),
-                             d.kv[3].as<float>(), d.kv[4].as<float>(), d.kv[5].as<float>(), d.kv[6].as<float>(),
-                             d.kv[7].as<float>(), d.kv[9].as<float>()};
-        for (int sweep = 0; sweep < 20; ++sweep) {
-            HO2D_CUDA(residual_fp64(A64, d.rhs.as<double>(), d.psi64.as<double>(), d.rres.as<double>(), rs, d.stream),
-                      "fp64 residual");
-            launches_ += 1;
-            HO2D_TRY(poll());
-            const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
-            last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
-            if (bn == 0.0) {
-                HO2D_CUDA(cudaMemsetAsync(d.psi64.get(), 0, nv * 8, d.stream), "memset");
-                last_res_ = 0.0;
-                break;
-            }
-            if (!(rn == rn)) break;  // NaN: reported by the caller
-            if (rn <= tol_ * tol_ * bn || last_iters_ >= max_iter_) break;
-            HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
-            HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
-            launches_ += 1;
-            int it = 0;
-            HO2D_TRY(run(A32, v, 1e-5, it));
-            last_iters_ += it;
-            HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
-            launches_ += 1;
-        }
-    }
-    prev_iters_ = std::max(1, mixed_ ? last_iters_ / 2 : last_iters_);
-    if (timing_) {
-        HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");
-        HO2D_CUDA(cudaEventSynchronize(d.evp1), "event");
-        float ms = 0.f;
-        HO2D_CUDA(cudaEventElapsedTime(&ms, d.evp0, d.evp1), "event");
-        poisson_ms_acc_ += ms;
-    }
-    if (!(last_res_ == last_res_)) return {7, "non-finite values in the Poisson solve (vorticity blew up)"};
-    return {0, ""};
-}
-
-// ------------------------------------------------------------------ stages
 template <typename T>
 static FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
     DeviceBuffer* mm = f32 ? d.m32 : d.m64;
@@ -341,6 +363,131 @@ static FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
     return g;
 }
 
+template <typename T>
+static MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
+    MfOp<T> op;
+    op.K = K;
+    op.g = geom_of<T>(d, m, f32);
+    op.b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
+    op.zero_bc = d.zero_bc.as<double>();
+    op.dinv = f32 ? (const T*)d.dinv32.get() : (const T*)d.dinv64.get();
+    op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
+    op.bcol = d.bcol.as<int>();
+    return op;
+}
+
+template <typename T>
+static BicgVectors<T> krylov_vectors(DeviceState& d, T* x, const T* b) {
+    BicgVectors<T> v;
+    v.x = x;
+    v.r = d.kv[0].as<T>();
+    v.rhat = d.kv[1].as<T>();
+    v.p = d.kv[2].as<T>();
+    v.v = d.kv[3].as<T>();
+    v.s = d.kv[4].as<T>();
+    v.t = d.kv[5].as<T>();
+    v.ph = d.kv[6].as<T>();
+    v.sh = d.kv[7].as<T>();
+    v.b = b;
+    v.tv = d.ktv.as<T>();
+    v.tg = d.ktg.as<T>();
+    v.xtv = d.kxtv.as<T>();
+    v.xtg = d.kxtg.as<T>();
+    return v;
+}
+
+// ------------------------------------------------------------------ Poisson
+Error Solver::poisson_solve() {
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t nv = (size_t)N * K * K;
+    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
+    if (timing_) HO2D_CUDA(cudaEventRecord(d.evp0, d.stream), "event");
+    auto poll = [&]() -> Error {
+        HO2D_CUDA(cudaMemcpyAsync(d.h_sc, d.scalars.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream),
+                  "poll");
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "poll");
+        return {0, ""};
+    };
+    // runs BiCGSTAB to completion on (A, v); returns iterations
+    auto run = [&](auto A, auto v, const auto& pc, double tol, int& iters) -> Error {
+        HO2D_CUDA(krylov_init(A, v, rs, tol, d.stream), "krylov init");
+        launches_ += 3;
+        HO2D_TRY(poll());
+        int chunk = std::max(1, prev_iters_ - 1);
+        while (!d.h_sc->done) {
+            for (int c = 0; c < chunk; ++c) {
+                HO2D_CUDA(krylov_iteration(A, v, rs, max_iter_, pc, d.stream), "krylov iteration");
+                launches_ += krylov_launches_per_iteration(pc);
+            }
+            HO2D_TRY(poll());
+            chunk = 2;
+        }
+        iters = d.h_sc->it;
+        return {0, ""};
+    };
+    last_iters_ = 0;
+    int sweeps = 0;
+    bool finite = true;
+    if (!mixed_) {
+        const MfOp<double> A = make_op<double>(d, mesh_, K, false);
+        const BicgVectors<double> v = krylov_vectors<double>(d, d.psi64.as<double>(), d.rhs.as<double>());
+        int it = 0;
+        HO2D_TRY(run(A, v, d.pc64, tol_, it));
+        last_iters_ = it;
+        const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
+        finite = std::isfinite(bn) && std::isfinite(rn);
+        last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
+    } else {
+        // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator: every
+        // exit passes through an FP64 residual of the current psi
+        const MfOp<double> A64 = make_op<double>(d, mesh_, K, false);
+        const MfOp<float> A32 = make_op<float>(d, mesh_, K, true);
+        const BicgVectors<float> v = krylov_vectors<float>(d, d.kv[8].as<float>(), d.kv[9].as<float>());
+        for (;; ++sweeps) {
+            HO2D_CUDA(mf_residual<double>(A64, d.rhs.as<double>(), d.psi64.as<double>(), d.kxtv.as<double>(),
+                                          d.kxtg.as<double>(), d.rres.as<double>(), rs, d.stream),
+                      "fp64 residual");
+            launches_ += 2;
+            HO2D_TRY(poll());
+            const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
+            finite = std::isfinite(bn) && std::isfinite(rn);
+            last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
+            if (!finite) break;
+            if (bn == 0.0) {
+                HO2D_CUDA(cudaMemsetAsync(d.psi64.get(), 0, nv * 8, d.stream), "memset");
+                last_res_ = 0.0;
+                break;
+            }
+            if (rn <= tol_ * tol_ * bn || sweeps >= 30) break;
+            HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
+            HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
+            launches_ += 1;
+            int it = 0;
+            HO2D_TRY(run(A32, v, d.pc32, inner_tol_, it));
+            last_iters_ += it;
+            HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
+            launches_ += 1;
+        }
+    }
+    ++n_solves_;
+    if (verbose_)
+        std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e\n", n_solves_, last_iters_,
+                     sweeps, last_res_);
+    prev_iters_ = std::max(1, mixed_ ? last_iters_ / std::max(1, sweeps) : last_iters_);
+    if (timing_) {
+        HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");
+        HO2D_CUDA(cudaEventSynchronize(d.evp1), "event");
+        float ms = 0.f;
+        HO2D_CUDA(cudaEventElapsedTime(&ms, d.evp0, d.evp1), "event");
+        poisson_ms_acc_ += ms;
+    }
+    if (!finite || !std::isfinite(last_res_))
+        return {7, "non-finite values in the Poisson solve (vorticity blew up)"};
+    return {0, ""};
+}
+
+// ------------------------------------------------------------------ stages
 template <typename T>
 Error Solver::stage_t(double coeff, int rk_stage, bool update) {
     DeviceState& d = *d_;
@@ -495,41 +642,55 @@ Error Solver::time_steps(int nsteps, double* total_ms, double* poisson_ms) {
     return {0, ""};
 }
 
-// Average duration of the Poisson SpMV kernel (the solver's own k_spmv_v) over `reps`
+// Average duration of the Poisson operator kernel (k_mf_apply: y = A x, matrix-free, the
+// same device code as every operator application inside the Krylov solve) over `reps`
 // launches between CUDA events on the handle's stream, and its algorithmic bytes per
-// launch: every stored block entry once, x and rhat once per element row, v written once,
-// the block-column table once.
+// launch: x, the 5 volume metrics and y once per DOF, the face traces (value and normal
+// derivative) and the 3 face metrics once per face point, 8 connectivity words per element.
 Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     if (!setup_done_) return {1, "not set up"};
     if (reps <= 0) return {1, "reps must be positive"};
     DeviceState& d = *d_;
     HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
     const int N = mesh_.n_el, K = in_.knod;
-    const size_t K2 = (size_t)K * K;
-    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
-    size_t nblocks = 0;
-    for (int c : op_.block_col) nblocks += c >= 0;
     const size_t w = mixed_ ? 4 : 8;
-    if (bytes) *bytes = double(nblocks * K2 * K2 * w + 3 * (size_t)N * K2 * w + op_.block_col.size() * 4);
-    HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+    if (bytes) *bytes = double((size_t)N * ((7 * (size_t)K * K + 20 * (size_t)K) * w + 32));
     if (!mixed_) {
-        BsrOp<double> A{N, K, d.A64.as<double>(), d.bcol.as<int>(), d.dinv64.as<double>()};
-        BicgVectors<double> v{d.psi64.as<double>(), d.kv[0].as<double>(), d.kv[1].as<double>(), d.kv[2].as<double>(),
-                              d.kv[3].as<double>(), d.kv[4].as<double>(), d.kv[5].as<double>(), d.kv[6].as<double>(),
-                              d.kv[7].as<double>(), d.rhs.as<double>()};
-        HO2D_CUDA(krylov_spmv_only(A, v, rs, reps, d.stream), "spmv");
+        const MfOp<double> op = make_op<double>(d, mesh_, K, false);
+        HO2D_CUDA(mf_apply_op<double>(op, d.psi64.as<double>(), d.kxtv.as<double>(), d.kxtg.as<double>(),
+                                      d.kv[5].as<double>(), d.stream), "apply");
+        HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+        HO2D_CUDA(mf_apply_only<double>(op, d.psi64.as<double>(), d.kxtv.as<double>(), d.kxtg.as<double>(),
+                                        d.kv[5].as<double>(), reps, d.stream), "apply");
     } else {
-        BsrOp<float> A{N, K, d.A32.as<float>(), d.bcol.as<int>(), d.dinv32.as<float>()};
-        BicgVectors<float> v{d.kv[8].as<float>(), d.kv[0].as<float>(), d.kv[1].as<float>(), d.kv[2].as<float>(),
-                             d.kv[3].as<float>(), d.kv[4].as<float>(), d.kv[5].as<float>(), d.kv[6].as<float>(),
-                             d.kv[7].as<float>(), d.kv[9].as<float>()};
-        HO2D_CUDA(krylov_spmv_only(A, v, rs, reps, d.stream), "spmv");
+        const MfOp<float> op = make_op<float>(d, mesh_, K, true);
+        HO2D_CUDA(mf_apply_op<float>(op, d.psiT.as<float>(), d.kxtv.as<float>(), d.kxtg.as<float>(),
+                                     d.kv[5].as<float>(), d.stream), "apply");
+        HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+        HO2D_CUDA(mf_apply_only<float>(op, d.psiT.as<float>(), d.kxtv.as<float>(), d.kxtg.as<float>(),
+                                       d.kv[5].as<float>(), reps, d.stream), "apply");
     }
     HO2D_CUDA(cudaEventRecord(d.ev1, d.stream), "event");
     HO2D_CUDA(cudaEventSynchronize(d.ev1), "event");
     float ms = 0.f;
     HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
     if (avg_ms) *avg_ms = ms / reps;
+    return {0, ""};
+}
+
+// y = A psi on the device in FP64 (the matrix-free Poisson operator), for checks
+Error Solver::apply_poisson(const double* x, double* y) {
+    if (!setup_done_) return {1, "not set up"};
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    HO2D_CUDA(cudaMemcpy(d.kv[4].get(), x, nv * 8, cudaMemcpyHostToDevice), "copy");
+    const MfOp<double> op = make_op<double>(d, mesh_, in_.knod, false);
+    HO2D_CUDA(mf_apply_op<double>(op, d.kv[4].as<double>(), d.kxtv.as<double>(), d.kxtg.as<double>(),
+                                  d.kv[5].as<double>(), d.stream), "apply");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    HO2D_CUDA(cudaMemcpy(y, d.kv[5].get(), nv * 8, cudaMemcpyDeviceToHost), "copy");
     return {0, ""};
 }
 

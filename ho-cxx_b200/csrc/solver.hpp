@@ -47,6 +47,7 @@ class Solver {
     Error set_precision(int mode);
     Error time_steps(int nsteps, double* total_ms, double* poisson_ms);
     Error profile_spmv(int reps, double* avg_ms, double* bytes);
+    Error apply_poisson(const double* x, double* y);
 
     Error get_volume(int which, double* out);  // [N][K][K]
     Error get_velocity(double* out);           // [N][K][K][2]
@@ -62,6 +63,7 @@ class Solver {
     int n_eb() const { return mesh_.n_eb; }
     int lnod() const { return mesh_.lnod; }
     double time() const { return time_; }
+    void set_time(double t) { time_ = t; }
     double dt() const { return in_.dt; }
     int precision() const { return mixed_ ? 1 : 0; }
     int last_poisson_iterations() const { return last_iters_; }
@@ -80,6 +82,7 @@ class Solver {
     template <typename T>
     Error velocity_only_t();
     Error upload_precision_arrays();
+    Error setup_preconditioner();
     Error cuda(cudaError_t e, const char* what);
 
     Input in_;
@@ -96,6 +99,11 @@ class Solver {
     int last_iters_ = 0, prev_iters_ = 8;
     double last_res_ = 0.0;
     int64_t launches_ = 0;
+    long n_solves_ = 0;
+    int coarse_levels_ = 0;
+    std::vector<int> coarse_sizes_;
+    double inner_tol_ = 1e-4;        // FP32 inner solve: relative reduction per refinement sweep
+    bool verbose_ = false;           // HO2D_VERBOSE=1: one line per Poisson solve on stderr
     bool timing_ = false;
     double poisson_ms_acc_ = 0.0;
     std::unique_ptr<DeviceState> d_;

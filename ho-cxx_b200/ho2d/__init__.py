@@ -148,6 +148,9 @@ class HO_2D:
         self._check(self._lib.ho2d_get_time(self._h, ctypes.byref(t), ctypes.byref(dt)))
         return t.value, dt.value
 
+    def set_time(self, t: float) -> None:
+        self._check(self._lib.ho2d_set_time(self._h, float(t)))
+
     def time_steps(self, nsteps: int):
         """Advance nsteps and return (total device ms, Poisson device ms) from CUDA events."""
         tot, pois = ctypes.c_double(), ctypes.c_double()
@@ -159,6 +162,13 @@ class HO_2D:
         ms, by = ctypes.c_double(), ctypes.c_double()
         self._check(self._lib.ho2d_profile_spmv(self._h, int(reps), ctypes.byref(ms), ctypes.byref(by)))
         return ms.value, by.value
+
+    def apply_poisson(self, x) -> np.ndarray:
+        """y = A x with the device's (matrix-free) Poisson operator, FP64."""
+        a = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros_like(a)
+        self._check(self._lib.ho2d_apply_poisson(self._h, a.size, capi.dptr(a), capi.dptr(out)))
+        return out
 
     def launch_count(self) -> int:
         n = ctypes.c_int64()

@@ -47,8 +47,10 @@ SIGNATURES = {
     "ho2d_set_poisson_tolerance": (ctypes.c_int, [_P, _D, _I]),
     "ho2d_poisson_stats": (ctypes.c_int, [_P, _IP, _DP]),
     "ho2d_get_time": (ctypes.c_int, [_P, _DP, _DP]),
+    "ho2d_set_time": (ctypes.c_int, [_P, _D]),
     "ho2d_time_steps": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_profile_spmv": (ctypes.c_int, [_P, _I, _DP, _DP]),
+    "ho2d_apply_poisson": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_last_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "ho2d_last_error": (ctypes.c_char_p, [_P]),
 }

@@ -114,13 +114,22 @@ int ho2d_set_poisson_tolerance(ho2d_solver* handle, double rel_tol, int32_t max_
 int ho2d_poisson_stats(ho2d_solver* handle, int32_t* iterations, double* rel_residual);
 /* Current solver time and time-step size. */
 int ho2d_get_time(ho2d_solver* handle, double* time, double* dt);
+/* Sets the current solver time (the reference's time_start / current_time,
+ * src/HO_2D.hpp:164), e.g. to restart a run or to start inside the pulsatile inflow
+ * cycle of problem types 2 and 3. */
+int ho2d_set_time(ho2d_solver* handle, double time);
 /* Runs nsteps time steps and reports device time between CUDA events recorded on the
  * handle's stream around them: total milliseconds and the part spent in Poisson solves. */
 int ho2d_time_steps(ho2d_solver* handle, int32_t nsteps, double* total_ms, double* poisson_ms);
-/* Runs the Poisson solver's block-SpMV kernel `reps` times back to back (on the current
- * Krylov vectors, in the active precision) between CUDA events on the handle's stream;
- * returns the average launch duration and the algorithmic bytes one launch must move. */
+/* Runs the Poisson operator kernel (matrix-free y = A psi, the kernel every operator
+ * application of the Krylov solve uses) `reps` times back to back on the current psi, in
+ * the active precision, between CUDA events on the handle's stream; returns the average
+ * launch duration and the algorithmic bytes one launch must move. */
 int ho2d_profile_spmv(ho2d_solver* handle, int32_t reps, double* avg_ms, double* bytes_per_launch);
+/* y = A x in FP64 with the device's Poisson operator: the matrix the reference assembles
+ * in form_Laplace_operator_matrix (src/HO_2D.cpp:1533-1804), applied matrix-free;
+ * len = N_el*Knod*Knod. */
+int ho2d_apply_poisson(ho2d_solver* handle, int32_t len, const double* x, double* y);
 /* Total number of kernel launches this handle has issued since it was created. */
 int ho2d_last_launch_count(ho2d_solver* handle, int64_t* launches);
 /* Text of the last error on this handle ("" if none). The pointer stays valid until the

@@ -25,6 +25,7 @@
 //   --time N               time N steps (no dumps) and print a JSON line
 //   --time-stages N        time N RK stages (Euler_time_integrate on the current vorticity,
 //                          coefficients cycling 0, .5, .5, 1) and print a JSON line
+//   --t0 T                 start the time loop at time T instead of 0
 //   --verbose              keep the reference's stdout
 #include "HO_2D.hpp"
 
@@ -105,7 +106,7 @@ int main(int argc, char** argv) {
     }
     std::string input = argv[1], outdir = argv[2];
     bool do_setup = false, verbose = false, do_stage = false;
-    double stage_coeff = 0.0, dt_override = -1.0;
+    double stage_coeff = 0.0, dt_override = -1.0, t0 = 0.0;
     long nsteps = 0, every = 0, ntime = 0, nstages = 0;
     std::string init_vort, lid;
     for (int i = 3; i < argc; ++i) {
@@ -120,6 +121,7 @@ int main(int argc, char** argv) {
         else if (a == "--every" && i + 1 < argc) every = std::atol(argv[++i]);
         else if (a == "--time" && i + 1 < argc) ntime = std::atol(argv[++i]);
         else if (a == "--time-stages" && i + 1 < argc) nstages = std::atol(argv[++i]);
+        else if (a == "--t0" && i + 1 < argc) t0 = std::atof(argv[++i]);
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     mkdir(outdir.c_str(), 0755);
@@ -159,7 +161,7 @@ int main(int argc, char** argv) {
         std::copy(w.begin(), w.end(), &ho.BC_parl_vel[0][0]);
     }
     for (size_t i = 0; i < N * K * K; ++i) ho.vorticity[0][0][i] = ho.initial_vorticity[0][0][i];
-    ho.current_time = ho.time_start;
+    ho.current_time = ho.time_start + t0;
 
     if (do_setup) {
         std::vector<int32_t> nbr(N * 4), nside(N * 4), onb(N * 4), bidx(N * 4);
