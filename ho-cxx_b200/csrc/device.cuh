@@ -13,7 +13,7 @@ constexpr int kDirichlet = 0, kNeumann = 1;
 template <int K>
 struct Shape {
     static constexpr int K2 = K * K;
-    static constexpr int EPB = (256 / K2) > 64 ? 64 : ((256 / K2) > 0 ? (256 / K2) : 1);
+    static constexpr int EPB = (256 / K2) > 32 ? 32 : ((256 / K2) > 0 ? (256 / K2) : 1);
     static constexpr int THREADS = ((EPB * K2 + 31) / 32) * 32;  // whole warps; tail threads idle
     static constexpr int NF = 4 * K;  // face points per element
 };

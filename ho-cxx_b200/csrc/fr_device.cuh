@@ -10,6 +10,17 @@
 
 namespace ho2d {
 
+// Copies the 1-D basis tables from the kernel-parameter bank into shared memory: the
+// FR loops index them per thread, which would serialise constant-cache reads. The
+// caller synchronises before use.
+template <typename T>
+__device__ __forceinline__ void stage_bases(DevBases<T>& dst, const DevBases<T>& src) {
+    constexpr int NW = (int)(sizeof(DevBases<T>) / sizeof(T));
+    const T* s = reinterpret_cast<const T*>(&src);
+    T* d = reinterpret_cast<T*>(&dst);
+    for (int t = threadIdx.x; t < NW; t += blockDim.x) d[t] = s[t];
+}
+
 template <int K>
 __device__ __forceinline__ int bf_index(int side, int k) {
     return (side / 2) * (K - 2 * k - 1) + k;

@@ -27,8 +27,10 @@ namespace ho2d {
 // ----------------------------------------------------------------------------------
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) trace_kernel(int N, const T* __restrict__ f, T* __restrict__ tv,
-                                                                   T* __restrict__ tg, DevBases<T> b) {
+                                                                   T* __restrict__ tg, DevBases<T> bp) {
     using S = Shape<K>;
+    __shared__ DevBases<T> b;
+    stage_bases(b, bp);
     __shared__ T s_f[S::EPB][S::K2];
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
@@ -46,9 +48,11 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) trace_kernel(int N, const T
 }
 
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g, DevBases<T> b, BcArrays bc,
+__global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g, DevBases<T> bp, BcArrays bc,
                                                                       VelocityArgs<T> a) {
     using S = Shape<K>;
+    __shared__ DevBases<T> b;
+    stage_bases(b, bp);
     constexpr int K2 = S::K2, NF = S::NF, EPB = S::EPB;
     __shared__ T s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2], s_w[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
     __shared__ T s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF];
@@ -122,9 +126,11 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g
 }
 
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) residual_kernel(FrGeom<T> g, DevBases<T> b, BcArrays bc,
+__global__ void __launch_bounds__(Shape<K>::THREADS) residual_kernel(FrGeom<T> g, DevBases<T> bp, BcArrays bc,
                                                                       ResidualArgs<T> a) {
     using S = Shape<K>;
+    __shared__ DevBases<T> b;
+    stage_bases(b, bp);
     constexpr int K2 = S::K2, NF = S::NF, EPB = S::EPB;
     __shared__ T s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
     __shared__ T s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF], s_ut[EPB][NF],

@@ -121,6 +121,10 @@ cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const R
                              const Precond<T>& pc, cudaStream_t s);
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc);
+// a whole solve (initial residual + device-side while loop of iterations) as a CUDA graph
+template <typename T>
+cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+                                 int max_iter, const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out);
 // r = b - A x with ||r||^2 -> sc->rnorm2, ||b||^2 -> sc->bnorm2 (traces of x into xtv/xtg)
 template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,

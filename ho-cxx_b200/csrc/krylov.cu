@@ -83,28 +83,181 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     return true;
 }
 
-// Shared-memory working set of one CTA (EPB elements).
+// Shared-memory working set of one CTA (EPB elements) for the operator.
 template <int K, typename T>
 struct MfShared {
     static constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
     T x[EPB][K2], a[EPB][K2], b[EPB][K2];
-    T tv[EPB][NF], tg[EPB][NF], com[EPB][NF], cg[EPB][NF], fb[EPB][NF];
+    // own face: traces (recomputed) and metrics; neighbour face: traces and metrics
+    T tv[EPB][NF], tg[EPB][NF], fA[EPB][NF], fB[EPB][NF], fJ[EPB][NF];
+    T ntv[EPB][NF], ntg[EPB][NF], nfA[EPB][NF], nfB[EPB][NF], nfJ[EPB][NF];
+    T com[EPB][NF], cg[EPB][NF], fb[EPB][NF];
+    int nb[EPB][4], nijp[EPB][4];  // neighbour element / its face; boundary: -1 - switch
+    DevBases<T> bas;               // basis tables staged from the parameter bank
 };
 
-// y = A x at (el, ij); x's own traces are recomputed, the neighbours' come from tv/tg.
-// Collective. Leaves x of the element in sm.x.
+// y = A x at (el, ij) for the homogeneous-boundary Poisson operator: the method-2 FR
+// Laplacian of fr_device.cuh's lap_element, restaged so that all global data arrive in
+// two rounds (own data and connectivity, then the neighbours' face data) and every
+// later phase synchronises through shared memory only. Collective.
 template <int K, typename T>
 __device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
                       MfShared<K, T>& sm, bool active, int le, int el, int ij) {
-    constexpr int K2 = K * K, NF = 4 * K;
-    const int lei = active ? le : 0;
-    if (active) sm.x[le][ij] = x[el * K2 + ij];
+    constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
+    const FrGeom<T>& g = op.g;
+    stage_bases(sm.bas, op.b);
+    const DevBases<T>& b = sm.bas;
+    const int j = ij / K, i = ij % K;
+    // round 1: x, volume metrics, connectivity
+    T xx = T(0), xe = T(0), yx = T(0), ye = T(0), J = T(1);
+    if (active) {
+        const int p = el * K2 + ij;
+        sm.x[le][ij] = x[p];
+        xx = g.xxi[p]; xe = g.xeta[p]; yx = g.yxi[p]; ye = g.yeta[p]; J = g.J[p];
+    }
+    for (int f = threadIdx.x; f < EPB * 4; f += blockDim.x) {
+        const int l = f / 4, face = f % 4, e2 = blockIdx.x * EPB + l;
+        if (e2 < g.N) {
+            const int nb = g.face_nb[e2 * 4 + face];
+            sm.nb[l][face] = nb >= 0 ? nb : -1 - g.sw_p[-nb - 1];
+            sm.nijp[l][face] = g.face_nijp[e2 * 4 + face];
+        }
+    }
+    __syncthreads();
+    // round 2: own face metrics and traces, the neighbours' traces and face metrics
+    if (active)
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K;
+            const int q = (el * 4 + ijp) * K + k;
+            sm.fA[le][o] = g.fA[q];
+            sm.fB[le][o] = g.fB[q];
+            sm.fJ[le][o] = g.fJ[q];
+            face_trace<K, T>(sm.x[le], b, o, sm.tv[le][o], sm.tg[le][o]);
+            const int nb = sm.nb[le][ijp];
+            if (nb >= 0) {
+                const int nijp = sm.nijp[le][ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                const int nq = (nb * 4 + nijp) * K + (rev ? K - 1 - k : k);
+                sm.ntv[le][o] = tv[nq];
+                sm.ntg[le][o] = tg[nq];
+                sm.nfA[le][o] = g.fA[nq];
+                sm.nfB[le][o] = g.fB[nq];
+                sm.nfJ[le][o] = g.fJ[nq];
+            }
+        }
+    __syncthreads();
+    // common values: average inside, 0 on Dirichlet faces (homogeneous), Neumann below
+    if (active)
+        for (int o = ij; o < NF; o += K2) {
+            const int nb = sm.nb[le][o / K];
+            sm.com[le][o] = nb >= 0 ? T(0.5) * (sm.tv[le][o] + sm.ntv[le][o]) : T(0);
+        }
+    __syncthreads();
+    // homogeneous Neumann faces: K x K system for the common value (src/HO_2D.cpp:2899-2924)
+    for (int ijp = ij; active && ijp < 4; ijp += K2) {
+        if (sm.nb[le][ijp] != -1 - kNeumann) continue;
+        const int lr = ijp & 1;
+        T M[K][K], r[K], xs[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int o = ijp * K + k;
+            r[k] = -sm.fA[le][o] * (sm.tg[le][o] - sm.tv[le][o] * b.gp[lr]);
+#pragma unroll
+            for (int c = 0; c < K; ++c) M[k][c] = -sm.fB[le][o] * b.D[c * K + k];
+            M[k][k] += sm.fA[le][o] * b.gp[lr];
+        }
+#pragma unroll
+        for (int c = 0; c < K - 1; ++c)
+#pragma unroll
+            for (int r2 = c + 1; r2 < K; ++r2) {
+                const T fct = M[r2][c] / M[c][c];
+                r[r2] -= fct * r[c];
+#pragma unroll
+                for (int cc = c + 1; cc < K; ++cc) M[r2][cc] -= fct * M[c][cc];
+            }
+#pragma unroll
+        for (int r2 = K - 1; r2 >= 0; --r2) {
+            T acc = T(0);
+#pragma unroll
+            for (int cc = r2 + 1; cc < K; ++cc) acc += M[r2][cc] * xs[cc];
+            xs[r2] = (r[r2] - acc) / M[r2][r2];
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) sm.com[le][ijp * K + k] = xs[k];
+    }
+    __syncthreads();
+    // corrected normal fluxes, averaged with the neighbour's on interior faces
+    if (active)
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            const int nb = sm.nb[le][ijp];
+            if (nb == -1 - kNeumann) {
+                sm.cg[le][o] = T(0);
+                continue;
+            }
+            const T com = sm.com[le][o];
+            T cross = T(0);
+#pragma unroll
+            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
+            const T dv = sm.tg[le][o] + (com - sm.tv[le][o]) * b.gp[lr];
+            const T fl = (dv * sm.fA[le][o] - cross * sm.fB[le][o]) / sm.fJ[le][o];
+            if (nb < 0) {
+                sm.cg[le][o] = fl;
+            } else {
+                const int nijp = sm.nijp[le][ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                const int jn = rev ? K - 1 - k : k;
+                T crn = T(0);
+#pragma unroll
+                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
+                const T dvn = sm.ntg[le][o] + (com - sm.ntv[le][o]) * b.gp[nijp & 1];
+                const T fln = (dvn * sm.nfA[le][o] - crn * sm.nfB[le][o]) / sm.nfJ[le][o];
+                sm.cg[le][o] = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
+            }
+        }
+    __syncthreads();
+    // contravariant gradient (src/HO_2D.cpp:2775-2792)
+    T ft = T(0), gt = T(0);
+    if (active) {
+        T dx = T(0), de = T(0);
+#pragma unroll
+        for (int d = 0; d < K; ++d) {
+            dx += sm.x[le][j * K + d] * b.D[d * K + i];
+            de += sm.x[le][d * K + i] * b.D[d * K + j];
+        }
+        dx += (sm.com[le][0 * K + j] - sm.tv[le][0 * K + j]) * b.gR[i * 2 + 0];
+        dx += (sm.com[le][1 * K + j] - sm.tv[le][1 * K + j]) * b.gR[i * 2 + 1];
+        de += (sm.com[le][2 * K + i] - sm.tv[le][2 * K + i]) * b.gR[j * 2 + 0];
+        de += (sm.com[le][3 * K + i] - sm.tv[le][3 * K + i]) * b.gR[j * 2 + 1];
+        ft = (dx * (xe * xe + ye * ye) - de * (xx * xe + yx * ye)) / J;
+        gt = (de * (xx * xx + yx * yx) - dx * (xx * xe + yx * ye)) / J;
+        sm.a[le][ij] = ft;
+        sm.b[le][ij] = gt;
+    }
     __syncthreads();
     if (active)
-        for (int o = ij; o < NF; o += K2) face_trace<K, T>(sm.x[le], op.b, o, sm.tv[le][o], sm.tg[le][o]);
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            T v = sm.cg[le][o];
+            if (ijp < 2) {
+#pragma unroll
+                for (int d = 0; d < K; ++d) v -= sm.a[le][k * K + d] * b.sbb[d * 2 + lr];
+            } else {
+#pragma unroll
+                for (int d = 0; d < K; ++d) v -= sm.b[le][d * K + k] * b.sbb[d * 2 + lr];
+            }
+            sm.fb[le][o] = v;
+        }
     __syncthreads();
-    return lap_element<K, T>(active, el, ij, op.g, op.b, tv, tg, sm.x[lei], sm.tv[lei], sm.tg[lei], sm.com[lei],
-                             sm.cg[lei], sm.a[lei], sm.b[lei], sm.fb[lei], op.g.sw_p, op.zero_bc);
+    if (!active) return T(0);
+    T lap = T(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) lap += sm.a[le][j * K + d] * b.D[d * K + i];
+    lap += sm.fb[le][0 * K + j] * b.gR[i * 2 + 0] + sm.fb[le][1 * K + j] * b.gR[i * 2 + 1];
+#pragma unroll
+    for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * b.D[d * K + j];
+    lap += sm.fb[le][2 * K + i] * b.gR[j * 2 + 0] + sm.fb[le][3 * K + i] * b.gR[j * 2 + 1];
+    return lap;
 }
 
 // face traces of an element vector held in shared memory
@@ -192,6 +345,8 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, Bi
     const KrylovScalars* sc = rs.sc;
     if (sc->done) return;
     __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
+    __shared__ DevBases<T> sbas;
+    stage_bases(sbas, op.b);
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
@@ -223,7 +378,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, Bi
         sz[le][ij] = z;
     }
     __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], op.b, v.tv, v.tg, active, el, ij);
+    emit_traces<K, T>(sz[active ? le : 0], sbas, v.tv, v.tg, active, el, ij);
 }
 
 // two-level smoothing step: z = e + w D^{-1} (f - A e), e = P ec element-wise constant;
@@ -237,6 +392,8 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const
     constexpr int K2 = S::K2;
     if (pc_skip(sc, mode)) return;
     __shared__ T sr[S::EPB][K2], sz[S::EPB][K2];
+    __shared__ DevBases<T> sbas;
+    stage_bases(sbas, op.b);
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
@@ -257,7 +414,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const
         sz[le][ij] = zz;
     }
     __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], op.b, tv, tg, active, el, ij);
+    emit_traces<K, T>(sz[active ? le : 0], sbas, tv, tg, active, el, ij);
 }
 
 // v = A ph; alpha = rho / (rhat, v)
@@ -296,6 +453,8 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_supdate(MfOp<T> op, Bi
     KrylovScalars* sc = rs.sc;
     if (sc->done) return;
     __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
+    __shared__ DevBases<T> sbas;
+    stage_bases(sbas, op.b);
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
@@ -322,7 +481,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_supdate(MfOp<T> op, Bi
             sz[le][ij] = z;
         }
         __syncthreads();
-        emit_traces<K, T>(sz[active ? le : 0], op.b, v.tv, v.tg, active, el, ij);
+        emit_traces<K, T>(sz[active ? le : 0], sbas, v.tv, v.tg, active, el, ij);
     }
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -399,6 +558,18 @@ __global__ void k_finish_s_exit(KrylovScalars* sc) {
     if (!sc->done && sc->s_exit) sc->done = 1;
 }
 
+// same, and sets the condition of the graph's while node: iterate while not done. Every
+// body execution either increments `it` (capped at max_iter by k_xr_update) or finds
+// `done` set, so the device-side loop always ends.
+__global__ void k_finish_loop(KrylovScalars* sc, cudaGraphConditionalHandle h) {
+    if (!sc->done && sc->s_exit) sc->done = 1;
+    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
+}
+
+__global__ void k_set_loop(const KrylovScalars* sc, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
+}
+
 // r = b - A x (FP64 refinement residual); ||r||^2 -> rnorm2, ||b||^2 -> bnorm2
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_residual(MfOp<T> op, const double* __restrict__ b,
@@ -448,20 +619,19 @@ __device__ __forceinline__ T csr_row(const DevCsr<T>& A, const T* __restrict__ x
     return acc;
 }
 
+// pre-smoothing from zero and residual in one pass: t = f - A (m .* f)
 template <typename T>
-__global__ void k_c_smooth0(int n, const T* __restrict__ m, const T* __restrict__ f, T* __restrict__ u,
-                            const KrylovScalars* sc, int mode) {
+__global__ void k_c_pre(DevCsr<T> A, const T* __restrict__ m, const T* __restrict__ f, T* __restrict__ t,
+                        const KrylovScalars* sc, int mode) {
     if (pc_skip(sc, mode)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) u[i] = m[i] * f[i];
-}
-
-template <typename T>
-__global__ void k_c_residual(DevCsr<T> A, const T* __restrict__ f, const T* __restrict__ u, T* __restrict__ t,
-                             const KrylovScalars* sc, int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < A.n) t[i] = f[i] - csr_row<T>(A, u, i);
+    if (i >= A.n) return;
+    T acc = T(0);
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+        const int j = A.col[k];
+        acc += A.val[k] * (m[j] * f[j]);
+    }
+    t[i] = f[i] - acc;
 }
 
 template <typename T>
@@ -472,30 +642,34 @@ __global__ void k_c_spmv(DevCsr<T> M, const T* __restrict__ x, T* __restrict__ y
     if (i < M.n) y[i] = csr_row<T>(M, x, i);
 }
 
+// coarse-grid correction and post-smoothing in one pass:
+// u' = m .* f + P uc (recomputed per use), u2 = u' + m .* (f - A u')
 template <typename T>
-__global__ void k_c_prolong_add(DevCsr<T> P, const T* __restrict__ uc, T* __restrict__ u, const KrylovScalars* sc,
-                                int mode) {
+__global__ void k_c_post(DevCsr<T> A, DevCsr<T> P, const T* __restrict__ m, const T* __restrict__ f,
+                         const T* __restrict__ uc, T* __restrict__ u2, const KrylovScalars* sc, int mode) {
     if (pc_skip(sc, mode)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.n) u[i] += csr_row<T>(P, uc, i);
+    if (i >= A.n) return;
+    T acc = T(0), ui = T(0);
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+        const int j = A.col[k];
+        const T uj = m[j] * f[j] + csr_row<T>(P, uc, j);
+        acc += A.val[k] * uj;
+        if (j == i) ui = uj;
+    }
+    if (A.ptr[i] == A.ptr[i + 1] || ui == T(0)) ui = m[i] * f[i] + csr_row<T>(P, uc, i);
+    u2[i] = ui + m[i] * (f[i] - acc);
 }
 
+// coarsest level: u = inv f with the inverse stored column-major (coalesced reads)
 template <typename T>
-__global__ void k_c_smooth(DevCsr<T> A, const T* __restrict__ m, const T* __restrict__ f, const T* __restrict__ u,
-                           T* __restrict__ u2, const KrylovScalars* sc, int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < A.n) u2[i] = u[i] + m[i] * (f[i] - csr_row<T>(A, u, i));
-}
-
-template <typename T>
-__global__ void k_c_dense(int n, const T* __restrict__ inv, const T* __restrict__ f, T* __restrict__ u,
+__global__ void k_c_dense(int n, const T* __restrict__ inv_t, const T* __restrict__ f, T* __restrict__ u,
                           const KrylovScalars* sc, int mode) {
     if (pc_skip(sc, mode)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     T acc = T(0);
-    for (int j = 0; j < n; ++j) acc += inv[(size_t)i * n + j] * f[j];
+    for (int j = 0; j < n; ++j) acc += inv_t[(size_t)j * n + i] * f[j];
     u[i] = acc;
 }
 
@@ -529,7 +703,7 @@ static unsigned kgrid(int N) {
 
 int krylov_max_blocks(int K, int N) {
     const int k2 = K * K;
-    const int epb = (256 / k2) > 64 ? 64 : ((256 / k2) > 0 ? 256 / k2 : 1);
+    const int epb = (256 / k2) > 32 ? 32 : ((256 / k2) > 0 ? 256 / k2 : 1);
     return (N + epb - 1) / epb;
 }
 
@@ -554,12 +728,10 @@ static void coarse_cycle(const Precond<T>& pc, int l, const KrylovScalars* sc, i
         return;
     }
     const CoarseLevel<T>& C = pc.lev[l + 1];
-    k_c_smooth0<T><<<g, 128, 0, s>>>(L.n, L.m, L.f, L.u, sc, mode);
-    k_c_residual<T><<<g, 128, 0, s>>>(L.A, L.f, L.u, L.t, sc, mode);
+    k_c_pre<T><<<g, 128, 0, s>>>(L.A, L.m, L.f, L.t, sc, mode);
     k_c_spmv<T><<<(unsigned)((C.n + 127) / 128), 128, 0, s>>>(L.R, L.t, C.f, sc, mode);
     coarse_cycle(pc, l + 1, sc, mode, s);
-    k_c_prolong_add<T><<<g, 128, 0, s>>>(L.P, C.out, L.u, sc, mode);
-    k_c_smooth<T><<<g, 128, 0, s>>>(L.A, L.m, L.f, L.u, L.u2, sc, mode);
+    k_c_post<T><<<g, 128, 0, s>>>(L.A, L.P, L.m, L.f, C.out, L.u2, sc, mode);
 }
 
 template <int K, typename T>
@@ -588,7 +760,7 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc) {
     if (pc.nlev == 0) return 6;
-    const int coarse = 5 * (pc.nlev - 1) + 1;
+    const int coarse = 3 * (pc.nlev - 1) + 1;
     return 6 + 2 * (coarse + 1);
 }
 
@@ -597,6 +769,48 @@ cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const R
                              const Precond<T>& pc, cudaStream_t s) {
     HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, s)));
     k_finish_s_exit<<<1, 1, 0, s>>>(rs.sc);
+    return cudaGetLastError();
+}
+
+// Captures a whole solve into `*graph_out`: initial residual, then a while node whose body
+// is one BiCGSTAB iteration; the loop condition lives on the device, so a solve is one
+// graph launch with no host round trip.
+template <typename T>
+cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+                                 int max_iter, const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle h;
+    if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) return e;
+    if ((e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    krylov_init<T>(op, v, rs, tol, s);
+    k_set_loop<<<1, 1, 0, s>>>(rs.sc, h);
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t cg = nullptr;
+    if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &ndeps)) != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    if ((e = cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp)) != cudaSuccess) return e;
+    if ((e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+        return e;
+    if ((e = cudaStreamEndCapture(s, &g)) != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, s)));
+    k_finish_loop<<<1, 1, 0, s>>>(rs.sc, h);
+    if ((e = cudaStreamEndCapture(s, &body)) != cudaSuccess) return e;
+    *graph_out = g;
     return cudaGetLastError();
 }
 
@@ -640,6 +854,8 @@ cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s)
     template cudaError_t krylov_iteration<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, int,    \
                                              const Precond<T>&, cudaStream_t);                                    \
     template int krylov_launches_per_iteration<T>(const Precond<T>&);                                             \
+    template cudaError_t krylov_capture_solve<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,     \
+                                                 double, int, const Precond<T>&, cudaStream_t, cudaGraph_t*);     \
     template cudaError_t mf_residual<T>(const MfOp<T>&, const double*, const T*, T*, T*, double*,                 \
                                         const ReduceScratch&, cudaStream_t);                                      \
     template cudaError_t mf_apply_op<T>(const MfOp<T>&, const T*, T*, T*, T*, cudaStream_t);                      \

@@ -37,6 +37,23 @@ void DeviceBuffer::reset() {
     n_ = 0;
 }
 
+// A captured Krylov solve and the parameters baked into it.
+struct SolveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double tol = -1.0;
+    int max_iter = -1;
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        tol = -1.0;
+        max_iter = -1;
+    }
+    ~SolveGraph() { reset(); }
+};
+
 struct DeviceState {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -73,6 +90,7 @@ struct DeviceState {
     DeviceBuffer dense64, dense32;
     Precond<double> pc64;
     Precond<float> pc32;
+    SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
@@ -131,6 +149,8 @@ DevCsr<TM> view(const DeviceState::CsrBufs& b, int n, bool f32) {
 Solver::Solver() : d_(new DeviceState) {
     const char* v = std::getenv("HO2D_VERBOSE");
     verbose_ = v && v[0] && v[0] != '0';
+    const char* g = std::getenv("HO2D_GRAPHS");
+    use_graphs_ = !(g && g[0] == '0');
 }
 Solver::~Solver() = default;
 
@@ -259,6 +279,8 @@ Error Solver::setup_preconditioner() {
     const int N = mesh_.n_el;
     d.pc64 = Precond<double>();
     d.pc32 = Precond<float>();
+    d.graph64.reset();
+    d.graph32.reset();
     d.lev.clear();
     const char* mode = std::getenv("HO2D_PRECOND");
     if (mode && std::string(mode) == "bj") return {0, ""};
@@ -280,8 +302,11 @@ Error Solver::setup_preconditioner() {
         for (DeviceBuffer* v : {&b->f, &b->u, &b->t, &b->u2}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
         d.lev.push_back(std::move(b));
     }
-    HO2D_CUDA(upload(d.dense64, H.dense_inv), "upload dense");
-    HO2D_CUDA(upload_as<float>(d.dense32, H.dense_inv), "upload dense");
+    std::vector<double> inv_t(H.dense_inv.size());  // column-major for coalesced device reads
+    for (int i = 0; i < H.n_dense; ++i)
+        for (int j = 0; j < H.n_dense; ++j) inv_t[(size_t)j * H.n_dense + i] = H.dense_inv[(size_t)i * H.n_dense + j];
+    HO2D_CUDA(upload(d.dense64, inv_t), "upload dense");
+    HO2D_CUDA(upload_as<float>(d.dense32, inv_t), "upload dense");
     auto fill = [&](auto& pc, bool f32) {
         using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense_inv)>::type>::type;
         using TM = T;
@@ -410,7 +435,24 @@ Error Solver::poisson_solve() {
         return {0, ""};
     };
     // runs BiCGSTAB to completion on (A, v); returns iterations
-    auto run = [&](auto A, auto v, const auto& pc, double tol, int& iters) -> Error {
+    // one solve: by default a single launch of the captured graph (initial residual and a
+    // device-side while loop); with HO2D_GRAPHS=0 the host enqueues batches of iterations
+    // and polls the done flag between batches
+    auto run = [&](auto A, auto v, const auto& pc, double tol, int& iters, SolveGraph& sg) -> Error {
+        if (use_graphs_) {
+            if (!sg.exec || sg.tol != tol || sg.max_iter != max_iter_) {
+                sg.reset();
+                HO2D_CUDA(krylov_capture_solve(A, v, rs, tol, max_iter_, pc, d.stream, &sg.graph), "graph capture");
+                HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
+                sg.tol = tol;
+                sg.max_iter = max_iter_;
+            }
+            HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
+            HO2D_TRY(poll());
+            iters = d.h_sc->it;
+            launches_ += 4 + (int64_t)iters * (krylov_launches_per_iteration(pc) + 1);
+            return {0, ""};
+        }
         HO2D_CUDA(krylov_init(A, v, rs, tol, d.stream), "krylov init");
         launches_ += 3;
         HO2D_TRY(poll());
@@ -433,7 +475,7 @@ Error Solver::poisson_solve() {
         const MfOp<double> A = make_op<double>(d, mesh_, K, false);
         const BicgVectors<double> v = krylov_vectors<double>(d, d.psi64.as<double>(), d.rhs.as<double>());
         int it = 0;
-        HO2D_TRY(run(A, v, d.pc64, tol_, it));
+        HO2D_TRY(run(A, v, d.pc64, tol_, it, d.graph64));
         last_iters_ = it;
         const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
         finite = std::isfinite(bn) && std::isfinite(rn);
@@ -464,7 +506,7 @@ Error Solver::poisson_solve() {
             HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
             launches_ += 1;
             int it = 0;
-            HO2D_TRY(run(A32, v, d.pc32, inner_tol_, it));
+            HO2D_TRY(run(A32, v, d.pc32, inner_tol_, it, d.graph32));
             last_iters_ += it;
             HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
             launches_ += 1;
