@@ -217,6 +217,14 @@ int ho2d_apply_poisson(ho2d_solver* h, int32_t len, const double* x, double* y) 
     });
 }
 
+int ho2d_apply_poisson_noalloc(ho2d_solver* h, int32_t len, const double* x_device, double* y_device) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), x_device);
+        if (e.code) return e;
+        return h->s.apply_poisson_noalloc(x_device, y_device);
+    });
+}
+
 int ho2d_last_launch_count(ho2d_solver* h, int64_t* launches) {
     return guarded(h, [&]() -> ho2d::Error {
         if (launches) *launches = h->s.launches();

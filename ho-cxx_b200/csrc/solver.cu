@@ -18,6 +18,7 @@
 #include "device.cuh"
 #include "fr_launch.hpp"
 #include "host_amg.hpp"
+#include "noalloc.hpp"
 #include "solver.hpp"
 
 namespace ho2d {
@@ -91,6 +92,7 @@ struct DeviceState {
     Precond<double> pc64;
     Precond<float> pc32;
     SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
+    double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
@@ -195,6 +197,7 @@ Error Solver::setup() {
     for (cudaEvent_t* e : {&d.ev0, &d.ev1, &d.evp0, &d.evp1})
         if (!*e) HO2D_CUDA(cudaEventCreate(e), "cudaEventCreate");
     if (!d.h_sc) HO2D_CUDA(cudaMallocHost(&d.h_sc, sizeof(KrylovScalars)), "cudaMallocHost");
+    HO2D_TRY(noalloc_scratch(d.device, &d.noalloc_scratch));  // once per device, this device current
 
     const int N = mesh_.n_el, K = in_.knod, K2 = K * K, neb = mesh_.n_eb;
     const size_t nv = (size_t)N * K2, nf = (size_t)N * 4 * K;
@@ -717,6 +720,26 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     float ms = 0.f;
     HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
     if (avg_ms) *avg_ms = ms / reps;
+    return {0, ""};
+}
+
+// y = A x on caller-owned device buffers without allocating: the operand's face traces
+// go to the fixed scratch of noalloc.cu (shared by every call on this device).
+Error Solver::apply_poisson_noalloc(const double* dx, double* dy) {
+    if (!setup_done_) return {1, "not set up"};
+    if (!dx || !dy) return {1, "null device buffer"};
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod;
+    const size_t need = 2 * (size_t)N * 4 * K;
+    if (need > kNoAllocScratchDoubles)
+        return {1, "mesh too large for the fixed scratch of the allocation-free entry point: N_el*Knod = " +
+                       std::to_string((size_t)N * K) + " exceeds " + std::to_string(kNoAllocScratchDoubles / 8)};
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    double* tv = d.noalloc_scratch;
+    double* tg = tv + (size_t)N * 4 * K;
+    const MfOp<double> op = make_op<double>(d, mesh_, K, false);
+    HO2D_CUDA(mf_apply_op<double>(op, dx, tv, tg, dy, d.stream), "apply");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     return {0, ""};
 }
 

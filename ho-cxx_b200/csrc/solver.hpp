@@ -48,6 +48,7 @@ class Solver {
     Error time_steps(int nsteps, double* total_ms, double* poisson_ms);
     Error profile_spmv(int reps, double* avg_ms, double* bytes);
     Error apply_poisson(const double* x, double* y);
+    Error apply_poisson_noalloc(const double* dx, double* dy);
 
     Error get_volume(int which, double* out);  // [N][K][K]
     Error get_velocity(double* out);           // [N][K][K][2]

@@ -130,6 +130,19 @@ int ho2d_profile_spmv(ho2d_solver* handle, int32_t reps, double* avg_ms, double*
  * in form_Laplace_operator_matrix (src/HO_2D.cpp:1533-1804), applied matrix-free;
  * len = N_el*Knod*Knod. */
 int ho2d_apply_poisson(ho2d_solver* handle, int32_t len, const double* x, double* y);
+/* No counterpart in the reference. Allocation-free variant of ho2d_apply_poisson for
+ * callers that cannot let a library call cudaMalloc: codes that own all device memory
+ * through their own pool or a fixed budget, or that must not trigger the implicit device
+ * synchronisation an allocation can cause in the middle of their own work. x_device and
+ * y_device are caller-owned DEVICE buffers of len = N_el*Knod*Knod doubles on the
+ * handle's device (y = A x, FP64, on the handle's stream, synchronous at return). The
+ * only working memory is a fixed 8 MiB array compiled into the library (face traces of
+ * x), so meshes with N_el*Knod > 131072 are rejected with HO2D_ERR_ARG. Its device
+ * address is looked up once per device inside ho2d_setup; this call itself allocates
+ * nothing. Every call on a device shares that array and nothing in it needs clearing
+ * (it is fully rewritten from x before it is read), so calls that overlap on the GPU --
+ * from different handles or streams on the same device -- race on it. */
+int ho2d_apply_poisson_noalloc(ho2d_solver* handle, int32_t len, const double* x_device, double* y_device);
 /* Total number of kernel launches this handle has issued since it was created. */
 int ho2d_last_launch_count(ho2d_solver* handle, int64_t* launches);
 /* Text of the last error on this handle ("" if none). The pointer stays valid until the
