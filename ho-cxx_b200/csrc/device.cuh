@@ -69,4 +69,10 @@ struct KrylovScalars {
     int it, done, breakdown, s_exit, zero_rhs, pad;
 };
 
+// A preconditioner application is skipped once the solve is done, and the second one of
+// an iteration (mode 1) also when the iteration exits early after its s update.
+__device__ __forceinline__ bool pc_skip(const KrylovScalars* sc, int mode) {
+    return sc->done || (mode == 1 && sc->s_exit);
+}
+
 }  // namespace ho2d

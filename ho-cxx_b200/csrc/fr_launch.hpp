@@ -57,13 +57,34 @@ cudaError_t launch_bc_update(int n_eb, int K, int ptype, double tc, double y_min
                              cudaStream_t s);
 
 // ---- Krylov (krylov.cu)
+// Static data of the matrix-free Poisson operator (the method-2 FR Laplacian with
+// homogeneous boundary values), laid out so that an element reads only its own rows:
+//   G11, G12, G22  [N][K2]  contravariant metric coefficients: (g_eta.g_eta)/J,
+//                           -(g_xi.g_eta)/J, (g_xi.g_xi)/J
+//   fa, fb         [N][4K]  face coefficients g.g/J_f and g1.g2/J_f of this element
+//   nfa, nfb       [N][4K]  the same coefficients of the neighbour across each face point
+//   code           [N][4]   interior face: nijp + 4 * rev; Dirichlet: -1;
+//                           Neumann: -2 - boundary edge index
+//   minv           [N_eb][K][K]  inverse of the common-value system of a Neumann edge
+//   scat           [N][4K]  where a face point's traces go in the neighbour's incoming
+//                           slots (-1 on the boundary): producers of an operand write
+//                           its traces there, so the operator reads them as its own rows
+template <typename T>
+struct PoisGeom {
+    int N = 0;
+    const T *G11 = nullptr, *G12 = nullptr, *G22 = nullptr;
+    const T *fa = nullptr, *fb = nullptr, *nfa = nullptr, *nfb = nullptr;
+    const T* minv = nullptr;
+    const int* code = nullptr;
+    const int* scat = nullptr;
+};
+
 // Matrix-free FR Laplacian (the Poisson operator) plus the preconditioner's element data.
 template <typename T>
 struct MfOp {
     int K;
-    FrGeom<T> g;            // metrics, connectivity, Poisson BC switches (g.sw_p)
+    PoisGeom<T> g;
     DevBases<T> b;
-    const double* zero_bc;  // [N_eb * K] zeros: homogeneous boundary values
     const T* dinv;          // [N][K2][K2] inverse diagonal blocks, transposed ([rs][ij])
     const T* rowsum;        // [N][5][K2] row sums of the 5 blocks of each element row
     const int* bcol;        // [N][5] element of each block (slot 0 = self, 1 + ijp = neighbours)
@@ -73,8 +94,8 @@ template <typename T>
 struct BicgVectors {
     T *x, *r, *rhat, *p, *v, *s, *t, *ph, *sh;
     const T* b;
-    T *tv, *tg;    // face traces of the operand of the next operator application (ph or sh)
-    T *xtv, *xtg;  // face traces of x (initial residual)
+    T *tv, *tg;    // incoming face traces of the operand of the next operator application
+    T *xtv, *xtg;  // incoming face traces of x (initial residual)
 };
 
 struct ReduceScratch {
@@ -83,35 +104,64 @@ struct ReduceScratch {
     KrylovScalars* sc;   // device scalars
 };
 
-// scalar CSR matrix on the device
+// Row-padded sparse matrix on the device: row i holds w entries at [i * w, (i + 1) * w);
+// padding entries have column 0 and value 0. col == nullptr means dense (column = k).
 template <typename T>
-struct DevCsr {
-    int n;
-    const int* ptr;
-    const int* col;
-    const T* val;
+struct DevEll {
+    int n = 0, w = 0;
+    int g = 1;  // lanes that cooperate on one row (a power of two <= 32)
+    const int* col = nullptr;
+    const T* val = nullptr;
 };
 
-// one coarse level of the two-level preconditioner (level 0 = one value per element)
+// One level of the coarse hierarchy (level 0 = one value per element). Its V(1,1) cycle
+// is f_next = M f and u = S f + Q u_next (host_amg.hpp has the formulas).
 template <typename T>
 struct CoarseLevel {
-    int n;
-    DevCsr<T> A, P, R;  // P, R unused on the coarsest level
-    const T* m;         // SPAI-0 weights
-    T *f, *u, *t, *u2;  // right-hand side, iterate, residual, smoothed iterate
-    T* out;             // where this level's cycle leaves its result (u2, or u when coarsest)
+    int n = 0;
+    DevEll<T> M, S, Q;  // empty on the coarsest level
+    T* f = nullptr;     // right-hand side (global memory)
+    T* u = nullptr;     // result (global memory)
+    int sf = -1, su = -1;  // offsets (in T) of f and u in the cluster kernel's shared memory
 };
 
-constexpr int kMaxLevels = 24;
+constexpr int kMaxLevels = 16;
 
-// preconditioner: nlev == 0 -> block-Jacobi; otherwise the two-level V(0,1) cycle
+// Preconditioner: nlev == 0 -> block-Jacobi; otherwise the two-level cycle whose coarse
+// part runs levels [0, top) as grid-wide kernels and levels [top, nlev) in one thread-block
+// cluster, which reads f_top from global memory and leaves u_o, o = min(top + 1, nlev - 1),
+// in global memory.
 template <typename T>
 struct Precond {
     int nlev = 0;
+    int top = 0;
+    int cluster = 8;  // CTAs in the coarse-cycle cluster
+    int smem = 0;     // dynamic shared memory of the cluster kernel, bytes
     double omega = 1.0;  // weight of the block-Jacobi smoothing step
     CoarseLevel<T> lev[kMaxLevels];
-    const T* dense_inv = nullptr;  // inverse of the coarsest operator
+    DevEll<T> dense;  // row-major inverse of the coarsest operator (col == nullptr)
 };
+
+// What the fine smoothing step needs of the coarse result: u0 directly (one level), or
+// the level-0 up step u0 = S0 f0 + Q0 u1 evaluated per element where it is used.
+template <typename T>
+struct CoarseOut {
+    const T* u0 = nullptr;
+    DevEll<T> S, Q;
+    const T* f0 = nullptr;
+    const T* u1 = nullptr;
+};
+
+// picks the cluster size and sets the cluster kernel's attributes; call once per Precond
+template <typename T>
+cudaError_t coarse_prepare(Precond<T>& pc);
+// enqueues the coarse part of one preconditioner application on f_0 = pc.lev[0].f
+template <typename T>
+cudaError_t coarse_cycle(const Precond<T>& pc, const KrylovScalars* sc, int mode, cudaStream_t s);
+template <typename T>
+int coarse_launches(const Precond<T>& pc);
+template <typename T>
+CoarseOut<T> coarse_out(const Precond<T>& pc);
 
 template <typename T>
 cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,

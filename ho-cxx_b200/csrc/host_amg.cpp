@@ -70,6 +70,48 @@ Csr multiply(const Csr& A, const Csr& B) {
     return C;
 }
 
+// I - diag(l) A diag(r); an empty l or r means no scaling on that side. Every row gets an
+// explicit diagonal entry.
+Csr identity_minus_scaled(const Csr& A, const std::vector<double>& l, const std::vector<double>& r) {
+    Csr C;
+    C.n = A.n;
+    C.m = A.m;
+    C.ptr.assign(A.n + 1, 0);
+    for (int i = 0; i < A.n; ++i) {
+        bool diag = false;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            const int j = A.col[k];
+            if (!diag && j > i) {
+                C.col.push_back(i);
+                C.val.push_back(1.0);
+                diag = true;
+            }
+            double v = -A.val[k] * (l.empty() ? 1.0 : l[i]) * (r.empty() ? 1.0 : r[j]);
+            if (j == i) {
+                v += 1.0;
+                diag = true;
+            }
+            C.col.push_back(j);
+            C.val.push_back(v);
+        }
+        if (!diag) {
+            C.col.push_back(i);
+            C.val.push_back(1.0);
+        }
+        C.ptr[i + 1] = (int)C.col.size();
+    }
+    return C;
+}
+
+// 2 diag(m) - diag(m) A diag(m)
+Csr smoothing_part(const Csr& A, const std::vector<double>& m) {
+    Csr C = identity_minus_scaled(A, m, m);  // I - mAm, with an explicit diagonal
+    for (int i = 0; i < C.n; ++i)
+        for (int k = C.ptr[i]; k < C.ptr[i + 1]; ++k)
+            if (C.col[k] == i) C.val[k] += 2.0 * m[i] - 1.0;
+    return C;
+}
+
 std::vector<double> spai0(const Csr& A) {
     std::vector<double> m(A.n, 0.0);
     for (int i = 0; i < A.n; ++i) {
@@ -219,6 +261,21 @@ bool dense_inverse(int n, const Csr& A, std::vector<double>& inv) {
 
 }  // namespace
 
+Ell to_ell(const Csr& A) {
+    Ell E;
+    E.n = A.n;
+    E.m = A.m;
+    for (int i = 0; i < A.n; ++i) E.w = std::max(E.w, A.ptr[i + 1] - A.ptr[i]);
+    E.col.assign((size_t)E.n * E.w, 0);
+    E.val.assign((size_t)E.n * E.w, 0.0);
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            E.col[(size_t)i * E.w + (k - A.ptr[i])] = A.col[k];
+            E.val[(size_t)i * E.w + (k - A.ptr[i])] = A.val[k];
+        }
+    return E;
+}
+
 Csr p0_coarse_operator(const PoissonOperator& op, int N) {
     const int K2 = op.K2;
     Csr A;
@@ -266,6 +323,12 @@ Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H) {
         H.levels.push_back(next);
     }
     for (auto& L : H.levels) L.m = spai0(L.A);
+    for (size_t l = 0; l + 1 < H.levels.size(); ++l) {
+        AmgLevel& L = H.levels[l];
+        L.M = multiply(L.R, identity_minus_scaled(L.A, {}, L.m));
+        L.S = smoothing_part(L.A, L.m);
+        L.Q = multiply(identity_minus_scaled(L.A, L.m, {}), L.P);
+    }
     const Csr& Ab = H.levels.back().A;
     if (Ab.n > 4 * kDenseMax) return {4, "coarse Poisson problem did not coarsen below the dense-solve size"};
     H.n_dense = Ab.n;

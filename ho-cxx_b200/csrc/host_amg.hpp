@@ -18,7 +18,21 @@ struct Csr {
 struct AmgLevel {
     Csr A, P, R;            // P, R empty on the coarsest level
     std::vector<double> m;  // SPAI-0 smoother weights
+    // The V(1,1) cycle of this level with pre-smoothing from zero, u' = m .* f, and
+    // post-smoothing u = u'' + m .* (f - A u''), u'' = u' + P u_c, as three fixed operators:
+    //   f_c = M f,  u = S f + Q u_c   with
+    //   M = R (I - A diag(m)),  S = 2 diag(m) - diag(m) A diag(m),  Q = (I - diag(m) A) P.
+    Csr M, S, Q;  // empty on the coarsest level
 };
+
+// Row-padded (ELL) copy of a sparse matrix: every row holds exactly w entries, padding
+// entries have column 0 and value 0, so a row is read without a row pointer.
+struct Ell {
+    int n = 0, m = 0, w = 0;
+    std::vector<int> col;     // [n][w]
+    std::vector<double> val;  // [n][w]
+};
+Ell to_ell(const Csr& A);
 
 struct CoarseHierarchy {
     std::vector<AmgLevel> levels;  // levels[0] is the P0 (one value per element) operator

@@ -60,7 +60,9 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     __threadfence();
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
+        // the partial loads are independent: unrolled, a thread keeps up to 8 in flight
         double x = 0.0;
+#pragma unroll 8
         for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) x += __ldcg(&partials[j * gridDim.x + i]);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
@@ -88,136 +90,74 @@ template <int K, typename T>
 struct MfShared {
     static constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
     T x[EPB][K2], a[EPB][K2], b[EPB][K2];
-    // own face: traces (recomputed) and metrics; neighbour face: traces and metrics
-    T tv[EPB][NF], tg[EPB][NF], fA[EPB][NF], fB[EPB][NF], fJ[EPB][NF];
-    T ntv[EPB][NF], ntg[EPB][NF], nfA[EPB][NF], nfB[EPB][NF], nfJ[EPB][NF];
-    T com[EPB][NF], cg[EPB][NF], fb[EPB][NF];
-    int nb[EPB][4], nijp[EPB][4];  // neighbour element / its face; boundary: -1 - switch
+    T tv[EPB][NF], tg[EPB][NF];    // own traces, recomputed from x
+    T ntv[EPB][NF], ntg[EPB][NF];  // incoming traces of the neighbours
+    T fa[EPB][NF], fb[EPB][NF], nfa[EPB][NF], nfb[EPB][NF];
+    T com[EPB][NF], cg[EPB][NF];   // common values; common normal fluxes (then their jumps)
+    int code[EPB][4];
     DevBases<T> bas;               // basis tables staged from the parameter bank
 };
 
 // y = A x at (el, ij) for the homogeneous-boundary Poisson operator: the method-2 FR
-// Laplacian of fr_device.cuh's lap_element, restaged so that all global data arrive in
-// two rounds (own data and connectivity, then the neighbours' face data) and every
-// later phase synchronises through shared memory only. Collective.
+// Laplacian of fr_device.cuh's lap_element. Every global read is one of the element's
+// own rows (its x, metric coefficients, face coefficients and incoming traces), so all
+// of them are issued in a single round; five barrier phases follow. Collective.
 template <int K, typename T>
 __device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
                       MfShared<K, T>& sm, bool active, int le, int el, int ij) {
-    constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
-    const FrGeom<T>& g = op.g;
-    stage_bases(sm.bas, op.b);
-    const DevBases<T>& b = sm.bas;
+    constexpr int K2 = K * K, NF = 4 * K;
+    const PoisGeom<T>& g = op.g;
     const int j = ij / K, i = ij % K;
-    // round 1: x, volume metrics, connectivity
-    T xx = T(0), xe = T(0), yx = T(0), ye = T(0), J = T(1);
+    // round of loads: everything is indexed by this element only
+    T g11 = T(0), g12 = T(0), g22 = T(0);
     if (active) {
         const int p = el * K2 + ij;
         sm.x[le][ij] = x[p];
-        xx = g.xxi[p]; xe = g.xeta[p]; yx = g.yxi[p]; ye = g.yeta[p]; J = g.J[p];
-    }
-    for (int f = threadIdx.x; f < EPB * 4; f += blockDim.x) {
-        const int l = f / 4, face = f % 4, e2 = blockIdx.x * EPB + l;
-        if (e2 < g.N) {
-            const int nb = g.face_nb[e2 * 4 + face];
-            sm.nb[l][face] = nb >= 0 ? nb : -1 - g.sw_p[-nb - 1];
-            sm.nijp[l][face] = g.face_nijp[e2 * 4 + face];
+        g11 = g.G11[p];
+        g12 = g.G12[p];
+        g22 = g.G22[p];
+        for (int o = ij; o < NF; o += K2) {
+            const int q = el * NF + o;
+            sm.fa[le][o] = g.fa[q];
+            sm.fb[le][o] = g.fb[q];
+            sm.nfa[le][o] = g.nfa[q];
+            sm.nfb[le][o] = g.nfb[q];
+            sm.ntv[le][o] = tv[q];
+            sm.ntg[le][o] = tg[q];
         }
+        for (int c = ij; c < 4; c += K2) sm.code[le][c] = g.code[el * 4 + c];
     }
+    stage_bases(sm.bas, op.b);
     __syncthreads();
-    // round 2: own face metrics and traces, the neighbours' traces and face metrics
+    const DevBases<T>& b = sm.bas;
+    // own traces; common values on interior (average) and Dirichlet (zero) faces
     if (active)
         for (int o = ij; o < NF; o += K2) {
-            const int ijp = o / K, k = o % K;
-            const int q = (el * 4 + ijp) * K + k;
-            sm.fA[le][o] = g.fA[q];
-            sm.fB[le][o] = g.fB[q];
-            sm.fJ[le][o] = g.fJ[q];
-            face_trace<K, T>(sm.x[le], b, o, sm.tv[le][o], sm.tg[le][o]);
-            const int nb = sm.nb[le][ijp];
-            if (nb >= 0) {
-                const int nijp = sm.nijp[le][ijp];
-                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
-                const int nq = (nb * 4 + nijp) * K + (rev ? K - 1 - k : k);
-                sm.ntv[le][o] = tv[nq];
-                sm.ntg[le][o] = tg[nq];
-                sm.nfA[le][o] = g.fA[nq];
-                sm.nfB[le][o] = g.fB[nq];
-                sm.nfJ[le][o] = g.fJ[nq];
-            }
+            T v, d;
+            face_trace<K, T>(sm.x[le], b, o, v, d);
+            sm.tv[le][o] = v;
+            sm.tg[le][o] = d;
+            sm.com[le][o] = sm.code[le][o / K] >= 0 ? T(0.5) * (v + sm.ntv[le][o]) : T(0);
         }
     __syncthreads();
-    // common values: average inside, 0 on Dirichlet faces (homogeneous), Neumann below
+    // homogeneous Neumann faces: com = Minv r with r_m = -fa_m (tg_m - tv_m g'(+-1)), the
+    // K x K common-value system of src/HO_2D.cpp:2899-2924 inverted once at setup
     if (active)
         for (int o = ij; o < NF; o += K2) {
-            const int nb = sm.nb[le][o / K];
-            sm.com[le][o] = nb >= 0 ? T(0.5) * (sm.tv[le][o] + sm.ntv[le][o]) : T(0);
-        }
-    __syncthreads();
-    // homogeneous Neumann faces: K x K system for the common value (src/HO_2D.cpp:2899-2924)
-    for (int ijp = ij; active && ijp < 4; ijp += K2) {
-        if (sm.nb[le][ijp] != -1 - kNeumann) continue;
-        const int lr = ijp & 1;
-        T M[K][K], r[K], xs[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int o = ijp * K + k;
-            r[k] = -sm.fA[le][o] * (sm.tg[le][o] - sm.tv[le][o] * b.gp[lr]);
-#pragma unroll
-            for (int c = 0; c < K; ++c) M[k][c] = -sm.fB[le][o] * b.D[c * K + k];
-            M[k][k] += sm.fA[le][o] * b.gp[lr];
-        }
-#pragma unroll
-        for (int c = 0; c < K - 1; ++c)
-#pragma unroll
-            for (int r2 = c + 1; r2 < K; ++r2) {
-                const T fct = M[r2][c] / M[c][c];
-                r[r2] -= fct * r[c];
-#pragma unroll
-                for (int cc = c + 1; cc < K; ++cc) M[r2][cc] -= fct * M[c][cc];
-            }
-#pragma unroll
-        for (int r2 = K - 1; r2 >= 0; --r2) {
+            const int ijp = o / K, k = o % K, c = sm.code[le][ijp];
+            if (c > -2) continue;
+            const T gp = b.gp[ijp & 1];
+            const T* mi = g.minv + ((size_t)(-2 - c) * K + k) * K;
             T acc = T(0);
 #pragma unroll
-            for (int cc = r2 + 1; cc < K; ++cc) acc += M[r2][cc] * xs[cc];
-            xs[r2] = (r[r2] - acc) / M[r2][r2];
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) sm.com[le][ijp * K + k] = xs[k];
-    }
-    __syncthreads();
-    // corrected normal fluxes, averaged with the neighbour's on interior faces
-    if (active)
-        for (int o = ij; o < NF; o += K2) {
-            const int ijp = o / K, k = o % K, lr = ijp & 1;
-            const int nb = sm.nb[le][ijp];
-            if (nb == -1 - kNeumann) {
-                sm.cg[le][o] = T(0);
-                continue;
+            for (int m = 0; m < K; ++m) {
+                const int om = ijp * K + m;
+                acc -= mi[m] * sm.fa[le][om] * (sm.tg[le][om] - sm.tv[le][om] * gp);
             }
-            const T com = sm.com[le][o];
-            T cross = T(0);
-#pragma unroll
-            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
-            const T dv = sm.tg[le][o] + (com - sm.tv[le][o]) * b.gp[lr];
-            const T fl = (dv * sm.fA[le][o] - cross * sm.fB[le][o]) / sm.fJ[le][o];
-            if (nb < 0) {
-                sm.cg[le][o] = fl;
-            } else {
-                const int nijp = sm.nijp[le][ijp];
-                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
-                const int jn = rev ? K - 1 - k : k;
-                T crn = T(0);
-#pragma unroll
-                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
-                const T dvn = sm.ntg[le][o] + (com - sm.ntv[le][o]) * b.gp[nijp & 1];
-                const T fln = (dvn * sm.nfA[le][o] - crn * sm.nfB[le][o]) / sm.nfJ[le][o];
-                sm.cg[le][o] = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
-            }
+            sm.com[le][o] = acc;
         }
     __syncthreads();
-    // contravariant gradient (src/HO_2D.cpp:2775-2792)
-    T ft = T(0), gt = T(0);
+    // contravariant gradient (src/HO_2D.cpp:2775-2792) and common normal fluxes
     if (active) {
         T dx = T(0), de = T(0);
 #pragma unroll
@@ -229,12 +169,36 @@ __device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __res
         dx += (sm.com[le][1 * K + j] - sm.tv[le][1 * K + j]) * b.gR[i * 2 + 1];
         de += (sm.com[le][2 * K + i] - sm.tv[le][2 * K + i]) * b.gR[j * 2 + 0];
         de += (sm.com[le][3 * K + i] - sm.tv[le][3 * K + i]) * b.gR[j * 2 + 1];
-        ft = (dx * (xe * xe + ye * ye) - de * (xx * xe + yx * ye)) / J;
-        gt = (de * (xx * xx + yx * yx) - dx * (xx * xe + yx * ye)) / J;
-        sm.a[le][ij] = ft;
-        sm.b[le][ij] = gt;
+        sm.a[le][ij] = dx * g11 + de * g12;
+        sm.b[le][ij] = de * g22 + dx * g12;
+        for (int o = ij; o < NF; o += K2) {
+            const int ijp = o / K, k = o % K, c = sm.code[le][ijp];
+            if (c <= -2) {
+                sm.cg[le][o] = T(0);
+                continue;
+            }
+            const T com = sm.com[le][o];
+            T cross = T(0);
+#pragma unroll
+            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
+            const T dv = sm.tg[le][o] + (com - sm.tv[le][o]) * b.gp[ijp & 1];
+            const T fl = dv * sm.fa[le][o] - cross * sm.fb[le][o];
+            if (c < 0) {
+                sm.cg[le][o] = fl;
+            } else {
+                const int nijp = c & 3, rev = c >> 2;
+                const int jn = rev ? K - 1 - k : k;
+                T crn = T(0);
+#pragma unroll
+                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
+                const T dvn = sm.ntg[le][o] + (com - sm.ntv[le][o]) * b.gp[nijp & 1];
+                const T fln = dvn * sm.nfa[le][o] - crn * sm.nfb[le][o];
+                sm.cg[le][o] = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
+            }
+        }
     }
     __syncthreads();
+    // flux jumps: common flux minus the interior flux extrapolated to the face
     if (active)
         for (int o = ij; o < NF; o += K2) {
             const int ijp = o / K, k = o % K, lr = ijp & 1;
@@ -246,31 +210,47 @@ __device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __res
 #pragma unroll
                 for (int d = 0; d < K; ++d) v -= sm.b[le][d * K + k] * b.sbb[d * 2 + lr];
             }
-            sm.fb[le][o] = v;
+            sm.cg[le][o] = v;
         }
     __syncthreads();
     if (!active) return T(0);
     T lap = T(0);
 #pragma unroll
     for (int d = 0; d < K; ++d) lap += sm.a[le][j * K + d] * b.D[d * K + i];
-    lap += sm.fb[le][0 * K + j] * b.gR[i * 2 + 0] + sm.fb[le][1 * K + j] * b.gR[i * 2 + 1];
+    lap += sm.cg[le][0 * K + j] * b.gR[i * 2 + 0] + sm.cg[le][1 * K + j] * b.gR[i * 2 + 1];
 #pragma unroll
     for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * b.D[d * K + j];
-    lap += sm.fb[le][2 * K + i] * b.gR[j * 2 + 0] + sm.fb[le][3 * K + i] * b.gR[j * 2 + 1];
+    lap += sm.cg[le][2 * K + i] * b.gR[j * 2 + 0] + sm.cg[le][3 * K + i] * b.gR[j * 2 + 1];
     return lap;
 }
 
-// face traces of an element vector held in shared memory
+// Scatter destinations of the face points thread ij emits (prefetched at kernel start).
+template <int K>
+struct TraceDst {
+    static constexpr int K2 = K * K, NF = 4 * K, NO = (NF + K2 - 1) / K2;
+    int dst[NO];
+    __device__ __forceinline__ void load(const int* scat, bool active, int el, int ij) {
+#pragma unroll
+        for (int q = 0; q < NO; ++q) {
+            const int o = ij + q * K2;
+            dst[q] = (active && o < NF) ? scat[el * NF + o] : -1;
+        }
+    }
+};
+
+// face traces of an element vector held in shared memory, written to the neighbours'
+// incoming slots
 template <int K, typename T>
-__device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, T* tv, T* tg, bool active, int el,
+__device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, const TraceDst<K>& td, T* tv, T* tg,
                                             int ij) {
-    constexpr int K2 = K * K, NF = 4 * K;
-    if (!active) return;
-    for (int o = ij; o < NF; o += K2) {
+    constexpr int K2 = K * K;
+#pragma unroll
+    for (int q = 0; q < TraceDst<K>::NO; ++q) {
+        if (td.dst[q] < 0) continue;
         T v, d;
-        face_trace<K, T>(sy, b, o, v, d);
-        tv[el * NF + o] = v;
-        tg[el * NF + o] = d;
+        face_trace<K, T>(sy, b, ij + q * K2, v, d);
+        tv[td.dst[q]] = v;
+        tg[td.dst[q]] = d;
     }
 }
 
@@ -285,13 +265,29 @@ __device__ __forceinline__ T block_apply(const T* __restrict__ dinv, const T* sy
     return acc;
 }
 
-__device__ __forceinline__ bool pc_skip(const KrylovScalars* sc, int mode) {
-    return sc->done || (mode == 1 && sc->s_exit);
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------- fine-level kernels
+// incoming face traces of x (the operand of an operator application that no Krylov
+// kernel produced: the initial guess, a refinement iterate, a caller's vector)
+template <int K, typename T>
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_trace_in(MfOp<T> op, const T* __restrict__ x, T* __restrict__ tv,
+                                                                 T* __restrict__ tg) {
+    using S = Shape<K>;
+    __shared__ T sx[S::EPB][S::K2];
+    __shared__ DevBases<T> sbas;
+    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
+    const int el = blockIdx.x * S::EPB + le;
+    const bool active = le < S::EPB && el < op.g.N;
+    TraceDst<K> td;
+    td.load(op.g.scat, active, el, ij);
+    if (active) sx[le][ij] = x[el * S::K2 + ij];
+    stage_bases(sbas, op.b);
+    __syncthreads();
+    emit_traces<K, T>(sx[active ? le : 0], sbas, td, tv, tg, ij);
+}
+
+
 // r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
@@ -336,85 +332,123 @@ __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
     if (i < n) x[i] = T(0);
 }
 
+// Vector kernels take kVecTiles element tiles per CTA (tile blockIdx.x + t * gridDim.x),
+// so the whole vector is covered in one wave of CTAs, and every thread issues its loads
+// before it reads the solve's `done` flag: the addresses are valid whatever the flag
+// says, so the flag's round trip overlaps the data loads.
+constexpr int kVecTiles = 2;
+
 // p = r + beta (p - omega v) (= r on the first iteration); then either ph = D^{-1} p with
 // its traces (block-Jacobi) or the element sums of p (two-level: coarse right-hand side)
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
                                                                    T* rc) {
     using S = Shape<K>;
+    constexpr int NT = kVecTiles;
     const KrylovScalars* sc = rs.sc;
-    if (sc->done) return;
-    __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
+    __shared__ T sp[NT][S::EPB][S::K2], sz[S::EPB][S::K2];
     __shared__ DevBases<T> sbas;
-    stage_bases(sbas, op.b);
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const int p = el * S::K2 + ij;
-    if (active) {
-        T pv;
-        if (sc->it == 0) {
-            pv = v.r[p];
-        } else {
-            const double beta = (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
-            pv = v.r[p] + T(beta) * (v.p[p] - T(sc->omega) * v.v[p]);
-        }
-        v.p[p] = pv;
-        sp[le][ij] = pv;
+    int el[NT], p[NT];
+    bool act[NT];
+    T r[NT], pp[NT], vv[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
+        act[t] = le < S::EPB && el[t] < op.g.N;
+        p[t] = el[t] * S::K2 + ij;
+        r[t] = act[t] ? v.r[p[t]] : T(0);
+        pp[t] = act[t] ? v.p[p[t]] : T(0);
+        vv[t] = act[t] ? v.v[p[t]] : T(0);
+    }
+    if (sc->done) return;
+    const bool first = sc->it == 0;
+    const double beta = first ? 0.0 : (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
+    const T omega = T(sc->omega);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const T pv = first ? r[t] : r[t] + T(beta) * (pp[t] - omega * vv[t]);
+        if (act[t]) v.p[p[t]] = pv;
+        if (le < S::EPB) sp[t][le][ij] = pv;
     }
     __syncthreads();
     if (rc) {
-        if (active && ij == 0) {
-            T sum = T(0);
 #pragma unroll
-            for (int q = 0; q < S::K2; ++q) sum += sp[le][q];
-            rc[el] = sum;
-        }
+        for (int t = 0; t < NT; ++t)
+            if (act[t] && ij == 0) {
+                T sum = T(0);
+#pragma unroll
+                for (int q = 0; q < S::K2; ++q) sum += sp[t][le][q];
+                rc[el[t]] = sum;
+            }
         return;
     }
-    if (active) {
-        const T z = block_apply<K, T>(op.dinv, sp[le], el, ij);
-        v.ph[p] = z;
-        sz[le][ij] = z;
+    stage_bases(sbas, op.b);
+    for (int t = 0; t < NT; ++t) {
+        TraceDst<K> td;
+        td.load(op.g.scat, act[t], el[t], ij);
+        if (act[t]) {
+            const T z = block_apply<K, T>(op.dinv, sp[t][le], el[t], ij);
+            v.ph[p[t]] = z;
+            sz[le][ij] = z;
+        }
+        __syncthreads();
+        emit_traces<K, T>(sz[act[t] ? le : 0], sbas, td, v.tv, v.tg, ij);
+        __syncthreads();
     }
-    __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], sbas, v.tv, v.tg, active, el, ij);
 }
 
-// two-level smoothing step: z = e + w D^{-1} (f - A e), e = P ec element-wise constant;
-// writes z and its face traces
+// two-level smoothing step: z = e + w D^{-1} (f - A e), e = P u0 element-wise constant;
+// writes z and its face traces. u0 of the element and of its four face neighbours comes
+// either straight from the coarse cycle (one-level hierarchy) or from the level-0 up
+// step u0 = S0 f0 + Q0 u1, evaluated here by five threads per element.
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const T* __restrict__ f,
-                                                                const T* __restrict__ ec, T* __restrict__ z,
-                                                                T* __restrict__ tv, T* __restrict__ tg, double w,
-                                                                const KrylovScalars* sc, int mode) {
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const T* __restrict__ f, CoarseOut<T> co,
+                                                                T* __restrict__ z, T* __restrict__ tv,
+                                                                T* __restrict__ tg, double w, const KrylovScalars* sc,
+                                                                int mode) {
     using S = Shape<K>;
     constexpr int K2 = S::K2;
-    if (pc_skip(sc, mode)) return;
-    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2];
+    const bool skip = pc_skip(sc, mode);  // read early: the round trip overlaps the loads below
+    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], ue[S::EPB][5];
     __shared__ DevBases<T> sbas;
     stage_bases(sbas, op.b);
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const int p = el * K2 + ij;
+    TraceDst<K> td;
+    td.load(op.g.scat, active, el, ij);
+    if (active && ij < 5) {
+        const int c = op.bcol[el * 5 + ij];
+        T u = T(0);
+        if (c >= 0) {
+            if (co.u0) {
+                u = co.u0[c];
+            } else {
+                const size_t rs = (size_t)c * co.S.w, rq = (size_t)c * co.Q.w;
+                for (int k = 0; k < co.S.w; ++k) u += co.S.val[rs + k] * co.f0[co.S.col[rs + k]];
+                for (int k = 0; k < co.Q.w; ++k) u += co.Q.val[rq + k] * co.u1[co.Q.col[rq + k]];
+            }
+        }
+        ue[le][ij] = u;
+    }
+    __syncthreads();
+    if (skip) return;
     if (active) {
         T ae = T(0);
 #pragma unroll
-        for (int s = 0; s < 5; ++s) {
-            const int c = op.bcol[el * 5 + s];
-            if (c >= 0) ae += op.rowsum[((size_t)el * 5 + s) * K2 + ij] * ec[c];
-        }
+        for (int s = 0; s < 5; ++s) ae += op.rowsum[((size_t)el * 5 + s) * K2 + ij] * ue[le][s];
         sr[le][ij] = f[p] - ae;
     }
     __syncthreads();
     if (active) {
-        const T zz = ec[el] + T(w) * block_apply<K, T>(op.dinv, sr[le], el, ij);
+        const T zz = ue[le][0] + T(w) * block_apply<K, T>(op.dinv, sr[le], el, ij);
         z[p] = zz;
         sz[le][ij] = zz;
     }
     __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], sbas, tv, tg, active, el, ij);
+    emit_traces<K, T>(sz[active ? le : 0], sbas, td, tv, tg, ij);
 }
 
 // v = A ph; alpha = rho / (rhat, v)
@@ -422,12 +456,15 @@ template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
-    if (sc->done) return;
+    // read before the operator's loads so the round trips overlap; the flag is uniform
+    // over the grid (only this kernel's last CTA writes it, after every CTA has read it)
+    const int done = sc->done;
     __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const T y = mf_apply<K, T>(op, v.ph, v.tv, v.tg, sm, active, le, el, ij);
+    if (done) return;
     double part[1] = {0.0};
     if (active) {
         const int p = el * S::K2 + ij;
@@ -450,38 +487,58 @@ template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_supdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
                                                                    T* rc) {
     using S = Shape<K>;
+    constexpr int NT = kVecTiles;
     KrylovScalars* sc = rs.sc;
-    if (sc->done) return;
-    __shared__ T sp[S::EPB][S::K2], sz[S::EPB][S::K2];
+    __shared__ T sp[NT][S::EPB][S::K2], sz[S::EPB][S::K2];
     __shared__ DevBases<T> sbas;
-    stage_bases(sbas, op.b);
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const int p = el * S::K2 + ij;
+    int el[NT], p[NT];
+    bool act[NT];
+    T r[NT], vv[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
+        act[t] = le < S::EPB && el[t] < op.g.N;
+        p[t] = el[t] * S::K2 + ij;
+        r[t] = act[t] ? v.r[p[t]] : T(0);
+        vv[t] = act[t] ? v.v[p[t]] : T(0);
+    }
+    if (sc->done) return;
+    const T alpha = T(sc->alpha);
     double part[1] = {0.0};
-    if (active) {
-        const T s = v.r[p] - T(sc->alpha) * v.v[p];
-        v.s[p] = s;
-        sp[le][ij] = s;
-        part[0] = double(s) * double(s);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const T sv = r[t] - alpha * vv[t];
+        if (act[t]) {
+            v.s[p[t]] = sv;
+            part[0] += double(sv) * double(sv);
+        }
+        if (le < S::EPB) sp[t][le][ij] = sv;
     }
     __syncthreads();
     if (rc) {
-        if (active && ij == 0) {
-            T sum = T(0);
 #pragma unroll
-            for (int q = 0; q < S::K2; ++q) sum += sp[le][q];
-            rc[el] = sum;
-        }
+        for (int t = 0; t < NT; ++t)
+            if (act[t] && ij == 0) {
+                T sum = T(0);
+#pragma unroll
+                for (int q = 0; q < S::K2; ++q) sum += sp[t][le][q];
+                rc[el[t]] = sum;
+            }
     } else {
-        if (active) {
-            const T z = block_apply<K, T>(op.dinv, sp[le], el, ij);
-            v.sh[p] = z;
-            sz[le][ij] = z;
+        stage_bases(sbas, op.b);
+        for (int t = 0; t < NT; ++t) {
+            TraceDst<K> td;
+            td.load(op.g.scat, act[t], el[t], ij);
+            if (act[t]) {
+                const T z = block_apply<K, T>(op.dinv, sp[t][le], el[t], ij);
+                v.sh[p[t]] = z;
+                sz[le][ij] = z;
+            }
+            __syncthreads();
+            emit_traces<K, T>(sz[act[t] ? le : 0], sbas, td, v.tv, v.tg, ij);
+            __syncthreads();
         }
-        __syncthreads();
-        emit_traces<K, T>(sz[active ? le : 0], sbas, v.tv, v.tg, active, el, ij);
     }
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -495,12 +552,13 @@ template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     using S = Shape<K>;
     KrylovScalars* sc = rs.sc;
-    if (sc->done || sc->s_exit) return;
+    const bool skip = sc->done || sc->s_exit;  // read early: the round trip overlaps the operator's loads
     __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const T y = mf_apply<K, T>(op, v.sh, v.tv, v.tg, sm, active, le, el, ij);
+    if (skip) return;
     double part[2] = {0.0, 0.0};
     if (active) {
         const int p = el * S::K2 + ij;
@@ -518,15 +576,30 @@ template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
                                                                   int max_iter) {
     using S = Shape<K>;
+    constexpr int NT = kVecTiles;
     KrylovScalars* sc = rs.sc;
-    if (sc->done) return;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < N;
-    const int p = el * S::K2 + ij;
-    const double alpha = sc->alpha;
+    int p[NT];
+    bool act[NT];
+    T x[NT], ph[NT], sh[NT], sv[NT], tv[NT], rh[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const int el = (blockIdx.x + t * gridDim.x) * S::EPB + le;
+        act[t] = le < S::EPB && el < N;
+        p[t] = el * S::K2 + ij;
+        x[t] = act[t] ? v.x[p[t]] : T(0);
+        ph[t] = act[t] ? v.ph[p[t]] : T(0);
+        sh[t] = act[t] ? v.sh[p[t]] : T(0);
+        sv[t] = act[t] ? v.s[p[t]] : T(0);
+        tv[t] = act[t] ? v.t[p[t]] : T(0);
+        rh[t] = act[t] ? v.rhat[p[t]] : T(0);
+    }
+    if (sc->done) return;
+    const T alpha = T(sc->alpha);
     if (sc->s_exit) {  // ||s|| already below tolerance: x += alpha ph and stop
-        if (active) v.x[p] += T(alpha) * v.ph[p];
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+            if (act[t]) v.x[p[t]] = x[t] + alpha * ph[t];
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             sc->rnorm2 = sc->snorm2;
             sc->it += 1;
@@ -535,13 +608,15 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVect
     }
     const double omega = sc->omega;
     double part[2] = {0.0, 0.0};
-    if (active) {
-        v.x[p] += T(alpha) * v.ph[p] + T(omega) * v.sh[p];
-        const T r = v.s[p] - T(omega) * v.t[p];
-        v.r[p] = r;
-        part[0] = double(r) * double(r);
-        part[1] = double(v.rhat[p]) * double(r);
-    }
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+        if (act[t]) {
+            v.x[p[t]] = x[t] + (alpha * ph[t] + T(omega) * sh[t]);
+            const T r = sv[t] - T(omega) * tv[t];
+            v.r[p[t]] = r;
+            part[0] += double(r) * double(r);
+            part[1] += double(rh[t]) * double(r);
+        }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         sc->rnorm2 = out[0];
@@ -611,68 +686,6 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_apply(MfOp<T> op, cons
     if (active) y[el * S::K2 + ij] = yy;
 }
 
-// ---------------------------------------------------------------- coarse levels (scalar CSR)
-template <typename T>
-__device__ __forceinline__ T csr_row(const DevCsr<T>& A, const T* __restrict__ x, int i) {
-    T acc = T(0);
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) acc += A.val[k] * x[A.col[k]];
-    return acc;
-}
-
-// pre-smoothing from zero and residual in one pass: t = f - A (m .* f)
-template <typename T>
-__global__ void k_c_pre(DevCsr<T> A, const T* __restrict__ m, const T* __restrict__ f, T* __restrict__ t,
-                        const KrylovScalars* sc, int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
-    T acc = T(0);
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-        const int j = A.col[k];
-        acc += A.val[k] * (m[j] * f[j]);
-    }
-    t[i] = f[i] - acc;
-}
-
-template <typename T>
-__global__ void k_c_spmv(DevCsr<T> M, const T* __restrict__ x, T* __restrict__ y, const KrylovScalars* sc,
-                         int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M.n) y[i] = csr_row<T>(M, x, i);
-}
-
-// coarse-grid correction and post-smoothing in one pass:
-// u' = m .* f + P uc (recomputed per use), u2 = u' + m .* (f - A u')
-template <typename T>
-__global__ void k_c_post(DevCsr<T> A, DevCsr<T> P, const T* __restrict__ m, const T* __restrict__ f,
-                         const T* __restrict__ uc, T* __restrict__ u2, const KrylovScalars* sc, int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
-    T acc = T(0), ui = T(0);
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-        const int j = A.col[k];
-        const T uj = m[j] * f[j] + csr_row<T>(P, uc, j);
-        acc += A.val[k] * uj;
-        if (j == i) ui = uj;
-    }
-    if (A.ptr[i] == A.ptr[i + 1] || ui == T(0)) ui = m[i] * f[i] + csr_row<T>(P, uc, i);
-    u2[i] = ui + m[i] * (f[i] - acc);
-}
-
-// coarsest level: u = inv f with the inverse stored column-major (coalesced reads)
-template <typename T>
-__global__ void k_c_dense(int n, const T* __restrict__ inv_t, const T* __restrict__ f, T* __restrict__ u,
-                          const KrylovScalars* sc, int mode) {
-    if (pc_skip(sc, mode)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T acc = T(0);
-    for (int j = 0; j < n; ++j) acc += inv_t[(size_t)j * n + i] * f[j];
-    u[i] = acc;
-}
-
 __global__ void k_d2f(const double* a, float* b, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
@@ -711,27 +724,11 @@ template <typename T>
 cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
                         cudaStream_t s) {
     const int N = op.g.N;
-    cudaError_t e = launch_trace<T>(op.K, N, v.x, v.xtv, v.xtg, op.b, s);
-    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v.x, v.xtv, v.xtg)));
     HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v, rs, tol)));
     const size_t n = (size_t)N * op.K * op.K;
     k_zero_if<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v.x, n, rs.sc);
     return cudaGetLastError();
-}
-
-template <typename T>
-static void coarse_cycle(const Precond<T>& pc, int l, const KrylovScalars* sc, int mode, cudaStream_t s) {
-    const CoarseLevel<T>& L = pc.lev[l];
-    const unsigned g = (unsigned)((L.n + 127) / 128);
-    if (l == pc.nlev - 1) {
-        k_c_dense<T><<<g, 128, 0, s>>>(L.n, pc.dense_inv, L.f, L.u, sc, mode);
-        return;
-    }
-    const CoarseLevel<T>& C = pc.lev[l + 1];
-    k_c_pre<T><<<g, 128, 0, s>>>(L.A, L.m, L.f, L.t, sc, mode);
-    k_c_spmv<T><<<(unsigned)((C.n + 127) / 128), 128, 0, s>>>(L.R, L.t, C.f, sc, mode);
-    coarse_cycle(pc, l + 1, sc, mode, s);
-    k_c_post<T><<<g, 128, 0, s>>>(L.A, L.P, L.m, L.f, C.out, L.u2, sc, mode);
 }
 
 template <int K, typename T>
@@ -742,26 +739,26 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
     constexpr int th = Shape<K>::THREADS;
     const bool mg = pc.nlev > 0;
     T* rc = mg ? pc.lev[0].f : nullptr;
-    k_mf_pupdate<K, T><<<g, th, 0, s>>>(op, v, rs, rc);
+    const unsigned gv = (g + kVecTiles - 1) / kVecTiles;
+    k_mf_pupdate<K, T><<<gv, th, 0, s>>>(op, v, rs, rc);
     if (mg) {
-        coarse_cycle(pc, 0, rs.sc, 0, s);
-        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.p, pc.lev[0].out, v.ph, v.tv, v.tg, pc.omega, rs.sc, 0);
+        coarse_cycle<T>(pc, rs.sc, 0, s);
+        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.p, coarse_out(pc), v.ph, v.tv, v.tg, pc.omega, rs.sc, 0);
     }
     k_mf_v<K, T><<<g, th, 0, s>>>(op, v, rs);
-    k_mf_supdate<K, T><<<g, th, 0, s>>>(op, v, rs, rc);
+    k_mf_supdate<K, T><<<gv, th, 0, s>>>(op, v, rs, rc);
     if (mg) {
-        coarse_cycle(pc, 0, rs.sc, 1, s);
-        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.s, pc.lev[0].out, v.sh, v.tv, v.tg, pc.omega, rs.sc, 1);
+        coarse_cycle<T>(pc, rs.sc, 1, s);
+        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.s, coarse_out(pc), v.sh, v.tv, v.tg, pc.omega, rs.sc, 1);
     }
     k_mf_t<K, T><<<g, th, 0, s>>>(op, v, rs);
-    k_xr_update<K, T><<<g, th, 0, s>>>(N, v, rs, max_iter);
+    k_xr_update<K, T><<<gv, th, 0, s>>>(N, v, rs, max_iter);
 }
 
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc) {
     if (pc.nlev == 0) return 6;
-    const int coarse = 3 * (pc.nlev - 1) + 1;
-    return 6 + 2 * (coarse + 1);
+    return 6 + 2 * (coarse_launches(pc) + 1);
 }
 
 template <typename T>
@@ -817,8 +814,7 @@ cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, con
 template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
                         const ReduceScratch& rs, cudaStream_t s) {
-    cudaError_t e = launch_trace<T>(op.K, op.g.N, x, xtv, xtg, op.b, s);
-    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
     HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
                                                                                                   rs)));
     return cudaGetLastError();
@@ -826,8 +822,7 @@ cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, 
 
 template <typename T>
 cudaError_t mf_apply_op(const MfOp<T>& op, const T* x, T* xtv, T* xtg, T* y, cudaStream_t s) {
-    cudaError_t e = launch_trace<T>(op.K, op.g.N, x, xtv, xtg, op.b, s);
-    if (e != cudaSuccess) return e;
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
     HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
     return cudaGetLastError();
 }

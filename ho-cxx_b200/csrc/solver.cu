@@ -73,19 +73,22 @@ struct DeviceState {
     DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
     // Poisson operator and Krylov workspace
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
-    DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol, zero_bc;
+    DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
+    // matrix-free operator data: G11, G12, G22, fa, fb, nfa, nfb, minv (PoisGeom)
+    DeviceBuffer pg64[8], pg32[8], pcode, pscat;
+    std::vector<double> pg_host[8];  // kept for the FP32 copies made on demand
     DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
     DeviceBuffer ktv, ktg, kxtv, kxtg;  // face traces of the Krylov operand and of x
     DeviceBuffer partials, counter, scalars;
     KrylovScalars* h_sc = nullptr;
-    // two-level preconditioner: fine scratch, coarse hierarchy (per level: A, P, R CSR
-    // with FP64 and FP32 values, SPAI-0 weights, work vectors)
-    struct CsrBufs {
-        DeviceBuffer ptr, col, v64, v32;
+    // two-level preconditioner: per coarse level the row-padded cycle operators M, S, Q
+    // (FP64 and FP32 values) and the level's f and u (sized for FP64, reused for FP32)
+    struct EllBufs {
+        DeviceBuffer col, v64, v32;
     };
     struct LevelBufs {
-        CsrBufs A, P, R;
-        DeviceBuffer m64, m32, f, u, t, u2;
+        EllBufs M, S, Q;
+        DeviceBuffer f, u;
     };
     std::vector<std::unique_ptr<LevelBufs>> lev;
     DeviceBuffer dense64, dense32;
@@ -93,6 +96,7 @@ struct DeviceState {
     Precond<float> pc32;
     SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
     double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
+    DeviceBuffer l2flush;               // written between timed steps to evict L2
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
@@ -133,17 +137,29 @@ cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
     return upload(buf, c);
 }
 
-cudaError_t upload_csr(DeviceState::CsrBufs& b, const Csr& A) {
+cudaError_t upload_ell(DeviceState::EllBufs& b, const Ell& A) {
     cudaError_t e;
-    if ((e = upload(b.ptr, A.ptr.empty() ? std::vector<int>{0} : A.ptr)) != cudaSuccess) return e;
     if ((e = upload(b.col, A.col.empty() ? std::vector<int>{0} : A.col)) != cudaSuccess) return e;
     if ((e = upload(b.v64, A.val.empty() ? std::vector<double>{0.0} : A.val)) != cudaSuccess) return e;
     return upload_as<float>(b.v32, A.val.empty() ? std::vector<double>{0.0} : A.val);
 }
 
+// lanes per row for a row-padded matrix of width w: about w/2, a power of two in [4, 32]
+int lanes_for(int w) {
+    int g = 4;
+    while (g < 32 && 2 * g <= std::max(1, w / 2)) g *= 2;
+    return g;
+}
+
 template <typename TM>
-DevCsr<TM> view(const DeviceState::CsrBufs& b, int n, bool f32) {
-    return DevCsr<TM>{n, b.ptr.as<int>(), b.col.as<int>(), f32 ? (const TM*)b.v32.get() : (const TM*)b.v64.get()};
+DevEll<TM> view(const DeviceState::EllBufs& b, const Ell& A, int g, bool f32) {
+    DevEll<TM> v;
+    v.n = A.n;
+    v.w = A.w;
+    v.g = g;
+    v.col = b.col.as<int>();
+    v.val = f32 ? (const TM*)b.v32.get() : (const TM*)b.v64.get();
+    return v;
 }
 
 }  // namespace
@@ -257,10 +273,11 @@ Error Solver::setup() {
     HO2D_CUDA(upload(d.dinv64, op_.dinv), "upload block-Jacobi");
     HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
-    HO2D_CUDA(upload(d.zero_bc, std::vector<double>(std::max<size_t>(1, (size_t)neb * K), 0.0)), "alloc");
+    HO2D_TRY(build_poisson_geometry(fnb, fnijp));
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
     d.rowsum32.reset();
+    for (auto& b : d.pg32) b.reset();
     HO2D_TRY(setup_preconditioner());
     for (auto& b : d.kv) HO2D_CUDA(upload(b, zv), "alloc Krylov");
     const int mb = krylov_max_blocks(K, N);
@@ -272,6 +289,91 @@ Error Solver::setup() {
     setup_done_ = true;
     if (mixed_) HO2D_TRY(upload_precision_arrays());
     HO2D_CUDA(cudaDeviceSynchronize(), "setup");
+    return {0, ""};
+}
+
+// Static data of the matrix-free Poisson operator (PoisGeom in fr_launch.hpp): metric and
+// face coefficients with the divisions by J and J_f done here, the neighbour's face
+// coefficients gathered into this element's rows, face codes, the inverted K x K
+// common-value system of every Neumann edge, and the trace scatter table.
+Error Solver::build_poisson_geometry(const std::vector<int>& fnb, const std::vector<int>& fnijp) {
+    DeviceState& d = *d_;
+    const int N = mesh_.n_el, K = in_.knod, K2 = K * K, NF = 4 * K, neb = mesh_.n_eb;
+    const size_t nv = (size_t)N * K2, nf = (size_t)N * NF;
+    std::vector<double>* h = d.pg_host;
+    for (int a = 0; a < 3; ++a) h[a].assign(nv, 0.0);
+    for (int a = 3; a < 7; ++a) h[a].assign(nf, 0.0);
+    h[7].assign((size_t)std::max(1, neb) * K * K, 0.0);
+    for (size_t p = 0; p < nv; ++p) {
+        const double xx = M_.xxi[p], xe = M_.xeta[p], yx = M_.yxi[p], ye = M_.yeta[p], J = M_.J[p];
+        h[0][p] = (xe * xe + ye * ye) / J;
+        h[1][p] = -(xx * xe + yx * ye) / J;
+        h[2][p] = (xx * xx + yx * yx) / J;
+    }
+    for (size_t q = 0; q < nf; ++q) {
+        h[3][q] = M_.fA[q] / M_.fJ[q];
+        h[4][q] = M_.fB[q] / M_.fJ[q];
+    }
+    std::vector<int> code((size_t)N * 4), scat(nf, -1);
+    for (int el = 0; el < N; ++el)
+        for (int ijp = 0; ijp < 4; ++ijp) {
+            const int nb = fnb[(size_t)el * 4 + ijp];
+            if (nb >= 0) {
+                const int nijp = fnijp[(size_t)el * 4 + ijp];
+                const int rev = (ijp + nijp - ijp / 2 - nijp / 2 + 1) % 2;
+                code[(size_t)el * 4 + ijp] = nijp + 4 * rev;
+                for (int k = 0; k < K; ++k) {
+                    const size_t q = ((size_t)el * 4 + ijp) * K + k;
+                    const size_t nq = ((size_t)nb * 4 + nijp) * K + (rev ? K - 1 - k : k);
+                    h[5][q] = h[3][nq];
+                    h[6][q] = h[4][nq];
+                    scat[nq] = (int)q;  // the neighbour's point feeds this element's slot
+                }
+                continue;
+            }
+            const int e = -nb - 1;
+            if (bc_.sw_p[e] != kNeumann) {
+                code[(size_t)el * 4 + ijp] = -1;
+                continue;
+            }
+            code[(size_t)el * 4 + ijp] = -2 - e;
+            // M[k][c] = -fb_k l_c'(x_k) + fa_k g'(+-1) delta_kc (rows scaled by 1/J_f)
+            const int lr = ijp & 1;
+            std::vector<double> A((size_t)K * K), I((size_t)K * K, 0.0);
+            for (int k = 0; k < K; ++k) {
+                const size_t q = ((size_t)el * 4 + ijp) * K + k;
+                for (int c = 0; c < K; ++c) A[(size_t)k * K + c] = -h[4][q] * B_.D[(size_t)c * K + k];
+                A[(size_t)k * K + k] += h[3][q] * B_.gp[lr];
+                I[(size_t)k * K + k] = 1.0;
+            }
+            for (int c = 0; c < K; ++c) {  // Gauss-Jordan with partial pivoting
+                int piv = c;
+                for (int r = c + 1; r < K; ++r)
+                    if (std::fabs(A[(size_t)r * K + c]) > std::fabs(A[(size_t)piv * K + c])) piv = r;
+                if (A[(size_t)piv * K + c] == 0.0) return {3, "singular Neumann common-value system"};
+                for (int m = 0; m < K; ++m) {
+                    std::swap(A[(size_t)c * K + m], A[(size_t)piv * K + m]);
+                    std::swap(I[(size_t)c * K + m], I[(size_t)piv * K + m]);
+                }
+                const double inv = 1.0 / A[(size_t)c * K + c];
+                for (int m = 0; m < K; ++m) {
+                    A[(size_t)c * K + m] *= inv;
+                    I[(size_t)c * K + m] *= inv;
+                }
+                for (int r = 0; r < K; ++r) {
+                    if (r == c) continue;
+                    const double f = A[(size_t)r * K + c];
+                    for (int m = 0; m < K; ++m) {
+                        A[(size_t)r * K + m] -= f * A[(size_t)c * K + m];
+                        I[(size_t)r * K + m] -= f * I[(size_t)c * K + m];
+                    }
+                }
+            }
+            std::copy(I.begin(), I.end(), h[7].begin() + (size_t)e * K * K);
+        }
+    for (int a = 0; a < 8; ++a) HO2D_CUDA(upload(d.pg64[a], h[a]), "upload Poisson operator data");
+    HO2D_CUDA(upload(d.pcode, code), "upload Poisson face codes");
+    HO2D_CUDA(upload(d.pscat, scat), "upload trace scatter table");
     return {0, ""};
 }
 
@@ -293,47 +395,70 @@ Error Solver::setup_preconditioner() {
     HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H));
     if ((int)H.levels.size() > kMaxLevels) return {4, "coarse hierarchy too deep"};
     const int nl = (int)H.levels.size();
+    // levels below `top` run inside the cluster kernel: their f and u copies (FP64 sized)
+    // must fit its shared memory and the level it restricts into must be small
+    constexpr size_t kClusterSmemBudget = 160 * 1024;
+    constexpr int kClusterRowsMax = 8192;
+    auto smem_below = [&](int t) {
+        size_t n = 0;
+        for (int l = t + 1; l < nl; ++l) n += 2 * (size_t)H.levels[l].A.n;
+        return n * sizeof(double);
+    };
+    int top = 0;
+    while (top < nl - 1 && (smem_below(top) > kClusterSmemBudget || H.levels[top + 1].A.n > kClusterRowsMax)) ++top;
+    if (const char* ft = std::getenv("HO2D_COARSE_TOP")) top = std::max(top, std::min(nl - 1, std::atoi(ft)));
+    std::vector<Ell> eM(nl), eS(nl), eQ(nl);
     for (int l = 0; l < nl; ++l) {
         const AmgLevel& L = H.levels[l];
         auto b = std::unique_ptr<DeviceState::LevelBufs>(new DeviceState::LevelBufs);
-        HO2D_CUDA(upload_csr(b->A, L.A), "upload coarse A");
-        HO2D_CUDA(upload_csr(b->P, L.P), "upload coarse P");
-        HO2D_CUDA(upload_csr(b->R, L.R), "upload coarse R");
-        HO2D_CUDA(upload(b->m64, L.m), "upload smoother");
-        HO2D_CUDA(upload_as<float>(b->m32, L.m), "upload smoother");
+        if (l + 1 < nl) {
+            eM[l] = to_ell(L.M);
+            eS[l] = to_ell(L.S);
+            eQ[l] = to_ell(L.Q);
+            HO2D_CUDA(upload_ell(b->M, eM[l]), "upload coarse M");
+            HO2D_CUDA(upload_ell(b->S, eS[l]), "upload coarse S");
+            HO2D_CUDA(upload_ell(b->Q, eQ[l]), "upload coarse Q");
+        }
         const std::vector<double> z(std::max(1, L.A.n), 0.0);
-        for (DeviceBuffer* v : {&b->f, &b->u, &b->t, &b->u2}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
+        for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
         d.lev.push_back(std::move(b));
     }
-    std::vector<double> inv_t(H.dense_inv.size());  // column-major for coalesced device reads
-    for (int i = 0; i < H.n_dense; ++i)
-        for (int j = 0; j < H.n_dense; ++j) inv_t[(size_t)j * H.n_dense + i] = H.dense_inv[(size_t)i * H.n_dense + j];
-    HO2D_CUDA(upload(d.dense64, inv_t), "upload dense");
-    HO2D_CUDA(upload_as<float>(d.dense32, inv_t), "upload dense");
-    auto fill = [&](auto& pc, bool f32) {
-        using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense_inv)>::type>::type;
-        using TM = T;
+    HO2D_CUDA(upload(d.dense64, H.dense_inv), "upload dense");
+    HO2D_CUDA(upload_as<float>(d.dense32, H.dense_inv), "upload dense");
+    auto fill = [&](auto& pc, bool f32) -> cudaError_t {
+        using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
         pc.nlev = nl;
+        pc.top = top;
         pc.omega = omega;
-        pc.dense_inv = f32 ? (const TM*)d.dense32.get() : (const TM*)d.dense64.get();
+        pc.dense.n = pc.dense.w = H.n_dense;
+        pc.dense.g = lanes_for(H.n_dense);
+        pc.dense.col = nullptr;
+        pc.dense.val = f32 ? (const T*)d.dense32.get() : (const T*)d.dense64.get();
+        int off = 0;
         for (int l = 0; l < nl; ++l) {
-            const AmgLevel& L = H.levels[l];
             auto& b = *d.lev[l];
             auto& c = pc.lev[l];
-            c.n = L.A.n;
-            c.A = view<TM>(b.A, L.A.n, f32);
-            c.P = view<TM>(b.P, L.P.n, f32);
-            c.R = view<TM>(b.R, L.R.n, f32);
-            c.m = f32 ? (const TM*)b.m32.get() : (const TM*)b.m64.get();
+            c.n = H.levels[l].A.n;
+            if (l + 1 < nl) {
+                c.M = view<T>(b.M, eM[l], lanes_for(eM[l].w), f32);
+                const int g = lanes_for(std::max(eS[l].w, eQ[l].w));
+                c.S = view<T>(b.S, eS[l], g, f32);
+                c.Q = view<T>(b.Q, eQ[l], g, f32);
+            }
             c.f = b.f.as<T>();
             c.u = b.u.as<T>();
-            c.t = b.t.as<T>();
-            c.u2 = b.u2.as<T>();
-            c.out = (l == nl - 1) ? c.u : c.u2;
+            c.sf = c.su = -1;
+            if (l > top) {
+                c.sf = off;
+                c.su = off + c.n;
+                off += 2 * c.n;
+            }
         }
+        pc.smem = off * (int)sizeof(T);
+        return coarse_prepare(pc);
     };
-    fill(d.pc64, false);
-    fill(d.pc32, true);
+    HO2D_CUDA(fill(d.pc64, false), "coarse cluster kernel attributes");
+    HO2D_CUDA(fill(d.pc32, true), "coarse cluster kernel attributes");
     coarse_levels_ = nl;
     coarse_sizes_.clear();
     for (const auto& L : H.levels) coarse_sizes_.push_back(L.A.n);
@@ -347,6 +472,7 @@ Error Solver::upload_precision_arrays() {
     for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
     HO2D_CUDA(upload_as<float>(d.dinv32, op_.dinv), "upload fp32 block-Jacobi");
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
+    for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");
     d.have32 = true;
     return {0, ""};
 }
@@ -395,9 +521,19 @@ template <typename T>
 static MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
     MfOp<T> op;
     op.K = K;
-    op.g = geom_of<T>(d, m, f32);
+    op.g.N = m.n_el;
+    const DeviceBuffer* pg = f32 ? d.pg32 : d.pg64;
+    op.g.G11 = pg[0].as<T>();
+    op.g.G12 = pg[1].as<T>();
+    op.g.G22 = pg[2].as<T>();
+    op.g.fa = pg[3].as<T>();
+    op.g.fb = pg[4].as<T>();
+    op.g.nfa = pg[5].as<T>();
+    op.g.nfb = pg[6].as<T>();
+    op.g.minv = pg[7].as<T>();
+    op.g.code = d.pcode.as<int>();
+    op.g.scat = d.pscat.as<int>();
     op.b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
-    op.zero_bc = d.zero_bc.as<double>();
     op.dinv = f32 ? (const T*)d.dinv32.get() : (const T*)d.dinv64.get();
     op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
     op.bcol = d.bcol.as<int>();
@@ -671,18 +807,29 @@ Error Solver::time_steps(int nsteps, double* total_ms, double* poisson_ms) {
     if (!setup_done_) return {1, "ho2d_time_steps called before ho2d_setup"};
     DeviceState& d = *d_;
     HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    // twice the 126 MB L2: writing it before a step evicts what the previous step left there
+    constexpr size_t kFlushBytes = size_t(256) << 20;
+    if (!d.l2flush.get()) HO2D_CUDA(d.l2flush.alloc(kFlushBytes), "cudaMalloc");
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     timing_ = true;
     poisson_ms_acc_ = 0.0;
-    HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
-    Error e = step(nsteps);
+    double total = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        HO2D_CUDA(cudaMemsetAsync(d.l2flush.get(), s & 0xff, kFlushBytes, d.stream), "L2 flush");
+        HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
+        Error e = step(1);
+        if (e.code) {
+            timing_ = false;
+            return e;
+        }
+        HO2D_CUDA(cudaEventRecord(d.ev1, d.stream), "event");
+        HO2D_CUDA(cudaEventSynchronize(d.ev1), "event");
+        float ms = 0.f;
+        HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
+        total += ms;
+    }
     timing_ = false;
-    HO2D_TRY(e);
-    HO2D_CUDA(cudaEventRecord(d.ev1, d.stream), "event");
-    HO2D_CUDA(cudaEventSynchronize(d.ev1), "event");
-    float ms = 0.f;
-    HO2D_CUDA(cudaEventElapsedTime(&ms, d.ev0, d.ev1), "event");
-    if (total_ms) *total_ms = ms;
+    if (total_ms) *total_ms = total;
     if (poisson_ms) *poisson_ms = poisson_ms_acc_;
     return {0, ""};
 }
@@ -690,8 +837,8 @@ Error Solver::time_steps(int nsteps, double* total_ms, double* poisson_ms) {
 // Average duration of the Poisson operator kernel (k_mf_apply: y = A x, matrix-free, the
 // same device code as every operator application inside the Krylov solve) over `reps`
 // launches between CUDA events on the handle's stream, and its algorithmic bytes per
-// launch: x, the 5 volume metrics and y once per DOF, the face traces (value and normal
-// derivative) and the 3 face metrics once per face point, 8 connectivity words per element.
+// launch: per point x, the 3 metric coefficients and y; per face point the 4 face
+// coefficients and the 2 incoming traces; 4 face codes per element.
 Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     if (!setup_done_) return {1, "not set up"};
     if (reps <= 0) return {1, "reps must be positive"};
@@ -699,7 +846,7 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
     const int N = mesh_.n_el, K = in_.knod;
     const size_t w = mixed_ ? 4 : 8;
-    if (bytes) *bytes = double((size_t)N * ((7 * (size_t)K * K + 20 * (size_t)K) * w + 32));
+    if (bytes) *bytes = double((size_t)N * ((5 * (size_t)K * K + 24 * (size_t)K) * w + 16));
     if (!mixed_) {
         const MfOp<double> op = make_op<double>(d, mesh_, K, false);
         HO2D_CUDA(mf_apply_op<double>(op, d.psi64.as<double>(), d.kxtv.as<double>(), d.kxtg.as<double>(),

@@ -84,6 +84,7 @@ class Solver {
     Error velocity_only_t();
     Error upload_precision_arrays();
     Error setup_preconditioner();
+    Error build_poisson_geometry(const std::vector<int>& fnb, const std::vector<int>& fnijp);
     Error cuda(cudaError_t e, const char* what);
 
     Input in_;

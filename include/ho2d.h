@@ -119,7 +119,9 @@ int ho2d_get_time(ho2d_solver* handle, double* time, double* dt);
  * cycle of problem types 2 and 3. */
 int ho2d_set_time(ho2d_solver* handle, double time);
 /* Runs nsteps time steps and reports device time between CUDA events recorded on the
- * handle's stream around them: total milliseconds and the part spent in Poisson solves. */
+ * handle's stream around each step: total milliseconds and the part spent in Poisson
+ * solves. Before each step (outside its events) a 256 MiB device buffer is written, so
+ * no step starts with the previous step's data in the 126 MB L2. */
 int ho2d_time_steps(ho2d_solver* handle, int32_t nsteps, double* total_ms, double* poisson_ms);
 /* Runs the Poisson operator kernel (matrix-free y = A psi, the kernel every operator
  * application of the Krylov solve uses) `reps` times back to back on the current psi, in

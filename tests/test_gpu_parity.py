@@ -148,3 +148,23 @@ def test_nonfinite_vorticity_rejected(tmp_path):
     with pytest.raises(capi.HO2DError) as e:
         s.set_vorticity(w)
     assert e.value.code == 7
+
+
+# every split of the coarse cycle between grid-wide kernels and the cluster kernel, and
+# plain block-Jacobi, converge to the same streamfunction (3,600 elements: 3 coarse levels)
+@pytest.mark.parametrize("env", [{}, {"HO2D_COARSE_TOP": "1"}, {"HO2D_COARSE_TOP": "99"},
+                                 {"HO2D_PRECOND": "bj"}])
+def test_preconditioner_layouts_agree_with_oracle(tmp_path, monkeypatch, env):
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    inp = meshgen.make_case("cavityj60", str(tmp_path), knod=3, steps=2)
+    c = O.Case(inp)
+    rng = np.random.Generator(np.random.PCG64(5))
+    w0 = rng.standard_normal((c.N, c.K, c.K))
+    c.omega = w0.copy()
+    c.run(2)
+    s = solver_for(inp, max_iter=5000)
+    s.set_vorticity(w0)
+    s.solve_advection_diffusion(2)
+    assert rel(s.get_streamfunction(), c.psi) < TOL64
+    assert rel(s.get_vorticity(), c.omega) < TOL64
