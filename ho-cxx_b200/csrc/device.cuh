@@ -67,6 +67,7 @@ struct KrylovScalars {
     double rho, rho_old, alpha, omega, beta;
     double bnorm2, rnorm2, snorm2, eps2;
     int it, done, breakdown, s_exit, zero_rhs, pad;
+    double tol;  // relative tolerance of the next solve, written by the host before it starts
 };
 
 // A preconditioner application is skipped once the solve is done, and the second one of

@@ -120,23 +120,16 @@ template <typename T>
 struct CoarseLevel {
     int n = 0;
     DevEll<T> M, S, Q;  // empty on the coarsest level
-    T* f = nullptr;     // right-hand side (global memory)
-    T* u = nullptr;     // result (global memory)
-    int sf = -1, su = -1;  // offsets (in T) of f and u in the cluster kernel's shared memory
+    T* f = nullptr;     // right-hand side (zero-padded past n)
+    T* u = nullptr;     // result
 };
 
 constexpr int kMaxLevels = 16;
 
-// Preconditioner: nlev == 0 -> block-Jacobi; otherwise the two-level cycle whose coarse
-// part runs levels [0, top) as grid-wide kernels and levels [top, nlev) in one thread-block
-// cluster, which reads f_top from global memory and leaves u_o, o = min(top + 1, nlev - 1),
-// in global memory.
+// Preconditioner: nlev == 0 -> block-Jacobi; otherwise the two-level cycle (coarse.cu)
 template <typename T>
 struct Precond {
     int nlev = 0;
-    int top = 0;
-    int cluster = 8;  // CTAs in the coarse-cycle cluster
-    int smem = 0;     // dynamic shared memory of the cluster kernel, bytes
     double omega = 1.0;  // weight of the block-Jacobi smoothing step
     CoarseLevel<T> lev[kMaxLevels];
     DevEll<T> dense;  // row-major inverse of the coarsest operator (col == nullptr)
@@ -152,9 +145,6 @@ struct CoarseOut {
     const T* u1 = nullptr;
 };
 
-// picks the cluster size and sets the cluster kernel's attributes; call once per Precond
-template <typename T>
-cudaError_t coarse_prepare(Precond<T>& pc);
 // enqueues the coarse part of one preconditioner application on f_0 = pc.lev[0].f
 template <typename T>
 cudaError_t coarse_cycle(const Precond<T>& pc, const KrylovScalars* sc, int mode, cudaStream_t s);
@@ -164,8 +154,7 @@ template <typename T>
 CoarseOut<T> coarse_out(const Precond<T>& pc);
 
 template <typename T>
-cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
-                        cudaStream_t s);
+cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, cudaStream_t s);
 template <typename T>
 cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                              const Precond<T>& pc, cudaStream_t s);
@@ -173,8 +162,8 @@ template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc);
 // a whole solve (initial residual + device-side while loop of iterations) as a CUDA graph
 template <typename T>
-cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
-                                 int max_iter, const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out);
+cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                                 const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out);
 // r = b - A x with ||r||^2 -> sc->rnorm2, ||b||^2 -> sc->bnorm2 (traces of x into xtv/xtg)
 template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,

@@ -10,7 +10,7 @@
 //   strength |a_ij| > 0.08 sqrt(|a_ii a_jj|), greedy plain aggregation, piecewise-constant
 //   tentative prolongator, one damped-Jacobi smoothing step of it on the filtered matrix
 //   with omega = (4/3) / rho(D^-1 A_f) (Gershgorin bound), R = P^T, A_c = R A P;
-//   SPAI-0 smoothers (Broeker & Grote 2002); dense inverse once n <= kDenseMax.
+//   SPAI-0 smoothers (Broeker & Grote 2002); dense inverse of the last level.
 #include <algorithm>
 #include <cmath>
 
@@ -224,36 +224,54 @@ bool sa_prolongator(const Csr& A, Csr& P) {
     return true;
 }
 
+// Inverse by LU with partial pivoting (rows updated in parallel), then one forward and
+// back substitution per column of the identity (columns in parallel).
 bool dense_inverse(int n, const Csr& A, std::vector<double>& inv) {
     std::vector<double> a((size_t)n * n, 0.0);
-    inv.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) {
-        inv[(size_t)i * n + i] = 1.0;
+    for (int i = 0; i < n; ++i)
         for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) a[(size_t)i * n + A.col[k]] += A.val[k];
-    }
+    std::vector<int> piv(n);
     for (int k = 0; k < n; ++k) {
         int p = k;
         for (int i = k + 1; i < n; ++i)
             if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)p * n + k])) p = i;
         if (a[(size_t)p * n + k] == 0.0) return false;
+        piv[k] = p;
         if (p != k)
-            for (int j = 0; j < n; ++j) {
-                std::swap(a[(size_t)k * n + j], a[(size_t)p * n + j]);
-                std::swap(inv[(size_t)k * n + j], inv[(size_t)p * n + j]);
-            }
+            for (int j = 0; j < n; ++j) std::swap(a[(size_t)k * n + j], a[(size_t)p * n + j]);
         const double d = 1.0 / a[(size_t)k * n + k];
-        for (int j = 0; j < n; ++j) {
-            a[(size_t)k * n + j] *= d;
-            inv[(size_t)k * n + j] *= d;
+        const double* rk = &a[(size_t)k * n];
+#pragma omp parallel for schedule(static) if (n - k > 256)
+        for (int i = k + 1; i < n; ++i) {
+            double* ri = &a[(size_t)i * n];
+            const double l = ri[k] * d;
+            ri[k] = l;
+            if (l != 0.0)
+                for (int j = k + 1; j < n; ++j) ri[j] -= l * rk[j];
         }
-        for (int i = 0; i < n; ++i) {
-            if (i == k) continue;
-            const double l = a[(size_t)i * n + k];
-            if (l == 0.0) continue;
-            for (int j = 0; j < n; ++j) {
-                a[(size_t)i * n + j] -= l * a[(size_t)k * n + j];
-                inv[(size_t)i * n + j] -= l * inv[(size_t)k * n + j];
+    }
+    inv.assign((size_t)n * n, 0.0);
+#pragma omp parallel
+    {
+        std::vector<double> x(n);
+#pragma omp for schedule(dynamic, 16)
+        for (int c = 0; c < n; ++c) {
+            std::fill(x.begin(), x.end(), 0.0);
+            x[c] = 1.0;
+            for (int k = 0; k < n; ++k) std::swap(x[k], x[piv[k]]);
+            for (int i = 1; i < n; ++i) {
+                const double* ri = &a[(size_t)i * n];
+                double s = x[i];
+                for (int j = 0; j < i; ++j) s -= ri[j] * x[j];
+                x[i] = s;
             }
+            for (int i = n - 1; i >= 0; --i) {
+                const double* ri = &a[(size_t)i * n];
+                double s = x[i];
+                for (int j = i + 1; j < n; ++j) s -= ri[j] * x[j];
+                x[i] = s / ri[i];
+            }
+            for (int i = 0; i < n; ++i) inv[(size_t)i * n + c] = x[i];
         }
     }
     return true;
@@ -266,6 +284,7 @@ Ell to_ell(const Csr& A) {
     E.n = A.n;
     E.m = A.m;
     for (int i = 0; i < A.n; ++i) E.w = std::max(E.w, A.ptr[i + 1] - A.ptr[i]);
+    E.w = (E.w + 3) / 4 * 4;  // rows start on 16-byte boundaries
     E.col.assign((size_t)E.n * E.w, 0);
     E.val.assign((size_t)E.n * E.w, 0.0);
     for (int i = 0; i < A.n; ++i)
@@ -305,11 +324,15 @@ Csr p0_coarse_operator(const PoissonOperator& op, int N) {
     return A;
 }
 
-Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H) {
+Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max, int dense_max_first) {
     H = CoarseHierarchy();
     H.levels.emplace_back();
     H.levels[0].A = A1;
-    while (H.levels.back().A.n > kDenseMax && H.levels.size() < 25) {
+    auto coarsen = [&]() {
+        const int n = H.levels.back().A.n;
+        return n > (H.levels.size() == 1 ? dense_max_first : dense_max);
+    };
+    while (coarsen() && H.levels.size() < 16) {
         AmgLevel& L = H.levels.back();
         Csr P;
         if (!sa_prolongator(L.A, P)) break;
@@ -330,7 +353,8 @@ Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H) {
         L.Q = multiply(identity_minus_scaled(L.A, L.m, {}), L.P);
     }
     const Csr& Ab = H.levels.back().A;
-    if (Ab.n > 4 * kDenseMax) return {4, "coarse Poisson problem did not coarsen below the dense-solve size"};
+    if (Ab.n > 2 * std::max(dense_max, kDenseMax))
+        return {4, "coarse Poisson problem did not coarsen below the dense-solve size"};
     H.n_dense = Ab.n;
     if (!dense_inverse(Ab.n, Ab, H.dense_inv)) return {3, "singular coarsest Poisson operator"};
     return {0, ""};

@@ -7,7 +7,12 @@
 
 namespace ho2d {
 
-constexpr int kDenseMax = 384;  // the coarsest level is inverted densely below this size
+// The coarsest level is inverted densely once it has at most this many rows; the device
+// applies the inverse as one grid-wide matrix-vector product (4096^2 FP32 values = 64 MB).
+// Level 0 is inverted densely only below kDenseMaxFirst rows: beyond that one coarsening
+// step is cheaper than a large dense P0 level.
+constexpr int kDenseMax = 4096;
+constexpr int kDenseMaxFirst = 1024;
 
 struct Csr {
     int n = 0, m = 0;
@@ -25,8 +30,9 @@ struct AmgLevel {
     Csr M, S, Q;  // empty on the coarsest level
 };
 
-// Row-padded (ELL) copy of a sparse matrix: every row holds exactly w entries, padding
-// entries have column 0 and value 0, so a row is read without a row pointer.
+// Row-padded (ELL) copy of a sparse matrix: every row holds exactly w entries (w a
+// multiple of 4), padding entries have column 0 and value 0, so a row is read without a
+// row pointer and every row starts on a 16-byte boundary.
 struct Ell {
     int n = 0, m = 0, w = 0;
     std::vector<int> col;     // [n][w]
@@ -42,6 +48,9 @@ struct CoarseHierarchy {
 
 // A1 = P^T A P for P = element indicator: the sum of each K^2 x K^2 block.
 Csr p0_coarse_operator(const PoissonOperator& op, int N);
-Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H);
+// Coarsens A1 until a level has at most dense_max rows (level 0 itself: at most
+// dense_max_first rows) and inverts that level densely.
+Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max = kDenseMax,
+                             int dense_max_first = kDenseMaxFirst);
 
 }  // namespace ho2d

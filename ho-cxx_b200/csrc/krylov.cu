@@ -290,8 +290,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_trace_in(MfOp<T> op, cons
 
 // r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
-                                                                double tol) {
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     using S = Shape<K>;
     __shared__ MfShared<K, T> sm;
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
@@ -313,7 +312,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgV
         KrylovScalars* sc = rs.sc;
         sc->rnorm2 = out[0];
         sc->bnorm2 = out[1];
-        sc->eps2 = tol * tol * out[1];
+        sc->eps2 = sc->tol * sc->tol * out[1];
         sc->rho = out[0];
         sc->rho_old = sc->alpha = sc->omega = 1.0;
         sc->beta = 0.0;
@@ -721,11 +720,11 @@ int krylov_max_blocks(int K, int N) {
 }
 
 template <typename T>
-cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs,
                         cudaStream_t s) {
     const int N = op.g.N;
     HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v.x, v.xtv, v.xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v, rs, tol)));
+    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v, rs)));
     const size_t n = (size_t)N * op.K * op.K;
     k_zero_if<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v.x, n, rs.sc);
     return cudaGetLastError();
@@ -773,7 +772,7 @@ cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const R
 // is one BiCGSTAB iteration; the loop condition lives on the device, so a solve is one
 // graph launch with no host round trip.
 template <typename T>
-cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, double tol,
+cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs,
                                  int max_iter, const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out) {
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaGraphCreate(&g, 0);
@@ -783,7 +782,7 @@ cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, con
     if ((e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
         cudaSuccess)
         return e;
-    krylov_init<T>(op, v, rs, tol, s);
+    krylov_init<T>(op, v, rs, s);
     k_set_loop<<<1, 1, 0, s>>>(rs.sc, h);
     cudaStreamCaptureStatus st;
     const cudaGraphNode_t* deps = nullptr;
@@ -844,13 +843,13 @@ cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s)
 }
 
 #define HO2D_INSTANTIATE_KRYLOV(T)                                                                                \
-    template cudaError_t krylov_init<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, double,     \
+    template cudaError_t krylov_init<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,             \
                                         cudaStream_t);                                                            \
     template cudaError_t krylov_iteration<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, int,    \
                                              const Precond<T>&, cudaStream_t);                                    \
     template int krylov_launches_per_iteration<T>(const Precond<T>&);                                             \
     template cudaError_t krylov_capture_solve<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,     \
-                                                 double, int, const Precond<T>&, cudaStream_t, cudaGraph_t*);     \
+                                                 int, const Precond<T>&, cudaStream_t, cudaGraph_t*);             \
     template cudaError_t mf_residual<T>(const MfOp<T>&, const double*, const T*, T*, T*, double*,                 \
                                         const ReduceScratch&, cudaStream_t);                                      \
     template cudaError_t mf_apply_op<T>(const MfOp<T>&, const T*, T*, T*, T*, cudaStream_t);                      \

@@ -42,14 +42,12 @@ void DeviceBuffer::reset() {
 struct SolveGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    double tol = -1.0;
     int max_iter = -1;
     void reset() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
-        tol = -1.0;
         max_iter = -1;
     }
     ~SolveGraph() { reset(); }
@@ -378,7 +376,8 @@ Error Solver::build_poisson_geometry(const std::vector<int>& fnb, const std::vec
 }
 
 // Builds the P0 coarse hierarchy on the host and the device views of both precisions.
-// HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight.
+// HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight;
+// HO2D_DENSE_MAX bounds the dense coarsest level (a test hook for other hierarchy shapes).
 Error Solver::setup_preconditioner() {
     DeviceState& d = *d_;
     const int N = mesh_.n_el;
@@ -391,22 +390,12 @@ Error Solver::setup_preconditioner() {
     if (mode && std::string(mode) == "bj") return {0, ""};
     const char* om = std::getenv("HO2D_MG_OMEGA");
     const double omega = om ? std::atof(om) : 1.0;
+    const char* dm = std::getenv("HO2D_DENSE_MAX");
+    const int dmax = dm ? std::max(1, std::atoi(dm)) : kDenseMax;
     CoarseHierarchy H;
-    HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H));
+    HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H, dmax, dm ? dmax : kDenseMaxFirst));
     if ((int)H.levels.size() > kMaxLevels) return {4, "coarse hierarchy too deep"};
     const int nl = (int)H.levels.size();
-    // levels below `top` run inside the cluster kernel: their f and u copies (FP64 sized)
-    // must fit its shared memory and the level it restricts into must be small
-    constexpr size_t kClusterSmemBudget = 160 * 1024;
-    constexpr int kClusterRowsMax = 8192;
-    auto smem_below = [&](int t) {
-        size_t n = 0;
-        for (int l = t + 1; l < nl; ++l) n += 2 * (size_t)H.levels[l].A.n;
-        return n * sizeof(double);
-    };
-    int top = 0;
-    while (top < nl - 1 && (smem_below(top) > kClusterSmemBudget || H.levels[top + 1].A.n > kClusterRowsMax)) ++top;
-    if (const char* ft = std::getenv("HO2D_COARSE_TOP")) top = std::max(top, std::min(nl - 1, std::atoi(ft)));
     std::vector<Ell> eM(nl), eS(nl), eQ(nl);
     for (int l = 0; l < nl; ++l) {
         const AmgLevel& L = H.levels[l];
@@ -419,22 +408,27 @@ Error Solver::setup_preconditioner() {
             HO2D_CUDA(upload_ell(b->S, eS[l]), "upload coarse S");
             HO2D_CUDA(upload_ell(b->Q, eQ[l]), "upload coarse Q");
         }
-        const std::vector<double> z(std::max(1, L.A.n), 0.0);
+        const std::vector<double> z((size_t)L.A.n + 4, 0.0);  // zero padding for 16-byte reads
         for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
         d.lev.push_back(std::move(b));
     }
-    HO2D_CUDA(upload(d.dense64, H.dense_inv), "upload dense");
-    HO2D_CUDA(upload_as<float>(d.dense32, H.dense_inv), "upload dense");
-    auto fill = [&](auto& pc, bool f32) -> cudaError_t {
+    // coarsest inverse, rows padded to a multiple of 4 entries (16-byte row starts)
+    const int nd = H.n_dense, wd = (nd + 3) / 4 * 4;
+    std::vector<double> dpad((size_t)nd * wd, 0.0);
+    for (int i = 0; i < nd; ++i)
+        std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
+                  dpad.begin() + (size_t)i * wd);
+    HO2D_CUDA(upload(d.dense64, dpad), "upload dense");
+    HO2D_CUDA(upload_as<float>(d.dense32, dpad), "upload dense");
+    auto fill = [&](auto& pc, bool f32) {
         using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
         pc.nlev = nl;
-        pc.top = top;
         pc.omega = omega;
-        pc.dense.n = pc.dense.w = H.n_dense;
-        pc.dense.g = lanes_for(H.n_dense);
+        pc.dense.n = nd;
+        pc.dense.w = wd;
+        pc.dense.g = 32;
         pc.dense.col = nullptr;
         pc.dense.val = f32 ? (const T*)d.dense32.get() : (const T*)d.dense64.get();
-        int off = 0;
         for (int l = 0; l < nl; ++l) {
             auto& b = *d.lev[l];
             auto& c = pc.lev[l];
@@ -447,21 +441,18 @@ Error Solver::setup_preconditioner() {
             }
             c.f = b.f.as<T>();
             c.u = b.u.as<T>();
-            c.sf = c.su = -1;
-            if (l > top) {
-                c.sf = off;
-                c.su = off + c.n;
-                off += 2 * c.n;
-            }
         }
-        pc.smem = off * (int)sizeof(T);
-        return coarse_prepare(pc);
     };
-    HO2D_CUDA(fill(d.pc64, false), "coarse cluster kernel attributes");
-    HO2D_CUDA(fill(d.pc32, true), "coarse cluster kernel attributes");
+    fill(d.pc64, false);
+    fill(d.pc32, true);
     coarse_levels_ = nl;
     coarse_sizes_.clear();
     for (const auto& L : H.levels) coarse_sizes_.push_back(L.A.n);
+    if (verbose_) {
+        std::fprintf(stderr, "  coarse levels:");
+        for (int n : coarse_sizes_) std::fprintf(stderr, " %d", n);
+        std::fprintf(stderr, " (the last inverted densely)\n");
+    }
     return {0, ""};
 }
 
@@ -578,12 +569,17 @@ Error Solver::poisson_solve() {
     // device-side while loop); with HO2D_GRAPHS=0 the host enqueues batches of iterations
     // and polls the done flag between batches
     auto run = [&](auto A, auto v, const auto& pc, double tol, int& iters, SolveGraph& sg) -> Error {
+        // the tolerance travels in the device scalars, so one captured graph serves any
+        // tolerance (the stream is idle here: every earlier read of h_sc was synchronised)
+        d.h_sc->tol = tol;
+        HO2D_CUDA(cudaMemcpyAsync(&d.scalars.as<KrylovScalars>()->tol, &d.h_sc->tol, sizeof(double),
+                                  cudaMemcpyHostToDevice, d.stream),
+                  "tolerance");
         if (use_graphs_) {
-            if (!sg.exec || sg.tol != tol || sg.max_iter != max_iter_) {
+            if (!sg.exec || sg.max_iter != max_iter_) {
                 sg.reset();
-                HO2D_CUDA(krylov_capture_solve(A, v, rs, tol, max_iter_, pc, d.stream, &sg.graph), "graph capture");
+                HO2D_CUDA(krylov_capture_solve(A, v, rs, max_iter_, pc, d.stream, &sg.graph), "graph capture");
                 HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
-                sg.tol = tol;
                 sg.max_iter = max_iter_;
             }
             HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
@@ -592,7 +588,7 @@ Error Solver::poisson_solve() {
             launches_ += 4 + (int64_t)iters * (krylov_launches_per_iteration(pc) + 1);
             return {0, ""};
         }
-        HO2D_CUDA(krylov_init(A, v, rs, tol, d.stream), "krylov init");
+        HO2D_CUDA(krylov_init(A, v, rs, d.stream), "krylov init");
         launches_ += 3;
         HO2D_TRY(poll());
         int chunk = std::max(1, prev_iters_ - 1);
@@ -644,8 +640,12 @@ Error Solver::poisson_solve() {
             HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
             HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
             launches_ += 1;
+            // ask the inner solve for no more reduction than this sweep needs: the last
+            // sweep typically needs one order of magnitude, not inner_tol_'s four
+            const double need = 0.3 * tol_ / last_res_;
+            const double itol = std::min(0.5, std::max(inner_tol_, need));
             int it = 0;
-            HO2D_TRY(run(A32, v, d.pc32, inner_tol_, it, d.graph32));
+            HO2D_TRY(run(A32, v, d.pc32, itol, it, d.graph32));
             last_iters_ += it;
             HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
             launches_ += 1;

@@ -105,7 +105,7 @@ class Solver {
     int coarse_levels_ = 0;
     std::vector<int> coarse_sizes_;
     double inner_tol_ = 1e-4;        // FP32 inner solve: relative reduction per refinement sweep
-    bool verbose_ = false;           // HO2D_VERBOSE=1: one line per Poisson solve on stderr
+    bool verbose_ = false;           // HO2D_VERBOSE=1: coarse levels and one line per Poisson solve on stderr
     bool use_graphs_ = true;         // HO2D_GRAPHS=0: host-driven Krylov loop instead of a CUDA graph
     bool timing_ = false;
     double poisson_ms_acc_ = 0.0;

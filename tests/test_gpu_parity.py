@@ -150,9 +150,10 @@ def test_nonfinite_vorticity_rejected(tmp_path):
     assert e.value.code == 7
 
 
-# every split of the coarse cycle between grid-wide kernels and the cluster kernel, and
-# plain block-Jacobi, converge to the same streamfunction (3,600 elements: 3 coarse levels)
-@pytest.mark.parametrize("env", [{}, {"HO2D_COARSE_TOP": "1"}, {"HO2D_COARSE_TOP": "99"},
+# every shape of the coarse hierarchy -- P0 + dense level (default), a dense P0 level,
+# three levels with a grid-wide up step -- and plain block-Jacobi converge to the same
+# streamfunction (3,600 elements)
+@pytest.mark.parametrize("env", [{}, {"HO2D_DENSE_MAX": "100"}, {"HO2D_DENSE_MAX": "5000"},
                                  {"HO2D_PRECOND": "bj"}])
 def test_preconditioner_layouts_agree_with_oracle(tmp_path, monkeypatch, env):
     for k, v in env.items():
