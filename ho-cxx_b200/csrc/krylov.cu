@@ -397,52 +397,113 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, Bi
     }
 }
 
+// Part `part` (0..4) of u0 at element c = S0_c . f0 + Q0_c . u1 (a row of the level-0
+// up step): the row entries part, part + 5, ... The first two of each row are loaded
+// before any gather, so a part costs two dependent rounds of loads.
+template <typename T>
+__device__ __forceinline__ T up0_part(const CoarseOut<T>& co, int c, int part) {
+    const size_t rs = (size_t)c * co.S.w, rq = (size_t)c * co.Q.w;
+    T sv[2], qv[2];
+    int sj[2], qj[2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const int k = part + 5 * m;
+        const bool ins = k < co.S.w, inq = k < co.Q.w;
+        sv[m] = ins ? co.S.val[rs + k] : T(0);
+        sj[m] = ins ? co.S.col[rs + k] : 0;
+        qv[m] = inq ? co.Q.val[rq + k] : T(0);
+        qj[m] = inq ? co.Q.col[rq + k] : 0;
+    }
+    T u = sv[0] * co.f0[sj[0]] + qv[0] * co.u1[qj[0]] + sv[1] * co.f0[sj[1]] + qv[1] * co.u1[qj[1]];
+    for (int k = part + 10; k < co.S.w; k += 5) u += co.S.val[rs + k] * co.f0[co.S.col[rs + k]];
+    for (int k = part + 10; k < co.Q.w; k += 5) u += co.Q.val[rq + k] * co.u1[co.Q.col[rq + k]];
+    return u;
+}
+
+// Whether k_mf_post stages its CTA's inverse blocks (EPB x K^4 values, contiguous in
+// memory) in shared memory: when they fit in 32 KB of static shared memory.
+template <int K, typename T>
+struct PostStage {
+    static constexpr int K4 = K * K * K * K;
+    static constexpr size_t kBytes = (size_t)Shape<K>::EPB * K4 * sizeof(T) + 32;  // + 16-byte alignment slack
+    static constexpr bool kOn = kBytes <= 32768;
+};
+
 // two-level smoothing step: z = e + w D^{-1} (f - A e), e = P u0 element-wise constant;
 // writes z and its face traces. u0 of the element and of its four face neighbours comes
 // either straight from the coarse cycle (one-level hierarchy) or from the level-0 up
-// step u0 = S0 f0 + Q0 u1, evaluated here by five threads per element.
+// step u0 = S0 f0 + Q0 u1, evaluated here as 25 partial sums (five per slot) spread over
+// the element's threads. Everything that
+// does not depend on u0 starts first: the CTA's inverse blocks are copied into shared
+// memory asynchronously (cp.async, 16-byte pieces of the 16-byte-aligned superset of the
+// blocks; the buffer is padded past its end) and the block row sums and f are loaded, so
+// all of it overlaps the up step's dependent loads.
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const T* __restrict__ f, CoarseOut<T> co,
                                                                 T* __restrict__ z, T* __restrict__ tv,
                                                                 T* __restrict__ tg, double w, const KrylovScalars* sc,
                                                                 int mode) {
     using S = Shape<K>;
+    using PS = PostStage<K, T>;
     constexpr int K2 = S::K2;
     const bool skip = pc_skip(sc, mode);  // read early: the round trip overlaps the loads below
-    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], ue[S::EPB][5];
+    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25];
     __shared__ DevBases<T> sbas;
-    stage_bases(sbas, op.b);
+    __shared__ __align__(16) unsigned char sd_raw[PS::kOn ? PS::kBytes : 16];
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const int p = el * K2 + ij;
+    const T* dblk = op.dinv + (size_t)el * PS::K4;  // this element's inverse block ([rs][ij])
+    if constexpr (PS::kOn) {
+        const int el0 = blockIdx.x * S::EPB;
+        const int el1 = min(el0 + S::EPB, op.g.N);
+        const size_t b0 = (size_t)el0 * PS::K4 * sizeof(T), b1 = (size_t)el1 * PS::K4 * sizeof(T);
+        const size_t a0 = b0 & ~size_t(15), a1 = (b1 + 15) & ~size_t(15);
+        const char* g = reinterpret_cast<const char*>(op.dinv) + a0;
+        const unsigned sb = (unsigned)__cvta_generic_to_shared(sd_raw);
+        for (size_t o = 16 * (size_t)threadIdx.x; o < a1 - a0; o += 16 * (size_t)blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + (unsigned)o), "l"(g + o) : "memory");
+        dblk = reinterpret_cast<const T*>(sd_raw + (b0 - a0)) + (size_t)le * PS::K4;
+    }
     TraceDst<K> td;
     td.load(op.g.scat, active, el, ij);
-    if (active && ij < 5) {
-        const int c = op.bcol[el * 5 + ij];
-        T u = T(0);
-        if (c >= 0) {
-            if (co.u0) {
-                u = co.u0[c];
-            } else {
-                const size_t rs = (size_t)c * co.S.w, rq = (size_t)c * co.Q.w;
-                for (int k = 0; k < co.S.w; ++k) u += co.S.val[rs + k] * co.f0[co.S.col[rs + k]];
-                for (int k = 0; k < co.Q.w; ++k) u += co.Q.val[rq + k] * co.u1[co.Q.col[rq + k]];
-            }
-        }
-        ue[le][ij] = u;
+    T rsum[5], fp = T(0);
+    if (active) {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) rsum[s] = op.rowsum[((size_t)el * 5 + s) * K2 + ij];
+        fp = f[p];
     }
+    stage_bases(sbas, op.b);
+    // u0 of block slot s (element bcol[5 el + s]) as five partial sums pu[s][part]
+    if (active)
+        for (int t = ij; t < 25; t += K2) {
+            const int slot = t / 5, part = t % 5;
+            const int c = op.bcol[el * 5 + slot];
+            T u = T(0);
+            if (c >= 0) u = co.u0 ? (part == 0 ? co.u0[c] : T(0)) : up0_part(co, c, part);
+            pu[le][t] = u;
+        }
+    if constexpr (PS::kOn) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     if (skip) return;
+    T u_self = T(0);
     if (active) {
         T ae = T(0);
 #pragma unroll
-        for (int s = 0; s < 5; ++s) ae += op.rowsum[((size_t)el * 5 + s) * K2 + ij] * ue[le][s];
-        sr[le][ij] = f[p] - ae;
+        for (int s = 0; s < 5; ++s) {
+            const T us = pu[le][5 * s] + pu[le][5 * s + 1] + pu[le][5 * s + 2] + pu[le][5 * s + 3] + pu[le][5 * s + 4];
+            ae += rsum[s] * us;
+            if (s == 0) u_self = us;
+        }
+        sr[le][ij] = fp - ae;
     }
     __syncthreads();
     if (active) {
-        const T zz = ue[le][0] + T(w) * block_apply<K, T>(op.dinv, sr[le], el, ij);
+        T acc = T(0);
+#pragma unroll
+        for (int r = 0; r < K2; ++r) acc += dblk[r * K2 + ij] * sr[le][r];
+        const T zz = u_self + T(w) * acc;
         z[p] = zz;
         sz[le][ij] = zz;
     }

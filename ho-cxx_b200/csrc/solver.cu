@@ -268,6 +268,9 @@ Error Solver::setup() {
         for (int rs = 0; rs < K2; ++rs)
             for (int ij = 0; ij < K2; ++ij) op_.rowsum[eb * K2 + ij] += blk[rs * K2 + ij];
     }
+    // 8 zero entries past the end: the smoothing kernel copies the 16-byte-aligned
+    // superset of a CTA's blocks into shared memory
+    op_.dinv.resize(op_.dinv.size() + 8, 0.0);
     HO2D_CUDA(upload(d.dinv64, op_.dinv), "upload block-Jacobi");
     HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
