@@ -251,10 +251,13 @@ def run_ours(args, rank, world, local, phys):
     with tempfile.TemporaryDirectory() as tmp:
         inp = make_workload(tmp, args.case, args.knod, args.steps)
         solvers = {}
-        for prec in ("mixed", "fp64"):
+        # headline: FP64 FR stage with the FP32 Krylov inside FP64 refinement (meets the
+        # 1e-6 vorticity target); "mixed_fp32_stage" also runs the FR stage in FP32
+        modes = {"mixed": ho2d.MIXED_KRYLOV, "fp64": ho2d.FP64, "mixed_fp32_stage": ho2d.MIXED}
+        for prec, mode in modes.items():
             s = ho2d.HO_2D()
             s.read_input_file(inp)
-            s.set_precision(ho2d.MIXED if prec == "mixed" else ho2d.FP64)
+            s.set_precision(mode)
             s.setup()
             s.set_time(args.t0)
             solvers[prec] = s
@@ -262,7 +265,7 @@ def run_ours(args, rank, world, local, phys):
         n_dof = s0.N_el * s0.Knod * s0.Knod
         results = {}
         clocks = None
-        for prec in ("mixed", "fp64"):
+        for prec in modes:
             s = solvers[prec]
             s.solve_advection_diffusion(args.warmup)
             dist.barrier()
@@ -282,6 +285,8 @@ def run_ours(args, rank, world, local, phys):
         w_mixed = solvers["mixed"].get_vorticity()
         w_fp64 = solvers["fp64"].get_vorticity()
         l2 = float(np.linalg.norm(w_mixed - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
+        w_f32 = solvers["mixed_fp32_stage"].get_vorticity()
+        l2_f32 = float(np.linalg.norm(w_f32 - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
         # end to end through the public API with host buffers: H2D of the step's input
         # vorticity from pinned memory, the step, D2H of the resulting vorticity
         s = solvers["mixed"]
@@ -300,11 +305,14 @@ def run_ours(args, rank, world, local, phys):
         e2e = {"value": dist.sum(n_dof * e2e_steps) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n_dof * 8,
                "d2h_bytes_per_step": n_dof * 8}
         peak, peak_kind = measured_peaks()
+        # DRAM bytes (read + write) of one k_mf_apply<5, float> launch on this workload, from
+        # the ncu capture summarised in profiles/k_mf_apply_bfs14625_k5_fp32.md
+        traffic = 13119232 if (args.case == "bfs" and args.knod == 5) else None
         m = results["mixed"]
         achieved = m["spmv_bytes"] / (m["spmv_ms"] * 1e-3) / 1e9
         roofline = {"bound": "hbm", "kernel": "k_mf_apply (matrix-free Poisson operator, FP32 inner Krylov)",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_kind": peak_kind, "traffic": None,
+                    "peak_kind": peak_kind, "traffic": traffic,
                     "launch_ms": m["spmv_ms"], "algorithmic_bytes_per_launch": m["spmv_bytes"]}
         f = results["fp64"]
         roofline_fp64 = {"kernel": "k_mf_apply (FP64)", "achieved": f["spmv_bytes"] / (f["spmv_ms"] * 1e-3) / 1e9,
@@ -327,6 +335,14 @@ def run_ours(args, rank, world, local, phys):
                     "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"],
                              "poisson_ms_per_step": f["poisson_ms_per_step"], "roofline": roofline_fp64,
                              "poisson_iterations_last_solve": f["iters"]},
+                    "precision": "HO2D_MIXED_KRYLOV: FP64 FR stage and RK update, FP32 BiCGSTAB with FP32 "
+                                 "preconditioner inside FP64 iterative refinement of the Poisson solve",
+                    "mixed_fp32_stage": {"precision": "HO2D_MIXED: FR stage also in FP32",
+                                         "value": results["mixed_fp32_stage"]["value"],
+                                         "ms_per_step": results["mixed_fp32_stage"]["ms_per_step"],
+                                         "poisson_ms_per_step": results["mixed_fp32_stage"]["poisson_ms_per_step"],
+                                         "poisson_iterations_last_solve": results["mixed_fp32_stage"]["iters"],
+                                         "l2_rel_vorticity_vs_fp64": l2_f32},
                     "mixed_over_fp64": m["value"] / f["value"],
                     "l2_rel_vorticity_mixed_vs_fp64": l2,
                     "l2_after_steps": args.warmup + args.steps,

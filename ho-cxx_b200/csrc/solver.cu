@@ -288,7 +288,7 @@ Error Solver::setup() {
     HO2D_CUDA(cudaMemset(d.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
     time_ = 0.0;
     setup_done_ = true;
-    if (mixed_) HO2D_TRY(upload_precision_arrays());
+    if (stage32_ || krylov32_) HO2D_TRY(upload_precision_arrays());
     HO2D_CUDA(cudaDeviceSynchronize(), "setup");
     return {0, ""};
 }
@@ -472,17 +472,23 @@ Error Solver::upload_precision_arrays() {
 }
 
 Error Solver::set_precision(int mode) {
-    if (mode != 0 && mode != 1) return {1, "precision must be HO2D_FP64 (0) or HO2D_MIXED (1)"};
-    const bool was = mixed_;
-    mixed_ = mode == 1;
-    if (setup_done_ && mixed_ != was) {
-        if (mixed_) HO2D_TRY(upload_precision_arrays());
-        // re-derive the stage input in the new precision from the FP64 vorticity
-        DeviceState& d = *d_;
-        const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
-        if (mixed_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
-        else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
-        HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    if (mode < 0 || mode > 2)
+        return {1, "precision must be HO2D_FP64 (0), HO2D_MIXED (1) or HO2D_MIXED_KRYLOV (2)"};
+    const bool was = stage32_;
+    stage32_ = mode == 1;
+    krylov32_ = mode != 0;
+    if (setup_done_) {
+        if (stage32_ || krylov32_) HO2D_TRY(upload_precision_arrays());
+        if (stage32_ != was) {
+            // re-derive the stage input in the new precision from the FP64 vorticity
+            DeviceState& d = *d_;
+            const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+            if (stage32_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
+            else
+                HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream),
+                          "copy");
+            HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+        }
     }
     return {0, ""};
 }
@@ -609,7 +615,7 @@ Error Solver::poisson_solve() {
     last_iters_ = 0;
     int sweeps = 0;
     bool finite = true;
-    if (!mixed_) {
+    if (!krylov32_) {
         const MfOp<double> A = make_op<double>(d, mesh_, K, false);
         const BicgVectors<double> v = krylov_vectors<double>(d, d.psi64.as<double>(), d.rhs.as<double>());
         int it = 0;
@@ -658,7 +664,7 @@ Error Solver::poisson_solve() {
     if (verbose_)
         std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e\n", n_solves_, last_iters_,
                      sweeps, last_res_);
-    prev_iters_ = std::max(1, mixed_ ? last_iters_ / std::max(1, sweeps) : last_iters_);
+    prev_iters_ = std::max(1, krylov32_ ? last_iters_ / std::max(1, sweeps) : last_iters_);
     if (timing_) {
         HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");
         HO2D_CUDA(cudaEventSynchronize(d.evp1), "event");
@@ -754,7 +760,7 @@ Error Solver::velocity_only_t() {
 }
 
 Error Solver::stage_impl(double coeff, int rk_stage, bool update) {
-    return mixed_ ? stage_t<float>(coeff, rk_stage, update) : stage_t<double>(coeff, rk_stage, update);
+    return stage32_ ? stage_t<float>(coeff, rk_stage, update) : stage_t<double>(coeff, rk_stage, update);
 }
 
 Error Solver::step(int nsteps) {
@@ -787,10 +793,10 @@ Error Solver::solve() {
     HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
     const int nt = in_.num_steps, df = std::max(1, in_.dump_freq);
     for (int ti = 0; ti < nt; ++ti) {
-        if (ti % df == 0) HO2D_TRY(mixed_ ? velocity_only_t<float>() : velocity_only_t<double>());
+        if (ti % df == 0) HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
         HO2D_TRY(step(1));
     }
-    if (nt % df == 0) HO2D_TRY(mixed_ ? velocity_only_t<float>() : velocity_only_t<double>());
+    if (nt % df == 0) HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
     HO2D_CUDA(cudaStreamSynchronize(d_->stream), "solve");
     return {0, ""};
 }
@@ -848,9 +854,9 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     DeviceState& d = *d_;
     HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
     const int N = mesh_.n_el, K = in_.knod;
-    const size_t w = mixed_ ? 4 : 8;
+    const size_t w = krylov32_ ? 4 : 8;
     if (bytes) *bytes = double((size_t)N * ((5 * (size_t)K * K + 24 * (size_t)K) * w + 16));
-    if (!mixed_) {
+    if (!krylov32_) {
         const MfOp<double> op = make_op<double>(d, mesh_, K, false);
         HO2D_CUDA(mf_apply_op<double>(op, d.psi64.as<double>(), d.kxtv.as<double>(), d.kxtg.as<double>(),
                                       d.kv[5].as<double>(), d.stream), "apply");
@@ -928,7 +934,7 @@ Error Solver::get_volume(int which, double* out) {
             return {0, ""};
         default: return {1, "unknown field"};
     }
-    if (typed && mixed_) {
+    if (typed && stage32_) {
         std::vector<float> tmp(nv);
         HO2D_CUDA(cudaMemcpy(tmp.data(), src, nv * 4, cudaMemcpyDeviceToHost), "copy");
         std::copy(tmp.begin(), tmp.end(), out);
@@ -944,7 +950,7 @@ Error Solver::get_velocity(double* out) {
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     std::vector<double> u(nv), v(nv);
-    if (mixed_) {
+    if (stage32_) {
         std::vector<float> uf(nv), vf(nv);
         HO2D_CUDA(cudaMemcpy(uf.data(), d.u.get(), nv * 4, cudaMemcpyDeviceToHost), "copy");
         HO2D_CUDA(cudaMemcpy(vf.data(), d.v.get(), nv * 4, cudaMemcpyDeviceToHost), "copy");
@@ -969,7 +975,7 @@ Error Solver::set_vorticity(const double* in) {
         if (!std::isfinite(in[i])) return {7, "non-finite value in the vorticity passed in"};
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     HO2D_CUDA(cudaMemcpy(d.omega.get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
-    if (mixed_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
+    if (stage32_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
     else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     return {0, ""};

@@ -66,7 +66,7 @@ class Solver {
     double time() const { return time_; }
     void set_time(double t) { time_ = t; }
     double dt() const { return in_.dt; }
-    int precision() const { return mixed_ ? 1 : 0; }
+    int precision() const { return krylov32_ ? (stage32_ ? 1 : 2) : 0; }
     int last_poisson_iterations() const { return last_iters_; }
     double last_poisson_residual() const { return last_res_; }
     int64_t launches() const { return launches_; }
@@ -94,7 +94,8 @@ class Solver {
     BoundaryConditions bc_;
     PoissonOperator op_;
     bool input_done_ = false, setup_done_ = false;
-    bool mixed_ = false;
+    bool stage32_ = false;   // FR stage kernels in FP32 (HO2D_MIXED)
+    bool krylov32_ = false;  // FP32 BiCGSTAB inside FP64 refinement (HO2D_MIXED, HO2D_MIXED_KRYLOV)
     double time_ = 0.0;
     double tol_ = 1e-12;
     int max_iter_ = 500;

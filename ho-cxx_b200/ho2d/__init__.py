@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 
 from . import capi
-from .capi import FP64, MIXED, HO2DError  # noqa: F401
+from .capi import FP64, MIXED, MIXED_KRYLOV, HO2DError  # noqa: F401
 
 
 class HO_2D:

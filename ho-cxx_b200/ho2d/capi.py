@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "lib
 HO2D_OK = 0
 STATUS = {0: "HO2D_OK", 1: "HO2D_ERR_ARG", 2: "HO2D_ERR_IO", 3: "HO2D_ERR_MESH", 4: "HO2D_ERR_UNSUPPORTED",
           5: "HO2D_ERR_CUDA", 6: "HO2D_ERR_NOT_CONVERGED", 7: "HO2D_ERR_NONFINITE"}
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_KRYLOV = 0, 1, 2
 BC_POISSON, BC_NORMAL_VEL, BC_PARL_VEL, BC_DIFFUSION, BC_VORTICITY, BC_VELOCITY_JUMP, BC_ADVECTION = range(7)
 FIELD_VORTICITY, FIELD_STREAMFUNCTION, FIELD_RHS_DIFFUSIVE, FIELD_RHS_ADVECTIVE, FIELD_STAGE_K, FIELD_JACOBIAN = range(6)
 

@@ -33,8 +33,9 @@ enum ho2d_status {
 };
 
 enum ho2d_precision {
-    HO2D_FP64 = 0,  /* every device array and operation in double precision */
-    HO2D_MIXED = 1  /* FP32 FR residual and Krylov, FP64 refinement residual and RK accumulation */
+    HO2D_FP64 = 0,          /* every device array and operation in double precision */
+    HO2D_MIXED = 1,         /* FP32 FR residual and Krylov, FP64 refinement residual and RK accumulation */
+    HO2D_MIXED_KRYLOV = 2   /* FP64 FR residual; FP32 Krylov inside FP64 refinement of the Poisson solve */
 };
 
 /* which boundary-edge array [N_eb][Knod] ho2d_get_boundary / ho2d_set_boundary address */
@@ -104,7 +105,8 @@ int ho2d_set_boundary(ho2d_solver* handle, int32_t which, int32_t len, const dou
  * len = 2*N_el*Knod*Knod. */
 int ho2d_get_solution_points(ho2d_solver* handle, int32_t len, double* buf);
 
-/* HO2D_FP64 (default) or HO2D_MIXED; may be called before or after ho2d_setup. */
+/* HO2D_FP64 (default), HO2D_MIXED or HO2D_MIXED_KRYLOV; may be called before or after
+ * ho2d_setup. */
 int ho2d_set_precision(ho2d_solver* handle, int32_t mode);
 /* Poisson solve controls: relative tolerance on ||b - A psi|| / ||b|| (default 1e-12)
  * and iteration cap (default 500). */

@@ -105,3 +105,14 @@ def test_valid_mesh_reaches_device_setup(tmp_path):
     path = meshgen.make_case("cyl4x8", str(tmp_path), steps=1)
     code, msg = _setup_code(path)
     assert code in (0, 5), msg
+
+
+def test_precision_modes():
+    lib, h = _handle()
+    try:
+        for mode in (capi.FP64, capi.MIXED, capi.MIXED_KRYLOV):
+            assert lib.ho2d_set_precision(h, mode) == capi.HO2D_OK
+        assert lib.ho2d_set_precision(h, 3) == 1  # HO2D_ERR_ARG
+        assert b"HO2D_MIXED_KRYLOV" in lib.ho2d_last_error(h)
+    finally:
+        lib.ho2d_destroy(h)

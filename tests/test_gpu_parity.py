@@ -8,7 +8,7 @@ import pytest
 
 from conftest import GOLDEN, GOLDEN_CASES
 
-from ho2d import FP64, MIXED, HO_2D, capi, meshgen
+from ho2d import FP64, MIXED, MIXED_KRYLOV, HO_2D, capi, meshgen
 
 import ho2d_oracle as O
 
@@ -138,6 +138,20 @@ def test_mixed_precision_close_to_fp64(tmp_path):
     assert err < 1e-4, err
     it, res = mix.poisson_stats()
     assert res < 1e-11
+
+
+def test_mixed_krylov_matches_fp64(tmp_path):
+    # FP64 FR stage with the FP32 Krylov inside FP64 refinement: the only difference from
+    # FP64 is the Poisson solve's round-off below its 1e-12 tolerance
+    inp = meshgen.make_case("cavityj8", str(tmp_path), knod=4, steps=5)
+    ref = solver_for(inp, tol=1e-12)
+    mix = solver_for(inp, precision=MIXED_KRYLOV, tol=1e-12)
+    ref.solve_advection_diffusion(20)
+    mix.solve_advection_diffusion(20)
+    w64, w32 = ref.get_vorticity(), mix.get_vorticity()
+    err = np.linalg.norm(w32 - w64) / np.linalg.norm(w64)
+    assert err < 1e-9, err
+    assert mix.poisson_stats()[1] < 1e-11
 
 
 def test_nonfinite_vorticity_rejected(tmp_path):
