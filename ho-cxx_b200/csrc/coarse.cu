@@ -30,8 +30,8 @@ constexpr int kChunks = 4;    // row chunks of G entries loaded before any is us
 // acc[r] += A_row[r] . x over the row chunks of one lane. All kRowBatch x kChunks loads
 // of a step are issued before the first gather, so a lane keeps that many L2 requests in
 // flight instead of waiting once per chunk.
-template <typename T>
-__device__ __forceinline__ void ell_accumulate(const DevEll<T>& A, const T* x, const int (&row)[kRowBatch],
+template <typename T, typename X>
+__device__ __forceinline__ void ell_accumulate(const DevEll<T>& A, const X& x, const int (&row)[kRowBatch],
                                                const bool (&ok)[kRowBatch], int G, int sub, T (&acc)[kRowBatch]) {
     const int w = A.w;
     const int nch = (w + G - 1) / G;
@@ -56,12 +56,12 @@ __device__ __forceinline__ void ell_accumulate(const DevEll<T>& A, const T* x, c
 }
 
 // grid-wide down (f_next = M f) or up (u = S f + Q u_next): G lanes per row, the group's
-// lanes combine their partial sums with an xor-shuffle tree
-template <typename T>
-__global__ void __launch_bounds__(256) k_coarse_rows(DevEll<T> A, const T* __restrict__ xa, DevEll<T> B,
-                                                      const T* __restrict__ xb, int has_b, T* __restrict__ y,
-                                                      const KrylovScalars* sc, int mode) {
-    const bool skip = pc_skip(sc, mode);  // read early: the round trip overlaps the loads
+// lanes combine their partial sums with an xor-shuffle tree. XA is a plain vector, or
+// (the level-0 restriction) the right-hand side formed from the element sums.
+template <typename T, typename XA>
+__global__ void __launch_bounds__(256) k_coarse_rows(DevEll<T> A, XA xa, DevEll<T> B, const T* __restrict__ xb,
+                                                      int has_b, T* __restrict__ y, const KrylovScalars* sc) {
+    const bool skip = sc->done;  // read early: the round trip overlaps the loads
     const int G = A.g;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int group = gid / G, sub = gid % G, ngroups = (int)(gridDim.x * blockDim.x) / G;
@@ -111,11 +111,10 @@ constexpr int kGemvUnroll = 8;
 // flight; f is read in the same pieces (its buffer is zero-padded past n).
 template <typename T>
 __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv(DevEll<T> W, const T* __restrict__ f,
-                                                                 T* __restrict__ u, const KrylovScalars* sc,
-                                                                 int mode) {
+                                                                 T* __restrict__ u, const KrylovScalars* sc) {
     using V = Vec16<T>;
     using VT = typename V::type;
-    const bool skip = pc_skip(sc, mode);
+    const bool skip = sc->done;
     const int lane = threadIdx.x & 31;
     const int row = blockIdx.x * kGemvWarps + (threadIdx.x >> 5);
     if (row >= W.n) return;
@@ -142,6 +141,30 @@ __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv(DevEll<T> W, con
     if (lane == 0 && !skip) u[row] = acc;
 }
 
+// u0 = W f0 when the P0 level itself is the dense one (small meshes): f0 is formed from
+// the element sums as it is read, one warp per row, scalar loads
+template <typename T>
+__global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv_f0(DevEll<T> W, BicgVectors<T> v,
+                                                                    T* __restrict__ u, const KrylovScalars* sc,
+                                                                    int mode) {
+    const bool skip = sc->done;
+    const F0<T> f = f0_of(v, sc, mode);
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * kGemvWarps + (threadIdx.x >> 5);
+    if (row >= W.n) return;
+    const T* wr = W.val + (size_t)row * W.w;
+    T acc = T(0);
+    for (int k = lane; k < W.n; k += 32) acc += __ldg(wr + k) * f[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0 && !skip) u[row] = acc;
+}
+
+// level-0 restriction with the right-hand side formed from the element sums
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_rows_f0(DevEll<T> M, BicgVectors<T> v, T* __restrict__ y,
+                                                         const KrylovScalars* sc, int mode);
+
 template <typename T>
 unsigned rows_grid(const DevEll<T>& A) {
     const long long lanes = (long long)A.n * A.g;
@@ -150,21 +173,57 @@ unsigned rows_grid(const DevEll<T>& A) {
     return (unsigned)(blocks < 1 ? 1 : blocks);
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_rows_f0(DevEll<T> M, BicgVectors<T> v, T* __restrict__ y,
+                                                         const KrylovScalars* sc, int mode) {
+    // the same row loop as k_coarse_rows, gathering f0 = a + cb b + cc c
+    const bool skip = sc->done;
+    const F0<T> xa = f0_of(v, sc, mode);
+    const int G = M.g;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int group = gid / G, sub = gid % G, ngroups = (int)(gridDim.x * blockDim.x) / G;
+    const int iters = (M.n + ngroups - 1) / ngroups;
+    for (int it = 0; it < iters; it += kRowBatch) {
+        T acc[kRowBatch];
+        int row[kRowBatch];
+        bool ok[kRowBatch];
+#pragma unroll
+        for (int r = 0; r < kRowBatch; ++r) {
+            acc[r] = T(0);
+            row[r] = group + (it + r) * ngroups;
+            ok[r] = it + r < iters && row[r] < M.n;
+        }
+        ell_accumulate<T>(M, xa, row, ok, G, sub, acc);
+#pragma unroll
+        for (int r = 0; r < kRowBatch; ++r) {
+            T a = acc[r];
+            for (int off = G >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+            if (sub == 0 && ok[r] && !skip) y[row[r]] = a;
+        }
+    }
+}
+
 }  // namespace
 
 template <typename T>
-cudaError_t coarse_cycle(const Precond<T>& pc, const KrylovScalars* sc, int mode, cudaStream_t s) {
+cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const KrylovScalars* sc, int mode,
+                         cudaStream_t s) {
     const int d = pc.nlev - 1;
-    for (int l = 0; l < d; ++l) {
-        const CoarseLevel<T>& L = pc.lev[l];
-        k_coarse_rows<T><<<rows_grid(L.M), 256, 0, s>>>(L.M, L.f, DevEll<T>(), nullptr, 0, pc.lev[l + 1].f, sc,
-                                                         mode);
-    }
     const unsigned gd = (unsigned)((pc.dense.n + kGemvWarps - 1) / kGemvWarps);
-    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc, mode);
+    if (d == 0) {
+        k_dense_gemv_f0<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, v, pc.lev[0].u, sc, mode);
+        return cudaGetLastError();
+    }
+    k_coarse_rows_f0<T><<<rows_grid(pc.lev[0].M), 256, 0, s>>>(pc.lev[0].M, v, pc.lev[1].f, sc, mode);
+    for (int l = 1; l < d; ++l) {
+        const CoarseLevel<T>& L = pc.lev[l];
+        k_coarse_rows<T, const T*><<<rows_grid(L.M), 256, 0, s>>>(L.M, L.f, DevEll<T>(), nullptr, 0,
+                                                                   pc.lev[l + 1].f, sc);
+    }
+    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc);
     for (int l = d - 1; l >= 1; --l) {
         const CoarseLevel<T>& L = pc.lev[l];
-        k_coarse_rows<T><<<rows_grid(L.S), 256, 0, s>>>(L.S, L.f, L.Q, pc.lev[l + 1].u, 1, L.u, sc, mode);
+        k_coarse_rows<T, const T*><<<rows_grid(L.S), 256, 0, s>>>(L.S, L.f, L.Q, pc.lev[l + 1].u, 1, L.u, sc);
     }
     return cudaGetLastError();
 }
@@ -184,14 +243,14 @@ CoarseOut<T> coarse_out(const Precond<T>& pc) {
     } else {
         c.S = pc.lev[0].S;
         c.Q = pc.lev[0].Q;
-        c.f0 = pc.lev[0].f;
         c.u1 = pc.lev[1].u;
     }
     return c;
 }
 
 #define HO2D_INSTANTIATE_COARSE(T)                                                                   \
-    template cudaError_t coarse_cycle<T>(const Precond<T>&, const KrylovScalars*, int, cudaStream_t); \
+    template cudaError_t coarse_cycle<T>(const Precond<T>&, const BicgVectors<T>&, const KrylovScalars*, int,  \
+                                         cudaStream_t);                                                      \
     template int coarse_launches<T>(const Precond<T>&);                                              \
     template CoarseOut<T> coarse_out<T>(const Precond<T>&);
 

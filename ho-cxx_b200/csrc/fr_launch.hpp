@@ -96,7 +96,42 @@ struct BicgVectors {
     const T* b;
     T *tv, *tg;    // incoming face traces of the operand of the next operator application
     T *xtv, *xtg;  // incoming face traces of x (initial residual)
+    // element sums (N entries, zero-padded) of r, of v, and of p in two buffers that
+    // alternate with the iteration count: the coarse right-hand sides P^T p and P^T s are
+    // linear combinations of them, formed wherever they are read
+    T *er, *ev, *ep[2];
 };
+
+// The level-0 coarse right-hand side of one preconditioner application, formed where it
+// is read: f0[e] = a[e] + cb b[e] + cc c[e].
+//   mode 0 (p = r + beta (p - omega v)):  f0 = er + beta ep_prev - beta omega ev
+//                                          (= er on the first iteration)
+//   mode 1 (s = r - alpha v):             f0 = er - alpha ev
+template <typename T>
+struct F0 {
+    const T *a, *b, *c;
+    T cb, cc;
+    __device__ __forceinline__ T operator[](int e) const { return a[e] + cb * b[e] + cc * c[e]; }
+};
+
+template <typename T>
+__device__ __forceinline__ F0<T> f0_of(const BicgVectors<T>& v, const KrylovScalars* sc, int mode) {
+    F0<T> f;
+    f.a = v.er;
+    f.b = f.c = v.er;  // zero weight unless set below
+    f.cb = f.cc = T(0);
+    if (mode == 1) {
+        f.b = v.ev;
+        f.cb = T(-sc->alpha);
+    } else if (sc->it > 0) {
+        const double beta = (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
+        f.b = v.ep[sc->it & 1];
+        f.c = v.ev;
+        f.cb = T(beta);
+        f.cc = T(-beta * sc->omega);
+    }
+    return f;
+}
 
 struct ReduceScratch {
     double* partials;    // [4 * max_blocks]
@@ -136,18 +171,20 @@ struct Precond {
 };
 
 // What the fine smoothing step needs of the coarse result: u0 directly (one level), or
-// the level-0 up step u0 = S0 f0 + Q0 u1 evaluated per element where it is used.
+// the level-0 up step u0 = S0 f0 + Q0 u1 evaluated per element where it is used (f0 is
+// formed from the element sums, F0 above).
 template <typename T>
 struct CoarseOut {
     const T* u0 = nullptr;
     DevEll<T> S, Q;
-    const T* f0 = nullptr;
     const T* u1 = nullptr;
 };
 
-// enqueues the coarse part of one preconditioner application on f_0 = pc.lev[0].f
+// enqueues the coarse part of one preconditioner application (mode 0: on P^T p, mode 1:
+// on P^T s, both formed from the element sums in v)
 template <typename T>
-cudaError_t coarse_cycle(const Precond<T>& pc, const KrylovScalars* sc, int mode, cudaStream_t s);
+cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const KrylovScalars* sc, int mode,
+                         cudaStream_t s);
 template <typename T>
 int coarse_launches(const Precond<T>& pc);
 template <typename T>

@@ -265,6 +265,22 @@ __device__ __forceinline__ T block_apply(const T* __restrict__ dinv, const T* sy
     return acc;
 }
 
+// Element sums of a per-point value: every thread of element le stores its value, then
+// thread ij == 0 of each element adds the K^2 values in a fixed order. Collective.
+template <int K, typename T>
+__device__ __forceinline__ void element_sum(T (&buf)[Shape<K>::EPB][Shape<K>::K2], T val, bool active, int le, int ij,
+                                            int el, T* out) {
+    __syncthreads();  // buf may still be read by the phase before
+    if (active) buf[le][ij] = val;
+    __syncthreads();
+    if (active && ij == 0) {
+        T sum = T(0);
+#pragma unroll
+        for (int q = 0; q < Shape<K>::K2; ++q) sum += buf[le][q];
+        out[el] = sum;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- fine-level kernels
@@ -298,15 +314,17 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgV
     const bool active = le < S::EPB && el < op.g.N;
     const T y = mf_apply<K, T>(op, v.x, v.xtv, v.xtg, sm, active, le, el, ij);
     double part[2] = {0.0, 0.0};
+    T r = T(0);
     if (active) {
         const int p = el * S::K2 + ij;
         const T bb = v.b[p];
-        const T r = bb - y;
+        r = bb - y;
         v.r[p] = r;
         v.rhat[p] = r;
         part[0] = double(r) * double(r);
         part[1] = double(bb) * double(bb);
     }
+    element_sum<K, T>(sm.a, r, active, le, ij, el, v.er);
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         KrylovScalars* sc = rs.sc;
@@ -337,71 +355,11 @@ __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
 // says, so the flag's round trip overlaps the data loads.
 constexpr int kVecTiles = 2;
 
-// p = r + beta (p - omega v) (= r on the first iteration); then either ph = D^{-1} p with
-// its traces (block-Jacobi) or the element sums of p (two-level: coarse right-hand side)
-template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_pupdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
-                                                                   T* rc) {
-    using S = Shape<K>;
-    constexpr int NT = kVecTiles;
-    const KrylovScalars* sc = rs.sc;
-    __shared__ T sp[NT][S::EPB][S::K2], sz[S::EPB][S::K2];
-    __shared__ DevBases<T> sbas;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    int el[NT], p[NT];
-    bool act[NT];
-    T r[NT], pp[NT], vv[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
-        act[t] = le < S::EPB && el[t] < op.g.N;
-        p[t] = el[t] * S::K2 + ij;
-        r[t] = act[t] ? v.r[p[t]] : T(0);
-        pp[t] = act[t] ? v.p[p[t]] : T(0);
-        vv[t] = act[t] ? v.v[p[t]] : T(0);
-    }
-    if (sc->done) return;
-    const bool first = sc->it == 0;
-    const double beta = first ? 0.0 : (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
-    const T omega = T(sc->omega);
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        const T pv = first ? r[t] : r[t] + T(beta) * (pp[t] - omega * vv[t]);
-        if (act[t]) v.p[p[t]] = pv;
-        if (le < S::EPB) sp[t][le][ij] = pv;
-    }
-    __syncthreads();
-    if (rc) {
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-            if (act[t] && ij == 0) {
-                T sum = T(0);
-#pragma unroll
-                for (int q = 0; q < S::K2; ++q) sum += sp[t][le][q];
-                rc[el[t]] = sum;
-            }
-        return;
-    }
-    stage_bases(sbas, op.b);
-    for (int t = 0; t < NT; ++t) {
-        TraceDst<K> td;
-        td.load(op.g.scat, act[t], el[t], ij);
-        if (act[t]) {
-            const T z = block_apply<K, T>(op.dinv, sp[t][le], el[t], ij);
-            v.ph[p[t]] = z;
-            sz[le][ij] = z;
-        }
-        __syncthreads();
-        emit_traces<K, T>(sz[act[t] ? le : 0], sbas, td, v.tv, v.tg, ij);
-        __syncthreads();
-    }
-}
-
 // Part `part` (0..4) of u0 at element c = S0_c . f0 + Q0_c . u1 (a row of the level-0
 // up step): the row entries part, part + 5, ... The first two of each row are loaded
 // before any gather, so a part costs two dependent rounds of loads.
 template <typename T>
-__device__ __forceinline__ T up0_part(const CoarseOut<T>& co, int c, int part) {
+__device__ __forceinline__ T up0_part(const CoarseOut<T>& co, const F0<T>& f0, int c, int part) {
     const size_t rs = (size_t)c * co.S.w, rq = (size_t)c * co.Q.w;
     T sv[2], qv[2];
     int sj[2], qj[2];
@@ -414,8 +372,8 @@ __device__ __forceinline__ T up0_part(const CoarseOut<T>& co, int c, int part) {
         qv[m] = inq ? co.Q.val[rq + k] : T(0);
         qj[m] = inq ? co.Q.col[rq + k] : 0;
     }
-    T u = sv[0] * co.f0[sj[0]] + qv[0] * co.u1[qj[0]] + sv[1] * co.f0[sj[1]] + qv[1] * co.u1[qj[1]];
-    for (int k = part + 10; k < co.S.w; k += 5) u += co.S.val[rs + k] * co.f0[co.S.col[rs + k]];
+    T u = sv[0] * f0[sj[0]] + qv[0] * co.u1[qj[0]] + sv[1] * f0[sj[1]] + qv[1] * co.u1[qj[1]];
+    for (int k = part + 10; k < co.S.w; k += 5) u += co.S.val[rs + k] * f0[co.S.col[rs + k]];
     for (int k = part + 10; k < co.Q.w; k += 5) u += co.Q.val[rq + k] * co.u1[co.Q.col[rq + k]];
     return u;
 }
@@ -429,24 +387,27 @@ struct PostStage {
     static constexpr bool kOn = kBytes <= 32768;
 };
 
-// two-level smoothing step: z = e + w D^{-1} (f - A e), e = P u0 element-wise constant;
-// writes z and its face traces. u0 of the element and of its four face neighbours comes
-// either straight from the coarse cycle (one-level hierarchy) or from the level-0 up
-// step u0 = S0 f0 + Q0 u1, evaluated here as 25 partial sums (five per slot) spread over
-// the element's threads. Everything that
-// does not depend on u0 starts first: the CTA's inverse blocks are copied into shared
-// memory asynchronously (cp.async, 16-byte pieces of the 16-byte-aligned superset of the
-// blocks; the buffer is padded past its end) and the block row sums and f are loaded, so
-// all of it overlaps the up step's dependent loads.
+// Preconditioner application, with the BiCGSTAB vector update that produces its operand:
+//   mode 0:  p = r + beta (p - omega v)  (p = r on the first iteration),  f = p -> ph
+//   mode 1:  s = r - alpha v, ||s||^2 (s_exit test),                      f = s -> sh
+// then the two-level smoothing step z = e + w D^{-1} (f - A e), e = P u0 element-wise
+// constant, with z's face traces. u0 of the element and of its four face neighbours comes
+// straight from the coarse cycle (one-level hierarchy), or from the level-0 up step
+// u0 = S0 f0 + Q0 u1 evaluated here as 25 partial sums (five per slot) spread over the
+// element's threads, or is zero (block-Jacobi, no coarse level). Mode 0 also stores the
+// element sums of the new p for the next iteration. Everything that does not depend on u0
+// starts first: the CTA's inverse blocks are copied into shared memory asynchronously
+// (cp.async, 16-byte pieces of the 16-byte-aligned superset of the blocks; the buffer is
+// padded past its end), and the block row sums and the vectors are loaded, so all of it
+// overlaps the up step's dependent loads.
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const T* __restrict__ f, CoarseOut<T> co,
-                                                                T* __restrict__ z, T* __restrict__ tv,
-                                                                T* __restrict__ tg, double w, const KrylovScalars* sc,
-                                                                int mode) {
+__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
+                                                                int has_coarse, double w, ReduceScratch rs, int mode) {
     using S = Shape<K>;
     using PS = PostStage<K, T>;
     constexpr int K2 = S::K2;
-    const bool skip = pc_skip(sc, mode);  // read early: the round trip overlaps the loads below
+    KrylovScalars* sc = rs.sc;
+    const int done = sc->done;  // uniform; read early so the round trip overlaps the loads
     __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25];
     __shared__ DevBases<T> sbas;
     __shared__ __align__(16) unsigned char sd_raw[PS::kOn ? PS::kBytes : 16];
@@ -468,25 +429,45 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const
     }
     TraceDst<K> td;
     td.load(op.g.scat, active, el, ij);
-    T rsum[5], fp = T(0);
+    T rsum[5], rr = T(0), pp = T(0), vv = T(0);
     if (active) {
 #pragma unroll
         for (int s = 0; s < 5; ++s) rsum[s] = op.rowsum[((size_t)el * 5 + s) * K2 + ij];
-        fp = f[p];
+        rr = v.r[p];
+        vv = v.v[p];
+        if (mode == 0) pp = v.p[p];
     }
     stage_bases(sbas, op.b);
+    const F0<T> f0 = f0_of(v, sc, mode);
     // u0 of block slot s (element bcol[5 el + s]) as five partial sums pu[s][part]
     if (active)
         for (int t = ij; t < 25; t += K2) {
             const int slot = t / 5, part = t % 5;
             const int c = op.bcol[el * 5 + slot];
             T u = T(0);
-            if (c >= 0) u = co.u0 ? (part == 0 ? co.u0[c] : T(0)) : up0_part(co, c, part);
+            if (c >= 0 && has_coarse) u = co.u0 ? (part == 0 ? co.u0[c] : T(0)) : up0_part(co, f0, c, part);
             pu[le][t] = u;
         }
+    if (mode == 0 && has_coarse && active && ij == 0) v.ep[(sc->it + 1) & 1][el] = f0[el];
+    // the operand: p or s
+    T f;
+    if (mode == 0) {
+        if (sc->it == 0) {
+            f = rr;
+        } else {
+            const double beta = (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
+            f = rr + T(beta) * (pp - T(sc->omega) * vv);
+        }
+    } else {
+        f = rr - T(sc->alpha) * vv;
+    }
+    if (active && !done) {
+        if (mode == 0) v.p[p] = f;
+        else v.s[p] = f;
+    }
     if constexpr (PS::kOn) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    if (skip) return;
+    if (done) return;
     T u_self = T(0);
     if (active) {
         T ae = T(0);
@@ -496,9 +477,10 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const
             ae += rsum[s] * us;
             if (s == 0) u_self = us;
         }
-        sr[le][ij] = fp - ae;
+        sr[le][ij] = f - ae;
     }
     __syncthreads();
+    T* z = mode == 0 ? v.ph : v.sh;
     if (active) {
         T acc = T(0);
 #pragma unroll
@@ -508,7 +490,15 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, const
         sz[le][ij] = zz;
     }
     __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], sbas, td, tv, tg, ij);
+    emit_traces<K, T>(sz[active ? le : 0], sbas, td, v.tv, v.tg, ij);
+    if (mode == 1) {
+        double part[1] = {active ? double(f) * double(f) : 0.0};
+        double out[1];
+        if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
+            sc->snorm2 = out[0];
+            sc->s_exit = out[0] <= sc->eps2;
+        }
+    }
 }
 
 // v = A ph; alpha = rho / (rhat, v)
@@ -531,6 +521,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVect
         v.v[p] = y;
         part[0] = double(v.rhat[p]) * double(y);
     }
+    element_sum<K, T>(sm.a, y, active, le, ij, el, v.ev);
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         if (out[0] == 0.0 || sc->rho == 0.0) {
@@ -539,71 +530,6 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVect
         } else {
             sc->alpha = sc->rho / out[0];
         }
-    }
-}
-
-// s = r - alpha v; ||s||^2; then sh = D^{-1} s with traces, or the element sums of s
-template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_supdate(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs,
-                                                                   T* rc) {
-    using S = Shape<K>;
-    constexpr int NT = kVecTiles;
-    KrylovScalars* sc = rs.sc;
-    __shared__ T sp[NT][S::EPB][S::K2], sz[S::EPB][S::K2];
-    __shared__ DevBases<T> sbas;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    int el[NT], p[NT];
-    bool act[NT];
-    T r[NT], vv[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
-        act[t] = le < S::EPB && el[t] < op.g.N;
-        p[t] = el[t] * S::K2 + ij;
-        r[t] = act[t] ? v.r[p[t]] : T(0);
-        vv[t] = act[t] ? v.v[p[t]] : T(0);
-    }
-    if (sc->done) return;
-    const T alpha = T(sc->alpha);
-    double part[1] = {0.0};
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        const T sv = r[t] - alpha * vv[t];
-        if (act[t]) {
-            v.s[p[t]] = sv;
-            part[0] += double(sv) * double(sv);
-        }
-        if (le < S::EPB) sp[t][le][ij] = sv;
-    }
-    __syncthreads();
-    if (rc) {
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-            if (act[t] && ij == 0) {
-                T sum = T(0);
-#pragma unroll
-                for (int q = 0; q < S::K2; ++q) sum += sp[t][le][q];
-                rc[el[t]] = sum;
-            }
-    } else {
-        stage_bases(sbas, op.b);
-        for (int t = 0; t < NT; ++t) {
-            TraceDst<K> td;
-            td.load(op.g.scat, act[t], el[t], ij);
-            if (act[t]) {
-                const T z = block_apply<K, T>(op.dinv, sp[t][le], el[t], ij);
-                v.sh[p[t]] = z;
-                sz[le][ij] = z;
-            }
-            __syncthreads();
-            emit_traces<K, T>(sz[act[t] ? le : 0], sbas, td, v.tv, v.tg, ij);
-            __syncthreads();
-        }
-    }
-    double out[1];
-    if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
-        sc->snorm2 = out[0];
-        sc->s_exit = out[0] <= sc->eps2;
     }
 }
 
@@ -631,22 +557,30 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_t(MfOp<T> op, BicgVect
         sc->omega = out[1] > 0.0 ? out[0] / out[1] : 0.0;
 }
 
-// x += alpha ph + omega sh; r = s - omega t; ||r||^2, (rhat, r); convergence test
+// x += alpha ph + omega sh; r = s - omega t; ||r||^2, (rhat, r); element sums of r;
+// convergence test. After an s-exit (||s|| already below tolerance) only x += alpha ph.
+// The last CTA to finish ends the iteration: it updates the scalars, sets `done`, and
+// inside a captured solve sets the condition of the graph's while node (iterate while
+// not done). Every CTA reads `done` and `s_exit` before any CTA arrives at the counter,
+// so the last CTA may change them. Every body execution either increments `it` (capped at
+// max_iter) or finds `done` set and clears the condition, so the device loop always ends.
 template <int K, typename T>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
-                                                                  int max_iter) {
+                                                                  int max_iter, cudaGraphConditionalHandle h,
+                                                                  int has_handle) {
     using S = Shape<K>;
     constexpr int NT = kVecTiles;
     KrylovScalars* sc = rs.sc;
+    __shared__ T sr[S::EPB][S::K2];
     const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    int p[NT];
+    int p[NT], el[NT];
     bool act[NT];
     T x[NT], ph[NT], sh[NT], sv[NT], tv[NT], rh[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
-        const int el = (blockIdx.x + t * gridDim.x) * S::EPB + le;
-        act[t] = le < S::EPB && el < N;
-        p[t] = el * S::K2 + ij;
+        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
+        act[t] = le < S::EPB && el[t] < N;
+        p[t] = el[t] * S::K2 + ij;
         x[t] = act[t] ? v.x[p[t]] : T(0);
         ph[t] = act[t] ? v.ph[p[t]] : T(0);
         sh[t] = act[t] ? v.sh[p[t]] : T(0);
@@ -654,51 +588,42 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVect
         tv[t] = act[t] ? v.t[p[t]] : T(0);
         rh[t] = act[t] ? v.rhat[p[t]] : T(0);
     }
-    if (sc->done) return;
-    const T alpha = T(sc->alpha);
-    if (sc->s_exit) {  // ||s|| already below tolerance: x += alpha ph and stop
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-            if (act[t]) v.x[p[t]] = x[t] + alpha * ph[t];
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            sc->rnorm2 = sc->snorm2;
-            sc->it += 1;
-        }
+    if (sc->done) {  // the solve ended earlier in this body (breakdown)
+        if (has_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
         return;
     }
+    const T alpha = T(sc->alpha);
+    const bool s_exit = sc->s_exit;
     const double omega = sc->omega;
     double part[2] = {0.0, 0.0};
 #pragma unroll
-    for (int t = 0; t < NT; ++t)
-        if (act[t]) {
+    for (int t = 0; t < NT; ++t) {
+        T r = T(0);
+        if (s_exit) {
+            if (act[t]) v.x[p[t]] = x[t] + alpha * ph[t];
+        } else if (act[t]) {
             v.x[p[t]] = x[t] + (alpha * ph[t] + T(omega) * sh[t]);
-            const T r = sv[t] - T(omega) * tv[t];
+            r = sv[t] - T(omega) * tv[t];
             v.r[p[t]] = r;
             part[0] += double(r) * double(r);
             part[1] += double(rh[t]) * double(r);
         }
+        if (!s_exit) element_sum<K, T>(sr, r, act[t], le, ij, el[t], v.er);
+    }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
-        sc->rnorm2 = out[0];
-        sc->rho_old = sc->rho;
-        sc->rho = out[1];
         sc->it += 1;
-        if (out[0] <= sc->eps2 || sc->it >= max_iter || omega == 0.0) sc->done = 1;
+        if (s_exit) {
+            sc->rnorm2 = sc->snorm2;
+            sc->done = 1;
+        } else {
+            sc->rnorm2 = out[0];
+            sc->rho_old = sc->rho;
+            sc->rho = out[1];
+            if (out[0] <= sc->eps2 || sc->it >= max_iter || omega == 0.0) sc->done = 1;
+        }
+        if (has_handle) cudaGraphSetConditional(h, sc->done ? 0u : 1u);
     }
-}
-
-// ends the solve after an s-exit iteration (a separate launch: every CTA of k_xr_update
-// has read s_exit before done changes)
-__global__ void k_finish_s_exit(KrylovScalars* sc) {
-    if (!sc->done && sc->s_exit) sc->done = 1;
-}
-
-// same, and sets the condition of the graph's while node: iterate while not done. Every
-// body execution either increments `it` (capped at max_iter by k_xr_update) or finds
-// `done` set, so the device-side loop always ends.
-__global__ void k_finish_loop(KrylovScalars* sc, cudaGraphConditionalHandle h) {
-    if (!sc->done && sc->s_exit) sc->done = 1;
-    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
 }
 
 __global__ void k_set_loop(const KrylovScalars* sc, cudaGraphConditionalHandle h) {
@@ -791,41 +716,36 @@ cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const Reduce
     return cudaGetLastError();
 }
 
+// One BiCGSTAB iteration: [coarse cycle on P^T p] -> p update + smoothing (ph) -> v = A ph
+// -> [coarse cycle on P^T s] -> s update + smoothing (sh) -> t = A sh -> x, r update and
+// loop control.
 template <int K, typename T>
 static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
-                           const Precond<T>& pc, cudaStream_t s) {
+                           const Precond<T>& pc, cudaGraphConditionalHandle h, int has_handle, cudaStream_t s) {
     const int N = op.g.N;
     const unsigned g = kgrid<K>(N);
     constexpr int th = Shape<K>::THREADS;
-    const bool mg = pc.nlev > 0;
-    T* rc = mg ? pc.lev[0].f : nullptr;
+    const int mg = pc.nlev > 0;
+    const CoarseOut<T> co = mg ? coarse_out(pc) : CoarseOut<T>();
     const unsigned gv = (g + kVecTiles - 1) / kVecTiles;
-    k_mf_pupdate<K, T><<<gv, th, 0, s>>>(op, v, rs, rc);
-    if (mg) {
-        coarse_cycle<T>(pc, rs.sc, 0, s);
-        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.p, coarse_out(pc), v.ph, v.tv, v.tg, pc.omega, rs.sc, 0);
-    }
+    if (mg) coarse_cycle<T>(pc, v, rs.sc, 0, s);
+    k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, 0);
     k_mf_v<K, T><<<g, th, 0, s>>>(op, v, rs);
-    k_mf_supdate<K, T><<<gv, th, 0, s>>>(op, v, rs, rc);
-    if (mg) {
-        coarse_cycle<T>(pc, rs.sc, 1, s);
-        k_mf_post<K, T><<<g, th, 0, s>>>(op, v.s, coarse_out(pc), v.sh, v.tv, v.tg, pc.omega, rs.sc, 1);
-    }
+    if (mg) coarse_cycle<T>(pc, v, rs.sc, 1, s);
+    k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, 1);
     k_mf_t<K, T><<<g, th, 0, s>>>(op, v, rs);
-    k_xr_update<K, T><<<gv, th, 0, s>>>(N, v, rs, max_iter);
+    k_xr_update<K, T><<<gv, th, 0, s>>>(N, v, rs, max_iter, h, has_handle);
 }
 
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc) {
-    if (pc.nlev == 0) return 6;
-    return 6 + 2 * (coarse_launches(pc) + 1);
+    return 5 + 2 * coarse_launches(pc);
 }
 
 template <typename T>
 cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                              const Precond<T>& pc, cudaStream_t s) {
-    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, s)));
-    k_finish_s_exit<<<1, 1, 0, s>>>(rs.sc);
+    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, cudaGraphConditionalHandle(), 0, s)));
     return cudaGetLastError();
 }
 
@@ -864,8 +784,7 @@ cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, con
     if ((e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
         cudaSuccess)
         return e;
-    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, s)));
-    k_finish_loop<<<1, 1, 0, s>>>(rs.sc, h);
+    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, h, 1, s)));
     if ((e = cudaStreamEndCapture(s, &body)) != cudaSuccess) return e;
     *graph_out = g;
     return cudaGetLastError();

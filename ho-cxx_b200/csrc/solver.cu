@@ -76,6 +76,7 @@ struct DeviceState {
     DeviceBuffer pg64[8], pg32[8], pcode, pscat;
     std::vector<double> pg_host[8];  // kept for the FP32 copies made on demand
     DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
+    DeviceBuffer esum[4];  // element sums of r, v, p (two alternating buffers), N + 4 entries
     DeviceBuffer ktv, ktg, kxtv, kxtg;  // face traces of the Krylov operand and of x
     DeviceBuffer partials, counter, scalars;
     KrylovScalars* h_sc = nullptr;
@@ -281,6 +282,7 @@ Error Solver::setup() {
     for (auto& b : d.pg32) b.reset();
     HO2D_TRY(setup_preconditioner());
     for (auto& b : d.kv) HO2D_CUDA(upload(b, zv), "alloc Krylov");
+    for (auto& b : d.esum) HO2D_CUDA(upload(b, std::vector<double>((size_t)N + 4, 0.0)), "alloc element sums");
     const int mb = krylov_max_blocks(K, N);
     HO2D_CUDA(upload(d.partials, std::vector<double>((size_t)4 * mb, 0.0)), "alloc partials");
     HO2D_CUDA(upload(d.counter, std::vector<unsigned>(1, 0u)), "alloc counter");
@@ -557,6 +559,10 @@ static BicgVectors<T> krylov_vectors(DeviceState& d, T* x, const T* b) {
     v.tg = d.ktg.as<T>();
     v.xtv = d.kxtv.as<T>();
     v.xtg = d.kxtg.as<T>();
+    v.er = d.esum[0].as<T>();
+    v.ev = d.esum[1].as<T>();
+    v.ep[0] = d.esum[2].as<T>();
+    v.ep[1] = d.esum[3].as<T>();
     return v;
 }
 
@@ -594,7 +600,7 @@ Error Solver::poisson_solve() {
             HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
             HO2D_TRY(poll());
             iters = d.h_sc->it;
-            launches_ += 4 + (int64_t)iters * (krylov_launches_per_iteration(pc) + 1);
+            launches_ += 4 + (int64_t)iters * krylov_launches_per_iteration(pc);
             return {0, ""};
         }
         HO2D_CUDA(krylov_init(A, v, rs, d.stream), "krylov init");
