@@ -103,8 +103,8 @@ struct MfShared {
 // own rows (its x, metric coefficients, face coefficients and incoming traces), so all
 // of them are issued in a single round; five barrier phases follow. Collective.
 template <int K, typename T>
-__device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
-                      MfShared<K, T>& sm, bool active, int le, int el, int ij) {
+__device__ T mf_apply_gen(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv,
+                          const T* __restrict__ tg, MfShared<K, T>& sm, bool active, int le, int el, int ij) {
     constexpr int K2 = K * K, NF = 4 * K;
     const PoisGeom<T>& g = op.g;
     const int j = ij / K, i = ij % K;
@@ -222,6 +222,144 @@ __device__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __res
     for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * b.D[d * K + j];
     lap += sm.cg[le][2 * K + i] * b.gR[j * 2 + 0] + sm.cg[le][3 * K + i] * b.gR[j * 2 + 1];
     return lap;
+}
+
+// mf_apply for K >= 4, where every face point has a thread of its own (4K <= K^2): the
+// basis values a thread uses (its row and column of D, its Radau derivatives, the
+// extrapolation weights of its face point) and its face point's own data stay in
+// registers, and shared memory carries only what other threads read. Same arithmetic,
+// same order of operations as mf_apply. Collective.
+template <int K, typename T>
+__device__ T mf_apply_1f(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
+                         MfShared<K, T>& sm, bool active, int le, int el, int ij) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    static_assert(NF <= K2, "one face point per thread");
+    const PoisGeom<T>& g = op.g;
+    const int j = ij / K, i = ij % K;
+    const bool face = active && ij < NF;
+    const int ijp = ij / K, k = ij % K, lr = ijp & 1;  // this thread's face point (if face)
+    T g11 = T(0), g12 = T(0), g22 = T(0);
+    T fa = T(0), fb = T(0), nfa = T(0), nfb = T(0), ntv = T(0), ntg = T(0);
+    if (active) {
+        const int p = el * K2 + ij;
+        sm.x[le][ij] = x[p];
+        g11 = g.G11[p];
+        g12 = g.G12[p];
+        g22 = g.G22[p];
+        if (face) {
+            const int q = el * NF + ij;
+            fa = g.fa[q];
+            fb = g.fb[q];
+            nfa = g.nfa[q];
+            nfb = g.nfb[q];
+            ntv = tv[q];
+            ntg = tg[q];
+            sm.fa[le][ij] = fa;
+        }
+        if (ij < 4) sm.code[le][ij] = g.code[el * 4 + ij];
+    }
+    stage_bases(sm.bas, op.b);
+    __syncthreads();
+    const DevBases<T>& b = sm.bas;
+    T Di[K], Dj[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+        Di[d] = b.D[d * K + i];
+        Dj[d] = b.D[d * K + j];
+    }
+    const T gRi0 = b.gR[i * 2 + 0], gRi1 = b.gR[i * 2 + 1], gRj0 = b.gR[j * 2 + 0], gRj1 = b.gR[j * 2 + 1];
+    const int c = face ? sm.code[le][ijp] : -1;
+    // own trace and common value (interior: average; Dirichlet: zero)
+    T tvv = T(0), tgv = T(0);
+    if (face) {
+        face_trace<K, T>(sm.x[le], b, ij, tvv, tgv);
+        sm.tv[le][ij] = tvv;
+        sm.tg[le][ij] = tgv;
+        sm.com[le][ij] = c >= 0 ? T(0.5) * (tvv + ntv) : T(0);
+    }
+    __syncthreads();
+    // homogeneous Neumann faces: com = Minv r, r_m = -fa_m (tg_m - tv_m g'(+-1))
+    if (face && c <= -2) {
+        const T gp = b.gp[lr];
+        const T* mi = g.minv + ((size_t)(-2 - c) * K + k) * K;
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            const int om = ijp * K + m;
+            acc -= mi[m] * sm.fa[le][om] * (sm.tg[le][om] - sm.tv[le][om] * gp);
+        }
+        sm.com[le][ij] = acc;
+    }
+    __syncthreads();
+    // contravariant gradient and this face point's common normal flux (kept in a register)
+    T cg = T(0);
+    if (active) {
+        T dx = T(0), de = T(0);
+#pragma unroll
+        for (int d = 0; d < K; ++d) {
+            dx += sm.x[le][j * K + d] * Di[d];
+            de += sm.x[le][d * K + i] * Dj[d];
+        }
+        dx += (sm.com[le][0 * K + j] - sm.tv[le][0 * K + j]) * gRi0;
+        dx += (sm.com[le][1 * K + j] - sm.tv[le][1 * K + j]) * gRi1;
+        de += (sm.com[le][2 * K + i] - sm.tv[le][2 * K + i]) * gRj0;
+        de += (sm.com[le][3 * K + i] - sm.tv[le][3 * K + i]) * gRj1;
+        sm.a[le][ij] = dx * g11 + de * g12;
+        sm.b[le][ij] = de * g22 + dx * g12;
+        if (face && c > -2) {
+            const T com = sm.com[le][ij];
+            T cross = T(0);
+#pragma unroll
+            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
+            const T dv = tgv + (com - tvv) * b.gp[lr];
+            const T fl = dv * fa - cross * fb;
+            if (c < 0) {
+                cg = fl;
+            } else {
+                const int nijp = c & 3, rev = c >> 2;
+                const int jn = rev ? K - 1 - k : k;
+                T crn = T(0);
+#pragma unroll
+                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
+                const T dvn = ntg + (com - ntv) * b.gp[nijp & 1];
+                const T fln = dvn * nfa - crn * nfb;
+                cg = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
+            }
+        }
+    }
+    __syncthreads();
+    // flux jump at this face point: common flux minus the interior flux extrapolated to it
+    if (face) {
+        T v = cg;
+        if (ijp < 2) {
+#pragma unroll
+            for (int d = 0; d < K; ++d) v -= sm.a[le][k * K + d] * b.sbb[d * 2 + lr];
+        } else {
+#pragma unroll
+            for (int d = 0; d < K; ++d) v -= sm.b[le][d * K + k] * b.sbb[d * 2 + lr];
+        }
+        sm.cg[le][ij] = v;
+    }
+    __syncthreads();
+    if (!active) return T(0);
+    T lap = T(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) lap += sm.a[le][j * K + d] * Di[d];
+    lap += sm.cg[le][0 * K + j] * gRi0 + sm.cg[le][1 * K + j] * gRi1;
+#pragma unroll
+    for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * Dj[d];
+    lap += sm.cg[le][2 * K + i] * gRj0 + sm.cg[le][3 * K + i] * gRj1;
+    return lap;
+}
+
+// y = A x at (el, ij): the register-resident form when every face point has its own
+// thread (K >= 4), the general form otherwise. Collective.
+template <int K, typename T>
+__device__ __forceinline__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv,
+                                      const T* __restrict__ tg, MfShared<K, T>& sm, bool active, int le, int el,
+                                      int ij) {
+    if constexpr (4 * K <= K * K) return mf_apply_1f<K, T>(op, x, tv, tg, sm, active, le, el, ij);
+    else return mf_apply_gen<K, T>(op, x, tv, tg, sm, active, le, el, ij);
 }
 
 // Scatter destinations of the face points thread ij emits (prefetched at kernel start).
