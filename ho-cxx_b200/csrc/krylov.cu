@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     constexpr int K2 = S::K2;
     KrylovScalars* sc = rs.sc;
     const int done = sc->done;  // uniform; read early so the round trip overlaps the loads
-    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25];
+    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25], ue[S::EPB][5];
     __shared__ DevBases<T> sbas;
     __shared__ __align__(16) unsigned char sd_raw[PS::kOn ? PS::kBytes : 16];
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
@@ -561,8 +561,9 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
         const size_t a0 = b0 & ~size_t(15), a1 = (b1 + 15) & ~size_t(15);
         const char* g = reinterpret_cast<const char*>(op.dinv) + a0;
         const unsigned sb = (unsigned)__cvta_generic_to_shared(sd_raw);
-        for (size_t o = 16 * (size_t)threadIdx.x; o < a1 - a0; o += 16 * (size_t)blockDim.x)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + (unsigned)o), "l"(g + o) : "memory");
+        const unsigned nbytes = (unsigned)(a1 - a0);  // < 32 KB
+        for (unsigned o = 16u * threadIdx.x; o < nbytes; o += 16u * blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + o), "l"(g + o) : "memory");
         dblk = reinterpret_cast<const T*>(sd_raw + (b0 - a0)) + (size_t)le * PS::K4;
     }
     TraceDst<K> td;
@@ -606,15 +607,16 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     if constexpr (PS::kOn) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     if (done) return;
+    // the five slot values, each the sum of its five parts (part 0..4 in order)
+    if (active && ij < 5)
+        ue[le][ij] = pu[le][5 * ij] + pu[le][5 * ij + 1] + pu[le][5 * ij + 2] + pu[le][5 * ij + 3] + pu[le][5 * ij + 4];
+    __syncthreads();
     T u_self = T(0);
     if (active) {
         T ae = T(0);
 #pragma unroll
-        for (int s = 0; s < 5; ++s) {
-            const T us = pu[le][5 * s] + pu[le][5 * s + 1] + pu[le][5 * s + 2] + pu[le][5 * s + 3] + pu[le][5 * s + 4];
-            ae += rsum[s] * us;
-            if (s == 0) u_self = us;
-        }
+        for (int s = 0; s < 5; ++s) ae += rsum[s] * ue[le][s];
+        u_self = ue[le][0];
         sr[le][ij] = f - ae;
     }
     __syncthreads();
