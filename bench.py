@@ -285,6 +285,14 @@ def run_ours(args, rank, world, local, phys):
         w_mixed = solvers["mixed"].get_vorticity()
         w_fp64 = solvers["fp64"].get_vorticity()
         l2 = float(np.linalg.norm(w_mixed - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
+        forces = None
+        try:  # meshes with a body ("object" boundary): FP64 drag and lift of each mode
+            fm, ff = solvers["mixed"].forces(), solvers["fp64"].forces()
+            forces = {"mixed": fm, "fp64": ff,
+                      "rel_diff_mixed_vs_fp64": float(np.hypot(fm[0] - ff[0], fm[1] - ff[1]) /
+                                                      max(np.hypot(*ff), 1e-300))}
+        except ho2d.HO2DError:
+            pass
         w_f32 = solvers["mixed_fp32_stage"].get_vorticity()
         l2_f32 = float(np.linalg.norm(w_f32 - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
         # end to end through the public API with host buffers: H2D of the step's input
@@ -346,6 +354,7 @@ def run_ours(args, rank, world, local, phys):
                     "mixed_over_fp64": m["value"] / f["value"],
                     "l2_rel_vorticity_mixed_vs_fp64": l2,
                     "l2_after_steps": args.warmup + args.steps,
+                    "body_force": forces,
                     "clocks": clocks, "e2e": e2e, "gpu_launches": m["launches"], "roofline": roofline,
                     "cpu_baseline": cb}
             print(json.dumps(line))

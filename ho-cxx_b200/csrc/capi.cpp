@@ -225,6 +225,10 @@ int ho2d_apply_poisson_noalloc(ho2d_solver* h, int32_t len, const double* x_devi
     });
 }
 
+int ho2d_get_forces(ho2d_solver* h, double* fx, double* fy) {
+    return guarded(h, [&]() { return h->s.get_forces(fx, fy); });
+}
+
 int ho2d_last_launch_count(ho2d_solver* h, int64_t* launches) {
     return guarded(h, [&]() -> ho2d::Error {
         if (launches) *launches = h->s.launches();

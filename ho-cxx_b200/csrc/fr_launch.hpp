@@ -213,6 +213,11 @@ template <typename T>
 cudaError_t mf_apply_only(const MfOp<T>& op, const T* x, const T* xtv, const T* xtg, T* y, int reps, cudaStream_t s);
 int krylov_max_blocks(int K, int N);
 
+// out[0..1] = FP64 force on a body from its boundary points' precomputed coefficients
+// (forces.cu): coef [npts][4], idx = index of each point in the boundary arrays
+cudaError_t launch_body_force(int npts, const double* coef, const int* idx, const double* dwdn, const double* wall,
+                              double* out, cudaStream_t s);
+
 // elementwise helpers
 cudaError_t launch_copy_d2f(const double* a, float* b, size_t n, cudaStream_t s);
 cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s);  // x += e

@@ -96,6 +96,7 @@ struct DeviceState {
     SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
     double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
     DeviceBuffer l2flush;               // written between timed steps to evict L2
+    DeviceBuffer fcoef, fidx, fout;     // body-force coefficients, boundary indices, result
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
@@ -276,6 +277,7 @@ Error Solver::setup() {
     HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
     HO2D_TRY(build_poisson_geometry(fnb, fnijp));
+    HO2D_TRY(setup_forces());
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
     d.rowsum32.reset();
@@ -377,6 +379,81 @@ Error Solver::build_poisson_geometry(const std::vector<int>& fnb, const std::vec
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload(d.pg64[a], h[a]), "upload Poisson operator data");
     HO2D_CUDA(upload(d.pcode, code), "upload Poisson face codes");
     HO2D_CUDA(upload(d.pscat, scat), "upload trace scatter table");
+    return {0, ""};
+}
+
+// Per boundary point of the group "object": the coefficients of the body force
+// (forces.cu) F = sum (cdx, cdy) dw/dn_stored + (cwx, cwy) w_wall, where
+//   cdx = nu w_k |g| sigma y,  cdy = -nu w_k |g| sigma x,  cwx = nu w_k |g| t_x,  cwy = nu w_k |g| t_y,
+// (x, y) the point, |g| the face length per unit of the face coordinate, w_k the Gauss
+// weight, t = z x n with n the inward normal of the element (from the body into the
+// fluid), and sigma = +1 on W/S faces, -1 on E/N faces: the stored normal derivative is
+// taken towards the +xi / +eta side of the face (the element interior on W/S faces).
+Error Solver::setup_forces() {
+    DeviceState& d = *d_;
+    force_points_ = 0;
+    int grp = -1;
+    for (size_t g = 0; g < mesh_.group_names.size(); ++g)
+        if (mesh_.group_names[g] == "object") grp = (int)g;
+    if (grp < 0) return {0, ""};
+    const int K = in_.knod, L = mesh_.lnod, lin = L - 1;
+    const double nu = in_.reyn_inv;
+    std::vector<double> coef;
+    std::vector<int> idx;
+    for (int e = 0; e < mesh_.n_eb; ++e) {
+        if (mesh_.be_group[e] != grp) continue;
+        const int el = mesh_.be_el[e], side = mesh_.be_side[e], ijp = kF2I[side];
+        const int dd = ijp / 2, t = ijp % 2;
+        const double sigma = (ijp % 2 == 0) ? 1.0 : -1.0;
+        const double tsign = (ijp == 1 || ijp == 2) ? 1.0 : -1.0;  // counter-clockwise traversal
+        for (int k = 0; k < K; ++k) {
+            double x = 0, y = 0, dx = 0, dy = 0;  // position and derivative along the face
+            for (int j = 0; j < L; ++j)
+                for (int i = 0; i < L; ++i) {
+                    const int nd = mesh_.elem_nodes[el][tensor2fem(i, j, lin)];
+                    const double X = mesh_.node_xy[2 * nd], Y = mesh_.node_xy[2 * nd + 1];
+                    double w0, w1;
+                    if (dd == 0) {  // W/E face: xi = -+1, eta = x_k
+                        w0 = B_.gbb[i * 2 + t] * B_.gsb[j * K + k];
+                        w1 = B_.gbb[i * 2 + t] * B_.gsgb[j * K + k];
+                    } else {  // S/N face: eta = -+1, xi = x_k
+                        w0 = B_.gsb[i * K + k] * B_.gbb[j * 2 + t];
+                        w1 = B_.gsgb[i * K + k] * B_.gbb[j * 2 + t];
+                    }
+                    x += w0 * X;
+                    y += w0 * Y;
+                    dx += w1 * X;
+                    dy += w1 * Y;
+                }
+            const double len = std::sqrt(dx * dx + dy * dy);
+            const double tcx = tsign * dx / len, tcy = tsign * dy / len;  // element's ccw tangent
+            const double tx = -tcx, ty = -tcy;                            // t = z x n = -t_ccw
+            const double ds = nu * B_.w[k] * len;
+            coef.insert(coef.end(), {ds * sigma * y, -ds * sigma * x, ds * tx, ds * ty});
+            idx.push_back(e * K + (side / 2) * (K - 2 * k - 1) + k);
+        }
+    }
+    force_points_ = (int)idx.size();
+    HO2D_CUDA(upload(d.fcoef, coef), "upload force coefficients");
+    HO2D_CUDA(upload(d.fidx, idx), "upload force indices");
+    HO2D_CUDA(d.fout.alloc(2 * sizeof(double)), "alloc force result");
+    return {0, ""};
+}
+
+Error Solver::get_forces(double* fx, double* fy) {
+    if (!setup_done_) return {1, "not set up"};
+    if (force_points_ == 0) return {1, "the mesh has no boundary group named \"object\""};
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    HO2D_CUDA(launch_body_force(force_points_, d.fcoef.as<double>(), d.fidx.as<int>(), d.bc_d.as<double>(),
+                                d.bc_w.as<double>(), d.fout.as<double>(), d.stream),
+              "body force");
+    launches_ += 1;
+    double out[2];
+    HO2D_CUDA(cudaMemcpyAsync(out, d.fout.get(), sizeof(out), cudaMemcpyDeviceToHost, d.stream), "copy");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    if (fx) *fx = out[0];
+    if (fy) *fy = out[1];
     return {0, ""};
 }
 

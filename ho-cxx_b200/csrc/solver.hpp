@@ -56,6 +56,9 @@ class Solver {
     Error get_boundary(int which, double* out);
     Error set_boundary(int which, const double* in);
     Error get_solution_points(double* out);
+    // FP64 force (ρ = 1) on the boundary group named "object", from the wall vorticity and
+    // its normal flux of the latest stage
+    Error get_forces(double* fx, double* fy);
 
     bool is_setup() const { return setup_done_; }
     const Input& input() const { return in_; }
@@ -85,6 +88,8 @@ class Solver {
     Error upload_precision_arrays();
     Error setup_preconditioner();
     Error build_poisson_geometry(const std::vector<int>& fnb, const std::vector<int>& fnijp);
+    Error setup_forces();
+    int force_points_ = 0;  // boundary points of the "object" group (0: none)
     Error cuda(cudaError_t e, const char* what);
 
     Input in_;

@@ -170,6 +170,12 @@ class HO_2D:
         self._check(self._lib.ho2d_apply_poisson(self._h, a.size, capi.dptr(a), capi.dptr(out)))
         return out
 
+    def forces(self):
+        """FP64 force (fx = drag, fy = lift; density 1) on the boundary group "object"."""
+        fx, fy = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.ho2d_get_forces(self._h, ctypes.byref(fx), ctypes.byref(fy)))
+        return fx.value, fy.value
+
     def launch_count(self) -> int:
         n = ctypes.c_int64()
         self._check(self._lib.ho2d_last_launch_count(self._h, ctypes.byref(n)))

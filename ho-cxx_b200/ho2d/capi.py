@@ -52,6 +52,7 @@ SIGNATURES = {
     "ho2d_profile_spmv": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_apply_poisson": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_apply_poisson_noalloc": (ctypes.c_int, [_P, _I, ctypes.c_void_p, ctypes.c_void_p]),
+    "ho2d_get_forces": (ctypes.c_int, [_P, _DP, _DP]),
     "ho2d_last_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "ho2d_last_error": (ctypes.c_char_p, [_P]),
 }

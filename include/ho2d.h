@@ -147,6 +147,12 @@ int ho2d_apply_poisson(ho2d_solver* handle, int32_t len, const double* x, double
  * (it is fully rewritten from x before it is read), so calls that overlap on the GPU --
  * from different handles or streams on the same device -- race on it. */
 int ho2d_apply_poisson_noalloc(ho2d_solver* handle, int32_t len, const double* x_device, double* y_device);
+/* No counterpart in the reference. FP64 force per unit depth (density 1) on the boundary
+ * group named "object" (problem type 3): fx (drag) and fy (lift) from the wall vorticity and
+ * its normal flux of the latest stage, dp/ds = nu d(omega)/dn plus the skin friction
+ * nu omega t (Koumoutsakos & Leonard, JFM 1995). Drag and lift coefficients are 2 F / (U^2 D).
+ * HO2D_ERR_ARG when the mesh has no "object" group. */
+int ho2d_get_forces(ho2d_solver* handle, double* fx, double* fy);
 /* Total number of kernel launches this handle has issued since it was created. */
 int ho2d_last_launch_count(ho2d_solver* handle, int64_t* launches);
 /* Text of the last error on this handle ("" if none). The pointer stays valid until the

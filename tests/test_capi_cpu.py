@@ -116,3 +116,13 @@ def test_precision_modes():
         assert b"HO2D_MIXED_KRYLOV" in lib.ho2d_last_error(h)
     finally:
         lib.ho2d_destroy(h)
+
+
+def test_forces_need_setup():
+    lib, h = _handle()
+    try:
+        fx, fy = ctypes.c_double(), ctypes.c_double()
+        assert lib.ho2d_get_forces(h, ctypes.byref(fx), ctypes.byref(fy)) == 1
+        assert b"set up" in lib.ho2d_last_error(h)
+    finally:
+        lib.ho2d_destroy(h)

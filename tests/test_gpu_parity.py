@@ -183,3 +183,50 @@ def test_preconditioner_layouts_agree_with_oracle(tmp_path, monkeypatch, env):
     s.solve_advection_diffusion(2)
     assert rel(s.get_streamfunction(), c.psi) < TOL64
     assert rel(s.get_vorticity(), c.omega) < TOL64
+
+
+def test_body_force_matches_restatement(tmp_path):
+    # the device sum against the same force integral restated from the mesh geometry and the
+    # exported boundary arrays; orientation here comes from the element centroid instead of
+    # the element's counter-clockwise traversal used by the library
+    inp = meshgen.make_case("cyl6x12", str(tmp_path), knod=4, steps=2)
+    s = solver_for(inp)
+    rng = np.random.Generator(np.random.PCG64(21))
+    s.set_vorticity(rng.standard_normal((s.N_el, s.Knod, s.Knod)))
+    s.solve_advection_diffusion(2)
+    fx, fy = s.forces()
+    c = O.Case(inp)
+    K, L, B = c.K, c.L, c.B
+    w_wall = s.get_boundary(capi.BC_VORTICITY).reshape(-1, K)
+    dwdn = s.get_boundary(capi.BC_DIFFUSION).reshape(-1, K)
+    gx = np.linspace(-1.0, 1.0, L)
+    nu = 1.0 / 100.0
+    ref = np.zeros(2)
+    edges = dict(c.mesh.groups)["object"]
+    for e in edges:
+        el, side = int(c.mesh.be_el[e]), int(c.mesh.be_side[e])
+        ijp = int(O.F2I[side])
+        Xe = c.X[el]
+        centroid = Xe.reshape(-1, 2).mean(0)
+        for k in range(K):
+            a = B.xs[k]
+            xi, eta = {0: (-1.0, a), 1: (1.0, a), 2: (a, -1.0), 3: (a, 1.0)}[ijp]
+            lx, dlx = O.lagrange(gx, [xi])
+            ly, dly = O.lagrange(gx, [eta])
+            pos = np.einsum("j,i,jic->c", ly[:, 0], lx[:, 0], Xe)
+            if ijp < 2:
+                tan = np.einsum("j,i,jic->c", dly[:, 0], lx[:, 0], Xe)
+            else:
+                tan = np.einsum("j,i,jic->c", ly[:, 0], dlx[:, 0], Xe)
+            length = np.linalg.norm(tan)
+            n = np.array([-tan[1], tan[0]]) / length
+            if n @ (centroid - pos) < 0:
+                n = -n
+            t = np.array([-n[1], n[0]])  # z x n
+            idx = (side // 2) * (K - 2 * k - 1) + k
+            dn = (1.0 if ijp % 2 == 0 else -1.0) * dwdn[e, idx]
+            om = w_wall[e, idx]
+            ds = nu * B.w[k] * length
+            ref += ds * np.array([pos[1] * dn + om * t[0], -pos[0] * dn + om * t[1]])
+    scale = max(np.abs(ref).max(), 1e-300)
+    assert abs(fx - ref[0]) <= 1e-10 * scale and abs(fy - ref[1]) <= 1e-10 * scale, (fx, fy, ref)
