@@ -180,6 +180,7 @@ def cpu_baseline(inp, stages, t0=1.5):
                       f"({d['poisson_iterations']} shim BiCGSTAB iterations, tol 1e-15, maxiter 150; "
                       f"shim solver, not AMGCL 1.4.0)",
             "poisson_ms_per_step": 4.0 * d["poisson_seconds"] / d["stages"] * 1e3,
+            "ms_per_step": 4.0 * per_stage * 1e3, "dof": d["dof"],
             "cpu": _cpu_model(), "nproc": os.cpu_count()}
 
 
@@ -208,9 +209,10 @@ def run_reference(args, rank, world):
             return
         vals = [cb["value"]]
         value = statistics.median(vals)
-        dof = None
+        dof = cb["dof"]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "warmup": 0, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "impl": "reference",
                 "config": {"workload": workload_name(args), "dof": dof},
                 "cpu_baseline": dict(cb, value=value),

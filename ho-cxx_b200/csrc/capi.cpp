@@ -93,7 +93,8 @@ int ho2d_stage(ho2d_solver* h, double coeff) {
     return guarded(h, [&]() { return h->s.stage(coeff); });
 }
 
-int ho2d_solveto(ho2d_solver* h, double outerdt, int32_t numstep, int32_t integtype, double reyn) {
+int ho2d_solveto(ho2d_solver* h, double outerdt, int32_t numstep, int32_t integtype, double reyn, int32_t region) {
+    (void)region;  // names output files in the reference; nothing is written here
     return guarded(h, [&]() { return h->s.solveto(outerdt, numstep, integtype, reyn); });
 }
 

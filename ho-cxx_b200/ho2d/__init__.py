@@ -83,7 +83,8 @@ class HO_2D:
         return self.get_field(capi.FIELD_STAGE_K)
 
     def solveto_d(self, outerdt: float, numstep: int, integtype: int, reyn: float, region: int = 0) -> None:
-        self._check(self._lib.ho2d_solveto(self._h, float(outerdt), int(numstep), int(integtype), float(reyn)))
+        self._check(self._lib.ho2d_solveto(self._h, float(outerdt), int(numstep), int(integtype), float(reyn),
+                                           int(region)))
 
     # -- data exchange
     def _vol(self, comps=1):

@@ -33,7 +33,7 @@ SIGNATURES = {
     "ho2d_solve": (ctypes.c_int, [_P]),
     "ho2d_step": (ctypes.c_int, [_P, _I]),
     "ho2d_stage": (ctypes.c_int, [_P, _D]),
-    "ho2d_solveto": (ctypes.c_int, [_P, _D, _I, _I, _D]),
+    "ho2d_solveto": (ctypes.c_int, [_P, _D, _I, _I, _D, _I]),
     "ho2d_get_sizes": (ctypes.c_int, [_P, _IP, _IP, _IP, _IP]),
     "ho2d_get_vort": (ctypes.c_int, [_P, _I, _DP]),
     "ho2d_set_vort": (ctypes.c_int, [_P, _I, _DP]),

@@ -44,8 +44,8 @@ class HO_2D {
     void form_Laplace_operator_matrix() { ensure_setup(); }
     char solve_vorticity_streamfunction() { return (char)check(ho2d_solve(h_)); }
     char solve_advection_diffusion() { return (char)check(ho2d_step(h_, 1)); }
-    void solveto_d(double outerdt, int32_t numstep, int32_t integtype, double reyn, int32_t = 0) {
-        check(ho2d_solveto(h_, outerdt, numstep, integtype, reyn));
+    void solveto_d(double outerdt, int32_t numstep, int32_t integtype, double reyn, int32_t region = 0) {
+        check(ho2d_solveto(h_, outerdt, numstep, integtype, reyn, region));
     }
     void setsolnvort_d(int32_t len, const double* v) { check(ho2d_set_vort(h_, len, v)); }
     void getallvorts_d(int32_t len, double* v) { check(ho2d_get_vort(h_, len, v)); }

@@ -81,8 +81,11 @@ int ho2d_step(ho2d_solver* handle, int32_t nsteps);
  * on the current vorticity, without advancing time; results via ho2d_get_field. */
 int ho2d_stage(ho2d_solver* handle, double coeff);
 /* Replaces HO_2D::solveto_d (src/HO_2D.cpp:4194-4233) for the non-hybrid problem types:
- * dt = outerdt / numstep, integrator `integtype`, Re = reyn, numstep steps. */
-int ho2d_solveto(ho2d_solver* handle, double outerdt, int32_t numstep, int32_t integtype, double reyn);
+ * dt = outerdt / numstep, integrator `integtype`, Re = reyn, numstep steps. `region` only
+ * names the reference's optional substep VTK files (src/HO_2D.cpp:4217-4230); no files are
+ * written here, so it is accepted and has no effect. */
+int ho2d_solveto(ho2d_solver* handle, double outerdt, int32_t numstep, int32_t integtype, double reyn,
+                 int32_t region);
 
 /* Sizes after ho2d_setup: elements, Knod, boundary edges, geometry nodes per edge. */
 int ho2d_get_sizes(ho2d_solver* handle, int32_t* n_el, int32_t* knod, int32_t* n_edges_boundary,
