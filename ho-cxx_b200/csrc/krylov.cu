@@ -608,8 +608,9 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     __syncthreads();
     if (done) return;
     // the five slot values, each the sum of its five parts (part 0..4 in order)
-    if (active && ij < 5)
-        ue[le][ij] = pu[le][5 * ij] + pu[le][5 * ij + 1] + pu[le][5 * ij + 2] + pu[le][5 * ij + 3] + pu[le][5 * ij + 4];
+    if (active)
+        for (int q = ij; q < 5; q += K2)  // K^2 < 5 threads per element for K <= 2
+            ue[le][q] = pu[le][5 * q] + pu[le][5 * q + 1] + pu[le][5 * q + 2] + pu[le][5 * q + 3] + pu[le][5 * q + 4];
     __syncthreads();
     T u_self = T(0);
     if (active) {

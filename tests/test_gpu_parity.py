@@ -107,10 +107,16 @@ def test_solve_and_solveto_match_steps():
     assert rel(s2.get_vorticity(), ref["traj_vort_3"]) < TOL64
 
 
+# K = 2..8: the reference stops at K = 5 (src/HO_2D.cpp:522-525), the oracle does not; K < 4
+# runs the operator's general form, K >= 4 the register-resident one, K = 8 is the maximum
 @pytest.mark.parametrize("name,knod,steps,kw", [
     ("cavityj10", 5, 4, {}),
     ("cyl6x12", 4, 4, {"advection_type": 2}),
     ("bfs3", 3, 3, {"x_out": 4.0}),
+    ("cavityj8", 2, 3, {}),
+    ("cyl6x12", 6, 2, {}),
+    ("cavityj8", 7, 2, {"advection_type": 2}),
+    ("cavityj6", 8, 2, {}),
 ])
 def test_against_oracle(tmp_path, name, knod, steps, kw):
     inp = meshgen.make_case(name, str(tmp_path), knod=knod, steps=steps, **kw)
