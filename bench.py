@@ -317,7 +317,7 @@ def run_ours(args, rank, world, local, phys):
         peak, peak_kind = measured_peaks()
         # DRAM bytes (read + write) of one k_mf_apply<5, float> launch on this workload, from
         # the ncu capture summarised in profiles/k_mf_apply_bfs14625_k5_fp32.md
-        traffic = 13119232 if (args.case == "bfs" and args.knod == 5) else None
+        traffic = 13118720 if (args.case == "bfs" and args.knod == 5) else None
         m = results["mixed"]
         achieved = m["spmv_bytes"] / (m["spmv_ms"] * 1e-3) / 1e9
         roofline = {"bound": "hbm", "kernel": "k_mf_apply (matrix-free Poisson operator, FP32 inner Krylov)",
