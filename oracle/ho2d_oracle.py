@@ -804,7 +804,12 @@ class Case:
         return rhs.ravel()
 
     def solve_poisson(self, vort):
-        self.psi = self.lu.solve(self.poisson_rhs(vort)).reshape(self.N, self.K, self.K)
+        rhs = self.poisson_rhs(vort)
+        if np.iscomplexobj(rhs):  # complex-step derivatives (ho2d_cs): the LU is real
+            psi = self.lu.solve(np.ascontiguousarray(rhs.real)) + 1j * self.lu.solve(np.ascontiguousarray(rhs.imag))
+        else:
+            psi = self.lu.solve(rhs)
+        self.psi = psi.reshape(self.N, self.K, self.K)
 
     def velocity(self):
         """u = dpsi/dy, v = -dpsi/dx with side outputs (src/HO_2D.cpp:3174-3366)."""
@@ -890,7 +895,7 @@ class Case:
 
     def _boundary_face_values(self, arr_eb):
         """Boundary-edge array [N_eb][K] mapped onto faces [N,4,K] (zero elsewhere)."""
-        out = np.zeros((self.N, 4, self.K))
+        out = np.zeros((self.N, 4, self.K), dtype=np.result_type(arr_eb, float))
         for ijp in range(4):
             bnd = self.f_bidx[:, ijp] >= 0
             e = self.f_bidx[bnd, ijp]
@@ -913,9 +918,10 @@ class Case:
         s = sgn[..., None]
         avg = 0.5 * (flx + s * fn)
         dw = wv - wn
-        big = np.abs(dw) > 1e-4
+        big = np.abs(np.real(dw)) > 1e-4
         a = np.where(big, (flx - s * fn) / np.where(big, dw, 1.0), 0.0)
-        upw = avg + np.where(big, 0.5 * SGN[None, :, None] * np.abs(a) * dw, 0.0)
+        # |a| written as a sgn(Re a): the same value, and complex-step differentiable
+        upw = avg + np.where(big, 0.5 * SGN[None, :, None] * (a * np.sign(np.real(a))) * dw, 0.0)
         up[inter] = upw[inter]
         return self._lift_divergence(fx, fy, up)
 
@@ -945,7 +951,7 @@ class Case:
         wv, _ = self._traces(vort)
         wn, _ = self._nbr_gather(wv)
         t = (np.arange(4) % 2)[None, :, None].astype(float)
-        pos = cvf > 0.0
+        pos = np.real(cvf) > 0.0
         upw = np.where(pos, cvf * (t * wv + (1 - t) * wn), cvf * ((1 - t) * wv + t * wn))
         up = np.where(inter[..., None], upw, self._boundary_face_values(self.bc_adv))
         return self._lift_divergence(fx, fy, up)
