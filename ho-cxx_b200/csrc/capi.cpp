@@ -158,6 +158,13 @@ int ho2d_set_boundary(ho2d_solver* h, int32_t which, int32_t len, const double* 
     });
 }
 
+int ho2d_get_boundary_points(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, 2 * nbnd(h), buf);
+        return e.code ? e : h->s.get_boundary_points(buf);
+    });
+}
+
 int ho2d_get_solution_points(ho2d_solver* h, int32_t len, double* buf) {
     return guarded(h, [&]() -> ho2d::Error {
         ho2d::Error e = check_len(h, len, 2 * nvol(h), buf);
@@ -228,6 +235,58 @@ int ho2d_apply_poisson_noalloc(ho2d_solver* h, int32_t len, const double* x_devi
 
 int ho2d_get_forces(ho2d_solver* h, double* fx, double* fy) {
     return guarded(h, [&]() { return h->s.get_forces(fx, fy); });
+}
+
+int ho2d_adjoint_forward(ho2d_solver* h, int32_t nsteps, int32_t ckpt_every) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};
+        return h->s.adjoint_forward(nsteps, ckpt_every);
+    });
+}
+
+int ho2d_adjoint_backward(ho2d_solver* h, int32_t len, const double* dJ_domegaT, double* grad_omega0, int32_t len_pv,
+                          double* grad_parl_vel) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), dJ_domegaT);
+        if (e.code) return e;
+        if (!grad_omega0) return {HO2D_ERR_ARG, "null output buffer"};
+        if (grad_parl_vel || len_pv) {
+            e = check_len(h, len_pv, nbnd(h), grad_parl_vel);
+            if (e.code) return e;
+        }
+        return h->s.adjoint_backward(dJ_domegaT, grad_omega0, grad_parl_vel);
+    });
+}
+
+int ho2d_stage_adjoint(ho2d_solver* h, double coeff, int32_t len, const double* lam_k, double* lam_w, int32_t len_pv,
+                       double* lam_pv) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), lam_k);
+        if (e.code) return e;
+        if (!lam_w) return {HO2D_ERR_ARG, "null output buffer"};
+        if (lam_pv || len_pv) {
+            e = check_len(h, len_pv, nbnd(h), lam_pv);
+            if (e.code) return e;
+        }
+        return h->s.stage_adjoint(coeff, lam_k, lam_w, lam_pv);
+    });
+}
+
+int ho2d_apply_poisson_transpose(ho2d_solver* h, int32_t len, const double* x, double* y) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), x);
+        if (e.code) return e;
+        if (!y) return {HO2D_ERR_ARG, "null output buffer"};
+        return h->s.apply_poisson_transpose(x, y);
+    });
+}
+
+int ho2d_adjoint_stats(ho2d_solver* h, int32_t* iterations, double* rel_residual) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (iterations) *iterations = h->s.last_adjoint_iterations();
+        if (rel_residual) *rel_residual = h->s.last_adjoint_residual();
+        return {0, ""};
+    });
 }
 
 int ho2d_last_launch_count(ho2d_solver* h, int64_t* launches) {

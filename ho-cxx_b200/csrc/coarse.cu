@@ -95,12 +95,21 @@ struct Vec16<float> {
     using type = float4;
     static constexpr int N = 4;
     __device__ static float dot(const float4& a, const float4& b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+    // zero the components at and past `keep` (the tail of a vector that ends inside a piece)
+    __device__ static void keep_first(float4& v, int keep) {
+        if (keep < 4) v.w = 0.f;
+        if (keep < 3) v.z = 0.f;
+        if (keep < 2) v.y = 0.f;
+    }
 };
 template <>
 struct Vec16<double> {
     using type = double2;
     static constexpr int N = 2;
     __device__ static double dot(const double2& a, const double2& b) { return a.x * b.x + a.y * b.y; }
+    __device__ static void keep_first(double2& v, int keep) {
+        if (keep < 2) v.y = 0.0;
+    }
 };
 
 constexpr int kGemvWarps = 8;  // rows (one warp each) per CTA
@@ -119,6 +128,7 @@ __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv(DevEll<T> W, con
     const int row = blockIdx.x * kGemvWarps + (threadIdx.x >> 5);
     if (row >= W.n) return;
     const int nvec = (W.n + V::N - 1) / V::N;
+    const int tail = W.n - (nvec - 1) * V::N;  // entries of the last piece inside the vector
     const VT* wr = reinterpret_cast<const VT*>(W.val + (size_t)row * W.w);
     const VT* fv = reinterpret_cast<const VT*>(f);
     T acc = T(0);
@@ -130,6 +140,9 @@ __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv(DevEll<T> W, con
             if (c < nvec) {
                 a[q] = __ldg(wr + c);
                 b[q] = __ldg(fv + c);
+                // the padding of f is zero when written in this precision, but a buffer
+                // shared by both precisions may hold the other one's bytes there
+                if (c == nvec - 1) V::keep_first(b[q], tail);
             }
         }
 #pragma unroll
@@ -228,6 +241,42 @@ cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const Kr
     return cudaGetLastError();
 }
 
+// The whole cycle on a plain level-0 right-hand side f0 (N entries, zero-padded to a
+// multiple of 4): u0 = cycle(f0) in pc.lev[0].u, level 0's own up step included. Used by
+// the transposed solve of the adjoint, whose preconditioner forms f0 in its own kernel.
+template <typename T>
+cudaError_t coarse_cycle_vec(const Precond<T>& pc, const T* f0, const KrylovScalars* sc, cudaStream_t s) {
+    const int d = pc.nlev - 1;
+    if (d < 0) return cudaSuccess;
+    const unsigned gd = (unsigned)((pc.dense.n + kGemvWarps - 1) / kGemvWarps);
+    if (d == 0) {
+        k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, f0, pc.lev[0].u, sc);
+        return cudaGetLastError();
+    }
+    k_coarse_rows<T, const T*><<<rows_grid(pc.lev[0].M), 256, 0, s>>>(pc.lev[0].M, f0, DevEll<T>(), nullptr, 0,
+                                                                       pc.lev[1].f, sc);
+    for (int l = 1; l < d; ++l) {
+        const CoarseLevel<T>& L = pc.lev[l];
+        k_coarse_rows<T, const T*><<<rows_grid(L.M), 256, 0, s>>>(L.M, L.f, DevEll<T>(), nullptr, 0,
+                                                                   pc.lev[l + 1].f, sc);
+    }
+    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc);
+    for (int l = d - 1; l >= 1; --l) {
+        const CoarseLevel<T>& L = pc.lev[l];
+        k_coarse_rows<T, const T*><<<rows_grid(L.S), 256, 0, s>>>(L.S, L.f, L.Q, pc.lev[l + 1].u, 1, L.u, sc);
+    }
+    const CoarseLevel<T>& L0 = pc.lev[0];
+    k_coarse_rows<T, const T*><<<rows_grid(L0.S), 256, 0, s>>>(L0.S, f0, L0.Q, pc.lev[1].u, 1, L0.u, sc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+int coarse_vec_launches(const Precond<T>& pc) {
+    if (pc.nlev <= 0) return 0;
+    const int d = pc.nlev - 1;
+    return d == 0 ? 1 : 2 * d + 1;
+}
+
 template <typename T>
 int coarse_launches(const Precond<T>& pc) {
     if (pc.nlev <= 0) return 0;
@@ -252,6 +301,8 @@ CoarseOut<T> coarse_out(const Precond<T>& pc) {
     template cudaError_t coarse_cycle<T>(const Precond<T>&, const BicgVectors<T>&, const KrylovScalars*, int,  \
                                          cudaStream_t);                                                      \
     template int coarse_launches<T>(const Precond<T>&);                                              \
+    template cudaError_t coarse_cycle_vec<T>(const Precond<T>&, const T*, const KrylovScalars*, cudaStream_t); \
+    template int coarse_vec_launches<T>(const Precond<T>&);                                          \
     template CoarseOut<T> coarse_out<T>(const Precond<T>&);
 
 HO2D_INSTANTIATE_COARSE(double)

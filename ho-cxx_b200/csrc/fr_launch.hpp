@@ -187,6 +187,11 @@ cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const Kr
                          cudaStream_t s);
 template <typename T>
 int coarse_launches(const Precond<T>& pc);
+// the whole cycle on a plain level-0 right-hand side: u0 -> pc.lev[0].u (coarse.cu)
+template <typename T>
+cudaError_t coarse_cycle_vec(const Precond<T>& pc, const T* f0, const KrylovScalars* sc, cudaStream_t s);
+template <typename T>
+int coarse_vec_launches(const Precond<T>& pc);
 template <typename T>
 CoarseOut<T> coarse_out(const Precond<T>& pc);
 

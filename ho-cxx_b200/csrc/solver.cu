@@ -20,6 +20,7 @@
 #include "host_amg.hpp"
 #include "noalloc.hpp"
 #include "solver.hpp"
+#include "solver_state.hpp"
 
 namespace ho2d {
 
@@ -38,131 +39,6 @@ void DeviceBuffer::reset() {
     n_ = 0;
 }
 
-// A captured Krylov solve and the parameters baked into it.
-struct SolveGraph {
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int max_iter = -1;
-    void reset() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-        max_iter = -1;
-    }
-    ~SolveGraph() { reset(); }
-};
-
-struct DeviceState {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
-    // connectivity and boundary tables
-    DeviceBuffer face_nb, face_nijp, be_group, sw_p, sw_d, noslip, role, be_ijp;
-    DevBases<double> b64;
-    DevBases<float> b32;
-    // metrics: xxi, xeta, yxi, yeta, J, fA, fB, fJ, fAn
-    DeviceBuffer m64[9], m32[9];
-    bool have32 = false;
-    // boundary arrays (double)
-    DeviceBuffer bc_p, bc_nv, bc_pv, bc_d, bc_w, vjump, bc_adv, edge_y, bsrc;
-    // fields
-    DeviceBuffer omega, acc, psi64, rhs, rres;
-    DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
-    // Poisson operator and Krylov workspace
-    // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
-    DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
-    // matrix-free operator data: G11, G12, G22, fa, fb, nfa, nfb, minv (PoisGeom)
-    DeviceBuffer pg64[8], pg32[8], pcode, pscat;
-    std::vector<double> pg_host[8];  // kept for the FP32 copies made on demand
-    DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
-    DeviceBuffer esum[4];  // element sums of r, v, p (two alternating buffers), N + 4 entries
-    DeviceBuffer ktv, ktg, kxtv, kxtg;  // face traces of the Krylov operand and of x
-    DeviceBuffer partials, counter, scalars;
-    KrylovScalars* h_sc = nullptr;
-    // two-level preconditioner: per coarse level the row-padded cycle operators M, S, Q
-    // (FP64 and FP32 values) and the level's f and u (sized for FP64, reused for FP32)
-    struct EllBufs {
-        DeviceBuffer col, v64, v32;
-    };
-    struct LevelBufs {
-        EllBufs M, S, Q;
-        DeviceBuffer f, u;
-    };
-    std::vector<std::unique_ptr<LevelBufs>> lev;
-    DeviceBuffer dense64, dense32;
-    Precond<double> pc64;
-    Precond<float> pc32;
-    SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
-    double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
-    DeviceBuffer l2flush;               // written between timed steps to evict L2
-    DeviceBuffer fcoef, fidx, fout;     // body-force coefficients, boundary indices, result
-
-    ~DeviceState() {
-        if (h_sc) cudaFreeHost(h_sc);
-        for (cudaEvent_t e : {ev0, ev1, evp0, evp1})
-            if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-namespace {
-
-template <typename T>
-DevBases<T> make_dev_bases(const Bases& B) {
-    DevBases<T> d;
-    std::memset(&d, 0, sizeof(d));
-    for (int i = 0; i < B.K * B.K; ++i) d.D[i] = T(B.D[i]);
-    for (int i = 0; i < B.K * 2; ++i) {
-        d.sbb[i] = T(B.sbb[i]);
-        d.sbgb[i] = T(B.sbgb[i]);
-        d.R[i] = T(B.R[i]);
-        d.gR[i] = T(B.gR[i]);
-    }
-    d.gp[0] = T(B.gp[0]);
-    d.gp[1] = T(B.gp[1]);
-    return d;
-}
-
-template <typename T>
-cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& h) {
-    cudaError_t e = buf.alloc(h.size() * sizeof(T));
-    if (e != cudaSuccess || h.empty()) return e;
-    return cudaMemcpy(buf.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
-}
-
-template <typename T>
-cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
-    std::vector<T> c(h.begin(), h.end());
-    return upload(buf, c);
-}
-
-cudaError_t upload_ell(DeviceState::EllBufs& b, const Ell& A) {
-    cudaError_t e;
-    if ((e = upload(b.col, A.col.empty() ? std::vector<int>{0} : A.col)) != cudaSuccess) return e;
-    if ((e = upload(b.v64, A.val.empty() ? std::vector<double>{0.0} : A.val)) != cudaSuccess) return e;
-    return upload_as<float>(b.v32, A.val.empty() ? std::vector<double>{0.0} : A.val);
-}
-
-// lanes per row for a row-padded matrix of width w: about w/2, a power of two in [4, 32]
-int lanes_for(int w) {
-    int g = 4;
-    while (g < 32 && 2 * g <= std::max(1, w / 2)) g *= 2;
-    return g;
-}
-
-template <typename TM>
-DevEll<TM> view(const DeviceState::EllBufs& b, const Ell& A, int g, bool f32) {
-    DevEll<TM> v;
-    v.n = A.n;
-    v.w = A.w;
-    v.g = g;
-    v.col = b.col.as<int>();
-    v.val = f32 ? (const TM*)b.v32.get() : (const TM*)b.v64.get();
-    return v;
-}
-
-}  // namespace
 
 Solver::Solver() : d_(new DeviceState) {
     const char* v = std::getenv("HO2D_VERBOSE");
@@ -177,12 +53,6 @@ Error Solver::cuda(cudaError_t e, const char* what) {
     return {5, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-#define HO2D_TRY(expr)                 \
-    do {                               \
-        Error _e = (expr);             \
-        if (_e.code) return _e;        \
-    } while (0)
-#define HO2D_CUDA(call, what) HO2D_TRY(cuda((call), what))
 
 Error Solver::read_input(const std::string& path) {
     Input in;
@@ -457,6 +327,70 @@ Error Solver::get_forces(double* fx, double* fy) {
     return {0, ""};
 }
 
+// Uploads a coarse hierarchy (cycle operators of every level, level vectors, padded dense
+// inverse of the coarsest level) and fills the device views of both precisions.
+Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vector<std::unique_ptr<LevelBufs>>& lev,
+                               DeviceBuffer& dense64, DeviceBuffer& dense32, Precond<double>& pc64,
+                               Precond<float>& pc32, std::vector<int>* sizes) {
+    if ((int)H.levels.size() > kMaxLevels) return {4, "coarse hierarchy too deep"};
+    const int nl = (int)H.levels.size();
+    lev.clear();
+    std::vector<Ell> eM(nl), eS(nl), eQ(nl);
+    for (int l = 0; l < nl; ++l) {
+        const AmgLevel& L = H.levels[l];
+        auto b = std::unique_ptr<LevelBufs>(new LevelBufs);
+        if (l + 1 < nl) {
+            eM[l] = to_ell(L.M);
+            eS[l] = to_ell(L.S);
+            eQ[l] = to_ell(L.Q);
+            HO2D_CUDA(upload_ell(b->M, eM[l]), "upload coarse M");
+            HO2D_CUDA(upload_ell(b->S, eS[l]), "upload coarse S");
+            HO2D_CUDA(upload_ell(b->Q, eQ[l]), "upload coarse Q");
+        }
+        const std::vector<double> z((size_t)L.A.n + 4, 0.0);  // zero padding for 16-byte reads
+        for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
+        lev.push_back(std::move(b));
+    }
+    // coarsest inverse, rows padded to a multiple of 4 entries (16-byte row starts)
+    const int nd = H.n_dense, wd = (nd + 3) / 4 * 4;
+    std::vector<double> dpad((size_t)nd * wd, 0.0);
+    for (int i = 0; i < nd; ++i)
+        std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
+                  dpad.begin() + (size_t)i * wd);
+    HO2D_CUDA(upload(dense64, dpad), "upload dense");
+    HO2D_CUDA(upload_as<float>(dense32, dpad), "upload dense");
+    auto fill = [&](auto& pc, bool f32) {
+        using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
+        pc.nlev = nl;
+        pc.omega = omega;
+        pc.dense.n = nd;
+        pc.dense.w = wd;
+        pc.dense.g = 32;
+        pc.dense.col = nullptr;
+        pc.dense.val = f32 ? (const T*)dense32.get() : (const T*)dense64.get();
+        for (int l = 0; l < nl; ++l) {
+            auto& b = *lev[l];
+            auto& c = pc.lev[l];
+            c.n = H.levels[l].A.n;
+            if (l + 1 < nl) {
+                c.M = view<T>(b.M, eM[l], lanes_for(eM[l].w), f32);
+                const int g = lanes_for(std::max(eS[l].w, eQ[l].w));
+                c.S = view<T>(b.S, eS[l], g, f32);
+                c.Q = view<T>(b.Q, eQ[l], g, f32);
+            }
+            c.f = b.f.as<T>();
+            c.u = b.u.as<T>();
+        }
+    };
+    fill(pc64, false);
+    fill(pc32, true);
+    if (sizes) {
+        sizes->clear();
+        for (const auto& L : H.levels) sizes->push_back(L.A.n);
+    }
+    return {0, ""};
+}
+
 // Builds the P0 coarse hierarchy on the host and the device views of both precisions.
 // HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight;
 // HO2D_DENSE_MAX bounds the dense coarsest level (a test hook for other hierarchy shapes).
@@ -476,60 +410,8 @@ Error Solver::setup_preconditioner() {
     const int dmax = dm ? std::max(1, std::atoi(dm)) : kDenseMax;
     CoarseHierarchy H;
     HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H, dmax, dm ? dmax : kDenseMaxFirst));
-    if ((int)H.levels.size() > kMaxLevels) return {4, "coarse hierarchy too deep"};
-    const int nl = (int)H.levels.size();
-    std::vector<Ell> eM(nl), eS(nl), eQ(nl);
-    for (int l = 0; l < nl; ++l) {
-        const AmgLevel& L = H.levels[l];
-        auto b = std::unique_ptr<DeviceState::LevelBufs>(new DeviceState::LevelBufs);
-        if (l + 1 < nl) {
-            eM[l] = to_ell(L.M);
-            eS[l] = to_ell(L.S);
-            eQ[l] = to_ell(L.Q);
-            HO2D_CUDA(upload_ell(b->M, eM[l]), "upload coarse M");
-            HO2D_CUDA(upload_ell(b->S, eS[l]), "upload coarse S");
-            HO2D_CUDA(upload_ell(b->Q, eQ[l]), "upload coarse Q");
-        }
-        const std::vector<double> z((size_t)L.A.n + 4, 0.0);  // zero padding for 16-byte reads
-        for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
-        d.lev.push_back(std::move(b));
-    }
-    // coarsest inverse, rows padded to a multiple of 4 entries (16-byte row starts)
-    const int nd = H.n_dense, wd = (nd + 3) / 4 * 4;
-    std::vector<double> dpad((size_t)nd * wd, 0.0);
-    for (int i = 0; i < nd; ++i)
-        std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
-                  dpad.begin() + (size_t)i * wd);
-    HO2D_CUDA(upload(d.dense64, dpad), "upload dense");
-    HO2D_CUDA(upload_as<float>(d.dense32, dpad), "upload dense");
-    auto fill = [&](auto& pc, bool f32) {
-        using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
-        pc.nlev = nl;
-        pc.omega = omega;
-        pc.dense.n = nd;
-        pc.dense.w = wd;
-        pc.dense.g = 32;
-        pc.dense.col = nullptr;
-        pc.dense.val = f32 ? (const T*)d.dense32.get() : (const T*)d.dense64.get();
-        for (int l = 0; l < nl; ++l) {
-            auto& b = *d.lev[l];
-            auto& c = pc.lev[l];
-            c.n = H.levels[l].A.n;
-            if (l + 1 < nl) {
-                c.M = view<T>(b.M, eM[l], lanes_for(eM[l].w), f32);
-                const int g = lanes_for(std::max(eS[l].w, eQ[l].w));
-                c.S = view<T>(b.S, eS[l], g, f32);
-                c.Q = view<T>(b.Q, eQ[l], g, f32);
-            }
-            c.f = b.f.as<T>();
-            c.u = b.u.as<T>();
-        }
-    };
-    fill(d.pc64, false);
-    fill(d.pc32, true);
-    coarse_levels_ = nl;
-    coarse_sizes_.clear();
-    for (const auto& L : H.levels) coarse_sizes_.push_back(L.A.n);
+    HO2D_TRY(upload_hierarchy(H, omega, d.lev, d.dense64, d.dense32, d.pc64, d.pc32, &coarse_sizes_));
+    coarse_levels_ = (int)coarse_sizes_.size();
     if (verbose_) {
         std::fprintf(stderr, "  coarse levels:");
         for (int n : coarse_sizes_) std::fprintf(stderr, " %d", n);
@@ -570,77 +452,6 @@ Error Solver::set_precision(int mode) {
         }
     }
     return {0, ""};
-}
-
-template <typename T>
-static FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
-    DeviceBuffer* mm = f32 ? d.m32 : d.m64;
-    FrGeom<T> g;
-    g.N = m.n_el;
-    g.n_eb = m.n_eb;
-    g.face_nb = d.face_nb.as<int>();
-    g.face_nijp = d.face_nijp.as<int>();
-    g.xxi = mm[0].as<T>();
-    g.xeta = mm[1].as<T>();
-    g.yxi = mm[2].as<T>();
-    g.yeta = mm[3].as<T>();
-    g.J = mm[4].as<T>();
-    g.fA = mm[5].as<T>();
-    g.fB = mm[6].as<T>();
-    g.fJ = mm[7].as<T>();
-    g.fAn = mm[8].as<T>();
-    g.be_group = d.be_group.as<int>();
-    g.sw_p = d.sw_p.as<int>();
-    g.sw_d = d.sw_d.as<int>();
-    g.noslip = d.noslip.as<int>();
-    return g;
-}
-
-template <typename T>
-static MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
-    MfOp<T> op;
-    op.K = K;
-    op.g.N = m.n_el;
-    const DeviceBuffer* pg = f32 ? d.pg32 : d.pg64;
-    op.g.G11 = pg[0].as<T>();
-    op.g.G12 = pg[1].as<T>();
-    op.g.G22 = pg[2].as<T>();
-    op.g.fa = pg[3].as<T>();
-    op.g.fb = pg[4].as<T>();
-    op.g.nfa = pg[5].as<T>();
-    op.g.nfb = pg[6].as<T>();
-    op.g.minv = pg[7].as<T>();
-    op.g.code = d.pcode.as<int>();
-    op.g.scat = d.pscat.as<int>();
-    op.b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
-    op.dinv = f32 ? (const T*)d.dinv32.get() : (const T*)d.dinv64.get();
-    op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
-    op.bcol = d.bcol.as<int>();
-    return op;
-}
-
-template <typename T>
-static BicgVectors<T> krylov_vectors(DeviceState& d, T* x, const T* b) {
-    BicgVectors<T> v;
-    v.x = x;
-    v.r = d.kv[0].as<T>();
-    v.rhat = d.kv[1].as<T>();
-    v.p = d.kv[2].as<T>();
-    v.v = d.kv[3].as<T>();
-    v.s = d.kv[4].as<T>();
-    v.t = d.kv[5].as<T>();
-    v.ph = d.kv[6].as<T>();
-    v.sh = d.kv[7].as<T>();
-    v.b = b;
-    v.tv = d.ktv.as<T>();
-    v.tg = d.ktg.as<T>();
-    v.xtv = d.kxtv.as<T>();
-    v.xtg = d.kxtg.as<T>();
-    v.er = d.esum[0].as<T>();
-    v.ev = d.esum[1].as<T>();
-    v.ep[0] = d.esum[2].as<T>();
-    v.ep[1] = d.esum[3].as<T>();
-    return v;
 }
 
 // ------------------------------------------------------------------ Poisson
@@ -761,8 +572,11 @@ Error Solver::poisson_solve() {
 }
 
 // ------------------------------------------------------------------ stages
+// One stage at the current stage input. With solve == false the Poisson solve is skipped
+// and the stage works from the psi already in place (the adjoint recomputes a stored
+// stage's fields this way).
 template <typename T>
-Error Solver::stage_t(double coeff, int rk_stage, bool update) {
+Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     DeviceState& d = *d_;
     const int N = mesh_.n_el, K = in_.knod;
     const size_t nv = (size_t)N * K * K;
@@ -776,11 +590,14 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update) {
     HO2D_CUDA(launch_bc_update(mesh_.n_eb, K, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
                                d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, d.stream),
               "bc_update");
-    HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
-                                    d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
-              "poisson_rhs");
-    launches_ += 2;
-    HO2D_TRY(poisson_solve());
+    launches_ += 1;
+    if (solve) {
+        HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
+                                        d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
+                  "poisson_rhs");
+        launches_ += 1;
+        HO2D_TRY(poisson_solve());
+    }
     const T* psi = f32 ? d.psiT.as<T>() : reinterpret_cast<const T*>(d.psi64.get());
     if (f32) {
         HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), nv, d.stream), "d2f");
@@ -1095,6 +912,31 @@ Error Solver::set_boundary(int which, const double* in) {
     return {0, ""};
 }
 
+// Coordinates of the boundary flux points in the order of the boundary arrays
+// ([N_eb][K][x, y], index e*K + (side/2)(K-2k-1) + k for face point k of edge e's face).
+Error Solver::get_boundary_points(double* out) {
+    if (!setup_done_) return {1, "not set up"};
+    const int K = in_.knod, L = mesh_.lnod, lin = L - 1;
+    for (int e = 0; e < mesh_.n_eb; ++e) {
+        const int el = mesh_.be_el[e], side = mesh_.be_side[e], ijp = kF2I[side];
+        const int dd = ijp / 2, t = ijp % 2;
+        for (int k = 0; k < K; ++k) {
+            double x = 0.0, y = 0.0;
+            for (int j = 0; j < L; ++j)
+                for (int i = 0; i < L; ++i) {
+                    const int nd = mesh_.elem_nodes[el][tensor2fem(i, j, lin)];
+                    const double w = dd == 0 ? B_.gbb[i * 2 + t] * B_.gsb[j * K + k] : B_.gsb[i * K + k] * B_.gbb[j * 2 + t];
+                    x += w * mesh_.node_xy[2 * nd];
+                    y += w * mesh_.node_xy[2 * nd + 1];
+                }
+            const size_t q = (size_t)e * K + (side / 2) * (K - 2 * k - 1) + k;
+            out[2 * q] = x;
+            out[2 * q + 1] = y;
+        }
+    }
+    return {0, ""};
+}
+
 Error Solver::get_solution_points(double* out) {
     if (!setup_done_) return {1, "not set up"};
     const int N = mesh_.n_el, K = in_.knod, L = mesh_.lnod;
@@ -1115,5 +957,8 @@ Error Solver::get_solution_points(double* out) {
             }
     return {0, ""};
 }
+
+// the adjoint driver (adjoint_driver.cu) recomputes stages in FP64
+template Error Solver::stage_t<double>(double, int, bool, bool);
 
 }  // namespace ho2d

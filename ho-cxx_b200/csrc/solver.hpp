@@ -31,7 +31,12 @@ class DeviceBuffer {
     size_t n_ = 0;
 };
 
-struct DeviceState;  // defined in solver.cu
+struct DeviceState;   // solver_state.hpp
+struct AdjointState;  // solver_state.hpp
+struct LevelBufs;     // solver_state.hpp
+struct CoarseHierarchy;
+template <typename T>
+struct Precond;
 
 class Solver {
   public:
@@ -56,9 +61,26 @@ class Solver {
     Error get_boundary(int which, double* out);
     Error set_boundary(int which, const double* in);
     Error get_solution_points(double* out);
+    Error get_boundary_points(double* out);  // [N_eb][K][2] in boundary-array order
     // FP64 force (ρ = 1) on the boundary group named "object", from the wall vorticity and
     // its normal flux of the latest stage
     Error get_forces(double* fx, double* fy);
+
+    // ---- discrete adjoint (adjoint_driver.cu)
+    // nsteps time steps from the current state, keeping the vorticity every ckpt_every
+    // steps for the backward sweep
+    Error adjoint_forward(int nsteps, int ckpt_every);
+    // gradient of J(omega(T)) with respect to omega at the start of the last
+    // adjoint_forward and to BC_parl_vel, from dJ/d(omega(T)); the state at T is kept
+    Error adjoint_backward(const double* dJ_dw, double* grad_w0, double* grad_pv);
+    // adjoint of one stage (stage(coeff)) at the current state: lam_k -> lam of the stage
+    // input vorticity and of BC_parl_vel
+    Error stage_adjoint(double coeff, const double* lam_k, double* lam_w, double* lam_pv);
+    // y = A^T x with the transposed matrix-free Poisson operator (FP64)
+    Error apply_poisson_transpose(const double* x, double* y);
+    int adjoint_steps() const;
+    int last_adjoint_iterations() const { return last_adj_iters_; }
+    double last_adjoint_residual() const { return last_adj_res_; }
 
     bool is_setup() const { return setup_done_; }
     const Input& input() const { return in_; }
@@ -82,13 +104,21 @@ class Solver {
     Error stage_impl(double coeff, int rk_stage, bool update);
     Error poisson_solve();
     template <typename T>
-    Error stage_t(double coeff, int rk_stage, bool update);
+    Error stage_t(double coeff, int rk_stage, bool update, bool solve = true);
     template <typename T>
     Error velocity_only_t();
     Error upload_precision_arrays();
     Error setup_preconditioner();
     Error build_poisson_geometry(const std::vector<int>& fnb, const std::vector<int>& fnijp);
     Error setup_forces();
+    Error upload_hierarchy(const CoarseHierarchy& H, double omega, std::vector<std::unique_ptr<LevelBufs>>& lev,
+                           DeviceBuffer& dense64, DeviceBuffer& dense32, Precond<double>& pc64, Precond<float>& pc32,
+                           std::vector<int>* sizes);
+    Error adjoint_prepare();
+    Error stage_adjoint_dev(double coeff, double* out);
+    Error transposed_solve(const double* rhs, double* mu);
+    template <typename T>
+    Error kt_run(T* x, const T* b, bool f32, double tol, int& iters);
     int force_points_ = 0;  // boundary points of the "object" group (0: none)
     Error cuda(cudaError_t e, const char* what);
 
@@ -116,6 +146,9 @@ class Solver {
     bool timing_ = false;
     double poisson_ms_acc_ = 0.0;
     std::unique_ptr<DeviceState> d_;
+    std::unique_ptr<AdjointState> adj_;
+    int last_adj_iters_ = 0, adj_prev_iters_ = 8;
+    double last_adj_res_ = 0.0;
 };
 
 }  // namespace ho2d

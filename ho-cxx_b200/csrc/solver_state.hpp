@@ -1,0 +1,255 @@
+// solver_state.hpp -- device state of one solver instance and the helpers that build its
+// kernel arguments; shared by solver.cu (stage, step, Poisson) and adjoint_driver.cu.
+#pragma once
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "device.cuh"
+#include "fr_launch.hpp"
+#include "host_amg.hpp"
+#include "solver.hpp"
+
+namespace ho2d {
+
+// Device copy of one row-padded matrix (FP64 and FP32 values) and of one coarse level.
+struct EllBufs {
+    DeviceBuffer col, v64, v32;
+};
+struct LevelBufs {
+    EllBufs M, S, Q;
+    DeviceBuffer f, u;
+};
+
+// A captured Krylov solve and the parameters baked into it.
+struct SolveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int max_iter = -1;
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        max_iter = -1;
+    }
+    ~SolveGraph() { reset(); }
+};
+
+struct DeviceState {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+    // connectivity and boundary tables
+    DeviceBuffer face_nb, face_nijp, be_group, sw_p, sw_d, noslip, role, be_ijp;
+    DevBases<double> b64;
+    DevBases<float> b32;
+    // metrics: xxi, xeta, yxi, yeta, J, fA, fB, fJ, fAn
+    DeviceBuffer m64[9], m32[9];
+    bool have32 = false;
+    // boundary arrays (double)
+    DeviceBuffer bc_p, bc_nv, bc_pv, bc_d, bc_w, vjump, bc_adv, edge_y, bsrc;
+    // fields
+    DeviceBuffer omega, acc, psi64, rhs, rres;
+    DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
+    // Poisson operator and Krylov workspace
+    // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
+    DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
+    // matrix-free operator data: G11, G12, G22, fa, fb, nfa, nfb, minv (PoisGeom)
+    DeviceBuffer pg64[8], pg32[8], pcode, pscat;
+    std::vector<double> pg_host[8];  // kept for the FP32 copies made on demand
+    DeviceBuffer kv[10];  // r, rhat, p, v, s, t, ph, sh, x (inner), b (inner)
+    DeviceBuffer esum[4];  // element sums of r, v, p (two alternating buffers), N + 4 entries
+    DeviceBuffer ktv, ktg, kxtv, kxtg;  // face traces of the Krylov operand and of x
+    DeviceBuffer partials, counter, scalars;
+    KrylovScalars* h_sc = nullptr;
+    // two-level preconditioner: per coarse level the row-padded cycle operators M, S, Q
+    // (FP64 and FP32 values) and the level's f and u (sized for FP64, reused for FP32)
+    using EllBufs = ho2d::EllBufs;
+    using LevelBufs = ho2d::LevelBufs;
+    std::vector<std::unique_ptr<LevelBufs>> lev;
+    DeviceBuffer dense64, dense32;
+    Precond<double> pc64;
+    Precond<float> pc32;
+    SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
+    double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
+    DeviceBuffer l2flush;               // written between timed steps to evict L2
+    DeviceBuffer fcoef, fidx, fout;     // body-force coefficients, boundary indices, result
+
+    ~DeviceState() {
+        if (h_sc) cudaFreeHost(h_sc);
+        for (cudaEvent_t e : {ev0, ev1, evp0, evp1})
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// Device state of the discrete adjoint, allocated on first use.
+struct AdjointState {
+    bool ready = false;
+    // preconditioner of the transposed Poisson problem: column sums of A's blocks, and the
+    // coarse hierarchy of (P^T A P)^T
+    std::vector<std::unique_ptr<LevelBufs>> lev;
+    DeviceBuffer dense64, dense32, rowsumT64, rowsumT32;
+    Precond<double> pc64;
+    Precond<float> pc32;
+    // BiCGSTAB on A^T: x r rhat p v s t ph sh dir (sized for FP64), element sums, slots
+    DeviceBuffer kv[10];
+    DeviceBuffer f0, sv, sg, partials, counter, scalars;
+    DeviceBuffer res64, x32, b32;  // refinement: FP64 residual, FP32 correction and right-hand side
+    // stage adjoint: lam of k (in), of omega (out) and the intermediate arrays
+    DeviceBuffer lam_k, lw_out, lw_dir, lux, luy, lw_stage, lpsi_dir, lpsi, mu;
+    DeviceBuffer swv, swg, sU, spv, spg;  // incoming slots [N][4K] (boundary entries stay zero)
+    DeviceBuffer lbc_d, lbc_nv, lpv;      // boundary adjoints [N_eb][K]
+    // time loop: lam of omega, per-stage results, checkpoints and one segment of stages
+    DeviceBuffer lam, mus[4];
+    std::vector<std::unique_ptr<DeviceBuffer>> ckpt;
+    DeviceBuffer seg_w, seg_psi, wT, psiT;
+    int nsteps = -1, every = 1;
+    double t0 = 0.0;
+};
+
+namespace {
+
+template <typename T>
+DevBases<T> make_dev_bases(const Bases& B) {
+    DevBases<T> d;
+    std::memset(&d, 0, sizeof(d));
+    for (int i = 0; i < B.K * B.K; ++i) d.D[i] = T(B.D[i]);
+    for (int i = 0; i < B.K * 2; ++i) {
+        d.sbb[i] = T(B.sbb[i]);
+        d.sbgb[i] = T(B.sbgb[i]);
+        d.R[i] = T(B.R[i]);
+        d.gR[i] = T(B.gR[i]);
+    }
+    d.gp[0] = T(B.gp[0]);
+    d.gp[1] = T(B.gp[1]);
+    return d;
+}
+
+template <typename T>
+cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& h) {
+    cudaError_t e = buf.alloc(h.size() * sizeof(T));
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpy(buf.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <typename T>
+cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
+    std::vector<T> c(h.begin(), h.end());
+    return upload(buf, c);
+}
+
+inline cudaError_t upload_ell(DeviceState::EllBufs& b, const Ell& A) {
+    cudaError_t e;
+    if ((e = upload(b.col, A.col.empty() ? std::vector<int>{0} : A.col)) != cudaSuccess) return e;
+    if ((e = upload(b.v64, A.val.empty() ? std::vector<double>{0.0} : A.val)) != cudaSuccess) return e;
+    return upload_as<float>(b.v32, A.val.empty() ? std::vector<double>{0.0} : A.val);
+}
+
+// lanes per row for a row-padded matrix of width w: about w/2, a power of two in [4, 32]
+inline int lanes_for(int w) {
+    int g = 4;
+    while (g < 32 && 2 * g <= std::max(1, w / 2)) g *= 2;
+    return g;
+}
+
+template <typename TM>
+DevEll<TM> view(const DeviceState::EllBufs& b, const Ell& A, int g, bool f32) {
+    DevEll<TM> v;
+    v.n = A.n;
+    v.w = A.w;
+    v.g = g;
+    v.col = b.col.as<int>();
+    v.val = f32 ? (const TM*)b.v32.get() : (const TM*)b.v64.get();
+    return v;
+}
+
+
+template <typename T>
+FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
+    DeviceBuffer* mm = f32 ? d.m32 : d.m64;
+    FrGeom<T> g;
+    g.N = m.n_el;
+    g.n_eb = m.n_eb;
+    g.face_nb = d.face_nb.as<int>();
+    g.face_nijp = d.face_nijp.as<int>();
+    g.xxi = mm[0].as<T>();
+    g.xeta = mm[1].as<T>();
+    g.yxi = mm[2].as<T>();
+    g.yeta = mm[3].as<T>();
+    g.J = mm[4].as<T>();
+    g.fA = mm[5].as<T>();
+    g.fB = mm[6].as<T>();
+    g.fJ = mm[7].as<T>();
+    g.fAn = mm[8].as<T>();
+    g.be_group = d.be_group.as<int>();
+    g.sw_p = d.sw_p.as<int>();
+    g.sw_d = d.sw_d.as<int>();
+    g.noslip = d.noslip.as<int>();
+    return g;
+}
+
+template <typename T>
+MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
+    MfOp<T> op;
+    op.K = K;
+    op.g.N = m.n_el;
+    const DeviceBuffer* pg = f32 ? d.pg32 : d.pg64;
+    op.g.G11 = pg[0].as<T>();
+    op.g.G12 = pg[1].as<T>();
+    op.g.G22 = pg[2].as<T>();
+    op.g.fa = pg[3].as<T>();
+    op.g.fb = pg[4].as<T>();
+    op.g.nfa = pg[5].as<T>();
+    op.g.nfb = pg[6].as<T>();
+    op.g.minv = pg[7].as<T>();
+    op.g.code = d.pcode.as<int>();
+    op.g.scat = d.pscat.as<int>();
+    op.b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
+    op.dinv = f32 ? (const T*)d.dinv32.get() : (const T*)d.dinv64.get();
+    op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
+    op.bcol = d.bcol.as<int>();
+    return op;
+}
+
+template <typename T>
+BicgVectors<T> krylov_vectors(DeviceState& d, T* x, const T* b) {
+    BicgVectors<T> v;
+    v.x = x;
+    v.r = d.kv[0].as<T>();
+    v.rhat = d.kv[1].as<T>();
+    v.p = d.kv[2].as<T>();
+    v.v = d.kv[3].as<T>();
+    v.s = d.kv[4].as<T>();
+    v.t = d.kv[5].as<T>();
+    v.ph = d.kv[6].as<T>();
+    v.sh = d.kv[7].as<T>();
+    v.b = b;
+    v.tv = d.ktv.as<T>();
+    v.tg = d.ktg.as<T>();
+    v.xtv = d.kxtv.as<T>();
+    v.xtg = d.kxtg.as<T>();
+    v.er = d.esum[0].as<T>();
+    v.ev = d.esum[1].as<T>();
+    v.ep[0] = d.esum[2].as<T>();
+    v.ep[1] = d.esum[3].as<T>();
+    return v;
+}
+
+
+}  // namespace
+
+// Inside Solver members: return the first failing status.
+#define HO2D_TRY(expr)                 \
+    do {                               \
+        Error _e = (expr);             \
+        if (_e.code) return _e;        \
+    } while (0)
+#define HO2D_CUDA(call, what) HO2D_TRY(cuda((call), what))
+
+}  // namespace ho2d

@@ -133,6 +133,12 @@ class HO_2D:
         return out
 
     # -- controls and statistics
+    def get_boundary_points(self) -> np.ndarray:
+        """[N_eb][K][x, y] of the boundary flux points, in the boundary arrays' order."""
+        out = np.zeros((self.N_edges_boundary, self.Knod, 2))
+        self._check(self._lib.ho2d_get_boundary_points(self._h, out.size, capi.dptr(out)))
+        return out
+
     def set_precision(self, mode: int) -> None:
         self._check(self._lib.ho2d_set_precision(self._h, int(mode)))
 
@@ -176,6 +182,43 @@ class HO_2D:
         fx, fy = ctypes.c_double(), ctypes.c_double()
         self._check(self._lib.ho2d_get_forces(self._h, ctypes.byref(fx), ctypes.byref(fy)))
         return fx.value, fy.value
+
+    # -- discrete adjoint (no counterpart in the reference; ho2d.adjoint wraps it for torch)
+    def adjoint_forward(self, nsteps: int, ckpt_every: int = 25) -> None:
+        """nsteps time steps from the current state, keeping the vorticity every ckpt_every steps."""
+        self._check(self._lib.ho2d_adjoint_forward(self._h, int(nsteps), int(ckpt_every)))
+
+    def adjoint_backward(self, dJ_domegaT):
+        """(dJ/d omega0 [N_el][K][K], dJ/d BC_parl_vel [N_eb][K]) from dJ/d omega(T)."""
+        g = np.ascontiguousarray(dJ_domegaT, dtype=np.float64).ravel()
+        gw = np.zeros_like(g)
+        gpv = np.zeros(self.N_edges_boundary * self.Knod)
+        self._check(self._lib.ho2d_adjoint_backward(self._h, g.size, capi.dptr(g), capi.dptr(gw), gpv.size,
+                                                    capi.dptr(gpv)))
+        return gw.reshape(self.N_el, self.Knod, self.Knod), gpv.reshape(self.N_edges_boundary, self.Knod)
+
+    def stage_adjoint(self, coeff: float, lam_k):
+        """Adjoint of Euler_time_integrate(coeff) at the current state: (lam of the stage
+        input [N_el][K][K], lam of BC_parl_vel [N_eb][K]) from lam of k."""
+        lk = np.ascontiguousarray(lam_k, dtype=np.float64).ravel()
+        lw = np.zeros_like(lk)
+        lpv = np.zeros(self.N_edges_boundary * self.Knod)
+        self._check(self._lib.ho2d_stage_adjoint(self._h, float(coeff), lk.size, capi.dptr(lk), capi.dptr(lw),
+                                                 lpv.size, capi.dptr(lpv)))
+        return lw.reshape(self.N_el, self.Knod, self.Knod), lpv.reshape(self.N_edges_boundary, self.Knod)
+
+    def apply_poisson_transpose(self, x) -> np.ndarray:
+        """y = A^T x with the transposed matrix-free Poisson operator, FP64."""
+        a = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros_like(a)
+        self._check(self._lib.ho2d_apply_poisson_transpose(self._h, a.size, capi.dptr(a), capi.dptr(out)))
+        return out
+
+    def adjoint_stats(self):
+        """(iterations, relative residual) of the last transposed Poisson solve."""
+        it, res = ctypes.c_int32(), ctypes.c_double()
+        self._check(self._lib.ho2d_adjoint_stats(self._h, ctypes.byref(it), ctypes.byref(res)))
+        return it.value, res.value
 
     def launch_count(self) -> int:
         n = ctypes.c_int64()

@@ -53,6 +53,12 @@ SIGNATURES = {
     "ho2d_apply_poisson": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_apply_poisson_noalloc": (ctypes.c_int, [_P, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "ho2d_get_forces": (ctypes.c_int, [_P, _DP, _DP]),
+    "ho2d_get_boundary_points": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_adjoint_forward": (ctypes.c_int, [_P, _I, _I]),
+    "ho2d_adjoint_backward": (ctypes.c_int, [_P, _I, _DP, _DP, _I, _DP]),
+    "ho2d_stage_adjoint": (ctypes.c_int, [_P, _D, _I, _DP, _DP, _I, _DP]),
+    "ho2d_apply_poisson_transpose": (ctypes.c_int, [_P, _I, _DP, _DP]),
+    "ho2d_adjoint_stats": (ctypes.c_int, [_P, _IP, _DP]),
     "ho2d_last_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "ho2d_last_error": (ctypes.c_char_p, [_P]),
 }

@@ -265,6 +265,29 @@ def viscous_dt(mesh: QuadMesh, knod: int, reyn: float, c: float = 1.5) -> float:
 
 
 # Named cases: (mesh builder, problem_type, Re, velocity scale for the CFL dt)
+def sine_spectrum(xy: np.ndarray, seed: int, modes: int = 4) -> np.ndarray:
+    """Seeded smooth cavity vorticity: sum_{m,n=1..modes} c_mn sin(m pi x) sin(n pi y) with
+    c_mn ~ N(0, 1) / (m^2 + n^2), evaluated at points xy[..., 2] of the unit square (the
+    sine modes vanish on its walls)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = np.arange(1, modes + 1)
+    c = rng.standard_normal((modes, modes)) / (m[:, None] ** 2 + m[None, :] ** 2)
+    sx = np.sin(np.pi * xy[..., 0, None] * m)  # [..., modes]
+    sy = np.sin(np.pi * xy[..., 1, None] * m)
+    return np.einsum("...m,...n,mn->...", sx, sy, c)
+
+
+def lid_coefficients(seed: int, modes: int = 4, sigma: float = 0.05) -> np.ndarray:
+    """a_m ~ N(0, sigma^2) of the lid profile u(x) = 1 + sum_m a_m sin(m pi x)."""
+    return np.random.Generator(np.random.PCG64(seed)).normal(0.0, sigma, modes)
+
+
+def lid_velocity(x: np.ndarray, a: np.ndarray) -> np.ndarray:
+    """u(x) = 1 + sum_m a_m sin(m pi x)."""
+    m = np.arange(1, len(a) + 1)
+    return 1.0 + np.sin(np.pi * np.asarray(x)[..., None] * m) @ np.asarray(a)
+
+
 def make_case(name: str, outdir: str, knod: int | None = None, steps: int = 10, dt: float | None = None,
               **kw) -> str:
     """Write ``<outdir>/input.dat`` and its mesh for a named synthetic case; returns the input path.

@@ -107,6 +107,10 @@ int ho2d_set_boundary(ho2d_solver* handle, int32_t which, int32_t len, const dou
 /* Solution-point coordinates [el][j][i][x,y] (like getsolnpts_d, src/HO_2D.cpp:3946-3980),
  * len = 2*N_el*Knod*Knod. */
 int ho2d_get_solution_points(ho2d_solver* handle, int32_t len, double* buf);
+/* No counterpart in the reference. Coordinates of the boundary flux points [N_eb][Knod][x,y]
+ * in the order of the boundary-edge arrays (ho2d_get_boundary), len = 2*N_eb*Knod: the
+ * points where BC_parl_vel and the other boundary arrays live. */
+int ho2d_get_boundary_points(ho2d_solver* handle, int32_t len, double* buf);
 
 /* HO2D_FP64 (default), HO2D_MIXED or HO2D_MIXED_KRYLOV; may be called before or after
  * ho2d_setup. */
@@ -156,6 +160,35 @@ int ho2d_apply_poisson_noalloc(ho2d_solver* handle, int32_t len, const double* x
  * nu omega t (Koumoutsakos & Leonard, JFM 1995). Drag and lift coefficients are 2 F / (U^2 D).
  * HO2D_ERR_ARG when the mesh has no "object" group. */
 int ho2d_get_forces(ho2d_solver* handle, double* fx, double* fy);
+/* ---- Discrete adjoint. No counterpart in the reference: gradients of a scalar
+ * J(omega(T)) of the vorticity after nsteps time steps with respect to the initial
+ * vorticity and to BC_parl_vel (the wall velocity of no-slip walls, constant in time),
+ * by the transpose of the discrete time loop of solve_advection_diffusion
+ * (src/HO_2D.cpp:1465-1531): stage kernels run backwards, a transposed Poisson solve per
+ * stage. Advection type 1; precision HO2D_FP64, or HO2D_MIXED_KRYLOV, whose forward and
+ * transposed Poisson solves are FP32 Krylov inside FP64 refinement (HO2D_MIXED is
+ * rejected with HO2D_ERR_UNSUPPORTED). */
+/* Runs nsteps time steps from the current state (as ho2d_step) and keeps the vorticity
+ * every ckpt_every steps for the backward sweep. */
+int ho2d_adjoint_forward(ho2d_solver* handle, int32_t nsteps, int32_t ckpt_every);
+/* From dJ/d(omega(T)) (len = N_el*Knod*Knod) returns dJ/d(omega) at the start of the last
+ * ho2d_adjoint_forward (same length) and dJ/d(BC_parl_vel) (len_pv = N_eb*Knod; 0 with a
+ * null buffer skips it). Each segment of ckpt_every steps is recomputed from its
+ * checkpoint; afterwards the solver is back at the state and time reached by the forward
+ * sweep. */
+int ho2d_adjoint_backward(ho2d_solver* handle, int32_t len, const double* dJ_domegaT, double* grad_omega0,
+                          int32_t len_pv, double* grad_parl_vel);
+/* Adjoint of one ho2d_stage(coeff) at the current state: lam_k, the adjoint of the
+ * stage's k (len = N_el*Knod*Knod), to lam_w, the adjoint of the stage input, and lam_pv,
+ * the adjoint of BC_parl_vel (len_pv = N_eb*Knod, or 0 with a null buffer). */
+int ho2d_stage_adjoint(ho2d_solver* handle, double coeff, int32_t len, const double* lam_k, double* lam_w,
+                       int32_t len_pv, double* lam_pv);
+/* y = A^T x in FP64 with the transposed matrix-free Poisson operator; len = N_el*Knod*Knod. */
+int ho2d_apply_poisson_transpose(ho2d_solver* handle, int32_t len, const double* x, double* y);
+/* Krylov iterations (summed over refinement sweeps) and final relative residual of the
+ * last transposed Poisson solve. */
+int ho2d_adjoint_stats(ho2d_solver* handle, int32_t* iterations, double* rel_residual);
+
 /* Total number of kernel launches this handle has issued since it was created. */
 int ho2d_last_launch_count(ho2d_solver* handle, int64_t* launches);
 /* Text of the last error on this handle ("" if none). The pointer stays valid until the
