@@ -46,6 +46,13 @@ def parse():
     ap.add_argument("--cpu-stages", type=int, default=1, help="RK stages timed for the CPU baseline sample")
     ap.add_argument("--t0", type=float, default=1.5, help="start time inside the pulsatile inflow cycle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="the differentiation case instead of the step benchmark: lid-driven cavity, K=5, Re=1000, "
+                         "RK4; adjoint gradient (FP64 and mixed) against central differences")
+    ap.add_argument("--adj-n", type=int, default=64, help="cavity elements per side (differentiation case)")
+    ap.add_argument("--adj-steps", type=int, default=500)
+    ap.add_argument("--adj-ckpt", type=int, default=25)
+    ap.add_argument("--adj-dirs", type=int, default=20)
     return ap.parse_args()
 
 
@@ -363,11 +370,43 @@ def run_ours(args, rank, world, local, phys):
     dist.close()
 
 
+def run_adjoint(args, rank):
+    """One JSON line: the adjoint gradient's largest relative error against central
+    differences over the seeded directions (FP64 headline, mixed beside it), and the
+    wall time of the forward and backward sweeps."""
+    from ho2d import adjoint_case
+
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        r = adjoint_case.run(tmp, n=args.adj_n, knod=args.knod, steps=args.adj_steps, ckpt=args.adj_ckpt,
+                             ndir=args.adj_dirs)
+    f = r["fp64"]
+    line = {"metric": "adjoint gradient relative error vs central differences (h=1e-6)",
+            "value": f["max_rel_error"], "unit": "relative error", "n_gpus": 1, "higher_is_better": False,
+            "dtype": "f64", "data": "synthetic (seeded sine-mode vorticity, seeded lid profile)",
+            "config": {"workload": f"lid-driven cavity {args.adj_n}x{args.adj_n}, K={args.knod}, Re=1000, RK4, "
+                                   f"{args.adj_steps} steps, checkpoints every {args.adj_ckpt}, "
+                                   f"{args.adj_dirs} directions in (omega0, lid coefficients)",
+                       "n_el": r["n_el"], "dof": r["dof"], "dt": r["dt"]},
+            "gradient_s": f["forward_s"] + f["backward_s"],
+            "gradient_over_forward": (f["forward_s"] + f["backward_s"]) / max(f["forward_s"], 1e-12),
+            "adjoint_state_bytes": r["adjoint_state_bytes"], "fd_seconds": r["fd_seconds"],
+            "fp64": f, "mixed": r["mixed"]}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.adjoint:
+        visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = [d for d in visible.split(",") if d.strip()] if visible else None
+        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local % len(devs)] if devs else str(local)
+        run_adjoint(args, rank)
         return
     # one GPU per rank: each replica sees only its own device
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")

@@ -1,0 +1,132 @@
+"""The differentiation case: gradient of a final-time vorticity misfit by the discrete
+adjoint, checked against central finite differences on the device.
+
+Lid-driven cavity, n x n uniform quads (default 64 x 64), K = 5, Re = 1000, RK4. The
+initial vorticity is the seeded sine spectrum of ``meshgen.sine_spectrum`` (seed 4); the
+lid is u(x) = 1 + sum_{m=1..4} a_m sin(m pi x) with a_m ~ N(0, 0.05) (seed 41);
+J = 0.5 ||omega(T) - omega_target||^2 with omega_target = omega(T) of a run from the
+seed-42 spectrum under the same lid. The gradient with respect to (omega0, a) comes from
+the adjoint (checkpoints every ``ckpt`` steps); it is checked along ``ndir`` seeded
+directions (seed 43) against (J(x + h d) - J(x - h d)) / 2h of the FP64 forward. All
+fields are synthetic: no dataset is involved.
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import FP64, MIXED_KRYLOV, HO_2D, capi, meshgen
+
+
+def cavity_dt(n: int, knod: int, u_max: float = 1.2, cfl: float = 0.5) -> float:
+    """dt = cfl h / (u_max K^2), h = 1/n: the CFL-0.5 step of the benchmark cases."""
+    return cfl * (1.0 / n) / (u_max * knod * knod)
+
+
+class DifferentiationCase:
+    def __init__(self, workdir: str, n: int = 64, knod: int = 5, reyn: float = 1000.0, steps: int = 500,
+                 tol: float = 1e-13, max_iter: int = 2000):
+        self.n, self.knod, self.reyn, self.steps = n, knod, reyn, steps
+        self.dt = cavity_dt(n, knod)
+        self.inp = meshgen.make_case(f"cavity{n}", workdir, knod=knod, steps=steps, dt=self.dt, reyn=reyn)
+        self.tol, self.max_iter = tol, max_iter
+        self.s = self.solver(FP64)
+        s = self.s
+        xy = s.getsolnpts_d()
+        bp = s.get_boundary_points()
+        self.top = s.get_boundary(capi.BC_PARL_VEL) == -1.0  # BC_parl_vel = -1 on the lid (problem type 1)
+        self.bx = bp[..., 0]
+        self.w0 = meshgen.sine_spectrum(xy, seed=4)
+        self.a = meshgen.lid_coefficients(seed=41)
+        m = np.arange(1, len(self.a) + 1)
+        # d BC_parl_vel / d a_m on the lid (BC_parl_vel = -u there)
+        self.dpv_da = np.where(self.top[..., None], -np.sin(np.pi * self.bx[..., None] * m), 0.0)
+        self.target = self.run(s, meshgen.sine_spectrum(xy, seed=42), self.a)
+
+    def solver(self, precision: int) -> HO_2D:
+        s = HO_2D()
+        s.read_input_file(self.inp)
+        s.set_precision(precision)
+        s.set_poisson_tolerance(self.tol, self.max_iter)
+        s.setup()
+        return s
+
+    def pv(self, a) -> np.ndarray:
+        return np.where(self.top, -meshgen.lid_velocity(self.bx, a), 0.0)
+
+    def _start(self, s: HO_2D, w0, a) -> None:
+        s.set_time(0.0)
+        s.set_boundary(capi.BC_PARL_VEL, self.pv(a))
+        s.setsolnvort_d(w0)
+
+    def run(self, s: HO_2D, w0, a) -> np.ndarray:
+        self._start(s, w0, a)
+        s.solve_advection_diffusion(self.steps)
+        return s.getallvorts_d()
+
+    def J(self, w0, a) -> float:
+        return 0.5 * float(np.sum((self.run(self.s, w0, a) - self.target) ** 2))
+
+    def gradient(self, precision: int, ckpt: int) -> dict:
+        """Adjoint gradient (dJ/d omega0, dJ/d a) and the wall time of its two sweeps."""
+        s = self.s if precision == FP64 else self.solver(precision)
+        self._start(s, self.w0, self.a)
+        l0 = s.launch_count()
+        t0 = time.perf_counter()
+        s.adjoint_forward(self.steps, ckpt)
+        t1 = time.perf_counter()
+        wT = s.getallvorts_d()
+        gw, gpv = s.adjoint_backward(wT - self.target)
+        t2 = time.perf_counter()
+        it, res = s.adjoint_stats()
+        ga = np.einsum("ekm,ek->m", self.dpv_da, gpv)
+        return dict(gw=gw, ga=ga, J=0.5 * float(np.sum((wT - self.target) ** 2)), forward_s=t1 - t0,
+                    backward_s=t2 - t1, launches=s.launch_count() - l0, last_transposed_iterations=it,
+                    last_transposed_residual=res)
+
+    def directions(self, ndir: int, seed: int = 43):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        return [(rng.standard_normal(self.w0.shape), rng.standard_normal(self.a.shape)) for _ in range(ndir)]
+
+    def finite_differences(self, dirs, h: float = 1e-6):
+        out = []
+        for dw, da in dirs:
+            jp = self.J(self.w0 + h * dw, self.a + h * da)
+            jm = self.J(self.w0 - h * dw, self.a - h * da)
+            out.append((jp - jm) / (2.0 * h))
+        return np.array(out)
+
+    @staticmethod
+    def directional(g: dict, dirs) -> np.ndarray:
+        return np.array([float(np.vdot(g["gw"], dw) + np.vdot(g["ga"], da)) for dw, da in dirs])
+
+    def state_bytes(self, ckpt: int) -> int:
+        """Device bytes the adjoint keeps for the time loop: FP64 checkpoints and one
+        segment of RK4 stage inputs and streamfunctions."""
+        nv = self.s.N_el * self.knod ** 2
+        nck = (self.steps + ckpt - 1) // ckpt
+        return 8 * nv * (nck + 2 * ckpt * 4)
+
+
+def run(workdir: str, n: int = 64, knod: int = 5, steps: int = 500, ckpt: int = 25, ndir: int = 20,
+        h: float = 1e-6) -> dict:
+    """FP64 and mixed-precision adjoint gradients of the case against FP64 central
+    differences; returns the errors and timings."""
+    c = DifferentiationCase(workdir, n=n, knod=knod, steps=steps)
+    dirs = c.directions(ndir)
+    t0 = time.perf_counter()
+    fd = c.finite_differences(dirs, h)
+    fd_s = time.perf_counter() - t0
+    out = {"n_el": c.s.N_el, "dof": c.s.N_el * knod * knod, "dt": c.dt, "steps": steps, "ckpt_every": ckpt,
+           "directions": ndir, "h": h, "fd_seconds": fd_s, "adjoint_state_bytes": c.state_bytes(ckpt)}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED_KRYLOV)):
+        g = c.gradient(prec, ckpt)
+        ad = c.directional(g, dirs)
+        err = np.abs(ad - fd) / np.maximum(np.abs(fd), 1e-300)
+        out[name] = {"max_rel_error": float(err.max()), "median_rel_error": float(np.median(err)),
+                     "J": g["J"], "forward_s": g["forward_s"], "backward_s": g["backward_s"],
+                     "launches": g["launches"], "last_transposed_iterations": g["last_transposed_iterations"],
+                     "grad_lid": [float(x) for x in g["ga"]]}
+    return out
