@@ -221,13 +221,21 @@ __device__ void kt_finish(int op, double a, double b, KrylovScalars* sc, int max
     }
 }
 
+// One vector step of the iteration. Every CTA reads `done` and `s_exit` before any CTA
+// arrives at the counter, so the last CTA may change them. Inside a captured solve the XR
+// step sets the condition of the graph's while node (iterate while not done); a body
+// execution either increments `it` (the XR step sets done at max_iter) or finds done set
+// and clears the condition, so the device loop always ends.
 template <typename T>
 __global__ void __launch_bounds__(kKtThreads) k_kt_vec(int op, size_t n, TVectors<T> v, const T* __restrict__ rb,
                                                         const T* __restrict__ ry, T* __restrict__ rr, TReduce red,
-                                                        int max_iter) {
+                                                        int max_iter, cudaGraphConditionalHandle h, int has_handle) {
     KrylovScalars* sc = red.sc;
     if (op != KT_INIT && op != KT_RES) {
-        if (sc->done) return;
+        if (sc->done) {
+            if (op == KT_XR && has_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+            return;
+        }
         if (op == KT_OMEGA && sc->s_exit) return;
     }
     const int s_exit = sc->s_exit;
@@ -311,12 +319,18 @@ __global__ void __launch_bounds__(kKtThreads) k_kt_vec(int op, size_t n, TVector
     }
     *red.counter = 0u;
     kt_finish(op, a, b, sc, max_iter);
+    if (op == KT_XR && has_handle) cudaGraphSetConditional(h, sc->done ? 0u : 1u);
+}
+
+__global__ void k_kt_set_loop(const KrylovScalars* sc, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
 }
 
 template <typename T>
 cudaError_t kt_vec(int op, size_t n, const TVectors<T>& v, const TReduce& r, int max_iter, cudaStream_t s,
-                   const T* rb = nullptr, const T* ry = nullptr, T* rr = nullptr) {
-    k_kt_vec<T><<<kKtGrid, kKtThreads, 0, s>>>(op, n, v, rb, ry, rr, r, max_iter);
+                   const T* rb = nullptr, const T* ry = nullptr, T* rr = nullptr,
+                   cudaGraphConditionalHandle h = cudaGraphConditionalHandle(), int has_handle = 0) {
+    k_kt_vec<T><<<kKtGrid, kKtThreads, 0, s>>>(op, n, v, rb, ry, rr, r, max_iter, h, has_handle);
     return cudaGetLastError();
 }
 
@@ -394,8 +408,9 @@ cudaError_t kt_init(size_t n, const TVectors<T>& v, const TReduce& r, cudaStream
 }
 
 template <typename T>
-cudaError_t kt_iteration(int K, const FrGeom<T>& g, const DevBases<T>& b, const TVectors<T>& v, const TPrecond<T>& pc,
-                         const TReduce& r, int max_iter, cudaStream_t s) {
+cudaError_t kt_iteration_impl(int K, const FrGeom<T>& g, const DevBases<T>& b, const TVectors<T>& v,
+                              const TPrecond<T>& pc, const TReduce& r, int max_iter, cudaGraphConditionalHandle h,
+                              int has_handle, cudaStream_t s) {
     const int N = g.N;
     const size_t n = (size_t)N * K * K;
     cudaError_t e;
@@ -406,8 +421,56 @@ cudaError_t kt_iteration(int K, const FrGeom<T>& g, const DevBases<T>& b, const 
     if ((e = pc_transpose_apply<T>(K, N, pc, v.s, v.sh, v.f0, r.sc, 1, s)) != cudaSuccess) return e;
     if ((e = poisson_transpose<T>(K, g, b, v.sh, v.t, v.dir, v.sv, v.sg, r.sc, 1, s)) != cudaSuccess) return e;
     if ((e = kt_vec<T>(KT_OMEGA, n, v, r, max_iter, s)) != cudaSuccess) return e;
-    if ((e = kt_vec<T>(KT_XR, n, v, r, max_iter, s)) != cudaSuccess) return e;
+    if ((e = kt_vec<T>(KT_XR, n, v, r, max_iter, s, nullptr, nullptr, nullptr, h, has_handle)) != cudaSuccess)
+        return e;
     return kt_vec<T>(KT_P, n, v, r, max_iter, s);
+}
+
+template <typename T>
+cudaError_t kt_iteration(int K, const FrGeom<T>& g, const DevBases<T>& b, const TVectors<T>& v, const TPrecond<T>& pc,
+                         const TReduce& r, int max_iter, cudaStream_t s) {
+    return kt_iteration_impl<T>(K, g, b, v, pc, r, max_iter, cudaGraphConditionalHandle(), 0, s);
+}
+
+// A whole solve as a CUDA graph: init, then a while node whose body is one iteration.
+template <typename T>
+cudaError_t kt_capture_solve(int K, const FrGeom<T>& g, const DevBases<T>& b, const TVectors<T>& v,
+                             const TPrecond<T>& pc, const TReduce& r, int max_iter, cudaStream_t s,
+                             cudaGraph_t* graph_out) {
+    const size_t n = (size_t)g.N * K * K;
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaGraphCreate(&gr, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle h;
+    if ((e = cudaGraphConditionalHandleCreate(&h, gr, 0, 0)) != cudaSuccess) return e;
+    if ((e = cudaStreamBeginCaptureToGraph(s, gr, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    kt_vec<T>(KT_INIT, n, v, r, max_iter, s);
+    k_kt_set_loop<<<1, 1, 0, s>>>(r.sc, h);
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t cg = nullptr;
+    if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &ndeps)) != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    if ((e = cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp)) != cudaSuccess) return e;
+    if ((e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+        return e;
+    if ((e = cudaStreamEndCapture(s, &gr)) != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    kt_iteration_impl<T>(K, g, b, v, pc, r, max_iter, h, 1, s);
+    if ((e = cudaStreamEndCapture(s, &body)) != cudaSuccess) return e;
+    *graph_out = gr;
+    return cudaGetLastError();
 }
 
 template <typename T>
@@ -447,6 +510,8 @@ template cudaError_t launch_velocity_adjoint<double>(int, const FrGeom<double>&,
     template cudaError_t kt_iteration<T>(int, const FrGeom<T>&, const DevBases<T>&, const TVectors<T>&,          \
                                          const TPrecond<T>&, const TReduce&, int, cudaStream_t);                 \
     template int kt_launches_per_iteration<T>(const TPrecond<T>&);                                               \
+    template cudaError_t kt_capture_solve<T>(int, const FrGeom<T>&, const DevBases<T>&, const TVectors<T>&,      \
+                                             const TPrecond<T>&, const TReduce&, int, cudaStream_t, cudaGraph_t*);  \
     template cudaError_t kt_residual<T>(size_t, const T*, const T*, T*, const TReduce&, cudaStream_t);
 
 HO2D_INSTANTIATE_ADJ(double)

@@ -183,6 +183,26 @@ Error Solver::kt_run(T* x, const T* b, bool f32, double tol, int& iters) {
     HO2D_CUDA(cudaMemsetAsync(a.sg.get(), 0, a.sg.bytes(), d.stream), "memset");
     d.h_sc->tol = tol;  // the stream is idle: the last read of h_sc was synchronised
     HO2D_CUDA(cudaMemcpyAsync(&red.sc->tol, &d.h_sc->tol, sizeof(double), cudaMemcpyHostToDevice, d.stream), "tol");
+    if (use_graphs_) {
+        // one launch of the captured solve (init and a device-side while loop); the graph
+        // bakes in the operands, so it is recaptured when they change
+        const int gi = f32 ? 1 : 0;
+        SolveGraph& sg = a.graph[gi];
+        if (!sg.exec || sg.max_iter != max_iter_ || a.graph_x[gi] != (const void*)x || a.graph_b[gi] != (const void*)b) {
+            sg.reset();
+            HO2D_CUDA(kt_capture_solve<T>(K, g, bb, v, pc, red, max_iter_, d.stream, &sg.graph), "graph capture");
+            HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
+            sg.max_iter = max_iter_;
+            a.graph_x[gi] = x;
+            a.graph_b[gi] = b;
+        }
+        HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
+        HO2D_CUDA(cudaMemcpyAsync(d.h_sc, red.sc, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream), "poll");
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "poll");
+        iters = d.h_sc->it;
+        launches_ += 2 + (int64_t)iters * kt_launches_per_iteration<T>(pc);
+        return {0, ""};
+    }
     HO2D_CUDA(kt_init<T>(n, v, red, d.stream), "transposed init");
     launches_ += 1;
     // batches of iterations between polls of the done flag; an iteration enqueued after

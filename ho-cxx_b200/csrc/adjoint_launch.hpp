@@ -63,6 +63,11 @@ cudaError_t kt_iteration(int K, const FrGeom<T>& g, const DevBases<T>& b, const 
                          const TReduce& r, int max_iter, cudaStream_t s);
 template <typename T>
 int kt_launches_per_iteration(const TPrecond<T>& pc);
+// a whole solve (init + device-side while loop of iterations) as a CUDA graph
+template <typename T>
+cudaError_t kt_capture_solve(int K, const FrGeom<T>& g, const DevBases<T>& b, const TVectors<T>& v,
+                             const TPrecond<T>& pc, const TReduce& r, int max_iter, cudaStream_t s,
+                             cudaGraph_t* graph_out);
 // r = b - y with ||r||^2 -> sc->rnorm2 and ||b||^2 -> sc->bnorm2
 template <typename T>
 cudaError_t kt_residual(size_t n, const T* b, const T* y, T* r, const TReduce& rr, cudaStream_t s);

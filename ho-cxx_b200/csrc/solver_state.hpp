@@ -101,6 +101,9 @@ struct AdjointState {
     DeviceBuffer kv[10];
     DeviceBuffer f0, sv, sg, partials, counter, scalars;
     DeviceBuffer res64, x32, b32;  // refinement: FP64 residual, FP32 correction and right-hand side
+    SolveGraph graph[2];           // captured transposed solves (FP64, FP32) and their operands
+    const void* graph_x[2] = {nullptr, nullptr};
+    const void* graph_b[2] = {nullptr, nullptr};
     // stage adjoint: lam of k (in), of omega (out) and the intermediate arrays
     DeviceBuffer lam_k, lw_out, lw_dir, lux, luy, lw_stage, lpsi_dir, lpsi, mu;
     DeviceBuffer swv, swg, sU, spv, spg;  // incoming slots [N][4K] (boundary entries stay zero)
