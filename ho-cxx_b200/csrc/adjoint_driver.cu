@@ -324,6 +324,7 @@ Error Solver::stage_adjoint_dev(double coeff, double* out) {
 
 static Error adjoint_supported(const Input& in, bool stage32) {
     if (in.adv_type != 1) return {4, "the adjoint is implemented for advection type 1"};
+    if (in.problem_type == 11) return {4, "the adjoint does not cover hybrid runs (problem type 11)"};
     if (stage32) return {4, "the adjoint needs the FP64 stage: precision HO2D_FP64 or HO2D_MIXED_KRYLOV"};
     return {0, ""};
 }

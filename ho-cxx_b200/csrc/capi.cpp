@@ -237,6 +237,101 @@ int ho2d_get_forces(ho2d_solver* h, double* fx, double* fy) {
     return guarded(h, [&]() { return h->s.get_forces(fx, fy); });
 }
 
+int ho2d_set_defaults(ho2d_solver* h) {
+    return guarded(h, [&]() -> ho2d::Error {
+        h->s.set_defaults();
+        return {0, ""};
+    });
+}
+
+int ho2d_enable_hybrid(ho2d_solver* h) {
+    return guarded(h, [&]() -> ho2d::Error {
+        h->s.enable_hybrid();
+        return {0, ""};
+    });
+}
+
+int ho2d_set_elemorder(ho2d_solver* h, int32_t knod) {
+    return guarded(h, [&]() { return h->s.set_elemorder(knod); });
+}
+
+int ho2d_load_mesh_arrays(ho2d_solver* h, int32_t iorder, int32_t nxy, const double* xy, int32_t nidx,
+                          const int32_t* idx, int32_t nwall, const int32_t* idxwall, int32_t nopen,
+                          const int32_t* idxopen) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!xy || !idx || (nwall > 0 && !idxwall) || (nopen > 0 && !idxopen)) return {HO2D_ERR_ARG, "null buffer"};
+        return h->s.load_mesh_arrays(iorder, nxy, xy, nidx, idx, nwall, idxwall, nopen, idxopen);
+    });
+}
+
+int ho2d_load_inout_arrays(ho2d_solver* h, int32_t ninval, const double* velin, int32_t nin, const int32_t* idxin,
+                           int32_t noutval, const double* velout, int32_t nout, const int32_t* idxout) {
+    return guarded(h, [&]() {
+        return h->s.load_inout_arrays(ninval, velin, nin, idxin, noutval, velout, nout, idxout);
+    });
+}
+
+int ho2d_process_mesh_input(ho2d_solver* h) {
+    return guarded(h, [&]() { return h->s.process_mesh_input(); });
+}
+
+int ho2d_get_solution_areas(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.get_solution_areas(buf);
+    });
+}
+
+int ho2d_get_open_point_count(ho2d_solver* h, int32_t* len) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!len) return {HO2D_ERR_ARG, "null output"};
+        *len = h->s.open_point_count();
+        return {0, ""};
+    });
+}
+
+int ho2d_get_open_points(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, (size_t)h->s.open_point_count(), buf);
+        return e.code ? e : h->s.get_open_points(buf);
+    });
+}
+
+int ho2d_set_open_velocities(ho2d_solver* h, int32_t len, const double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, (size_t)h->s.open_point_count(), buf);
+        return e.code ? e : h->s.set_open_velocities(buf);
+    });
+}
+
+int ho2d_set_open_vorticity(ho2d_solver* h, int32_t len, const double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, (size_t)h->s.open_point_count() / 2, buf);
+        return e.code ? e : h->s.set_open_vorticity(buf);
+    });
+}
+
+int ho2d_set_ptog_weights(ho2d_solver* h, int32_t len, const double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, nvol(h), buf);
+        return e.code ? e : h->s.set_ptog_weights(buf);
+    });
+}
+
+int ho2d_get_hoquad_weights(ho2d_solver* h, int32_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        ho2d::Error e = check_len(h, len, (size_t)h->s.knod() * h->s.knod(), buf);
+        return e.code ? e : h->s.get_hoquad_weights(buf);
+    });
+}
+
+int ho2d_clean_up(ho2d_solver* h) {
+    return guarded(h, [&]() -> ho2d::Error {
+        h->s.release();
+        return {0, ""};
+    });
+}
+
 int ho2d_adjoint_forward(ho2d_solver* h, int32_t nsteps, int32_t ckpt_every) {
     return guarded(h, [&]() -> ho2d::Error {
         if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};

@@ -348,11 +348,13 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) poisson_rhs_kernel(int N, c
     rhs[p] = r;
 }
 
-// Time-dependent BC refresh (problem types 2 and 3) and the flip of normal velocities
-// and Neumann vorticity BCs into the local h direction, one thread per edge point.
+// Time-dependent BC refresh (problem types 2 and 3; hybrid runs, type 11) and the flip of
+// normal velocities and Neumann vorticity BCs into the local h direction, one thread per
+// edge point. Roles: 1 inlet, 2 top, 3 bottom, 4 object; hybrid 5 open, 6 wall, 7 inlet.
 __global__ void bc_update_kernel(int n_eb, int K, int ptype, double tc, double y_min, double y_max,
                                  const int* __restrict__ role, const int* __restrict__ be_ijp,
-                                 const int* __restrict__ sw_d, const double* __restrict__ edge_y, BcArrays bc) {
+                                 const int* __restrict__ sw_d, const double* __restrict__ edge_y, BcArrays bc,
+                                 HybridBc hb) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n_eb * K) return;
     const int e = idx / K;
@@ -379,6 +381,19 @@ __global__ void bc_update_kernel(int n_eb, int K, int ptype, double tc, double y
             bc.bc_pv[idx] = tc;
         } else if (r == 4) {
             bc.bc_p[idx] = tc * 0.5 * (y_max - y_min);
+        }
+    } else if (ptype == 11) {  // src/HO_2D.cpp:2104-2191
+        if (r == 5) {
+            const double pv = -(hb.fac1 * hb.vp0[idx] + hb.fac2 * hb.vp1[idx]);
+            bc.bc_nv[idx] = -(hb.fac1 * hb.vn0[idx] + hb.fac2 * hb.vn1[idx]);
+            bc.bc_pv[idx] = pv;
+            bc.bc_p[idx] = pv;
+            bc.bc_d[idx] = hb.fac1 * hb.w0[idx] + hb.fac2 * hb.w1[idx];
+        } else if (r == 6) {
+            bc.bc_nv[idx] = 0.0;
+            bc.bc_pv[idx] = 0.0;
+        } else if (r == 7) {
+            bc.bc_nv[idx] = -hb.inlet_nv[e];
         }
     }
     const double sign = 2.0 * (be_ijp[e] % 2) - 1.0;
@@ -437,13 +452,42 @@ cudaError_t launch_poisson_rhs(int K, int N, const int* face_nb, const T* w, con
 
 cudaError_t launch_bc_update(int n_eb, int K, int ptype, double tc, double y_min, double y_max, const int* role,
                              const int* be_ijp, const int* sw_d, const double* edge_y, const BcArrays& bc,
-                             cudaStream_t s) {
+                             const HybridBc& hb, cudaStream_t s) {
     const int n = n_eb * K;
     if (n == 0) return cudaSuccess;
+    if (ptype == 11 && !(hb.vn0 && hb.vn1 && hb.vp0 && hb.vp1 && hb.w0 && hb.w1 && hb.inlet_nv))
+        return cudaErrorInvalidValue;
     bc_update_kernel<<<(n + 127) / 128, 128, 0, s>>>(n_eb, K, ptype, tc, y_min, y_max, role, be_ijp, sw_d, edge_y,
-                                                     bc);
+                                                     bc, hb);
     return cudaGetLastError();
 }
+
+template <typename T>
+__global__ void hybrid_blend_kernel(size_t n, double* __restrict__ omega, T* __restrict__ w_stage,
+                                    const double* __restrict__ wgt, const double* __restrict__ v0,
+                                    const double* __restrict__ v1, double fac1, double fac2) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double w = wgt[i];
+        const double om = (1.0 - w) * omega[i] + w * (fac1 * v0[i] + fac2 * v1[i]);
+        omega[i] = om;
+        if (w_stage) w_stage[i] = T(om);
+    }
+}
+
+template <typename T>
+cudaError_t launch_hybrid_blend(size_t n, double* omega, T* w_stage, const double* wgt, const double* v0,
+                                const double* v1, double fac1, double fac2, cudaStream_t s) {
+    const size_t b = (n + 255) / 256;
+    hybrid_blend_kernel<T><<<(unsigned)(b > 1184 ? 1184 : (b < 1 ? 1 : b)), 256, 0, s>>>(n, omega, w_stage, wgt, v0, v1,
+                                                                                        fac1, fac2);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_hybrid_blend<double>(size_t, double*, double*, const double*, const double*,
+                                                 const double*, double, double, cudaStream_t);
+template cudaError_t launch_hybrid_blend<float>(size_t, double*, float*, const double*, const double*, const double*,
+                                                double, double, cudaStream_t);
 
 #define HO2D_INSTANTIATE_FR(T)                                                                                     \
     template cudaError_t launch_trace<T>(int, int, const T*, T*, T*, const DevBases<T>&, cudaStream_t);            \

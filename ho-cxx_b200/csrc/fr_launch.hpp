@@ -52,9 +52,24 @@ cudaError_t launch_residual(int K, const FrGeom<T>& g, const DevBases<T>& b, con
 template <typename T>
 cudaError_t launch_poisson_rhs(int K, int N, const int* face_nb, const T* w, const T* J, const double* bsrc,
                                const double* bc_p, double* rhs, cudaStream_t s);
+// Hybrid runs (problem type 11): the driver's open-boundary data at the start and end of
+// the outer time step ([N_eb][K], zero off the open boundary), the inlets' normal velocity
+// [N_eb], and the weights of the two ends at the stage's time.
+struct HybridBc {
+    const double *vn0 = nullptr, *vn1 = nullptr;  // normal velocity (outward)
+    const double *vp0 = nullptr, *vp1 = nullptr;  // parallel velocity
+    const double *w0 = nullptr, *w1 = nullptr;    // vorticity
+    const double* inlet_nv = nullptr;
+    double fac1 = 0.0, fac2 = 1.0;
+};
 cudaError_t launch_bc_update(int n_eb, int K, int ptype, double tc, double y_min, double y_max, const int* role,
                              const int* be_ijp, const int* sw_d, const double* edge_y, const BcArrays& bc,
-                             cudaStream_t s);
+                             const HybridBc& hb, cudaStream_t s);
+// omega = (1 - wgt) omega + wgt (fac1 v0 + fac2 v1) (src/HO_2D.cpp:2183-2189); also into the
+// stage input when w_stage is given (the first stage, whose input is omega itself)
+template <typename T>
+cudaError_t launch_hybrid_blend(size_t n, double* omega, T* w_stage, const double* wgt, const double* v0,
+                                const double* v1, double fac1, double fac2, cudaStream_t s);
 
 // ---- Krylov (krylov.cu)
 // Static data of the matrix-free Poisson operator (the method-2 FR Laplacian with

@@ -61,6 +61,9 @@ struct Mesh {
     std::vector<std::vector<int>> group_edges;
     std::vector<int> nbr, nbr_side, bidx;      // [n_el][4] by side; -1 where absent
     std::vector<int> be_el, be_side, be_group; // [n_eb]
+    // boundaries loaded from arrays (hybrid drivers): per-edge normal / parallel velocity
+    // given with the edge (NaN where none was given)
+    std::vector<double> edge_normvel, edge_parlvel;
 };
 
 // 1-D bases on the K Gauss-Legendre solution points and the L equispaced geometry nodes.
@@ -88,11 +91,23 @@ struct BoundaryConditions {
     std::vector<double> bc_p, bc_nv, bc_pv, bc_d;  // [N_eb][K]
     std::vector<double> edge_y;                    // [N_eb][K] y at the edge's solution points
     std::vector<int> role;                         // [N_eb] time-dependent role (see BcRole)
+    std::vector<double> inlet_nv;                  // [N_eb] hybrid inlets: the edge's normal velocity
     double y_min = 0.0, y_max = 0.0;
 };
 
 // Per-edge role in the time-dependent BC refresh of src/HO_2D.cpp:1979-2217.
-enum BcRole { ROLE_NONE = 0, ROLE_INLET = 1, ROLE_TOP = 2, ROLE_BOTTOM = 3, ROLE_OBJECT = 4 };
+// ROLE_OPEN / ROLE_WALL_H / ROLE_INLET_H: the "open", "wall" and "inlet" boundaries of a
+// hybrid run (problem type 11, 2104-2191).
+enum BcRole {
+    ROLE_NONE = 0,
+    ROLE_INLET = 1,
+    ROLE_TOP = 2,
+    ROLE_BOTTOM = 3,
+    ROLE_OBJECT = 4,
+    ROLE_OPEN = 5,
+    ROLE_WALL_H = 6,
+    ROLE_INLET_H = 7
+};
 
 // Poisson operator: 5 K^2 x K^2 blocks per element (transposed) and the boundary source.
 struct PoissonOperator {
@@ -107,6 +122,10 @@ struct PoissonOperator {
 
 Error read_input(const std::string& path, Input& in);
 Error read_msh(const std::string& path, int occ, Mesh& mesh);
+Error process_mesh(Mesh& mesh);
+Error mesh_from_arrays(int iorder, int nxy, const double* xy, int nidx, const int* idx, int nwall, const int* wall,
+                       int nopen, const int* open, Mesh& m);
+Error add_boundary_arrays(Mesh& m, const std::string& name, int n, const int* idx, int nval, const double* vals);
 Error make_bases(int K, int L, Bases& B);
 void make_metrics(const Mesh& mesh, const Bases& B, Metrics& M);
 Error setup_bcs(const Input& in, const Mesh& mesh, const Bases& B, BoundaryConditions& bc);

@@ -22,6 +22,12 @@
 
 namespace ho2d {
 
+#define HO2D_HOST_TRY(expr)     \
+    do {                        \
+        Error _e = (expr);      \
+        if (_e.code) return _e; \
+    } while (0)
+
 namespace {
 
 std::string dirname_of(const std::string& path) {
@@ -291,8 +297,17 @@ Error read_msh(const std::string& path, int occ, Mesh& m) {
             if (v < 0) return {3, "a quad references a missing node"};
             m.elem_nodes[q].push_back(v);
         }
+    return process_mesh(m);
+}
+
+// Neighbour search and boundary-edge ownership (src/Mesh.cpp:342-487, hash-based): fills
+// n_el, n_eb, nbr, nbr_side, bidx, be_el, be_side, be_group from node_xy, elem_nodes,
+// edge_nodes (boundary edges, group by group) and group_edges. Boundary edges take the
+// orientation of the element side they cover.
+Error process_mesh(Mesh& m) {
     m.n_el = (int)m.elem_nodes.size();
     m.n_eb = (int)m.edge_nodes.size();
+    if (m.n_el == 0) return {3, "the mesh has no elements"};
     // process_mesh: identify edges by their corner pair
     auto key = [](int a, int b) { return ((uint64_t)(uint32_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b); };
     std::unordered_map<uint64_t, int> edge_of;
@@ -356,6 +371,54 @@ Error read_msh(const std::string& path, int occ, Mesh& m) {
     m.be_group.assign(m.n_eb, -1);
     for (size_t g = 0; g < m.group_edges.size(); ++g)
         for (int e : m.group_edges[g]) m.be_group[e] = (int)g;
+    return {0, ""};
+}
+
+// load_mesh_arrays_d (src/HO_2D.cpp:3832-3886): nodes [nxy/2][2], elements of Lnod^2 node
+// indices each (Gmsh order), then the boundaries named "wall" and "open" as Lnod-node
+// edges. Boundaries "inlet" and "outlet" follow through add_boundary_arrays.
+Error mesh_from_arrays(int iorder, int nxy, const double* xy, int nidx, const int* idx, int nwall, const int* wall,
+                       int nopen, const int* open, Mesh& m) {
+    m = Mesh();
+    m.lnod = iorder + 1;
+    if (m.lnod < 2 || m.lnod > 4) return {4, "geometry order must be 1, 2 or 3 (Lnod 2..4)"};
+    if (nxy < 2 || nxy % 2 || !xy) return {1, "node array must hold x, y pairs"};
+    m.node_xy.assign(xy, xy + nxy);
+    const int nper = m.lnod * m.lnod, nn = nxy / 2;
+    if (nidx <= 0 || nidx % nper || !idx) return {1, "element index array is not a multiple of Lnod^2"};
+    m.elem_nodes.resize(nidx / nper);
+    for (size_t e = 0; e < m.elem_nodes.size(); ++e) {
+        m.elem_nodes[e].assign(idx + e * nper, idx + (e + 1) * nper);
+        for (int v : m.elem_nodes[e])
+            if (v < 0 || v >= nn) return {3, "an element references a node outside the node array"};
+    }
+    if (nwall > 0) HO2D_HOST_TRY(add_boundary_arrays(m, "wall", nwall, wall, 0, nullptr));
+    if (nopen > 0) HO2D_HOST_TRY(add_boundary_arrays(m, "open", nopen, open, 0, nullptr));
+    return {0, ""};
+}
+
+// arrays_to_boundary (src/HO_2D.cpp:3723-3829): one boundary group of n/Lnod edges, with
+// nval optional values: one per edge (normal velocity) or two (parallel, then normal).
+Error add_boundary_arrays(Mesh& m, const std::string& name, int n, const int* idx, int nval, const double* vals) {
+    if (n <= 0) return {0, ""};
+    if (!idx || n % m.lnod) return {1, "boundary " + name + ": index array is not a multiple of Lnod"};
+    const int ne = n / m.lnod, nn = (int)m.node_xy.size() / 2;
+    int per = 0;
+    if (nval > 0) {
+        if (!vals || nval % ne || nval / ne > 2) return {1, "boundary " + name + ": expected 1 or 2 values per edge"};
+        per = nval / ne;
+    }
+    m.group_names.push_back(name);
+    m.group_edges.emplace_back();
+    for (int i = 0; i < ne; ++i) {
+        std::vector<int> en(idx + (size_t)i * m.lnod, idx + (size_t)(i + 1) * m.lnod);
+        for (int v : en)
+            if (v < 0 || v >= nn) return {3, "boundary " + name + " references a node outside the node array"};
+        m.group_edges.back().push_back((int)m.edge_nodes.size());
+        m.edge_nodes.push_back(en);
+        m.edge_normvel.push_back(per == 1 ? vals[i] : (per == 2 ? vals[2 * i + 1] : std::nan("")));
+        m.edge_parlvel.push_back(per == 2 ? vals[2 * i] : std::nan(""));
+    }
     return {0, ""};
 }
 

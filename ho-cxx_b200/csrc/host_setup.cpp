@@ -246,6 +246,118 @@ std::vector<double> edge_y(const Mesh& m, const Bases& B, int e) {
 
 }  // namespace
 
+namespace {
+
+#define HO2D_SETUP_TRY(expr)    \
+    do {                        \
+        Error _e = (expr);      \
+        if (_e.code) return _e; \
+    } while (0)
+
+// Problem type 11 (src/HO_2D.cpp:893-1134). Boundaries by name: "open" (Neumann psi,
+// Dirichlet vorticity, values set every stage from the driver's data), "wall" (no slip),
+// "inlet" (Dirichlet psi and vorticity), "outlet" (Neumann psi and vorticity, zero). With
+// inlets, psi is marched along the chain of non-open boundary edges (each edge's second
+// node is the next edge's first): an inlet edge of length L with normal velocity v lowers
+// psi by L v and gets psi linear along it, the mean velocity's difference quotients with
+// its neighbours as vorticity and -v as BC_normal_vel; an outlet lowers psi the same way;
+// a wall takes the psi reached. The chain starts at the first edge that is neither inlet
+// nor outlet and assumes 2-node edges.
+Error setup_hybrid_bcs(const Mesh& m, const Bases& B, BoundaryConditions& bc) {
+    const int K = B.K, neb = m.n_eb, ng = (int)m.group_names.size();
+    enum { T_OTHER, T_OPEN, T_WALL, T_INLET, T_OUTLET };
+    std::vector<int> type(neb, T_OTHER);
+    bool have_inlets = false;
+    for (int g = 0; g < ng; ++g) {
+        const std::string& nm = m.group_names[g];
+        int t;
+        if (nm == "open") t = T_OPEN;
+        else if (nm == "wall") t = T_WALL;
+        else if (nm == "inlet") t = T_INLET;
+        else if (nm == "outlet") t = T_OUTLET;
+        else return {4, "hybrid run: boundary \"" + nm + "\" is not wall, open, inlet or outlet"};
+        bc.noslip[g] = t == T_WALL ? 1 : 0;
+        have_inlets = have_inlets || (t == T_INLET && !m.group_edges[g].empty());
+        for (int e : m.group_edges[g]) {
+            type[e] = t;
+            const size_t q0 = (size_t)e * K;
+            if (t == T_OPEN) {
+                bc.sw_p[e] = NEUMANN;
+                bc.sw_d[e] = DIRICHLET;
+                bc.role[e] = ROLE_OPEN;
+            } else if (t == T_WALL) {
+                bc.sw_p[e] = DIRICHLET;
+                bc.sw_d[e] = NEUMANN;
+                bc.role[e] = ROLE_WALL_H;
+            } else if (t == T_INLET) {
+                bc.sw_p[e] = DIRICHLET;
+                bc.sw_d[e] = DIRICHLET;
+                bc.role[e] = ROLE_INLET_H;
+            } else {
+                bc.sw_p[e] = NEUMANN;
+                bc.sw_d[e] = NEUMANN;
+            }
+            if (t == T_INLET || t == T_OUTLET) {
+                const double v = e < (int)m.edge_normvel.size() ? m.edge_normvel[e] : std::nan("");
+                if (!std::isfinite(v)) return {1, "hybrid run: an inlet or outlet edge has no normal velocity"};
+                if (t == T_INLET) bc.inlet_nv[e] = v;
+            }
+            std::fill_n(bc.bc_p.begin() + q0, K, 0.0);
+            std::fill_n(bc.bc_nv.begin() + q0, K, 0.0);
+            std::fill_n(bc.bc_pv.begin() + q0, K, 0.0);
+            std::fill_n(bc.bc_d.begin() + q0, K, 0.0);
+        }
+    }
+    if (!have_inlets) return {0, ""};
+    if (m.lnod != 2) return {4, "hybrid run: inlets need 2-node edges (Lnod = 2)"};
+    const int nnodes = (int)m.node_xy.size() / 2;
+    std::vector<int> firstnode(nnodes, 0);
+    for (int e = 0; e < neb; ++e)
+        if (type[e] != T_OPEN) firstnode[m.edge_nodes[e][0]] = e;
+    int istart = 0;
+    while (istart < neb && (type[istart] == T_INLET || type[istart] == T_OUTLET)) ++istart;
+    if (istart == neb) return {3, "hybrid run: every boundary edge is an inlet or outlet"};
+    std::vector<int> chain = {istart};
+    for (;;) {
+        const int next = firstnode[m.edge_nodes[chain.back()][1]];
+        if (next == chain.front()) break;
+        chain.push_back(next);
+        if ((int)chain.size() > neb) return {3, "hybrid run: the boundary edges do not close into a loop"};
+    }
+    const int nc = (int)chain.size();
+    std::vector<double> len(nc);
+    for (int i = 0; i < nc; ++i) {
+        const auto& en = m.edge_nodes[chain[i]];
+        const double dx = m.node_xy[2 * en[1]] - m.node_xy[2 * en[0]], dy = m.node_xy[2 * en[1] + 1] - m.node_xy[2 * en[0] + 1];
+        len[i] = std::sqrt(dx * dx + dy * dy);
+    }
+    auto inlet_v = [&](int i) { return type[chain[i]] == T_INLET ? m.edge_normvel[chain[i]] : 0.0; };
+    double psi_end = 0.0;
+    for (int i = 0; i < nc; ++i) {
+        const int e = chain[i];
+        const double psi_start = psi_end;
+        const size_t q0 = (size_t)e * K;
+        if (type[e] == T_INLET) {
+            const double v = m.edge_normvel[e];
+            psi_end -= len[i] * v;
+            const int ip = i == 0 ? nc - 1 : i - 1, in = i == nc - 1 ? 0 : i + 1;
+            const double w = (inlet_v(in) - v) / (len[in] + len[i]) + (v - inlet_v(ip)) / (len[i] + len[ip]);
+            for (int k = 0; k < K; ++k) {
+                bc.bc_p[q0 + k] = B.gsb[0 * K + k] * psi_start + B.gsb[1 * K + k] * psi_end;
+                bc.bc_d[q0 + k] = w;
+                bc.bc_nv[q0 + k] = -v;
+            }
+        } else if (type[e] == T_OUTLET) {
+            psi_end -= len[i] * m.edge_normvel[e];
+        } else if (type[e] == T_WALL) {
+            std::fill_n(bc.bc_p.begin() + q0, K, psi_end);
+        }
+    }
+    return {0, ""};
+}
+
+}  // namespace
+
 Error setup_bcs(const Input& in, const Mesh& m, const Bases& B, BoundaryConditions& bc) {
     const int K = B.K, neb = m.n_eb, ng = (int)m.group_names.size();
     bc.sw_p.assign(neb, DIRICHLET);
@@ -260,8 +372,11 @@ Error setup_bcs(const Input& in, const Mesh& m, const Bases& B, BoundaryConditio
         std::copy(y.begin(), y.end(), bc.edge_y.begin() + (size_t)e * K);
     }
     auto fill = [&](std::vector<double>& a, int e, double v) { std::fill_n(a.begin() + (size_t)e * K, K, v); };
+    bc.inlet_nv.assign(neb, 0.0);
     const int pt = in.problem_type;
-    if (pt == 1) {  // lid-driven cavity (src/HO_2D.cpp:700-727)
+    if (pt == 11) {  // hybrid run (src/HO_2D.cpp:893-1134)
+        HO2D_SETUP_TRY(setup_hybrid_bcs(m, B, bc));
+    } else if (pt == 1) {  // lid-driven cavity (src/HO_2D.cpp:700-727)
         std::fill(bc.noslip.begin(), bc.noslip.end(), 1);
         std::fill(bc.sw_p.begin(), bc.sw_p.end(), DIRICHLET);
         std::fill(bc.sw_d.begin(), bc.sw_d.end(), NEUMANN);

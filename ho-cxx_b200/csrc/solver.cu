@@ -70,6 +70,15 @@ Error Solver::setup() {
     if (!mesh_path.empty() && mesh_path[0] != '/') mesh_path = in_.base_dir + "/" + mesh_path;
     mesh_ = Mesh();
     HO2D_TRY(read_msh(mesh_path, in_.occ, mesh_));
+    return setup_from_mesh();
+}
+
+// Everything after the mesh (src/main.cpp:55-75, or process_mesh_input for a mesh loaded
+// from arrays): bases, metrics, BCs, the Poisson operator and its preconditioner, and the
+// device state.
+Error Solver::setup_from_mesh() {
+    setup_done_ = false;
+    adj_.reset();
     HO2D_TRY(make_bases(in_.knod, mesh_.lnod, B_));
     make_metrics(mesh_, B_, M_);
     for (double j : M_.J)
@@ -161,6 +170,8 @@ Error Solver::setup() {
     HO2D_CUDA(d.scalars.alloc(sizeof(KrylovScalars)), "alloc scalars");
     HO2D_CUDA(cudaMemset(d.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
     time_ = 0.0;
+    t_start_ = t_end_ = 0.0;
+    if (in_.problem_type == 11) HO2D_TRY(hybrid_upload());
     setup_done_ = true;
     if (stage32_ || krylov32_) HO2D_TRY(upload_precision_arrays());
     HO2D_CUDA(cudaDeviceSynchronize(), "setup");
@@ -572,6 +583,47 @@ Error Solver::poisson_solve() {
 }
 
 // ------------------------------------------------------------------ stages
+// update_BCs(t) (src/HO_2D.cpp:1979-2217) on the device: the time-dependent BC values of
+// problem types 2, 3 and 11 and the h-direction flip. For a hybrid run (type 11) it also
+// blends omega towards the driver's vorticity with the particle-to-grid weights, as the
+// reference does at every call; into_stage also blends the stage input, which is omega
+// itself in the first stage.
+template <typename T>
+Error Solver::update_bcs(double t, bool into_stage) {
+    DeviceState& d = *d_;
+    BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
+                d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
+    const double tc = 2.0 * std::fabs(std::sin(M_PI / 40.0 * t));
+    HybridBc hb;
+    const bool hyb = in_.problem_type == 11;
+    if (hyb) {
+        // weight of the start values: (t - t_start) / (t_end - t_start), as in the reference
+        // (so the end values apply at the outer step's start); end values before any outer step
+        hb.fac1 = t_end_ > t_start_ ? (t - t_start_) / (t_end_ - t_start_) : 0.0;
+        hb.fac2 = 1.0 - hb.fac1;
+        hb.vn0 = d.hyb[0].as<double>();
+        hb.vn1 = d.hyb[1].as<double>();
+        hb.vp0 = d.hyb[2].as<double>();
+        hb.vp1 = d.hyb[3].as<double>();
+        hb.w0 = d.hyb[4].as<double>();
+        hb.w1 = d.hyb[5].as<double>();
+        hb.inlet_nv = d.hyb_inlet_nv.as<double>();
+    }
+    HO2D_CUDA(launch_bc_update(mesh_.n_eb, in_.knod, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
+                               d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, hb, d.stream),
+              "bc_update");
+    launches_ += 1;
+    if (hyb) {
+        const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+        HO2D_CUDA(launch_hybrid_blend<T>(nv, d.omega.as<double>(), into_stage ? d.w_stage.as<T>() : nullptr,
+                                         d.hvort[2].as<double>(), d.hvort[0].as<double>(), d.hvort[1].as<double>(),
+                                         hb.fac1, hb.fac2, d.stream),
+                  "hybrid blend");
+        launches_ += 1;
+    }
+    return {0, ""};
+}
+
 // One stage at the current stage input. With solve == false the Poisson solve is skipped
 // and the stage works from the psi already in place (the adjoint recomputes a stored
 // stage's fields this way).
@@ -585,12 +637,7 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     const FrGeom<T> g = geom_of<T>(d, mesh_, f32);
     BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
                 d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
-    const double t = time_ + coeff * in_.dt;
-    const double tc = 2.0 * std::fabs(std::sin(M_PI / 40.0 * t));
-    HO2D_CUDA(launch_bc_update(mesh_.n_eb, K, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
-                               d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, d.stream),
-              "bc_update");
-    launches_ += 1;
+    HO2D_TRY(update_bcs<T>(time_ + coeff * in_.dt, rk_stage == 0));
     if (solve) {
         HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
                                         d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
@@ -641,10 +688,7 @@ Error Solver::velocity_only_t() {
     const FrGeom<T> g = geom_of<T>(d, mesh_, f32);
     BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
                 d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
-    const double tc = 2.0 * std::fabs(std::sin(M_PI / 40.0 * time_));
-    HO2D_CUDA(launch_bc_update(mesh_.n_eb, K, in_.problem_type, tc, bc_.y_min, bc_.y_max, d.role.as<int>(),
-                               d.be_ijp.as<int>(), d.sw_d.as<int>(), d.edge_y.as<double>(), bc, d.stream),
-              "bc_update");
+    HO2D_TRY(update_bcs<T>(time_, true));
     HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
                                     d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
               "poisson_rhs");
@@ -709,6 +753,10 @@ Error Solver::solveto(double outerdt, int numstep, int integtype, double reyn) {
     in_.dt = outerdt / numstep;
     in_.ti_type = integtype;
     in_.reyn_inv = reyn > 1e-3 ? 1.0 / reyn : -1.0;
+    // the outer step runs from the previous outer step's end (src/HO_2D.cpp:4208-4210)
+    t_start_ = t_end_;
+    time_ = t_start_;
+    t_end_ += outerdt;
     return step(numstep);
 }
 
@@ -874,6 +922,13 @@ Error Solver::set_vorticity(const double* in) {
     for (size_t i = 0; i < nv; ++i)
         if (!std::isfinite(in[i])) return {7, "non-finite value in the vorticity passed in"};
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    if (hybrid_ && d.hvort[1].get()) {
+        // hybrid operation (setsolnvort_d, src/HO_2D.cpp:4132-4152): the vorticity to blend
+        // in at the end of the outer step; the previous one becomes the start value
+        HO2D_CUDA(cudaMemcpy(d.hvort[0].get(), d.hvort[1].get(), nv * 8, cudaMemcpyDeviceToDevice), "copy");
+        HO2D_CUDA(cudaMemcpy(d.hvort[1].get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
+        return {0, ""};
+    }
     HO2D_CUDA(cudaMemcpy(d.omega.get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
     if (stage32_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
     else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");

@@ -66,6 +66,25 @@ class Solver {
     // its normal flux of the latest stage
     Error get_forces(double* fx, double* fy);
 
+    // ---- hybrid operation (hybrid.cu), the _d entry points of src/HO_2D.hpp:251-290
+    void set_defaults();
+    void enable_hybrid() { hybrid_ = true; }
+    Error set_elemorder(int k);
+    Error load_mesh_arrays(int iorder, int nxy, const double* xy, int nidx, const int* idx, int nwall,
+                           const int* wall, int nopen, const int* open);
+    Error load_inout_arrays(int ninval, const double* velin, int nin, const int* idxin, int noutval,
+                            const double* velout, int nout, const int* idxout);
+    Error process_mesh_input();
+    Error get_solution_areas(double* out);     // [N][K][K] w_j w_k J
+    int open_point_count() const;              // 2 * (open edges) * K
+    Error get_open_points(double* out);        // [open edges][K][x, y]
+    Error set_open_velocities(const double* xyvel);  // [open edges][K][u, v]
+    Error set_open_vorticity(const double* w);       // [open edges][K]
+    Error set_ptog_weights(const double* w);         // [N][K][K]
+    Error get_hoquad_weights(double* out);           // [K][K] 0.25 w_j w_k
+    bool hybrid() const { return hybrid_; }
+    void release();                                  // clean_up: device memory freed, setup undone
+
     // ---- discrete adjoint (adjoint_driver.cu)
     // nsteps time steps from the current state, keeping the vorticity every ckpt_every
     // steps for the backward sweep
@@ -107,6 +126,10 @@ class Solver {
     Error stage_t(double coeff, int rk_stage, bool update, bool solve = true);
     template <typename T>
     Error velocity_only_t();
+    template <typename T>
+    Error update_bcs(double t, bool into_stage);
+    Error setup_from_mesh();
+    Error hybrid_upload();
     Error upload_precision_arrays();
     Error setup_preconditioner();
     Error build_poisson_geometry(const std::vector<int>& fnb, const std::vector<int>& fnijp);
@@ -132,6 +155,11 @@ class Solver {
     bool stage32_ = false;   // FR stage kernels in FP32 (HO2D_MIXED)
     bool krylov32_ = false;  // FP32 BiCGSTAB inside FP64 refinement (HO2D_MIXED, HO2D_MIXED_KRYLOV)
     double time_ = 0.0;
+    // outer time step of solveto_d (src/HO_2D.cpp:4208-4210): hybrid BCs interpolate in it
+    double t_start_ = 0.0, t_end_ = 0.0;
+    bool hybrid_ = false;                     // enable_hybrid: set_vort feeds the blend target
+    std::vector<double> open_normal_;         // [N_eb][K][2] unit outward normal on open edges
+    std::vector<double> h_open_[6];           // host copies of the open-boundary data (start/end)
     double tol_ = 1e-12;
     int max_iter_ = 500;
     int last_iters_ = 0, prev_iters_ = 8;

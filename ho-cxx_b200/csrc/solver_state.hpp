@@ -79,6 +79,10 @@ struct DeviceState {
     double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
     DeviceBuffer l2flush;               // written between timed steps to evict L2
     DeviceBuffer fcoef, fidx, fout;     // body-force coefficients, boundary indices, result
+    // hybrid runs: open-boundary normal / parallel velocity and vorticity at the outer step's
+    // start and end [N_eb][K]; inlet normal velocity [N_eb]; the driver's vorticity at
+    // start and end and the particle-to-grid weights [N][K][K]
+    DeviceBuffer hyb[6], hyb_inlet_nv, hvort[3];
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);

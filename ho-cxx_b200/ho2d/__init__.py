@@ -132,6 +132,79 @@ class HO_2D:
         self._check(self._lib.ho2d_get_solution_points(self._h, out.size, capi.dptr(out)))
         return out
 
+    # -- hybrid operation (src/HO_2D.hpp:251-290): an external Lagrangian driver
+    def set_defaults(self) -> None:
+        self._check(self._lib.ho2d_set_defaults(self._h))
+        self._setup = False
+
+    def enable_hybrid(self) -> None:
+        self._check(self._lib.ho2d_enable_hybrid(self._h))
+
+    def set_elemorder(self, knod: int) -> None:
+        self._check(self._lib.ho2d_set_elemorder(self._h, int(knod)))
+
+    def load_mesh_arrays_d(self, iorder: int, xy, elems, wall=(), open_=()) -> None:
+        """Nodes (x, y pairs), elements (Lnod^2 Gmsh-ordered node indices each), and the
+        "wall" and "open" boundary edges (Lnod node indices each, counter-clockwise)."""
+        xy = np.ascontiguousarray(xy, dtype=np.float64).ravel()
+        el = np.ascontiguousarray(elems, dtype=np.int32).ravel()
+        w = np.ascontiguousarray(wall, dtype=np.int32).ravel()
+        o = np.ascontiguousarray(open_, dtype=np.int32).ravel()
+        self._check(self._lib.ho2d_load_mesh_arrays(self._h, int(iorder), xy.size, capi.dptr(xy), el.size,
+                                                    capi.iptr(el), w.size, capi.iptr(w), o.size, capi.iptr(o)))
+
+    def load_inout_arrays_d(self, velin=(), idxin=(), velout=(), idxout=()) -> None:
+        vi = np.ascontiguousarray(velin, dtype=np.float64).ravel()
+        ii = np.ascontiguousarray(idxin, dtype=np.int32).ravel()
+        vo = np.ascontiguousarray(velout, dtype=np.float64).ravel()
+        io = np.ascontiguousarray(idxout, dtype=np.int32).ravel()
+        self._check(self._lib.ho2d_load_inout_arrays(self._h, vi.size, capi.dptr(vi), ii.size, capi.iptr(ii),
+                                                     vo.size, capi.dptr(vo), io.size, capi.iptr(io)))
+
+    def process_mesh_input(self) -> None:
+        self._check(self._lib.ho2d_process_mesh_input(self._h))
+        self._setup = True
+        n, k, neb, lnod = (ctypes.c_int32() for _ in range(4))
+        self._check(self._lib.ho2d_get_sizes(self._h, ctypes.byref(n), ctypes.byref(k), ctypes.byref(neb),
+                                             ctypes.byref(lnod)))
+        self.N_el, self.Knod, self.N_edges_boundary, self.Lnod = n.value, k.value, neb.value, lnod.value
+
+    def getsolnareas_d(self) -> np.ndarray:
+        out = self._vol()
+        self._check(self._lib.ho2d_get_solution_areas(self._h, out.size, capi.dptr(out)))
+        return out
+
+    def getopenptlen(self) -> int:
+        n = ctypes.c_int32()
+        self._check(self._lib.ho2d_get_open_point_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def getopenpts_d(self) -> np.ndarray:
+        out = np.zeros(self.getopenptlen())
+        self._check(self._lib.ho2d_get_open_points(self._h, out.size, capi.dptr(out)))
+        return out.reshape(-1, self.Knod, 2)
+
+    def setopenvels_d(self, xyvel) -> None:
+        a = np.ascontiguousarray(xyvel, dtype=np.float64).ravel()
+        self._check(self._lib.ho2d_set_open_velocities(self._h, a.size, capi.dptr(a)))
+
+    def setopenvort_d(self, vort) -> None:
+        a = np.ascontiguousarray(vort, dtype=np.float64).ravel()
+        self._check(self._lib.ho2d_set_open_vorticity(self._h, a.size, capi.dptr(a)))
+
+    def setptogweights_d(self, wgt) -> None:
+        a = np.ascontiguousarray(wgt, dtype=np.float64).ravel()
+        self._check(self._lib.ho2d_set_ptog_weights(self._h, a.size, capi.dptr(a)))
+
+    def get_hoquad_weights_d(self) -> np.ndarray:
+        out = np.zeros((self.Knod, self.Knod))
+        self._check(self._lib.ho2d_get_hoquad_weights(self._h, out.size, capi.dptr(out)))
+        return out
+
+    def clean_up(self) -> None:
+        self._check(self._lib.ho2d_clean_up(self._h))
+        self._setup = False
+
     # -- controls and statistics
     def get_boundary_points(self) -> np.ndarray:
         """[N_eb][K][x, y] of the boundary flux points, in the boundary arrays' order."""

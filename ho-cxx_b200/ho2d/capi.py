@@ -54,6 +54,20 @@ SIGNATURES = {
     "ho2d_apply_poisson_noalloc": (ctypes.c_int, [_P, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "ho2d_get_forces": (ctypes.c_int, [_P, _DP, _DP]),
     "ho2d_get_boundary_points": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_set_defaults": (ctypes.c_int, [_P]),
+    "ho2d_enable_hybrid": (ctypes.c_int, [_P]),
+    "ho2d_set_elemorder": (ctypes.c_int, [_P, _I]),
+    "ho2d_load_mesh_arrays": (ctypes.c_int, [_P, _I, _I, _DP, _I, _IP, _I, _IP, _I, _IP]),
+    "ho2d_load_inout_arrays": (ctypes.c_int, [_P, _I, _DP, _I, _IP, _I, _DP, _I, _IP]),
+    "ho2d_process_mesh_input": (ctypes.c_int, [_P]),
+    "ho2d_get_solution_areas": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_get_open_point_count": (ctypes.c_int, [_P, _IP]),
+    "ho2d_get_open_points": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_set_open_velocities": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_set_open_vorticity": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_set_ptog_weights": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_get_hoquad_weights": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_clean_up": (ctypes.c_int, [_P]),
     "ho2d_adjoint_forward": (ctypes.c_int, [_P, _I, _I]),
     "ho2d_adjoint_backward": (ctypes.c_int, [_P, _I, _DP, _DP, _I, _DP]),
     "ho2d_stage_adjoint": (ctypes.c_int, [_P, _D, _I, _DP, _DP, _I, _DP]),
@@ -89,3 +103,7 @@ class HO2DError(RuntimeError):
 
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(_DP)
+
+
+def iptr(a: np.ndarray):
+    return a.ctypes.data_as(_IP)

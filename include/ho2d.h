@@ -160,6 +160,52 @@ int ho2d_apply_poisson_noalloc(ho2d_solver* handle, int32_t len, const double* x
  * nu omega t (Koumoutsakos & Leonard, JFM 1995). Drag and lift coefficients are 2 F / (U^2 D).
  * HO2D_ERR_ARG when the mesh has no "object" group. */
 int ho2d_get_forces(ho2d_solver* handle, double* fx, double* fy);
+/* ---- Hybrid operation: the entry points an external Lagrangian driver calls
+ * (src/HO_2D.hpp:251-290). Sequence: ho2d_set_defaults, ho2d_enable_hybrid,
+ * ho2d_set_elemorder, ho2d_load_mesh_arrays, ho2d_load_inout_arrays (optional),
+ * ho2d_process_mesh_input; then per outer step ho2d_set_open_velocities,
+ * ho2d_set_open_vorticity, ho2d_set_vort (the vorticity to blend in; hybrid mode only),
+ * ho2d_set_ptog_weights, ho2d_solveto and ho2d_get_vort. Problem type 11. */
+/* Replaces set_defaults (src/HO_2D.cpp:3697-3712): Knod 3, Re^-1 1, RK2, advection type 2,
+ * problem type 11, dt 1; takes the place of ho2d_read_input. */
+int ho2d_set_defaults(ho2d_solver* handle);
+/* Replaces enable_hybrid (3714-3716): ho2d_set_vort then sets the blend target. */
+int ho2d_enable_hybrid(ho2d_solver* handle);
+/* Replaces set_elemorder (3718-3720): Knod. */
+int ho2d_set_elemorder(ho2d_solver* handle, int32_t knod);
+/* Replaces load_mesh_arrays_d (3832-3886): geometry order iorder (Lnod - 1); nxy doubles of
+ * node coordinates (x, y pairs); nidx element node indices (Lnod^2 per element, Gmsh
+ * order, 0-based); nwall / nopen node indices of the "wall" / "open" boundary edges (Lnod
+ * per edge, in the element's counter-clockwise orientation). */
+int ho2d_load_mesh_arrays(ho2d_solver* handle, int32_t iorder, int32_t nxy, const double* xy, int32_t nidx,
+                          const int32_t* idx, int32_t nwall, const int32_t* idxwall, int32_t nopen,
+                          const int32_t* idxopen);
+/* Replaces load_inout_arrays_d (3889-3904): "inlet" and "outlet" edges, each with one
+ * normal velocity per edge (or two values: parallel, normal). */
+int ho2d_load_inout_arrays(ho2d_solver* handle, int32_t ninval, const double* velin, int32_t nin,
+                           const int32_t* idxin, int32_t noutval, const double* velout, int32_t nout,
+                           const int32_t* idxout);
+/* Replaces process_mesh_input (3907-3940): mesh processing and the device setup. */
+int ho2d_process_mesh_input(ho2d_solver* handle);
+/* Replaces getsolnareas_d (3983-3994): w_j w_k J per solution point, len = N_el*Knod*Knod. */
+int ho2d_get_solution_areas(ho2d_solver* handle, int32_t len, double* buf);
+/* Replaces getopenptlen (3996-4004): 2 * (open edges) * Knod. */
+int ho2d_get_open_point_count(ho2d_solver* handle, int32_t* len);
+/* Replaces getopenpts_d (4006-4031): [open edge][Knod][x, y] along each edge. */
+int ho2d_get_open_points(ho2d_solver* handle, int32_t len, double* buf);
+/* Replaces setopenvels_d (4035-4106): Cartesian velocity [open edge][Knod][u, v] at the end
+ * of the outer step; the previous values become the start values. */
+int ho2d_set_open_velocities(ho2d_solver* handle, int32_t len, const double* buf);
+/* Replaces setopenvort_d (4109-4129): vorticity [open edge][Knod] at the end of the outer step. */
+int ho2d_set_open_vorticity(ho2d_solver* handle, int32_t len, const double* buf);
+/* Replaces setptogweights_d (4156-4170): blend weights per solution point, len = N_el*Knod*Knod. */
+int ho2d_set_ptog_weights(ho2d_solver* handle, int32_t len, const double* buf);
+/* Replaces get_hoquad_weights_d (4252-4260): 0.25 w_j w_k, len = Knod*Knod. */
+int ho2d_get_hoquad_weights(ho2d_solver* handle, int32_t len, double* buf);
+/* Replaces clean_up (4274-4277): frees the device state; the handle stays valid. The
+ * reference's trigger_write (VTK files) is not provided. */
+int ho2d_clean_up(ho2d_solver* handle);
+
 /* ---- Discrete adjoint. No counterpart in the reference: gradients of a scalar
  * J(omega(T)) of the vorticity after nsteps time steps with respect to the initial
  * vorticity and to BC_parl_vel (the wall velocity of no-slip walls, constant in time),

@@ -27,6 +27,7 @@
 //                          coefficients cycling 0, .5, .5, 1) and print a JSON line
 //   --t0 T                 start the time loop at time T instead of 0
 //   --verbose              keep the reference's stdout
+// or:   ho2d_ref --hybrid SPECDIR OUTDIR [--verbose]   (see run_hybrid)
 #include "HO_2D.hpp"
 
 #include <sys/stat.h>
@@ -35,6 +36,8 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <map>
 
 namespace {
 
@@ -97,9 +100,104 @@ struct NullBuf : std::streambuf {
     int overflow(int c) override { return c; }
 };
 
+// A whole .npy file of the given dtype ("<f8" or "<i4"); missing file: empty.
+template <typename T>
+std::vector<T> read_npy_any(const std::string& path, const char* descr) {
+    std::vector<T> v;
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return v;
+    unsigned char pre[10];
+    if (std::fread(pre, 1, 10, f) != 10) std::exit(3);
+    const uint16_t hl = (uint16_t)(pre[8] | (pre[9] << 8));
+    std::string hdr(hl, ' ');
+    if (std::fread(&hdr[0], 1, hl, f) != hl) std::exit(3);
+    if (hdr.find(descr) == std::string::npos) {
+        std::fprintf(stderr, "%s: expected dtype %s\n", path.c_str(), descr);
+        std::exit(3);
+    }
+    const size_t a = hdr.find("'shape': (") + 10, b = hdr.find(')', a);
+    size_t count = 1;
+    std::string sh = hdr.substr(a, b - a);
+    size_t pos = 0;
+    while (pos < sh.size()) {
+        const size_t c = sh.find(',', pos);
+        const std::string tok = sh.substr(pos, c == std::string::npos ? std::string::npos : c - pos);
+        if (tok.find_first_of("0123456789") != std::string::npos) count *= std::stoul(tok);
+        if (c == std::string::npos) break;
+        pos = c + 1;
+    }
+    v.resize(count);
+    if (count && std::fread(v.data(), sizeof(T), count, f) != count) std::exit(3);
+    std::fclose(f);
+    return v;
+}
+
+// --hybrid SPECDIR OUTDIR: the reference's hybrid sequence (src/HO_2D.hpp:251-290) on
+// arrays from SPECDIR: spec.txt ("key value" lines: knod iorder nouter numstep outerdt
+// integ reyn), nodes.npy, elems.npy, wall.npy, open.npy, inlet.npy / inletvel.npy,
+// outlet.npy / outletvel.npy, ptog.npy, and per outer step s = -1 .. nouter-1 the driver
+// data vort_<s>.npy, openvel_<s>.npy, openvort_<s>.npy (s = -1 fills the "start" values
+// before the first step). Dumps vort_out_<s>.npy after each outer step.
+int run_hybrid(const std::string& spec, const std::string& outdir_in, bool verbose) {
+    std::map<std::string, double> kv;
+    {
+        std::ifstream f(spec + "/spec.txt");
+        std::string k;
+        double v;
+        while (f >> k >> v) kv[k] = v;
+    }
+    mkdir(outdir_in.c_str(), 0755);
+    char absout[4096];
+    if (!realpath(outdir_in.c_str(), absout)) { std::perror("realpath"); return 3; }
+    const std::string outdir = absout;
+    auto f8 = [&](const std::string& n) { return read_npy_any<double>(spec + "/" + n + ".npy", "<f8"); };
+    auto i4 = [&](const std::string& n) { return read_npy_any<int32_t>(spec + "/" + n + ".npy", "<i4"); };
+    std::vector<double> xy = f8("nodes"), inv = f8("inletvel"), outv = f8("outletvel"), ptog = f8("ptog");
+    std::vector<int32_t> el = i4("elems"), wall = i4("wall"), open = i4("open"), inl = i4("inlet"), outl = i4("outlet");
+    NullBuf nullbuf;
+    std::streambuf* saved = std::cout.rdbuf();
+    if (!verbose) std::cout.rdbuf(&nullbuf);
+    HO_2D s;
+    s.set_defaults();
+    s.enable_hybrid();
+    s.set_elemorder((int32_t)kv["knod"]);
+    s.load_mesh_arrays_d((int32_t)kv["iorder"], (int32_t)xy.size(), xy.data(), (int32_t)el.size(), el.data(),
+                         (int32_t)wall.size(), wall.data(), (int32_t)open.size(), open.data());
+    s.load_inout_arrays_d((int32_t)inv.size(), inv.data(), (int32_t)inl.size(), inl.data(), (int32_t)outv.size(),
+                          outv.data(), (int32_t)outl.size(), outl.data());
+    s.process_mesh_input();
+    const int32_t nv = s.mesh.N_el * s.Knod * s.Knod;
+    const int32_t nopen = s.getopenptlen();
+    if (!ptog.empty()) s.setptogweights_d(nv, ptog.data());
+    const int nouter = (int)kv["nouter"];
+    for (int st = -1; st < nouter; ++st) {
+        const std::string t = std::to_string(st);
+        std::vector<double> v = f8("vort_" + t), ov = f8("openvel_" + t), ow = f8("openvort_" + t);
+        if (!v.empty()) s.setsolnvort_d(nv, v.data());
+        if (!ov.empty()) s.setopenvels_d(nopen, ov.data());
+        if (!ow.empty()) s.setopenvort_d(nopen / 2, ow.data());
+        if (st < 0) continue;
+        s.solveto_d(kv["outerdt"], (int32_t)kv["numstep"], (int32_t)kv["integ"], kv["reyn"]);
+        std::vector<double> out(nv);
+        s.getallvorts_d(nv, out.data());
+        dump_f64(outdir, "vort_out_" + t, {(size_t)nv}, out.data());
+    }
+    std::vector<double> areas(nv), opts(std::max(1, nopen));
+    s.getsolnareas_d(nv, areas.data());
+    dump_f64(outdir, "areas", {(size_t)nv}, areas.data());
+    if (nopen > 0) {
+        s.getopenpts_d(nopen, opts.data());
+        dump_f64(outdir, "openpts", {(size_t)nopen}, opts.data());
+    }
+    std::cout.rdbuf(saved);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
+    if (argc >= 4 && std::string(argv[1]) == "--hybrid")
+        return run_hybrid(argv[2], argv[3], argc > 4 && std::string(argv[4]) == "--verbose");
     if (argc < 3) {
         std::fprintf(stderr, "usage: %s INPUT.dat OUTDIR [options]\n", argv[0]);
         return 2;
