@@ -21,6 +21,7 @@
 #include "noalloc.hpp"
 #include "solver.hpp"
 #include "solver_state.hpp"
+#include "adjoint_launch.hpp"
 
 namespace ho2d {
 
@@ -41,6 +42,8 @@ void DeviceBuffer::reset() {
 
 
 Solver::Solver() : d_(new DeviceState) {
+    const char* pe = std::getenv("HO2D_PSI_EXTRAP");
+    if (pe) psi_extrap_ = std::atoi(pe);
     const char* v = std::getenv("HO2D_VERBOSE");
     verbose_ = v && v[0] && v[0] != '0';
     const char* g = std::getenv("HO2D_GRAPHS");
@@ -171,6 +174,7 @@ Error Solver::setup_from_mesh() {
     HO2D_CUDA(cudaMemset(d.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
     time_ = 0.0;
     t_start_ = t_end_ = 0.0;
+    hist_count_ = 0;
     if (in_.problem_type == 11) HO2D_TRY(hybrid_upload());
     setup_done_ = true;
     if (stage32_ || krylov32_) HO2D_TRY(upload_precision_arrays());
@@ -715,9 +719,45 @@ Error Solver::step(int nsteps) {
     static const double c2[2] = {0.0, 1.0};
     const int ns = in_.ti_type == 4 ? 4 : (in_.ti_type == 2 ? 2 : 1);
     const double* c = in_.ti_type == 4 ? c4 : c2;
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    const int order = psi_extrap_;
+    if (order >= 2 && !d.psi_hist[0][0].get())
+        for (auto& row : d.psi_hist)
+            for (auto& b : row) HO2D_CUDA(b.alloc(nv * 8), "alloc psi history");
+    if (hist_dt_ != in_.dt || hist_ns_ != ns) {
+        hist_count_ = 0;
+        hist_dt_ = in_.dt;
+        hist_ns_ = ns;
+    }
     for (int i = 0; i < nsteps; ++i) {
-        for (int s = 0; s < ns; ++s) HO2D_TRY(stage_impl(c[s], s, true));
+        const int k = hist_step_;
+        for (int s = 0; s < ns; ++s) {
+            if (order >= 2 && hist_count_ >= order) {
+                // initial guess of this stage's Poisson solve: the same stage of the last
+                // steps, extrapolated in time (they are dt apart); the solve's tolerance is
+                // unchanged, only its starting point moves closer
+                double* psi = d.psi64.as<double>();
+                const double* h1 = d.psi_hist[(k + 2) % 3][s].as<double>();
+                const double* h2 = d.psi_hist[(k + 1) % 3][s].as<double>();
+                if (order == 2) {
+                    HO2D_CUDA(launch_axpby(nv, psi, 2.0, h1, -1.0, h2, d.stream), "psi guess");
+                } else {
+                    const double* h3 = d.psi_hist[k % 3][s].as<double>();
+                    HO2D_CUDA(launch_axpby(nv, psi, 3.0, h1, -3.0, h2, d.stream), "psi guess");
+                    HO2D_CUDA(launch_axpby(nv, psi, 1.0, psi, 1.0, h3, d.stream), "psi guess");
+                }
+                launches_ += order - 1;
+            }
+            HO2D_TRY(stage_impl(c[s], s, true));
+            if (order >= 2)
+                HO2D_CUDA(cudaMemcpyAsync(d.psi_hist[k % 3][s].get(), d.psi64.get(), nv * 8, cudaMemcpyDeviceToDevice,
+                                          d.stream),
+                          "psi history");
+        }
         time_ += in_.dt;
+        hist_step_ = (k + 1) % 3;
+        hist_count_ = std::min(hist_count_ + 1, 3);
     }
     HO2D_CUDA(cudaStreamSynchronize(d_->stream), "step");
     HO2D_CUDA(cudaGetLastError(), "step");
@@ -929,6 +969,7 @@ Error Solver::set_vorticity(const double* in) {
         HO2D_CUDA(cudaMemcpy(d.hvort[1].get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
         return {0, ""};
     }
+    hist_count_ = 0;  // the trajectory restarts: no psi history to extrapolate from
     HO2D_CUDA(cudaMemcpy(d.omega.get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
     if (stage32_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
     else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");

@@ -108,7 +108,10 @@ class Solver {
     int n_eb() const { return mesh_.n_eb; }
     int lnod() const { return mesh_.lnod; }
     double time() const { return time_; }
-    void set_time(double t) { time_ = t; }
+    void set_time(double t) {
+        time_ = t;
+        hist_count_ = 0;
+    }
     double dt() const { return in_.dt; }
     int precision() const { return krylov32_ ? (stage32_ ? 1 : 2) : 0; }
     int last_poisson_iterations() const { return last_iters_; }
@@ -158,6 +161,11 @@ class Solver {
     // outer time step of solveto_d (src/HO_2D.cpp:4208-4210): hybrid BCs interpolate in it
     double t_start_ = 0.0, t_end_ = 0.0;
     bool hybrid_ = false;                     // enable_hybrid: set_vort feeds the blend target
+    // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
+    // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
+    int psi_extrap_ = 3;
+    int hist_count_ = 0, hist_step_ = 0, hist_ns_ = 0;
+    double hist_dt_ = 0.0;
     std::vector<double> open_normal_;         // [N_eb][K][2] unit outward normal on open edges
     std::vector<double> h_open_[6];           // host copies of the open-boundary data (start/end)
     double tol_ = 1e-12;

@@ -83,6 +83,8 @@ struct DeviceState {
     // start and end [N_eb][K]; inlet normal velocity [N_eb]; the driver's vorticity at
     // start and end and the particle-to-grid weights [N][K][K]
     DeviceBuffer hyb[6], hyb_inlet_nv, hvort[3];
+    // psi of each RK stage of the last three steps (the next solve's initial guess)
+    DeviceBuffer psi_hist[3][4];
 
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);

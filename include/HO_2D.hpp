@@ -50,10 +50,46 @@ class HO_2D {
     void setsolnvort_d(int32_t len, const double* v) { check(ho2d_set_vort(h_, len, v)); }
     void getallvorts_d(int32_t len, double* v) { check(ho2d_get_vort(h_, len, v)); }
     void getsolnpts_d(int32_t len, double* xy) { check(ho2d_get_solution_points(h_, len, xy)); }
+    // length of the getsolnpts_d array: x, y per solution point (src/HO_2D.cpp:3942-3944)
     int32_t getsolnptlen() {
         int32_t n = 0, k = 0;
         check(ho2d_get_sizes(h_, &n, &k, nullptr, nullptr));
-        return n * k * k;
+        return 2 * n * k * k;
+    }
+
+    // hybrid operation (src/HO_2D.hpp:251-290)
+    void set_defaults() { check(ho2d_set_defaults(h_)); }
+    void enable_hybrid() { check(ho2d_enable_hybrid(h_)); }
+    void set_elemorder(int32_t eorder) { check(ho2d_set_elemorder(h_, eorder)); }
+    void load_mesh_arrays_d(int32_t iorder, int32_t nnodes, const double* xynodes, int32_t nelems,
+                            const int32_t* idxelems, int32_t nwall, const int32_t* idxwall, int32_t nopen,
+                            const int32_t* idxopen) {
+        check(ho2d_load_mesh_arrays(h_, iorder, nnodes, xynodes, nelems, idxelems, nwall, idxwall, nopen, idxopen));
+    }
+    void load_inout_arrays_d(int32_t ninval, const double* velin, int32_t nin, const int32_t* idxin,
+                             int32_t noutval, const double* velout, int32_t nout, const int32_t* idxout) {
+        check(ho2d_load_inout_arrays(h_, ninval, velin, nin, idxin, noutval, velout, nout, idxout));
+    }
+    void process_mesh_input() {
+        check(ho2d_process_mesh_input(h_));
+        setup_ = true;
+    }
+    void getsolnareas_d(int32_t len, double* areas) { check(ho2d_get_solution_areas(h_, len, areas)); }
+    int32_t getopenptlen() {
+        int32_t n = 0;
+        check(ho2d_get_open_point_count(h_, &n));
+        return n;
+    }
+    void getopenpts_d(int32_t len, double* xy) { check(ho2d_get_open_points(h_, len, xy)); }
+    void setopenvels_d(int32_t len, const double* xyvel) { check(ho2d_set_open_velocities(h_, len, xyvel)); }
+    void setopenvort_d(int32_t len, const double* vort) { check(ho2d_set_open_vorticity(h_, len, vort)); }
+    void setptogweights_d(int32_t len, const double* wgt) { check(ho2d_set_ptog_weights(h_, len, wgt)); }
+    void get_hoquad_weights_d(int32_t len, double* w) { check(ho2d_get_hoquad_weights(h_, len, w)); }
+    // VTK output (save_vorticity_vtk / save_smooth_vtk) is not provided
+    void trigger_write(int32_t, int32_t) { throw HO2DException(HO2D_ERR_UNSUPPORTED, "VTK output is not provided"); }
+    void clean_up() {
+        check(ho2d_clean_up(h_));
+        setup_ = false;
     }
     void set_precision(int mode) { check(ho2d_set_precision(h_, mode)); }
     ho2d_solver* handle() { return h_; }

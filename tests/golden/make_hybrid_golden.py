@@ -66,7 +66,8 @@ def annulus():
     th = np.linspace(0.0, 2 * np.pi, nt, endpoint=False)
     xy = np.array([[ri * np.cos(t), ri * np.sin(t)] for ri in r for t in th])
     idx = lambda i, j: i * nt + (j % nt)  # noqa: E731
-    quads = np.array([[idx(i, j), idx(i, j + 1), idx(i + 1, j + 1), idx(i + 1, j)] for i in range(nr) for j in range(nt)],
+    # counter-clockwise: outward, then along increasing theta
+    quads = np.array([[idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)] for i in range(nr) for j in range(nt)],
                      dtype=np.int32)
     inner = orient(quads, [(idx(0, j), idx(0, j + 1)) for j in range(nt)])
     outer = orient(quads, [(idx(nr, j), idx(nr, j + 1)) for j in range(nt)])
