@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--adj-steps", type=int, default=500)
     ap.add_argument("--adj-ckpt", type=int, default=25)
     ap.add_argument("--adj-dirs", type=int, default=20)
+    ap.add_argument("--adjoint-large", action="store_true",
+                    help="the combined large case: 512x512 jittered cavity, K=7, Re=5000, 200 RK4 steps, mixed "
+                         "forward + adjoint with FP32 states; gradient error against FP64 on the 128x128 mesh")
+    ap.add_argument("--large-n", type=int, default=512)
+    ap.add_argument("--large-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -401,6 +406,17 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.adjoint_large:
+        from ho2d import adjoint_case
+
+        if rank == 0:
+            with tempfile.TemporaryDirectory() as tmp:
+                r = adjoint_case.run_large(tmp, n=args.large_n, knod=7, steps=args.large_steps, ckpt=20)
+            print(json.dumps({"metric": "combined large case: adjoint gradient error (mixed, FP32 states) vs FP64 "
+                                        "adjoint on the 4x coarser mesh", "value": r["coarse"]["omega0_grad_rel_l2"],
+                              "unit": "relative L2", "higher_is_better": False, "n_gpus": 1,
+                              "data": "synthetic (seeded jitter, spectrum and lid)", "result": r}))
         return
     if args.adjoint:
         visible = os.environ.get("CUDA_VISIBLE_DEVICES")

@@ -360,6 +360,11 @@ __global__ void k_sub_scaled(size_t n, double* out, const double* x, const doubl
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = x[i] - J[i] * mu[i];
 }
 
+__global__ void k_copy_f2d(size_t n, const float* x, double* y) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = double(x[i]);
+}
+
 unsigned vec_grid(size_t n) {
     const size_t b = (n + 255) / 256;
     return (unsigned)(b < 1 ? 1 : (b > 4 * 148 ? 4 * 148 : b));
@@ -493,6 +498,11 @@ cudaError_t launch_axpby(size_t n, double* out, double a, const double* x, doubl
 cudaError_t launch_sub_scaled(size_t n, double* out, const double* x, const double* J, const double* mu,
                               cudaStream_t s) {
     k_sub_scaled<<<vec_grid(n), 256, 0, s>>>(n, out, x, J, mu);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_f2d(const float* x, double* y, size_t n, cudaStream_t s) {
+    k_copy_f2d<<<vec_grid(n), 256, 0, s>>>(n, x, y);
     return cudaGetLastError();
 }
 

@@ -364,6 +364,24 @@ Error Solver::apply_poisson_transpose(const double* x, double* y) {
     return {0, ""};
 }
 
+// One stored FP64 field of the time loop (checkpoint, segment stage input or psi), kept in
+// FP64 or, with FP32 state storage, rounded to FP32.
+Error Solver::store_state(void* dst, const double* src) {
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    if (adj_->state_bytes == 4) HO2D_CUDA(launch_copy_d2f(src, static_cast<float*>(dst), nv, d.stream), "store state");
+    else HO2D_CUDA(cudaMemcpyAsync(dst, src, nv * 8, cudaMemcpyDeviceToDevice, d.stream), "store state");
+    return {0, ""};
+}
+
+Error Solver::load_state(double* dst, const void* src) {
+    DeviceState& d = *d_;
+    const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
+    if (adj_->state_bytes == 4) HO2D_CUDA(launch_copy_f2d(static_cast<const float*>(src), dst, nv, d.stream), "load state");
+    else HO2D_CUDA(cudaMemcpyAsync(dst, src, nv * 8, cudaMemcpyDeviceToDevice, d.stream), "load state");
+    return {0, ""};
+}
+
 Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     HO2D_TRY(adjoint_supported(in_, stage32_));
     if (nsteps < 0 || ckpt_every < 1) return {1, "adjoint_forward needs nsteps >= 0 and ckpt_every >= 1"};
@@ -372,9 +390,16 @@ Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     AdjointState& a = *adj_;
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
     const int nck = (nsteps + ckpt_every - 1) / ckpt_every;
+    const size_t wb = adj_state32_ ? 4 : 8;  // bytes per stored value
+    if (a.state_bytes != wb) {
+        a.ckpt.clear();
+        a.seg_w.reset();
+        a.seg_psi.reset();
+        a.state_bytes = wb;
+    }
     while ((int)a.ckpt.size() < nck) {
         std::unique_ptr<DeviceBuffer> b(new DeviceBuffer);
-        HO2D_CUDA(b->alloc(nv * 8), "alloc checkpoint");
+        HO2D_CUDA(b->alloc(nv * wb), "alloc checkpoint");
         a.ckpt.push_back(std::move(b));
     }
     a.nsteps = -1;  // valid again once the sweep completes
@@ -383,10 +408,7 @@ Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     // the stage input of a step is omega itself
     HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
     for (int n = 0; n < nsteps; ++n) {
-        if (n % ckpt_every == 0)
-            HO2D_CUDA(cudaMemcpyAsync(a.ckpt[n / ckpt_every]->get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice,
-                                      d.stream),
-                      "checkpoint");
+        if (n % ckpt_every == 0) HO2D_TRY(store_state(a.ckpt[n / ckpt_every]->get(), d.omega.as<double>()));
         HO2D_TRY(step(1));
     }
     HO2D_CUDA(cudaMemcpyAsync(a.wT.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
@@ -406,13 +428,14 @@ Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* gra
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod, nb = (size_t)mesh_.n_eb * in_.knod;
     const Tableau tb = tableau(in_.ti_type);
     const int ns = tb.ns, every = a.every, nsteps = a.nsteps;
-    const size_t seg_bytes = (size_t)every * ns * nv * 8;
+    const size_t wb = a.state_bytes;
+    const size_t seg_bytes = (size_t)every * ns * nv * wb;
     if (a.seg_w.bytes() < seg_bytes) {
         HO2D_CUDA(a.seg_w.alloc(seg_bytes), "alloc segment");
         HO2D_CUDA(a.seg_psi.alloc(seg_bytes), "alloc segment");
     }
-    double* seg_w = a.seg_w.as<double>();
-    double* seg_psi = a.seg_psi.as<double>();
+    char* seg_w = static_cast<char*>(a.seg_w.get());
+    char* seg_psi = static_cast<char*>(a.seg_psi.get());
     double* lam = a.lam.as<double>();
     double* lk = a.lam_k.as<double>();
     auto copy = [&](void* dst, const void* src) -> Error {
@@ -425,26 +448,26 @@ Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* gra
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int n0 = seg * every, n1 = std::min(nsteps, n0 + every);
         // recompute the segment from its checkpoint, keeping every stage input and psi
-        HO2D_TRY(copy(d.omega.get(), a.ckpt[seg]->get()));
-        HO2D_TRY(copy(d.w_stage.get(), a.ckpt[seg]->get()));
+        HO2D_TRY(load_state(d.omega.as<double>(), a.ckpt[seg]->get()));
+        HO2D_TRY(copy(d.w_stage.get(), d.omega.get()));
         for (int n = n0; n < n1; ++n) {
             time_ = a.t0 + n * in_.dt;
             for (int s = 0; s < ns; ++s) {
-                const size_t idx = ((size_t)(n - n0) * ns + s) * nv;
-                HO2D_TRY(copy(seg_w + idx, d.w_stage.get()));
+                const size_t off = ((size_t)(n - n0) * ns + s) * nv * wb;
+                HO2D_TRY(store_state(seg_w + off, d.w_stage.as<double>()));
                 HO2D_TRY(stage_impl(tb.c[s], s, true));
-                HO2D_TRY(copy(seg_psi + idx, d.psi64.get()));
+                HO2D_TRY(store_state(seg_psi + off, d.psi64.as<double>()));
             }
         }
         // reverse sweep: lam_k_s = b_s lam + sum_{r > s} a_rs mu_r, lam += sum_s mu_s
         for (int n = n1 - 1; n >= n0; --n) {
             for (int s = ns - 1; s >= 0; --s) {
-                const size_t idx = ((size_t)(n - n0) * ns + s) * nv;
+                const size_t off = ((size_t)(n - n0) * ns + s) * nv * wb;
                 HO2D_CUDA(launch_axpby(nv, lk, tb.b[s], lam, 0.0, lam, d.stream), "lam_k");
                 for (int r = s + 1; r < ns; ++r)
                     if (tb.a[r][s] != 0.0) HO2D_CUDA(launch_axpby(nv, lk, 1.0, lk, tb.a[r][s], a.mus[r].as<double>(), d.stream), "lam_k");
-                HO2D_TRY(copy(d.w_stage.get(), seg_w + idx));
-                HO2D_TRY(copy(d.psi64.get(), seg_psi + idx));
+                HO2D_TRY(load_state(d.w_stage.as<double>(), seg_w + off));
+                HO2D_TRY(load_state(d.psi64.as<double>(), seg_psi + off));
                 time_ = a.t0 + n * in_.dt;
                 HO2D_TRY(stage_adjoint_dev(tb.c[s], a.mus[s].as<double>()));
             }

@@ -75,6 +75,8 @@ cudaError_t kt_residual(size_t n, const T* b, const T* y, T* r, const TReduce& r
 // ---- vector helpers (FP64)
 // out = a x + c y (out may alias x or y)
 cudaError_t launch_axpby(size_t n, double* out, double a, const double* x, double c, const double* y, cudaStream_t s);
+// y = x (FP32 -> FP64)
+cudaError_t launch_copy_f2d(const float* x, double* y, size_t n, cudaStream_t s);
 // out = x - J .* mu
 cudaError_t launch_sub_scaled(size_t n, double* out, const double* x, const double* J, const double* mu,
                               cudaStream_t s);

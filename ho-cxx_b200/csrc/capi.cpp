@@ -332,6 +332,14 @@ int ho2d_clean_up(ho2d_solver* h) {
     });
 }
 
+int ho2d_set_adjoint_storage(ho2d_solver* h, int32_t fp32) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (fp32 != 0 && fp32 != 1) return {HO2D_ERR_ARG, "storage must be 0 (FP64) or 1 (FP32)"};
+        h->s.set_adjoint_storage(fp32 == 1);
+        return {0, ""};
+    });
+}
+
 int ho2d_adjoint_forward(ho2d_solver* h, int32_t nsteps, int32_t ckpt_every) {
     return guarded(h, [&]() -> ho2d::Error {
         if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};

@@ -98,6 +98,8 @@ class Solver {
     // y = A^T x with the transposed matrix-free Poisson operator (FP64)
     Error apply_poisson_transpose(const double* x, double* y);
     int adjoint_steps() const;
+    // FP32 (true) or FP64 storage of checkpoints and recomputed stage states
+    void set_adjoint_storage(bool fp32) { adj_state32_ = fp32; }
     int last_adjoint_iterations() const { return last_adj_iters_; }
     double last_adjoint_residual() const { return last_adj_res_; }
 
@@ -143,6 +145,9 @@ class Solver {
     Error adjoint_prepare();
     Error stage_adjoint_dev(double coeff, double* out);
     Error transposed_solve(const double* rhs, double* mu);
+    Error store_state(void* dst, const double* src);
+    Error load_state(double* dst, const void* src);
+    bool adj_state32_ = false;
     template <typename T>
     Error kt_run(T* x, const T* b, bool f32, double tol, int& iters);
     int force_points_ = 0;  // boundary points of the "object" group (0: none)

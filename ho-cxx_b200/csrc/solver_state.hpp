@@ -120,6 +120,7 @@ struct AdjointState {
     DeviceBuffer seg_w, seg_psi, wT, psiT;
     int nsteps = -1, every = 1;
     double t0 = 0.0;
+    size_t state_bytes = 8;  // 8: FP64 state storage, 4: FP32
 };
 
 namespace {

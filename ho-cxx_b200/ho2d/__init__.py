@@ -257,6 +257,10 @@ class HO_2D:
         return fx.value, fy.value
 
     # -- discrete adjoint (no counterpart in the reference; ho2d.adjoint wraps it for torch)
+    def set_adjoint_storage(self, fp32: bool) -> None:
+        """FP32 (True) or FP64 storage of the adjoint's checkpoints and stage states."""
+        self._check(self._lib.ho2d_set_adjoint_storage(self._h, 1 if fp32 else 0))
+
     def adjoint_forward(self, nsteps: int, ckpt_every: int = 25) -> None:
         """nsteps time steps from the current state, keeping the vorticity every ckpt_every steps."""
         self._check(self._lib.ho2d_adjoint_forward(self._h, int(nsteps), int(ckpt_every)))

@@ -27,18 +27,21 @@ def cavity_dt(n: int, knod: int, u_max: float = 1.2, cfl: float = 0.5) -> float:
 
 class DifferentiationCase:
     def __init__(self, workdir: str, n: int = 64, knod: int = 5, reyn: float = 1000.0, steps: int = 500,
-                 tol: float = 1e-13, max_iter: int = 2000):
+                 tol: float = 1e-13, max_iter: int = 2000, jitter: float = 0.0, w0_seed: int = 4,
+                 precision: int = FP64):
         self.n, self.knod, self.reyn, self.steps = n, knod, reyn, steps
         self.dt = cavity_dt(n, knod)
-        self.inp = meshgen.make_case(f"cavity{n}", workdir, knod=knod, steps=steps, dt=self.dt, reyn=reyn)
+        name = f"cavityj{n}" if jitter > 0 else f"cavity{n}"
+        self.inp = meshgen.make_case(name, workdir, knod=knod, steps=steps, dt=self.dt, reyn=reyn, jitter=jitter,
+                                     seed=5)
         self.tol, self.max_iter = tol, max_iter
-        self.s = self.solver(FP64)
+        self.s = self.solver(precision)
         s = self.s
         xy = s.getsolnpts_d()
         bp = s.get_boundary_points()
         self.top = s.get_boundary(capi.BC_PARL_VEL) == -1.0  # BC_parl_vel = -1 on the lid (problem type 1)
         self.bx = bp[..., 0]
-        self.w0 = meshgen.sine_spectrum(xy, seed=4)
+        self.w0 = meshgen.sine_spectrum(xy, seed=w0_seed)
         self.a = meshgen.lid_coefficients(seed=41)
         m = np.arange(1, len(self.a) + 1)
         # d BC_parl_vel / d a_m on the lid (BC_parl_vel = -u there)
@@ -69,9 +72,10 @@ class DifferentiationCase:
     def J(self, w0, a) -> float:
         return 0.5 * float(np.sum((self.run(self.s, w0, a) - self.target) ** 2))
 
-    def gradient(self, precision: int, ckpt: int) -> dict:
+    def gradient(self, precision: int, ckpt: int, fp32_state: bool = False, solver: HO_2D | None = None) -> dict:
         """Adjoint gradient (dJ/d omega0, dJ/d a) and the wall time of its two sweeps."""
-        s = self.s if precision == FP64 else self.solver(precision)
+        s = solver if solver is not None else (self.s if precision == FP64 else self.solver(precision))
+        s.set_adjoint_storage(fp32_state)
         self._start(s, self.w0, self.a)
         l0 = s.launch_count()
         t0 = time.perf_counter()
@@ -129,4 +133,69 @@ def run(workdir: str, n: int = 64, knod: int = 5, steps: int = 500, ckpt: int = 
                      "J": g["J"], "forward_s": g["forward_s"], "backward_s": g["backward_s"],
                      "launches": g["launches"], "last_transposed_iterations": g["last_transposed_iterations"],
                      "grad_lid": [float(x) for x in g["ga"]]}
+    return out
+
+
+def device_memory_used() -> float | None:
+    """Bytes in use on the current device (all allocations of this process), or None."""
+    try:
+        import torch
+
+        free, total = torch.cuda.mem_get_info()
+        return float(total - free)
+    except Exception:
+        return None
+
+
+def host_memory_available() -> float:
+    for line in open("/proc/meminfo"):
+        if line.startswith("MemAvailable:"):
+            return float(line.split()[1]) * 1024.0
+    return 0.0
+
+
+def run_large(workdir: str, n: int = 512, knod: int = 7, steps: int = 200, ckpt: int = 20, coarse: int = 4,
+              host_bytes_needed: float = 60e9) -> dict:
+    """The combined large case: jittered cavity n x n (+/-0.1h, seed 5), K = 7, Re = 5000,
+    omega0 from the seeded spectrum (seed 3), lid and target as in the differentiation
+    case. (1) On the n/coarse mesh: the mixed-precision adjoint with FP32 state storage
+    against the FP64 adjoint with FP64 states (relative L2 difference of both gradients).
+    (2) On the full mesh: mixed forward + adjoint sweep, FP32 states, checkpoints every
+    `ckpt` steps: wall times and device memory. The full mesh is skipped (and the reason
+    reported) when the host has too little free memory for the assembly of its Poisson
+    blocks (5 K^4 FP64 values per element)."""
+    import os
+
+    out = {"n": n, "knod": knod, "steps": steps, "ckpt_every": ckpt}
+    nc = n // coarse
+    cdir = os.path.join(workdir, "coarse")
+    c = DifferentiationCase(cdir, n=nc, knod=knod, reyn=5000.0, steps=steps, tol=1e-12, max_iter=500, jitter=0.1,
+                            w0_seed=3)
+    g64 = c.gradient(FP64, ckpt, fp32_state=False)
+    g32 = c.gradient(MIXED_KRYLOV, ckpt, fp32_state=True)
+    out["coarse"] = {"n": nc, "dof": c.s.N_el * knod * knod, "dt": c.dt,
+                     "omega0_grad_rel_l2": float(np.linalg.norm(g32["gw"] - g64["gw"]) / np.linalg.norm(g64["gw"])),
+                     "lid_grad_rel_l2": float(np.linalg.norm(g32["ga"] - g64["ga"]) / np.linalg.norm(g64["ga"])),
+                     "fp64": {k: g64[k] for k in ("J", "forward_s", "backward_s")},
+                     "mixed_fp32_state": {k: g32[k] for k in ("J", "forward_s", "backward_s")}}
+    avail = host_memory_available()
+    out["host_memory_available"] = avail
+    if avail < host_bytes_needed:
+        out["full"] = {"skipped": f"host memory available {avail / 1e9:.0f} GB < {host_bytes_needed / 1e9:.0f} GB "
+                                  f"needed for the host assembly"}
+        return out
+    fdir = os.path.join(workdir, "full")
+    t0 = time.perf_counter()
+    f = DifferentiationCase(fdir, n=n, knod=knod, reyn=5000.0, steps=steps, tol=1e-12, max_iter=500, jitter=0.1,
+                            w0_seed=3, precision=MIXED_KRYLOV)
+    setup_s = time.perf_counter() - t0
+    m0 = device_memory_used()
+    g = f.gradient(MIXED_KRYLOV, ckpt, fp32_state=True, solver=f.s)
+    m1 = device_memory_used()
+    out["full"] = {"n_el": f.s.N_el, "dof": f.s.N_el * knod * knod, "dt": f.dt, "setup_and_target_s": setup_s,
+                   "forward_s": g["forward_s"], "backward_s": g["backward_s"], "J": g["J"],
+                   "grad_lid": [float(x) for x in g["ga"]], "omega0_grad_norm": float(np.linalg.norm(g["gw"])),
+                   "device_bytes_before_adjoint": m0, "device_bytes_after_adjoint": m1,
+                   "adjoint_state_bytes_fp32": f.state_bytes(ckpt) // 2,
+                   "last_transposed_iterations": g["last_transposed_iterations"]}
     return out

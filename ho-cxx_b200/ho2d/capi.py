@@ -68,6 +68,7 @@ SIGNATURES = {
     "ho2d_set_ptog_weights": (ctypes.c_int, [_P, _I, _DP]),
     "ho2d_get_hoquad_weights": (ctypes.c_int, [_P, _I, _DP]),
     "ho2d_clean_up": (ctypes.c_int, [_P]),
+    "ho2d_set_adjoint_storage": (ctypes.c_int, [_P, _I]),
     "ho2d_adjoint_forward": (ctypes.c_int, [_P, _I, _I]),
     "ho2d_adjoint_backward": (ctypes.c_int, [_P, _I, _DP, _DP, _I, _DP]),
     "ho2d_stage_adjoint": (ctypes.c_int, [_P, _D, _I, _DP, _DP, _I, _DP]),

@@ -214,6 +214,10 @@ int ho2d_clean_up(ho2d_solver* handle);
  * stage. Advection type 1; precision HO2D_FP64, or HO2D_MIXED_KRYLOV, whose forward and
  * transposed Poisson solves are FP32 Krylov inside FP64 refinement (HO2D_MIXED is
  * rejected with HO2D_ERR_UNSUPPORTED). */
+/* Storage of the adjoint's checkpoints and recomputed stage states: 0 = FP64 (default),
+ * 1 = FP32 (half the memory; the backward sweep then linearises about a trajectory
+ * recomputed from FP32-rounded states). Takes effect at the next ho2d_adjoint_forward. */
+int ho2d_set_adjoint_storage(ho2d_solver* handle, int32_t fp32);
 /* Runs nsteps time steps from the current state (as ho2d_step) and keeps the vorticity
  * every ckpt_every steps for the backward sweep. */
 int ho2d_adjoint_forward(ho2d_solver* handle, int32_t nsteps, int32_t ckpt_every);

@@ -134,6 +134,20 @@ def test_mixed_krylov_adjoint_matches_fp64():
         assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
 
 
+def test_fp32_state_storage_is_close_to_fp64():
+    inp = golden_input("cav4_rk4")
+    res = []
+    for fp32 in (False, True):
+        s = solver_for(inp)
+        s.set_adjoint_storage(fp32)
+        w0 = rng_of(50).standard_normal((s.N_el, s.Knod, s.Knod))
+        s.setsolnvort_d(w0)
+        s.adjoint_forward(6, 3)
+        res.append(s.adjoint_backward(rng_of(51).standard_normal(w0.shape)))
+    for a, b in zip(res[1], res[0]):
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b)
+
+
 def cavity_problem(tmp_path, n=12, knod=4, reyn=1000.0, steps=10, dt=2e-3):
     """A small version of the differentiation case: seeded sine-mode vorticity, lid
     u(x) = 1 + sum a_m sin(m pi x), target from a second seed."""
