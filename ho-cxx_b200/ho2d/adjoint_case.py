@@ -20,9 +20,13 @@ import numpy as np
 from . import FP64, MIXED_KRYLOV, HO_2D, capi, meshgen
 
 
-def cavity_dt(n: int, knod: int, u_max: float = 1.2, cfl: float = 0.5) -> float:
-    """dt = cfl h / (u_max K^2), h = 1/n: the CFL-0.5 step of the benchmark cases."""
-    return cfl * (1.0 / n) / (u_max * knod * knod)
+def cavity_dt(n: int, knod: int, u_max: float = 1.2, cfl: float = 0.5, reyn: float = 1000.0,
+              jitter: float = 0.0) -> float:
+    """The smaller of the CFL-0.5 step cfl h / (u_max K^2), h = 1/n, and the viscous bound
+    of explicit RK4 on the FR Laplacian 1.5 h_min^2 Re / K^4 (meshgen.viscous_dt), with
+    h_min = (1 - 2 jitter) / n the smallest edge a +/-jitter*h perturbation can leave."""
+    h_min = (1.0 - 2.0 * jitter) / n
+    return min(cfl * (1.0 / n) / (u_max * knod * knod), 1.5 * h_min * h_min * reyn / knod ** 4)
 
 
 class DifferentiationCase:
@@ -30,7 +34,7 @@ class DifferentiationCase:
                  tol: float = 1e-13, max_iter: int = 2000, jitter: float = 0.0, w0_seed: int = 4,
                  precision: int = FP64):
         self.n, self.knod, self.reyn, self.steps = n, knod, reyn, steps
-        self.dt = cavity_dt(n, knod)
+        self.dt = cavity_dt(n, knod, reyn=reyn, jitter=jitter)
         name = f"cavityj{n}" if jitter > 0 else f"cavity{n}"
         self.inp = meshgen.make_case(name, workdir, knod=knod, steps=steps, dt=self.dt, reyn=reyn, jitter=jitter,
                                      seed=5)
@@ -178,6 +182,10 @@ def run_large(workdir: str, n: int = 512, knod: int = 7, steps: int = 200, ckpt:
                      "lid_grad_rel_l2": float(np.linalg.norm(g32["ga"] - g64["ga"]) / np.linalg.norm(g64["ga"])),
                      "fp64": {k: g64[k] for k in ("J", "forward_s", "backward_s")},
                      "mixed_fp32_state": {k: g32[k] for k in ("J", "forward_s", "backward_s")}}
+    import json
+    import sys
+
+    print(json.dumps({"coarse": out["coarse"]}), file=sys.stderr, flush=True)
     avail = host_memory_available()
     out["host_memory_available"] = avail
     if avail < host_bytes_needed:
