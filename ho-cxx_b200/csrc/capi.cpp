@@ -237,6 +237,17 @@ int ho2d_get_forces(ho2d_solver* h, double* fx, double* fy) {
     return guarded(h, [&]() { return h->s.get_forces(fx, fy); });
 }
 
+int ho2d_set_output_dir(ho2d_solver* h, const char* dir) {
+    return guarded(h, [&]() -> ho2d::Error {
+        h->s.set_output_dir(dir ? dir : "");
+        return {0, ""};
+    });
+}
+
+int ho2d_write_vtk(ho2d_solver* h, int32_t indx, int32_t subidx, const char* dir) {
+    return guarded(h, [&]() { return h->s.write_vtk(indx, subidx, dir ? dir : ""); });
+}
+
 int ho2d_set_defaults(ho2d_solver* h) {
     return guarded(h, [&]() -> ho2d::Error {
         h->s.set_defaults();

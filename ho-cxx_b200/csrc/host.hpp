@@ -64,6 +64,11 @@ struct Mesh {
     // boundaries loaded from arrays (hybrid drivers): per-edge normal / parallel velocity
     // given with the edge (NaN where none was given)
     std::vector<double> edge_normvel, edge_parlvel;
+    // the node numbering of the input (the .msh file's node tags from the smallest, or the
+    // driver's node arrays): all its nodes and the input index of each compact node, as the
+    // reference numbers them in its VTK output
+    std::vector<double> file_xy;
+    std::vector<int> file_index;
 };
 
 // 1-D bases on the K Gauss-Legendre solution points and the L equispaced geometry nodes.

@@ -673,8 +673,12 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     ra.omega = d.omega.as<double>();
     ra.acc = d.acc.as<double>();
     ra.w_next = update ? d.w_stage.as<T>() : nullptr;
-    ra.rhs_diff = update ? nullptr : d.rhs_diff.as<T>();
-    ra.rhs_adv = update ? nullptr : d.rhs_adv.as<T>();
+    // the RHS terms are kept from a lone stage and from the last stage of a step (the
+    // reference's RHS arrays hold the last stage computed; its VTK output writes them)
+    const int ns = in_.ti_type == 4 ? 4 : (in_.ti_type == 2 ? 2 : 1);
+    const bool keep_rhs = !update || rk_stage == ns - 1;
+    ra.rhs_diff = keep_rhs ? d.rhs_diff.as<T>() : nullptr;
+    ra.rhs_adv = keep_rhs ? d.rhs_adv.as<T>() : nullptr;
     ra.k_out = update ? nullptr : d.kout.as<T>();
     HO2D_CUDA(launch_residual<T>(K, g, b, bc, ra, d.stream), "residual");
     launches_ += 3;
@@ -777,10 +781,16 @@ Error Solver::solve() {
     HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
     const int nt = in_.num_steps, df = std::max(1, in_.dump_freq);
     for (int ti = 0; ti < nt; ++ti) {
-        if (ti % df == 0) HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
+        if (ti % df == 0) {
+            HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
+            if (!output_dir_.empty()) HO2D_TRY(write_vtk(ti, -1, output_dir_));
+        }
         HO2D_TRY(step(1));
     }
-    if (nt % df == 0) HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
+    if (nt % df == 0) {
+        HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
+        if (!output_dir_.empty()) HO2D_TRY(write_vtk(nt, -1, output_dir_));
+    }
     HO2D_CUDA(cudaStreamSynchronize(d_->stream), "solve");
     return {0, ""};
 }

@@ -62,6 +62,10 @@ class Solver {
     Error set_boundary(int which, const double* in);
     Error get_solution_points(double* out);
     Error get_boundary_points(double* out);  // [N_eb][K][2] in boundary-array order
+    // save_vorticity_vtk + save_smooth_vtk of the current fields into dir (output.cu)
+    Error write_vtk(int indx, int subidx, const std::string& dir);
+    // directory for the VTK files ho2d_solve writes at dump steps ("" = none written)
+    void set_output_dir(const std::string& dir) { output_dir_ = dir; }
     // FP64 force (ρ = 1) on the boundary group named "object", from the wall vorticity and
     // its normal flux of the latest stage
     Error get_forces(double* fx, double* fy);
@@ -166,6 +170,7 @@ class Solver {
     // outer time step of solveto_d (src/HO_2D.cpp:4208-4210): hybrid BCs interpolate in it
     double t_start_ = 0.0, t_end_ = 0.0;
     bool hybrid_ = false;                     // enable_hybrid: set_vort feeds the blend target
+    std::string output_dir_;                  // where solve() writes its VTK files (empty: none)
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

@@ -201,6 +201,16 @@ class HO_2D:
         self._check(self._lib.ho2d_get_hoquad_weights(self._h, out.size, capi.dptr(out)))
         return out
 
+    def set_output_dir(self, path) -> None:
+        """Where solve_vorticity_streamfunction writes its VTK files (None: nowhere)."""
+        self._check(self._lib.ho2d_set_output_dir(self._h, None if path is None else str(path).encode()))
+
+    def trigger_write(self, indx: int, subidx: int = -1, path=None) -> None:
+        """The reference's two VTK files of the current fields (save_vorticity_vtk,
+        save_smooth_vtk) into path (None: the working directory)."""
+        self._check(self._lib.ho2d_write_vtk(self._h, int(indx), int(subidx),
+                                             None if path is None else str(path).encode()))
+
     def clean_up(self) -> None:
         self._check(self._lib.ho2d_clean_up(self._h))
         self._setup = False

@@ -54,6 +54,8 @@ SIGNATURES = {
     "ho2d_apply_poisson_noalloc": (ctypes.c_int, [_P, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "ho2d_get_forces": (ctypes.c_int, [_P, _DP, _DP]),
     "ho2d_get_boundary_points": (ctypes.c_int, [_P, _I, _DP]),
+    "ho2d_set_output_dir": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "ho2d_write_vtk": (ctypes.c_int, [_P, _I, _I, ctypes.c_char_p]),
     "ho2d_set_defaults": (ctypes.c_int, [_P]),
     "ho2d_enable_hybrid": (ctypes.c_int, [_P]),
     "ho2d_set_elemorder": (ctypes.c_int, [_P, _I]),

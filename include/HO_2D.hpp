@@ -85,8 +85,8 @@ class HO_2D {
     void setopenvort_d(int32_t len, const double* vort) { check(ho2d_set_open_vorticity(h_, len, vort)); }
     void setptogweights_d(int32_t len, const double* wgt) { check(ho2d_set_ptog_weights(h_, len, wgt)); }
     void get_hoquad_weights_d(int32_t len, double* w) { check(ho2d_get_hoquad_weights(h_, len, w)); }
-    // VTK output (save_vorticity_vtk / save_smooth_vtk) is not provided
-    void trigger_write(int32_t, int32_t) { throw HO2DException(HO2D_ERR_UNSUPPORTED, "VTK output is not provided"); }
+    // the two VTK files of the current fields into the working directory
+    void trigger_write(int32_t indx, int32_t subidx) { check(ho2d_write_vtk(h_, indx, subidx, nullptr)); }
     void clean_up() {
         check(ho2d_clean_up(h_));
         setup_ = false;

@@ -72,8 +72,17 @@ int ho2d_read_input(ho2d_solver* handle, const char* path);
 int ho2d_setup(ho2d_solver* handle);
 /* Replaces HO_2D::solve_vorticity_streamfunction (src/HO_2D.cpp:1390-1463) for
  * num_time_steps steps from the initial vorticity, including the extra Poisson solve and
- * velocity recovery at every dump step; VTK files are not written. */
+ * velocity recovery at every dump step; there it writes the reference's two VTK files
+ * (ho2d_write_vtk) into the directory set by ho2d_set_output_dir, if one is set. */
 int ho2d_solve(ho2d_solver* handle);
+/* Directory for the VTK files of ho2d_solve (NULL or "" = write none, the default). */
+int ho2d_set_output_dir(ho2d_solver* handle, const char* dir);
+/* Replaces save_vorticity_vtk and save_smooth_vtk (src/HO_2D.cpp:3369-3692), and
+ * trigger_write (4262-4271): writes vorticity<p>_K<K>[_<subidx>]_<indx>.vtk (solution
+ * points) and problem<p>_K<K>[_<subidx>]_<indx>.vtk (node averages) of the current fields
+ * into dir (NULL: the working directory); subidx < 0 leaves it out of the names. The
+ * reference's sample-point file is not written. */
+int ho2d_write_vtk(ho2d_solver* handle, int32_t indx, int32_t subidx, const char* dir);
 /* Replaces nsteps calls of HO_2D::solve_advection_diffusion (src/HO_2D.cpp:1465-1531),
  * advancing the solver time by dt after each. */
 int ho2d_step(ho2d_solver* handle, int32_t nsteps);

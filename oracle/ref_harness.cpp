@@ -26,6 +26,8 @@
 //   --time-stages N        time N RK stages (Euler_time_integrate on the current vorticity,
 //                          coefficients cycling 0, .5, .5, 1) and print a JSON line
 //   --t0 T                 start the time loop at time T instead of 0
+//   --solve                run solve_vorticity_streamfunction (writes the reference's VTK
+//                          files into the input's directory) and stop
 //   --verbose              keep the reference's stdout
 // or:   ho2d_ref --hybrid SPECDIR OUTDIR [--verbose]   (see run_hybrid)
 #include "HO_2D.hpp"
@@ -203,7 +205,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     std::string input = argv[1], outdir = argv[2];
-    bool do_setup = false, verbose = false, do_stage = false;
+    bool do_setup = false, verbose = false, do_stage = false, do_solve = false;
     double stage_coeff = 0.0, dt_override = -1.0, t0 = 0.0;
     long nsteps = 0, every = 0, ntime = 0, nstages = 0;
     std::string init_vort, lid;
@@ -220,6 +222,7 @@ int main(int argc, char** argv) {
         else if (a == "--time" && i + 1 < argc) ntime = std::atol(argv[++i]);
         else if (a == "--time-stages" && i + 1 < argc) nstages = std::atol(argv[++i]);
         else if (a == "--t0" && i + 1 < argc) t0 = std::atof(argv[++i]);
+        else if (a == "--solve") do_solve = true;
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     mkdir(outdir.c_str(), 0755);
@@ -342,6 +345,13 @@ int main(int argc, char** argv) {
         std::fclose(f);
     }
 
+    if (do_solve) {
+        // the reference's whole time loop with its own VTK output (written into the input's
+        // directory, the working directory here)
+        ho.solve_vorticity_streamfunction();
+        std::cout.rdbuf(saved);
+        return 0;
+    }
     if (do_stage) {
         ho.Euler_time_integrate(ho.vorticity, ho.k1, stage_coeff);
         dump_f64(outdir, "stage_psi", {N, K, K}, &ho.stream_function[0][0][0]);

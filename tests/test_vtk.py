@@ -1,0 +1,75 @@
+"""VTK output against the reference's own files.
+
+The reference (oracle/_ref/ho2d_ref --solve: solve_vorticity_streamfunction with its VTK
+writers, direct Poisson solve) and ho2d_solve with an output directory run the same golden
+case; both write vorticity<p>_K<K>_<step>.vtk and problem<p>_K<K>_<step>.vtk at the dump
+steps. The files must have the same lines and words; numbers agree to the printed six
+significant digits (relative 2e-5, plus 1e-8 of the file's largest value for values that
+are round-off around zero).
+"""
+
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, REPO
+
+REF = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
+
+
+def _num(t):
+    try:
+        return float(t)
+    except ValueError:
+        return None
+
+
+def compare_vtk(a_path, b_path):
+    a = open(a_path).read().split("\n")
+    b = open(b_path).read().split("\n")
+    assert len(a) == len(b), (a_path, len(a), len(b))
+    vals = [abs(x) for line in a for t in line.split() if (x := _num(t)) is not None and np.isfinite(x)]
+    scale = max(vals) if vals else 1.0
+    worst = 0.0
+    for la, lb in zip(a, b):
+        ta, tb = la.split(), lb.split()
+        assert len(ta) == len(tb), (la, lb)
+        for x, y in zip(ta, tb):
+            fx, fy = _num(x), _num(y)
+            if fx is None or fy is None:
+                assert x == y, (la, lb)
+            else:
+                d = abs(fx - fy)
+                assert d <= 2e-5 * max(abs(fx), abs(fy)) + 1e-8 * scale, (la, lb)
+                worst = max(worst, d / (abs(fx) + 1e-8 * scale))
+    return worst
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cav4_rk4", "bfs2_rk4", "cyl4x8_rk4"])
+def test_vtk_files_match_reference(tmp_path, case):
+    if not os.path.exists(REF):
+        pytest.skip("oracle/_ref/ho2d_ref not built")
+    from ho2d import HO_2D
+
+    d = tmp_path / "case"
+    shutil.copytree(os.path.join(GOLDEN, case), d)
+    env = dict(os.environ, HO_SHIM_SOLVER="direct")
+    subprocess.run([REF, str(d / "input.dat"), str(tmp_path / "refout"), "--solve"], check=True, env=env,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref_files = sorted(f for f in os.listdir(d) if f.endswith(".vtk"))
+    assert len(ref_files) >= 4
+    ours = tmp_path / "ours"
+    ours.mkdir()
+    s = HO_2D()
+    s.read_input_file(str(d / "input.dat"))
+    s.set_poisson_tolerance(1e-14, 2000)
+    s.setup()
+    s.set_output_dir(str(ours))
+    s.solve_vorticity_streamfunction()
+    assert sorted(os.listdir(ours)) == ref_files
+    for f in ref_files:
+        compare_vtk(str(ours / f), str(d / f))
