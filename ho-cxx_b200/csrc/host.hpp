@@ -64,11 +64,6 @@ struct Mesh {
     // boundaries loaded from arrays (hybrid drivers): per-edge normal / parallel velocity
     // given with the edge (NaN where none was given)
     std::vector<double> edge_normvel, edge_parlvel;
-    // the node numbering of the input (the .msh file's node tags from the smallest, or the
-    // driver's node arrays): all its nodes and the input index of each compact node, as the
-    // reference numbers them in its VTK output
-    std::vector<double> file_xy;
-    std::vector<int> file_index;
 };
 
 // 1-D bases on the K Gauss-Legendre solution points and the L equispaced geometry nodes.
@@ -137,6 +132,18 @@ Error setup_bcs(const Input& in, const Mesh& mesh, const Bases& B, BoundaryCondi
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
                       PoissonOperator& op);
 int tensor2fem(int i, int j, int lnod_in);
+
+// Fields written by the VTK output: volume arrays [N][K][K] (vorticity, streamfunction,
+// Cartesian velocity components, the two RHS terms), boundary arrays [N_eb][K]
+// (BC_vorticity, BC_normal_vel in the local h direction, BC_parl_vel).
+struct VtkFields {
+    const double *w, *psi, *u, *v, *rhs_diff, *rhs_adv;
+    const double *bc_w, *bc_nv, *bc_pv;
+};
+// save_vorticity_vtk + save_smooth_vtk (src/HO_2D.cpp:3369-3692) into dir ("" = working
+// directory); subidx < 0 leaves it out of the file names
+Error write_vtk_files(const Mesh& mesh, const Bases& B, int problem_type, const VtkFields& f, int indx, int subidx,
+                      const std::string& dir);
 int tensor2fem_1d(int i, int lnod_in);
 
 }  // namespace ho2d

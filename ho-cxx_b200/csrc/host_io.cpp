@@ -280,11 +280,9 @@ Error read_msh(const std::string& path, int occ, Mesh& m) {
             remap[t] = (int)(m.node_xy.size() / 2);
             m.node_xy.push_back(raw_xy[2 * t]);
             m.node_xy.push_back(raw_xy[2 * t + 1]);
-            m.file_index.push_back((int)t);
         }
         return remap[t];
     };
-    m.file_xy = raw_xy;
     m.edge_nodes.resize(edges_raw.size());
     for (size_t e = 0; e < edges_raw.size(); ++e)
         for (long t : edges_raw[e]) {
@@ -386,9 +384,6 @@ Error mesh_from_arrays(int iorder, int nxy, const double* xy, int nidx, const in
     if (m.lnod < 2 || m.lnod > 4) return {4, "geometry order must be 1, 2 or 3 (Lnod 2..4)"};
     if (nxy < 2 || nxy % 2 || !xy) return {1, "node array must hold x, y pairs"};
     m.node_xy.assign(xy, xy + nxy);
-    m.file_xy = m.node_xy;
-    m.file_index.resize(nxy / 2);
-    for (int i = 0; i < nxy / 2; ++i) m.file_index[i] = i;
     const int nper = m.lnod * m.lnod, nn = nxy / 2;
     if (nidx <= 0 || nidx % nper || !idx) return {1, "element index array is not a multiple of Lnod^2"};
     m.elem_nodes.resize(nidx / nper);

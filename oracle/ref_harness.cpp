@@ -27,7 +27,8 @@
 //                          coefficients cycling 0, .5, .5, 1) and print a JSON line
 //   --t0 T                 start the time loop at time T instead of 0
 //   --solve                run solve_vorticity_streamfunction (writes the reference's VTK
-//                          files into the input's directory) and stop
+//                          files into the input's directory), dump the fields the last
+//                          files were written from (solve_*.npy) and stop
 //   --verbose              keep the reference's stdout
 // or:   ho2d_ref --hybrid SPECDIR OUTDIR [--verbose]   (see run_hybrid)
 #include "HO_2D.hpp"
@@ -349,6 +350,20 @@ int main(int argc, char** argv) {
         // the reference's whole time loop with its own VTK output (written into the input's
         // directory, the working directory here)
         ho.solve_vorticity_streamfunction();
+        // the fields the last VTK files were written from
+        dump_f64(outdir, "solve_vorticity", {N, K, K}, &ho.vorticity[0][0][0]);
+        dump_f64(outdir, "solve_psi", {N, K, K}, &ho.stream_function[0][0][0]);
+        std::vector<double> vel(N * K * K * 2);
+        for (size_t i = 0; i < N * K * K; ++i) {
+            vel[2 * i] = (&ho.velocity_cart[0][0][0])[i].x;
+            vel[2 * i + 1] = (&ho.velocity_cart[0][0][0])[i].y;
+        }
+        dump_f64(outdir, "solve_vel", {N, K, K, 2}, vel.data());
+        dump_f64(outdir, "solve_rhs_diff", {N, K, K}, &ho.RHS_diffusive[0][0][0]);
+        dump_f64(outdir, "solve_rhs_adv", {N, K, K}, &ho.RHS_advective[0][0][0]);
+        dump_f64(outdir, "solve_bc_w", {Neb, K}, &ho.BC_vorticity[0][0]);
+        dump_f64(outdir, "solve_bc_nv", {Neb, K}, &ho.BC_normal_vel[0][0]);
+        dump_f64(outdir, "solve_bc_pv", {Neb, K}, &ho.BC_parl_vel[0][0]);
         std::cout.rdbuf(saved);
         return 0;
     }
