@@ -146,4 +146,17 @@ Error write_vtk_files(const Mesh& mesh, const Bases& B, int problem_type, const 
                       const std::string& dir);
 int tensor2fem_1d(int i, int lnod_in);
 
+// Hybrid operation (host_hybrid.cpp): the edges of the "open" boundary (null if none), the
+// getopenpts_d array length, solution-point areas [N][K][K], open-boundary points
+// [open edge][K][x, y], outward unit normals of the open edges [N_eb][K][2], and the
+// normal / parallel split of the driver's open-boundary velocities into [N_eb][K] arrays.
+const std::vector<int>* open_boundary_edges(const Mesh& m);
+int open_point_count(const Mesh& m, int K);
+void solution_areas(const Bases& B, const Metrics& M, int n_el, double* out);
+void open_points(const Mesh& m, const Bases& B, double* out);
+void open_normals(const Mesh& m, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
+                  std::vector<double>& nrm);
+void split_open_velocities(const Mesh& m, int K, const std::vector<double>& nrm, const double* xyvel, double* vn,
+                           double* vp);
+
 }  // namespace ho2d

@@ -374,7 +374,7 @@ Error process_mesh(Mesh& m) {
     return {0, ""};
 }
 
-// load_mesh_arrays_d (src/HO_2D.cpp:3832-3886): nodes [nxy/2][2], elements of Lnod^2 node
+// load_mesh_arrays_d (src/HO_2D.cpp:3823-3881): nodes [nxy/2][2], elements of Lnod^2 node
 // indices each (Gmsh order), then the boundaries named "wall" and "open" as Lnod-node
 // edges. Boundaries "inlet" and "outlet" follow through add_boundary_arrays.
 Error mesh_from_arrays(int iorder, int nxy, const double* xy, int nidx, const int* idx, int nwall, const int* wall,
@@ -397,7 +397,7 @@ Error mesh_from_arrays(int iorder, int nxy, const double* xy, int nidx, const in
     return {0, ""};
 }
 
-// arrays_to_boundary (src/HO_2D.cpp:3723-3829): one boundary group of n/Lnod edges, with
+// arrays_to_boundary (src/HO_2D.cpp:3724-3820): one boundary group of n/Lnod edges, with
 // nval optional values: one per edge (normal velocity) or two (parallel, then normal).
 Error add_boundary_arrays(Mesh& m, const std::string& name, int n, const int* idx, int nval, const double* vals) {
     if (n <= 0) return {0, ""};

@@ -1,5 +1,5 @@
 // hybrid.cu -- the hybrid-operation entry points of the reference's HO_2D
-// (src/HO_2D.hpp:251-290, src/HO_2D.cpp:3697-4278): an external Lagrangian (vortex)
+// (src/HO_2D.hpp:251-290, src/HO_2D.cpp:3698-4278): an external Lagrangian (vortex)
 // solver loads the mesh from arrays, sets the open-boundary velocity and vorticity and the
 // vorticity it wants blended in at the start and end of each outer step, and advances
 // with solveto_d. On the device the open-boundary values are interpolated in time and the
@@ -11,7 +11,7 @@
 
 namespace ho2d {
 
-// set_defaults (src/HO_2D.cpp:3697-3712)
+// set_defaults (src/HO_2D.cpp:3698-3713)
 void Solver::set_defaults() {
     Input in;
     in.knod = 3;
@@ -44,7 +44,7 @@ Error Solver::load_mesh_arrays(int iorder, int nxy, const double* xy, int nidx, 
     return mesh_from_arrays(iorder, nxy, xy, nidx, idx, nwall, wall, nopen, open, mesh_);
 }
 
-// load_inout_arrays_d (src/HO_2D.cpp:3889-3904): inlets, then outlets, each edge with its
+// load_inout_arrays_d (src/HO_2D.cpp:3884-3898): inlets, then outlets, each edge with its
 // normal velocity
 Error Solver::load_inout_arrays(int ninval, const double* velin, int nin, const int* idxin, int noutval,
                                 const double* velout, int nout, const int* idxout) {
@@ -53,7 +53,7 @@ Error Solver::load_inout_arrays(int ninval, const double* velin, int nin, const 
     return add_boundary_arrays(mesh_, "outlet", nout, idxout, noutval, velout);
 }
 
-// process_mesh_input (src/HO_2D.cpp:3907-3940)
+// process_mesh_input (src/HO_2D.cpp:3901-3937)
 Error Solver::process_mesh_input() {
     if (!input_done_) return {1, "call ho2d_set_defaults (or ho2d_read_input) first"};
     if (mesh_.elem_nodes.empty()) return {1, "load the mesh arrays first"};
@@ -62,11 +62,10 @@ Error Solver::process_mesh_input() {
 }
 
 // Device arrays of a hybrid run (zero until the driver sets them) and the unit outward
-// normals of the open edges: at face point k of the element that owns the edge, the
-// tangent (x_s, y_s) rotated (src/HO_2D.cpp:4040-4054), divided by |g|.
+// normals of the open edges (open_normals, host_hybrid.cpp).
 Error Solver::hybrid_upload() {
     DeviceState& d = *d_;
-    const int K = in_.knod, L = mesh_.lnod, lin = L - 1, neb = std::max(1, mesh_.n_eb);
+    const int K = in_.knod, neb = std::max(1, mesh_.n_eb);
     const size_t nv = (size_t)mesh_.n_el * K * K, nb = (size_t)neb * K;
     const std::vector<double> zb(nb, 0.0), zv(nv, 0.0);
     for (auto& b : d.hyb) HO2D_CUDA(upload(b, zb), "alloc hybrid boundary data");
@@ -75,97 +74,40 @@ Error Solver::hybrid_upload() {
     inl.resize(neb, 0.0);
     HO2D_CUDA(upload(d.hyb_inlet_nv, inl), "upload inlet velocities");
     for (auto& h : h_open_) h.assign(nb, 0.0);
-    open_normal_.assign(nb * 2, 0.0);
-    for (int e = 0; e < mesh_.n_eb; ++e) {
-        if (bc_.role[e] != ROLE_OPEN) continue;
-        const int el = mesh_.be_el[e], side = mesh_.be_side[e], ijp = kF2I[side];
-        const int dd = ijp / 2, t = ijp % 2;
-        const double coeff = 2.0 * t - 1.0;
-        for (int k = 0; k < K; ++k) {
-            double dx = 0.0, dy = 0.0;  // derivative along the face (xi on S/N faces, eta on W/E)
-            for (int j = 0; j < L; ++j)
-                for (int i = 0; i < L; ++i) {
-                    const int nd = mesh_.elem_nodes[el][tensor2fem(i, j, lin)];
-                    const double w = dd == 0 ? B_.gbb[i * 2 + t] * B_.gsgb[j * K + k] : B_.gsgb[i * K + k] * B_.gbb[j * 2 + t];
-                    dx += w * mesh_.node_xy[2 * nd];
-                    dy += w * mesh_.node_xy[2 * nd + 1];
-                }
-            const double an = M_.fAn[((size_t)el * 4 + ijp) * K + k];
-            const double nx = dd == 1 ? -dy : dy, ny = dd == 1 ? dx : -dx;
-            open_normal_[((size_t)e * K + k) * 2] = nx * coeff / an;
-            open_normal_[((size_t)e * K + k) * 2 + 1] = ny * coeff / an;
-        }
-    }
+    open_normals(mesh_, B_, M_, bc_, open_normal_);
+    open_normal_.resize(nb * 2, 0.0);
     return {0, ""};
 }
 
-int Solver::open_point_count() const {
-    for (size_t g = 0; g < mesh_.group_names.size(); ++g)
-        if (mesh_.group_names[g] == "open") return 2 * (int)mesh_.group_edges[g].size() * in_.knod;
-    return 0;
-}
+int Solver::open_point_count() const { return ho2d::open_point_count(mesh_, in_.knod); }
 
-static const std::vector<int>* open_edges(const Mesh& m) {
-    for (size_t g = 0; g < m.group_names.size(); ++g)
-        if (m.group_names[g] == "open") return &m.group_edges[g];
-    return nullptr;
-}
-
-// getopenpts_d (src/HO_2D.cpp:3999-4031): the K points of each open edge along the edge
+// getopenpts_d (src/HO_2D.cpp:4004-4042)
 Error Solver::get_open_points(double* out) {
     if (!setup_done_) return {1, "not set up"};
-    const std::vector<int>* oe = open_edges(mesh_);
-    if (!oe) return {0, ""};
-    const int K = in_.knod, L = mesh_.lnod, lin = L - 1;
-    for (size_t i = 0; i < oe->size(); ++i) {
-        const auto& en = mesh_.edge_nodes[(*oe)[i]];
-        for (int j = 0; j < K; ++j) {
-            double x = 0.0, y = 0.0;
-            for (int l = 0; l < L; ++l) {
-                const int nd = en[tensor2fem_1d(l, lin)];
-                x += B_.gsb[l * K + j] * mesh_.node_xy[2 * nd];
-                y += B_.gsb[l * K + j] * mesh_.node_xy[2 * nd + 1];
-            }
-            out[2 * (i * K + j)] = x;
-            out[2 * (i * K + j) + 1] = y;
-        }
-    }
+    open_points(mesh_, B_, out);
     return {0, ""};
 }
 
-// setopenvels_d (src/HO_2D.cpp:4035-4106): the end values become the start values; the new
-// Cartesian velocities, split into normal (outward) and parallel parts, become the end
-// values. Point j of edge i is paired with the normal at face point j of the owning
-// element, as in the reference.
+// setopenvels_d (src/HO_2D.cpp:4047-4122): the end values become the start values; the new
+// Cartesian velocities, split into normal (outward) and parallel parts
+// (split_open_velocities), become the end values.
 Error Solver::set_open_velocities(const double* xyvel) {
     if (!setup_done_ || in_.problem_type != 11) return {1, "not a set-up hybrid run (problem type 11)"};
     DeviceState& d = *d_;
-    const std::vector<int>* oe = open_edges(mesh_);
-    const int K = in_.knod;
     h_open_[0] = h_open_[1];
     h_open_[2] = h_open_[3];
-    if (oe)
-        for (size_t i = 0; i < oe->size(); ++i) {
-            const int e = (*oe)[i];
-            for (int j = 0; j < K; ++j) {
-                const size_t q = (size_t)e * K + j;
-                const double u = xyvel[2 * (i * K + j)], v = xyvel[2 * (i * K + j) + 1];
-                const double nx = open_normal_[2 * q], ny = open_normal_[2 * q + 1];
-                h_open_[1][q] = nx * u + ny * v;
-                h_open_[3][q] = nx * v - ny * u;
-            }
-        }
+    split_open_velocities(mesh_, in_.knod, open_normal_, xyvel, h_open_[1].data(), h_open_[3].data());
     for (int a = 0; a < 4; ++a)
         HO2D_CUDA(cudaMemcpy(d.hyb[a].get(), h_open_[a].data(), h_open_[a].size() * 8, cudaMemcpyHostToDevice),
                   "upload open velocities");
     return {0, ""};
 }
 
-// setopenvort_d (src/HO_2D.cpp:4109-4129)
+// setopenvort_d (src/HO_2D.cpp:4125-4145)
 Error Solver::set_open_vorticity(const double* w) {
     if (!setup_done_ || in_.problem_type != 11) return {1, "not a set-up hybrid run (problem type 11)"};
     DeviceState& d = *d_;
-    const std::vector<int>* oe = open_edges(mesh_);
+    const std::vector<int>* oe = open_boundary_edges(mesh_);
     const int K = in_.knod;
     h_open_[4] = h_open_[5];
     if (oe)
@@ -177,7 +119,7 @@ Error Solver::set_open_vorticity(const double* w) {
     return {0, ""};
 }
 
-// setptogweights_d (src/HO_2D.cpp:4156-4170)
+// setptogweights_d (src/HO_2D.cpp:4174-4187)
 Error Solver::set_ptog_weights(const double* w) {
     if (!setup_done_ || !d_->hvort[2].get()) return {1, "not a set-up hybrid run (problem type 11)"};
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
@@ -186,20 +128,14 @@ Error Solver::set_ptog_weights(const double* w) {
     return {0, ""};
 }
 
-// getsolnareas_d (src/HO_2D.cpp:3983-3994)
+// getsolnareas_d (src/HO_2D.cpp:3982-3992)
 Error Solver::get_solution_areas(double* out) {
     if (!setup_done_) return {1, "not set up"};
-    const int K = in_.knod;
-    for (int el = 0; el < mesh_.n_el; ++el)
-        for (int j = 0; j < K; ++j)
-            for (int k = 0; k < K; ++k) {
-                const size_t p = ((size_t)el * K + j) * K + k;
-                out[p] = B_.w[j] * B_.w[k] * M_.J[p];
-            }
+    solution_areas(B_, M_, mesh_.n_el, out);
     return {0, ""};
 }
 
-// get_hoquad_weights_d (src/HO_2D.cpp:4252-4260)
+// get_hoquad_weights_d (src/HO_2D.cpp:4252-4259)
 Error Solver::get_hoquad_weights(double* out) {
     if (!setup_done_) return {1, "not set up"};
     const int K = in_.knod;
@@ -208,7 +144,7 @@ Error Solver::get_hoquad_weights(double* out) {
     return {0, ""};
 }
 
-// clean_up (src/HO_2D.cpp:4274-4277): releases the device state; the handle can be set up again
+// clean_up (src/HO_2D.cpp:4275-4278): releases the device state; the handle can be set up again
 void Solver::release() {
     adj_.reset();
     d_.reset(new DeviceState);

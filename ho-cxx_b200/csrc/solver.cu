@@ -973,7 +973,7 @@ Error Solver::set_vorticity(const double* in) {
         if (!std::isfinite(in[i])) return {7, "non-finite value in the vorticity passed in"};
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     if (hybrid_ && d.hvort[1].get()) {
-        // hybrid operation (setsolnvort_d, src/HO_2D.cpp:4132-4152): the vorticity to blend
+        // hybrid operation (setsolnvort_d, src/HO_2D.cpp:4148-4170): the vorticity to blend
         // in at the end of the outer step; the previous one becomes the start value
         HO2D_CUDA(cudaMemcpy(d.hvort[0].get(), d.hvort[1].get(), nv * 8, cudaMemcpyDeviceToDevice), "copy");
         HO2D_CUDA(cudaMemcpy(d.hvort[1].get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");

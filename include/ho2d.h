@@ -175,7 +175,7 @@ int ho2d_get_forces(ho2d_solver* handle, double* fx, double* fy);
  * ho2d_process_mesh_input; then per outer step ho2d_set_open_velocities,
  * ho2d_set_open_vorticity, ho2d_set_vort (the vorticity to blend in; hybrid mode only),
  * ho2d_set_ptog_weights, ho2d_solveto and ho2d_get_vort. Problem type 11. */
-/* Replaces set_defaults (src/HO_2D.cpp:3697-3712): Knod 3, Re^-1 1, RK2, advection type 2,
+/* Replaces set_defaults (src/HO_2D.cpp:3698-3713): Knod 3, Re^-1 1, RK2, advection type 2,
  * problem type 11, dt 1; takes the place of ho2d_read_input. */
 int ho2d_set_defaults(ho2d_solver* handle);
 /* Replaces enable_hybrid (3714-3716): ho2d_set_vort then sets the blend target. */

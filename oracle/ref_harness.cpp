@@ -140,7 +140,8 @@ std::vector<T> read_npy_any(const std::string& path, const char* descr) {
 // integ reyn), nodes.npy, elems.npy, wall.npy, open.npy, inlet.npy / inletvel.npy,
 // outlet.npy / outletvel.npy, ptog.npy, and per outer step s = -1 .. nouter-1 the driver
 // data vort_<s>.npy, openvel_<s>.npy, openvort_<s>.npy (s = -1 fills the "start" values
-// before the first step). Dumps vort_out_<s>.npy after each outer step.
+// before the first step). Dumps vort_out_<s>.npy after each outer step, the setup it starts
+// from (setup_*.npy) and the split of each new open-boundary velocity (open_vel*_end_<s>.npy).
 int run_hybrid(const std::string& spec, const std::string& outdir_in, bool verbose) {
     std::map<std::string, double> kv;
     {
@@ -171,13 +172,57 @@ int run_hybrid(const std::string& spec, const std::string& outdir_in, bool verbo
     s.process_mesh_input();
     const int32_t nv = s.mesh.N_el * s.Knod * s.Knod;
     const int32_t nopen = s.getopenptlen();
+    // the setup the hybrid sequence starts from (setup_*.npy): mesh tables, Jacobians and
+    // the boundary conditions of problem type 11
+    const size_t N = s.mesh.N_el, K = s.Knod, Neb = s.mesh.N_edges_boundary;
+    {
+        std::vector<int32_t> nbr(N * 4), nside(N * 4), be_el(Neb), be_side(Neb), be_group(Neb, -1), swp(Neb), swd(Neb),
+            nsl(s.mesh.N_Gboundary);
+        for (size_t e = 0; e < N; ++e)
+            for (int q = 0; q < 4; ++q) {
+                const auto& en = s.mesh.elem_neighbor[e];
+                nbr[e * 4 + q] = en.is_on_boundary[q] ? -1 : (int32_t)en.neighbor[q];
+                nside[e * 4 + q] = en.is_on_boundary[q] ? -1 : en.neighbor_common_side[q];
+            }
+        for (size_t b = 0; b < Neb; ++b) {
+            be_el[b] = s.mesh.boundary_edges[b].element_index;
+            be_side[b] = s.mesh.boundary_edges[b].side;
+            swp[b] = s.BC_switch_Poisson[b];
+            swd[b] = s.BC_switch_diffusion[b];
+        }
+        for (int g = 0; g < s.mesh.N_Gboundary; ++g) {
+            for (unsigned e : s.mesh.boundaries[g].edges) be_group[e] = g;
+            nsl[g] = s.BC_no_slip[g] ? 1 : 0;
+        }
+        dump_i32(outdir, "setup_elem_neighbor", {N, 4}, nbr);
+        dump_i32(outdir, "setup_elem_neighbor_side", {N, 4}, nside);
+        dump_i32(outdir, "setup_bedge_element", {Neb}, be_el);
+        dump_i32(outdir, "setup_bedge_side", {Neb}, be_side);
+        dump_i32(outdir, "setup_bedge_group", {Neb}, be_group);
+        dump_i32(outdir, "setup_BC_switch_Poisson", {Neb}, swp);
+        dump_i32(outdir, "setup_BC_switch_diffusion", {Neb}, swd);
+        dump_i32(outdir, "setup_BC_no_slip", {(size_t)s.mesh.N_Gboundary}, nsl);
+        dump_f64(outdir, "setup_vol_jac", {N, K, K}, &s.vol_jac[0][0][0]);
+        dump_f64(outdir, "setup_face_Anorm", {N, 4, K}, &s.face_Anorm[0][0][0]);
+        dump_f64(outdir, "setup_BC_Poisson", {Neb, K}, &s.BC_Poisson[0][0]);
+        dump_f64(outdir, "setup_BC_normal_vel", {Neb, K}, &s.BC_normal_vel[0][0]);
+        dump_f64(outdir, "setup_BC_parl_vel", {Neb, K}, &s.BC_parl_vel[0][0]);
+        dump_f64(outdir, "setup_BC_diffusion", {Neb, K}, &s.BC_diffusion[0][0]);
+        dump_f64(outdir, "setup_boundary_source", {Neb, K * K, K}, &s.boundary_source[0][0][0]);
+    }
     if (!ptog.empty()) s.setptogweights_d(nv, ptog.data());
     const int nouter = (int)kv["nouter"];
     for (int st = -1; st < nouter; ++st) {
         const std::string t = std::to_string(st);
         std::vector<double> v = f8("vort_" + t), ov = f8("openvel_" + t), ow = f8("openvort_" + t);
         if (!v.empty()) s.setsolnvort_d(nv, v.data());
-        if (!ov.empty()) s.setopenvels_d(nopen, ov.data());
+        if (!ov.empty()) {
+            s.setopenvels_d(nopen, ov.data());
+            // the normal / parallel split of the new open-boundary velocities (rows: open
+            // edges in open-boundary order)
+            dump_f64(outdir, "open_velnorm_end_" + t, {(size_t)nopen / (2 * K), K}, &s.BC_VelNorm_end[0][0]);
+            dump_f64(outdir, "open_velparl_end_" + t, {(size_t)nopen / (2 * K), K}, &s.BC_VelParl_end[0][0]);
+        }
         if (!ow.empty()) s.setopenvort_d(nopen / 2, ow.data());
         if (st < 0) continue;
         s.solveto_d(kv["outerdt"], (int32_t)kv["numstep"], (int32_t)kv["integ"], kv["reyn"]);

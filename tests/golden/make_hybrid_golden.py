@@ -1,10 +1,12 @@
 """Golden vectors of the reference's hybrid operation (problem type 11).
 
 Writes ``tests/golden/hybrid/<case>/``: the driver's arrays (``spec.txt`` and ``*.npy``, the
-input of ``oracle/_ref/ho2d_ref --hybrid``) and ``hybrid_ref.npz``, the reference's own
+input of ``oracle/_ref/ho2d_ref --hybrid``), ``hybrid_ref.npz``, the reference's own
 results: the vorticity after each outer ``solveto_d`` step, the solution-point areas and
 the open-boundary points, with the shim's direct Poisson solver (HO_SHIM_SOLVER=direct) so
-that psi is the converged discrete solution. Run from the repository root after
+that psi is the converged discrete solution; and ``hybrid_setup_ref.npz``, the reference's
+state after ``process_mesh_input`` (mesh tables, Jacobians, boundary conditions: setup_*)
+and its normal / parallel split of each open-boundary velocity (open_vel*_end_<step>). Run from the repository root after
 ``make -C oracle``:
 
     python tests/golden/make_hybrid_golden.py
@@ -131,7 +133,10 @@ def make(name):
         env = dict(os.environ, HO_SHIM_SOLVER="direct")
         subprocess.run([REF, "--hybrid", d, tmp], check=True, env=env, stdout=subprocess.DEVNULL)
         out = {f[:-4]: np.load(os.path.join(tmp, f)) for f in os.listdir(tmp) if f.endswith(".npy")}
-    np.savez_compressed(os.path.join(d, "hybrid_ref.npz"), **out)
+    setup = {k: v for k, v in out.items() if k.startswith(("setup_", "open_"))}
+    run = {k: v for k, v in out.items() if k not in setup}
+    np.savez_compressed(os.path.join(d, "hybrid_ref.npz"), **run)
+    np.savez_compressed(os.path.join(d, "hybrid_setup_ref.npz"), **setup)
     print(name, {k: v.shape for k, v in out.items()})
 
 

@@ -1,0 +1,163 @@
+// host_harness.cpp -- host build of the library's setup code (ho-cxx_b200/csrc/host_io.cpp,
+// host_setup.cpp, host_hybrid.cpp) for CPU tests against the reference's own setup arrays:
+// a case is set up from an input.dat + Gmsh mesh, or from the arrays a hybrid driver
+// passes, and its tables are read out by name. Never part of the library.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+
+namespace {
+
+struct Case {
+    ho2d::Input in;
+    ho2d::Mesh m;
+    ho2d::Bases B;
+    ho2d::Metrics M;
+    ho2d::BoundaryConditions bc;
+    ho2d::PoissonOperator op;
+    std::vector<double> nrm;  // open-edge normals (problem type 11)
+    std::vector<double> tmp;
+};
+
+// the steps after the mesh, in the order of Solver::setup_from_mesh
+int finish(Case* c) {
+    ho2d::Error e = ho2d::make_bases(c->in.knod, c->m.lnod, c->B);
+    if (e.code) return e.code;
+    ho2d::make_metrics(c->m, c->B, c->M);
+    e = ho2d::setup_bcs(c->in, c->m, c->B, c->bc);
+    if (e.code) return e.code;
+    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, c->op);
+    if (c->in.problem_type == 11) ho2d::open_normals(c->m, c->B, c->M, c->bc, c->nrm);
+    return 0;
+}
+
+void* done(Case* c, int code, int* out) {
+    *out = code;
+    if (code) {
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+template <typename T>
+long copy_out(const std::vector<T>& v, double* out) {
+    if (out)
+        for (size_t i = 0; i < v.size(); ++i) out[i] = (double)v[i];
+    return (long)v.size();
+}
+
+}  // namespace
+
+extern "C" void* case_from_input(const char* path, int* code) {
+    auto* c = new Case;
+    ho2d::Error e = ho2d::read_input(path, c->in);
+    if (!e.code) {
+        std::string mp = c->in.mesh_file;
+        if (!mp.empty() && mp[0] != '/') mp = c->in.base_dir + "/" + mp;
+        e = ho2d::read_msh(mp, c->in.occ, c->m);
+    }
+    return done(c, e.code ? e.code : finish(c), code);
+}
+
+// A hybrid case (problem type 11, Knod knod) from the arrays of load_mesh_arrays_d and
+// load_inout_arrays_d, then process_mesh_input.
+extern "C" void* case_from_arrays(int knod, int iorder, int nxy, const double* xy, int nidx, const int* idx,
+                                  int nwall, const int* wall, int nopen, const int* open, int ninval,
+                                  const double* velin, int nin, const int* idxin, int noutval, const double* velout,
+                                  int nout, const int* idxout, int* code) {
+    auto* c = new Case;
+    c->in.knod = knod;
+    c->in.problem_type = 11;
+    c->in.adv_type = 2;
+    c->in.ti_type = 2;
+    ho2d::Error e = ho2d::mesh_from_arrays(iorder, nxy, xy, nidx, idx, nwall, wall, nopen, open, c->m);
+    if (!e.code) e = ho2d::add_boundary_arrays(c->m, "inlet", nin, idxin, ninval, velin);
+    if (!e.code) e = ho2d::add_boundary_arrays(c->m, "outlet", nout, idxout, noutval, velout);
+    if (!e.code) e = ho2d::process_mesh(c->m);
+    return done(c, e.code ? e.code : finish(c), code);
+}
+
+extern "C" void case_free(void* h) { delete static_cast<Case*>(h); }
+
+// N_el, Knod, Lnod, N_eb, boundary groups, Poisson entries above the 1e-14 filter
+extern "C" void case_dims(void* h, long* d) {
+    const Case* c = static_cast<Case*>(h);
+    d[0] = c->m.n_el;
+    d[1] = c->in.knod;
+    d[2] = c->m.lnod;
+    d[3] = c->m.n_eb;
+    d[4] = (long)c->m.group_names.size();
+    d[5] = (long)c->op.nnz;
+}
+
+extern "C" int case_group_name(void* h, int g, char* buf, int cap) {
+    const Case* c = static_cast<Case*>(h);
+    if (g < 0 || g >= (int)c->m.group_names.size() || cap < 1) return -1;
+    std::strncpy(buf, c->m.group_names[g].c_str(), cap - 1);
+    buf[cap - 1] = 0;
+    return 0;
+}
+
+// Length of the named array (and its values as doubles when out is not null); -1 if unknown.
+extern "C" long case_get(void* h, const char* name, double* out) {
+    Case* c = static_cast<Case*>(h);
+    const std::string n = name;
+    const ho2d::Mesh& m = c->m;
+    const ho2d::Bases& B = c->B;
+    const ho2d::Metrics& M = c->M;
+    const ho2d::BoundaryConditions& bc = c->bc;
+    const ho2d::PoissonOperator& op = c->op;
+    if (n == "nbr") return copy_out(m.nbr, out);
+    if (n == "nbr_side") return copy_out(m.nbr_side, out);
+    if (n == "bidx") return copy_out(m.bidx, out);
+    if (n == "be_el") return copy_out(m.be_el, out);
+    if (n == "be_side") return copy_out(m.be_side, out);
+    if (n == "be_group") return copy_out(m.be_group, out);
+    if (n == "xs") return copy_out(B.xs, out);
+    if (n == "w") return copy_out(B.w, out);
+    if (n == "sbb") return copy_out(B.sbb, out);
+    if (n == "sbgb") return copy_out(B.sbgb, out);
+    if (n == "D") return copy_out(B.D, out);
+    if (n == "R") return copy_out(B.R, out);
+    if (n == "gR") return copy_out(B.gR, out);
+    if (n == "J") return copy_out(M.J, out);
+    if (n == "G") return copy_out(M.G, out);
+    if (n == "GB") return copy_out(M.GB, out);
+    if (n == "fA") return copy_out(M.fA, out);
+    if (n == "fB") return copy_out(M.fB, out);
+    if (n == "fJ") return copy_out(M.fJ, out);
+    if (n == "fAn") return copy_out(M.fAn, out);
+    if (n == "sw_p") return copy_out(bc.sw_p, out);
+    if (n == "sw_d") return copy_out(bc.sw_d, out);
+    if (n == "noslip") return copy_out(bc.noslip, out);
+    if (n == "role") return copy_out(bc.role, out);
+    if (n == "bc_p") return copy_out(bc.bc_p, out);
+    if (n == "bc_nv") return copy_out(bc.bc_nv, out);
+    if (n == "bc_pv") return copy_out(bc.bc_pv, out);
+    if (n == "bc_d") return copy_out(bc.bc_d, out);
+    if (n == "blocks") return copy_out(op.blocks, out);
+    if (n == "block_col") return copy_out(op.block_col, out);
+    if (n == "bsrc") return copy_out(op.bsrc, out);
+    if (n == "dinv") return copy_out(op.dinv, out);
+    if (n == "open_normals") return copy_out(c->nrm, out);
+    if (n == "areas") {
+        c->tmp.assign((size_t)m.n_el * B.K * B.K, 0.0);
+        ho2d::solution_areas(B, M, m.n_el, c->tmp.data());
+        return copy_out(c->tmp, out);
+    }
+    if (n == "openpts") {
+        c->tmp.assign((size_t)ho2d::open_point_count(m, B.K), 0.0);
+        ho2d::open_points(m, B, c->tmp.data());
+        return copy_out(c->tmp, out);
+    }
+    return -1;
+}
+
+// split_open_velocities of the driver's open-boundary velocities into vn, vp [N_eb][K]
+extern "C" void case_split_open(void* h, const double* xyvel, double* vn, double* vp) {
+    const Case* c = static_cast<Case*>(h);
+    ho2d::split_open_velocities(c->m, c->in.knod, c->nrm, xyvel, vn, vp);
+}

@@ -1,0 +1,305 @@
+"""The library's host setup against the reference's own setup arrays, on the CPU.
+
+tests/host_harness.cpp compiles the library's host code (ho-cxx_b200/csrc/host_io.cpp,
+host_setup.cpp, host_hybrid.cpp) with g++ and sets up
+  * each golden case from its input.dat and Gmsh mesh: the mesh tables, bases, metrics,
+    boundary conditions and the Poisson operator's blocks are compared with the arrays the
+    reference dumped after its setup (ref.npz: setup_mesh .. form_Laplace_operator_matrix);
+  * each hybrid case from the driver's arrays (load_mesh_arrays_d, load_inout_arrays_d,
+    process_mesh_input): mesh tables, Jacobians, the boundary conditions of problem type 11
+    (wall / open / inlet / outlet switches and the inlet streamfunction chain), the
+    boundary source, solution-point areas, open-boundary points and the normal / parallel
+    split of the driver's open-boundary velocities against the reference's
+    (hybrid_setup_ref.npz, hybrid_ref.npz).
+Integer tables must be equal; FP64 values agree to round-off (1e-11 of the array's scale,
+1e-13 for the bases).
+"""
+
+import ctypes
+import json
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import GOLDEN, GOLDEN_CASES, REPO
+
+CSRC = os.path.join(REPO, "ho-cxx_b200", "csrc")
+HYB = os.path.join(GOLDEN, "hybrid")
+HYB_CASES = sorted(d for d in os.listdir(HYB) if os.path.isfile(os.path.join(HYB, d, "hybrid_setup_ref.npz")))
+TOL = 1e-11
+
+
+@pytest.fixture(scope="module")
+def lib(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    out = str(tmp_path_factory.mktemp("host_harness") / "libhost_harness.so")
+    srcs = [os.path.join(REPO, "tests", "host_harness.cpp")] + [os.path.join(CSRC, f) for f in
+                                                                 ("host_io.cpp", "host_setup.cpp", "host_hybrid.cpp")]
+    subprocess.run(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-I", CSRC, *srcs, "-o", out], check=True,
+                   capture_output=True, text=True)
+    L = ctypes.CDLL(out)
+    L.case_from_input.restype = ctypes.c_void_p
+    L.case_from_input.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    L.case_from_arrays.restype = ctypes.c_void_p
+    L.case_free.argtypes = [ctypes.c_void_p]
+    L.case_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+    L.case_group_name.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    L.case_get.restype = ctypes.c_long
+    L.case_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+    L.case_split_open.argtypes = [ctypes.c_void_p] * 4
+    return L
+
+
+class HostCase:
+    def __init__(self, lib, handle):
+        self.lib, self.h = lib, handle
+        d = (ctypes.c_long * 6)()
+        lib.case_dims(handle, d)
+        self.N, self.K, self.L, self.neb, self.ngroups, self.nnz = list(d)
+        buf = ctypes.create_string_buffer(256)
+        self.groups = []
+        for g in range(self.ngroups):
+            assert lib.case_group_name(handle, g, buf, 256) == 0
+            self.groups.append(buf.value.decode())
+
+    def __getitem__(self, name):
+        n = self.lib.case_get(self.h, name.encode(), None)
+        assert n >= 0, name
+        out = np.zeros(n)
+        self.lib.case_get(self.h, name.encode(), out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def ints(self, name):
+        return self[name].astype(np.int64)
+
+    def close(self):
+        self.lib.case_free(self.h)
+
+
+def rel(a, b):
+    return float(np.abs(np.ravel(a) - np.ravel(b)).max() / max(np.abs(b).max(), 1e-300))
+
+
+def close_abs(mine, ref, tol=TOL):
+    """|mine - ref| <= tol * max(1, |ref|) elementwise scale of the whole array."""
+    ref = np.asarray(ref, dtype=float)
+    return float(np.abs(np.ravel(mine) - ref.ravel()).max(initial=0.0)) <= tol * max(1.0, np.abs(ref).max(initial=0.0))
+
+
+def blocks_to_csr(c: HostCase):
+    """The assembled operator from the block form: block (el, slot)[rs][ij] is
+    A[el K^2 + ij, col K^2 + rs]; entries at or below 1e-14 in magnitude dropped as the
+    reference's assembly does."""
+    K2 = c.K * c.K
+    blocks = c["blocks"].reshape(c.N, 5, K2, K2)
+    col = c.ints("block_col").reshape(c.N, 5)
+    rows, cols, vals = [], [], []
+    ij = np.arange(K2)
+    for el in range(c.N):
+        for s in range(5):
+            if col[el, s] < 0:
+                continue
+            b = blocks[el, s]  # [rs][ij]
+            r = el * K2 + ij[None, :] + 0 * ij[:, None]
+            cc = col[el, s] * K2 + ij[:, None] + 0 * ij[None, :]
+            keep = np.abs(b) > 1e-14
+            rows.append(r[keep])
+            cols.append(cc[keep])
+            vals.append(b[keep])
+    n = c.N * K2
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+
+
+@pytest.fixture(scope="module", params=GOLDEN_CASES)
+def golden(request, lib):
+    d = os.path.join(GOLDEN, request.param)
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(os.path.join(d, "input.dat").encode(), ctypes.byref(code))
+    assert h, f"setup failed with code {code.value}"
+    c = HostCase(lib, h)
+    yield c, dict(np.load(os.path.join(d, "ref.npz"))), json.load(open(os.path.join(d, "meta.json")))
+    c.close()
+
+
+def test_mesh_tables(golden):
+    c, ref, meta = golden
+    assert (c.N, c.K, c.neb) == (meta["N_el"], meta["Knod"], meta["N_edges_boundary"])
+    assert c.groups == meta["boundaries"]
+    # elem_neighbor etc. are [el][side] with -1 where the side is on the boundary
+    np.testing.assert_array_equal(c.ints("nbr"), ref["elem_neighbor"].ravel())
+    np.testing.assert_array_equal(c.ints("nbr_side"), ref["elem_neighbor_side"].ravel())
+    np.testing.assert_array_equal(c.ints("bidx"), ref["elem_boundary_index"].ravel())
+    np.testing.assert_array_equal(c.ints("be_el"), ref["bedge_element"])
+    np.testing.assert_array_equal(c.ints("be_side"), ref["bedge_side"])
+
+
+def test_bases(golden):
+    c, ref, _ = golden
+    for mine, nm in [("xs", "sps_local_coor"), ("w", "sps_weight"), ("D", "sps_sps_grad_basis"),
+                     ("R", "sps_radau"), ("gR", "sps_grad_radau"), ("sbb", "sps_boundary_basis"),
+                     ("sbgb", "sps_boundary_grad_basis")]:
+        assert rel(c[mine], ref[nm]) < 1e-13, nm
+
+
+def test_metrics(golden):
+    c, ref, _ = golden
+    for mine, nm in [("J", "vol_jac"), ("G", "G"), ("GB", "GB"), ("fJ", "face_jac"), ("fA", "face_Acoef"),
+                     ("fAn", "face_Anorm")]:
+        assert rel(c[mine], ref[nm]) < TOL, nm
+    # face_Bcoef vanishes on affine meshes: compare absolutely against the face scale
+    assert np.abs(c["fB"] - ref["face_Bcoef"].ravel()).max() <= TOL * np.abs(ref["face_Acoef"]).max()
+
+
+def test_boundary_conditions(golden):
+    c, ref, _ = golden
+    np.testing.assert_array_equal(c.ints("sw_p"), ref["BC_switch_Poisson"])
+    np.testing.assert_array_equal(c.ints("sw_d"), ref["BC_switch_diffusion"])
+    for mine, nm in [("bc_p", "BC_Poisson"), ("bc_nv", "BC_normal_vel"), ("bc_pv", "BC_parl_vel"),
+                     ("bc_d", "BC_diffusion")]:
+        assert close_abs(c[mine], ref[nm]), nm
+
+
+def test_poisson_operator(golden):
+    c, ref, _ = golden
+    n = c.N * c.K ** 2
+    A = sp.csr_matrix((ref["A_val"], ref["A_col"], ref["A_ptr"][: n + 1]), shape=(n, n))
+    mine = blocks_to_csr(c)
+    assert c.nnz == A.nnz == mine.nnz
+    assert abs(mine - A).max() <= 1e-13 * abs(A).max()
+    assert rel(c["bsrc"], ref["boundary_source"]) < 1e-13
+
+
+def test_block_jacobi_inverse(golden):
+    """The inverse diagonal blocks of the block-Jacobi smoother."""
+    c, _, _ = golden
+    K2 = c.K * c.K
+    blocks = c["blocks"].reshape(c.N, 5, K2, K2)
+    col = c.ints("block_col").reshape(c.N, 5)
+    dinv = c["dinv"].reshape(c.N, K2, K2)
+    for el in range(c.N):
+        assert col[el, 0] == el
+        Dm = blocks[el, 0].T  # [ij][rs]
+        assert np.abs(dinv[el].T @ Dm - np.eye(K2)).max() <= 1e-12 * np.linalg.cond(Dm)
+
+
+def _hybrid_arrays(name):
+    d = os.path.join(HYB, name)
+    spec = {}
+    for line in open(os.path.join(d, "spec.txt")):
+        k, v = line.split()
+        spec[k] = float(v)
+    arrays = {f[:-4]: np.load(os.path.join(d, f)) for f in os.listdir(d) if f.endswith(".npy")}
+    return (spec, arrays, dict(np.load(os.path.join(d, "hybrid_setup_ref.npz"))),
+            dict(np.load(os.path.join(d, "hybrid_ref.npz"))))
+
+
+def _hybrid_case(lib, spec, a):
+    i32, f64 = np.int32, np.float64
+
+    def arr(key, dt):
+        v = np.ascontiguousarray(a.get(key, np.zeros(0, dt)), dtype=dt)
+        return len(v), v
+
+    keep = []
+
+    def ptr(v):
+        keep.append(v)
+        return v.ctypes.data_as(ctypes.c_void_p)
+
+    nxy, xy = arr("nodes", f64)
+    nidx, el = arr("elems", i32)
+    nw, wall = arr("wall", i32)
+    no, opn = arr("open", i32)
+    niv, inv = arr("inletvel", f64)
+    ni, inl = arr("inlet", i32)
+    nov, outv = arr("outletvel", f64)
+    nout, outl = arr("outlet", i32)
+    code = ctypes.c_int(0)
+    ci = ctypes.c_int
+    h = lib.case_from_arrays(ci(int(spec["knod"])), ci(int(spec["iorder"])), ci(nxy), ptr(xy), ci(nidx), ptr(el),
+                             ci(nw), ptr(wall), ci(no), ptr(opn), ci(niv), ptr(inv), ci(ni), ptr(inl), ci(nov),
+                             ptr(outv), ci(nout), ptr(outl), ctypes.byref(code))
+    assert h, f"hybrid setup failed with code {code.value}"
+    return HostCase(lib, h)
+
+
+@pytest.fixture(scope="module", params=HYB_CASES)
+def hybrid(request, lib):
+    spec, a, sref, rref = _hybrid_arrays(request.param)
+    c = _hybrid_case(lib, spec, a)
+    yield c, a, sref, rref
+    c.close()
+
+
+def test_hybrid_mesh_tables(hybrid):
+    c, _, s, _ = hybrid
+    np.testing.assert_array_equal(c.ints("nbr"), s["setup_elem_neighbor"].ravel())
+    np.testing.assert_array_equal(c.ints("nbr_side"), s["setup_elem_neighbor_side"].ravel())
+    np.testing.assert_array_equal(c.ints("be_el"), s["setup_bedge_element"])
+    np.testing.assert_array_equal(c.ints("be_side"), s["setup_bedge_side"])
+    np.testing.assert_array_equal(c.ints("be_group"), s["setup_bedge_group"])
+    assert rel(c["J"], s["setup_vol_jac"]) < TOL
+    assert rel(c["fAn"], s["setup_face_Anorm"]) < TOL
+
+
+def test_hybrid_boundary_conditions(hybrid):
+    c, _, s, _ = hybrid
+    np.testing.assert_array_equal(c.ints("sw_p"), s["setup_BC_switch_Poisson"])
+    np.testing.assert_array_equal(c.ints("sw_d"), s["setup_BC_switch_diffusion"])
+    np.testing.assert_array_equal(c.ints("noslip"), s["setup_BC_no_slip"])
+    for mine, nm in [("bc_p", "setup_BC_Poisson"), ("bc_nv", "setup_BC_normal_vel"),
+                     ("bc_pv", "setup_BC_parl_vel"), ("bc_d", "setup_BC_diffusion")]:
+        assert close_abs(c[mine], s[nm]), nm
+    assert rel(c["bsrc"], s["setup_boundary_source"]) < 1e-13 if np.abs(s["setup_boundary_source"]).max() > 0 \
+        else np.abs(c["bsrc"]).max() == 0
+
+
+def test_hybrid_inlet_chain_carries_the_inflow(hybrid):
+    """Independent of the reference: with inlets, the streamfunction on the walls differs
+    by the flow that enters between them (psi changes by -len * v_n along an inlet)."""
+    c, a, _, _ = hybrid
+    if "inlet" not in a:
+        pytest.skip("no inlets")
+    K = c.K
+    bc_p = c["bc_p"].reshape(c.neb, K)
+    grp = c.ints("be_group")
+    walls = bc_p[grp == c.groups.index("wall")]
+    levels = np.unique(np.round(walls[:, 0], 12))
+    nodes = a["nodes"].reshape(-1, 2)
+    inl = a["inlet"].reshape(-1, 2)
+    inflow = float(np.sum(-a["inletvel"] * np.linalg.norm(nodes[inl[:, 1]] - nodes[inl[:, 0]], axis=1)))
+    assert len(levels) == 2
+    assert abs(abs(levels[1] - levels[0]) - abs(inflow)) < 1e-12
+
+
+def test_hybrid_areas_and_open_points(hybrid):
+    c, _, _, r = hybrid
+    assert rel(c["areas"], r["areas"]) < 1e-13
+    if "openpts" in r:
+        assert rel(c["openpts"], r["openpts"]) < 1e-13
+    else:
+        assert len(c["openpts"]) == 0
+
+
+def test_hybrid_open_velocity_split(hybrid):
+    c, a, s, _ = hybrid
+    steps = sorted(int(k.rsplit("_", 1)[1]) for k in s if k.startswith("open_velnorm_end_"))
+    if not steps:
+        pytest.skip("no open boundary")
+    K = c.K
+    open_rows = np.flatnonzero(c.ints("be_group") == c.groups.index("open"))
+    nrm = c["open_normals"].reshape(c.neb, K, 2)
+    np.testing.assert_allclose(np.linalg.norm(nrm[open_rows], axis=-1), 1.0, rtol=1e-13)
+    for st in steps:
+        xyvel = np.ascontiguousarray(a[f"openvel_{st}"], dtype=np.float64)
+        vn, vp = np.zeros(c.neb * K), np.zeros(c.neb * K)
+        c.lib.case_split_open(c.h, xyvel.ctypes.data_as(ctypes.c_void_p), vn.ctypes.data_as(ctypes.c_void_p),
+                              vp.ctypes.data_as(ctypes.c_void_p))
+        vn, vp = vn.reshape(c.neb, K)[open_rows], vp.reshape(c.neb, K)[open_rows]
+        assert close_abs(vn, s[f"open_velnorm_end_{st}"], 1e-13), st
+        assert close_abs(vp, s[f"open_velparl_end_{st}"], 1e-13), st

@@ -31,7 +31,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_reduce_over_gloo():
     world = 2
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     for r in range(world):
         assert out[r] == (2.5, 30.0)  # max over ranks of 1.5 + rank; sum of 10, 20
