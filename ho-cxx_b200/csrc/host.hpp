@@ -140,10 +140,23 @@ struct VtkFields {
     const double *w, *psi, *u, *v, *rhs_diff, *rhs_adv;
     const double *bc_w, *bc_nv, *bc_pv;
 };
+// Points of the input's sample-points file (read_process_sample_points, host_samples.cpp):
+// coordinates [n][2], the element that holds each point, and the Lnod^2 geometry shape
+// functions (Gmsh node slots) at its local coordinates [n][Lnod^2].
+struct SamplePoints {
+    std::vector<double> xy;
+    std::vector<int> elem;
+    std::vector<double> shape;
+    size_t size() const { return elem.size(); }
+};
+// A missing file gives no points (no error), as in the reference.
+Error read_sample_points(const std::string& path, const Mesh& m, SamplePoints& sp);
+
 // save_vorticity_vtk + save_smooth_vtk (src/HO_2D.cpp:3369-3692) into dir ("" = working
-// directory); subidx < 0 leaves it out of the file names
+// directory); subidx < 0 leaves it out of the file names. With sample points (may be null)
+// also sampling_points<p>_K<K>_L<Lnod>_<indx>.dat.
 Error write_vtk_files(const Mesh& mesh, const Bases& B, int problem_type, const VtkFields& f, int indx, int subidx,
-                      const std::string& dir);
+                      const std::string& dir, const SamplePoints* samples = nullptr);
 int tensor2fem_1d(int i, int lnod_in);
 
 // Hybrid operation (host_hybrid.cpp): the edges of the "open" boundary (null if none), the

@@ -58,6 +58,7 @@ Error Solver::process_mesh_input() {
     if (!input_done_) return {1, "call ho2d_set_defaults (or ho2d_read_input) first"};
     if (mesh_.elem_nodes.empty()) return {1, "load the mesh arrays first"};
     HO2D_TRY(process_mesh(mesh_));
+    samples_ = SamplePoints();  // the reference reads no sample points here
     return setup_from_mesh();
 }
 

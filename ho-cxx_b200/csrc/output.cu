@@ -47,7 +47,7 @@ Error Solver::write_vtk(int indx, int subidx, const std::string& dir) {
     HO2D_CUDA(fetch<double>(bnv, d.bc_nv, nb), "copy");
     HO2D_CUDA(fetch<double>(bpv, d.bc_pv, nb), "copy");
     VtkFields fl{w.data(), psi.data(), u.data(), v.data(), rd.data(), ra.data(), bw.data(), bnv.data(), bpv.data()};
-    return write_vtk_files(mesh_, B_, in_.problem_type, fl, indx, subidx, dir);
+    return write_vtk_files(mesh_, B_, in_.problem_type, fl, indx, subidx, dir, &samples_);
 }
 
 }  // namespace ho2d

@@ -4,8 +4,9 @@
 // and number format (%g, the default of the reference's iostreams), the reference's node
 // numbering (the mesh reader's first-use order, src/Mesh.cpp:296-333), and the same
 // boundary treatment in the smooth file: boundary nodes take BC_vorticity and the Cartesian
-// velocity rebuilt from BC_normal_vel (local h direction) and BC_parl_vel. Sample-point
-// files are not written (the reference seeds its sample search from the clock).
+// velocity rebuilt from BC_normal_vel (local h direction) and BC_parl_vel. With sample
+// points, also the sample-point file of save_smooth_vtk (src/HO_2D.cpp:3592-3614): x, y and
+// the node-averaged vorticity and velocity interpolated with the geometry shape functions.
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -28,7 +29,7 @@ struct File {
 }  // namespace
 
 Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, const VtkFields& fl, int indx, int subidx,
-                      const std::string& dir) {
+                      const std::string& dir, const SamplePoints* samples) {
     const int N = mesh_.n_el, K = B_.K, K2 = K * K, L = mesh_.lnod, lin = L - 1, L2 = L * L;
     const size_t nv = (size_t)N * K2, nb = (size_t)mesh_.n_eb * K;
     const double *w = fl.w, *psi = fl.psi, *u = fl.u, *v = fl.v, *rd = fl.rhs_diff, *ra = fl.rhs_adv;
@@ -205,6 +206,23 @@ Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, cons
     for (size_t n = 0; n < nn; ++n) std::fprintf(f, "%g\n", np[n]);
     std::fprintf(f, "VECTORS velocity double \n");
     for (size_t n = 0; n < nn; ++n) std::fprintf(f, "%g %g 0.0\n", nux[n], nuy[n]);
+    if (!samples || samples->size() == 0) return {0, ""};
+    char sname[96];
+    std::snprintf(sname, sizeof(sname), "sampling_points%d_K%d_L%d_%05d.dat", problem_type, K, L, indx);
+    File sh(pre + sname);
+    if (!sh.f) return {2, "cannot write " + pre + sname};
+    for (size_t s = 0; s < samples->size(); ++s) {
+        const int el = samples->elem[s];
+        const double* sf = &samples->shape[s * L2];
+        double om_s = 0.0, ux = 0.0, uy = 0.0;
+        for (int l = 0; l < L2; ++l) {
+            const int nd = mesh_.elem_nodes[el][l];
+            om_s += sf[l] * nw[nd];
+            ux += sf[l] * nux[nd];
+            uy += sf[l] * nuy[nd];
+        }
+        std::fprintf(sh.f, "%g %g %g %g %g\n", samples->xy[2 * s], samples->xy[2 * s + 1], om_s, ux, uy);
+    }
     return {0, ""};
 }
 

@@ -73,6 +73,11 @@ Error Solver::setup() {
     if (!mesh_path.empty() && mesh_path[0] != '/') mesh_path = in_.base_dir + "/" + mesh_path;
     mesh_ = Mesh();
     HO2D_TRY(read_msh(mesh_path, in_.occ, mesh_));
+    // read_process_sample_points (src/main.cpp:65): the file name is taken relative to the
+    // input's directory, like the mesh file
+    std::string sample_path = in_.sample_file;
+    if (!sample_path.empty() && sample_path[0] != '/') sample_path = in_.base_dir + "/" + sample_path;
+    HO2D_TRY(read_sample_points(sample_path, mesh_, samples_));
     return setup_from_mesh();
 }
 

@@ -171,6 +171,7 @@ class Solver {
     double t_start_ = 0.0, t_end_ = 0.0;
     bool hybrid_ = false;                     // enable_hybrid: set_vort feeds the blend target
     std::string output_dir_;                  // where solve() writes its VTK files (empty: none)
+    SamplePoints samples_;                    // the input's sample points (VTK output)
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

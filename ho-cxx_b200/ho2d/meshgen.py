@@ -11,7 +11,9 @@ accepts (src/Mesh.cpp:93-340):
   tag), src/Mesh.cpp:141-152;
 * ``$Nodes``: one block, tags 1..N;
 * ``$Elements``: 2-node lines (type 1) per boundary curve and 4-node quads (type 3)
-  listed counter-clockwise, so the reader needs no OCC reorientation (flag 0).
+  listed counter-clockwise, so the reader needs no OCC reorientation (flag 0); or, for
+  quadratic geometry (input.dat Lnod 2), 3-node lines (type 8: ends, then midpoint) and
+  9-node quads (type 10: corners, edge midpoints, centre).
 
 Physical names follow the problem types of src/HO_2D.cpp:675-1238: cavity
 (``bottom_wall, right_wall, top, left_wall``), backward-facing step
@@ -32,8 +34,8 @@ import numpy as np
 @dataclass
 class QuadMesh:
     xy: np.ndarray  # [n_nodes, 2]
-    quads: np.ndarray  # [n_el, 4] node indices, counter-clockwise
-    boundaries: dict = field(default_factory=dict)  # name -> [n_edges, 2] node indices
+    quads: np.ndarray  # [n_el, 4] node indices, counter-clockwise (or [n_el, 9], Gmsh order)
+    boundaries: dict = field(default_factory=dict)  # name -> [n_edges, 2] node indices (or [n_edges, 3])
 
     @property
     def n_el(self) -> int:
@@ -186,16 +188,17 @@ def write_msh(mesh: QuadMesh, path: str) -> None:
     n_edges = sum(len(v) for v in mesh.boundaries.values())
     n_elem = n_edges + mesh.n_el
     lines += ["$EndNodes", "$Elements", f"{len(names) + 1} {n_elem} 1 {n_elem}"]
+    quadratic = mesh.quads.shape[1] == 9
     tag = 1
     for g, nm in enumerate(names):
         e = mesh.boundaries[nm]
-        lines.append(f"1 {g + 1} 1 {len(e)}")
-        for a, b in e:
-            lines.append(f"{tag} {a + 1} {b + 1}")
+        lines.append(f"1 {g + 1} {8 if quadratic else 1} {len(e)}")
+        for ed in e:
+            lines.append(f"{tag} " + " ".join(str(int(a) + 1) for a in ed))
             tag += 1
-    lines.append(f"2 1 3 {mesh.n_el}")
+    lines.append(f"2 1 {10 if quadratic else 3} {mesh.n_el}")
     for q in mesh.quads:
-        lines.append(f"{tag} {q[0] + 1} {q[1] + 1} {q[2] + 1} {q[3] + 1}")
+        lines.append(f"{tag} " + " ".join(str(int(a) + 1) for a in q))
         tag += 1
     lines.append("$EndElements")
     with open(path, "w") as f:
@@ -205,14 +208,15 @@ def write_msh(mesh: QuadMesh, path: str) -> None:
 def write_input_dat(path: str, mesh_file: str, knod: int, reyn: float, dt: float, num_steps: int,
                     problem_type: int, time_integration: int = 4, advection_type: int = 1,
                     dump_frequency: int | None = None, occ: int = 0, lhs_type: int = 3,
-                    sample_points: str = "none") -> None:
-    """Write the 17-field positional ``input.dat`` (src/HO_2D.cpp:213-317)."""
+                    sample_points: str = "none", lnod_in: int = 1) -> None:
+    """Write the 17-field positional ``input.dat`` (src/HO_2D.cpp:213-317); ``lnod_in`` is
+    the geometry order (1 bilinear, 2 quadratic)."""
     if dump_frequency is None:
         dump_frequency = max(num_steps, 1)
     fields = [
         ("Nel_i , Nel_j:", "1, 1"),
         ("Knod quantity:", str(knod)),
-        ("Lnod:", "1"),
+        ("Lnod:", str(lnod_in)),
         ("mesh file name:", mesh_file),
         ("if the file is written in OCC format or original gmsh format. zero means original, 1 means OCC format",
          str(occ)),

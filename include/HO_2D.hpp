@@ -37,7 +37,7 @@ class HO_2D {
     char setup_mesh() { return ensure_setup(); }
     char allocate_arrays() { return ensure_setup(); }
     void setup_sps_gps() { ensure_setup(); }
-    void read_process_sample_points() {}
+    void read_process_sample_points() {}  // the setup reads the input's sample points
     void form_bases() { ensure_setup(); }
     void form_metrics() { ensure_setup(); }
     void setup_IC_BC_SRC() { ensure_setup(); }

@@ -80,8 +80,11 @@ int ho2d_set_output_dir(ho2d_solver* handle, const char* dir);
 /* Replaces save_vorticity_vtk and save_smooth_vtk (src/HO_2D.cpp:3369-3692), and
  * trigger_write (4262-4271): writes vorticity<p>_K<K>[_<subidx>]_<indx>.vtk (solution
  * points) and problem<p>_K<K>[_<subidx>]_<indx>.vtk (node averages) of the current fields
- * into dir (NULL: the working directory); subidx < 0 leaves it out of the names. The
- * reference's sample-point file is not written. */
+ * into dir (NULL: the working directory); subidx < 0 leaves it out of the names. When the
+ * input names a sample-points file (read_process_sample_points, src/HO_2D.cpp:319-474,
+ * read at ho2d_setup relative to the input's directory), also
+ * sampling_points<p>_K<K>_L<Lnod>_<indx>.dat: x, y, vorticity, u, v per point
+ * (src/HO_2D.cpp:3592-3614). */
 int ho2d_write_vtk(ho2d_solver* handle, int32_t indx, int32_t subidx, const char* dir);
 /* Replaces nsteps calls of HO_2D::solve_advection_diffusion (src/HO_2D.cpp:1465-1531),
  * advancing the solver time by dt after each. */

@@ -9,8 +9,8 @@
 // allocate_arrays, setup_sps_gps, form_bases, form_metrics, setup_IC_BC_SRC,
 // form_Laplace_operator_matrix); the time loop mirrors
 // src/HO_2D.cpp:1407-1447 without the VTK writers (dump_frequency output only).
-// read_process_sample_points (src/HO_2D.cpp:319) is skipped: it is output-only and
-// seeds its ray casting from time(0).
+// read_process_sample_points (src/HO_2D.cpp:319) runs only with --samples: it is
+// output-only and seeds its ray casting from time(0).
 //
 // usage: ho2d_ref INPUT.dat OUTDIR [options]
 //   --setup                dump mesh tables, bases, metrics, BCs, Poisson matrix
@@ -29,6 +29,10 @@
 //   --solve                run solve_vorticity_streamfunction (writes the reference's VTK
 //                          files into the input's directory), dump the fields the last
 //                          files were written from (solve_*.npy) and stop
+//   --samples              run read_process_sample_points after setup_sps_gps, as
+//                          src/main.cpp:65 does (the sample file named in the input,
+//                          opened from the input's directory); --solve then also writes
+//                          the reference's sampling_points*.dat files
 //   --verbose              keep the reference's stdout
 // or:   ho2d_ref --hybrid SPECDIR OUTDIR [--verbose]   (see run_hybrid)
 #include "HO_2D.hpp"
@@ -251,7 +255,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     std::string input = argv[1], outdir = argv[2];
-    bool do_setup = false, verbose = false, do_stage = false, do_solve = false;
+    bool do_setup = false, verbose = false, do_stage = false, do_solve = false, do_samples = false;
     double stage_coeff = 0.0, dt_override = -1.0, t0 = 0.0;
     long nsteps = 0, every = 0, ntime = 0, nstages = 0;
     std::string init_vort, lid;
@@ -269,6 +273,7 @@ int main(int argc, char** argv) {
         else if (a == "--time-stages" && i + 1 < argc) nstages = std::atol(argv[++i]);
         else if (a == "--t0" && i + 1 < argc) t0 = std::atof(argv[++i]);
         else if (a == "--solve") do_solve = true;
+        else if (a == "--samples") do_samples = true;
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     mkdir(outdir.c_str(), 0755);
@@ -292,6 +297,7 @@ int main(int argc, char** argv) {
     if (ho.setup_mesh() != 0) { std::cout.rdbuf(saved); std::fprintf(stderr, "setup_mesh failed\n"); return 4; }
     if (ho.allocate_arrays() != 0) { std::cout.rdbuf(saved); std::fprintf(stderr, "allocate_arrays failed\n"); return 4; }
     ho.setup_sps_gps();
+    if (do_samples) ho.read_process_sample_points();
     ho.form_bases();
     ho.form_metrics();
     ho.setup_IC_BC_SRC();

@@ -1,4 +1,4 @@
-"""VTK output against the reference's own files.
+"""VTK and sample-point output against the reference's own files.
 
 CPU: the library's writer (host build, tests/vtk_harness.cpp) fed the fields the reference
 wrote its last files from must write the same files (on the cavity cases byte for byte;
@@ -64,10 +64,13 @@ def vtk_harness(tmp_path_factory):
     csrc = os.path.join(REPO, "ho-cxx_b200", "csrc")
     out = str(tmp_path_factory.mktemp("vtk_harness") / "libvtk_harness.so")
     srcs = [os.path.join(REPO, "tests", "vtk_harness.cpp")] + [os.path.join(csrc, f) for f in
-                                                                ("output_host.cpp", "host_io.cpp", "host_setup.cpp")]
+                                                                ("output_host.cpp", "host_io.cpp", "host_setup.cpp",
+                                                                 "host_samples.cpp")]
     subprocess.run(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-I", csrc, "-I", os.path.join(REPO, "include"),
                     *srcs, "-o", out], check=True, capture_output=True, text=True)
-    return ctypes.CDLL(out)
+    lib = ctypes.CDLL(out)
+    lib.sample_points_host.restype = ctypes.c_long
+    return lib
 
 
 @pytest.mark.parametrize("case", ["cav4_rk4", "cav4_euler_k3", "bfs2_rk4", "cyl4x8_rk4"])
@@ -90,12 +93,109 @@ def test_vtk_writer_reproduces_reference_files(tmp_path, vtk_harness, case):
     rc = vtk_harness.write_vtk_host(str(d / "mesh.msh").encode(), 0, knod, ptype, _dp(f["vorticity"]),
                                     _dp(f["psi"]), _dp(f["vel"][..., 0]), _dp(f["vel"][..., 1]), _dp(f["rhs_diff"]),
                                     _dp(f["rhs_adv"]), _dp(f["bc_w"]), _dp(f["bc_nv"]), _dp(f["bc_pv"]), nsteps, -1,
-                                    str(ours).encode())
+                                    str(ours).encode(), b"")
     assert rc == 0
     files = sorted(os.listdir(ours))
     assert files == [f"problem{ptype}_K{knod}_{nsteps:05d}.vtk", f"vorticity{ptype}_K{knod}_{nsteps:05d}.vtk"]
     for fn in files:  # identical except for round-off around zero (summation order)
         compare_vtk(str(ours / fn), str(d / fn))
+
+
+def q2_cavity(n=3, amp=0.04):
+    """Unit-square cavity of n x n 9-node quads whose interior is bent by
+    (x, y) += amp sin(pi x) sin(2 pi y) (1, 0.5): curved interior edges, straight walls."""
+    from ho2d import meshgen
+
+    m = 2 * n + 1
+    g = np.linspace(0.0, 1.0, m)
+    X, Y = np.meshgrid(g, g)  # [j][i]
+    b = amp * np.sin(np.pi * X) * np.sin(2 * np.pi * Y)
+    xy = np.stack([(X + b).ravel(), (Y + 0.5 * b).ravel()], -1)
+    nid = lambda i, j: j * m + i  # noqa: E731
+    quads = []
+    for j in range(n):
+        for i in range(n):
+            a, c = 2 * i, 2 * j
+            quads.append([nid(a, c), nid(a + 2, c), nid(a + 2, c + 2), nid(a, c + 2), nid(a + 1, c), nid(a + 2, c + 1),
+                          nid(a + 1, c + 2), nid(a, c + 1), nid(a + 1, c + 1)])
+    bnd = {"bottom_wall": [[nid(2 * i, 0), nid(2 * i + 2, 0), nid(2 * i + 1, 0)] for i in range(n)],
+           "right_wall": [[nid(m - 1, 2 * j), nid(m - 1, 2 * j + 2), nid(m - 1, 2 * j + 1)] for j in range(n)],
+           "top": [[nid(2 * i + 2, m - 1), nid(2 * i, m - 1), nid(2 * i + 1, m - 1)] for i in range(n)],
+           "left_wall": [[nid(0, 2 * j + 2), nid(0, 2 * j), nid(0, 2 * j + 1)] for j in range(n)]}
+    return meshgen.QuadMesh(xy, np.array(quads), {k: np.array(v) for k, v in bnd.items()})
+
+
+def msh_nodes(path):
+    """Node coordinates of a Gmsh 4.1 file written by meshgen or the golden generator."""
+    lines = open(path).read().split("\n")
+    i = lines.index("$Nodes")
+    nb, n = int(lines[i + 1].split()[0]), int(lines[i + 1].split()[1])
+    k, xy = i + 2, []
+    for _ in range(nb):
+        cnt = int(lines[k].split()[3])
+        xy += [[float(t) for t in lines[k + 1 + cnt + a].split()[:2]] for a in range(cnt)]
+        k += 1 + 2 * cnt
+    assert len(xy) == n
+    return np.array(xy)
+
+
+@pytest.mark.parametrize("case", ["cav4_rk4", "bfs2_rk4", "cyl4x8_rk4", "q2_cavity"])
+def test_sample_point_file_matches_reference(tmp_path, vtk_harness, case):
+    """read_process_sample_points + the sample-point file of save_smooth_vtk: 40 seeded
+    points in the mesh's bounding box, some outside the domain (the BFS step, the cylinder,
+    the box corners), so that both the polygon search and the nearest-node fallback run.
+    The reference (--solve --samples) and the library's writer, given the fields the
+    reference wrote from, must write the same file (values to the printed six digits), and
+    every point's shape functions must sum to one."""
+    if not os.path.exists(REF):
+        pytest.skip("oracle/_ref/ho2d_ref not built")
+    from ho2d import meshgen
+
+    d = tmp_path / "case"
+    if case == "q2_cavity":
+        d.mkdir()
+        meshgen.write_msh(q2_cavity(), str(d / "mesh.msh"))
+        meshgen.write_input_dat(str(d / "input.dat"), "mesh.msh", knod=4, reyn=100.0, dt=1e-3, num_steps=2,
+                                problem_type=1, lnod_in=2)
+    else:
+        shutil.copytree(os.path.join(GOLDEN, case), d)
+    lines = open(d / "input.dat").read().split("\n")
+    assert lines[-3] == "sample_points file"
+    lines[-2] = "samples.dat"
+    open(d / "input.dat", "w").write("\n".join(lines))
+    xy = msh_nodes(str(d / "mesh.msh"))
+    lo, hi = xy.min(axis=0), xy.max(axis=0)
+    rng = np.random.Generator(np.random.PCG64(7))
+    pts = lo - 0.02 * (hi - lo) + rng.random((40, 2)) * 1.04 * (hi - lo)
+    with open(d / "samples.dat", "w") as f:
+        for x, y in pts:
+            f.write(f"{x:.17g} {y:.17g}\n")
+    env = dict(os.environ, HO_SHIM_SOLVER="direct")
+    subprocess.run([REF, str(d / "input.dat"), str(tmp_path / "fields"), "--solve", "--samples"], check=True, env=env,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=300)
+    f = {k: np.load(tmp_path / "fields" / f"solve_{k}.npy") for k in
+         ("vorticity", "psi", "vel", "rhs_diff", "rhs_adv", "bc_w", "bc_nv", "bc_pv")}
+    knod, lnod_in, ptype, nsteps = int(lines[3]), int(lines[5]), int(lines[25]), int(lines[27])
+    ours = tmp_path / "ours"
+    ours.mkdir()
+    rc = vtk_harness.write_vtk_host(str(d / "mesh.msh").encode(), 0, knod, ptype, _dp(f["vorticity"]),
+                                    _dp(f["psi"]), _dp(f["vel"][..., 0]), _dp(f["vel"][..., 1]), _dp(f["rhs_diff"]),
+                                    _dp(f["rhs_adv"]), _dp(f["bc_w"]), _dp(f["bc_nv"]), _dp(f["bc_pv"]), nsteps, -1,
+                                    str(ours).encode(), str(d / "samples.dat").encode())
+    assert rc == 0
+    name = f"sampling_points{ptype}_K{knod}_L{lnod_in + 1}_{nsteps:05d}.dat"
+    assert os.path.exists(d / name) and os.path.exists(ours / name)
+    compare_vtk(str(ours / name), str(d / name))
+    assert len(open(ours / name).read().split("\n")) == len(pts) + 1
+    # the points outside the domain took the nearest-node fallback
+    L2 = (lnod_in + 1) ** 2
+    elem, shape = np.zeros(64, np.int32), np.zeros(64 * L2)
+    n = vtk_harness.sample_points_host(str(d / "mesh.msh").encode(), 0, str(d / "samples.dat").encode(),
+                                       elem.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(shape), 64)
+    assert n == len(pts)
+    sh = shape[: n * L2].reshape(n, L2)
+    np.testing.assert_allclose(sh.sum(axis=1), 1.0, atol=1e-12)  # a partition of unity
+    assert elem[:n].min() >= 0
 
 
 @pytest.mark.gpu
