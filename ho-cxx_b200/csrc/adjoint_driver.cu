@@ -107,7 +107,8 @@ Error Solver::adjoint_prepare() {
     HO2D_CUDA(a.scalars.alloc(sizeof(KrylovScalars)), "alloc scalars");
     HO2D_CUDA(cudaMemset(a.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
     // column sums of A's blocks: (A^T P u)(el, ij) = sum over the 5 block slots of el of
-    // u[c] * sum_r A[(c, r), (el, ij)], c = the slot's element
+    // u[c] * sum_r A[(c, r), (el, ij)], c = the slot's element: the column sums (over rows
+    // r, ascending) of block (c, s2), the slot of c whose column element is el
     std::vector<double> rsT((size_t)N * 5 * K2, 0.0);
     for (int el = 0; el < N; ++el)
         for (int s = 0; s < 5; ++s) {
@@ -117,12 +118,8 @@ Error Solver::adjoint_prepare() {
             for (int q = 0; q < 5; ++q)
                 if (op_.block_col[(size_t)c * 5 + q] == el) s2 = q;
             if (s2 < 0) return {3, "Poisson block structure is not symmetric"};
-            const double* blk = &op_.blocks[((size_t)c * 5 + s2) * K2 * K2];  // [col rs][row ij] of A
-            for (int ij = 0; ij < K2; ++ij) {
-                double acc = 0.0;
-                for (int r = 0; r < K2; ++r) acc += blk[(size_t)ij * K2 + r];
-                rsT[((size_t)el * 5 + s) * K2 + ij] = acc;
-            }
+            const double* cs = &op_.colsum[((size_t)c * 5 + s2) * K2];
+            std::copy(cs, cs + K2, rsT.begin() + ((size_t)el * 5 + s) * K2);
         }
     HO2D_CUDA(upload(a.rowsumT64, rsT), "upload transposed row sums");
     HO2D_CUDA(upload_as<float>(a.rowsumT32, rsT), "upload transposed row sums");

@@ -110,13 +110,18 @@ enum BcRole {
 };
 
 // Poisson operator: 5 K^2 x K^2 blocks per element (transposed) and the boundary source.
+// The device applies the operator matrix-free; of the blocks it needs only the inverse
+// diagonal blocks and sums, so the blocks themselves (5 K^4 values per element, 25 GB at
+// 262,144 elements and K = 7) are kept only on request.
 struct PoissonOperator {
     int K2 = 0;
-    std::vector<double> blocks;   // [N][5][K2][K2] (rs outer, ij inner)
+    std::vector<double> blocks;   // [N][5][K2][K2] (rs outer, ij inner); empty unless kept
     std::vector<int> block_col;   // [N][5] column element (-1 = empty slot)
     std::vector<double> bsrc;     // [N_eb][K2][K]
     std::vector<double> dinv;     // [N][K2][K2] inverse of the diagonal block (rs outer)
-    std::vector<double> rowsum;   // [N][5][K2] sum over rs of each block row
+    std::vector<double> rowsum;   // [N][5][K2] sum over rs of each block row (rs ascending)
+    std::vector<double> colsum;   // [N][5][K2] sum over ij of each block column (ij ascending)
+    std::vector<double> bsum;     // [N][5] sum of each block's entries (stored order)
     int64_t nnz = 0;              // entries surviving the |a| > 1e-14 filter
 };
 
@@ -130,7 +135,7 @@ Error make_bases(int K, int L, Bases& B);
 void make_metrics(const Mesh& mesh, const Bases& B, Metrics& M);
 Error setup_bcs(const Input& in, const Mesh& mesh, const Bases& B, BoundaryConditions& bc);
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
-                      PoissonOperator& op);
+                      PoissonOperator& op, bool keep_blocks = false);
 int tensor2fem(int i, int j, int lnod_in);
 
 // Fields written by the VTK output: volume arrays [N][K][K] (vorticity, streamfunction,

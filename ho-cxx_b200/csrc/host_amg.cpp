@@ -296,7 +296,6 @@ Ell to_ell(const Csr& A) {
 }
 
 Csr p0_coarse_operator(const PoissonOperator& op, int N) {
-    const int K2 = op.K2;
     Csr A;
     A.n = A.m = N;
     A.ptr.assign(N + 1, 0);
@@ -305,10 +304,7 @@ Csr p0_coarse_operator(const PoissonOperator& op, int N) {
         for (int s = 0; s < 5; ++s) {
             const int c = op.block_col[(size_t)el * 5 + s];
             if (c < 0) continue;
-            const double* b = &op.blocks[((size_t)el * 5 + s) * K2 * K2];
-            double sum = 0.0;
-            for (int q = 0; q < K2 * K2; ++q) sum += b[q];
-            row.push_back({c, sum});
+            row.push_back({c, op.bsum[(size_t)el * 5 + s]});
         }
         std::sort(row.begin(), row.end());
         for (size_t k = 0; k < row.size(); ++k) {

@@ -514,13 +514,16 @@ inline int bf_of(int side, int k, int K) { return (side / 2) * (K - 2 * k - 1) +
 }  // namespace
 
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
-                      PoissonOperator& op) {
+                      PoissonOperator& op, bool keep_blocks) {
     const int N = mesh.n_el, K = B.K, K2 = K * K, K4 = K2 * K2;
     op.K2 = K2;
-    op.blocks.assign((size_t)N * 5 * K4, 0.0);
+    op.blocks.assign(keep_blocks ? (size_t)N * 5 * K4 : 0, 0.0);
     op.block_col.assign((size_t)N * 5, -1);
     op.bsrc.assign((size_t)mesh.n_eb * K2 * K, 0.0);
     op.dinv.assign((size_t)N * K4, 0.0);
+    op.rowsum.assign((size_t)N * 5 * K2, 0.0);
+    op.colsum.assign((size_t)N * 5 * K2, 0.0);
+    op.bsum.assign((size_t)N * 5, 0.0);
     const std::vector<Entry> vol = volume_entries(B);
     std::vector<Entry> fw[2][2];
     for (int d = 0; d < 2; ++d)
@@ -529,7 +532,7 @@ void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const 
     int64_t nnz = 0;
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : nnz)
     for (int el = 0; el < N; ++el) {
-        std::vector<double> Lc(K4, 0.0), Ln(4 * (size_t)K4, 0.0), W(K2 * K), WN(K2 * K), Nm(K * K);
+        std::vector<double> Lc(K4, 0.0), Ln(4 * (size_t)K4, 0.0), W(K2 * K), WN(K2 * K), Nm(K * K), T(K4);
         const double* G = &M.G[(size_t)el * K2 * 4];
         for (const Entry& e : vol) Lc[e.row] += e.c * G[e.g];
         for (int ijp = 0; ijp < 4; ++ijp) {
@@ -622,27 +625,41 @@ void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const 
             }
         }
         op.block_col[(size_t)el * 5] = el;
-        // filter and store transposed: blocks[el][slot][rs][ij]
+        // filter, transpose (T[rs][ij]) and reduce each block: row sums over rs, column sums
+        // over ij and the block sum in the stored order
+        std::vector<double> Dm(K4);
         auto store = [&](const double* src, int slot) {
-            double* dst = &op.blocks[((size_t)el * 5 + slot) * K4];
             int64_t cnt = 0;
             for (int ij = 0; ij < K2; ++ij)
                 for (int rs = 0; rs < K2; ++rs) {
                     double v = src[ij * K2 + rs];
                     if (!(std::fabs(v) > 1e-14)) v = 0.0;
                     else ++cnt;
-                    dst[rs * K2 + ij] = v;
+                    T[rs * K2 + ij] = v;
+                    if (slot == 0) Dm[ij * K2 + rs] = v;
                 }
+            const size_t eb = (size_t)el * 5 + slot;
+            double* rsum = &op.rowsum[eb * K2];
+            double* csum = &op.colsum[eb * K2];
+            double tot = 0.0;
+            for (int rs = 0; rs < K2; ++rs)
+                for (int ij = 0; ij < K2; ++ij) {
+                    rsum[ij] += T[rs * K2 + ij];
+                    tot += T[rs * K2 + ij];
+                }
+            for (int rs = 0; rs < K2; ++rs) {
+                double acc = 0.0;
+                for (int ij = 0; ij < K2; ++ij) acc += T[rs * K2 + ij];
+                csum[rs] = acc;
+            }
+            op.bsum[eb] = tot;
+            if (keep_blocks) std::copy(T.begin(), T.end(), op.blocks.begin() + eb * K4);
             return cnt;
         };
         nnz += store(Lc.data(), 0);
         for (int ijp = 0; ijp < 4; ++ijp)
             if (op.block_col[(size_t)el * 5 + 1 + ijp] >= 0) nnz += store(&Ln[(size_t)ijp * K4], 1 + ijp);
         // inverse of the filtered diagonal block, stored transposed like the blocks
-        std::vector<double> Dm(K4);
-        const double* blk = &op.blocks[((size_t)el * 5) * K4];
-        for (int ij = 0; ij < K2; ++ij)
-            for (int rs = 0; rs < K2; ++rs) Dm[ij * K2 + rs] = blk[rs * K2 + ij];
         invert(K2, Dm);
         double* di = &op.dinv[(size_t)el * K4];
         for (int ij = 0; ij < K2; ++ij)

@@ -149,14 +149,8 @@ Error Solver::setup_from_mesh() {
         HO2D_CUDA(upload(*b, zv), "alloc fields");
     const std::vector<double> zf(nf, 0.0);
     for (DeviceBuffer* b : {&d.psi_tv, &d.psi_tg, &d.w_tv, &d.w_tg, &d.U_t}) HO2D_CUDA(upload(*b, zf), "alloc traces");
-    // Poisson operator
-    // row sums of every block (the two-level smoother's A e for element-wise constant e)
-    op_.rowsum.assign((size_t)N * 5 * K2, 0.0);
-    for (size_t eb = 0; eb < (size_t)N * 5; ++eb) {
-        const double* blk = &op_.blocks[eb * K2 * K2];
-        for (int rs = 0; rs < K2; ++rs)
-            for (int ij = 0; ij < K2; ++ij) op_.rowsum[eb * K2 + ij] += blk[rs * K2 + ij];
-    }
+    // Poisson operator: the inverse diagonal blocks and the row sums of every block (the
+    // two-level smoother's A e for element-wise constant e), from assemble_poisson
     // 8 zero entries past the end: the smoothing kernel copies the 16-byte-aligned
     // superset of a CTA's blocks into shared memory
     op_.dinv.resize(op_.dinv.size() + 8, 0.0);

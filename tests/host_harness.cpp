@@ -2,6 +2,7 @@
 // host_setup.cpp, host_hybrid.cpp) for CPU tests against the reference's own setup arrays:
 // a case is set up from an input.dat + Gmsh mesh, or from the arrays a hybrid driver
 // passes, and its tables are read out by name. Never part of the library.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -28,7 +29,7 @@ int finish(Case* c) {
     ho2d::make_metrics(c->m, c->B, c->M);
     e = ho2d::setup_bcs(c->in, c->m, c->B, c->bc);
     if (e.code) return e.code;
-    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, c->op);
+    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, c->op, /*keep_blocks=*/true);
     if (c->in.problem_type == 11) ho2d::open_normals(c->m, c->B, c->M, c->bc, c->nrm);
     return 0;
 }
@@ -110,6 +111,15 @@ extern "C" long case_get(void* h, const char* name, double* out) {
     const ho2d::Metrics& M = c->M;
     const ho2d::BoundaryConditions& bc = c->bc;
     const ho2d::PoissonOperator& op = c->op;
+    if (n == "node_xy") return copy_out(m.node_xy, out);
+    if (n == "elem_nodes" || n == "bedge_nodes") {  // [N][Lnod^2] node slots, [N_eb][Lnod] edge nodes
+        std::vector<int> flat;
+        if (n == "elem_nodes")
+            for (const auto& e : m.elem_nodes) flat.insert(flat.end(), e.begin(), e.end());
+        else
+            for (int e = 0; e < m.n_eb; ++e) flat.insert(flat.end(), m.edge_nodes[e].begin(), m.edge_nodes[e].end());
+        return copy_out(flat, out);
+    }
     if (n == "nbr") return copy_out(m.nbr, out);
     if (n == "nbr_side") return copy_out(m.nbr_side, out);
     if (n == "bidx") return copy_out(m.bidx, out);
@@ -154,6 +164,44 @@ extern "C" long case_get(void* h, const char* name, double* out) {
         return copy_out(c->tmp, out);
     }
     return -1;
+}
+
+// The block reductions assemble_poisson streams (row sums, column sums, block sums) against
+// the same sums taken from the kept blocks in the order their consumers summed them when
+// the blocks were stored (rs, then ij ascending; rows ascending; stored order), and a second
+// assembly without the blocks against the first. Returns the number of values that differ
+// in any bit, or -1 if the assembly without blocks kept some.
+extern "C" long case_check_block_reductions(void* h) {
+    const Case* c = static_cast<Case*>(h);
+    const ho2d::PoissonOperator& op = c->op;
+    const int K2 = op.K2;
+    const size_t nb = (size_t)c->m.n_el * 5;
+    long bad = 0;
+    for (size_t eb = 0; eb < nb; ++eb) {
+        const double* blk = &op.blocks[eb * K2 * K2];
+        std::vector<double> rs(K2, 0.0);
+        double tot = 0.0;
+        for (int r = 0; r < K2; ++r)
+            for (int ij = 0; ij < K2; ++ij) rs[ij] += blk[r * K2 + ij];
+        for (int q = 0; q < K2 * K2; ++q) tot += blk[q];
+        for (int x = 0; x < K2; ++x) {
+            double acc = 0.0;
+            for (int r = 0; r < K2; ++r) acc += blk[(size_t)x * K2 + r];
+            bad += std::memcmp(&acc, &op.colsum[eb * K2 + x], 8) != 0;
+            bad += std::memcmp(&rs[x], &op.rowsum[eb * K2 + x], 8) != 0;
+        }
+        bad += std::memcmp(&tot, &op.bsum[eb], 8) != 0;
+    }
+    ho2d::PoissonOperator s;
+    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, s);
+    if (!s.blocks.empty()) return -1;
+    auto diff = [](const std::vector<double>& a, const std::vector<double>& b) {
+        if (a.size() != b.size()) return (long)std::max(a.size(), b.size());
+        return (long)(std::memcmp(a.data(), b.data(), a.size() * 8) != 0);
+    };
+    bad += diff(s.dinv, op.dinv) + diff(s.rowsum, op.rowsum) + diff(s.colsum, op.colsum) + diff(s.bsum, op.bsum) +
+           diff(s.bsrc, op.bsrc) + (s.nnz != op.nnz) + (s.block_col != op.block_col);
+    return bad;
 }
 
 // split_open_velocities of the driver's open-boundary velocities into vn, vp [N_eb][K]

@@ -52,6 +52,8 @@ def lib(tmp_path_factory):
     L.case_get.restype = ctypes.c_long
     L.case_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
     L.case_split_open.argtypes = [ctypes.c_void_p] * 4
+    L.case_check_block_reductions.restype = ctypes.c_long
+    L.case_check_block_reductions.argtypes = [ctypes.c_void_p]
     return L
 
 
@@ -185,6 +187,66 @@ def test_block_jacobi_inverse(golden):
         assert col[el, 0] == el
         Dm = blocks[el, 0].T  # [ij][rs]
         assert np.abs(dinv[el].T @ Dm - np.eye(K2)).max() <= 1e-12 * np.linalg.cond(Dm)
+
+
+def test_streamed_block_reductions(golden):
+    """assemble_poisson keeps the blocks only on request. The row, column and block sums it
+    streams instead must be the sums of the kept blocks, bit for bit, in the summation order
+    the preconditioner setups used. An assembly without the blocks must give the same
+    outputs."""
+    c, _, _ = golden
+    assert c.lib.case_check_block_reductions(c.h) == 0
+
+
+def _roundtrip_meshes():
+    from ho2d import meshgen
+
+    from test_vtk import q2_cavity
+
+    return {"cavity_jittered": meshgen.cavity(6, jitter=0.2, seed=3),
+            "bfs": meshgen.backward_facing_step(h=1.0 / 3.0, jitter=0.15, seed=2),
+            "cylinder": meshgen.cylinder_ogrid(n_r=4, n_theta=12, r0=0.5, r1=3.0),
+            "q2_cavity": q2_cavity(n=3)}
+
+
+@pytest.mark.parametrize("name", ["cavity_jittered", "bfs", "cylinder", "q2_cavity"])
+def test_msh_writer_reader_round_trip(lib, tmp_path, name):
+    """meshgen.write_msh then the library's reader (read_msh, process_mesh): every element's
+    nodes in Gmsh slot order, every boundary group with its edges, coordinates exact
+    (written with 17 significant digits)."""
+    from ho2d import meshgen
+
+    mesh = _roundtrip_meshes()[name]
+    meshgen.write_msh(mesh, str(tmp_path / "mesh.msh"))
+    quadratic = mesh.quads.shape[1] == 9
+    meshgen.write_input_dat(str(tmp_path / "input.dat"), "mesh.msh", knod=3, reyn=100.0, dt=1e-3, num_steps=1,
+                            problem_type=1, lnod_in=2 if quadratic else 1)
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(str(tmp_path / "input.dat").encode(), ctypes.byref(code))
+    # problem type 1 only sets up the cavity's walls; any group names are accepted
+    assert h, f"setup failed with code {code.value}"
+    c = HostCase(lib, h)
+    try:
+        L2 = mesh.quads.shape[1]
+        assert (c.N, c.L * c.L) == (mesh.n_el, L2)
+        xy = c["node_xy"].reshape(-1, 2)
+        el = c.ints("elem_nodes").reshape(c.N, L2)
+        np.testing.assert_array_equal(xy[el], mesh.xy[mesh.quads])
+        assert c.groups == list(mesh.boundaries)
+        be = c.ints("bedge_nodes").reshape(c.neb, c.L)
+        grp = c.ints("be_group")
+        for g, nm in enumerate(c.groups):
+            ref = mesh.boundaries[nm]
+            mine = be[grp == g]
+            assert len(mine) == len(ref), nm
+            # ends as an unordered pair (the reader orients edges by their element), then the
+            # midpoint of a quadratic edge; both hold the ends first
+            def key(p):
+                return tuple(sorted(map(tuple, p[:2]))) + tuple(map(tuple, p[2:]))
+
+            assert sorted(key(xy[e]) for e in mine) == sorted(key(mesh.xy[e]) for e in ref), nm
+    finally:
+        c.close()
 
 
 def _hybrid_arrays(name):
