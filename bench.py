@@ -58,6 +58,11 @@ def parse():
                          "forward + adjoint with FP32 states; gradient error against FP64 on the 128x128 mesh")
     ap.add_argument("--large-n", type=int, default=512)
     ap.add_argument("--large-steps", type=int, default=200)
+    ap.add_argument("--strouhal", action="store_true",
+                    help="vortex shedding behind the cylinder (problem type 3, Re=100, 48x96 O-grid, K=4): "
+                         "Strouhal number, mean drag and lift amplitude in FP64 and mixed, and their differences")
+    ap.add_argument("--t-end", type=float, default=80.0, help="time units simulated for --strouhal")
+    ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
     return ap.parse_args()
 
 
@@ -417,6 +422,19 @@ def main():
                                         "adjoint on the 4x coarser mesh", "value": r["coarse"]["omega0_grad_rel_l2"],
                               "unit": "relative L2", "higher_is_better": False, "n_gpus": 1,
                               "data": "synthetic (seeded jitter, spectrum and lid)", "result": r}))
+        return
+    if args.strouhal:
+        from ho2d import shedding
+
+        if rank == 0:
+            with tempfile.TemporaryDirectory() as tmp:
+                r = shedding.run(tmp, t_end=args.t_end, knod=args.shed_knod)
+            print(json.dumps({"metric": "Strouhal number of the cylinder wake (lift frequency x D / U)",
+                              "value": r["fp64"]["St"], "unit": "St", "higher_is_better": None, "n_gpus": 1,
+                              "dtype": "f64", "data": "synthetic (generated O-grid; Gaussian-vortex start)",
+                              "config": {"workload": "cylinder wake, Re=100, O-grid r in [0.5, 15], "
+                                                     f"t_end={args.t_end}", **r["case"]},
+                              "fp64": r["fp64"], "mixed": r["mixed"], "difference": r["difference"]}))
         return
     if args.adjoint:
         visible = os.environ.get("CUDA_VISIBLE_DEVICES")
