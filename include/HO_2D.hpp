@@ -42,7 +42,16 @@ class HO_2D {
     void form_metrics() { ensure_setup(); }
     void setup_IC_BC_SRC() { ensure_setup(); }
     void form_Laplace_operator_matrix() { ensure_setup(); }
-    char solve_vorticity_streamfunction() { return (char)check(ho2d_solve(h_)); }
+    // the time loop; like the reference, writes the dump-step VTK (and sample-point) files
+    // into the working directory unless set_output_dir chose another one ("" = none)
+    char solve_vorticity_streamfunction() {
+        if (!output_dir_set_) set_output_dir(".");
+        return (char)check(ho2d_solve(h_));
+    }
+    void set_output_dir(const std::string& dir) {
+        check(ho2d_set_output_dir(h_, dir.c_str()));
+        output_dir_set_ = true;
+    }
     char solve_advection_diffusion() { return (char)check(ho2d_step(h_, 1)); }
     void solveto_d(double outerdt, int32_t numstep, int32_t integtype, double reyn, int32_t region = 0) {
         check(ho2d_solveto(h_, outerdt, numstep, integtype, reyn, region));
@@ -51,10 +60,13 @@ class HO_2D {
     void getallvorts_d(int32_t len, double* v) { check(ho2d_get_vort(h_, len, v)); }
     void getsolnpts_d(int32_t len, double* xy) { check(ho2d_get_solution_points(h_, len, xy)); }
     // length of the getsolnpts_d array: x, y per solution point (src/HO_2D.cpp:3942-3944)
-    int32_t getsolnptlen() {
+    int32_t getsolnptlen() { return 2 * getsolnlen(); }
+    // length of the getallvorts_d / setsolnvort_d arrays: N_el * Knod^2 (no counterpart in
+    // the reference, which takes the length from getsolnptlen / 2)
+    int32_t getsolnlen() {
         int32_t n = 0, k = 0;
         check(ho2d_get_sizes(h_, &n, &k, nullptr, nullptr));
-        return 2 * n * k * k;
+        return n * k * k;
     }
 
     // hybrid operation (src/HO_2D.hpp:251-290)
@@ -108,4 +120,5 @@ class HO_2D {
     }
     ho2d_solver* h_ = nullptr;
     bool setup_ = false;
+    bool output_dir_set_ = false;
 };

@@ -126,3 +126,33 @@ def test_forces_need_setup():
         assert b"set up" in lib.ho2d_last_error(h)
     finally:
         lib.ho2d_destroy(h)
+
+
+def _cli():
+    import shutil
+
+    if shutil.which("nvcc") is None and not os.path.exists("/usr/local/cuda/bin/nvcc"):
+        pytest.skip("nvcc not available to link the CLI")
+    from ho2d import build
+
+    build.build(cli=True)
+    return os.path.join(os.path.dirname(build.LIB), "ho2d_main")
+
+
+def test_cli_arguments_and_input_errors(tmp_path):
+    """The command-line drop-in for src/main.cpp: usage on an unknown option, the input
+    reader's error code for a missing file and for an unsupported setting; none of these
+    reach the device."""
+    import subprocess
+
+    exe = _cli()
+    r = subprocess.run([exe, "--bogus"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 255 and "Usage" in r.stdout
+    r = subprocess.run([exe, str(tmp_path / "nope.dat")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2 and r.stdout.startswith("error 2:"), r.stdout
+    path = meshgen.make_case("cavity4", str(tmp_path), steps=1)
+    lines = open(path).read().split("\n")
+    lines[21] = "7"  # time integration type 7 does not exist
+    open(path, "w").write("\n".join(lines))
+    r = subprocess.run([exe, path, "--mixed"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 4 and "error 4:" in r.stdout, r.stdout
