@@ -324,6 +324,7 @@ struct StageAdjArgs {
     T* slot_pg;
     double* lpv;           // lam of BC_parl_vel, accumulated over stages
     double dt, re_inv;
+    int adv_type = 1;      // 1: discontinuous upwind flux; 2: continuous volumetric flux
 };
 
 template <int K, typename T>
@@ -331,12 +332,96 @@ struct ResidualAdjScratch {
     static constexpr int K2 = K * K, NF = 4 * K;
     LapAdjScratch<K, T> lap;
     T w[K2], ux[K2], uy[K2], ldv[K2], lA[K2], lB[K2], lw[K2], lux[K2], luy[K2];
-    T tvw[NF], ut[NF], lup[NF], lut[NF], ltva[NF], nU[NF], nwv[NF];
+    T tvw[NF], ut[NF], lup[NF], lut[NF], ltva[NF], nU[NF], nwv[NF], com[NF];
 };
 
-// Reverse of residual_kernel without the RK update (advection type 1): lam_k -> lam of
-// omega (own chain), of U^xi / U^eta, of the neighbours' omega and U traces, of
-// BC_diffusion and of BC_normal_vel.
+// Step (2) of the residual adjoint for advection type 2. Forward: the common volumetric
+// flux com = (U_L + s U_R) / 2 on interior faces and BC_normal_vel |g| on boundary faces;
+// the upwind face flux com (c_L omega_L + c_R omega_R), (c_L, c_R) = (t, 1 - t) for com > 0
+// and (1 - t, t) otherwise, t = 1 on E/N faces; BC_advection on boundary faces; inside,
+// f = cx omega, g = cy omega with cx = U^xi + sum over the W/E faces of (com - U_face) times
+// the Radau value at the point (cy likewise with the S/N faces).
+template <int K, typename T, class C>
+HO2D_HD void residual_adjoint_continuous(const C& c, bool active, int el, const FrGeom<T>& g, const DevBases<T>& b,
+                                         const StageAdjArgs<T>& a, ResidualAdjScratch<K, T>& s) {
+    constexpr int K2 = K * K, NF = 4 * K;
+    LapAdjScratch<K, T>& L = s.lap;
+    // (2a) the common volumetric flux of every face
+    if (active)
+        for (int o = c.tid; o < NF; o += C::nt) {
+            const int ijp = o / K, k = o % K;
+            const int nb = g.face_nb[el * 4 + ijp];
+            if (nb >= 0) {
+                int nijp = 0;
+                const int nq = adj_neighbour_point<K, T>(g, el, ijp, k, nb, &nijp, nullptr);
+                const T sign = T(2 * ((ijp + nijp) % 2) - 1);
+                s.com[o] = T(0.5) * (s.ut[o] + sign * a.U_t[nq]);
+            } else {
+                const int be = (-nb - 1) * K + adj_bf<K>(ijp, k);
+                s.com[o] = T(a.bc_nv[be]) * g.fAn[(el * 4 + ijp) * K + k];
+            }
+        }
+    c.sync();
+    // (2b) lam of f, g at the points -> lam of omega, and of cx, cy (= lam of U^xi, U^eta)
+    if (active)
+        for (int ij = c.tid; ij < K2; ij += C::nt) {
+            const int hi = ij / K, lo = ij % K;
+            const T lA = s.lA[ij] - s.lup[0 * K + hi] * b.sbb[lo * 2 + 0] - s.lup[1 * K + hi] * b.sbb[lo * 2 + 1];
+            const T lB = s.lB[ij] - s.lup[2 * K + lo] * b.sbb[hi * 2 + 0] - s.lup[3 * K + lo] * b.sbb[hi * 2 + 1];
+            const T cx = s.ux[ij] + (s.com[0 * K + hi] - s.ut[0 * K + hi]) * b.R[lo * 2 + 0] +
+                         (s.com[1 * K + hi] - s.ut[1 * K + hi]) * b.R[lo * 2 + 1];
+            const T cy = s.uy[ij] + (s.com[2 * K + lo] - s.ut[2 * K + lo]) * b.R[hi * 2 + 0] +
+                         (s.com[3 * K + lo] - s.ut[3 * K + lo]) * b.R[hi * 2 + 1];
+            s.lw[ij] = lA * cx + lB * cy;
+            s.lux[ij] = lA * s.w[ij];
+            s.luy[ij] = lB * s.w[ij];
+        }
+    c.sync();
+    // (2c) per face: lam of com from the Radau corrections and from the upwind flux, then
+    //      lam of the own and the neighbour's U and omega traces, of BC_vorticity and of
+    //      BC_normal_vel
+    if (active)
+        for (int o = c.tid; o < NF; o += C::nt) {
+            const int ijp = o / K, k = o % K, lr = ijp & 1;
+            const int nb = g.face_nb[el * 4 + ijp];
+            T lcv = T(0);
+            if (ijp < 2) {
+                for (int i = 0; i < K; ++i) lcv += s.lux[k * K + i] * b.R[i * 2 + lr];
+            } else {
+                for (int j = 0; j < K; ++j) lcv += s.luy[j * K + k] * b.R[j * 2 + lr];
+            }
+            const T lup = s.lup[o];
+            T lut = -lcv, ltv = T(0), nU = T(0), nwv = T(0);
+            if (nb >= 0) {
+                int nijp = 0;
+                const int nq = adj_neighbour_point<K, T>(g, el, ijp, k, nb, &nijp, nullptr);
+                const T sign = T(2 * ((ijp + nijp) % 2) - 1);
+                const T wl = s.tvw[o], wr = a.w_tv[nq], cvf = s.com[o], t = T(ijp % 2);
+                const T cl = cvf > T(0) ? t : T(1) - t, cr = T(1) - cl;
+                const T lcom = lcv + lup * (cl * wl + cr * wr);
+                lut += T(0.5) * lcom;
+                nU = T(0.5) * sign * lcom;
+                ltv = lup * cvf * cl;
+                nwv = lup * cvf * cr;
+            } else {
+                const int be = (-nb - 1) * K + adj_bf<K>(ijp, k);
+                const int q = (el * 4 + ijp) * K + k;
+                L.lcom[o] = lup * T(a.bc_nv[be]) * g.fAn[q];
+                a.lbc_nv[be] = double((lup * T(a.bc_w[be]) + lcv) * g.fAn[q]);
+            }
+            s.lut[o] = lut;
+            s.ltva[o] = ltv;
+            s.nU[o] = nU;
+            s.nwv[o] = nwv;
+        }
+    c.sync();
+}
+
+// Reverse of residual_kernel without the RK update: lam_k -> lam of omega (own chain), of
+// U^xi / U^eta, of the neighbours' omega and U traces, of BC_diffusion and of
+// BC_normal_vel. Advection type 1 (discontinuous flux, src/HO_2D.cpp:2245-2437) or type 2
+// (continuous volumetric flux, 2439-2645); the upwind choices are those of the forward
+// state (fixed where the flux is not differentiable).
 template <int K, typename T, class C>
 HO2D_HD void residual_adjoint_body(const C& c, bool active, int el, const FrGeom<T>& g, const DevBases<T>& b,
                                    const StageAdjArgs<T>& a, ResidualAdjScratch<K, T>& s) {
@@ -399,6 +484,9 @@ HO2D_HD void residual_adjoint_body(const C& c, bool active, int el, const FrGeom
         }
     }
     c.sync();
+    if (a.adv_type == 2) {
+        residual_adjoint_continuous<K, T>(c, active, el, g, b, a, s);
+    } else {
     // (2) volume fluxes U omega; the upwind face flux and the advective boundary flux
     if (active) {
         for (int ij = c.tid; ij < K2; ij += C::nt) {
@@ -450,6 +538,7 @@ HO2D_HD void residual_adjoint_body(const C& c, bool active, int el, const FrGeom
         }
     }
     c.sync();
+    }
     // (3) transposed face-value maps of the advective part; then the diffusion chain
     if (active) {
         for (int ij = c.tid; ij < K2; ij += C::nt) {

@@ -132,6 +132,10 @@ class HO_2D:
         self._check(self._lib.ho2d_get_solution_points(self._h, out.size, capi.dptr(out)))
         return out
 
+    def getsolnptlen(self) -> int:
+        """Length of the getsolnpts_d array: x, y per solution point (src/HO_2D.cpp:3942-3944)."""
+        return 2 * self.N_el * self.Knod * self.Knod
+
     # -- hybrid operation (src/HO_2D.hpp:251-290): an external Lagrangian driver
     def set_defaults(self) -> None:
         self._check(self._lib.ho2d_set_defaults(self._h))

@@ -81,7 +81,7 @@ void forward_traces(const HostGeom& h, const double* w, const double* u, const d
 template <int K>
 int stage_adjoint_k(const HostGeom& h, const double* w, const double* u, const double* v, const double* bc_w,
                     const double* bc_nv, const double* lam_k, double dt, double re_inv, double* lw_stage, double* lpsi,
-                    double* lpv) {
+                    double* lpv, int adv_type) {
     constexpr int K2 = K * K, NF = 4 * K;
     const int N = h.g.N, neb = h.g.n_eb;
     std::vector<double> w_tv, U_t;
@@ -114,6 +114,7 @@ int stage_adjoint_k(const HostGeom& h, const double* w, const double* u, const d
     a.lpv = lpv;
     a.dt = dt;
     a.re_inv = re_inv;
+    a.adv_type = adv_type;
     const ElemCtx<1> c{0};
     {
         auto* s = new ResidualAdjScratch<K, double>;
@@ -160,9 +161,10 @@ extern "C" int stage_adjoint_host(int K, int N, int n_eb, const int* face_nb, co
                                   const double* fmet, const int* be_group, const int* sw_p, const int* sw_d,
                                   const int* noslip, const double* bases, const double* w, const double* u,
                                   const double* v, const double* bc_w, const double* bc_nv, const double* lam_k,
-                                  double dt, double re_inv, double* lw_stage, double* lpsi, double* lpv) {
+                                  double dt, double re_inv, double* lw_stage, double* lpsi, double* lpv,
+                                  int adv_type) {
     const HostGeom h = make_geom(K, N, n_eb, face_nb, face_nijp, met, fmet, be_group, sw_p, sw_d, noslip, bases);
-    HARNESS_DISPATCH(K, stage_adjoint_k<KK>(h, w, u, v, bc_w, bc_nv, lam_k, dt, re_inv, lw_stage, lpsi, lpv))
+    HARNESS_DISPATCH(K, stage_adjoint_k<KK>(h, w, u, v, bc_w, bc_nv, lam_k, dt, re_inv, lw_stage, lpsi, lpv, adv_type))
 }
 
 extern "C" int poisson_transpose_host(int K, int N, int n_eb, const int* face_nb, const int* face_nijp,

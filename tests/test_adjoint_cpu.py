@@ -8,7 +8,8 @@ with the oracle:
   * the adjoint of one stage by the dot-product test <lam_k, J v> = <J^T lam_k, v>, with
     J v the complex-step derivative of the oracle's stage (ho2d_cs) and the transposed
     Poisson solve done by the oracle's LU. The stage is taken at a random vorticity so
-    that every face flux and both upwind branches are exercised.
+    that every face flux and both upwind branches are exercised, for both advection
+    schemes (type 1, discontinuous flux; type 2, continuous volumetric flux).
 """
 
 import ctypes
@@ -26,6 +27,7 @@ import ho2d_oracle as O
 
 CSRC = os.path.join(REPO, "ho-cxx_b200", "csrc")
 CASES = ["cav4_rk4", "cav4_euler_k3", "bfs2_rk4", "cyl4x8_rk4"]  # advection type 1
+CASES_ADV2 = ["cavj6_adv2", "cyl4x8_rk2_adv2"]  # advection type 2 (continuous volumetric flux)
 
 
 def _cuda_include():
@@ -108,13 +110,14 @@ def stage_adjoint(harness, c, g, w, lam_k, coeff=0.0):
     bw, bnv = np.ascontiguousarray(st["bc_w"]), np.ascontiguousarray(st["bc_nv"])
     wc, lk = np.ascontiguousarray(w, dtype=float), np.ascontiguousarray(lam_k, dtype=float)
     rc = harness.stage_adjoint_host(*g.args(), _p(wc), _p(u), _p(v), _p(bw), _p(bnv), _p(lk),
-                                    ctypes.c_double(c.dt), ctypes.c_double(c.re_inv), _p(lw), _p(lpsi), _p(lpv))
+                                    ctypes.c_double(c.dt), ctypes.c_double(c.re_inv), _p(lw), _p(lpsi), _p(lpv),
+                                    ctypes.c_int(c.adv_type))
     assert rc == 0
     mu = c.lu.solve(lpsi, trans="T")  # psi = A^-1 (-J omega - ...): lam_omega -= J A^-T lam_psi
     return lw - c.M["J"].ravel() * mu, lpv
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + CASES_ADV2)
 def test_stage_adjoint_dot_product(harness, name):
     c = case_of(name)
     g = Geom(c)
