@@ -1,5 +1,6 @@
 // host_harness.cpp -- host build of the library's setup code (ho-cxx_b200/csrc/host_io.cpp,
-// host_setup.cpp, host_hybrid.cpp) for CPU tests against the reference's own setup arrays:
+// host_setup.cpp, host_hybrid.cpp, host_amg.cpp) for CPU tests against the reference's own
+// setup arrays and the coarse hierarchy's defining identities:
 // a case is set up from an input.dat + Gmsh mesh, or from the arrays a hybrid driver
 // passes, and its tables are read out by name. Never part of the library.
 #include <algorithm>
@@ -8,6 +9,7 @@
 #include <vector>
 
 #include "host.hpp"
+#include "host_amg.hpp"
 
 namespace {
 
@@ -20,7 +22,20 @@ struct Case {
     ho2d::PoissonOperator op;
     std::vector<double> nrm;  // open-edge normals (problem type 11)
     std::vector<double> tmp;
+    ho2d::CoarseHierarchy H;
 };
+
+const ho2d::Csr* level_matrix(const Case* c, int level, const std::string& which) {
+    if (level < 0 || level >= (int)c->H.levels.size()) return nullptr;
+    const ho2d::AmgLevel& L = c->H.levels[level];
+    if (which == "A") return &L.A;
+    if (which == "P") return &L.P;
+    if (which == "R") return &L.R;
+    if (which == "M") return &L.M;
+    if (which == "S") return &L.S;
+    if (which == "Q") return &L.Q;
+    return nullptr;
+}
 
 // the steps after the mesh, in the order of Solver::setup_from_mesh
 int finish(Case* c) {
@@ -202,6 +217,53 @@ extern "C" long case_check_block_reductions(void* h) {
     bad += diff(s.dinv, op.dinv) + diff(s.rowsum, op.rowsum) + diff(s.colsum, op.colsum) + diff(s.bsum, op.bsum) +
            diff(s.bsrc, op.bsrc) + (s.nnz != op.nnz) + (s.block_col != op.block_col);
     return bad;
+}
+
+// The coarse hierarchy of the case's P0 operator (p0_coarse_operator, build_coarse_hierarchy)
+// with the given dense-solve thresholds; returns the number of levels, or -code.
+extern "C" int case_build_hierarchy(void* h, int dense_max, int dense_max_first) {
+    Case* c = static_cast<Case*>(h);
+    const ho2d::Csr A1 = ho2d::p0_coarse_operator(c->op, c->m.n_el);
+    const ho2d::Error e = ho2d::build_coarse_hierarchy(A1, c->H, dense_max, dense_max_first);
+    return e.code ? -e.code : (int)c->H.levels.size();
+}
+
+// Matrix `which` (A, P, R, M, S, Q) of a level as CSR: dims = rows, columns, entries; the
+// arrays are filled when not null. Returns 0, or -1 for an unknown level or matrix.
+extern "C" int case_level_csr(void* h, int level, const char* which, long* dims, int* ptr, int* col, double* val) {
+    const ho2d::Csr* A = level_matrix(static_cast<Case*>(h), level, which);
+    if (!A) return -1;
+    dims[0] = A->n;
+    dims[1] = A->m;
+    dims[2] = (long)A->val.size();
+    if (ptr) std::copy(A->ptr.begin(), A->ptr.end(), ptr);
+    if (col) std::copy(A->col.begin(), A->col.end(), col);
+    if (val) std::copy(A->val.begin(), A->val.end(), val);
+    return 0;
+}
+
+// The same matrix as ELL (to_ell): dims = rows, columns, row width.
+extern "C" int case_level_ell(void* h, int level, const char* which, long* dims, int* col, double* val) {
+    const ho2d::Csr* A = level_matrix(static_cast<Case*>(h), level, which);
+    if (!A) return -1;
+    const ho2d::Ell E = ho2d::to_ell(*A);
+    dims[0] = E.n;
+    dims[1] = E.m;
+    dims[2] = E.w;
+    if (col) std::copy(E.col.begin(), E.col.end(), col);
+    if (val) std::copy(E.val.begin(), E.val.end(), val);
+    return 0;
+}
+
+// SPAI-0 weights of a level (length = its rows), or the dense inverse of the last level
+// (level = -1; length n_dense^2). Returns the length, or -1.
+extern "C" long case_level_vec(void* h, int level, double* out) {
+    const Case* c = static_cast<Case*>(h);
+    const std::vector<double>* v = level == -1 ? &c->H.dense_inv
+                                  : (level >= 0 && level < (int)c->H.levels.size() ? &c->H.levels[level].m : nullptr);
+    if (!v) return -1;
+    if (out) std::copy(v->begin(), v->end(), out);
+    return (long)v->size();
 }
 
 // split_open_velocities of the driver's open-boundary velocities into vn, vp [N_eb][K]

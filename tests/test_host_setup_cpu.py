@@ -39,7 +39,8 @@ def lib(tmp_path_factory):
         pytest.skip("g++ not available")
     out = str(tmp_path_factory.mktemp("host_harness") / "libhost_harness.so")
     srcs = [os.path.join(REPO, "tests", "host_harness.cpp")] + [os.path.join(CSRC, f) for f in
-                                                                 ("host_io.cpp", "host_setup.cpp", "host_hybrid.cpp")]
+                                                                 ("host_io.cpp", "host_setup.cpp", "host_hybrid.cpp",
+                                                                  "host_amg.cpp")]
     subprocess.run(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-I", CSRC, *srcs, "-o", out], check=True,
                    capture_output=True, text=True)
     L = ctypes.CDLL(out)
@@ -54,6 +55,11 @@ def lib(tmp_path_factory):
     L.case_split_open.argtypes = [ctypes.c_void_p] * 4
     L.case_check_block_reductions.restype = ctypes.c_long
     L.case_check_block_reductions.argtypes = [ctypes.c_void_p]
+    L.case_build_hierarchy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.case_level_csr.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p] + [ctypes.c_void_p] * 4
+    L.case_level_ell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p] + [ctypes.c_void_p] * 3
+    L.case_level_vec.restype = ctypes.c_long
+    L.case_level_vec.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     return L
 
 
@@ -365,3 +371,130 @@ def test_hybrid_open_velocity_split(hybrid):
         vn, vp = vn.reshape(c.neb, K)[open_rows], vp.reshape(c.neb, K)[open_rows]
         assert close_abs(vn, s[f"open_velnorm_end_{st}"], 1e-13), st
         assert close_abs(vp, s[f"open_velparl_end_{st}"], 1e-13), st
+
+
+# ---- coarse hierarchy of the Poisson preconditioner (host_amg.cpp) ----------------------
+
+
+def _level(c, level, which):
+    dims = (ctypes.c_long * 3)()
+    if c.lib.case_level_csr(c.h, level, which.encode(), dims, None, None, None) != 0:
+        return None
+    n, m, nnz = list(dims)
+    ptr, col, val = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    c.lib.case_level_csr(c.h, level, which.encode(), dims, ptr.ctypes.data_as(ctypes.c_void_p),
+                         col.ctypes.data_as(ctypes.c_void_p), val.ctypes.data_as(ctypes.c_void_p))
+    return sp.csr_matrix((val, col, ptr), shape=(n, m))
+
+
+def _vec(c, level):
+    n = c.lib.case_level_vec(c.h, level, None)
+    out = np.zeros(n)
+    c.lib.case_level_vec(c.h, level, out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+@pytest.fixture(scope="module", params=["bfs2_rk4", "cyl4x8_rk4", "cavity24j"])
+def hierarchy(request, lib, tmp_path_factory):
+    """A coarse hierarchy forced to coarsen (dense-solve size 8, or 64 on the 24 x 24
+    jittered cavity) and the assembled operator it starts from."""
+    if request.param.startswith("cavity"):
+        from ho2d import meshgen
+
+        inp = meshgen.make_case("cavityj24", str(tmp_path_factory.mktemp("amg")), knod=3, jitter=0.2, seed=7)
+        dense = 64
+    else:
+        inp = os.path.join(GOLDEN, request.param, "input.dat")
+        dense = 8
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(inp.encode(), ctypes.byref(code))
+    assert h, code.value
+    c = HostCase(lib, h)
+    L = lib.case_build_hierarchy(h, dense, dense)
+    assert L >= 2, L
+    yield c, L, blocks_to_csr(c)
+    c.close()
+
+
+def _dense_close(a, b, tol=1e-12):
+    a, b = np.asarray(a.todense() if sp.issparse(a) else a), np.asarray(b.todense() if sp.issparse(b) else b)
+    return np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1e-300)
+
+
+def test_p0_level_is_the_galerkin_operator(hierarchy):
+    """Level 0 = P^T A P for P the element indicator, A the assembled FR operator (which the
+    Poisson test above pins to the reference's matrix)."""
+    c, _, A = hierarchy
+    K2 = c.K * c.K
+    P = sp.csr_matrix((np.ones(c.N * K2), (np.arange(c.N * K2), np.repeat(np.arange(c.N), K2))),
+                      shape=(c.N * K2, c.N))
+    assert _dense_close(_level(c, 0, "A"), P.T @ A @ P)
+
+
+def test_coarse_levels_are_galerkin_products(hierarchy):
+    c, L, _ = hierarchy
+    for l in range(L - 1):
+        A, P, R = _level(c, l, "A"), _level(c, l, "P"), _level(c, l, "R")
+        assert P.shape == (A.shape[0], _level(c, l + 1, "A").shape[0])
+        assert P.shape[1] < P.shape[0]  # it coarsens
+        assert _dense_close(R, P.T, 0.0)
+        assert _dense_close(_level(c, l + 1, "A"), R @ A @ P)
+        assert (np.asarray(abs(P).sum(axis=0)).ravel() > 0).all()  # no empty aggregate
+
+
+def test_spai0_weights(hierarchy):
+    c, L, _ = hierarchy
+    for l in range(L):
+        A = _level(c, l, "A")
+        m = _vec(c, l)
+        d = A.diagonal()
+        s = np.asarray(A.multiply(A).sum(axis=1)).ravel()
+        np.testing.assert_allclose(m, d / s, rtol=1e-14)
+
+
+def test_cycle_operators(hierarchy):
+    """M = R (I - A diag(m)), S = 2 diag(m) - diag(m) A diag(m), Q = (I - diag(m) A) P, and
+    together they are the V(1,1) two-level cycle with SPAI-0 smoothing from zero and an
+    exact coarse solve."""
+    c, L, _ = hierarchy
+    rng = np.random.Generator(np.random.PCG64(9))
+    for l in range(L - 1):
+        A, P, R = _level(c, l, "A"), _level(c, l, "P"), _level(c, l, "R")
+        m = _vec(c, l)
+        Dm = sp.diags(m)
+        I = sp.identity(A.shape[0])
+        M, S, Q = _level(c, l, "M"), _level(c, l, "S"), _level(c, l, "Q")
+        assert _dense_close(M, R @ (I - A @ Dm))
+        assert _dense_close(S, 2 * Dm - Dm @ A @ Dm)
+        assert _dense_close(Q, (I - Dm @ A) @ P)
+        f = rng.standard_normal(A.shape[0])
+        Ac = (R @ A @ P).toarray()
+        u1 = m * f
+        uc = np.linalg.solve(Ac, R @ (f - A @ u1))
+        u2 = u1 + P @ uc
+        u = u2 + m * (f - A @ u2)
+        np.testing.assert_allclose(S @ f + Q @ np.linalg.solve(Ac, M @ f), u, rtol=1e-10,
+                                   atol=1e-12 * np.abs(u).max())
+
+
+def test_coarsest_dense_inverse(hierarchy):
+    c, L, _ = hierarchy
+    A = _level(c, L - 1, "A").toarray()
+    inv = _vec(c, -1).reshape(A.shape)
+    assert np.abs(inv @ A - np.eye(A.shape[0])).max() < 1e-10 * np.linalg.cond(A)
+
+
+def test_ell_copies(hierarchy):
+    c, L, _ = hierarchy
+    for l in range(L):
+        for which in ("A", "M", "S", "Q") if l < L - 1 else ("A",):
+            A = _level(c, l, which)
+            dims = (ctypes.c_long * 3)()
+            assert c.lib.case_level_ell(c.h, l, which.encode(), dims, None, None) == 0
+            n, m, w = list(dims)
+            assert w % 4 == 0 and w >= np.diff(A.indptr).max()
+            col, val = np.zeros(n * w, np.int32), np.zeros(n * w)
+            c.lib.case_level_ell(c.h, l, which.encode(), dims, col.ctypes.data_as(ctypes.c_void_p),
+                                 val.ctypes.data_as(ctypes.c_void_p))
+            E = sp.csr_matrix((val, (np.repeat(np.arange(n), w), col)), shape=(n, m))  # padding adds zeros
+            assert _dense_close(E, A, 0.0)
