@@ -12,6 +12,7 @@
 
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace ho2d {
@@ -163,6 +164,30 @@ Error read_sample_points(const std::string& path, const Mesh& m, SamplePoints& s
 Error write_vtk_files(const Mesh& mesh, const Bases& B, int problem_type, const VtkFields& f, int indx, int subidx,
                       const std::string& dir, const SamplePoints* samples = nullptr);
 int tensor2fem_1d(int i, int lnod_in);
+
+// The VTK files of one dump written on a background thread, so that the time loop goes on
+// while the ASCII files are formatted. The job owns host copies of the fields; the mesh,
+// bases and sample points are read in place and must not change until wait() returns.
+// One write is in flight at a time: submit() first waits for the previous one. wait()
+// returns the first error since the last wait(); the destructor waits.
+class VtkQueue {
+  public:
+    struct Job {
+        std::vector<double> w, psi, u, v, rhs_diff, rhs_adv, bc_w, bc_nv, bc_pv;
+        int problem_type = 0, indx = 0, subidx = -1;
+        std::string dir;
+    };
+    VtkQueue() = default;
+    VtkQueue(const VtkQueue&) = delete;
+    VtkQueue& operator=(const VtkQueue&) = delete;
+    ~VtkQueue() { wait(); }
+    Error submit(const Mesh& mesh, const Bases& B, const SamplePoints* samples, Job job);
+    Error wait();
+
+  private:
+    std::thread thread_;
+    Error err_{0, ""};
+};
 
 // Hybrid operation (host_hybrid.cpp): the edges of the "open" boundary (null if none), the
 // getopenpts_d array length, solution-point areas [N][K][K], open-boundary points

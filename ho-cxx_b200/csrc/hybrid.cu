@@ -41,6 +41,7 @@ Error Solver::set_elemorder(int k) {
 Error Solver::load_mesh_arrays(int iorder, int nxy, const double* xy, int nidx, const int* idx, int nwall,
                                const int* wall, int nopen, const int* open) {
     setup_done_ = false;
+    vtk_queue_.wait();  // a dump still being written reads the mesh
     return mesh_from_arrays(iorder, nxy, xy, nidx, idx, nwall, wall, nopen, open, mesh_);
 }
 
@@ -49,6 +50,7 @@ Error Solver::load_mesh_arrays(int iorder, int nxy, const double* xy, int nidx, 
 Error Solver::load_inout_arrays(int ninval, const double* velin, int nin, const int* idxin, int noutval,
                                 const double* velout, int nout, const int* idxout) {
     if (mesh_.elem_nodes.empty()) return {1, "load the mesh arrays first"};
+    vtk_queue_.wait();
     HO2D_TRY(add_boundary_arrays(mesh_, "inlet", nin, idxin, ninval, velin));
     return add_boundary_arrays(mesh_, "outlet", nout, idxout, noutval, velout);
 }
@@ -57,6 +59,7 @@ Error Solver::load_inout_arrays(int ninval, const double* velin, int nin, const 
 Error Solver::process_mesh_input() {
     if (!input_done_) return {1, "call ho2d_set_defaults (or ho2d_read_input) first"};
     if (mesh_.elem_nodes.empty()) return {1, "load the mesh arrays first"};
+    vtk_queue_.wait();  // a dump still being written reads the mesh
     HO2D_TRY(process_mesh(mesh_));
     samples_ = SamplePoints();  // the reference reads no sample points here
     return setup_from_mesh();
@@ -147,6 +150,7 @@ Error Solver::get_hoquad_weights(double* out) {
 
 // clean_up (src/HO_2D.cpp:4275-4278): releases the device state; the handle can be set up again
 void Solver::release() {
+    vtk_queue_.wait();
     adj_.reset();
     d_.reset(new DeviceState);
     setup_done_ = false;

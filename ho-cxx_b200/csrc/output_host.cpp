@@ -9,7 +9,10 @@
 // the node-averaged vorticity and velocity interpolated with the geometry shape functions.
 #include <cmath>
 #include <cstdio>
+#include <memory>
+#include <new>
 #include <string>
+#include <system_error>
 #include <vector>
 
 #include "host.hpp"
@@ -224,6 +227,35 @@ Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, cons
         std::fprintf(sh.f, "%g %g %g %g %g\n", samples->xy[2 * s], samples->xy[2 * s + 1], om_s, ux, uy);
     }
     return {0, ""};
+}
+
+Error VtkQueue::submit(const Mesh& mesh, const Bases& B, const SamplePoints* samples, Job job) {
+    Error e = wait();
+    if (e.code) return e;
+    auto owned = std::make_shared<Job>(std::move(job));
+    auto work = [this, &mesh, &B, samples, owned]() {
+        const Job& j = *owned;
+        const VtkFields f{j.w.data(),       j.psi.data(),  j.u.data(),     j.v.data(),    j.rhs_diff.data(),
+                          j.rhs_adv.data(), j.bc_w.data(), j.bc_nv.data(), j.bc_pv.data()};
+        try {
+            err_ = write_vtk_files(mesh, B, j.problem_type, f, j.indx, j.subidx, j.dir, samples);
+        } catch (const std::bad_alloc&) {
+            err_ = {5, "out of host memory writing the VTK files"};
+        }
+    };
+    try {
+        thread_ = std::thread(work);
+    } catch (const std::system_error&) {  // no thread to be had: write here
+        work();
+    }
+    return {0, ""};
+}
+
+Error VtkQueue::wait() {
+    if (thread_.joinable()) thread_.join();
+    Error e = err_;
+    err_ = {0, ""};
+    return e;
 }
 
 }  // namespace ho2d

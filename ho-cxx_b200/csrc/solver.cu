@@ -69,6 +69,7 @@ Error Solver::read_input(const std::string& path) {
 
 Error Solver::setup() {
     if (!input_done_) return {1, "ho2d_setup called before ho2d_read_input"};
+    vtk_queue_.wait();  // a dump still being written reads the mesh replaced here
     std::string mesh_path = in_.mesh_file;
     if (!mesh_path.empty() && mesh_path[0] != '/') mesh_path = in_.base_dir + "/" + mesh_path;
     mesh_ = Mesh();
@@ -779,19 +780,21 @@ Error Solver::solve() {
     if (!setup_done_) return {1, "ho2d_solve called before ho2d_setup"};
     HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
     const int nt = in_.num_steps, df = std::max(1, in_.dump_freq);
+    // dumps are written on the VTK queue's thread while the loop goes on; all are on disk
+    // when solve returns
     for (int ti = 0; ti < nt; ++ti) {
         if (ti % df == 0) {
             HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
-            if (!output_dir_.empty()) HO2D_TRY(write_vtk(ti, -1, output_dir_));
+            if (!output_dir_.empty()) HO2D_TRY(queue_vtk(ti, output_dir_));
         }
         HO2D_TRY(step(1));
     }
     if (nt % df == 0) {
         HO2D_TRY(stage32_ ? velocity_only_t<float>() : velocity_only_t<double>());
-        if (!output_dir_.empty()) HO2D_TRY(write_vtk(nt, -1, output_dir_));
+        if (!output_dir_.empty()) HO2D_TRY(queue_vtk(nt, output_dir_));
     }
     HO2D_CUDA(cudaStreamSynchronize(d_->stream), "solve");
-    return {0, ""};
+    return vtk_queue_.wait();
 }
 
 Error Solver::solveto(double outerdt, int numstep, int integtype, double reyn) {

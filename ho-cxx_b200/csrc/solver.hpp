@@ -131,6 +131,8 @@ class Solver {
   private:
     Error stage_impl(double coeff, int rk_stage, bool update);
     Error poisson_solve();
+    Error vtk_job(int indx, int subidx, const std::string& dir, VtkQueue::Job& j);  // output.cu
+    Error queue_vtk(int indx, const std::string& dir);
     template <typename T>
     Error stage_t(double coeff, int rk_stage, bool update, bool solve = true);
     template <typename T>
@@ -172,6 +174,7 @@ class Solver {
     bool hybrid_ = false;                     // enable_hybrid: set_vort feeds the blend target
     std::string output_dir_;                  // where solve() writes its VTK files (empty: none)
     SamplePoints samples_;                    // the input's sample points (VTK output)
+    VtkQueue vtk_queue_;                      // dumps being written (declared after what it reads)
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

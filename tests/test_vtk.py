@@ -99,6 +99,19 @@ def test_vtk_writer_reproduces_reference_files(tmp_path, vtk_harness, case):
     assert files == [f"problem{ptype}_K{knod}_{nsteps:05d}.vtk", f"vorticity{ptype}_K{knod}_{nsteps:05d}.vtk"]
     for fn in files:  # identical except for round-off around zero (summation order)
         compare_vtk(str(ours / fn), str(d / fn))
+    # the time loop's dumps go through VtkQueue's thread: the same bytes, for two dumps in a row
+    queued = tmp_path / "queued"
+    queued.mkdir()
+    rc = vtk_harness.write_vtk_queued_host(str(d / "mesh.msh").encode(), 0, knod, ptype, _dp(f["vorticity"]),
+                                           _dp(f["psi"]), _dp(f["vel"][..., 0]), _dp(f["vel"][..., 1]),
+                                           _dp(f["rhs_diff"]), _dp(f["rhs_adv"]), _dp(f["bc_w"]), _dp(f["bc_nv"]),
+                                           _dp(f["bc_pv"]), nsteps, str(queued).encode(), b"")
+    assert rc == 0
+    assert sorted(os.listdir(queued)) == sorted(files + [fn.replace(f"{nsteps:05d}", f"{nsteps + 1:05d}")
+                                                         for fn in files])
+    for fn in os.listdir(queued):
+        src = fn.replace(f"{nsteps + 1:05d}", f"{nsteps:05d}")
+        assert open(queued / fn).read() == open(ours / src).read(), fn
 
 
 def q2_cavity(n=3, amp=0.04):
