@@ -498,3 +498,65 @@ def test_ell_copies(hierarchy):
                                  val.ctypes.data_as(ctypes.c_void_p))
             E = sp.csr_matrix((val, (np.repeat(np.arange(n), w), col)), shape=(n, m))  # padding adds zeros
             assert _dense_close(E, A, 0.0)
+
+
+# ---- known answer: the reference's manufactured Poisson solution -----------------------
+
+
+def _bilinear_points(c, xi, eta):
+    """Physical coordinates of (xi, eta) in every bilinear element [N][..., 2]."""
+    xy = c["node_xy"].reshape(-1, 2)
+    en = c.ints("elem_nodes").reshape(c.N, 4)  # Gmsh slots SW, SE, NE, NW
+    N = [(1 - xi) * (1 - eta) / 4, (1 + xi) * (1 - eta) / 4, (1 + xi) * (1 + eta) / 4, (1 - xi) * (1 + eta) / 4]
+    return sum(N[a][None, ..., None] * xy[en[:, a]][(slice(None),) + (None,) * np.ndim(xi) + (slice(None),)]
+               for a in range(4))
+
+
+@pytest.mark.parametrize("jitter", [0.0, 0.2])
+def test_manufactured_poisson_solution_converges_spectrally(lib, tmp_path, jitter):
+    """The reference's Poisson test (src/HO_2D.cpp:1440, 1852-1879): omega =
+    -4 (r^2 + 1) exp(r^2), so that Lap psi = -omega has psi = exp(r^2); Dirichlet psi =
+    exp(r^2) on the walls of a 4 x 4 cavity. The library's assembled operator and boundary
+    source (the Poisson right-hand side -omega J - boundary_source . BC_Poisson) solved
+    exactly must approach exp(r^2) at the solution points spectrally in K."""
+    from ho2d import meshgen
+
+    errs = []
+    for K in (3, 4, 5, 6, 7):
+        d = tmp_path / f"k{K}_{jitter}"
+        inp = meshgen.make_case("cavityj4" if jitter else "cavity4", str(d), knod=K, jitter=jitter, seed=3)
+        code = ctypes.c_int(0)
+        h = lib.case_from_input(inp.encode(), ctypes.byref(code))
+        assert h, code.value
+        c = HostCase(lib, h)
+        try:
+            xs = c["xs"]
+            XI, ETA = np.meshgrid(xs, xs)  # [j][i]
+            sp_xy = _bilinear_points(c, XI, ETA)  # [N][j][i][2]
+            r2 = (sp_xy ** 2).sum(-1)
+            omega = -4.0 * (r2 + 1.0) * np.exp(r2)
+            # boundary flux points in boundary-array order: face point k of the element's
+            # side, stored at (side / 2)(K - 2k - 1) + k
+            bc_p = np.zeros((c.neb, K))
+            be_el, be_side = c.ints("be_el"), c.ints("be_side")
+            for e in range(c.neb):
+                side = be_side[e]
+                for k in range(K):
+                    t = xs[k]
+                    xi, eta = {0: (t, -1.0), 1: (1.0, t), 2: (t, 1.0), 3: (-1.0, t)}[side]
+                    p = _bilinear_points(c, np.array(xi), np.array(eta))[be_el[e]]
+                    bc_p[e, (side // 2) * (K - 2 * k - 1) + k] = np.exp((p ** 2).sum())
+            K2 = K * K
+            b = -(omega.reshape(c.N, K2) * c["J"].reshape(c.N, K2))
+            bsrc = c["bsrc"].reshape(c.neb, K2, K)
+            for e in range(c.neb):
+                b[be_el[e]] -= bsrc[e] @ bc_p[e]
+            from scipy.sparse.linalg import spsolve
+
+            psi = spsolve(blocks_to_csr(c).tocsc(), b.ravel())
+            errs.append(np.abs(psi - np.exp(r2).ravel()).max())
+        finally:
+            c.close()
+    errs = np.array(errs)
+    assert errs[-1] < 1e-6, errs
+    assert (errs[1:] < errs[:-1] / 3).all(), errs
