@@ -103,6 +103,8 @@ struct MfOp {
     const T* dinv;          // [N][K2][K2] inverse diagonal blocks, transposed ([rs][ij])
     const T* rowsum;        // [N][5][K2] row sums of the 5 blocks of each element row
     const int* bcol;        // [N][5] element of each block (slot 0 = self, 1 + ijp = neighbours)
+    // optional BF16 copy of dinv (bit patterns), read by the FP32 smoother when present
+    const unsigned short* dinv_bf16 = nullptr;
 };
 
 template <typename T>

@@ -20,6 +20,8 @@
 // needs, reduced deterministically (per-CTA partials summed in a fixed order by the last
 // CTA to finish); a `done` flag turns the rest of an enqueued batch into no-ops, so the
 // host only polls for convergence every few iterations.
+#include <type_traits>
+
 #include "device.cuh"
 #include "fr_device.cuh"
 #include "fr_launch.hpp"
@@ -392,17 +394,6 @@ __device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, c
     }
 }
 
-// z = Dinv y for one element, y in shared memory (Dinv stored [rs][ij])
-template <int K, typename T>
-__device__ __forceinline__ T block_apply(const T* __restrict__ dinv, const T* sy, int el, int ij) {
-    constexpr int K2 = K * K;
-    const T* d = dinv + (size_t)el * K2 * K2 + ij;
-    T acc = T(0);
-#pragma unroll
-    for (int rs = 0; rs < K2; ++rs) acc += __ldg(d + rs * K2) * sy[rs];
-    return acc;
-}
-
 // Element sums of a per-point value: every thread of element le stores its value, then
 // thread ij == 0 of each element adds the K^2 values in a fixed order. Collective.
 template <int K, typename T>
@@ -517,13 +508,21 @@ __device__ __forceinline__ T up0_part(const CoarseOut<T>& co, const F0<T>& f0, i
 }
 
 // Whether k_mf_post stages its CTA's inverse blocks (EPB x K^4 values, contiguous in
-// memory) in shared memory: when they fit in 32 KB of static shared memory.
-template <int K, typename T>
+// memory) in shared memory: when they fit in 32 KB of static shared memory. The blocks are
+// stored as T, or as BF16 bit patterns (BF16) for the FP32 smoother.
+template <int K, typename T, bool BF16 = false>
 struct PostStage {
+    using DT = typename std::conditional<BF16, unsigned short, T>::type;
     static constexpr int K4 = K * K * K * K;
-    static constexpr size_t kBytes = (size_t)Shape<K>::EPB * K4 * sizeof(T) + 32;  // + 16-byte alignment slack
+    static constexpr size_t kBytes = (size_t)Shape<K>::EPB * K4 * sizeof(DT) + 32;  // + 16-byte alignment slack
     static constexpr bool kOn = kBytes <= 32768;
 };
+
+__device__ __forceinline__ float block_value(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
+template <typename T>
+__device__ __forceinline__ T block_value(T v) {
+    return v;
+}
 
 // Preconditioner application, with the BiCGSTAB vector update that produces its operand:
 //   mode 0:  p = r + beta (p - omega v)  (p = r on the first iteration),  f = p -> ph
@@ -538,11 +537,12 @@ struct PostStage {
 // (cp.async, 16-byte pieces of the 16-byte-aligned superset of the blocks; the buffer is
 // padded past its end), and the block row sums and the vectors are loaded, so all of it
 // overlaps the up step's dependent loads.
-template <int K, typename T>
+template <int K, typename T, bool BF16 = false>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
                                                                 int has_coarse, double w, ReduceScratch rs, int mode) {
     using S = Shape<K>;
-    using PS = PostStage<K, T>;
+    using PS = PostStage<K, T, BF16>;
+    using DT = typename PS::DT;
     constexpr int K2 = S::K2;
     KrylovScalars* sc = rs.sc;
     const int done = sc->done;  // uniform; read early so the round trip overlaps the loads
@@ -553,18 +553,21 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const int p = el * K2 + ij;
-    const T* dblk = op.dinv + (size_t)el * PS::K4;  // this element's inverse block ([rs][ij])
+    const DT* dsrc;
+    if constexpr (BF16) dsrc = op.dinv_bf16;
+    else dsrc = op.dinv;
+    const DT* dblk = dsrc + (size_t)el * PS::K4;  // this element's inverse block ([rs][ij])
     if constexpr (PS::kOn) {
         const int el0 = blockIdx.x * S::EPB;
         const int el1 = min(el0 + S::EPB, op.g.N);
-        const size_t b0 = (size_t)el0 * PS::K4 * sizeof(T), b1 = (size_t)el1 * PS::K4 * sizeof(T);
+        const size_t b0 = (size_t)el0 * PS::K4 * sizeof(DT), b1 = (size_t)el1 * PS::K4 * sizeof(DT);
         const size_t a0 = b0 & ~size_t(15), a1 = (b1 + 15) & ~size_t(15);
-        const char* g = reinterpret_cast<const char*>(op.dinv) + a0;
+        const char* g = reinterpret_cast<const char*>(dsrc) + a0;
         const unsigned sb = (unsigned)__cvta_generic_to_shared(sd_raw);
         const unsigned nbytes = (unsigned)(a1 - a0);  // < 32 KB
         for (unsigned o = 16u * threadIdx.x; o < nbytes; o += 16u * blockDim.x)
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + o), "l"(g + o) : "memory");
-        dblk = reinterpret_cast<const T*>(sd_raw + (b0 - a0)) + (size_t)le * PS::K4;
+        dblk = reinterpret_cast<const DT*>(sd_raw + (b0 - a0)) + (size_t)le * PS::K4;
     }
     TraceDst<K> td;
     td.load(op.g.scat, active, el, ij);
@@ -625,7 +628,7 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     if (active) {
         T acc = T(0);
 #pragma unroll
-        for (int r = 0; r < K2; ++r) acc += dblk[r * K2 + ij] * sr[le][r];
+        for (int r = 0; r < K2; ++r) acc += T(block_value(dblk[r * K2 + ij])) * sr[le][r];
         const T zz = u_self + T(w) * acc;
         z[p] = zz;
         sz[le][ij] = zz;
@@ -869,11 +872,20 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
     const int mg = pc.nlev > 0;
     const CoarseOut<T> co = mg ? coarse_out(pc) : CoarseOut<T>();
     const unsigned gv = (g + kVecTiles - 1) / kVecTiles;
+    auto post = [&](int mode) {
+        if constexpr (std::is_same<T, float>::value) {
+            if (op.dinv_bf16) {
+                k_mf_post<K, T, true><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                return;
+            }
+        }
+        k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+    };
     if (mg) coarse_cycle<T>(pc, v, rs.sc, 0, s);
-    k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, 0);
+    post(0);
     k_mf_v<K, T><<<g, th, 0, s>>>(op, v, rs);
     if (mg) coarse_cycle<T>(pc, v, rs.sc, 1, s);
-    k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, 1);
+    post(1);
     k_mf_t<K, T><<<g, th, 0, s>>>(op, v, rs);
     k_xr_update<K, T><<<gv, th, 0, s>>>(N, v, rs, max_iter, h, has_handle);
 }

@@ -162,6 +162,7 @@ Error Solver::setup_from_mesh() {
     HO2D_TRY(setup_forces());
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
+    d.dinv_bf16.reset();
     d.rowsum32.reset();
     for (auto& b : d.pg32) b.reset();
     HO2D_TRY(setup_preconditioner());
@@ -441,6 +442,19 @@ Error Solver::upload_precision_arrays() {
     const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
     for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
     HO2D_CUDA(upload_as<float>(d.dinv32, op_.dinv), "upload fp32 block-Jacobi");
+    // HO2D_SMOOTHER_BF16=1: the FP32 smoother reads a BF16 copy of the inverse blocks (half
+    // the bytes; the preconditioner's precision changes only the inner iteration count)
+    if (const char* e = std::getenv("HO2D_SMOOTHER_BF16"); e && std::string(e) == "1") {
+        std::vector<uint16_t> h(op_.dinv.size());  // includes the zero padding past the end
+        for (size_t i = 0; i < h.size(); ++i) {
+            const float f = (float)op_.dinv[i];
+            uint32_t u;
+            std::memcpy(&u, &f, 4);
+            u += 0x7FFFu + ((u >> 16) & 1u);  // round to nearest, ties to even (finite values)
+            h[i] = (uint16_t)(u >> 16);
+        }
+        HO2D_CUDA(upload(d.dinv_bf16, h), "upload bf16 block-Jacobi");
+    }
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");
     d.have32 = true;
