@@ -135,8 +135,22 @@ Error add_boundary_arrays(Mesh& m, const std::string& name, int n, const int* id
 Error make_bases(int K, int L, Bases& B);
 void make_metrics(const Mesh& mesh, const Bases& B, Metrics& M);
 Error setup_bcs(const Input& in, const Mesh& mesh, const Bases& B, BoundaryConditions& bc);
+// Per-element data of the Kronecker-sum smoother (host_kron.cpp): the factors of each
+// element's fitted diagonal block, and the elements that keep the exact inverse block
+// (fit rejected, or ||I - M D||_2 > kKronDefectMax).
+constexpr double kKronDefectMax = 0.5;
+struct KronSmoother {
+    int K = 0;
+    std::vector<double> v;              // [N][4][K][K]: Vx, Vx^-1, Vy, Vy^-1
+    std::vector<double> lam;            // [N][2][K]: lx, ly
+    std::vector<unsigned char> exact;   // [N]: 1 = the exact inverse block is used
+    std::vector<double> defect;         // [N]: ||I - M D||_2 (infinity where rejected)
+};
+struct KronFit;
+void kron_store(const KronFit* f, double defect, int el, KronSmoother& ks);
+
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
-                      PoissonOperator& op, bool keep_blocks = false);
+                      PoissonOperator& op, bool keep_blocks = false, KronSmoother* kron = nullptr);
 int tensor2fem(int i, int j, int lnod_in);
 
 // Fields written by the VTK output: volume arrays [N][K][K] (vorticity, streamfunction,
@@ -188,6 +202,26 @@ class VtkQueue {
     std::thread thread_;
     Error err_{0, ""};
 };
+
+// Kronecker-sum approximation of an element's diagonal Poisson block (host_kron.cpp):
+// D ([ij][rs], K^2 x K^2) ~ I (x) Ax + Ay (x) I with Ax = Vx diag(lx) Vx^-1 and
+// Ay = Vy diag(ly) Vy^-1, all [K][K] row-major, eigenvectors as columns.
+struct KronFit {
+    int K = 0;
+    std::vector<double> vx, vxi, vy, vyi, lx, ly;
+};
+// Real eigenvalues of the n x n row-major A (false if a complex pair or no convergence).
+bool real_eigenvalues(int n, const double* A, double* lambda);
+// Eigenvectors for those eigenvalues as the columns of V (false if that fails).
+bool eigenvectors(int n, const double* A, const double* lambda, double* V);
+// Fit and factor; false when an eigenvalue is complex, a factor is singular or some
+// ly_j + lx_i vanishes (the exact inverse block is then the smoother's).
+bool kron_fit(int K, const double* D, KronFit& f);
+// z = (I (x) Ax + Ay (x) I)^-1 r for r, z [j][i]
+void kron_apply(const KronFit& f, const double* r, double* z);
+// ||I - M D||_2 of the fitted inverse M against the block it approximates (power
+// iteration: an estimate from below, to about 1e-3 relative)
+double kron_defect(const KronFit& f, const double* D);
 
 // Hybrid operation (host_hybrid.cpp): the edges of the "open" boundary (null if none), the
 // getopenpts_d array length, solution-point areas [N][K][K], open-boundary points

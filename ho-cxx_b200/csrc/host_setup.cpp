@@ -514,7 +514,7 @@ inline int bf_of(int side, int k, int K) { return (side / 2) * (K - 2 * k - 1) +
 }  // namespace
 
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
-                      PoissonOperator& op, bool keep_blocks) {
+                      PoissonOperator& op, bool keep_blocks, KronSmoother* kron) {
     const int N = mesh.n_el, K = B.K, K2 = K * K, K4 = K2 * K2;
     op.K2 = K2;
     op.blocks.assign(keep_blocks ? (size_t)N * 5 * K4 : 0, 0.0);
@@ -524,6 +524,13 @@ void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const 
     op.rowsum.assign((size_t)N * 5 * K2, 0.0);
     op.colsum.assign((size_t)N * 5 * K2, 0.0);
     op.bsum.assign((size_t)N * 5, 0.0);
+    if (kron) {
+        kron->K = K;
+        kron->v.assign((size_t)N * 4 * K * K, 0.0);
+        kron->lam.assign((size_t)N * 2 * K, 0.0);
+        kron->exact.assign(N, 1);
+        kron->defect.assign(N, 0.0);
+    }
     const std::vector<Entry> vol = volume_entries(B);
     std::vector<Entry> fw[2][2];
     for (int d = 0; d < 2; ++d)
@@ -659,6 +666,11 @@ void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const 
         nnz += store(Lc.data(), 0);
         for (int ijp = 0; ijp < 4; ++ijp)
             if (op.block_col[(size_t)el * 5 + 1 + ijp] >= 0) nnz += store(&Ln[(size_t)ijp * K4], 1 + ijp);
+        if (kron) {  // the Kronecker-sum fit of the filtered diagonal block ([ij][rs])
+            KronFit f;
+            const bool ok = kron_fit(K, Dm.data(), f);
+            kron_store(ok ? &f : nullptr, ok ? kron_defect(f, Dm.data()) : 0.0, el, *kron);
+        }
         // inverse of the filtered diagonal block, stored transposed like the blocks
         invert(K2, Dm);
         double* di = &op.dinv[(size_t)el * K4];

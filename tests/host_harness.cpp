@@ -271,3 +271,42 @@ extern "C" void case_split_open(void* h, const double* xyvel, double* vn, double
     const Case* c = static_cast<Case*>(h);
     ho2d::split_open_velocities(c->m, c->in.knod, c->nrm, xyvel, vn, vp);
 }
+
+// ---- Kronecker-sum smoother pieces (host_kron.cpp)
+
+extern "C" int kron_eigs(int n, const double* A, double* lam) { return ho2d::real_eigenvalues(n, A, lam) ? 1 : 0; }
+
+extern "C" int kron_vecs(int n, const double* A, const double* lam, double* V) {
+    return ho2d::eigenvectors(n, A, lam, V) ? 1 : 0;
+}
+
+// The fit of element el's diagonal block (from the kept blocks): applies the fitted inverse
+// to r ([j][i]) into z and returns ||I - M D||_2 in *defect; returns 1, or 0 if rejected.
+extern "C" int case_kron(void* h, int el, const double* r, double* z, double* defect) {
+    const Case* c = static_cast<Case*>(h);
+    const int K2 = c->op.K2, K = c->in.knod;
+    const double* blk = &c->op.blocks[(size_t)el * 5 * K2 * K2];  // slot 0, [rs][ij]
+    std::vector<double> D((size_t)K2 * K2);
+    for (int ij = 0; ij < K2; ++ij)
+        for (int rs = 0; rs < K2; ++rs) D[(size_t)ij * K2 + rs] = blk[(size_t)rs * K2 + ij];
+    ho2d::KronFit f;
+    if (!ho2d::kron_fit(K, D.data(), f)) return 0;
+    ho2d::kron_apply(f, r, z);
+    *defect = ho2d::kron_defect(f, D.data());
+    return 1;
+}
+
+// assemble_poisson again with the Kronecker-sum smoother data; returns the number of
+// elements that keep the exact inverse block, and their defects in defect[N] if not null
+extern "C" long case_kron_smoother(void* h, double* defect) {
+    Case* c = static_cast<Case*>(h);
+    ho2d::PoissonOperator op;
+    ho2d::KronSmoother ks;
+    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, op, false, &ks);
+    long n = 0;
+    for (int el = 0; el < c->m.n_el; ++el) {
+        n += ks.exact[el];
+        if (defect) defect[el] = ks.defect[el];
+    }
+    return n;
+}

@@ -65,7 +65,7 @@ def vtk_harness(tmp_path_factory):
     out = str(tmp_path_factory.mktemp("vtk_harness") / "libvtk_harness.so")
     srcs = [os.path.join(REPO, "tests", "vtk_harness.cpp")] + [os.path.join(csrc, f) for f in
                                                                 ("output_host.cpp", "host_io.cpp", "host_setup.cpp",
-                                                                 "host_samples.cpp")]
+                                                                 "host_samples.cpp", "host_kron.cpp")]
     subprocess.run(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-I", csrc, "-I", os.path.join(REPO, "include"),
                     *srcs, "-o", out], check=True, capture_output=True, text=True)
     lib = ctypes.CDLL(out)
