@@ -149,6 +149,10 @@ extern "C" long case_get(void* h, const char* name, double* out) {
     if (n == "R") return copy_out(B.R, out);
     if (n == "gR") return copy_out(B.gR, out);
     if (n == "J") return copy_out(M.J, out);
+    if (n == "xxi") return copy_out(M.xxi, out);
+    if (n == "xeta") return copy_out(M.xeta, out);
+    if (n == "yxi") return copy_out(M.yxi, out);
+    if (n == "yeta") return copy_out(M.yeta, out);
     if (n == "G") return copy_out(M.G, out);
     if (n == "GB") return copy_out(M.GB, out);
     if (n == "fA") return copy_out(M.fA, out);
@@ -309,4 +313,23 @@ extern "C" long case_kron_smoother(void* h, double* defect) {
         if (defect) defect[el] = ks.defect[el];
     }
     return n;
+}
+
+// make_bases(K, L) alone: the named table (xs, w, sbb, sbgb, D, R, gR, gsb, gsgb, gbb, gbgb,
+// gp) into out when not null; returns its length, or -code / -100 for an unknown name.
+extern "C" long bases_get(int K, int L, const char* name, double* out) {
+    ho2d::Bases B;
+    const ho2d::Error e = ho2d::make_bases(K, L, B);
+    if (e.code) return -e.code;
+    const std::string n = name;
+    const std::vector<double>* v = n == "xs" ? &B.xs : n == "w" ? &B.w : n == "sbb" ? &B.sbb : n == "sbgb" ? &B.sbgb
+                                 : n == "D" ? &B.D : n == "R" ? &B.R : n == "gR" ? &B.gR : n == "gsb" ? &B.gsb
+                                 : n == "gsgb" ? &B.gsgb : n == "gbb" ? &B.gbb : n == "gbgb" ? &B.gbgb : nullptr;
+    if (n == "gp") {
+        if (out) out[0] = B.gp[0], out[1] = B.gp[1];
+        return 2;
+    }
+    if (!v) return -100;
+    if (out) std::copy(v->begin(), v->end(), out);
+    return (long)v->size();
 }

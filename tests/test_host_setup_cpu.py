@@ -65,6 +65,8 @@ def lib(tmp_path_factory):
     L.case_kron.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.case_kron_smoother.restype = ctypes.c_long
     L.case_kron_smoother.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.bases_get.restype = ctypes.c_long
+    L.bases_get.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]
     return L
 
 
@@ -652,5 +654,110 @@ def test_kronecker_smoother_fallback_counts(lib, tmp_path, case, knod, expect):
         assert abs(n - expect) <= max(2, expect // 50), (n, expect)
         assert n == int((~(defect <= 0.5)).sum())
         assert np.median(defect[np.isfinite(defect)]) < 0.3
+    finally:
+        c.close()
+
+
+# ---- bases for every supported order (the reference stops at K = 5) ---------------------
+
+
+def _bases(lib, K, L, name):
+    n = lib.bases_get(K, L, name.encode(), None)
+    assert n > 0, (K, L, name, n)
+    out = np.zeros(n)
+    lib.bases_get(K, L, name.encode(), _p(out))
+    return out
+
+
+@pytest.mark.parametrize("K", range(1, 9))
+def test_solution_bases_against_legendre(lib, K):
+    """Gauss-Legendre points and weights (numpy's leggauss); Lagrange basis at the ends
+    (partition of unity, exact for degree < K); D exact on polynomials of degree < K;
+    the Radau corrections g_L = (-1)^K/2 (P_K - P_{K-1}) and g_R(x) = g_L(-x) with their
+    derivatives at the points; and the constants g'(-1), g'(+1) = -K(K+1)/2, +K(K+1)/2 of
+    the method-2 diffusion flux (src/HO_2D.cpp:548-549; not g_L's own end slope, which is
+    -K^2/2)."""
+    from numpy.polynomial import legendre as Lg
+
+    xs, w = _bases(lib, K, 2, "xs"), _bases(lib, K, 2, "w")
+    gx, gw = Lg.leggauss(K)
+    np.testing.assert_allclose(xs, gx, atol=1e-15 * K)
+    np.testing.assert_allclose(w, gw, atol=1e-14)
+    assert abs(w.sum() - 2.0) < 1e-14
+    sbb, sbgb = _bases(lib, K, 2, "sbb").reshape(K, 2), _bases(lib, K, 2, "sbgb").reshape(K, 2)
+    D = _bases(lib, K, 2, "D").reshape(K, K)  # D[k][m] = l_k'(x_m)
+    np.testing.assert_allclose(sbb.sum(axis=0), 1.0, atol=1e-13)
+    for deg in range(K):
+        p = np.polynomial.Polynomial.basis(deg)
+        vals = p(xs)
+        np.testing.assert_allclose(vals @ sbb, p(np.array([-1.0, 1.0])), atol=1e-12 * 4 ** K)
+        np.testing.assert_allclose(vals @ sbgb, p.deriv()(np.array([-1.0, 1.0])), atol=1e-11 * 4 ** K)
+        np.testing.assert_allclose(vals @ D, p.deriv()(xs), atol=1e-11 * 4 ** K)
+    R, gR = _bases(lib, K, 2, "R").reshape(K, 2), _bases(lib, K, 2, "gR").reshape(K, 2)
+    cK = np.zeros(K + 1)
+    cK[K] = 1.0
+    cK1 = np.zeros(K + 1)
+    cK1[K - 1] = 1.0
+    gL = 0.5 * (-1) ** K * (cK - cK1)
+    gLd = Lg.legder(gL)
+    assert abs(Lg.legval(-1.0, gL) - 1.0) < 1e-14 and abs(Lg.legval(1.0, gL)) < 1e-14
+    np.testing.assert_allclose(R[:, 0], Lg.legval(xs, gL), atol=1e-13)
+    np.testing.assert_allclose(R[:, 1], Lg.legval(-xs, gL), atol=1e-13)
+    np.testing.assert_allclose(gR[:, 0], Lg.legval(xs, gLd), atol=1e-11 * K * K)
+    np.testing.assert_allclose(gR[:, 1], -Lg.legval(-xs, gLd), atol=1e-11 * K * K)
+    gp = _bases(lib, K, 2, "gp")
+    np.testing.assert_allclose(gp, [-K * (K + 1) / 2, K * (K + 1) / 2], rtol=1e-15)
+    np.testing.assert_allclose(Lg.legval(-1.0, gLd), -K * K / 2, rtol=1e-12)
+
+
+@pytest.mark.parametrize("L", [2, 3, 4])
+def test_geometry_bases(lib, L):
+    """Equispaced Lagrange basis of the L geometry nodes at the solution points and at the
+    ends: partition of unity, exact for degree < L, derivatives likewise."""
+    K = 5
+    xs = _bases(lib, K, L, "xs")
+    gsb, gsgb = _bases(lib, K, L, "gsb").reshape(L, K), _bases(lib, K, L, "gsgb").reshape(L, K)
+    gbb, gbgb = _bases(lib, K, L, "gbb").reshape(L, 2), _bases(lib, K, L, "gbgb").reshape(L, 2)
+    nodes = np.linspace(-1.0, 1.0, L)
+    ends = np.array([-1.0, 1.0])
+    for deg in range(L):
+        p = np.polynomial.Polynomial.basis(deg)
+        np.testing.assert_allclose(p(nodes) @ gsb, p(xs), atol=1e-13)
+        np.testing.assert_allclose(p(nodes) @ gsgb, p.deriv()(xs), atol=1e-12)
+        np.testing.assert_allclose(p(nodes) @ gbb, p(ends), atol=1e-13)
+        np.testing.assert_allclose(p(nodes) @ gbgb, p.deriv()(ends), atol=1e-12)
+
+
+def test_bases_reject_unsupported_orders(lib):
+    assert lib.bases_get(0, 2, b"xs", None) < 0
+    assert lib.bases_get(9, 2, b"xs", None) < 0
+
+
+def test_affine_metrics_are_constant(lib, tmp_path):
+    """A mesh of equal parallelograms (the unit cavity sheared by x += 0.3 y, 3 x 3 cells):
+    x_xi = h/2, y_xi = 0, x_eta = 0.3 h/2, y_eta = h/2, J = h^2/4 at every solution point,
+    and every face Jacobian |g| is the half-length of its edge."""
+    from ho2d import meshgen
+
+    n, h = 3, 1.0 / 3
+    m = meshgen.cavity(n)
+    m.xy = m.xy.copy()
+    m.xy[:, 0] += 0.3 * m.xy[:, 1]
+    meshgen.write_msh(m, str(tmp_path / "mesh.msh"))
+    meshgen.write_input_dat(str(tmp_path / "input.dat"), "mesh.msh", knod=4, reyn=100.0, dt=1e-3, num_steps=1,
+                            problem_type=1)
+    code = ctypes.c_int(0)
+    hd = lib.case_from_input(str(tmp_path / "input.dat").encode(), ctypes.byref(code))
+    assert hd, code.value
+    c = HostCase(lib, hd)
+    try:
+        np.testing.assert_allclose(c["J"], h * h / 4, rtol=1e-13)
+        for name, val in (("xxi", h / 2), ("yxi", 0.0), ("xeta", 0.3 * h / 2), ("yeta", h / 2)):
+            np.testing.assert_allclose(c[name], val, atol=1e-14, err_msg=name)
+        fAn = c["fAn"].reshape(c.N, 4, c.K)  # ijp 0, 1: W/E faces (along eta); 2, 3: S/N (along xi)
+        np.testing.assert_allclose(fAn[:, :2], np.hypot(0.3, 1.0) * h / 2, rtol=1e-13)
+        np.testing.assert_allclose(fAn[:, 2:], h / 2, rtol=1e-13)
+        G = c["G"].reshape(c.N, c.K, c.K, 2, 2)  # (g_r . g_s) / J, constant
+        np.testing.assert_allclose(G - G[:1, :1, :1], 0.0, atol=1e-12)
     finally:
         c.close()
