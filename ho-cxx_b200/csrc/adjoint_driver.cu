@@ -222,6 +222,7 @@ Error Solver::kt_run(T* x, const T* b, bool f32, double tol, int& iters) {
 // mu = A^-T rhs (FP64 vectors): FP64 BiCGSTAB, or with a mixed-precision Krylov mode FP32
 // BiCGSTAB inside FP64 iterative refinement on the FP64 transposed residual.
 Error Solver::transposed_solve(const double* rhs, double* mu) {
+    const NvtxRange nvtx_range("ho2d.poisson_transpose");
     DeviceState& d = *d_;
     AdjointState& a = *adj_;
     const int N = mesh_.n_el, K = in_.knod;
@@ -384,6 +385,7 @@ Error Solver::load_state(double* dst, const void* src) {
 }
 
 Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
+    const NvtxRange nvtx_range("ho2d.adjoint_forward");
     HO2D_TRY(adjoint_supported(in_, stage32_));
     if (nsteps < 0 || ckpt_every < 1) return {1, "adjoint_forward needs nsteps >= 0 and ckpt_every >= 1"};
     HO2D_TRY(adjoint_prepare());
@@ -420,6 +422,7 @@ Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
 }
 
 Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* grad_pv) {
+    const NvtxRange nvtx_range("ho2d.adjoint_backward");
     HO2D_TRY(adjoint_supported(in_, stage32_));
     if (!adj_ || adj_->nsteps < 0) return {1, "ho2d_adjoint_backward needs a completed ho2d_adjoint_forward"};
     HO2D_TRY(adjoint_prepare());

@@ -55,6 +55,7 @@ Error Solver::vtk_job(int indx, int subidx, const std::string& dir, VtkQueue::Jo
 
 // trigger_write: the files are complete on return (after any dump still being written)
 Error Solver::write_vtk(int indx, int subidx, const std::string& dir) {
+    const NvtxRange nvtx_range("ho2d.write_vtk");
     if (!setup_done_) return {1, "not set up"};
     HO2D_TRY(vtk_queue_.wait());
     VtkQueue::Job j;
@@ -66,6 +67,7 @@ Error Solver::write_vtk(int indx, int subidx, const std::string& dir) {
 
 // a dump of the time loop: written on the queue's thread while the loop goes on
 Error Solver::queue_vtk(int indx, const std::string& dir) {
+    const NvtxRange nvtx_range("ho2d.queue_vtk");
     VtkQueue::Job j;
     HO2D_TRY(vtk_job(indx, -1, dir, j));
     return vtk_queue_.submit(mesh_, B_, &samples_, std::move(j));

@@ -68,6 +68,7 @@ Error Solver::read_input(const std::string& path) {
 }
 
 Error Solver::setup() {
+    const NvtxRange nvtx_range("ho2d.setup");
     if (!input_done_) return {1, "ho2d_setup called before ho2d_read_input"};
     vtk_queue_.wait();  // a dump still being written reads the mesh replaced here
     std::string mesh_path = in_.mesh_file;
@@ -485,6 +486,7 @@ Error Solver::set_precision(int mode) {
 
 // ------------------------------------------------------------------ Poisson
 Error Solver::poisson_solve() {
+    const NvtxRange nvtx_range("ho2d.poisson");
     DeviceState& d = *d_;
     const int N = mesh_.n_el, K = in_.knod;
     const size_t nv = (size_t)N * K * K;
@@ -647,6 +649,7 @@ Error Solver::update_bcs(double t, bool into_stage) {
 // stage's fields this way).
 template <typename T>
 Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
+    const NvtxRange nvtx_range("ho2d.stage");
     DeviceState& d = *d_;
     const int N = mesh_.n_el, K = in_.knod;
     const size_t nv = (size_t)N * K * K;
@@ -730,6 +733,7 @@ Error Solver::stage_impl(double coeff, int rk_stage, bool update) {
 }
 
 Error Solver::step(int nsteps) {
+    const NvtxRange nvtx_range("ho2d.step");
     if (!setup_done_) return {1, "ho2d_step called before ho2d_setup"};
     if (nsteps < 0) return {1, "nsteps must be non-negative"};
     HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
@@ -791,6 +795,7 @@ Error Solver::stage(double coeff) {
 }
 
 Error Solver::solve() {
+    const NvtxRange nvtx_range("ho2d.solve");
     if (!setup_done_) return {1, "ho2d_solve called before ho2d_setup"};
     HO2D_CUDA(cudaSetDevice(d_->device), "cudaSetDevice");
     const int nt = in_.num_steps, df = std::max(1, in_.dump_freq);

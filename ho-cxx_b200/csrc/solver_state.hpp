@@ -9,12 +9,24 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "device.cuh"
 #include "fr_launch.hpp"
 #include "host_amg.hpp"
 #include "solver.hpp"
 
 namespace ho2d {
+
+// A named NVTX range for the lifetime of a scope: setup, steps, stages, Poisson solves,
+// adjoint sweeps and VTK dumps show up by name in a profiler's timeline (ncu --nvtx
+// --nvtx-include); without an attached tool each push and pop is a cheap no-op.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Device copy of one row-padded matrix (FP64 and FP32 values) and of one coarse level.
 struct EllBufs {
