@@ -274,6 +274,13 @@ def _hybrid_arrays(name):
 
 
 def _hybrid_case(lib, spec, a):
+    h, code = _from_arrays(lib, spec, a)
+    assert h, f"hybrid setup failed with code {code}"
+    return HostCase(lib, h)
+
+
+def _from_arrays(lib, spec, a):
+    """case_from_arrays on a driver's arrays: (handle or None, status code)."""
     i32, f64 = np.int32, np.float64
 
     def arr(key, dt):
@@ -299,8 +306,7 @@ def _hybrid_case(lib, spec, a):
     h = lib.case_from_arrays(ci(int(spec["knod"])), ci(int(spec["iorder"])), ci(nxy), ptr(xy), ci(nidx), ptr(el),
                              ci(nw), ptr(wall), ci(no), ptr(opn), ci(niv), ptr(inv), ci(ni), ptr(inl), ci(nov),
                              ptr(outv), ci(nout), ptr(outl), ctypes.byref(code))
-    assert h, f"hybrid setup failed with code {code.value}"
-    return HostCase(lib, h)
+    return h, code.value
 
 
 @pytest.fixture(scope="module", params=HYB_CASES)
@@ -759,5 +765,47 @@ def test_affine_metrics_are_constant(lib, tmp_path):
         np.testing.assert_allclose(fAn[:, 2:], h / 2, rtol=1e-13)
         G = c["G"].reshape(c.N, c.K, c.K, 2, 2)  # (g_r . g_s) / J, constant
         np.testing.assert_allclose(G - G[:1, :1, :1], 0.0, atol=1e-12)
+    finally:
+        c.close()
+
+
+# ---- host-side fault injection: malformed meshes from a driver's arrays ------------------
+
+_XY = [[0, 0], [1, 0], [2, 0], [0, 1], [1, 1], [2, 1]]
+_QUADS = [[0, 1, 4, 3], [1, 2, 5, 4]]
+_WALL = [[0, 1], [1, 2], [2, 5], [5, 4], [4, 3], [3, 0]]
+
+
+def _arrays_case(lib, xy, quads, wall):
+    spec = {"knod": 3, "iorder": 1}
+    a = {"nodes": np.asarray(xy, float).ravel(), "elems": np.asarray(quads, np.int32).ravel(),
+         "wall": np.asarray(wall, np.int32).ravel()}
+    h, code = _from_arrays(lib, spec, a)
+    return (HostCase(lib, h) if h else None), code
+
+
+@pytest.mark.parametrize("what,xy,quads,wall", [
+    ("an element side no boundary edge covers", _XY, _QUADS, _WALL[:-1]),
+    ("a boundary edge inside the mesh", _XY, _QUADS, _WALL + [[1, 4]]),
+    ("a boundary edge on no element", _XY, _QUADS, _WALL + [[0, 5]]),
+    ("an edge shared by three elements", _XY + [[1, 2]], _QUADS + [[4, 1, 6, 6]], _WALL),
+    ("a quad with a repeated node", _XY, [[0, 1, 4, 4], [1, 2, 5, 4]], _WALL),
+    ("a boundary edge given twice", _XY, _QUADS, _WALL + [[0, 1]]),
+])
+def test_malformed_mesh_arrays_are_rejected(lib, what, xy, quads, wall):
+    """process_mesh returns the malformed-mesh code (3) instead of building tables whose
+    indices the kernels would follow."""
+    c, code = _arrays_case(lib, xy, quads, wall)
+    assert c is None and code == 3, what
+
+
+def test_clockwise_quad_has_negative_jacobian(lib):
+    """A clockwise quad passes the mesh processing; its Jacobian is negative, which the
+    library's setup rejects (non-positive element Jacobian, code 3)."""
+    c, code = _arrays_case(lib, _XY, [[0, 3, 4, 1], [1, 2, 5, 4]], _WALL)
+    assert code == 0
+    try:
+        J = c["J"].reshape(2, -1)
+        assert (J[0] < 0).all() and (J[1] > 0).all()
     finally:
         c.close()
