@@ -146,25 +146,32 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.f.close()
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                smax = max(smax, float(p[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
+        with open(self.path) as f:
+            out = summarize_clocks(f)
         os.remove(self.path)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return out
+
+
+def summarize_clocks(lines):
+    """Median SM clock, the largest max clock and the throttle reasons seen Active in
+    nvidia-smi CSV rows of ClockSampler.FIELDS (noheader, nounits); None without samples."""
+    sm, smax, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in lines:
+        p = [x.strip() for x in line.split(",")]
+        if len(p) < 9:
+            continue
+        try:
+            sm.append(float(p[1]))
+            smax = max(smax, float(p[2]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, p[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def measured_peaks():

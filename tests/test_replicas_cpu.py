@@ -47,3 +47,20 @@ def test_single_process_needs_no_group():
     assert d.max(3.0) == 3.0 and d.sum(4.0) == 4.0
     d.barrier()
     d.close()
+
+
+def test_clock_summary():
+    """bench.py's clock record from nvidia-smi rows: the median SM clock under load, the
+    max clock, and only the throttle reasons reported Active ("Not Active" is not one)."""
+    import sys
+
+    sys.path.insert(0, REPO)
+    import bench
+
+    rows = ["0, 1965, 1965, 700.1 , 0x0000000000000000, Not Active, Not Active, Not Active, Not Active\n",
+            "0, 1800, 1965, 990.5 , 0x0000000000000004, Not Active, Not Active, Not Active, Active\n",
+            "0, 1900, 1965, 950.0 , 0x0000000000000004, Not Active, Not Active, Not Active, Active\n",
+            "[N/A], [N/A], [N/A], [N/A], [N/A], [N/A], [N/A], [N/A], [N/A]\n", "garbage\n"]
+    out = bench.summarize_clocks(rows)
+    assert out == {"sm_mhz": 1900.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    assert bench.summarize_clocks([]) is None
