@@ -86,6 +86,33 @@ def cavity(n: int, jitter: float = 0.0, seed: int | None = None) -> QuadMesh:
     return QuadMesh(xy, quads, bnd)
 
 
+def cavity_q2(n: int, amp: float = 0.04) -> QuadMesh:
+    """Unit-square cavity of n x n 9-node (quadratic) quads whose interior is bent by
+    (x, y) += amp sin(pi x) sin(2 pi y) (1, 0.5): curved interior edges, straight walls.
+    Nodes in Gmsh order per quad (corners SW, SE, NE, NW, the edge midpoints, the centre);
+    boundary edges as (end, end, midpoint)."""
+    m = 2 * n + 1
+    g = np.linspace(0.0, 1.0, m)
+    X, Y = np.meshgrid(g, g)  # [j][i]
+    b = amp * np.sin(np.pi * X) * np.sin(2 * np.pi * Y)
+    xy = np.stack([(X + b).ravel(), (Y + 0.5 * b).ravel()], -1)
+
+    def nid(i, j):
+        return j * m + i
+
+    quads = []
+    for j in range(n):
+        for i in range(n):
+            a, c = 2 * i, 2 * j
+            quads.append([nid(a, c), nid(a + 2, c), nid(a + 2, c + 2), nid(a, c + 2), nid(a + 1, c), nid(a + 2, c + 1),
+                          nid(a + 1, c + 2), nid(a, c + 1), nid(a + 1, c + 1)])
+    bnd = {"bottom_wall": [[nid(2 * i, 0), nid(2 * i + 2, 0), nid(2 * i + 1, 0)] for i in range(n)],
+           "right_wall": [[nid(m - 1, 2 * j), nid(m - 1, 2 * j + 2), nid(m - 1, 2 * j + 1)] for j in range(n)],
+           "top": [[nid(2 * i + 2, m - 1), nid(2 * i, m - 1), nid(2 * i + 1, m - 1)] for i in range(n)],
+           "left_wall": [[nid(0, 2 * j + 2), nid(0, 2 * j), nid(0, 2 * j + 1)] for j in range(n)]}
+    return QuadMesh(xy, np.array(quads), {k: np.array(v) for k, v in bnd.items()})
+
+
 def backward_facing_step(h: float = 1.0 / 15.0, jitter: float = 0.15, seed: int | None = 2,
                          x_in: float = -5.0, x_out: float = 30.0) -> QuadMesh:
     """Backward-facing step: step height 1, expansion ratio 2.
@@ -296,13 +323,19 @@ def make_case(name: str, outdir: str, knod: int | None = None, steps: int = 10, 
               **kw) -> str:
     """Write ``<outdir>/input.dat`` and its mesh for a named synthetic case; returns the input path.
 
-    Cases: ``cavity<N>`` (uniform N x N cavity, Re=100, K=4, dt=1e-3),
+    Cases: ``cavity<N>`` (uniform N x N cavity, Re=100, K=4, dt=1e-3), ``cavityq<N>``
+    (N x N curved 9-node quads, cavity_q2),
     ``cavityj<N>`` (jittered +/-0.1h), ``bfs`` (the 14,625-quad step, K=5, Re=400,
     CFL-0.5 dt), ``bfs<m>`` (step with h = 1/m), ``cyl<nr>x<nt>`` (O-grid, K=5, Re=100).
     The step is the smaller of the CFL and the viscous bound (cfl_dt, viscous_dt).
     """
     os.makedirs(outdir, exist_ok=True)
-    if name.startswith("cavityj"):
+    if name.startswith("cavityq"):
+        n = int(name[7:])
+        mesh = cavity_q2(n, amp=kw.get("amp", 0.04))
+        ptype, reyn, k = 1, kw.get("reyn", 100.0), knod or 4
+        dt = dt or 1e-3
+    elif name.startswith("cavityj"):
         n = int(name[7:])
         mesh = cavity(n, jitter=kw.get("jitter", 0.1), seed=kw.get("seed", 5))
         ptype, reyn, k = 1, kw.get("reyn", 100.0), knod or 4
@@ -329,5 +362,6 @@ def make_case(name: str, outdir: str, knod: int | None = None, steps: int = 10, 
     path = os.path.join(outdir, "input.dat")
     write_input_dat(path, "mesh.msh", k, reyn, dt, steps, ptype,
                     advection_type=kw.get("advection_type", 1),
-                    time_integration=kw.get("time_integration", 4))
+                    time_integration=kw.get("time_integration", 4),
+                    lnod_in=2 if mesh.quads.shape[1] == 9 else 1)
     return path

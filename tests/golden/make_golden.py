@@ -11,7 +11,8 @@ solution) and stores, in ref.npz:
 * one stage (Euler_time_integrate) from a seeded random vorticity field;
 * a short trajectory (vorticity and psi after each step).
 
-usage: python tests/golden/make_golden.py [--check-shipped]
+usage: python tests/golden/make_golden.py [--check-shipped] [case ...]
+  case names restrict the run to those cases (default: all).
   --check-shipped additionally runs the oracle against the reference on the meshes
   shipped in the reference's input/ directory and prints the largest differences.
 """
@@ -43,6 +44,7 @@ CASES = {
     "cyl4x8_rk4": ("cyl4x8", {}, 5, 3),
     "cyl4x8_rk2_adv2": ("cyl4x8", {"time_integration": 2, "advection_type": 2}, 5, 3),
     "bfs2_rk4": ("bfs2", {"x_out": 6.0}, 5, 3),
+    "cavq3_rk4": ("cavityq3", {}, 4, 3),  # curved 9-node quads (input Lnod 2)
 }
 SEED = 7
 SETUP_ARRAYS = ["A_ptr", "A_col", "A_val", "boundary_source", "vol_jac", "G", "GB", "face_Acoef", "face_Bcoef",
@@ -122,7 +124,8 @@ def check_shipped() -> None:
 if __name__ == "__main__":
     if not os.path.exists(REF):
         sys.exit("oracle/_ref/ho2d_ref is missing: run `make -C oracle` first")
-    for nm in CASES:
+    names = [a for a in sys.argv[1:] if not a.startswith("--")] or list(CASES)
+    for nm in names:
         make_case(nm)
     if "--check-shipped" in sys.argv:
         check_shipped()

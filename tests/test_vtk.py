@@ -115,27 +115,9 @@ def test_vtk_writer_reproduces_reference_files(tmp_path, vtk_harness, case):
 
 
 def q2_cavity(n=3, amp=0.04):
-    """Unit-square cavity of n x n 9-node quads whose interior is bent by
-    (x, y) += amp sin(pi x) sin(2 pi y) (1, 0.5): curved interior edges, straight walls."""
     from ho2d import meshgen
 
-    m = 2 * n + 1
-    g = np.linspace(0.0, 1.0, m)
-    X, Y = np.meshgrid(g, g)  # [j][i]
-    b = amp * np.sin(np.pi * X) * np.sin(2 * np.pi * Y)
-    xy = np.stack([(X + b).ravel(), (Y + 0.5 * b).ravel()], -1)
-    nid = lambda i, j: j * m + i  # noqa: E731
-    quads = []
-    for j in range(n):
-        for i in range(n):
-            a, c = 2 * i, 2 * j
-            quads.append([nid(a, c), nid(a + 2, c), nid(a + 2, c + 2), nid(a, c + 2), nid(a + 1, c), nid(a + 2, c + 1),
-                          nid(a + 1, c + 2), nid(a, c + 1), nid(a + 1, c + 1)])
-    bnd = {"bottom_wall": [[nid(2 * i, 0), nid(2 * i + 2, 0), nid(2 * i + 1, 0)] for i in range(n)],
-           "right_wall": [[nid(m - 1, 2 * j), nid(m - 1, 2 * j + 2), nid(m - 1, 2 * j + 1)] for j in range(n)],
-           "top": [[nid(2 * i + 2, m - 1), nid(2 * i, m - 1), nid(2 * i + 1, m - 1)] for i in range(n)],
-           "left_wall": [[nid(0, 2 * j + 2), nid(0, 2 * j), nid(0, 2 * j + 1)] for j in range(n)]}
-    return meshgen.QuadMesh(xy, np.array(quads), {k: np.array(v) for k, v in bnd.items()})
+    return meshgen.cavity_q2(n, amp)
 
 
 def msh_nodes(path):
