@@ -809,3 +809,54 @@ def test_clockwise_quad_has_negative_jacobian(lib):
         assert (J[0] < 0).all() and (J[1] > 0).all()
     finally:
         c.close()
+
+
+# ---- the reference's own shipped meshes (read where they lie; skipped without them) -----
+
+REFERENCE_INPUT = "/root/reference/input"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
+
+
+@pytest.mark.parametrize("dat", ["input_cavity.dat", "input_bfs.dat", "input_cylinder.dat"])
+def test_host_setup_on_shipped_meshes(lib, tmp_path, dat):
+    """The reference's shipped inputs (quadratic cavity and step meshes, the OCC-oriented
+    cylinder at K = 3): the library's host setup against the reference's own setup dump
+    (oracle/_ref/ho2d_ref --setup) of the same files."""
+    if not (os.path.isdir(REFERENCE_INPUT) and os.path.exists(REF_BIN)):
+        pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")
+    lines = open(os.path.join(REFERENCE_INPUT, dat)).read().split("\n")
+    shutil.copy(os.path.join(REFERENCE_INPUT, lines[7].strip()), tmp_path)
+    lines[27] = "1"  # one time step: only the setup is compared
+    inp = tmp_path / "input.dat"
+    inp.write_text("\n".join(lines))
+    env = dict(os.environ, HO_SHIM_SOLVER="direct")
+    subprocess.run([REF_BIN, str(inp), str(tmp_path / "ref"), "--setup"], check=True, env=env,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=600)
+    ref = {f[:-4]: np.load(tmp_path / "ref" / f) for f in os.listdir(tmp_path / "ref") if f.endswith(".npy")}
+    meta = json.load(open(tmp_path / "ref" / "meta.json"))
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(str(inp).encode(), ctypes.byref(code))
+    assert h, code.value
+    c = HostCase(lib, h)
+    try:
+        assert (c.N, c.K, c.L, c.neb) == (meta["N_el"], meta["Knod"], meta["Lnod"], meta["N_edges_boundary"])
+        assert c.groups == meta["boundaries"]
+        for mine, nm in [("nbr", "elem_neighbor"), ("nbr_side", "elem_neighbor_side"),
+                         ("bidx", "elem_boundary_index"), ("be_el", "bedge_element"), ("be_side", "bedge_side"),
+                         ("sw_p", "BC_switch_Poisson"), ("sw_d", "BC_switch_diffusion")]:
+            np.testing.assert_array_equal(c.ints(mine), ref[nm].ravel(), err_msg=nm)
+        for mine, nm in [("J", "vol_jac"), ("G", "G"), ("GB", "GB"), ("fJ", "face_jac"), ("fA", "face_Acoef"),
+                         ("fAn", "face_Anorm")]:
+            assert rel(c[mine], ref[nm]) < TOL, nm
+        assert np.abs(c["fB"] - ref["face_Bcoef"].ravel()).max() <= TOL * np.abs(ref["face_Acoef"]).max()
+        for mine, nm in [("bc_p", "BC_Poisson"), ("bc_nv", "BC_normal_vel"), ("bc_pv", "BC_parl_vel"),
+                         ("bc_d", "BC_diffusion")]:
+            assert close_abs(c[mine], ref[nm]), nm
+        n = c.N * c.K ** 2
+        A = sp.csr_matrix((ref["A_val"], ref["A_col"], ref["A_ptr"][: n + 1]), shape=(n, n))
+        mine = blocks_to_csr(c)
+        assert c.nnz == A.nnz == mine.nnz
+        assert abs(mine - A).max() <= 1e-12 * abs(A).max()
+        assert rel(c["bsrc"], ref["boundary_source"]) < 1e-12
+    finally:
+        c.close()
