@@ -218,3 +218,37 @@ def test_vtk_files_match_reference(tmp_path, case):
     assert sorted(os.listdir(ours)) == ref_files
     for f in ref_files:
         compare_vtk(str(ours / f), str(d / f))
+
+
+def test_sample_points_of_the_shipped_cavity(tmp_path, vtk_harness):
+    """The reference's shipped cavity input with its own sample-points file
+    (input/sample_points.dat, points on the centrelines; read where they lie, skipped
+    without them), two time steps: the library's writer reproduces the reference's
+    sampling_points file from the fields the reference wrote it from."""
+    src = "/root/reference/input"
+    if not (os.path.isdir(src) and os.path.exists(REF)):
+        pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")
+    d = tmp_path / "case"
+    d.mkdir()
+    lines = open(os.path.join(src, "input_cavity.dat")).read().split("\n")
+    for f in (lines[7].strip(), "sample_points.dat"):
+        shutil.copy(os.path.join(src, f), d)
+    lines[27], lines[31] = "2", "2"  # two steps, files at steps 0 and 2
+    open(d / "input.dat", "w").write("\n".join(lines))
+    env = dict(os.environ, HO_SHIM_SOLVER="direct")
+    subprocess.run([REF, str(d / "input.dat"), str(tmp_path / "fields"), "--solve", "--samples"], check=True, env=env,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=600)
+    f = {k: np.load(tmp_path / "fields" / f"solve_{k}.npy") for k in
+         ("vorticity", "psi", "vel", "rhs_diff", "rhs_adv", "bc_w", "bc_nv", "bc_pv")}
+    knod, ptype = int(lines[3]), int(lines[25])
+    ours = tmp_path / "ours"
+    ours.mkdir()
+    rc = vtk_harness.write_vtk_host(str(d / lines[7].strip()).encode(), int(lines[9]), knod, ptype,
+                                    _dp(f["vorticity"]), _dp(f["psi"]), _dp(f["vel"][..., 0]), _dp(f["vel"][..., 1]),
+                                    _dp(f["rhs_diff"]), _dp(f["rhs_adv"]), _dp(f["bc_w"]), _dp(f["bc_nv"]),
+                                    _dp(f["bc_pv"]), 2, -1, str(ours).encode(), str(d / "sample_points.dat").encode())
+    assert rc == 0
+    names = [n for n in os.listdir(d) if n.startswith("sampling_points") and n.endswith("_00002.dat")]
+    assert len(names) == 1, os.listdir(d)
+    compare_vtk(str(ours / names[0]), str(d / names[0]))
+    assert len(open(ours / names[0]).read().split()) == 5 * 14  # 14 points, 5 values each
