@@ -73,7 +73,7 @@ def vtk_harness(tmp_path_factory):
     return lib
 
 
-@pytest.mark.parametrize("case", ["cav4_rk4", "cav4_euler_k3", "bfs2_rk4", "cyl4x8_rk4"])
+@pytest.mark.parametrize("case", ["cav4_rk4", "cav4_euler_k3", "bfs2_rk4", "cyl4x8_rk4", "cavq3_rk4"])
 def test_vtk_writer_reproduces_reference_files(tmp_path, vtk_harness, case):
     """The library's writer, given the fields the reference wrote its last files from,
     writes the same files (host build; the reference run on the CPU)."""
@@ -221,10 +221,11 @@ def test_vtk_files_match_reference(tmp_path, case):
 
 
 def test_sample_points_of_the_shipped_cavity(tmp_path, vtk_harness):
-    """The reference's shipped cavity input with its own sample-points file
-    (input/sample_points.dat, points on the centrelines; read where they lie, skipped
-    without them), two time steps: the library's writer reproduces the reference's
-    sampling_points file from the fields the reference wrote it from."""
+    """The reference's shipped cavity input (2,895 quadratic quads) with its own
+    sample-points file (input/sample_points.dat, points on the centrelines; read where they
+    lie, skipped without them), two time steps: the library's writer reproduces the
+    reference's sampling_points file and both VTK files from the fields the reference wrote
+    them from."""
     src = "/root/reference/input"
     if not (os.path.isdir(src) and os.path.exists(REF)):
         pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")
@@ -252,3 +253,5 @@ def test_sample_points_of_the_shipped_cavity(tmp_path, vtk_harness):
     assert len(names) == 1, os.listdir(d)
     compare_vtk(str(ours / names[0]), str(d / names[0]))
     assert len(open(ours / names[0]).read().split()) == 5 * 14  # 14 points, 5 values each
+    for vtk in (f"problem{ptype}_K{knod}_00002.vtk", f"vorticity{ptype}_K{knod}_00002.vtk"):  # 9-node quads
+        compare_vtk(str(ours / vtk), str(d / vtk))
