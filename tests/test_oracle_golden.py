@@ -90,3 +90,33 @@ def test_trajectory(golden):
         c.step()
         assert rel(c.omega, ref[f"traj_vort_{s}"]) < TOL, s
         assert rel(c.psi, ref[f"traj_psi_{s}"]) < TOL, s
+
+
+@pytest.mark.parametrize("dat", ["input_cavity.dat", "input_bfs.dat", "input_cylinder.dat"])
+def test_oracle_on_shipped_meshes(tmp_path, dat):
+    """The reference's own fixtures (input/: quadratic cavity and step, OCC cylinder, K = 3;
+    read where they lie, skipped without them): two time steps of the oracle against the
+    reference's run (oracle/_ref/ho2d_ref, direct Poisson solve) from the same seeded
+    vorticity."""
+    import shutil
+    import subprocess
+
+    from conftest import REPO
+
+    src = "/root/reference/input"
+    ref_bin = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
+    if not (os.path.isdir(src) and os.path.exists(ref_bin)):
+        pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")
+    lines = open(os.path.join(src, dat)).read().split("\n")
+    shutil.copy(os.path.join(src, lines[7].strip()), tmp_path)
+    lines[27] = "2"
+    inp = str(tmp_path / "input.dat")
+    open(inp, "w").write("\n".join(lines))
+    c = O.Case(inp)
+    w0 = np.random.Generator(np.random.PCG64(7)).standard_normal((c.N, c.K, c.K))
+    np.save(tmp_path / "w0.npy", w0)
+    subprocess.run([ref_bin, inp, str(tmp_path / "o"), "--init-vort", str(tmp_path / "w0.npy"), "--steps", "2"],
+                   check=True, env=dict(os.environ, HO_SHIM_SOLVER="direct"), stdout=subprocess.DEVNULL, timeout=600)
+    c.omega = w0
+    c.run(2)
+    assert rel(c.omega, np.load(tmp_path / "o" / "traj_vort_2.npy")) < TOL
