@@ -63,6 +63,9 @@ class HO_2D:
 
     allocate_arrays = setup_mesh
     setup_sps_gps = setup_mesh
+
+    def read_process_sample_points(self) -> None:
+        """Nothing to do: the setup reads the input's sample-points file."""
     form_bases = setup_mesh
     form_metrics = setup_mesh
     setup_IC_BC_SRC = setup_mesh
