@@ -66,6 +66,7 @@ class HO_2D:
 
     def read_process_sample_points(self) -> None:
         """Nothing to do: the setup reads the input's sample-points file."""
+
     form_bases = setup_mesh
     form_metrics = setup_mesh
     setup_IC_BC_SRC = setup_mesh
