@@ -63,6 +63,9 @@ def parse():
                          "Strouhal number, mean drag and lift amplitude in FP64 and mixed, and their differences")
     ap.add_argument("--t-end", type=float, default=80.0, help="time units simulated for --strouhal")
     ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
+    ap.add_argument("--l2-steps", type=int, default=0,
+                    help="also continue every precision mode to this many steps (outside the timed region) and "
+                         "report the relative vorticity L2 difference from FP64 there")
     return ap.parse_args()
 
 
@@ -321,6 +324,16 @@ def run_ours(args, rank, world, local, phys):
             pass
         w_f32 = solvers["mixed_fp32_stage"].get_vorticity()
         l2_f32 = float(np.linalg.norm(w_f32 - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
+        l2_long = None
+        done = args.warmup + args.steps
+        if args.l2_steps > done:  # the same steps in every mode, then the differences from FP64
+            for s_ in solvers.values():
+                s_.solve_advection_diffusion(args.l2_steps - done)
+            wf = solvers["fp64"].get_vorticity()
+            nf = max(np.linalg.norm(wf), 1e-300)
+            l2_long = {"steps": args.l2_steps,
+                       "mixed": float(np.linalg.norm(solvers["mixed"].get_vorticity() - wf) / nf),
+                       "mixed_fp32_stage": float(np.linalg.norm(solvers["mixed_fp32_stage"].get_vorticity() - wf) / nf)}
         # end to end through the public API with host buffers: H2D of the step's input
         # vorticity from pinned memory, the step, D2H of the resulting vorticity
         s = solvers["mixed"]
@@ -380,6 +393,7 @@ def run_ours(args, rank, world, local, phys):
                     "mixed_over_fp64": m["value"] / f["value"],
                     "l2_rel_vorticity_mixed_vs_fp64": l2,
                     "l2_after_steps": args.warmup + args.steps,
+                    "l2_rel_vorticity_vs_fp64_long": l2_long,
                     "body_force": forces,
                     "clocks": clocks, "e2e": e2e, "gpu_launches": m["launches"], "roofline": roofline,
                     "cpu_baseline": cb}
