@@ -149,3 +149,50 @@ def test_complex_step_matches_central_differences():
     km = CS.stage_forward_state(c, w - h * dw)["k"]
     fd = (kp - km) / (2 * h)
     assert np.linalg.norm(fd - dk) <= 1e-6 * np.linalg.norm(dk)
+
+
+_SANITIZED_RUN = """
+import ctypes, sys
+import numpy as np
+sys.path[:0] = sys.argv[2:]
+import test_adjoint_cpu as T
+H = ctypes.CDLL(sys.argv[1])
+for name in T.CASES + T.CASES_ADV2:
+    c = T.case_of(name)
+    g = T.Geom(c)
+    rng = np.random.default_rng(11)
+    w, lk = rng.standard_normal((c.N, c.K, c.K)), rng.standard_normal((c.N, c.K, c.K))
+    for coeff in (0.0, 0.5):
+        T.stage_adjoint(H, c, g, w, lk, coeff)
+    x = rng.standard_normal(c.N * c.K * c.K)
+    y = np.zeros_like(x)
+    assert H.poisson_transpose_host(*g.args(), T._p(x), T._p(y)) == 0
+print("clean")
+"""
+
+
+def test_element_bodies_under_sanitizers(tmp_path):
+    """The adjoint's element bodies (the source the device kernels are compiled from) under
+    AddressSanitizer and UBSan on every case of both advection schemes: the stage adjoint at
+    two stage coefficients and the transposed Poisson operator. Any report fails the run."""
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    import sys
+
+    so = str(tmp_path / "libadjoint_sanitized.so")
+    r = subprocess.run(["g++", "-O1", "-g", "-std=c++17", "-shared", "-fPIC", "-fsanitize=address,undefined",
+                        "-fno-omit-frame-pointer", "-I", _cuda_include(), "-I", CSRC,
+                        os.path.join(REPO, "tests", "adjoint_harness.cpp"), "-o", so], capture_output=True, text=True)
+    if r.returncode != 0 and "sanitize" in r.stderr:
+        pytest.skip("sanitizer runtimes not available")
+    assert r.returncode == 0, r.stderr[-2000:]
+    libs = [subprocess.run(["g++", f"-print-file-name={n}"], capture_output=True, text=True).stdout.strip()
+            for n in ("libasan.so", "libubsan.so")]
+    if not all(os.path.isabs(p) and os.path.exists(p) for p in libs):
+        pytest.skip("sanitizer runtimes not found")
+    env = dict(os.environ, LD_PRELOAD=":".join(libs), ASAN_OPTIONS="detect_leaks=0:halt_on_error=1",
+               UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
+    paths = [os.path.join(REPO, d) for d in ("tests", "oracle", "ho-cxx_b200")]
+    r = subprocess.run([sys.executable, "-c", _SANITIZED_RUN, so, *paths], capture_output=True, text=True, env=env,
+                       timeout=900)
+    assert r.returncode == 0 and "clean" in r.stdout and "runtime error" not in r.stderr, r.stderr[-3000:]
