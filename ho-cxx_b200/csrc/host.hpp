@@ -223,6 +223,16 @@ void kron_apply(const KronFit& f, const double* r, double* z);
 // iteration: an estimate from below, to about 1e-3 relative)
 double kron_defect(const KronFit& f, const double* D);
 
+// The BF16 bit pattern of a finite float, rounded to nearest with ties to even (the upper
+// 16 bits after adding 0x7FFF plus the lowest kept bit).
+inline uint16_t bf16_bits(float f) {
+    uint32_t u;
+    static_assert(sizeof(u) == sizeof(f), "float is 32 bits");
+    __builtin_memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
 // Hybrid operation (host_hybrid.cpp): the edges of the "open" boundary (null if none), the
 // getopenpts_d array length, solution-point areas [N][K][K], open-boundary points
 // [open edge][K][x, y], outward unit normals of the open edges [N_eb][K][2], and the

@@ -447,13 +447,7 @@ Error Solver::upload_precision_arrays() {
     // the bytes; the preconditioner's precision changes only the inner iteration count)
     if (const char* e = std::getenv("HO2D_SMOOTHER_BF16"); e && std::string(e) == "1") {
         std::vector<uint16_t> h(op_.dinv.size());  // includes the zero padding past the end
-        for (size_t i = 0; i < h.size(); ++i) {
-            const float f = (float)op_.dinv[i];
-            uint32_t u;
-            std::memcpy(&u, &f, 4);
-            u += 0x7FFFu + ((u >> 16) & 1u);  // round to nearest, ties to even (finite values)
-            h[i] = (uint16_t)(u >> 16);
-        }
+        for (size_t i = 0; i < h.size(); ++i) h[i] = bf16_bits((float)op_.dinv[i]);
         HO2D_CUDA(upload(d.dinv_bf16, h), "upload bf16 block-Jacobi");
     }
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");

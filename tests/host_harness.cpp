@@ -333,3 +333,8 @@ extern "C" long bases_get(int K, int L, const char* name, double* out) {
     if (out) std::copy(v->begin(), v->end(), out);
     return (long)v->size();
 }
+
+// bf16_bits over an array (the rounding of the optional BF16 smoother blocks)
+extern "C" void bf16_array(const float* x, uint16_t* out, int n) {
+    for (int i = 0; i < n; ++i) out[i] = ho2d::bf16_bits(x[i]);
+}

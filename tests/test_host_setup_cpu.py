@@ -891,3 +891,20 @@ def test_host_code_under_sanitizers(tmp_path):
     r = subprocess.run([exe, *args, str(out)], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0 and "runtime error" not in r.stderr and "Sanitizer" not in r.stderr, r.stderr[-3000:]
     assert r.stdout.count("vtk 0") == 4, r.stdout
+
+
+def test_bf16_rounding_matches_torch(lib):
+    """The rounding of the optional BF16 smoother blocks: round to nearest, ties to even,
+    bit for bit against torch's float32 -> bfloat16 conversion, on random values over the
+    whole finite range, exact ties, values one ulp either side of them, and subnormals."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.Generator(np.random.PCG64(12))
+    bits = rng.integers(0, 0x7F7FFFFF, 200000, dtype=np.uint32) | (rng.integers(0, 2, 200000, dtype=np.uint32) << 31)
+    ties = (rng.integers(0, 0x7F7F, 5000, dtype=np.uint32) << 16) | 0x8000
+    x = np.concatenate([bits, ties, ties + 1, ties - 1, np.arange(1, 5000, dtype=np.uint32)]).view(np.float32)
+    x = np.ascontiguousarray(x)
+    out = np.zeros(x.size, np.uint16)
+    lib.bf16_array.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.bf16_array(x.ctypes.data, out.ctypes.data, x.size)
+    ref = torch.from_numpy(x).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    np.testing.assert_array_equal(out, ref)
