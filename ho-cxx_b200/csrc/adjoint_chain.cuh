@@ -26,26 +26,9 @@
 #include <cmath>
 
 #include "device.cuh"
-
-#if defined(__CUDACC__)
-#define HO2D_HD __host__ __device__ __forceinline__
-#else
-#define HO2D_HD inline
-#endif
+#include "elem_ctx.cuh"
 
 namespace ho2d {
-
-// Threads of one element and their barrier.
-template <int NT>
-struct ElemCtx {
-    int tid;
-    static constexpr int nt = NT;
-    HO2D_HD void sync() const {
-#if defined(__CUDA_ARCH__)
-        __syncthreads();
-#endif
-    }
-};
 
 // Elements per CTA of the adjoint kernels: at most 128 threads, so that the per-element
 // scratch below stays inside the static shared-memory limit for every K <= 8.

@@ -10,6 +10,7 @@
 
 #include "host.hpp"
 #include "host_amg.hpp"
+#include "kron_apply.cuh"
 
 namespace {
 
@@ -337,4 +338,44 @@ extern "C" long bases_get(int K, int L, const char* name, double* out) {
 // bf16_bits over an array (the rounding of the optional BF16 smoother blocks)
 extern "C" void bf16_array(const float* x, uint16_t* out, int n) {
     for (int i = 0; i < n; ++i) out[i] = ho2d::bf16_bits(x[i]);
+}
+
+namespace {
+template <int K>
+void kron_body_k(const ho2d::KronFit& f, const double* r_in, double* z) {
+    constexpr int K2 = K * K;
+    double fac[4 * K2], lam[2 * K], r[K2], t[K2];
+    const std::vector<double>* m[4] = {&f.vx, &f.vxi, &f.vy, &f.vyi};
+    for (int a = 0; a < 4; ++a) std::copy(m[a]->begin(), m[a]->end(), fac + a * K2);
+    std::copy(f.lx.begin(), f.lx.end(), lam);
+    std::copy(f.ly.begin(), f.ly.end(), lam + K);
+    std::copy(r_in, r_in + K2, r);
+    const ho2d::ElemCtx<1> c{0};
+    ho2d::kron_apply_body<K, double>(c, true, fac, lam, r, t, z);
+}
+}  // namespace
+
+// The element body of the Kronecker-sum smoother (kron_apply.cuh, one thread) on element
+// el's fitted factors, applied to r into z; 0 if the fit is rejected.
+extern "C" int case_kron_body(void* h, int el, const double* r, double* z) {
+    const Case* c = static_cast<Case*>(h);
+    const int K2 = c->op.K2, K = c->in.knod;
+    const double* blk = &c->op.blocks[(size_t)el * 5 * K2 * K2];
+    std::vector<double> D((size_t)K2 * K2);
+    for (int ij = 0; ij < K2; ++ij)
+        for (int rs = 0; rs < K2; ++rs) D[(size_t)ij * K2 + rs] = blk[(size_t)rs * K2 + ij];
+    ho2d::KronFit f;
+    if (!ho2d::kron_fit(K, D.data(), f)) return 0;
+    switch (K) {
+        case 1: kron_body_k<1>(f, r, z); break;
+        case 2: kron_body_k<2>(f, r, z); break;
+        case 3: kron_body_k<3>(f, r, z); break;
+        case 4: kron_body_k<4>(f, r, z); break;
+        case 5: kron_body_k<5>(f, r, z); break;
+        case 6: kron_body_k<6>(f, r, z); break;
+        case 7: kron_body_k<7>(f, r, z); break;
+        case 8: kron_body_k<8>(f, r, z); break;
+        default: return 0;
+    }
+    return 1;
 }

@@ -908,3 +908,27 @@ def test_bf16_rounding_matches_torch(lib):
     lib.bf16_array(x.ctypes.data, out.ctypes.data, x.size)
     ref = torch.from_numpy(x).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
     np.testing.assert_array_equal(out, ref)
+
+
+@pytest.mark.parametrize("name", ["bfs2_rk4", "cavq3_rk4", "cyl4x8_rk4"])
+def test_kronecker_element_body_matches_host_apply(lib, name):
+    """The element body the device smoother will run (kron_apply.cuh, host build with one
+    thread) against kron_apply on every element's fitted factors."""
+    lib.case_kron_body.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(os.path.join(GOLDEN, name, "input.dat").encode(), ctypes.byref(code))
+    c = HostCase(lib, h)
+    try:
+        K2 = c.K * c.K
+        rng = np.random.Generator(np.random.PCG64(8))
+        for el in range(c.N):
+            r = rng.standard_normal(K2)
+            z_body, z_host = np.zeros(K2), np.zeros(K2)
+            dfx = ctypes.c_double(0.0)
+            ok_host = lib.case_kron(h, el, _p(r), _p(z_host), ctypes.byref(dfx))
+            ok_body = lib.case_kron_body(h, el, _p(r.copy()), _p(z_body))
+            assert ok_host == ok_body
+            if ok_body:
+                np.testing.assert_allclose(z_body, z_host, rtol=1e-12, atol=1e-14 * np.abs(z_host).max())
+    finally:
+        c.close()
