@@ -105,6 +105,11 @@ struct MfOp {
     const int* bcol;        // [N][5] element of each block (slot 0 = self, 1 + ijp = neighbours)
     // optional BF16 copy of dinv (bit patterns), read by the FP32 smoother when present
     const unsigned short* dinv_bf16 = nullptr;
+    // optional Kronecker-sum smoother (FP32): factors [N][4K^2 + 2K], the compact index of
+    // each element's exact block or -1 [N], and those exact blocks [n][K2][K2] ([rs][ij])
+    const T* kron_f = nullptr;
+    const int* kron_x = nullptr;
+    const T* kron_exact = nullptr;
 };
 
 template <typename T>

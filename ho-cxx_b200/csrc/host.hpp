@@ -148,6 +148,12 @@ struct KronSmoother {
 };
 struct KronFit;
 void kron_store(const KronFit* f, double defect, int el, KronSmoother& ks);
+// The device arrays of the Kronecker-sum smoother: per element its 4K^2 factors and 2K
+// eigenvalues [N][4K^2 + 2K] (zero where the exact block is used), the index of its exact
+// inverse block in the compact array, or -1 [N], and those blocks [n_exact][K^2][K^2]
+// taken from dinv (same [rs][ij] layout).
+void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv, std::vector<double>& factors,
+                        std::vector<int>& exact_index, std::vector<double>& exact_blocks);
 
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
                       PoissonOperator& op, bool keep_blocks = false, KronSmoother* kron = nullptr);

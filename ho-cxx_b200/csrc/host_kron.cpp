@@ -298,4 +298,25 @@ void kron_store(const KronFit* f, double defect, int el, KronSmoother& ks) {
     std::copy(f->ly.begin(), f->ly.end(), ks.lam.begin() + ((size_t)el * 2 + 1) * K);
 }
 
+void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv, std::vector<double>& factors,
+                        std::vector<int>& exact_index, std::vector<double>& exact_blocks) {
+    const int K = ks.K, K2 = K * K, K4 = K2 * K2, per = 4 * K2 + 2 * K;
+    const int N = (int)ks.exact.size();
+    factors.assign((size_t)N * per, 0.0);
+    exact_index.assign(N, -1);
+    exact_blocks.clear();
+    int n_exact = 0;
+    for (int el = 0; el < N; ++el) {
+        if (ks.exact[el]) {
+            exact_index[el] = n_exact++;
+            exact_blocks.insert(exact_blocks.end(), dinv.begin() + (size_t)el * K4, dinv.begin() + (size_t)(el + 1) * K4);
+            continue;
+        }
+        std::copy(ks.v.begin() + (size_t)el * 4 * K2, ks.v.begin() + (size_t)(el + 1) * 4 * K2,
+                  factors.begin() + (size_t)el * per);
+        std::copy(ks.lam.begin() + (size_t)el * 2 * K, ks.lam.begin() + (size_t)(el + 1) * 2 * K,
+                  factors.begin() + (size_t)el * per + 4 * K2);
+    }
+}
+
 }  // namespace ho2d

@@ -25,6 +25,7 @@
 #include "device.cuh"
 #include "fr_device.cuh"
 #include "fr_launch.hpp"
+#include "kron_apply.cuh"
 
 namespace ho2d {
 
@@ -507,15 +508,19 @@ __device__ __forceinline__ T up0_part(const CoarseOut<T>& co, const F0<T>& f0, i
     return u;
 }
 
-// Whether k_mf_post stages its CTA's inverse blocks (EPB x K^4 values, contiguous in
-// memory) in shared memory: when they fit in 32 KB of static shared memory. The blocks are
-// stored as T, or as BF16 bit patterns (BF16) for the FP32 smoother.
-template <int K, typename T, bool BF16 = false>
+// The smoother's element data (BS): 0 = inverse blocks in T; 1 = inverse blocks as BF16 bit
+// patterns (FP32 smoother); 2 = Kronecker-sum factors, with the exact blocks only for the
+// elements the fit does not approximate well (FP32 smoother). For BS 0 and 1, whether
+// k_mf_post stages its CTA's inverse blocks (EPB x K^4 values, contiguous in memory) in
+// shared memory: when they fit in 32 KB of static shared memory.
+template <int K, typename T, int BS = 0>
 struct PostStage {
-    using DT = typename std::conditional<BF16, unsigned short, T>::type;
+    using DT = typename std::conditional<BS == 1, unsigned short, T>::type;
     static constexpr int K4 = K * K * K * K;
     static constexpr size_t kBytes = (size_t)Shape<K>::EPB * K4 * sizeof(DT) + 32;  // + 16-byte alignment slack
-    static constexpr bool kOn = kBytes <= 32768;
+    static constexpr bool kOn = BS != 2 && kBytes <= 32768;
+    static constexpr int KF = 4 * K * K + 2 * K;  // Kronecker factors per element (BS 2)
+    static constexpr int KE = BS == 2 ? Shape<K>::EPB : 1;
 };
 
 __device__ __forceinline__ float block_value(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
@@ -537,11 +542,11 @@ __device__ __forceinline__ T block_value(T v) {
 // (cp.async, 16-byte pieces of the 16-byte-aligned superset of the blocks; the buffer is
 // padded past its end), and the block row sums and the vectors are loaded, so all of it
 // overlaps the up step's dependent loads.
-template <int K, typename T, bool BF16 = false>
+template <int K, typename T, int BS = 0>
 __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
                                                                 int has_coarse, double w, ReduceScratch rs, int mode) {
     using S = Shape<K>;
-    using PS = PostStage<K, T, BF16>;
+    using PS = PostStage<K, T, BS>;
     using DT = typename PS::DT;
     constexpr int K2 = S::K2;
     KrylovScalars* sc = rs.sc;
@@ -549,12 +554,13 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25], ue[S::EPB][5];
     __shared__ DevBases<T> sbas;
     __shared__ __align__(16) unsigned char sd_raw[PS::kOn ? PS::kBytes : 16];
+    __shared__ T kf[PS::KE][BS == 2 ? PS::KF : 1], kt[PS::KE][BS == 2 ? K2 : 1], kz[PS::KE][BS == 2 ? K2 : 1];
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
     const int el = blockIdx.x * S::EPB + le;
     const bool active = le < S::EPB && el < op.g.N;
     const int p = el * K2 + ij;
     const DT* dsrc;
-    if constexpr (BF16) dsrc = op.dinv_bf16;
+    if constexpr (BS == 1) dsrc = op.dinv_bf16;
     else dsrc = op.dinv;
     const DT* dblk = dsrc + (size_t)el * PS::K4;  // this element's inverse block ([rs][ij])
     if constexpr (PS::kOn) {
@@ -578,6 +584,13 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
         rr = v.r[p];
         vv = v.v[p];
         if (mode == 0) pp = v.p[p];
+    }
+    int kx = -1;  // BS 2: this element's exact block, or -1 for its Kronecker factors
+    if constexpr (BS == 2) {
+        if (active) {
+            kx = op.kron_x[el];
+            for (int q = ij; q < PS::KF; q += K2) kf[le][q] = op.kron_f[(size_t)el * PS::KF + q];
+        }
     }
     stage_bases(sbas, op.b);
     const F0<T> f0 = f0_of(v, sc, mode);
@@ -625,10 +638,24 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     }
     __syncthreads();
     T* z = mode == 0 ? v.ph : v.sh;
-    if (active) {
-        T acc = T(0);
+    T acc = T(0);
+    if constexpr (BS == 2) {
+        // the exact block where the fit falls back (read before the body reuses sr), then
+        // the Kronecker-sum step for the other elements; every thread passes the body's
+        // barriers
+        if (active && kx >= 0) {
+            const T* blk = op.kron_exact + (size_t)kx * PS::K4;
+            for (int r = 0; r < K2; ++r) acc += blk[r * K2 + ij] * sr[le][r];
+        }
+        const int lei = active ? le : 0;
+        const ElemCtx<K2> ec{ij};
+        kron_apply_body<K, T>(ec, active && kx < 0, kf[lei], kf[lei] + 4 * K2, sr[lei], kt[lei], kz[lei]);
+        if (active && kx < 0) acc = kz[le][ij];
+    } else if (active) {
 #pragma unroll
         for (int r = 0; r < K2; ++r) acc += T(block_value(dblk[r * K2 + ij])) * sr[le][r];
+    }
+    if (active) {
         const T zz = u_self + T(w) * acc;
         z[p] = zz;
         sz[le][ij] = zz;
@@ -874,8 +901,12 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
     const unsigned gv = (g + kVecTiles - 1) / kVecTiles;
     auto post = [&](int mode) {
         if constexpr (std::is_same<T, float>::value) {
+            if (op.kron_f) {
+                k_mf_post<K, T, 2><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                return;
+            }
             if (op.dinv_bf16) {
-                k_mf_post<K, T, true><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                k_mf_post<K, T, 1><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
                 return;
             }
         }

@@ -94,7 +94,10 @@ Error Solver::setup_from_mesh() {
     for (double j : M_.J)
         if (!(j > 0.0)) return {3, "non-positive element Jacobian: check the element orientation"};
     HO2D_TRY(setup_bcs(in_, mesh_, B_, bc_));
-    assemble_poisson(mesh_, B_, M_, bc_, op_);
+    // HO2D_SMOOTHER_KRON=1: the Kronecker-sum fit of every diagonal block for the FP32 smoother
+    const char* kron_env = std::getenv("HO2D_SMOOTHER_KRON");
+    kron_ = KronSmoother();
+    assemble_poisson(mesh_, B_, M_, bc_, op_, false, kron_env && std::string(kron_env) == "1" ? &kron_ : nullptr);
 
     DeviceState& d = *d_;
     HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
@@ -164,6 +167,7 @@ Error Solver::setup_from_mesh() {
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
     d.dinv_bf16.reset();
+    for (DeviceBuffer* b : {&d.kron_f, &d.kron_x, &d.kron_exact}) b->reset();
     d.rowsum32.reset();
     for (auto& b : d.pg32) b.reset();
     HO2D_TRY(setup_preconditioner());
@@ -449,6 +453,15 @@ Error Solver::upload_precision_arrays() {
         std::vector<uint16_t> h(op_.dinv.size());  // includes the zero padding past the end
         for (size_t i = 0; i < h.size(); ++i) h[i] = bf16_bits((float)op_.dinv[i]);
         HO2D_CUDA(upload(d.dinv_bf16, h), "upload bf16 block-Jacobi");
+    }
+    if (kron_.K > 0) {  // the Kronecker-sum smoother's arrays (FP32), set up with HO2D_SMOOTHER_KRON=1
+        std::vector<double> f, ex;
+        std::vector<int> xi;
+        kron_device_arrays(kron_, op_.dinv, f, xi, ex);
+        if (ex.empty()) ex.assign(1, 0.0);
+        HO2D_CUDA(upload_as<float>(d.kron_f, f), "upload Kronecker factors");
+        HO2D_CUDA(upload(d.kron_x, xi), "upload Kronecker exact-block index");
+        HO2D_CUDA(upload_as<float>(d.kron_exact, ex), "upload Kronecker exact blocks");
     }
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");

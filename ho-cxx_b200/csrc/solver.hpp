@@ -175,6 +175,7 @@ class Solver {
     std::string output_dir_;                  // where solve() writes its VTK files (empty: none)
     SamplePoints samples_;                    // the input's sample points (VTK output)
     VtkQueue vtk_queue_;                      // dumps being written (declared after what it reads)
+    KronSmoother kron_;                       // Kronecker-sum smoother data (HO2D_SMOOTHER_KRON=1)
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

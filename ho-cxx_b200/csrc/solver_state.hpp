@@ -72,6 +72,9 @@ struct DeviceState {
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
     DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
     DeviceBuffer dinv_bf16;  // BF16 copy of dinv for the FP32 smoother (HO2D_SMOOTHER_BF16=1)
+    // Kronecker-sum smoother for the FP32 solve (HO2D_SMOOTHER_KRON=1): factors, exact-block
+    // index per element, compact exact blocks
+    DeviceBuffer kron_f, kron_x, kron_exact;
     // matrix-free operator data: G11, G12, G22, fa, fb, nfa, nfb, minv (PoisGeom)
     DeviceBuffer pg64[8], pg32[8], pcode, pscat;
     std::vector<double> pg_host[8];  // kept for the FP32 copies made on demand
@@ -236,6 +239,10 @@ MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
     op.b = *reinterpret_cast<const DevBases<T>*>(f32 ? (const void*)&d.b32 : (const void*)&d.b64);
     op.dinv = f32 ? (const T*)d.dinv32.get() : (const T*)d.dinv64.get();
     op.dinv_bf16 = f32 ? (const unsigned short*)d.dinv_bf16.get() : nullptr;
+    const bool kron = f32 && d.kron_f.get();
+    op.kron_f = kron ? (const T*)d.kron_f.get() : nullptr;
+    op.kron_x = kron ? d.kron_x.as<int>() : nullptr;
+    op.kron_exact = kron ? (const T*)d.kron_exact.get() : nullptr;
     op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
     op.bcol = d.bcol.as<int>();
     return op;

@@ -379,3 +379,43 @@ extern "C" int case_kron_body(void* h, int el, const double* r, double* z) {
     }
     return 1;
 }
+
+// kron_device_arrays of the case: the elements' packed factors applied by the element body
+// (or their exact block) to r, as the device smoother will; returns the number of exact
+// elements. z [N][K^2], r [N][K^2].
+extern "C" long case_kron_device(void* h, const double* r, double* z) {
+    Case* c = static_cast<Case*>(h);
+    const int K = c->in.knod, K2 = K * K, K4 = K2 * K2, per = 4 * K2 + 2 * K;
+    ho2d::PoissonOperator op;
+    ho2d::KronSmoother ks;
+    ho2d::assemble_poisson(c->m, c->B, c->M, c->bc, op, false, &ks);
+    std::vector<double> f, ex;
+    std::vector<int> xi;
+    ho2d::kron_device_arrays(ks, op.dinv, f, xi, ex);
+    long n_exact = 0;
+    for (int el = 0; el < c->m.n_el; ++el) {
+        const double* re = r + (size_t)el * K2;
+        double* ze = z + (size_t)el * K2;
+        if (xi[el] >= 0) {
+            ++n_exact;
+            const double* blk = &ex[(size_t)xi[el] * K4];
+            for (int ij = 0; ij < K2; ++ij) {
+                double acc = 0.0;
+                for (int rs = 0; rs < K2; ++rs) acc += blk[rs * K2 + ij] * re[rs];
+                ze[ij] = acc;
+            }
+            continue;
+        }
+        std::vector<double> rr(re, re + K2), t(K2);
+        const double* fe = &f[(size_t)el * per];
+        const ho2d::ElemCtx<1> cx{0};
+        switch (K) {
+            case 3: ho2d::kron_apply_body<3, double>(cx, true, fe, fe + 4 * K2, rr.data(), t.data(), ze); break;
+            case 4: ho2d::kron_apply_body<4, double>(cx, true, fe, fe + 4 * K2, rr.data(), t.data(), ze); break;
+            case 5: ho2d::kron_apply_body<5, double>(cx, true, fe, fe + 4 * K2, rr.data(), t.data(), ze); break;
+            case 7: ho2d::kron_apply_body<7, double>(cx, true, fe, fe + 4 * K2, rr.data(), t.data(), ze); break;
+            default: return -1;
+        }
+    }
+    return n_exact;
+}

@@ -932,3 +932,35 @@ def test_kronecker_element_body_matches_host_apply(lib, name):
                 np.testing.assert_allclose(z_body, z_host, rtol=1e-12, atol=1e-14 * np.abs(z_host).max())
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("name", ["bfs2_rk4", "cavq3_rk4", "cav4_euler_k3"])
+def test_kronecker_device_arrays(lib, name):
+    """The packed arrays the device smoother reads (kron_device_arrays) applied element by
+    element as the kernel will (the element body on the factors, or the exact block where
+    the fit falls back) equal the fitted inverse (kron_apply) and the exact inverse."""
+    lib.case_kron_device.restype = ctypes.c_long
+    lib.case_kron_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    code = ctypes.c_int(0)
+    h = lib.case_from_input(os.path.join(GOLDEN, name, "input.dat").encode(), ctypes.byref(code))
+    c = HostCase(lib, h)
+    try:
+        K2 = c.K * c.K
+        r = np.random.Generator(np.random.PCG64(9)).standard_normal(c.N * K2)
+        z = np.zeros_like(r)
+        n_exact = lib.case_kron_device(h, _p(r), _p(z))
+        assert n_exact >= 0
+        dinv = c["dinv"][: c.N * K2 * K2].reshape(c.N, K2, K2)  # [rs][ij]
+        exact = 0
+        for el in range(c.N):
+            re = r[el * K2:(el + 1) * K2].copy()
+            zk = np.zeros(K2)
+            dfx = ctypes.c_double(0.0)
+            if lib.case_kron(h, el, _p(re), _p(zk), ctypes.byref(dfx)) and dfx.value <= 0.5:
+                np.testing.assert_allclose(z[el * K2:(el + 1) * K2], zk, rtol=1e-12, atol=1e-14 * np.abs(zk).max())
+            else:
+                exact += 1
+                np.testing.assert_allclose(z[el * K2:(el + 1) * K2], dinv[el].T @ re, rtol=1e-12)
+        assert exact == n_exact
+    finally:
+        c.close()
