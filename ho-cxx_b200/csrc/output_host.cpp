@@ -9,6 +9,7 @@
 // the node-averaged vorticity and velocity interpolated with the geometry shape functions.
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <memory>
 #include <new>
 #include <string>
@@ -241,6 +242,8 @@ Error VtkQueue::submit(const Mesh& mesh, const Bases& B, const SamplePoints* sam
             err_ = write_vtk_files(mesh, B, j.problem_type, f, j.indx, j.subidx, j.dir, samples);
         } catch (const std::bad_alloc&) {
             err_ = {5, "out of host memory writing the VTK files"};
+        } catch (const std::exception& ex) {  // nothing may leave the writer thread
+            err_ = {5, std::string("writing the VTK files: ") + ex.what()};
         }
     };
     try {
