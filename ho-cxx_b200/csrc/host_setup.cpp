@@ -50,36 +50,44 @@ void lagrange_at(const std::vector<double>& nodes, double x, double* V, double* 
     }
 }
 
-// In-place Gauss-Jordan inverse with partial pivoting of an n x n row-major matrix.
-bool invert(int n, std::vector<double>& a) {
-    std::vector<double> inv((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+// In-place Gauss-Jordan inverse with partial pivoting of an n x n row-major matrix
+// (n <= kMaxK^2). Step k swaps the pivot row into place, scales it, and eliminates column k
+// from every other row; column k then holds the inverse's column (its entries start as the
+// identity's), so the inverse builds up in a itself and the row swaps are undone as column
+// swaps at the end: n^3 multiply-adds and no scratch beyond two rows. The row update is
+// compiled twice, for AVX2 and for the baseline, and picked at load time; neither contracts
+// to FMA, so both give the same bits as the textbook two-matrix form.
+__attribute__((target_clones("avx2", "default"))) bool invert(int n, std::vector<double>& a) {
+    constexpr int kMax = kMaxK * kMaxK;
+    if (n < 1 || n > kMax || a.size() < (size_t)n * n) return false;
+    int piv[kMax];
+    double rk[kMax];  // the scaled pivot row, kept apart so the row updates vectorise
+    double* m = a.data();
     for (int k = 0; k < n; ++k) {
         int p = k;
         for (int i = k + 1; i < n; ++i)
-            if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)p * n + k])) p = i;
-        if (a[(size_t)p * n + k] == 0.0) return false;
+            if (std::fabs(m[(size_t)i * n + k]) > std::fabs(m[(size_t)p * n + k])) p = i;
+        if (m[(size_t)p * n + k] == 0.0) return false;
+        piv[k] = p;
         if (p != k)
-            for (int j = 0; j < n; ++j) {
-                std::swap(a[(size_t)k * n + j], a[(size_t)p * n + j]);
-                std::swap(inv[(size_t)k * n + j], inv[(size_t)p * n + j]);
-            }
-        const double d = 1.0 / a[(size_t)k * n + k];
-        for (int j = 0; j < n; ++j) {
-            a[(size_t)k * n + j] *= d;
-            inv[(size_t)k * n + j] *= d;
-        }
+            for (int j = 0; j < n; ++j) std::swap(m[(size_t)k * n + j], m[(size_t)p * n + j]);
+        double* row = m + (size_t)k * n;
+        const double d = 1.0 / row[k];
+        row[k] = 1.0;
+        for (int j = 0; j < n; ++j) rk[j] = row[j] * d;
+        for (int j = 0; j < n; ++j) row[j] = rk[j];
         for (int i = 0; i < n; ++i) {
             if (i == k) continue;
-            const double l = a[(size_t)i * n + k];
+            double* __restrict__ ri = m + (size_t)i * n;
+            const double l = ri[k];
             if (l == 0.0) continue;
-            for (int j = 0; j < n; ++j) {
-                a[(size_t)i * n + j] -= l * a[(size_t)k * n + j];
-                inv[(size_t)i * n + j] -= l * inv[(size_t)k * n + j];
-            }
+            ri[k] = 0.0;
+            for (int j = 0; j < n; ++j) ri[j] -= l * rk[j];
         }
     }
-    a.swap(inv);
+    for (int k = n - 1; k >= 0; --k)
+        if (piv[k] != k)
+            for (int i = 0; i < n; ++i) std::swap(m[(size_t)i * n + k], m[(size_t)i * n + piv[k]]);
     return true;
 }
 

@@ -202,6 +202,43 @@ def test_block_jacobi_inverse(golden):
         assert np.abs(dinv[el].T @ Dm - np.eye(K2)).max() <= 1e-12 * np.linalg.cond(Dm)
 
 
+def _two_matrix_gauss_jordan(D):
+    """Gauss-Jordan with partial pivoting (first row of largest magnitude) on [A | I] for a
+    stack of matrices, each step rounding a product and then a difference, as the host code
+    does without FMA."""
+    a = D.copy()
+    N, n, _ = a.shape
+    inv = np.broadcast_to(np.eye(n), a.shape).copy()
+    ar = np.arange(N)
+    for k in range(n):
+        p = k + np.argmax(np.abs(a[:, k:, k]), axis=1)
+        assert (a[ar, p, k] != 0.0).all()
+        for m in (a, inv):
+            rk = m[ar, k].copy()
+            m[ar, k] = m[ar, p]
+            m[ar, p] = rk
+        d = 1.0 / a[:, k, k]
+        a[:, k, :] *= d[:, None]
+        inv[:, k, :] *= d[:, None]
+        for i in range(n):
+            if i != k:
+                l = a[:, i, k].copy()
+                a[:, i, :] -= l[:, None] * a[:, k, :]
+                inv[:, i, :] -= l[:, None] * inv[:, k, :]
+    return inv
+
+
+def test_block_inverse_bits(golden):
+    """The in-place inverse (one matrix, column swaps undone at the end; the AVX2 or the
+    baseline clone, whichever this CPU selects) gives the same bits as the two-matrix
+    elimination on every diagonal block."""
+    c, _, _ = golden
+    K2 = c.K * c.K
+    Dm = c["blocks"].reshape(c.N, 5, K2, K2)[:, 0].transpose(0, 2, 1)  # [ij][rs]
+    dinv = c["dinv"][: c.N * K2 * K2].reshape(c.N, K2, K2).transpose(0, 2, 1)
+    assert np.array_equal(dinv, _two_matrix_gauss_jordan(Dm))
+
+
 def test_streamed_block_reductions(golden):
     """assemble_poisson keeps the blocks only on request. The row, column and block sums it
     streams instead must be the sums of the kept blocks, bit for bit, in the summation order
