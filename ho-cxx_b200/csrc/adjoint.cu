@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(AShape<K>::THREADS) k_pc_transpose(int N, cons
     __syncthreads();
     if (!active) return;
     // (D^-1)[a][b] is stored at [b][a]; row ij of D^-T is therefore contiguous
-    const T* d = dinv + (size_t)el * K2 * K2 + (size_t)ij * K2;
+    const T* d = dinv + (size_t)el * padded_count(K2 * K2, (int)sizeof(T)) + (size_t)ij * K2;
     T acc = T(0);
 #pragma unroll
     for (int rs = 0; rs < K2; ++rs) acc += d[rs] * q[le][rs];

@@ -176,6 +176,23 @@ int ho2d_set_precision(ho2d_solver* h, int32_t mode) {
     return guarded(h, [&]() { return h->s.set_precision(mode); });
 }
 
+int ho2d_profile_krylov(ho2d_solver* h, int32_t iterations, double* ms, double* bytes) {
+    return guarded(h, [&]() { return h->s.profile_krylov(iterations, ms, bytes); });
+}
+
+int ho2d_set_smoother(ho2d_solver* h, int32_t kind) {
+    return guarded(h, [&]() { return h->s.set_smoother(kind); });
+}
+
+int ho2d_get_smoother(ho2d_solver* h, int32_t* kind, int32_t* exact_blocks) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};
+        if (kind) *kind = h->s.smoother();
+        if (exact_blocks) *exact_blocks = h->s.smoother_exact_blocks();
+        return {0, ""};
+    });
+}
+
 int ho2d_set_poisson_tolerance(ho2d_solver* h, double rel_tol, int32_t max_iter) {
     return guarded(h, [&]() -> ho2d::Error {
         if (!(rel_tol > 0.0) || max_iter <= 0) return {HO2D_ERR_ARG, "tolerance and iteration cap must be positive"};
@@ -188,6 +205,13 @@ int ho2d_poisson_stats(ho2d_solver* h, int32_t* iterations, double* rel_residual
     return guarded(h, [&]() -> ho2d::Error {
         if (iterations) *iterations = h->s.last_poisson_iterations();
         if (rel_residual) *rel_residual = h->s.last_poisson_residual();
+        return {0, ""};
+    });
+}
+
+int ho2d_solve_counters(ho2d_solver* h, int64_t* solves, int64_t* iterations, int64_t* sweeps) {
+    return guarded(h, [&]() -> ho2d::Error {
+        h->s.counters(solves, iterations, sweeps);
         return {0, ""};
     });
 }

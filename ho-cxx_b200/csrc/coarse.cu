@@ -284,6 +284,24 @@ int coarse_launches(const Precond<T>& pc) {
     return d + 1 + (d > 1 ? d - 1 : 0);
 }
 
+// Algorithmic bytes of one coarse cycle as coarse_cycle launches it: every row-padded
+// operator's values and column indices, the dense inverse, each level's right-hand side
+// read and result written; the level-0 right-hand side is formed from three element-sum
+// vectors.
+template <typename T>
+int coarse_cycle_bytes(const Precond<T>& pc) {
+    if (pc.nlev <= 0) return 0;
+    const int d = pc.nlev - 1;
+    auto ell = [](const DevEll<T>& A) { return (double)A.n * A.w * (sizeof(T) + (A.col ? 4 : 0)); };
+    double b = (double)pc.dense.n * pc.dense.w * sizeof(T) + 2.0 * pc.dense.n * sizeof(T);
+    if (d == 0) return (int)(b + 3.0 * pc.dense.n * sizeof(T));
+    b += ell(pc.lev[0].M) + 3.0 * pc.lev[0].n * sizeof(T) + pc.lev[1].n * sizeof(T);
+    for (int l = 1; l < d; ++l) b += ell(pc.lev[l].M) + (double)(pc.lev[l].n + pc.lev[l + 1].n) * sizeof(T);
+    for (int l = d - 1; l >= 1; --l)
+        b += ell(pc.lev[l].S) + ell(pc.lev[l].Q) + (double)(2 * pc.lev[l].n + pc.lev[l + 1].n) * sizeof(T);
+    return (int)b;
+}
+
 template <typename T>
 CoarseOut<T> coarse_out(const Precond<T>& pc) {
     CoarseOut<T> c;
@@ -303,7 +321,8 @@ CoarseOut<T> coarse_out(const Precond<T>& pc) {
     template int coarse_launches<T>(const Precond<T>&);                                              \
     template cudaError_t coarse_cycle_vec<T>(const Precond<T>&, const T*, const KrylovScalars*, cudaStream_t); \
     template int coarse_vec_launches<T>(const Precond<T>&);                                          \
-    template CoarseOut<T> coarse_out<T>(const Precond<T>&);
+    template CoarseOut<T> coarse_out<T>(const Precond<T>&);                                          \
+    template int coarse_cycle_bytes<T>(const Precond<T>&);
 
 HO2D_INSTANTIATE_COARSE(double)
 HO2D_INSTANTIATE_COARSE(float)

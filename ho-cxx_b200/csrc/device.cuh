@@ -9,6 +9,13 @@ namespace ho2d {
 
 constexpr int kDirichlet = 0, kNeumann = 1;
 
+// Per-element stride, in values of elem_bytes bytes, of the preconditioner's element data
+// (the K^4 inverse blocks, the Kronecker-sum factors): n rounded up to a whole number of
+// 16-byte pieces, so that every element's data starts on a 16-byte boundary.
+__host__ __device__ constexpr int padded_count(int n, int elem_bytes) {
+    return (n * elem_bytes + 15) / 16 * 16 / elem_bytes;
+}
+
 // Threads: K^2 per element (one per solution point), EPB elements per CTA.
 template <int K>
 struct Shape {
@@ -68,6 +75,15 @@ struct KrylovScalars {
     double bnorm2, rnorm2, snorm2, eps2;
     int it, done, breakdown, s_exit, zero_rhs, pad;
     double tol;  // relative tolerance of the next solve, written by the host before it starts
+    // FP64 iterative refinement around the FP32 solve when it runs on the device (one graph
+    // per solve): the target on the FP64 residual, the smallest inner reduction asked of a
+    // sweep and the sweep cap (written by the host), then the sweeps done, the inner
+    // iterations summed over them, the last relative FP64 residual, whether it was finite
+    // and whether the right-hand side was zero (written by the device)
+    double tol_outer, inner_tol;
+    int max_sweeps, sweeps, iters_total, finite, zero_psi;
+    int dev_error;  // nonzero: a kernel's bounded wait ran out (the host reports it)
+    double res;
 };
 
 // A preconditioner application is skipped once the solve is done, and the second one of

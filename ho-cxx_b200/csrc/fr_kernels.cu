@@ -47,15 +47,19 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) trace_kernel(int N, const T
     }
 }
 
-template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g, DevBases<T> bp, BcArrays bc,
-                                                                      VelocityArgs<T> a) {
+template <int K, typename T, typename TP>
+__global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<TP> g, DevBases<TP> bp,
+                                                                      DevBases<T> bwp, BcArrays bc,
+                                                                      VelocityArgs<T, TP> a) {
     using S = Shape<K>;
-    __shared__ DevBases<T> b;
+    __shared__ DevBases<TP> b;
+    __shared__ DevBases<T> bw;
     stage_bases(b, bp);
+    stage_bases(bw, bwp);
     constexpr int K2 = S::K2, NF = S::NF, EPB = S::EPB;
-    __shared__ T s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2], s_w[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
-    __shared__ T s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF];
+    __shared__ TP s_f[EPB][K2], s_a[EPB][K2], s_b[EPB][K2];
+    __shared__ T s_w[EPB][K2], s_ux[EPB][K2], s_uy[EPB][K2];
+    __shared__ TP s_tv[EPB][NF], s_tg[EPB][NF], s_com[EPB][NF], s_cg[EPB][NF], s_fb[EPB][NF];
     const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
     const int el = blockIdx.x * EPB + le;
     const bool active = le < EPB && el < g.N;
@@ -66,10 +70,10 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g
     }
     __syncthreads();
     if (active)
-        for (int o = ij; o < NF; o += K2) face_trace<K, T>(s_f[le], b, o, s_tv[le][o], s_tg[le][o]);
+        for (int o = ij; o < NF; o += K2) face_trace<K, TP>(s_f[le], b, o, s_tv[le][o], s_tg[le][o]);
     __syncthreads();
-    face_common<K, T>(active, el, ij, g, b, a.psi_tv, a.psi_tg, s_tv[lei], s_tg[lei], s_com[lei], s_cg[lei], g.sw_p,
-                      bc.bc_p, true);
+    face_common<K, TP>(active, el, ij, g, b, a.psi_tv, a.psi_tg, s_tv[lei], s_tg[lei], s_com[lei], s_cg[lei], g.sw_p,
+                       bc.bc_p, true);
     // boundary side outputs: velocity_jump / BC_normal_vel, then the no-slip diffusion BC
     if (active) {
         for (int o = ij; o < NF; o += K2) {
@@ -83,8 +87,8 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g
             if (g.sw_p[e] == kDirichlet) {
                 vj = double(s_cg[le][o]) / double(g.fAn[q]);
             } else {
-                const T vsign = T(1 - 2 * (ijp / 2));
-                T nv = T(0);
+                const TP vsign = TP(1 - 2 * (ijp / 2));
+                TP nv = TP(0);
 #pragma unroll
                 for (int d = 0; d < K; ++d) nv += vsign * s_com[le][ijp * K + d] * b.D[d * K + k];
                 bc.bc_nv[be] = double(nv / g.fAn[q]);
@@ -96,31 +100,31 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) velocity_kernel(FrGeom<T> g
             bc.vjump[be] = vj;
         }
     }
-    T ft = T(0), gt = T(0);
-    contravariant_gradient<K, T>(active, el, ij, g, b, s_f[lei], s_tv[lei], s_com[lei], s_cg[lei], s_a[lei],
-                                 s_b[lei], s_fb[lei], ft, gt);
+    TP ft = TP(0), gt = TP(0);
+    contravariant_gradient<K, TP>(active, el, ij, g, b, s_f[lei], s_tv[lei], s_com[lei], s_cg[lei], s_a[lei],
+                                  s_b[lei], s_fb[lei], ft, gt);
     if (active) {
         const int j = ij / K, i = ij % K, p = el * K2 + ij;
-        const T tx = ft + s_fb[le][0 * K + j] * b.R[i * 2 + 0] + s_fb[le][1 * K + j] * b.R[i * 2 + 1];
-        const T ty = gt + s_fb[le][2 * K + i] * b.R[j * 2 + 0] + s_fb[le][3 * K + i] * b.R[j * 2 + 1];
-        const T xx = g.xxi[p], xe = g.xeta[p], yx = g.yxi[p], ye = g.yeta[p], J = g.J[p];
-        const T dpdx = (tx * xx + ty * xe) / J;
-        const T dpdy = (tx * yx + ty * ye) / J;
-        const T u = dpdy, v = -dpdx;
-        a.u[p] = u;
-        a.v[p] = v;
-        s_ux[le][ij] = u * ye - v * xe;   // contravariant volumetric fluxes J u.grad(xi), J u.grad(eta)
-        s_uy[le][ij] = -u * yx + v * xx;
+        const TP tx = ft + s_fb[le][0 * K + j] * b.R[i * 2 + 0] + s_fb[le][1 * K + j] * b.R[i * 2 + 1];
+        const TP ty = gt + s_fb[le][2 * K + i] * b.R[j * 2 + 0] + s_fb[le][3 * K + i] * b.R[j * 2 + 1];
+        const TP xx = g.xxi[p], xe = g.xeta[p], yx = g.yxi[p], ye = g.yeta[p], J = g.J[p];
+        const TP dpdx = (tx * xx + ty * xe) / J;
+        const TP dpdy = (tx * yx + ty * ye) / J;
+        const TP u = dpdy, v = -dpdx;
+        a.u[p] = T(u);
+        a.v[p] = T(v);
+        s_ux[le][ij] = T(u * ye - v * xe);   // contravariant volumetric fluxes J u.grad(xi), J u.grad(eta)
+        s_uy[le][ij] = T(-u * yx + v * xx);
     }
     __syncthreads();
     if (active) {
         for (int o = ij; o < NF; o += K2) {
             const int ijp = o / K;
             T wv, wg;
-            face_trace<K, T>(s_w[le], b, o, wv, wg);
+            face_trace<K, T>(s_w[le], bw, o, wv, wg);
             a.w_tv[el * NF + o] = wv;
             a.w_tg[el * NF + o] = wg;
-            a.U_t[el * NF + o] = face_value<K, T>(ijp < 2 ? s_ux[le] : s_uy[le], b, o);
+            a.U_t[el * NF + o] = face_value<K, T>(ijp < 2 ? s_ux[le] : s_uy[le], bw, o);
         }
     }
 }
@@ -428,10 +432,11 @@ cudaError_t launch_trace(int K, int N, const T* f, T* tv, T* tg, const DevBases<
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_velocity(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
-                            const VelocityArgs<T>& a, cudaStream_t s) {
-    HO2D_DISPATCH_K(K, (velocity_kernel<KK, T><<<grid_for<KK>(g.N), Shape<KK>::THREADS, 0, s>>>(g, b, bc, a)));
+template <typename T, typename TP>
+cudaError_t launch_velocity(int K, const FrGeom<TP>& g, const DevBases<TP>& bp, const DevBases<T>& bw,
+                            const BcArrays& bc, const VelocityArgs<T, TP>& a, cudaStream_t s) {
+    HO2D_DISPATCH_K(K, (velocity_kernel<KK, T, TP><<<grid_for<KK>(g.N), Shape<KK>::THREADS, 0, s>>>(g, bp, bw, bc,
+                                                                                                       a)));
     return cudaGetLastError();
 }
 
@@ -491,8 +496,9 @@ template cudaError_t launch_hybrid_blend<float>(size_t, double*, float*, const d
 
 #define HO2D_INSTANTIATE_FR(T)                                                                                     \
     template cudaError_t launch_trace<T>(int, int, const T*, T*, T*, const DevBases<T>&, cudaStream_t);            \
-    template cudaError_t launch_velocity<T>(int, const FrGeom<T>&, const DevBases<T>&, const BcArrays&,           \
-                                            const VelocityArgs<T>&, cudaStream_t);                                 \
+    template cudaError_t launch_velocity<T, double>(int, const FrGeom<double>&, const DevBases<double>&,         \
+                                                    const DevBases<T>&, const BcArrays&,                          \
+                                                    const VelocityArgs<T, double>&, cudaStream_t);                 \
     template cudaError_t launch_residual<T>(int, const FrGeom<T>&, const DevBases<T>&, const BcArrays&,           \
                                             const ResidualArgs<T>&, cudaStream_t);                                 \
     template cudaError_t launch_poisson_rhs<T>(int, int, const int*, const T*, const T*, const double*,           \

@@ -7,11 +7,16 @@
 
 namespace ho2d {
 
-template <typename T>
+// TP is the precision of psi and of everything derived from it (face values, common
+// values, the gradient, the wall velocity jump); T that of omega and of the outputs. The
+// FP32 stage keeps TP = double: the velocity is a derivative of psi, and the wall's
+// velocity jump is divided by dt Re^-1 into the diffusion BC, which would carry FP32
+// round-off of psi amplified by both.
+template <typename T, typename TP = T>
 struct VelocityArgs {
-    const T* psi;     // [N][K][K]
-    const T* psi_tv;  // psi face traces (values, normal derivatives)
-    const T* psi_tg;
+    const TP* psi;     // [N][K][K]
+    const TP* psi_tv;  // psi face traces (values, normal derivatives)
+    const TP* psi_tg;
     const T* w;       // stage input vorticity
     T* u;             // Cartesian velocity
     T* v;
@@ -43,9 +48,10 @@ struct ResidualArgs {
 
 template <typename T>
 cudaError_t launch_trace(int K, int N, const T* f, T* tv, T* tg, const DevBases<T>& b, cudaStream_t s);
-template <typename T>
-cudaError_t launch_velocity(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
-                            const VelocityArgs<T>& a, cudaStream_t s);
+// g and bp in the precision of psi (TP), bw in that of omega (T)
+template <typename T, typename TP>
+cudaError_t launch_velocity(int K, const FrGeom<TP>& g, const DevBases<TP>& bp, const DevBases<T>& bw,
+                            const BcArrays& bc, const VelocityArgs<T, TP>& a, cudaStream_t s);
 template <typename T>
 cudaError_t launch_residual(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
                             const ResidualArgs<T>& a, cudaStream_t s);
@@ -216,6 +222,8 @@ template <typename T>
 int coarse_vec_launches(const Precond<T>& pc);
 template <typename T>
 CoarseOut<T> coarse_out(const Precond<T>& pc);
+template <typename T>
+int coarse_cycle_bytes(const Precond<T>& pc);
 
 template <typename T>
 cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, cudaStream_t s);
@@ -224,10 +232,23 @@ cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const R
                              const Precond<T>& pc, cudaStream_t s);
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc);
+// one iteration as krylov_iteration, with the boundaries between its launches recorded on
+// 8 events (coarse, smoothing, operator, coarse, smoothing, operator, update)
+template <typename T>
+cudaError_t krylov_iteration_timed(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                                   const Precond<T>& pc, cudaEvent_t* ev, cudaStream_t s);
 // a whole solve (initial residual + device-side while loop of iterations) as a CUDA graph
 template <typename T>
 cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                                  const Precond<T>& pc, cudaStream_t s, cudaGraph_t* graph_out);
+// a whole mixed-precision solve (FP64 refinement around the FP32 BiCGSTAB, both loops on
+// the device) as a CUDA graph; the refinement controls are read from the scalars
+// (tol_outer, inner_tol, max_sweeps) and its results written there (krylov.cu)
+cudaError_t krylov_capture_refined_solve(const MfOp<double>& A64, const MfOp<float>& A32,
+                                         const BicgVectors<float>& v32, const ReduceScratch& rs, int max_iter,
+                                         const Precond<float>& pc, double* psi64, const double* rhs, double* r64,
+                                         double* xtv64, double* xtg64, cudaStream_t s, cudaGraph_t* graph_out);
+int krylov_refined_launches(int sweeps, int inner_iters, const Precond<float>& pc);
 // r = b - A x with ||r||^2 -> sc->rnorm2, ||b||^2 -> sc->bnorm2 (traces of x into xtv/xtg)
 template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
@@ -239,6 +260,9 @@ cudaError_t mf_apply_op(const MfOp<T>& op, const T* x, T* xtv, T* xtg, T* y, cud
 template <typename T>
 cudaError_t mf_apply_only(const MfOp<T>& op, const T* x, const T* xtv, const T* xtg, T* y, int reps, cudaStream_t s);
 int krylov_max_blocks(int K, int N);
+// per-device set-up of the Krylov kernels for order K (krylov.cu): before the first launch
+// or graph capture on the device
+cudaError_t krylov_configure(int K);
 
 // out[0..1] = FP64 force on a body from its boundary points' precomputed coefficients
 // (forces.cu): coef [npts][4], idx = index of each point in the boundary arrays

@@ -26,6 +26,8 @@
 #include "fr_device.cuh"
 #include "fr_launch.hpp"
 #include "kron_apply.cuh"
+#include "rows.cuh"
+#include "bulk_copy.cuh"
 
 namespace ho2d {
 
@@ -88,283 +90,6 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     return true;
 }
 
-// Shared-memory working set of one CTA (EPB elements) for the operator.
-template <int K, typename T>
-struct MfShared {
-    static constexpr int K2 = K * K, NF = 4 * K, EPB = Shape<K>::EPB;
-    T x[EPB][K2], a[EPB][K2], b[EPB][K2];
-    T tv[EPB][NF], tg[EPB][NF];    // own traces, recomputed from x
-    T ntv[EPB][NF], ntg[EPB][NF];  // incoming traces of the neighbours
-    T fa[EPB][NF], fb[EPB][NF], nfa[EPB][NF], nfb[EPB][NF];
-    T com[EPB][NF], cg[EPB][NF];   // common values; common normal fluxes (then their jumps)
-    int code[EPB][4];
-    DevBases<T> bas;               // basis tables staged from the parameter bank
-};
-
-// y = A x at (el, ij) for the homogeneous-boundary Poisson operator: the method-2 FR
-// Laplacian of fr_device.cuh's lap_element. Every global read is one of the element's
-// own rows (its x, metric coefficients, face coefficients and incoming traces), so all
-// of them are issued in a single round; five barrier phases follow. Collective.
-template <int K, typename T>
-__device__ T mf_apply_gen(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv,
-                          const T* __restrict__ tg, MfShared<K, T>& sm, bool active, int le, int el, int ij) {
-    constexpr int K2 = K * K, NF = 4 * K;
-    const PoisGeom<T>& g = op.g;
-    const int j = ij / K, i = ij % K;
-    // round of loads: everything is indexed by this element only
-    T g11 = T(0), g12 = T(0), g22 = T(0);
-    if (active) {
-        const int p = el * K2 + ij;
-        sm.x[le][ij] = x[p];
-        g11 = g.G11[p];
-        g12 = g.G12[p];
-        g22 = g.G22[p];
-        for (int o = ij; o < NF; o += K2) {
-            const int q = el * NF + o;
-            sm.fa[le][o] = g.fa[q];
-            sm.fb[le][o] = g.fb[q];
-            sm.nfa[le][o] = g.nfa[q];
-            sm.nfb[le][o] = g.nfb[q];
-            sm.ntv[le][o] = tv[q];
-            sm.ntg[le][o] = tg[q];
-        }
-        for (int c = ij; c < 4; c += K2) sm.code[le][c] = g.code[el * 4 + c];
-    }
-    stage_bases(sm.bas, op.b);
-    __syncthreads();
-    const DevBases<T>& b = sm.bas;
-    // own traces; common values on interior (average) and Dirichlet (zero) faces
-    if (active)
-        for (int o = ij; o < NF; o += K2) {
-            T v, d;
-            face_trace<K, T>(sm.x[le], b, o, v, d);
-            sm.tv[le][o] = v;
-            sm.tg[le][o] = d;
-            sm.com[le][o] = sm.code[le][o / K] >= 0 ? T(0.5) * (v + sm.ntv[le][o]) : T(0);
-        }
-    __syncthreads();
-    // homogeneous Neumann faces: com = Minv r with r_m = -fa_m (tg_m - tv_m g'(+-1)), the
-    // K x K common-value system of src/HO_2D.cpp:2899-2924 inverted once at setup
-    if (active)
-        for (int o = ij; o < NF; o += K2) {
-            const int ijp = o / K, k = o % K, c = sm.code[le][ijp];
-            if (c > -2) continue;
-            const T gp = b.gp[ijp & 1];
-            const T* mi = g.minv + ((size_t)(-2 - c) * K + k) * K;
-            T acc = T(0);
-#pragma unroll
-            for (int m = 0; m < K; ++m) {
-                const int om = ijp * K + m;
-                acc -= mi[m] * sm.fa[le][om] * (sm.tg[le][om] - sm.tv[le][om] * gp);
-            }
-            sm.com[le][o] = acc;
-        }
-    __syncthreads();
-    // contravariant gradient (src/HO_2D.cpp:2775-2792) and common normal fluxes
-    if (active) {
-        T dx = T(0), de = T(0);
-#pragma unroll
-        for (int d = 0; d < K; ++d) {
-            dx += sm.x[le][j * K + d] * b.D[d * K + i];
-            de += sm.x[le][d * K + i] * b.D[d * K + j];
-        }
-        dx += (sm.com[le][0 * K + j] - sm.tv[le][0 * K + j]) * b.gR[i * 2 + 0];
-        dx += (sm.com[le][1 * K + j] - sm.tv[le][1 * K + j]) * b.gR[i * 2 + 1];
-        de += (sm.com[le][2 * K + i] - sm.tv[le][2 * K + i]) * b.gR[j * 2 + 0];
-        de += (sm.com[le][3 * K + i] - sm.tv[le][3 * K + i]) * b.gR[j * 2 + 1];
-        sm.a[le][ij] = dx * g11 + de * g12;
-        sm.b[le][ij] = de * g22 + dx * g12;
-        for (int o = ij; o < NF; o += K2) {
-            const int ijp = o / K, k = o % K, c = sm.code[le][ijp];
-            if (c <= -2) {
-                sm.cg[le][o] = T(0);
-                continue;
-            }
-            const T com = sm.com[le][o];
-            T cross = T(0);
-#pragma unroll
-            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
-            const T dv = sm.tg[le][o] + (com - sm.tv[le][o]) * b.gp[ijp & 1];
-            const T fl = dv * sm.fa[le][o] - cross * sm.fb[le][o];
-            if (c < 0) {
-                sm.cg[le][o] = fl;
-            } else {
-                const int nijp = c & 3, rev = c >> 2;
-                const int jn = rev ? K - 1 - k : k;
-                T crn = T(0);
-#pragma unroll
-                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
-                const T dvn = sm.ntg[le][o] + (com - sm.ntv[le][o]) * b.gp[nijp & 1];
-                const T fln = dvn * sm.nfa[le][o] - crn * sm.nfb[le][o];
-                sm.cg[le][o] = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
-            }
-        }
-    }
-    __syncthreads();
-    // flux jumps: common flux minus the interior flux extrapolated to the face
-    if (active)
-        for (int o = ij; o < NF; o += K2) {
-            const int ijp = o / K, k = o % K, lr = ijp & 1;
-            T v = sm.cg[le][o];
-            if (ijp < 2) {
-#pragma unroll
-                for (int d = 0; d < K; ++d) v -= sm.a[le][k * K + d] * b.sbb[d * 2 + lr];
-            } else {
-#pragma unroll
-                for (int d = 0; d < K; ++d) v -= sm.b[le][d * K + k] * b.sbb[d * 2 + lr];
-            }
-            sm.cg[le][o] = v;
-        }
-    __syncthreads();
-    if (!active) return T(0);
-    T lap = T(0);
-#pragma unroll
-    for (int d = 0; d < K; ++d) lap += sm.a[le][j * K + d] * b.D[d * K + i];
-    lap += sm.cg[le][0 * K + j] * b.gR[i * 2 + 0] + sm.cg[le][1 * K + j] * b.gR[i * 2 + 1];
-#pragma unroll
-    for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * b.D[d * K + j];
-    lap += sm.cg[le][2 * K + i] * b.gR[j * 2 + 0] + sm.cg[le][3 * K + i] * b.gR[j * 2 + 1];
-    return lap;
-}
-
-// mf_apply for K >= 4, where every face point has a thread of its own (4K <= K^2): the
-// basis values a thread uses (its row and column of D, its Radau derivatives, the
-// extrapolation weights of its face point) and its face point's own data stay in
-// registers, and shared memory carries only what other threads read. Same arithmetic,
-// same order of operations as mf_apply. Collective.
-template <int K, typename T>
-__device__ T mf_apply_1f(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv, const T* __restrict__ tg,
-                         MfShared<K, T>& sm, bool active, int le, int el, int ij) {
-    constexpr int K2 = K * K, NF = 4 * K;
-    static_assert(NF <= K2, "one face point per thread");
-    const PoisGeom<T>& g = op.g;
-    const int j = ij / K, i = ij % K;
-    const bool face = active && ij < NF;
-    const int ijp = ij / K, k = ij % K, lr = ijp & 1;  // this thread's face point (if face)
-    T g11 = T(0), g12 = T(0), g22 = T(0);
-    T fa = T(0), fb = T(0), nfa = T(0), nfb = T(0), ntv = T(0), ntg = T(0);
-    if (active) {
-        const int p = el * K2 + ij;
-        sm.x[le][ij] = x[p];
-        g11 = g.G11[p];
-        g12 = g.G12[p];
-        g22 = g.G22[p];
-        if (face) {
-            const int q = el * NF + ij;
-            fa = g.fa[q];
-            fb = g.fb[q];
-            nfa = g.nfa[q];
-            nfb = g.nfb[q];
-            ntv = tv[q];
-            ntg = tg[q];
-            sm.fa[le][ij] = fa;
-        }
-        if (ij < 4) sm.code[le][ij] = g.code[el * 4 + ij];
-    }
-    stage_bases(sm.bas, op.b);
-    __syncthreads();
-    const DevBases<T>& b = sm.bas;
-    T Di[K], Dj[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) {
-        Di[d] = b.D[d * K + i];
-        Dj[d] = b.D[d * K + j];
-    }
-    const T gRi0 = b.gR[i * 2 + 0], gRi1 = b.gR[i * 2 + 1], gRj0 = b.gR[j * 2 + 0], gRj1 = b.gR[j * 2 + 1];
-    const int c = face ? sm.code[le][ijp] : -1;
-    // own trace and common value (interior: average; Dirichlet: zero)
-    T tvv = T(0), tgv = T(0);
-    if (face) {
-        face_trace<K, T>(sm.x[le], b, ij, tvv, tgv);
-        sm.tv[le][ij] = tvv;
-        sm.tg[le][ij] = tgv;
-        sm.com[le][ij] = c >= 0 ? T(0.5) * (tvv + ntv) : T(0);
-    }
-    __syncthreads();
-    // homogeneous Neumann faces: com = Minv r, r_m = -fa_m (tg_m - tv_m g'(+-1))
-    if (face && c <= -2) {
-        const T gp = b.gp[lr];
-        const T* mi = g.minv + ((size_t)(-2 - c) * K + k) * K;
-        T acc = T(0);
-#pragma unroll
-        for (int m = 0; m < K; ++m) {
-            const int om = ijp * K + m;
-            acc -= mi[m] * sm.fa[le][om] * (sm.tg[le][om] - sm.tv[le][om] * gp);
-        }
-        sm.com[le][ij] = acc;
-    }
-    __syncthreads();
-    // contravariant gradient and this face point's common normal flux (kept in a register)
-    T cg = T(0);
-    if (active) {
-        T dx = T(0), de = T(0);
-#pragma unroll
-        for (int d = 0; d < K; ++d) {
-            dx += sm.x[le][j * K + d] * Di[d];
-            de += sm.x[le][d * K + i] * Dj[d];
-        }
-        dx += (sm.com[le][0 * K + j] - sm.tv[le][0 * K + j]) * gRi0;
-        dx += (sm.com[le][1 * K + j] - sm.tv[le][1 * K + j]) * gRi1;
-        de += (sm.com[le][2 * K + i] - sm.tv[le][2 * K + i]) * gRj0;
-        de += (sm.com[le][3 * K + i] - sm.tv[le][3 * K + i]) * gRj1;
-        sm.a[le][ij] = dx * g11 + de * g12;
-        sm.b[le][ij] = de * g22 + dx * g12;
-        if (face && c > -2) {
-            const T com = sm.com[le][ij];
-            T cross = T(0);
-#pragma unroll
-            for (int m = 0; m < K; ++m) cross += sm.com[le][ijp * K + m] * b.D[m * K + k];
-            const T dv = tgv + (com - tvv) * b.gp[lr];
-            const T fl = dv * fa - cross * fb;
-            if (c < 0) {
-                cg = fl;
-            } else {
-                const int nijp = c & 3, rev = c >> 2;
-                const int jn = rev ? K - 1 - k : k;
-                T crn = T(0);
-#pragma unroll
-                for (int m = 0; m < K; ++m) crn += sm.com[le][ijp * K + (rev ? K - 1 - m : m)] * b.D[m * K + jn];
-                const T dvn = ntg + (com - ntv) * b.gp[nijp & 1];
-                const T fln = dvn * nfa - crn * nfb;
-                cg = T(0.5) * (fl + T(2 * ((ijp + nijp) % 2) - 1) * fln);
-            }
-        }
-    }
-    __syncthreads();
-    // flux jump at this face point: common flux minus the interior flux extrapolated to it
-    if (face) {
-        T v = cg;
-        if (ijp < 2) {
-#pragma unroll
-            for (int d = 0; d < K; ++d) v -= sm.a[le][k * K + d] * b.sbb[d * 2 + lr];
-        } else {
-#pragma unroll
-            for (int d = 0; d < K; ++d) v -= sm.b[le][d * K + k] * b.sbb[d * 2 + lr];
-        }
-        sm.cg[le][ij] = v;
-    }
-    __syncthreads();
-    if (!active) return T(0);
-    T lap = T(0);
-#pragma unroll
-    for (int d = 0; d < K; ++d) lap += sm.a[le][j * K + d] * Di[d];
-    lap += sm.cg[le][0 * K + j] * gRi0 + sm.cg[le][1 * K + j] * gRi1;
-#pragma unroll
-    for (int d = 0; d < K; ++d) lap += sm.b[le][d * K + i] * Dj[d];
-    lap += sm.cg[le][2 * K + i] * gRj0 + sm.cg[le][3 * K + i] * gRj1;
-    return lap;
-}
-
-// y = A x at (el, ij): the register-resident form when every face point has its own
-// thread (K >= 4), the general form otherwise. Collective.
-template <int K, typename T>
-__device__ __forceinline__ T mf_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tv,
-                                      const T* __restrict__ tg, MfShared<K, T>& sm, bool active, int le, int el,
-                                      int ij) {
-    if constexpr (4 * K <= K * K) return mf_apply_1f<K, T>(op, x, tv, tg, sm, active, le, el, ij);
-    else return mf_apply_gen<K, T>(op, x, tv, tg, sm, active, le, el, ij);
-}
-
 // Scatter destinations of the face points thread ij emits (prefetched at kernel start).
 template <int K>
 struct TraceDst {
@@ -395,66 +120,58 @@ __device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, c
     }
 }
 
-// Element sums of a per-point value: every thread of element le stores its value, then
-// thread ij == 0 of each element adds the K^2 values in a fixed order. Collective.
-template <int K, typename T>
-__device__ __forceinline__ void element_sum(T (&buf)[Shape<K>::EPB][Shape<K>::K2], T val, bool active, int le, int ij,
-                                            int el, T* out) {
-    __syncthreads();  // buf may still be read by the phase before
-    if (active) buf[le][ij] = val;
-    __syncthreads();
-    if (active && ij == 0) {
-        T sum = T(0);
-#pragma unroll
-        for (int q = 0; q < Shape<K>::K2; ++q) sum += buf[le][q];
-        out[el] = sum;
-    }
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------- fine-level kernels
+// The operator kernels run row-parallel (rows.cuh): K threads per element, Rows<K>::EPC
+// elements per CTA.
+template <int K>
+static __host__ __device__ constexpr unsigned rgrid_of(int N) {
+    return (unsigned)((N + Rows<K>::EPC - 1) / Rows<K>::EPC);
+}
+
 // incoming face traces of x (the operand of an operator application that no Krylov
 // kernel produced: the initial guess, a refinement iterate, a caller's vector)
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_trace_in(MfOp<T> op, const T* __restrict__ x, T* __restrict__ tv,
-                                                                 T* __restrict__ tg) {
-    using S = Shape<K>;
-    __shared__ T sx[S::EPB][S::K2];
-    __shared__ DevBases<T> sbas;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    TraceDst<K> td;
-    td.load(op.g.scat, active, el, ij);
-    if (active) sx[le][ij] = x[el * S::K2 + ij];
-    stage_bases(sbas, op.b);
-    __syncthreads();
-    emit_traces<K, T>(sx[active ? le : 0], sbas, td, tv, tg, ij);
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_trace_in(MfOp<T> op, const T* __restrict__ x, T* __restrict__ tv,
+                                                                T* __restrict__ tg) {
+    __shared__ T buf[Rows<K>::WARPS][Rows<K>::EPW][K][K];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T row[K];
+    int dst[4];
+    if (ix.active) {
+        load_row<K, T>(x + (size_t)ix.el * K * K + ix.t * K, row);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) dst[f] = op.g.scat[(size_t)ix.el * 4 * K + f * K + ix.t];
+    }
+    row_emit_traces<K, T>(op.b, buf[ix.warp][ix.lw], row, dst, tv, tg, ix.t, ix.active);
 }
 
-
-// r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2
+// r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2; element sums of r
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
-    using S = Shape<K>;
-    __shared__ MfShared<K, T> sm;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const T y = mf_apply<K, T>(op, v.x, v.xtv, v.xtg, sm, active, le, el, ij);
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
+    __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T y[K];
+    row_apply<K, T>(op, v.x, v.xtv, v.xtg, sm[ix.warp], ix, y);
     double part[2] = {0.0, 0.0};
-    T r = T(0);
-    if (active) {
-        const int p = el * S::K2 + ij;
-        const T bb = v.b[p];
-        r = bb - y;
-        v.r[p] = r;
-        v.rhat[p] = r;
-        part[0] = double(r) * double(r);
-        part[1] = double(bb) * double(bb);
+    T rsum = T(0);
+    if (ix.active) {
+        const size_t p = (size_t)ix.el * K * K + ix.t * K;
+        T bb[K], r[K];
+        load_row<K, T>(v.b + p, bb);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            r[i] = bb[i] - y[i];
+            rsum += r[i];
+            part[0] += double(r[i]) * double(r[i]);
+            part[1] += double(bb[i]) * double(bb[i]);
+        }
+        store_row<K, T>(v.r + p, r);
+        store_row<K, T>(v.rhat + p, r);
     }
-    element_sum<K, T>(sm.a, r, active, le, ij, el, v.er);
+    const T tot = element_total<K, T>(rsum, ix.lw);
+    if (ix.active && ix.t == 0) v.er[ix.el] = tot;
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         KrylovScalars* sc = rs.sc;
@@ -479,11 +196,6 @@ __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
     if (i < n) x[i] = T(0);
 }
 
-// Vector kernels take kVecTiles element tiles per CTA (tile blockIdx.x + t * gridDim.x),
-// so the whole vector is covered in one wave of CTAs, and every thread issues its loads
-// before it reads the solve's `done` flag: the addresses are valid whatever the flag
-// says, so the flag's round trip overlaps the data loads.
-constexpr int kVecTiles = 2;
 
 // Part `part` (0..4) of u0 at element c = S0_c . f0 + Q0_c . u1 (a row of the level-0
 // up step): the row entries part, part + 5, ... The first two of each row are loaded
@@ -510,23 +222,92 @@ __device__ __forceinline__ T up0_part(const CoarseOut<T>& co, const F0<T>& f0, i
 
 // The smoother's element data (BS): 0 = inverse blocks in T; 1 = inverse blocks as BF16 bit
 // patterns (FP32 smoother); 2 = Kronecker-sum factors, with the exact blocks only for the
-// elements the fit does not approximate well (FP32 smoother). For BS 0 and 1, whether
-// k_mf_post stages its CTA's inverse blocks (EPB x K^4 values, contiguous in memory) in
-// shared memory: when they fit in 32 KB of static shared memory.
-template <int K, typename T, int BS = 0>
-struct PostStage {
+// elements the fit does not approximate well (FP32 smoother). Each element's data starts on
+// a 16-byte boundary (padded_count). For BS 0 and 1 a warp's EPW blocks are one contiguous
+// span, copied into shared memory by one bulk copy when the span is at most 26 KB (so a
+// CTA's four spans leave room for two CTAs per SM); larger blocks are read from global
+// memory directly.
+template <int K, typename T, int BS>
+struct PostRows {
     using DT = typename std::conditional<BS == 1, unsigned short, T>::type;
-    static constexpr int K4 = K * K * K * K;
-    static constexpr size_t kBytes = (size_t)Shape<K>::EPB * K4 * sizeof(DT) + 32;  // + 16-byte alignment slack
-    static constexpr bool kOn = BS != 2 && kBytes <= 32768;
-    static constexpr int KF = 4 * K * K + 2 * K;  // Kronecker factors per element (BS 2)
-    static constexpr int KE = BS == 2 ? Shape<K>::EPB : 1;
+    static constexpr int K2 = K * K, K4 = K2 * K2;
+    static constexpr int STRIDE = padded_count(K4, (int)sizeof(DT));  // values of DT per element
+    static constexpr int SPAN = Rows<K>::EPW * STRIDE * (int)sizeof(DT);  // bytes per warp
+    static constexpr bool kStage = BS != 2 && SPAN <= 26 * 1024;
+    static constexpr int SMEM = kStage ? Rows<K>::WARPS * SPAN : 0;  // dynamic shared memory
+    static constexpr int KF = 4 * K2 + 2 * K;                      // Kronecker factors per element
+    static constexpr int KFS = padded_count(KF, (int)sizeof(T));
+    static constexpr int XSTRIDE = padded_count(K4, (int)sizeof(T));  // compact exact blocks (BS 2)
 };
 
 __device__ __forceinline__ float block_value(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
 template <typename T>
 __device__ __forceinline__ T block_value(T v) {
     return v;
+}
+
+// K consecutive block values (row t of one r-slice of an element block, [rs][ij] layout),
+// widened to T; vector loads as wide as the slice's alignment allows (its offset is a
+// multiple of K values from a 16-byte-aligned block start).
+template <int K, typename T, typename DT>
+__device__ __forceinline__ void load_slice(const DT* p, T (&v)[K]) {
+    constexpr int AL = (K * (int)sizeof(DT)) % 16 == 0 ? 16 : ((K * (int)sizeof(DT)) % 8 == 0 ? 8 : ((K * (int)sizeof(DT)) % 4 == 0 ? 4 : (int)sizeof(DT)));
+    if constexpr (sizeof(DT) == 2) {
+        if constexpr (AL >= 4) {
+#pragma unroll
+            for (int i = 0; i < K; i += 2) {
+                const unsigned w = *reinterpret_cast<const unsigned*>(p + i);
+                v[i] = __uint_as_float(w << 16);
+                v[i + 1] = __uint_as_float(w & 0xffff0000u);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; ++i) v[i] = block_value(p[i]);
+        }
+    } else if constexpr (AL == 16 && sizeof(DT) == 4) {
+#pragma unroll
+        for (int i = 0; i < K; i += 4) {
+            const float4 q = *reinterpret_cast<const float4*>(p + i);
+            v[i] = q.x;
+            v[i + 1] = q.y;
+            v[i + 2] = q.z;
+            v[i + 3] = q.w;
+        }
+    } else if constexpr (AL >= 8 && sizeof(DT) == 4) {
+#pragma unroll
+        for (int i = 0; i < K; i += 2) {
+            const float2 q = *reinterpret_cast<const float2*>(p + i);
+            v[i] = q.x;
+            v[i + 1] = q.y;
+        }
+    } else if constexpr (AL == 16 && sizeof(DT) == 8) {
+#pragma unroll
+        for (int i = 0; i < K; i += 2) {
+            const double2 q = *reinterpret_cast<const double2*>(p + i);
+            v[i] = q.x;
+            v[i + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; ++i) v[i] = T(p[i]);
+    }
+}
+
+// acc[i] = sum_r blk[r][t K + i] sr[r] over the K^2 values r of the element's residual sr
+// (shared memory): row t of D^-1 sr.
+template <int K, typename T, typename DT>
+__device__ __forceinline__ void block_rows(const DT* blk, const T* sr, int t, T (&acc)[K]) {
+    constexpr int K2 = K * K;
+#pragma unroll
+    for (int i = 0; i < K; ++i) acc[i] = T(0);
+#pragma unroll 4
+    for (int r = 0; r < K2; ++r) {
+        T m[K];
+        load_slice<K, T, DT>(blk + r * K2 + t * K, m);
+        const T s = sr[r];
+#pragma unroll
+        for (int i = 0; i < K; ++i) acc[i] += m[i] * s;
+    }
 }
 
 // Preconditioner application, with the BiCGSTAB vector update that produces its operand:
@@ -537,133 +318,196 @@ __device__ __forceinline__ T block_value(T v) {
 // straight from the coarse cycle (one-level hierarchy), or from the level-0 up step
 // u0 = S0 f0 + Q0 u1 evaluated here as 25 partial sums (five per slot) spread over the
 // element's threads, or is zero (block-Jacobi, no coarse level). Mode 0 also stores the
-// element sums of the new p for the next iteration. Everything that does not depend on u0
-// starts first: the CTA's inverse blocks are copied into shared memory asynchronously
-// (cp.async, 16-byte pieces of the 16-byte-aligned superset of the blocks; the buffer is
-// padded past its end), and the block row sums and the vectors are loaded, so all of it
-// overlaps the up step's dependent loads.
+// element sums of the new p for the next iteration. Row-parallel (rows.cuh): thread t of
+// an element owns row t. The warp's inverse blocks are requested first, by one bulk copy
+// into shared memory (PostRows::kStage), so the copy overlaps the up step's dependent
+// loads and the vector loads.
 template <int K, typename T, int BS = 0>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
-                                                                int has_coarse, double w, ReduceScratch rs, int mode) {
-    using S = Shape<K>;
-    using PS = PostStage<K, T, BS>;
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
+                                                               int has_coarse, double w, ReduceScratch rs, int mode) {
+    using R = Rows<K>;
+    using PS = PostRows<K, T, BS>;
     using DT = typename PS::DT;
-    constexpr int K2 = S::K2;
+    constexpr int K2 = R::K2, EPW = R::EPW;
     KrylovScalars* sc = rs.sc;
     const int done = sc->done;  // uniform; read early so the round trip overlaps the loads
-    __shared__ T sr[S::EPB][K2], sz[S::EPB][K2], pu[S::EPB][25], ue[S::EPB][5];
-    __shared__ DevBases<T> sbas;
-    __shared__ __align__(16) unsigned char sd_raw[PS::kOn ? PS::kBytes : 16];
-    __shared__ T kf[PS::KE][BS == 2 ? PS::KF : 1], kt[PS::KE][BS == 2 ? K2 : 1], kz[PS::KE][BS == 2 ? K2 : 1];
-    const int le = threadIdx.x / K2, ij = threadIdx.x % K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const int p = el * K2 + ij;
+    extern __shared__ __align__(128) unsigned char post_dyn[];
+    __shared__ __align__(8) uint64_t bar[R::WARPS];
+    __shared__ T pu[R::WARPS][EPW][25];
+    __shared__ __align__(16) T sr[R::WARPS][EPW][K2];
+    __shared__ T zb[R::WARPS][EPW][K][K];
+    __shared__ __align__(16) T kf[BS == 2 ? R::WARPS : 1][BS == 2 ? EPW : 1][BS == 2 ? PS::KFS : 1];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    const int t = ix.t, lw = ix.lw, el = ix.el;
+    const bool act = ix.active;
     const DT* dsrc;
     if constexpr (BS == 1) dsrc = op.dinv_bf16;
     else dsrc = op.dinv;
-    const DT* dblk = dsrc + (size_t)el * PS::K4;  // this element's inverse block ([rs][ij])
-    if constexpr (PS::kOn) {
-        const int el0 = blockIdx.x * S::EPB;
-        const int el1 = min(el0 + S::EPB, op.g.N);
-        const size_t b0 = (size_t)el0 * PS::K4 * sizeof(DT), b1 = (size_t)el1 * PS::K4 * sizeof(DT);
-        const size_t a0 = b0 & ~size_t(15), a1 = (b1 + 15) & ~size_t(15);
-        const char* g = reinterpret_cast<const char*>(dsrc) + a0;
-        const unsigned sb = (unsigned)__cvta_generic_to_shared(sd_raw);
-        const unsigned nbytes = (unsigned)(a1 - a0);  // < 32 KB
-        for (unsigned o = 16u * threadIdx.x; o < nbytes; o += 16u * blockDim.x)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + o), "l"(g + o) : "memory");
-        dblk = reinterpret_cast<const DT*>(sd_raw + (b0 - a0)) + (size_t)le * PS::K4;
+    // this warp's blocks: one bulk copy, issued before anything else
+    const int wel0 = (blockIdx.x * R::WARPS + ix.warp) * EPW;
+    const int wn = min(EPW, op.g.N - wel0);  // elements of this warp (<= 0: none)
+    const DT* blk = dsrc + (size_t)el * PS::STRIDE;
+    if constexpr (PS::kStage) {
+        DT* stage = reinterpret_cast<DT*>(post_dyn + (size_t)ix.warp * PS::SPAN);
+        if (!done && wn > 0 && ix.lane == 0) {
+            mbar_init(&bar[ix.warp]);
+            const unsigned bytes = (unsigned)(wn * PS::STRIDE * (int)sizeof(DT));
+            mbar_arrive_expect(&bar[ix.warp], bytes);
+            bulk_load(stage, dsrc + (size_t)wel0 * PS::STRIDE, bytes, &bar[ix.warp]);
+        }
+        blk = stage + (size_t)lw * PS::STRIDE;
     }
-    TraceDst<K> td;
-    td.load(op.g.scat, active, el, ij);
-    T rsum[5], rr = T(0), pp = T(0), vv = T(0);
-    if (active) {
+    // this thread's rows of the vectors and block row sums, its face points' destinations
+    const size_t p = (size_t)el * K2 + t * K;
+    T rr[K], vv[K], pp[K], rsum[5][K];
+    int dst[4];
+    if (act) {
+        load_row<K, T>(v.r + p, rr);
+        load_row<K, T>(v.v + p, vv);
+        if (mode == 0) load_row<K, T>(v.p + p, pp);
 #pragma unroll
-        for (int s = 0; s < 5; ++s) rsum[s] = op.rowsum[((size_t)el * 5 + s) * K2 + ij];
-        rr = v.r[p];
-        vv = v.v[p];
-        if (mode == 0) pp = v.p[p];
+        for (int s = 0; s < 5; ++s) load_row<K, T>(op.rowsum + ((size_t)el * 5 + s) * K2 + t * K, rsum[s]);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) dst[f] = op.g.scat[(size_t)el * 4 * K + f * K + t];
     }
     int kx = -1;  // BS 2: this element's exact block, or -1 for its Kronecker factors
     if constexpr (BS == 2) {
-        if (active) {
+        if (act) {
             kx = op.kron_x[el];
-            for (int q = ij; q < PS::KF; q += K2) kf[le][q] = op.kron_f[(size_t)el * PS::KF + q];
+            for (int q = t; q < PS::KF; q += K) kf[ix.warp][lw][q] = op.kron_f[(size_t)el * PS::KFS + q];
         }
     }
-    stage_bases(sbas, op.b);
     const F0<T> f0 = f0_of(v, sc, mode);
     // u0 of block slot s (element bcol[5 el + s]) as five partial sums pu[s][part]
-    if (active)
-        for (int t = ij; t < 25; t += K2) {
-            const int slot = t / 5, part = t % 5;
+    if (act)
+        for (int q = t; q < 25; q += K) {
+            const int slot = q / 5, part = q % 5;
             const int c = op.bcol[el * 5 + slot];
             T u = T(0);
             if (c >= 0 && has_coarse) u = co.u0 ? (part == 0 ? co.u0[c] : T(0)) : up0_part(co, f0, c, part);
-            pu[le][t] = u;
+            pu[ix.warp][lw][q] = u;
         }
-    if (mode == 0 && has_coarse && active && ij == 0) v.ep[(sc->it + 1) & 1][el] = f0[el];
+    if (mode == 0 && has_coarse && act && t == 0) v.ep[(sc->it + 1) & 1][el] = f0[el];
     // the operand: p or s
-    T f;
+    T f[K];
     if (mode == 0) {
         if (sc->it == 0) {
-            f = rr;
+#pragma unroll
+            for (int i = 0; i < K; ++i) f[i] = rr[i];
         } else {
             const double beta = (sc->rho / sc->rho_old) * (sc->alpha / sc->omega);
-            f = rr + T(beta) * (pp - T(sc->omega) * vv);
+            const T om = T(sc->omega);
+#pragma unroll
+            for (int i = 0; i < K; ++i) f[i] = rr[i] + T(beta) * (pp[i] - om * vv[i]);
         }
     } else {
-        f = rr - T(sc->alpha) * vv;
-    }
-    if (active && !done) {
-        if (mode == 0) v.p[p] = f;
-        else v.s[p] = f;
-    }
-    if constexpr (PS::kOn) asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
-    if (done) return;
-    // the five slot values, each the sum of its five parts (part 0..4 in order)
-    if (active)
-        for (int q = ij; q < 5; q += K2)  // K^2 < 5 threads per element for K <= 2
-            ue[le][q] = pu[le][5 * q] + pu[le][5 * q + 1] + pu[le][5 * q + 2] + pu[le][5 * q + 3] + pu[le][5 * q + 4];
-    __syncthreads();
-    T u_self = T(0);
-    if (active) {
-        T ae = T(0);
+        const T al = T(sc->alpha);
 #pragma unroll
-        for (int s = 0; s < 5; ++s) ae += rsum[s] * ue[le][s];
-        u_self = ue[le][0];
-        sr[le][ij] = f - ae;
+        for (int i = 0; i < K; ++i) f[i] = rr[i] - al * vv[i];
     }
-    __syncthreads();
-    T* z = mode == 0 ? v.ph : v.sh;
-    T acc = T(0);
-    if constexpr (BS == 2) {
-        // the exact block where the fit falls back (read before the body reuses sr), then
-        // the Kronecker-sum step for the other elements; every thread passes the body's
-        // barriers
-        if (active && kx >= 0) {
-            const T* blk = op.kron_exact + (size_t)kx * PS::K4;
-            for (int r = 0; r < K2; ++r) acc += blk[r * K2 + ij] * sr[le][r];
+    if (done) return;  // uniform over the grid: no copy was issued
+    if (act) store_row<K, T>((mode == 0 ? v.p : v.s) + p, f);
+    __syncwarp();
+    // the five slot values, each the sum of its five parts (part 0..4 in order), and the
+    // smoother's residual row f - A e
+    T ue[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const T* pq = pu[ix.warp][lw] + 5 * q;
+        ue[q] = pq[0] + pq[1] + pq[2] + pq[3] + pq[4];
+    }
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            T ae = T(0);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) ae += rsum[s][i] * ue[s];
+            sr[ix.warp][lw][t * K + i] = f[i] - ae;
         }
-        const int lei = active ? le : 0;
-        const ElemCtx<K2> ec{ij};
-        kron_apply_body<K, T>(ec, active && kx < 0, kf[lei], kf[lei] + 4 * K2, sr[lei], kt[lei], kz[lei]);
-        if (active && kx < 0) acc = kz[le][ij];
-    } else if (active) {
+    }
+    __syncwarp();
+    if constexpr (PS::kStage) {
+        if (wn > 0 && !mbar_wait_bounded(&bar[ix.warp], 0, kBulkWaitPolls)) {
+            // record the failure for the host and give the copy a second bounded wait; the
+            // kernel then runs to its end so the grid-wide reduction stays consistent
+            if (ix.lane == 0) atomicExch(&sc->dev_error, 1);
+            mbar_wait_bounded(&bar[ix.warp], 0, kBulkWaitPolls);
+        }
+    }
+    T* z = mode == 0 ? v.ph : v.sh;
+    const T* srow = sr[ix.warp][lw];
+    T acc[K];
+    if constexpr (BS == 2) {
+        // exact block where the fit falls back, Kronecker-sum step (fast diagonalisation,
+        // the element body of kron_apply.cuh by rows) for the others; the transposes are
+        // warp-collective, so every lane runs them
+        const bool kr = act && kx < 0;
+        if (act && kx >= 0) block_rows<K, T, T>(op.kron_exact + (size_t)kx * PS::XSTRIDE, srow, t, acc);
+        const T* fk = kf[ix.warp][lw];
+        const T *vx = fk, *vxi = fk + K2, *vy = fk + 2 * K2, *vyi = fk + 3 * K2, *lx = fk + 4 * K2, *ly = lx + K;
+        T c1[K], r1[K], r2[K], c2[K], c3[K], r3[K];
+        // column t of Vy^-1 R
 #pragma unroll
-        for (int r = 0; r < K2; ++r) acc += T(block_value(dblk[r * K2 + ij])) * sr[le][r];
+        for (int j = 0; j < K; ++j) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) s += vyi[j * K + l] * srow[l * K + t];
+            }
+            c1[j] = s;
+        }
+        col_to_row<K, T>(zb[ix.warp][lw], c1, r1, t, kr);
+        // row t of (Vy^-1 R Vx^-T) ./ (ly_t + lx_i)
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) s += r1[k] * vxi[i * K + k];
+                s = s / (ly[t] + lx[i]);
+            }
+            r2[i] = s;
+        }
+        __syncwarp();  // zb is rewritten next
+        rows_to_col<K, T>(zb[ix.warp][lw], r2, c2, t, kr);
+        // column t of Vy (that), then row t of the product with Vx^T
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) s += vy[j * K + l] * c2[l];
+            }
+            c3[j] = s;
+        }
+        __syncwarp();
+        col_to_row<K, T>(zb[ix.warp][lw], c3, r3, t, kr);
+        if (kr) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                T s = T(0);
+#pragma unroll
+                for (int k = 0; k < K; ++k) s += r3[k] * vx[i * K + k];
+                acc[i] = s;
+            }
+        }
+        __syncwarp();  // zb is the trace buffer below
+    } else {
+        if (act) block_rows<K, T, DT>(blk, srow, t, acc);
     }
-    if (active) {
-        const T zz = u_self + T(w) * acc;
-        z[p] = zz;
-        sz[le][ij] = zz;
+    T zz[K];
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) zz[i] = ue[0] + T(w) * acc[i];
+        store_row<K, T>(z + p, zz);
     }
-    __syncthreads();
-    emit_traces<K, T>(sz[active ? le : 0], sbas, td, v.tv, v.tg, ij);
+    row_emit_traces<K, T>(op.b, zb[ix.warp][lw], zz, dst, v.tv, v.tg, t, act);
     if (mode == 1) {
-        double part[1] = {active ? double(f) * double(f) : 0.0};
+        double part[1] = {0.0};
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) part[0] += double(f[i]) * double(f[i]);
+        }
         double out[1];
         if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
             sc->snorm2 = out[0];
@@ -672,27 +516,33 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_post(MfOp<T> op, BicgV
     }
 }
 
-// v = A ph; alpha = rho / (rhat, v)
+// v = A ph; alpha = rho / (rhat, v); element sums of v
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
-    using S = Shape<K>;
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
     // read before the operator's loads so the round trips overlap; the flag is uniform
     // over the grid (only this kernel's last CTA writes it, after every CTA has read it)
     const int done = sc->done;
-    __shared__ MfShared<K, T> sm;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const T y = mf_apply<K, T>(op, v.ph, v.tv, v.tg, sm, active, le, el, ij);
+    __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T y[K];
+    row_apply<K, T>(op, v.ph, v.tv, v.tg, sm[ix.warp], ix, y);
     if (done) return;
     double part[1] = {0.0};
-    if (active) {
-        const int p = el * S::K2 + ij;
-        v.v[p] = y;
-        part[0] = double(v.rhat[p]) * double(y);
+    T ysum = T(0);
+    if (ix.active) {
+        const size_t p = (size_t)ix.el * K * K + ix.t * K;
+        T rh[K];
+        load_row<K, T>(v.rhat + p, rh);
+        store_row<K, T>(v.v + p, y);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            ysum += y[i];
+            part[0] += double(rh[i]) * double(y[i]);
+        }
     }
-    element_sum<K, T>(sm.a, y, active, le, ij, el, v.ev);
+    const T tot = element_total<K, T>(ysum, ix.lw);
+    if (ix.active && ix.t == 0) v.ev[ix.el] = tot;
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         if (out[0] == 0.0 || sc->rho == 0.0) {
@@ -706,22 +556,25 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_v(MfOp<T> op, BicgVect
 
 // t = A sh; omega = (t, s) / (t, t)
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
-    using S = Shape<K>;
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
     const bool skip = sc->done || sc->s_exit;  // read early: the round trip overlaps the operator's loads
-    __shared__ MfShared<K, T> sm;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const T y = mf_apply<K, T>(op, v.sh, v.tv, v.tg, sm, active, le, el, ij);
+    __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T y[K];
+    row_apply<K, T>(op, v.sh, v.tv, v.tg, sm[ix.warp], ix, y);
     if (skip) return;
     double part[2] = {0.0, 0.0};
-    if (active) {
-        const int p = el * S::K2 + ij;
-        v.t[p] = y;
-        part[0] = double(y) * double(v.s[p]);
-        part[1] = double(y) * double(y);
+    if (ix.active) {
+        const size_t p = (size_t)ix.el * K * K + ix.t * K;
+        T sv[K];
+        load_row<K, T>(v.s + p, sv);
+        store_row<K, T>(v.t + p, y);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            part[0] += double(y[i]) * double(sv[i]);
+            part[1] += double(y[i]) * double(y[i]);
+        }
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0)
@@ -735,29 +588,22 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_t(MfOp<T> op, BicgVect
 // not done). Every CTA reads `done` and `s_exit` before any CTA arrives at the counter,
 // so the last CTA may change them. Every body execution either increments `it` (capped at
 // max_iter) or finds `done` set and clears the condition, so the device loop always ends.
+// Each thread updates one element row; its loads are issued before the flag is read.
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
-                                                                  int max_iter, cudaGraphConditionalHandle h,
-                                                                  int has_handle) {
-    using S = Shape<K>;
-    constexpr int NT = kVecTiles;
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
+                                                                 int max_iter, cudaGraphConditionalHandle h,
+                                                                 int has_handle) {
     KrylovScalars* sc = rs.sc;
-    __shared__ T sr[S::EPB][S::K2];
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    int p[NT], el[NT];
-    bool act[NT];
-    T x[NT], ph[NT], sh[NT], sv[NT], tv[NT], rh[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        el[t] = (blockIdx.x + t * gridDim.x) * S::EPB + le;
-        act[t] = le < S::EPB && el[t] < N;
-        p[t] = el[t] * S::K2 + ij;
-        x[t] = act[t] ? v.x[p[t]] : T(0);
-        ph[t] = act[t] ? v.ph[p[t]] : T(0);
-        sh[t] = act[t] ? v.sh[p[t]] : T(0);
-        sv[t] = act[t] ? v.s[p[t]] : T(0);
-        tv[t] = act[t] ? v.t[p[t]] : T(0);
-        rh[t] = act[t] ? v.rhat[p[t]] : T(0);
+    const RowIdx<K> ix(N, blockIdx.x);
+    const size_t p = (size_t)ix.el * K * K + ix.t * K;
+    T x[K], ph[K], sh[K], sv[K], tv[K], rh[K];
+    if (ix.active) {
+        load_row<K, T>(v.x + p, x);
+        load_row<K, T>(v.ph + p, ph);
+        load_row<K, T>(v.sh + p, sh);
+        load_row<K, T>(v.s + p, sv);
+        load_row<K, T>(v.t + p, tv);
+        load_row<K, T>(v.rhat + p, rh);
     }
     if (sc->done) {  // the solve ended earlier in this body (breakdown)
         if (has_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
@@ -767,19 +613,29 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_xr_update(int N, BicgVect
     const bool s_exit = sc->s_exit;
     const double omega = sc->omega;
     double part[2] = {0.0, 0.0};
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-        T r = T(0);
+    T rsum = T(0);
+    if (ix.active) {
         if (s_exit) {
-            if (act[t]) v.x[p[t]] = x[t] + alpha * ph[t];
-        } else if (act[t]) {
-            v.x[p[t]] = x[t] + (alpha * ph[t] + T(omega) * sh[t]);
-            r = sv[t] - T(omega) * tv[t];
-            v.r[p[t]] = r;
-            part[0] += double(r) * double(r);
-            part[1] += double(rh[t]) * double(r);
+#pragma unroll
+            for (int i = 0; i < K; ++i) x[i] = x[i] + alpha * ph[i];
+            store_row<K, T>(v.x + p, x);
+        } else {
+            T r[K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                x[i] = x[i] + (alpha * ph[i] + T(omega) * sh[i]);
+                r[i] = sv[i] - T(omega) * tv[i];
+                rsum += r[i];
+                part[0] += double(r[i]) * double(r[i]);
+                part[1] += double(rh[i]) * double(r[i]);
+            }
+            store_row<K, T>(v.x + p, x);
+            store_row<K, T>(v.r + p, r);
         }
-        if (!s_exit) element_sum<K, T>(sr, r, act[t], le, ij, el[t], v.er);
+    }
+    if (!s_exit) {
+        const T tot = element_total<K, T>(rsum, ix.lw);
+        if (ix.active && ix.t == 0) v.er[ix.el] = tot;
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -803,23 +659,26 @@ __global__ void k_set_loop(const KrylovScalars* sc, cudaGraphConditionalHandle h
 
 // r = b - A x (FP64 refinement residual); ||r||^2 -> rnorm2, ||b||^2 -> bnorm2
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_residual(MfOp<T> op, const double* __restrict__ b,
-                                                                    const T* __restrict__ x, const T* __restrict__ xtv,
-                                                                    const T* __restrict__ xtg, double* __restrict__ r,
-                                                                    ReduceScratch rs) {
-    using S = Shape<K>;
-    __shared__ MfShared<K, T> sm;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const T y = mf_apply<K, T>(op, x, xtv, xtg, sm, active, le, el, ij);
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_residual(MfOp<T> op, const double* __restrict__ b,
+                                                                   const T* __restrict__ x, const T* __restrict__ xtv,
+                                                                   const T* __restrict__ xtg, double* __restrict__ r,
+                                                                   ReduceScratch rs) {
+    __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T y[K];
+    row_apply<K, T>(op, x, xtv, xtg, sm[ix.warp], ix, y);
     double part[2] = {0.0, 0.0};
-    if (active) {
-        const int p = el * S::K2 + ij;
-        const double rr = b[p] - double(y);
-        r[p] = rr;
-        part[0] = rr * rr;
-        part[1] = b[p] * b[p];
+    if (ix.active) {
+        const size_t p = (size_t)ix.el * K * K + ix.t * K;
+        double bb[K], rr[K];
+        load_row<K, double>(b + p, bb);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            rr[i] = bb[i] - double(y[i]);
+            part[0] += rr[i] * rr[i];
+            part[1] += bb[i] * bb[i];
+        }
+        store_row<K, double>(r + p, rr);
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -830,16 +689,73 @@ __global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_residual(MfOp<T> op, c
 
 // y = A x (operator only)
 template <int K, typename T>
-__global__ void __launch_bounds__(Shape<K>::THREADS) k_mf_apply(MfOp<T> op, const T* __restrict__ x,
-                                                                 const T* __restrict__ xtv, const T* __restrict__ xtg,
-                                                                 T* __restrict__ y) {
-    using S = Shape<K>;
-    __shared__ MfShared<K, T> sm;
-    const int le = threadIdx.x / S::K2, ij = threadIdx.x % S::K2;
-    const int el = blockIdx.x * S::EPB + le;
-    const bool active = le < S::EPB && el < op.g.N;
-    const T yy = mf_apply<K, T>(op, x, xtv, xtg, sm, active, le, el, ij);
-    if (active) y[el * S::K2 + ij] = yy;
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_apply(MfOp<T> op, const T* __restrict__ x,
+                                                                const T* __restrict__ xtv, const T* __restrict__ xtg,
+                                                                T* __restrict__ y) {
+    __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    T yy[K];
+    row_apply<K, T>(op, x, xtv, xtg, sm[ix.warp], ix, yy);
+    if (ix.active) store_row<K, T>(y + (size_t)ix.el * K * K + ix.t * K, yy);
+}
+
+// ---------------------------------------------------------------- FP64 refinement on the device
+// The mixed-precision solve as one graph: FP64 residual, then while the refinement
+// continues { FP32 right-hand side, inner BiCGSTAB (its own while node), psi += x,
+// FP64 residual }. k_refine_ctl decides after every FP64 residual, with the rule the
+// host loop uses: stop on a non-finite or zero residual norm, at the target or at the
+// sweep cap; otherwise ask the inner solve for max(inner_tol, 0.3 target / current)
+// relative reduction (at most 0.5), so the last sweep does not overshoot.
+__global__ void k_refine_begin(KrylovScalars* sc) {
+    sc->sweeps = 0;
+    sc->iters_total = 0;
+    sc->zero_psi = 0;
+    sc->finite = 1;
+}
+
+__global__ void k_refine_ctl(KrylovScalars* sc, cudaGraphConditionalHandle h) {
+    const double bn = sc->bnorm2, rn = sc->rnorm2;
+    const bool fin = isfinite(bn) && isfinite(rn);
+    double res = bn > 0.0 ? sqrt(rn / bn) : 0.0;
+    bool stop = !fin;
+    if (fin && bn == 0.0) {
+        sc->zero_psi = 1;
+        res = 0.0;
+        stop = true;
+    }
+    if (!stop && (rn <= sc->tol_outer * sc->tol_outer * bn || sc->sweeps >= sc->max_sweeps)) stop = true;
+    sc->res = res;
+    sc->finite = fin;
+    if (!stop) {
+        const double need = 0.3 * sc->tol_outer / res;
+        sc->tol = fmin(0.5, fmax(sc->inner_tol, need));
+        sc->sweeps += 1;
+    }
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+// right-hand side of the inner solve (the FP64 residual rounded to FP32) and its zero
+// initial guess
+__global__ void k_refine_prep(const double* __restrict__ r, float* __restrict__ b, float* __restrict__ x, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        b[i] = (float)r[i];
+        x[i] = 0.f;
+    }
+}
+
+// psi += x; the inner iterations are added to the solve's total
+__global__ void k_refine_axpy(const float* __restrict__ e, double* __restrict__ x, size_t n, KrylovScalars* sc) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += (double)e[i];
+    if (i == 0) sc->iters_total += sc->it;
+}
+
+// a zero right-hand side gives psi = 0
+__global__ void k_refine_finish(double* __restrict__ x, size_t n, const KrylovScalars* sc) {
+    if (!sc->zero_psi) return;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = 0.0;
 }
 
 __global__ void k_d2f(const double* a, float* b, size_t n) {
@@ -865,10 +781,6 @@ __global__ void k_axpy_f2d(const float* e, double* x, size_t n) {
         default: return cudaErrorInvalidValue;             \
     }
 
-template <int K>
-static unsigned kgrid(int N) {
-    return (unsigned)((N + Shape<K>::EPB - 1) / Shape<K>::EPB);
-}
 
 int krylov_max_blocks(int K, int N) {
     const int k2 = K * K;
@@ -880,8 +792,8 @@ template <typename T>
 cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs,
                         cudaStream_t s) {
     const int N = op.g.N;
-    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v.x, v.xtv, v.xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<kgrid<KK>(N), Shape<KK>::THREADS, 0, s>>>(op, v, rs)));
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<rgrid_of<KK>(N), Rows<KK>::THREADS, 0, s>>>(op, v.x, v.xtv, v.xtg)));
+    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<rgrid_of<KK>(N), Rows<KK>::THREADS, 0, s>>>(op, v, rs)));
     const size_t n = (size_t)N * op.K * op.K;
     k_zero_if<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v.x, n, rs.sc);
     return cudaGetLastError();
@@ -890,35 +802,72 @@ cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const Reduce
 // One BiCGSTAB iteration: [coarse cycle on P^T p] -> p update + smoothing (ph) -> v = A ph
 // -> [coarse cycle on P^T s] -> s update + smoothing (sh) -> t = A sh -> x, r update and
 // loop control.
+// With ev (8 events) the boundaries between the launches are recorded on the stream:
+// ev[0] coarse ev[1] smoothing ev[2] operator ev[3] coarse ev[4] smoothing ev[5] operator
+// ev[6] update ev[7].
 template <int K, typename T>
 static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
-                           const Precond<T>& pc, cudaGraphConditionalHandle h, int has_handle, cudaStream_t s) {
+                           const Precond<T>& pc, cudaGraphConditionalHandle h, int has_handle, cudaStream_t s,
+                           cudaEvent_t* ev = nullptr) {
+    auto mark = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], s);
+    };
     const int N = op.g.N;
-    const unsigned g = kgrid<K>(N);
-    constexpr int th = Shape<K>::THREADS;
     const int mg = pc.nlev > 0;
     const CoarseOut<T> co = mg ? coarse_out(pc) : CoarseOut<T>();
-    const unsigned gv = (g + kVecTiles - 1) / kVecTiles;
+    const unsigned gp = rgrid_of<K>(N);
+    constexpr int tp = Rows<K>::THREADS;
     auto post = [&](int mode) {
         if constexpr (std::is_same<T, float>::value) {
             if (op.kron_f) {
-                k_mf_post<K, T, 2><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                k_mf_post<K, T, 2><<<gp, tp, PostRows<K, T, 2>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
                 return;
             }
             if (op.dinv_bf16) {
-                k_mf_post<K, T, 1><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                k_mf_post<K, T, 1><<<gp, tp, PostRows<K, T, 1>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
                 return;
             }
         }
-        k_mf_post<K, T><<<g, th, 0, s>>>(op, v, co, mg, pc.omega, rs, mode);
+        k_mf_post<K, T, 0><<<gp, tp, PostRows<K, T, 0>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
     };
+    const unsigned gr = rgrid_of<K>(N);
+    mark(0);
     if (mg) coarse_cycle<T>(pc, v, rs.sc, 0, s);
+    mark(1);
     post(0);
-    k_mf_v<K, T><<<g, th, 0, s>>>(op, v, rs);
+    mark(2);
+    k_mf_v<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    mark(3);
     if (mg) coarse_cycle<T>(pc, v, rs.sc, 1, s);
+    mark(4);
     post(1);
-    k_mf_t<K, T><<<g, th, 0, s>>>(op, v, rs);
-    k_xr_update<K, T><<<gv, th, 0, s>>>(N, v, rs, max_iter, h, has_handle);
+    mark(5);
+    k_mf_t<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    mark(6);
+    k_xr_update<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(N, v, rs, max_iter, h, has_handle);
+    mark(7);
+}
+
+// Dynamic shared memory of the smoothing kernels that stage their blocks (above the
+// 48 KB a launch gets without asking); once per device before the first launch or capture.
+template <int K>
+static cudaError_t configure_post() {
+    cudaError_t e = cudaSuccess;
+    auto one = [&](auto kern, int bytes) {
+        if (e == cudaSuccess && bytes > 0)
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    };
+    one(k_mf_post<K, double, 0>, PostRows<K, double, 0>::SMEM);
+    one(k_mf_post<K, float, 0>, PostRows<K, float, 0>::SMEM);
+    one(k_mf_post<K, float, 1>, PostRows<K, float, 1>::SMEM);
+    one(k_mf_post<K, float, 2>, PostRows<K, float, 2>::SMEM);
+    return e;
+}
+
+cudaError_t krylov_configure(int K) {
+    cudaError_t e = cudaSuccess;
+    HO2D_KSWITCH(K, (e = configure_post<KK>()));
+    return e;
 }
 
 template <typename T>
@@ -930,6 +879,13 @@ template <typename T>
 cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                              const Precond<T>& pc, cudaStream_t s) {
     HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, cudaGraphConditionalHandle(), 0, s)));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t krylov_iteration_timed(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
+                                   const Precond<T>& pc, cudaEvent_t* ev, cudaStream_t s) {
+    HO2D_KSWITCH(op.K, (iteration_impl<KK, T>(op, v, rs, max_iter, pc, cudaGraphConditionalHandle(), 0, s, ev)));
     return cudaGetLastError();
 }
 
@@ -974,26 +930,106 @@ cudaError_t krylov_capture_solve(const MfOp<T>& op, const BicgVectors<T>& v, con
     return cudaGetLastError();
 }
 
+// Captures a whole mixed-precision solve (FP64 refinement around the FP32 BiCGSTAB) into
+// `*graph_out`: the refinement loop and each sweep's BiCGSTAB loop are nested while nodes
+// whose conditions are set on the device, so a solve is one graph launch and no host
+// round trip. psi64 is updated in place; rhs, the FP64 residual r64 and the FP64 traces
+// (xtv64, xtg64) are the refinement's vectors; v32 holds the inner solve's (v32.b is the
+// inner right-hand side, v32.x its solution).
+cudaError_t krylov_capture_refined_solve(const MfOp<double>& A64, const MfOp<float>& A32,
+                                         const BicgVectors<float>& v32, const ReduceScratch& rs, int max_iter,
+                                         const Precond<float>& pc, double* psi64, const double* rhs, double* r64,
+                                         double* xtv64, double* xtg64, cudaStream_t s, cudaGraph_t* graph_out) {
+    const size_t n = (size_t)A64.g.N * A64.K * A64.K;
+    const unsigned gn = (unsigned)((n + 255) / 256);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle ho, hi;
+    if ((e = cudaGraphConditionalHandleCreate(&ho, g, 0, 0)) != cudaSuccess) return e;
+    if ((e = cudaGraphConditionalHandleCreate(&hi, g, 0, 0)) != cudaSuccess) return e;
+    // adds a while node on handle h after the capture's current dependencies and returns
+    // its body graph; the stream's capture continues after the node
+    auto add_while = [&](cudaGraphConditionalHandle h, cudaGraph_t* body) -> cudaError_t {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraph_t cg = nullptr;
+        cudaError_t err = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &ndeps);
+        if (err != cudaSuccess) return err;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if ((err = cudaGraphAddNode(&node, cg, deps, ndeps, &cp)) != cudaSuccess) return err;
+        if ((err = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+            return err;
+        *body = cp.conditional.phGraph_out[0];
+        return cudaSuccess;
+    };
+    // top level: reset, FP64 residual, decision, the refinement loop, zero-rhs fix-up
+    if ((e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    k_refine_begin<<<1, 1, 0, s>>>(rs.sc);
+    mf_residual<double>(A64, rhs, psi64, xtv64, xtg64, r64, rs, s);
+    k_refine_ctl<<<1, 1, 0, s>>>(rs.sc, ho);
+    cudaGraph_t outer = nullptr;
+    if ((e = add_while(ho, &outer)) != cudaSuccess) return e;
+    k_refine_finish<<<gn, 256, 0, s>>>(psi64, n, rs.sc);
+    if ((e = cudaStreamEndCapture(s, &g)) != cudaSuccess) return e;
+    // one refinement sweep
+    if ((e = cudaStreamBeginCaptureToGraph(s, outer, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    k_refine_prep<<<gn, 256, 0, s>>>(r64, const_cast<float*>(v32.b), v32.x, n);
+    krylov_init<float>(A32, v32, rs, s);
+    k_set_loop<<<1, 1, 0, s>>>(rs.sc, hi);
+    cudaGraph_t inner = nullptr;
+    if ((e = add_while(hi, &inner)) != cudaSuccess) return e;
+    k_refine_axpy<<<gn, 256, 0, s>>>(v32.x, psi64, n, rs.sc);
+    mf_residual<double>(A64, rhs, psi64, xtv64, xtg64, r64, rs, s);
+    k_refine_ctl<<<1, 1, 0, s>>>(rs.sc, ho);
+    if ((e = cudaStreamEndCapture(s, &outer)) != cudaSuccess) return e;
+    // one BiCGSTAB iteration
+    if ((e = cudaStreamBeginCaptureToGraph(s, inner, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return e;
+    HO2D_KSWITCH(A32.K, (iteration_impl<KK, float>(A32, v32, rs, max_iter, pc, hi, 1, s)));
+    if ((e = cudaStreamEndCapture(s, &inner)) != cudaSuccess) return e;
+    *graph_out = g;
+    return cudaGetLastError();
+}
+
+// kernel launches of one captured refined solve: begin, residual, decision and fix-up, then
+// per sweep right-hand side, initial residual (3), loop set-up, update, residual and
+// decision, plus the inner iterations
+int krylov_refined_launches(int sweeps, int inner_iters, const Precond<float>& pc) {
+    return 5 + sweeps * 9 + inner_iters * krylov_launches_per_iteration(pc);
+}
+
 template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
                         const ReduceScratch& rs, cudaStream_t s) {
-    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
+    HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
                                                                                                   rs)));
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t mf_apply_op(const MfOp<T>& op, const T* x, T* xtv, T* xtg, T* y, cudaStream_t s) {
-    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
+    HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
+    HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t mf_apply_only(const MfOp<T>& op, const T* x, const T* xtv, const T* xtg, T* y, int reps, cudaStream_t s) {
     for (int r = 0; r < reps; ++r)
-        HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<kgrid<KK>(op.g.N), Shape<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
+        HO2D_KSWITCH(op.K, (k_mf_apply<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, x, xtv, xtg, y)));
     return cudaGetLastError();
 }
 
@@ -1012,6 +1048,8 @@ cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s)
     template cudaError_t krylov_iteration<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, int,    \
                                              const Precond<T>&, cudaStream_t);                                    \
     template int krylov_launches_per_iteration<T>(const Precond<T>&);                                             \
+    template cudaError_t krylov_iteration_timed<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,   \
+                                                   int, const Precond<T>&, cudaEvent_t*, cudaStream_t);           \
     template cudaError_t krylov_capture_solve<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,     \
                                                  int, const Precond<T>&, cudaStream_t, cudaGraph_t*);             \
     template cudaError_t mf_residual<T>(const MfOp<T>&, const double*, const T*, T*, T*, double*,                 \

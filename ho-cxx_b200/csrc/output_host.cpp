@@ -238,12 +238,19 @@ Error VtkQueue::submit(const Mesh& mesh, const Bases& B, const SamplePoints* sam
         const Job& j = *owned;
         const VtkFields f{j.w.data(),       j.psi.data(),  j.u.data(),     j.v.data(),    j.rhs_diff.data(),
                           j.rhs_adv.data(), j.bc_w.data(), j.bc_nv.data(), j.bc_pv.data()};
+        // nothing may leave the writer thread: every exception becomes an error status, and
+        // building the message (which allocates) may itself throw, so it has a fixed fallback
         try {
-            err_ = write_vtk_files(mesh, B, j.problem_type, f, j.indx, j.subidx, j.dir, samples);
-        } catch (const std::bad_alloc&) {
-            err_ = {5, "out of host memory writing the VTK files"};
-        } catch (const std::exception& ex) {  // nothing may leave the writer thread
-            err_ = {5, std::string("writing the VTK files: ") + ex.what()};
+            try {
+                err_ = write_vtk_files(mesh, B, j.problem_type, f, j.indx, j.subidx, j.dir, samples);
+            } catch (const std::bad_alloc&) {
+                err_ = {5, "out of host memory writing the VTK files"};
+            } catch (const std::exception& ex) {
+                err_ = {5, std::string("writing the VTK files: ") + ex.what()};
+            }
+        } catch (...) {
+            err_.code = 5;
+            err_.msg = "VTK write fail";  // 14 characters: fits the string's inline buffer
         }
     };
     try {

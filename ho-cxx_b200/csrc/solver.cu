@@ -9,6 +9,7 @@
 //                  + k = dt (adv + diff) + the RK combination of solve_advection_diffusion
 // Nothing crosses PCIe inside a step except the Krylov convergence flag polled by the host.
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -94,10 +95,21 @@ Error Solver::setup_from_mesh() {
     for (double j : M_.J)
         if (!(j > 0.0)) return {3, "non-positive element Jacobian: check the element orientation"};
     HO2D_TRY(setup_bcs(in_, mesh_, B_, bc_));
-    // HO2D_SMOOTHER_KRON=1: the Kronecker-sum fit of every diagonal block for the FP32 smoother
-    const char* kron_env = std::getenv("HO2D_SMOOTHER_KRON");
+    // smoother of the FP32 preconditioner: the requested kind, else the environment
+    // (HO2D_SMOOTHER_KRON=1, HO2D_SMOOTHER_BF16=1), else exact FP32 blocks
+    smoother_kind_ = smoother_req_;
+    if (smoother_kind_ < 0) {
+        auto on = [](const char* nm) {
+            const char* e = std::getenv(nm);
+            return e && std::string(e) == "1";
+        };
+        smoother_kind_ = on("HO2D_SMOOTHER_KRON") ? 2 : (on("HO2D_SMOOTHER_BF16") ? 1 : 0);
+    }
+    // kind 2: the Kronecker-sum fit of every diagonal block, made while the blocks stream by
     kron_ = KronSmoother();
-    assemble_poisson(mesh_, B_, M_, bc_, op_, false, kron_env && std::string(kron_env) == "1" ? &kron_ : nullptr);
+    assemble_poisson(mesh_, B_, M_, bc_, op_, false, smoother_kind_ == 2 ? &kron_ : nullptr);
+    smoother_exact_ = 0;
+    for (unsigned char x : kron_.exact) smoother_exact_ += x ? 1 : 0;
 
     DeviceState& d = *d_;
     HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
@@ -106,6 +118,7 @@ Error Solver::setup_from_mesh() {
         if (!*e) HO2D_CUDA(cudaEventCreate(e), "cudaEventCreate");
     if (!d.h_sc) HO2D_CUDA(cudaMallocHost(&d.h_sc, sizeof(KrylovScalars)), "cudaMallocHost");
     HO2D_TRY(noalloc_scratch(d.device, &d.noalloc_scratch));  // once per device, this device current
+    HO2D_CUDA(krylov_configure(in_.knod), "kernel set-up");
 
     const int N = mesh_.n_el, K = in_.knod, K2 = K * K, neb = mesh_.n_eb;
     const size_t nv = (size_t)N * K2, nf = (size_t)N * 4 * K;
@@ -156,10 +169,10 @@ Error Solver::setup_from_mesh() {
     for (DeviceBuffer* b : {&d.psi_tv, &d.psi_tg, &d.w_tv, &d.w_tg, &d.U_t}) HO2D_CUDA(upload(*b, zf), "alloc traces");
     // Poisson operator: the inverse diagonal blocks and the row sums of every block (the
     // two-level smoother's A e for element-wise constant e), from assemble_poisson
-    // 8 zero entries past the end: the smoothing kernel copies the 16-byte-aligned
-    // superset of a CTA's blocks into shared memory
-    op_.dinv.resize(op_.dinv.size() + 8, 0.0);
-    HO2D_CUDA(upload(d.dinv64, op_.dinv), "upload block-Jacobi");
+    // every element's block starts on a 16-byte boundary (padded_count): the smoothing
+    // kernel stages blocks with bulk copies
+    const int K4 = K2 * K2;
+    HO2D_CUDA(upload(d.dinv64, padded_rows<double>(op_.dinv, N, K4, padded_count(K4, 8))), "upload block-Jacobi");
     HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
     HO2D_TRY(build_poisson_geometry(fnb, fnijp));
@@ -422,6 +435,7 @@ Error Solver::setup_preconditioner() {
     d.pc32 = Precond<float>();
     d.graph64.reset();
     d.graph32.reset();
+    d.graph_mixed.reset();
     d.lev.clear();
     const char* mode = std::getenv("HO2D_PRECOND");
     if (mode && std::string(mode) == "bj") return {0, ""};
@@ -446,26 +460,37 @@ Error Solver::upload_precision_arrays() {
     if (d.have32) return {0, ""};
     const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
     for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
-    HO2D_CUDA(upload_as<float>(d.dinv32, op_.dinv), "upload fp32 block-Jacobi");
-    // HO2D_SMOOTHER_BF16=1: the FP32 smoother reads a BF16 copy of the inverse blocks (half
-    // the bytes; the preconditioner's precision changes only the inner iteration count)
-    if (const char* e = std::getenv("HO2D_SMOOTHER_BF16"); e && std::string(e) == "1") {
-        std::vector<uint16_t> h(op_.dinv.size());  // includes the zero padding past the end
-        for (size_t i = 0; i < h.size(); ++i) h[i] = bf16_bits((float)op_.dinv[i]);
+    const int N = mesh_.n_el, K = in_.knod, K2 = K * K, K4 = K2 * K2;
+    HO2D_CUDA(upload(d.dinv32, padded_rows<float>(op_.dinv, N, K4, padded_count(K4, 4))), "upload fp32 block-Jacobi");
+    // smoother kind 1: the FP32 smoother reads a BF16 copy of the inverse blocks (half the
+    // bytes; the preconditioner's precision changes only the inner iteration count)
+    if (smoother_kind_ == 1) {
+        const int st = padded_count(K4, 2);
+        std::vector<uint16_t> h((size_t)N * st + 1, 0);
+        for (size_t e = 0; e < (size_t)N; ++e)
+            for (int i = 0; i < K4; ++i) h[e * st + i] = bf16_bits((float)op_.dinv[e * K4 + i]);
         HO2D_CUDA(upload(d.dinv_bf16, h), "upload bf16 block-Jacobi");
     }
-    if (kron_.K > 0) {  // the Kronecker-sum smoother's arrays (FP32), set up with HO2D_SMOOTHER_KRON=1
+    if (kron_.K > 0) {  // the Kronecker-sum smoother's arrays (FP32), smoother kind 2
         std::vector<double> f, ex;
         std::vector<int> xi;
         kron_device_arrays(kron_, op_.dinv, f, xi, ex);
-        if (ex.empty()) ex.assign(1, 0.0);
-        HO2D_CUDA(upload_as<float>(d.kron_f, f), "upload Kronecker factors");
+        const int per = 4 * K2 + 2 * K;
+        HO2D_CUDA(upload(d.kron_f, padded_rows<float>(f, N, per, padded_count(per, 4))), "upload Kronecker factors");
         HO2D_CUDA(upload(d.kron_x, xi), "upload Kronecker exact-block index");
-        HO2D_CUDA(upload_as<float>(d.kron_exact, ex), "upload Kronecker exact blocks");
+        HO2D_CUDA(upload(d.kron_exact, padded_rows<float>(ex, ex.size() / K4, K4, padded_count(K4, 4))),
+                  "upload Kronecker exact blocks");
     }
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");
     d.have32 = true;
+    return {0, ""};
+}
+
+Error Solver::set_smoother(int kind) {
+    if (kind < -1 || kind > 2)
+        return {1, "smoother must be HO2D_SMOOTHER_BLOCKS (0), HO2D_SMOOTHER_BF16 (1) or HO2D_SMOOTHER_KRON (2)"};
+    smoother_req_ = kind;
     return {0, ""};
 }
 
@@ -503,6 +528,7 @@ Error Solver::poisson_solve() {
         HO2D_CUDA(cudaMemcpyAsync(d.h_sc, d.scalars.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream),
                   "poll");
         HO2D_CUDA(cudaStreamSynchronize(d.stream), "poll");
+        if (d.h_sc->dev_error) return {5, "a device-side wait for a bulk copy ran out (the GPU did not complete it)"};
         return {0, ""};
     };
     // runs BiCGSTAB to completion on (A, v); returns iterations
@@ -556,9 +582,44 @@ Error Solver::poisson_solve() {
         const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
         finite = std::isfinite(bn) && std::isfinite(rn);
         last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
+    } else if (use_graphs_) {
+        // FP64 iterative refinement around an FP32 BiCGSTAB, both loops on the device: one
+        // graph launch and one read of the scalars per solve
+        const MfOp<double> A64 = make_op<double>(d, mesh_, K, false);
+        const MfOp<float> A32 = make_op<float>(d, mesh_, K, true);
+        const BicgVectors<float> v = krylov_vectors<float>(d, d.kv[8].as<float>(), d.kv[9].as<float>());
+        SolveGraph& sg = d.graph_mixed;
+        if (!sg.exec || sg.max_iter != max_iter_) {
+            sg.reset();
+            HO2D_CUDA(krylov_capture_refined_solve(A64, A32, v, rs, max_iter_, d.pc32, d.psi64.as<double>(),
+                                                   d.rhs.as<double>(), d.rres.as<double>(), d.kxtv.as<double>(),
+                                                   d.kxtg.as<double>(), d.stream, &sg.graph),
+                      "graph capture");
+            HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
+            sg.max_iter = max_iter_;
+        }
+        // the refinement's controls travel in the device scalars (the stream is idle: every
+        // earlier read of h_sc was synchronised)
+        d.h_sc->tol_outer = tol_;
+        d.h_sc->inner_tol = inner_tol_;
+        d.h_sc->max_sweeps = 30;
+        static_assert(offsetof(KrylovScalars, inner_tol) == offsetof(KrylovScalars, tol_outer) + sizeof(double) &&
+                          offsetof(KrylovScalars, max_sweeps) == offsetof(KrylovScalars, inner_tol) + sizeof(double),
+                      "refinement controls are contiguous");
+        HO2D_CUDA(cudaMemcpyAsync(&d.scalars.as<KrylovScalars>()->tol_outer, &d.h_sc->tol_outer,
+                                  2 * sizeof(double) + sizeof(int), cudaMemcpyHostToDevice, d.stream),
+                  "refinement controls");
+        HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
+        HO2D_TRY(poll());
+        sweeps = d.h_sc->sweeps;
+        last_iters_ = d.h_sc->iters_total;
+        finite = d.h_sc->finite != 0;
+        last_res_ = d.h_sc->res;
+        launches_ += krylov_refined_launches(sweeps, last_iters_, d.pc32);
     } else {
-        // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator: every
-        // exit passes through an FP64 residual of the current psi
+        // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator, driven
+        // from the host (HO2D_GRAPHS=0): every exit passes through an FP64 residual of the
+        // current psi
         const MfOp<double> A64 = make_op<double>(d, mesh_, K, false);
         const MfOp<float> A32 = make_op<float>(d, mesh_, K, true);
         const BicgVectors<float> v = krylov_vectors<float>(d, d.kv[8].as<float>(), d.kv[9].as<float>());
@@ -593,6 +654,8 @@ Error Solver::poisson_solve() {
         }
     }
     ++n_solves_;
+    iters_total_ += last_iters_;
+    sweeps_total_ += krylov32_ ? sweeps : 0;
     if (verbose_)
         std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e\n", n_solves_, last_iters_,
                      sweeps, last_res_);
@@ -673,15 +736,13 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
         launches_ += 1;
         HO2D_TRY(poisson_solve());
     }
-    const T* psi = f32 ? d.psiT.as<T>() : reinterpret_cast<const T*>(d.psi64.get());
-    if (f32) {
-        HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), nv, d.stream), "d2f");
-        launches_ += 1;
-    }
-    HO2D_CUDA(launch_trace<T>(K, N, psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), b, d.stream), "trace");
-    VelocityArgs<T> va{psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), d.w_stage.as<T>(), d.u.as<T>(), d.v.as<T>(),
-                       d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
-    HO2D_CUDA(launch_velocity<T>(K, g, b, bc, va, d.stream), "velocity");
+    // the velocity is derived from psi in FP64 in both precisions (VelocityArgs)
+    const double* psi = d.psi64.as<double>();
+    const FrGeom<double> g64 = geom_of<double>(d, mesh_, false);
+    HO2D_CUDA(launch_trace<double>(K, N, psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.b64, d.stream), "trace");
+    VelocityArgs<T, double> va{psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.w_stage.as<T>(), d.u.as<T>(),
+                               d.v.as<T>(), d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
+    HO2D_CUDA((launch_velocity<T, double>(K, g64, d.b64, b, bc, va, d.stream)), "velocity");
     ResidualArgs<T> ra;
     ra.w = d.w_stage.as<T>();
     ra.u = d.u.as<T>();
@@ -725,13 +786,13 @@ Error Solver::velocity_only_t() {
                                     d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
               "poisson_rhs");
     HO2D_TRY(poisson_solve());
-    const T* psi = f32 ? d.psiT.as<T>() : reinterpret_cast<const T*>(d.psi64.get());
-    if (f32) HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), nv, d.stream), "d2f");
-    HO2D_CUDA(launch_trace<T>(K, N, psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), b, d.stream), "trace");
-    VelocityArgs<T> va{psi, d.psi_tv.as<T>(), d.psi_tg.as<T>(), d.w_stage.as<T>(), d.u.as<T>(), d.v.as<T>(),
-                       d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
-    HO2D_CUDA(launch_velocity<T>(K, g, b, bc, va, d.stream), "velocity");
-    launches_ += 4 + (f32 ? 1 : 0);
+    const double* psi = d.psi64.as<double>();
+    const FrGeom<double> g64 = geom_of<double>(d, mesh_, false);
+    HO2D_CUDA(launch_trace<double>(K, N, psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.b64, d.stream), "trace");
+    VelocityArgs<T, double> va{psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.w_stage.as<T>(), d.u.as<T>(),
+                               d.v.as<T>(), d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
+    HO2D_CUDA((launch_velocity<T, double>(K, g64, d.b64, b, bc, va, d.stream)), "velocity");
+    launches_ += 4;
     return {0, ""};
 }
 
@@ -891,6 +952,7 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
                                         d.kv[5].as<double>(), reps, d.stream), "apply");
     } else {
         const MfOp<float> op = make_op<float>(d, mesh_, K, true);
+        HO2D_CUDA(launch_copy_d2f(d.psi64.as<double>(), d.psiT.as<float>(), (size_t)N * K * K, d.stream), "d2f");
         HO2D_CUDA(mf_apply_op<float>(op, d.psiT.as<float>(), d.kxtv.as<float>(), d.kxtg.as<float>(),
                                      d.kv[5].as<float>(), d.stream), "apply");
         HO2D_CUDA(cudaEventRecord(d.ev0, d.stream), "event");
@@ -905,11 +967,104 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
     return {0, ""};
 }
 
+// Per-launch device time of the Krylov kernels inside BiCGSTAB iterations of the active
+// precision's solve, and their algorithmic bytes per launch: [0] the smoothing kernel
+// (vector update + two-level smoothing step + traces), [1] the operator kernels (v = A ph,
+// t = A sh), [2] the x/r update, [3] one coarse cycle. The iterations run on the current
+// state without a CUDA graph, with events between the launches on the handle's stream: the
+// FP32 solve of a refinement sweep on the FP64 residual of the current psi (mixed modes),
+// or the FP64 solve of the last right-hand side from a zero guess (FP64). Their tolerance
+// is zero, so none of them ends early; psi is not changed.
+Error Solver::profile_krylov(int reps, double* ms, double* bytes) {
+    if (!setup_done_) return {1, "not set up"};
+    if (reps <= 0 || reps > 1000) return {1, "reps must be in 1..1000"};
+    DeviceState& d = *d_;
+    HO2D_CUDA(cudaSetDevice(d.device), "cudaSetDevice");
+    const int N = mesh_.n_el, K = in_.knod, K2 = K * K;
+    const size_t nv = (size_t)N * K2;
+    for (cudaEvent_t& e : d.prof_ev)
+        if (!e) HO2D_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    ReduceScratch rs{d.partials.as<double>(), d.counter.as<unsigned>(), d.scalars.as<KrylovScalars>()};
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    d.h_sc->tol = 0.0;
+    HO2D_CUDA(cudaMemcpyAsync(&d.scalars.as<KrylovScalars>()->tol, &d.h_sc->tol, sizeof(double),
+                              cudaMemcpyHostToDevice, d.stream),
+              "tolerance");
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    auto run = [&](auto A, auto v, const auto& pc) -> Error {
+        HO2D_CUDA(krylov_init(A, v, rs, d.stream), "krylov init");
+        for (int r = 0; r < reps; ++r) {
+            HO2D_CUDA(krylov_iteration_timed(A, v, rs, 1 << 30, pc, d.prof_ev, d.stream), "krylov iteration");
+            HO2D_CUDA(cudaEventSynchronize(d.prof_ev[7]), "event");
+            float t[7];
+            for (int i = 0; i < 7; ++i) HO2D_CUDA(cudaEventElapsedTime(&t[i], d.prof_ev[i], d.prof_ev[i + 1]), "event");
+            acc[3] += t[0] + t[3];
+            acc[0] += t[1] + t[4];
+            acc[1] += t[2] + t[5];
+            acc[2] += t[6];
+        }
+        return {0, ""};
+    };
+    const int bw = krylov32_ ? 4 : 8;
+    int coarse_bytes = 0;
+    if (krylov32_) {
+        const MfOp<double> A64 = make_op<double>(d, mesh_, K, false);
+        const MfOp<float> A32 = make_op<float>(d, mesh_, K, true);
+        const BicgVectors<float> v = krylov_vectors<float>(d, d.kv[8].as<float>(), d.kv[9].as<float>());
+        HO2D_CUDA(mf_residual<double>(A64, d.rhs.as<double>(), d.psi64.as<double>(), d.kxtv.as<double>(),
+                                      d.kxtg.as<double>(), d.rres.as<double>(), rs, d.stream),
+                  "fp64 residual");
+        HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
+        HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
+        HO2D_TRY(run(A32, v, d.pc32));
+        coarse_bytes = coarse_cycle_bytes(d.pc32);
+    } else {
+        const MfOp<double> A = make_op<double>(d, mesh_, K, false);
+        const BicgVectors<double> v = krylov_vectors<double>(d, d.kv[8].as<double>(), d.rhs.as<double>());
+        HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(double), d.stream), "memset");
+        HO2D_TRY(run(A, v, d.pc64));
+        coarse_bytes = coarse_cycle_bytes(d.pc64);
+    }
+    HO2D_CUDA(cudaMemcpyAsync(d.h_sc, d.scalars.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, d.stream),
+              "poll");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    if (d.h_sc->done && d.h_sc->it < reps)
+        return {1, "the profiled iterations ended early (breakdown): no per-kernel times"};
+    if (ms) {
+        ms[0] = acc[0] / (2.0 * reps);
+        ms[1] = acc[1] / (2.0 * reps);
+        ms[2] = acc[2] / reps;
+        ms[3] = acc[3] / (2.0 * reps);
+    }
+    if (bytes) {
+        // smoother element data: the inverse block in its storage, or the Kronecker factors
+        // plus the exact blocks of the elements that keep them
+        const double K4 = (double)K2 * K2;
+        double blk = K4 * bw;
+        if (krylov32_ && smoother_kind_ == 1) blk = K4 * 2;
+        if (krylov32_ && smoother_kind_ == 2) blk = (4.0 * K2 + 2 * K) * 4 + (double)smoother_exact_ / N * K4 * 4;
+        // per element: block, 5 block row sums, r and v (and p in mode 0: half the
+        // launches) read, p or s and z written, z's 4K face traces (value and derivative)
+        // written, 4K trace destinations and 5 coarse-slot indices read
+        bytes[0] = (double)N * (blk + 5.0 * K2 * bw + 4.5 * K2 * bw + 8.0 * K * bw + 16.0 * K + 20.0);
+        // per element: operand, 3 metric coefficients, rhat or s, result; 4 face coefficients
+        // and 2 incoming traces per face point; 4 face codes; the element sum
+        bytes[1] = (double)N * ((6.0 * K2 + 24.0 * K) * bw + 16.0 + bw);
+        // x, ph, sh, s, t, rhat read; x and r written; the element sum of r
+        bytes[2] = (double)N * (8.0 * K2 * bw + bw);
+        bytes[3] = coarse_bytes;
+    }
+    return {0, ""};
+}
+
 // y = A x on caller-owned device buffers without allocating: the operand's face traces
 // go to the fixed scratch of noalloc.cu (shared by every call on this device).
 Error Solver::apply_poisson_noalloc(const double* dx, double* dy) {
     if (!setup_done_) return {1, "not set up"};
     if (!dx || !dy) return {1, "null device buffer"};
+    // the operator kernels move element rows in 16-byte pieces
+    if ((reinterpret_cast<uintptr_t>(dx) | reinterpret_cast<uintptr_t>(dy)) % 16 != 0)
+        return {1, "device buffers must be 16-byte aligned (cudaMalloc's alignment)"};
     DeviceState& d = *d_;
     const int N = mesh_.n_el, K = in_.knod;
     const size_t need = 2 * (size_t)N * 4 * K;

@@ -52,6 +52,7 @@ class Solver {
     Error set_precision(int mode);
     Error time_steps(int nsteps, double* total_ms, double* poisson_ms);
     Error profile_spmv(int reps, double* avg_ms, double* bytes);
+    Error profile_krylov(int reps, double* ms, double* bytes);  // [4] each
     Error apply_poisson(const double* x, double* y);
     Error apply_poisson_noalloc(const double* dx, double* dy);
 
@@ -120,9 +121,21 @@ class Solver {
     }
     double dt() const { return in_.dt; }
     int precision() const { return krylov32_ ? (stage32_ ? 1 : 2) : 0; }
+    // smoother of the FP32 preconditioner: 0 exact inverse blocks in FP32, 1 the same blocks
+    // in BF16, 2 Kronecker-sum factors with exact blocks where the fit is poor; -1 = from the
+    // environment (HO2D_SMOOTHER_KRON=1, HO2D_SMOOTHER_BF16=1). Takes effect at setup.
+    Error set_smoother(int kind);
+    int smoother() const { return smoother_kind_; }
+    int smoother_exact_blocks() const { return smoother_exact_; }
     int last_poisson_iterations() const { return last_iters_; }
     double last_poisson_residual() const { return last_res_; }
     int64_t launches() const { return launches_; }
+    // cumulative since setup: Poisson solves, inner Krylov iterations, refinement sweeps
+    void counters(int64_t* solves, int64_t* iters, int64_t* sweeps) const {
+        if (solves) *solves = n_solves_;
+        if (iters) *iters = iters_total_;
+        if (sweeps) *sweeps = sweeps_total_;
+    }
     void set_poisson_tolerance(double tol, int max_iter) {
         tol_ = tol;
         max_iter_ = max_iter;
@@ -175,7 +188,10 @@ class Solver {
     std::string output_dir_;                  // where solve() writes its VTK files (empty: none)
     SamplePoints samples_;                    // the input's sample points (VTK output)
     VtkQueue vtk_queue_;                      // dumps being written (declared after what it reads)
-    KronSmoother kron_;                       // Kronecker-sum smoother data (HO2D_SMOOTHER_KRON=1)
+    KronSmoother kron_;                       // Kronecker-sum smoother data (smoother kind 2)
+    int smoother_req_ = -1;                   // requested smoother kind (-1: environment)
+    int smoother_kind_ = 0;                   // kind in use since the last setup
+    int smoother_exact_ = 0;                  // kind 2: elements that keep their exact block
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;
@@ -189,6 +205,7 @@ class Solver {
     double last_res_ = 0.0;
     int64_t launches_ = 0;
     long n_solves_ = 0;
+    int64_t iters_total_ = 0, sweeps_total_ = 0;
     int coarse_levels_ = 0;
     std::vector<int> coarse_sizes_;
     double inner_tol_ = 1e-4;        // FP32 inner solve: relative reduction per refinement sweep

@@ -56,6 +56,7 @@ struct DeviceState {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+    cudaEvent_t prof_ev[8] = {};  // launch boundaries of a profiled Krylov iteration
     // connectivity and boundary tables
     DeviceBuffer face_nb, face_nijp, be_group, sw_p, sw_d, noslip, role, be_ijp;
     DevBases<double> b64;
@@ -92,6 +93,7 @@ struct DeviceState {
     Precond<double> pc64;
     Precond<float> pc32;
     SolveGraph graph64, graph32;  // captured Krylov solves (FP64 solve, FP32 inner solve)
+    SolveGraph graph_mixed;       // captured mixed-precision solve (refinement loop included)
     double* noalloc_scratch = nullptr;  // device address of noalloc.cu's fixed scratch
     DeviceBuffer l2flush;               // written between timed steps to evict L2
     DeviceBuffer fcoef, fidx, fout;     // body-force coefficients, boundary indices, result
@@ -105,6 +107,8 @@ struct DeviceState {
     ~DeviceState() {
         if (h_sc) cudaFreeHost(h_sc);
         for (cudaEvent_t e : {ev0, ev1, evp0, evp1})
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : prof_ev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -168,6 +172,17 @@ template <typename T>
 cudaError_t upload_as(DeviceBuffer& buf, const std::vector<double>& h) {
     std::vector<T> c(h.begin(), h.end());
     return upload(buf, c);
+}
+
+// n rows of `len` values from h, each padded with zeros to `stride` values (the device
+// layout of the per-element preconditioner data, padded_count in device.cuh), converted
+// to T.
+template <typename T>
+std::vector<T> padded_rows(const std::vector<double>& h, size_t n, int len, int stride) {
+    std::vector<T> out(n * (size_t)stride + 1, T(0));  // one spare value: never an empty allocation
+    for (size_t r = 0; r < n; ++r)
+        for (int i = 0; i < len; ++i) out[r * stride + i] = T(h[r * len + i]);
+    return out;
 }
 
 inline cudaError_t upload_ell(DeviceState::EllBufs& b, const Ell& A) {

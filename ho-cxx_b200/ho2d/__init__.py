@@ -233,6 +233,16 @@ class HO_2D:
     def set_precision(self, mode: int) -> None:
         self._check(self._lib.ho2d_set_precision(self._h, int(mode)))
 
+    def set_smoother(self, kind: int) -> None:
+        """Smoother of the FP32 preconditioner for the next setup (capi.SMOOTHER_*; -1: default)."""
+        self._check(self._lib.ho2d_set_smoother(self._h, int(kind)))
+
+    def smoother(self):
+        """(kind in use, elements that keep their exact inverse block under SMOOTHER_KRON)."""
+        k, n = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._lib.ho2d_get_smoother(self._h, ctypes.byref(k), ctypes.byref(n)))
+        return k.value, n.value
+
     def set_poisson_tolerance(self, rel_tol: float, max_iter: int) -> None:
         self._check(self._lib.ho2d_set_poisson_tolerance(self._h, float(rel_tol), int(max_iter)))
 
@@ -240,6 +250,12 @@ class HO_2D:
         it, res = ctypes.c_int32(), ctypes.c_double()
         self._check(self._lib.ho2d_poisson_stats(self._h, ctypes.byref(it), ctypes.byref(res)))
         return it.value, res.value
+
+    def solve_counters(self):
+        """(Poisson solves, Krylov iterations, refinement sweeps) since setup."""
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self._lib.ho2d_solve_counters(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     def time(self):
         t, dt = ctypes.c_double(), ctypes.c_double()
@@ -260,6 +276,16 @@ class HO_2D:
         ms, by = ctypes.c_double(), ctypes.c_double()
         self._check(self._lib.ho2d_profile_spmv(self._h, int(reps), ctypes.byref(ms), ctypes.byref(by)))
         return ms.value, by.value
+
+    def profile_krylov(self, iterations: int = 20):
+        """Per-launch device ms and algorithmic bytes of the Krylov kernels inside BiCGSTAB
+        iterations on the current state: dict kernel -> (ms, bytes) for "smoother",
+        "operator", "xr_update" and "coarse_cycle"."""
+        ms = (ctypes.c_double * 4)()
+        by = (ctypes.c_double * 4)()
+        self._check(self._lib.ho2d_profile_krylov(self._h, int(iterations), ms, by))
+        names = ("smoother", "operator", "xr_update", "coarse_cycle")
+        return {n: (ms[i], by[i]) for i, n in enumerate(names)}
 
     def apply_poisson(self, x) -> np.ndarray:
         """y = A x with the device's (matrix-free) Poisson operator, FP64."""

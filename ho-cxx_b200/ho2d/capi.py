@@ -17,6 +17,7 @@ STATUS = {0: "HO2D_OK", 1: "HO2D_ERR_ARG", 2: "HO2D_ERR_IO", 3: "HO2D_ERR_MESH",
           5: "HO2D_ERR_CUDA", 6: "HO2D_ERR_NOT_CONVERGED", 7: "HO2D_ERR_NONFINITE"}
 FP64, MIXED, MIXED_KRYLOV = 0, 1, 2
 BC_POISSON, BC_NORMAL_VEL, BC_PARL_VEL, BC_DIFFUSION, BC_VORTICITY, BC_VELOCITY_JUMP, BC_ADVECTION = range(7)
+SMOOTHER_BLOCKS, SMOOTHER_BF16, SMOOTHER_KRON = range(3)
 FIELD_VORTICITY, FIELD_STREAMFUNCTION, FIELD_RHS_DIFFUSIVE, FIELD_RHS_ADVECTIVE, FIELD_STAGE_K, FIELD_JACOBIAN = range(6)
 
 # exported symbol -> (restype, argtypes); every name declared in include/ho2d.h
@@ -44,12 +45,17 @@ SIGNATURES = {
     "ho2d_set_boundary": (ctypes.c_int, [_P, _I, _I, _DP]),
     "ho2d_get_solution_points": (ctypes.c_int, [_P, _I, _DP]),
     "ho2d_set_precision": (ctypes.c_int, [_P, _I]),
+    "ho2d_set_smoother": (ctypes.c_int, [_P, _I]),
+    "ho2d_get_smoother": (ctypes.c_int, [_P, _IP, _IP]),
     "ho2d_set_poisson_tolerance": (ctypes.c_int, [_P, _D, _I]),
     "ho2d_poisson_stats": (ctypes.c_int, [_P, _IP, _DP]),
     "ho2d_get_time": (ctypes.c_int, [_P, _DP, _DP]),
+    "ho2d_solve_counters": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int64)]),
     "ho2d_set_time": (ctypes.c_int, [_P, _D]),
     "ho2d_time_steps": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_profile_spmv": (ctypes.c_int, [_P, _I, _DP, _DP]),
+    "ho2d_profile_krylov": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_apply_poisson": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_apply_poisson_noalloc": (ctypes.c_int, [_P, _I, ctypes.c_void_p, ctypes.c_void_p]),
     "ho2d_get_forces": (ctypes.c_int, [_P, _DP, _DP]),

@@ -38,6 +38,17 @@ enum ho2d_precision {
     HO2D_MIXED_KRYLOV = 2   /* FP64 FR residual; FP32 Krylov inside FP64 refinement of the Poisson solve */
 };
 
+/* Smoother of the FP32 Poisson preconditioner (HO2D_MIXED, HO2D_MIXED_KRYLOV). No
+ * counterpart in the reference, whose AMGCL relaxation is fixed at compile time
+ * (src/HO_2D.hpp:54). The FP64 solve always uses exact FP64 inverse blocks. */
+enum ho2d_smoother {
+    HO2D_SMOOTHER_BLOCKS = 0,  /* exact inverse of each element's diagonal block, FP32 */
+    HO2D_SMOOTHER_BF16 = 1,    /* the same blocks stored in BF16 (half the bytes) */
+    HO2D_SMOOTHER_KRON = 2     /* Kronecker-sum fit of each block, inverted by fast
+                                  diagonalisation (4K^2+2K values per element); the exact
+                                  block where the fit is poor */
+};
+
 /* which boundary-edge array [N_eb][Knod] ho2d_get_boundary / ho2d_set_boundary address */
 enum ho2d_boundary_array {
     HO2D_BC_POISSON = 0,        /* BC_Poisson: psi or d(psi)/dn */
@@ -127,12 +138,23 @@ int ho2d_get_boundary_points(ho2d_solver* handle, int32_t len, double* buf);
 /* HO2D_FP64 (default), HO2D_MIXED or HO2D_MIXED_KRYLOV; may be called before or after
  * ho2d_setup. */
 int ho2d_set_precision(ho2d_solver* handle, int32_t mode);
+/* Selects the FP32 preconditioner's smoother (enum ho2d_smoother) for the next
+ * ho2d_setup; -1 restores the default (HO2D_SMOOTHER_KRON=1 or HO2D_SMOOTHER_BF16=1 in the
+ * environment, else HO2D_SMOOTHER_BLOCKS). No counterpart in the reference. */
+int ho2d_set_smoother(ho2d_solver* handle, int32_t kind);
+/* The smoother in use since the last ho2d_setup and, for HO2D_SMOOTHER_KRON, how many
+ * elements keep their exact inverse block (0 otherwise). */
+int ho2d_get_smoother(ho2d_solver* handle, int32_t* kind, int32_t* exact_blocks);
 /* Poisson solve controls: relative tolerance on ||b - A psi|| / ||b|| (default 1e-12)
  * and iteration cap (default 500). */
 int ho2d_set_poisson_tolerance(ho2d_solver* handle, double rel_tol, int32_t max_iter);
 /* Statistics of the last Poisson solve: Krylov iterations (inner iterations summed over
  * refinement sweeps) and final relative residual. */
 int ho2d_poisson_stats(ho2d_solver* handle, int32_t* iterations, double* rel_residual);
+/* No counterpart in the reference. Totals since ho2d_setup: Poisson solves, Krylov
+ * iterations (inner iterations of all refinement sweeps in the mixed modes) and FP64
+ * refinement sweeps (0 in HO2D_FP64). Any pointer may be NULL. */
+int ho2d_solve_counters(ho2d_solver* handle, int64_t* solves, int64_t* iterations, int64_t* sweeps);
 /* Current solver time and time-step size. */
 int ho2d_get_time(ho2d_solver* handle, double* time, double* dt);
 /* Sets the current solver time (the reference's time_start / current_time,
@@ -149,6 +171,12 @@ int ho2d_time_steps(ho2d_solver* handle, int32_t nsteps, double* total_ms, doubl
  * the active precision, between CUDA events on the handle's stream; returns the average
  * launch duration and the algorithmic bytes one launch must move. */
 int ho2d_profile_spmv(ho2d_solver* handle, int32_t reps, double* avg_ms, double* bytes_per_launch);
+/* No counterpart in the reference. Device time of the Krylov kernels inside `iterations`
+ * BiCGSTAB iterations of the active precision's Poisson solve on the current state (run
+ * without a CUDA graph, CUDA events between the launches on the handle's stream; psi is
+ * not changed), and their algorithmic bytes per launch. ms[4] and bytes[4]: [0] smoothing
+ * kernel, [1] operator kernel, [2] x/r update, [3] one coarse cycle; per launch averages. */
+int ho2d_profile_krylov(ho2d_solver* handle, int32_t iterations, double* ms, double* bytes);
 /* y = A x in FP64 with the device's Poisson operator: the matrix the reference assembles
  * in form_Laplace_operator_matrix (src/HO_2D.cpp:1533-1804), applied matrix-free;
  * len = N_el*Knod*Knod. */
@@ -158,7 +186,12 @@ int ho2d_apply_poisson(ho2d_solver* handle, int32_t len, const double* x, double
  * through their own pool or a fixed budget, or that must not trigger the implicit device
  * synchronisation an allocation can cause in the middle of their own work. x_device and
  * y_device are caller-owned DEVICE buffers of len = N_el*Knod*Knod doubles on the
- * handle's device (y = A x, FP64, on the handle's stream, synchronous at return). The
+ * handle's device, each 16-byte aligned as cudaMalloc returns them (HO2D_ERR_ARG
+ * otherwise) (y = A x, FP64, synchronous at return: y_device is complete when the
+ * call returns). The call runs on the handle's own non-blocking stream, which is not
+ * ordered after the caller's streams or the legacy default stream: whatever wrote
+ * x_device must have completed before the call (synchronise the stream or event that
+ * wrote it). The
  * only working memory is a fixed 8 MiB array compiled into the library (face traces of
  * x), so meshes with N_el*Knod > 131072 are rejected with HO2D_ERR_ARG. Its device
  * address is looked up once per device inside ho2d_setup; this call itself allocates

@@ -9,6 +9,20 @@ for p in (os.path.join(REPO, "ho-cxx_b200"), os.path.join(REPO, "oracle"), REPO)
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
+
+
+def reference_root() -> str:
+    """Root of the reference's sources: $HO2D_REFERENCE, else BASELINE.json's
+    reference_path (absent on machines without the reference)."""
+    env = os.environ.get("HO2D_REFERENCE")
+    if env:
+        return env
+    import json
+
+    try:
+        return json.load(open(os.path.join(REPO, "BASELINE.json")))["reference_path"]
+    except (OSError, KeyError, ValueError):
+        return ""
 GOLDEN_CASES = sorted(d for d in os.listdir(GOLDEN) if os.path.isfile(os.path.join(GOLDEN, d, "ref.npz")))
 
 

@@ -36,6 +36,11 @@ from ho2d import meshgen  # noqa: E402
 
 REF = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
 
+
+def reference_root() -> str:
+    """Root of the reference's sources: $HO2D_REFERENCE, else BASELINE.json's reference_path."""
+    return os.environ.get("HO2D_REFERENCE") or json.load(open(os.path.join(REPO, "BASELINE.json")))["reference_path"]
+
 # name: (meshgen case, keyword overrides, knod, steps)
 CASES = {
     "cav4_rk4": ("cavity4", {}, 4, 3),
@@ -101,7 +106,7 @@ def make_case(name: str) -> None:
 def check_shipped() -> None:
     import ho2d_oracle as O
 
-    src_dir = "/root/reference/input"
+    src_dir = os.path.join(reference_root(), "input")
     for dat in ("input_cavity.dat", "input_bfs.dat", "input_cylinder.dat"):
         with tempfile.TemporaryDirectory() as tmp:
             lines = open(os.path.join(src_dir, dat)).read().split("\n")

@@ -25,7 +25,7 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from conftest import GOLDEN, GOLDEN_CASES, REPO
+from conftest import GOLDEN, GOLDEN_CASES, REPO, reference_root
 
 CSRC = os.path.join(REPO, "ho-cxx_b200", "csrc")
 HYB = os.path.join(GOLDEN, "hybrid")
@@ -850,7 +850,7 @@ def test_clockwise_quad_has_negative_jacobian(lib):
 
 # ---- the reference's own shipped meshes (read where they lie; skipped without them) -----
 
-REFERENCE_INPUT = "/root/reference/input"
+REFERENCE_INPUT = os.path.join(reference_root(), "input")
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
 
 

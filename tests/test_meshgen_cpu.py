@@ -90,3 +90,26 @@ def test_differentiation_case_fields():
     assert a.shape == (4,) and np.abs(a).max() < 0.25
     u = meshgen.lid_velocity(t, a)
     np.testing.assert_allclose(u[[0, -1]], 1.0, atol=1e-12)  # corners keep u = 1
+
+
+@pytest.mark.parametrize("name", ["cfg1_cavity16", "cfg2_bfs"])
+def test_config_goldens_match_generated_inputs(tmp_path, name):
+    """The benchmark configurations' golden vectors were made by the reference from the
+    input.dat and mesh.msh that meshgen writes now, byte for byte (the GPU parity tests
+    regenerate them instead of storing the meshes)."""
+    import json
+    import os
+    import sys
+
+    from conftest import GOLDEN
+
+    meta_path = os.path.join(GOLDEN, name, "meta.json")
+    if not os.path.exists(meta_path):
+        pytest.skip(f"{name} golden not generated")
+    sys.path.insert(0, GOLDEN)
+    import make_config_golden as CG
+
+    meta = json.load(open(meta_path))
+    inp = CG.write_case(name, str(tmp_path))
+    assert CG.sha256(inp) == meta["input_sha256"]
+    assert CG.sha256(os.path.join(os.path.dirname(inp), "mesh.msh")) == meta["mesh_sha256"]

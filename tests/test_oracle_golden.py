@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from conftest import GOLDEN, GOLDEN_CASES
+from conftest import GOLDEN, GOLDEN_CASES, reference_root
 
 import ho2d_oracle as O
 
@@ -103,7 +103,7 @@ def test_oracle_on_shipped_meshes(tmp_path, dat):
 
     from conftest import REPO
 
-    src = "/root/reference/input"
+    src = os.path.join(reference_root(), "input")
     ref_bin = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
     if not (os.path.isdir(src) and os.path.exists(ref_bin)):
         pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")

@@ -20,7 +20,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, REPO
+from conftest import GOLDEN, REPO, reference_root
 
 REF = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
 
@@ -226,7 +226,7 @@ def test_sample_points_of_the_shipped_cavity(tmp_path, vtk_harness):
     lie, skipped without them), two time steps: the library's writer reproduces the
     reference's sampling_points file and both VTK files from the fields the reference wrote
     them from."""
-    src = "/root/reference/input"
+    src = os.path.join(reference_root(), "input")
     if not (os.path.isdir(src) and os.path.exists(REF)):
         pytest.skip("the reference's input/ directory or oracle/_ref/ho2d_ref is not available")
     d = tmp_path / "case"

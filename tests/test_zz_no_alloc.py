@@ -27,7 +27,14 @@ def _cudart():
     rt.cudaMalloc.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t]
     rt.cudaFree.argtypes = [ctypes.c_void_p]
     rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    rt.cudaMemGetInfo.argtypes = [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
     return rt
+
+
+def _free_bytes(rt):
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
 
 
 class DeviceArray:
@@ -69,8 +76,12 @@ def test_noalloc_matches_allocating_entry_point_twice(case):
             x = rng.standard_normal((s.N_el, s.Knod, s.Knod))
             y_ref = s.apply_poisson(x).ravel()
             dx.upload(x)
+            # device memory is handed out in pages of at least 2 MiB: any allocation inside
+            # the call would show as a drop of the free bytes
+            free0 = _free_bytes(rt)
             code = s._lib.ho2d_apply_poisson_noalloc(s._h, n, dx.p, dy.p)
             assert code == 0, s._lib.ho2d_last_error(s._h)
+            assert _free_bytes(rt) == free0
             y = dy.download()
             assert np.abs(y - y_ref).max() <= TOL * np.abs(y_ref).max()
     finally:
