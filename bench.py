@@ -1,16 +1,18 @@
 """Benchmark: DOF-updates/s and Poisson ms/step of the FR time step on one B200.
 
-Workload (default): the backward-facing step with ~15,000 jittered quads (14,625
-elements, h = 1/15, +/-0.15h interior jitter, seed 2), K = P+1 = 5 (365,625 DOF),
-Re = 400, RK4 at CFL 0.5, parabolic pulsatile inlet -- synthetic mesh of the stated
-shape (no dataset is involved). Each rank is an independent replica (the path has no
-data-path collective); `value` sums DOF updates over ranks and divides by the slowest
-rank's device time.
+Headline workload (default): flow around a cylinder on a 256 x 512 O-grid (radial stretch
+1.02, r in [0.5, 20]; 131,072 quads), K = P+1 = 6 (4,718,592 DOF), Re = 100, RK4 at the
+smaller of the CFL-0.5 and the viscous step, impulsive start -- a seeded synthetic mesh of
+the stated shape (no dataset is involved). Each rank is an independent replica (the path
+has no data-path collective); `value` sums DOF updates over ranks and divides by the
+slowest rank's device time.
 
-The headline precision is mixed (FP32 FR residual + FP32 BiCGSTAB inside FP64 iterative
-refinement, FP64 RK accumulation); the FP64 plain path is timed on the same workload and
-reported under "fp64", with the relative L2 vorticity difference between the two after
-the same steps.
+The headline precision is HO2D_MIXED_KRYLOV: FP64 FR stage and RK update, FP32 BiCGSTAB
+with the FP32 preconditioner inside FP64 iterative refinement of the Poisson solve (the
+device-resident refinement loop). The FP64 plain path (every array and operation in
+FP64, exact FP64 inverse blocks) is timed on the same workload under "fp64", and the
+all-FP32-stage mode (HO2D_MIXED) under "mixed_fp32_stage", each with its relative L2
+vorticity difference from FP64 after the same steps and after --l2-steps steps.
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -33,6 +35,13 @@ sys.path.insert(0, os.path.join(REPO, "ho-cxx_b200"))
 METRIC = "DOF-updates/s + Poisson ms/step, mixed vs FP64 on one B200 at stated L2 error"
 UNIT = "DOF-updates/s"
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "ho2d_ref")
+TRAFFIC = os.path.join(REPO, "profiles", "dram_traffic.json")
+SMOOTHERS = {"blocks": 0, "bf16": 1, "kron": 2}
+# algorithmic bytes per DOF-update of the FP64 FR stage kernels (trace, velocity, residual
+# with the RK update), four stages of an RK4 step: per element and stage, velocity pass
+# psi + 5 volume metrics + 3 face metrics + table -> u, v; residual pass omega, u, v,
+# metrics, face metrics, table, omega_n and the RK accumulator
+STAGE_BYTES_PER_DOF_UPDATE = {4: 848, 5: 804, 6: 775, 7: 755}
 
 
 def parse():
@@ -41,11 +50,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", default="bfs")
-    ap.add_argument("--knod", type=int, default=5)
-    ap.add_argument("--cpu-stages", type=int, default=1, help="RK stages timed for the CPU baseline sample")
-    ap.add_argument("--t0", type=float, default=1.5, help="start time inside the pulsatile inflow cycle")
+    ap.add_argument("--case", default="cyl256x512")
+    ap.add_argument("--knod", type=int, default=None, help="K = P + 1 (default 6 for cylinders, 5 for the step)")
+    ap.add_argument("--smoother", default="bf16", choices=sorted(SMOOTHERS),
+                    help="smoother of the FP32 preconditioner in the mixed modes")
+    ap.add_argument("--t0", type=float, default=None, help="start time (default 1.5 for the step's pulsatile inlet)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--l2-steps", type=int, default=1000,
+                    help="continue every precision mode to this many steps (outside the timed region) and report "
+                         "the relative vorticity L2 difference from FP64 there (0: off)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary workloads (the step's 1000-step error, the 512^2 K=7 cavity)")
     ap.add_argument("--adjoint", action="store_true",
                     help="the differentiation case instead of the step benchmark: lid-driven cavity, K=5, Re=1000, "
                          "RK4; adjoint gradient (FP64 and mixed) against central differences")
@@ -63,10 +78,12 @@ def parse():
                          "Strouhal number, mean drag and lift amplitude in FP64 and mixed, and their differences")
     ap.add_argument("--t-end", type=float, default=80.0, help="time units simulated for --strouhal")
     ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
-    ap.add_argument("--l2-steps", type=int, default=0,
-                    help="also continue every precision mode to this many steps (outside the timed region) and "
-                         "report the relative vorticity L2 difference from FP64 there")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.knod is None:
+        a.knod = 6 if a.case.startswith("cyl") else (5 if a.case.startswith("bfs") else 4)
+    if a.t0 is None:
+        a.t0 = 1.5 if a.case.startswith("bfs") else 0.0
+    return a
 
 
 def dist_env():
@@ -77,11 +94,10 @@ def dist_env():
 
 
 class Dist:
-    """Barrier and max-reduce of host floats across replicas (gloo; nothing GPU-side)."""
+    """Barrier and max/sum-reduce of host floats across replicas (gloo; nothing GPU-side)."""
 
     def __init__(self, world):
         self.world = world
-        self.pg = None
         if world > 1:
             import datetime
 
@@ -94,33 +110,37 @@ class Dist:
         if self.world > 1:
             self.td.barrier()
 
-    def max(self, x: float) -> float:
+    def _reduce(self, x, op):
         if self.world == 1:
             return x
         import torch
 
         t = torch.tensor([x], dtype=torch.float64)
-        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        self.td.all_reduce(t, op=op)
         return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.td.ReduceOp.MAX) if self.world > 1 else x
 
     def sum(self, x: float) -> float:
-        if self.world == 1:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64)
-        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(x, self.td.ReduceOp.SUM) if self.world > 1 else x
 
     def close(self):
         if self.world > 1:
             self.td.destroy_process_group()
 
 
-def make_workload(tmp, case, knod, steps):
-    from ho2d import meshgen
-
-    return meshgen.make_case(case, tmp, knod=knod, steps=steps)
+def workload_name(case, knod, t0=0.0):
+    if case == "bfs":
+        return (f"backward-facing step, 14,625 jittered quads (+/-0.15h, seed 2), K={knod}, Re=400, RK4, "
+                f"CFL-0.5 dt, pulsatile parabolic inlet from t={t0}")
+    if case.startswith("cyl"):
+        nr, nt = case[3:].split("x")
+        return (f"cylinder O-grid {nr} x {nt} (radial stretch 1.02, r in [0.5, 20]), K={knod}, Re=100, RK4 at the "
+                f"smaller of the CFL-0.5 and viscous steps, impulsive start")
+    if case.startswith("cavityj"):
+        return f"lid-driven cavity {case[7:]}^2 jittered (+/-0.1h), K={knod}, RK4"
+    return f"{case}, K={knod}"
 
 
 class ClockSampler:
@@ -128,9 +148,8 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: str):
         self.proc = None
-        self.path = None
         if shutil.which("nvidia-smi") is None:
             return
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -185,30 +204,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(inp, stages, t0=1.5):
-    """The reference's own CPU step (oracle/_ref: src/HO_2D.cpp + src/Mesh.cpp built against
-    the oracle's Eigen/AMGCL API shim), single thread, timed over `stages` RK stages of
-    the same workload; DOF-updates/s = DOF / (4 * seconds per stage)."""
-    if not os.path.exists(REF_BIN):
+def measured_traffic(kernel, case, knod, precision):
+    """DRAM bytes (read + write) per element of one launch of `kernel` on this workload, from
+    the ncu capture recorded in profiles/dram_traffic.json; None when there is none."""
+    if not os.path.exists(TRAFFIC):
         return None
-    r = subprocess.run([REF_BIN, inp, os.path.join(os.path.dirname(inp), "refout"), "--time-stages", str(stages),
-                        "--t0", str(t0)],
-                       capture_output=True, text=True, timeout=1800)
-    if r.returncode != 0:
-        return None
-    # the reference's destructor prints a line after the harness's JSON record
-    d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
-    per_stage = d["seconds"] / d["stages"]
-    value = d["dof"] / (4.0 * per_stage)
-    return {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"{d['stages']} RK4 stage(s) of the same mesh (DOF {d['dof']}) from t={t0}, omega=0, "
-                      f"reference setup excluded; "
-                      f"Poisson solve {d['poisson_seconds']:.1f} s of {d['seconds']:.1f} s "
-                      f"({d['poisson_iterations']} shim BiCGSTAB iterations, tol 1e-15, maxiter 150; "
-                      f"shim solver, not AMGCL 1.4.0)",
-            "poisson_ms_per_step": 4.0 * d["poisson_seconds"] / d["stages"] * 1e3,
-            "ms_per_step": 4.0 * per_stage * 1e3, "dof": d["dof"],
-            "cpu": _cpu_model(), "nproc": os.cpu_count()}
+    for e in json.load(open(TRAFFIC)).get("captures", []):
+        if (e["kernel"], e["case"], e["knod"], e["precision"]) == (kernel, case, knod, precision):
+            return e
+    return None
 
 
 def _cpu_model():
@@ -221,37 +225,75 @@ def _cpu_model():
     return "unknown"
 
 
+def reference_sample(case, knod, stages, t0, tmp):
+    """The reference's own CPU step (oracle/_ref: src/HO_2D.cpp + src/Mesh.cpp built against
+    the oracle's Eigen/AMGCL API shim), single thread, timed over `stages` RK4 stages.
+
+    The reference stops at Knod = 5 and its mesh processing is quadratic in the element
+    count, so the cylinder workloads are sampled on the 32 x 64 O-grid of the same shape at
+    K = 5 (the K = 5 substitute), from a seeded N(0, 1) vorticity (PCG64 seed 3) -- from
+    rest its first Poisson solves are trivial. Other workloads run on their own mesh (K
+    capped at 5) from rest at t0. Returns a dict, or None when the binary is missing or
+    fails."""
+    import numpy as np
+
+    from ho2d import meshgen
+
+    if not os.path.exists(REF_BIN):
+        return None
+    k = min(knod, 5)
+    if case.startswith("cyl"):
+        sub = "cyl32x64"
+        inp = meshgen.make_case(sub, os.path.join(tmp, "ref_" + sub), knod=k, steps=1)
+        w0 = np.random.Generator(np.random.PCG64(3)).standard_normal((32 * 64, k, k))
+        w0p = os.path.join(tmp, "ref_w0.npy")
+        np.save(w0p, w0)
+        extra = ["--init-vort", w0p]
+        what = (f"K=5 substitute: the 32 x 64 O-grid of the same shape (2,048 quads) at K={k}, seeded N(0,1) "
+                f"vorticity (PCG64 seed 3); the reference rejects K > 5 and its quadratic mesh processing "
+                f"rules out the 131,072-quad mesh")
+    else:
+        inp = meshgen.make_case(case, os.path.join(tmp, "ref_" + case), knod=k, steps=1)
+        extra = []
+        what = f"the same mesh at K={k}, omega=0 from t={t0}"
+    r = subprocess.run([REF_BIN, inp, os.path.join(tmp, "refout"), "--time-stages", str(stages), "--t0", str(t0)]
+                       + extra, capture_output=True, text=True, timeout=3600)
+    if r.returncode != 0:
+        return None
+    # the reference's destructor prints a line after the harness's JSON record
+    d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    per_stage = d["seconds"] / d["stages"]
+    return {"value": d["dof"] / (4.0 * per_stage), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{d['stages']} RK4 stage(s) ({d['stages'] / 4:g} step), {what}; reference setup excluded; "
+                      f"Poisson {d['poisson_seconds']:.1f} s of {d['seconds']:.1f} s, {d['poisson_iterations']} "
+                      f"BiCGSTAB iterations (shim solver, not AMGCL 1.4.0; tol 1e-15, maxiter 150)",
+            "stages_timed": d["stages"], "seconds": d["seconds"],
+            "poisson_ms_per_step": 4.0 * d["poisson_seconds"] / d["stages"] * 1e3,
+            "ms_per_step": 4.0 * per_stage * 1e3, "dof": d["dof"], "cpu": _cpu_model(), "nproc": os.cpu_count()}
+
+
 def run_reference(args, rank, world):
+    """Reference arm: one full RK4 step (4 stages) of the reference's CPU path on the
+    workload's reference sample, rank 0 only."""
     if rank != 0:
         return
     with tempfile.TemporaryDirectory() as tmp:
-        inp = make_workload(tmp, args.case, args.knod, 1)
         if not os.path.exists(REF_BIN):
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ho2d_ref was not built"}))
             return
-        # one bounded sample (a full RK4 stage of the reference takes ~80 s on this mesh)
-        cb = cpu_baseline(inp, args.cpu_stages, args.t0)
+        cb = reference_sample(args.case, args.knod, 4, args.t0, tmp)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
             return
-        vals = [cb["value"]]
-        value = statistics.median(vals)
-        dof = cb["dof"]
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": 0, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None,
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": workload_name(args), "dof": dof},
-                "cpu_baseline": dict(cb, value=value),
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "config": {"workload": workload_name(args.case, args.knod, args.t0), "reference_dof": cb["dof"],
+                           "stages_timed": cb["stages_timed"]},
+                "poisson_ms_per_step": cb["poisson_ms_per_step"],
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
-
-
-def workload_name(args):
-    if args.case == "bfs":
-        return (f"backward-facing step, 14,625 jittered quads (+/-0.15h, seed 2), K={args.knod}, Re=400, RK4, "
-                f"CFL-0.5 dt, pulsatile parabolic inlet")
-    return f"{args.case}, K={args.knod}"
 
 
 def pinned_like(n):
@@ -271,49 +313,117 @@ def pinned_like(n):
     return np.frombuffer(buf, dtype=np.float64)
 
 
+def make_solver(inp, mode, smoother, t0):
+    import ho2d
+
+    s = ho2d.HO_2D()
+    s.read_input_file(inp)
+    s.set_precision(mode)
+    s.set_smoother(smoother)
+    s.setup()
+    s.set_time(t0)
+    return s
+
+
+def rel_l2(a, b):
+    import numpy as np
+
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def step_bytes(prof, iters_per_step, sweeps_per_step, solves_per_step, dof, knod, n_el, mixed):
+    """Algorithmic bytes of one time step: the Krylov iterations (two smoothing steps, two
+    operator applications, the x/r update and two coarse cycles each), the per-sweep FP64
+    residual and FP32 restart of the mixed modes (or the FP64 initial residual), and the FP64
+    stage kernels."""
+    it = 2 * prof["smoother"][1] + 2 * prof["operator"][1] + prof["xr_update"][1] + 2 * prof["coarse_cycle"][1]
+    op64 = n_el * ((6 * knod * knod + 24 * knod) * 8 + 24)  # one FP64 operator launch
+    per_sweep = (op64 + prof["operator"][1] + 4 * dof * 4) if mixed else 0.0
+    per_solve = op64 if not mixed else 0.0
+    stage = STAGE_BYTES_PER_DOF_UPDATE.get(knod, 775) * dof
+    return iters_per_step * it + sweeps_per_step * per_sweep + solves_per_step * per_solve + stage
+
+
+def time_mode(s, args, dist, phys, sample_clocks):
+    n_dof = s.N_el * s.Knod * s.Knod
+    s.solve_advection_diffusion(args.warmup)
+    dist.barrier()
+    sampler = ClockSampler(phys) if sample_clocks else None
+    l0 = s.launch_count()
+    c0 = s.solve_counters()
+    tot_ms, pois_ms = s.time_steps(args.steps)
+    c1 = s.solve_counters()
+    launches = s.launch_count() - l0
+    clocks = sampler.stop() if sampler else None
+    dist.barrier()
+    tmax = dist.max(tot_ms)
+    pmax = dist.max(pois_ms)
+    return {"ms_per_step": tmax / args.steps, "poisson_ms_per_step": pmax / args.steps,
+            "value": dist.sum(n_dof * args.steps) / (tmax / 1e3), "launches": launches,
+            "iters_per_step": (c1[1] - c0[1]) / args.steps, "sweeps_per_step": (c1[2] - c0[2]) / args.steps,
+            "solves_per_step": (c1[0] - c0[0]) / args.steps, "iters_last_solve": s.poisson_stats()[0],
+            "clocks": clocks}
+
+
+def secondary_workloads(args, tmp):
+    """Outside the timed region of the headline: the step (14,625 quads, K = 5) after 1000
+    steps in both mixed modes against FP64, and the 512^2 jittered cavity at K = 7 (mixed and
+    FP64 step times)."""
+    import ho2d
+    from ho2d import meshgen
+
+    out = {}
+    inp = meshgen.make_case("bfs", os.path.join(tmp, "bfs"), knod=5, steps=10)
+    sv = {m: make_solver(inp, mode, SMOOTHERS[args.smoother], 1.5)
+          for m, mode in (("fp64", ho2d.FP64), ("mixed", ho2d.MIXED_KRYLOV), ("mixed_fp32_stage", ho2d.MIXED))}
+    for s in sv.values():
+        s.solve_advection_diffusion(1000)
+    wf = sv["fp64"].get_vorticity()
+    out["bfs14625_k5_l2_after_1000_steps"] = {"workload": workload_name("bfs", 5, 1.5),
+                                              "mixed": rel_l2(sv["mixed"].get_vorticity(), wf),
+                                              "mixed_fp32_stage": rel_l2(sv["mixed_fp32_stage"].get_vorticity(), wf)}
+    del sv
+    from ho2d.adjoint_case import cavity_dt
+
+    dt = cavity_dt(512, 7, reyn=5000.0, jitter=0.1)
+    inp = meshgen.make_case("cavityj512", os.path.join(tmp, "cav512"), knod=7, steps=10, dt=dt, reyn=5000.0,
+                            jitter=0.1, seed=5)
+    res = {}
+    for m, mode in (("mixed", ho2d.MIXED_KRYLOV), ("fp64", ho2d.FP64)):
+        s = make_solver(inp, mode, SMOOTHERS[args.smoother], 0.0)
+        s.set_vorticity(meshgen.sine_spectrum(s.getsolnpts_d(), seed=3))
+        s.solve_advection_diffusion(2)
+        tot, pois = s.time_steps(4)
+        n_dof = s.N_el * s.Knod * s.Knod
+        res[m] = {"ms_per_step": tot / 4, "poisson_ms_per_step": pois / 4, "value": n_dof * 4 / (tot / 1e3),
+                  "iters_last_solve": s.poisson_stats()[0]}
+        del s
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    res["workload"] = ("lid-driven cavity 512^2, interior jitter +/-0.1h (seed 5), K=7 (12,845,056 DOF), Re=5000, "
+                       f"dt={dt:.3g}, seeded sine-spectrum vorticity (seed 3), 4 timed steps after 2")
+    out["cavity512_k7"] = res
+    return out
+
+
 def run_ours(args, rank, world, local, phys):
     dist = Dist(world)
     import numpy as np
 
     import ho2d
+    from ho2d import meshgen
 
     with tempfile.TemporaryDirectory() as tmp:
-        inp = make_workload(tmp, args.case, args.knod, args.steps)
-        solvers = {}
-        # headline: FP64 FR stage with the FP32 Krylov inside FP64 refinement (meets the
-        # 1e-6 vorticity target); "mixed_fp32_stage" also runs the FR stage in FP32
+        inp = meshgen.make_case(args.case, tmp, knod=args.knod, steps=args.steps)
+        sm = SMOOTHERS[args.smoother]
         modes = {"mixed": ho2d.MIXED_KRYLOV, "fp64": ho2d.FP64, "mixed_fp32_stage": ho2d.MIXED}
-        for prec, mode in modes.items():
-            s = ho2d.HO_2D()
-            s.read_input_file(inp)
-            s.set_precision(mode)
-            s.setup()
-            s.set_time(args.t0)
-            solvers[prec] = s
+        solvers = {m: make_solver(inp, mode, sm, args.t0) for m, mode in modes.items()}
         s0 = solvers["mixed"]
-        n_dof = s0.N_el * s0.Knod * s0.Knod
-        results = {}
-        clocks = None
-        for prec in modes:
-            s = solvers[prec]
-            s.solve_advection_diffusion(args.warmup)
-            dist.barrier()
-            sampler = ClockSampler(phys) if prec == "mixed" else None
-            l0 = s.launch_count()
-            tot_ms, pois_ms = s.time_steps(args.steps)
-            launches = s.launch_count() - l0
-            if sampler:
-                clocks = sampler.stop()
-            dist.barrier()
-            tmax = dist.max(tot_ms)
-            pmax = dist.max(pois_ms)
-            spmv_ms, spmv_bytes = s.profile_spmv(30)
-            results[prec] = {"ms_per_step": tmax / args.steps, "poisson_ms_per_step": pmax / args.steps,
-                             "value": dist.sum(n_dof * args.steps) / (tmax / 1e3), "launches": launches,
-                             "spmv_ms": spmv_ms, "spmv_bytes": spmv_bytes, "iters": s.poisson_stats()[0]}
-        w_mixed = solvers["mixed"].get_vorticity()
-        w_fp64 = solvers["fp64"].get_vorticity()
-        l2 = float(np.linalg.norm(w_mixed - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
+        n_el, knod = s0.N_el, s0.Knod
+        n_dof = n_el * knod * knod
+        results = {m: time_mode(solvers[m], args, dist, phys, m == "mixed") for m in modes}
+        # per-kernel times inside BiCGSTAB iterations on the state the timed steps left
+        prof = {m: solvers[m].profile_krylov(30) for m in ("mixed", "fp64")}
+        w = {m: solvers[m].get_vorticity() for m in modes}
         forces = None
         try:  # meshes with a body ("object" boundary): FP64 drag and lift of each mode
             fm, ff = solvers["mixed"].forces(), solvers["fp64"].forces()
@@ -322,23 +432,11 @@ def run_ours(args, rank, world, local, phys):
                                                       max(np.hypot(*ff), 1e-300))}
         except ho2d.HO2DError:
             pass
-        w_f32 = solvers["mixed_fp32_stage"].get_vorticity()
-        l2_f32 = float(np.linalg.norm(w_f32 - w_fp64) / max(np.linalg.norm(w_fp64), 1e-300))
-        l2_long = None
-        done = args.warmup + args.steps
-        if args.l2_steps > done:  # the same steps in every mode, then the differences from FP64
-            for s_ in solvers.values():
-                s_.solve_advection_diffusion(args.l2_steps - done)
-            wf = solvers["fp64"].get_vorticity()
-            nf = max(np.linalg.norm(wf), 1e-300)
-            l2_long = {"steps": args.l2_steps,
-                       "mixed": float(np.linalg.norm(solvers["mixed"].get_vorticity() - wf) / nf),
-                       "mixed_fp32_stage": float(np.linalg.norm(solvers["mixed_fp32_stage"].get_vorticity() - wf) / nf)}
         # end to end through the public API with host buffers: H2D of the step's input
         # vorticity from pinned memory, the step, D2H of the resulting vorticity
         s = solvers["mixed"]
         host_in = pinned_like(n_dof)
-        host_in[:] = w_mixed.ravel()
+        host_in[:] = w["mixed"].ravel()
         host_out = pinned_like(n_dof)
         e2e_steps = max(3, args.steps // 2)
         dist.barrier()
@@ -351,52 +449,89 @@ def run_ours(args, rank, world, local, phys):
         e2e_s = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.sum(n_dof * e2e_steps) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n_dof * 8,
                "d2h_bytes_per_step": n_dof * 8}
+        # the same steps in every mode from here on (the e2e steps advanced only "mixed"):
+        # the long differences start from the state after warm-up + timed steps
+        l2_long = None
+        done = args.warmup + args.steps
+        if args.l2_steps > done:
+            solvers["mixed"].set_vorticity(w["mixed"])
+            solvers["mixed"].set_time(solvers["fp64"].time()[0])
+            for s_ in solvers.values():
+                s_.solve_advection_diffusion(args.l2_steps - done)
+            wf = solvers["fp64"].get_vorticity()
+            l2_long = {"steps": args.l2_steps, "mixed": rel_l2(solvers["mixed"].get_vorticity(), wf),
+                       "mixed_fp32_stage": rel_l2(solvers["mixed_fp32_stage"].get_vorticity(), wf),
+                       "note": "mixed restarted from its own state after the e2e steps, at the FP64 run's time"}
+        del solvers, s
         peak, peak_kind = measured_peaks()
-        # DRAM bytes (read + write) of one k_mf_apply<5, float> launch on this workload, from
-        # the ncu capture summarised in profiles/k_mf_apply_bfs14625_k5_fp32.md
-        traffic = 13118720 if (args.case == "bfs" and args.knod == 5) else None
-        m = results["mixed"]
-        achieved = m["spmv_bytes"] / (m["spmv_ms"] * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": "k_mf_apply (matrix-free Poisson operator, FP32 inner Krylov)",
-                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_kind": peak_kind, "traffic": traffic,
-                    "launch_ms": m["spmv_ms"], "algorithmic_bytes_per_launch": m["spmv_bytes"]}
-        f = results["fp64"]
-        roofline_fp64 = {"kernel": "k_mf_apply (FP64)", "achieved": f["spmv_bytes"] / (f["spmv_ms"] * 1e-3) / 1e9,
-                         "launch_ms": f["spmv_ms"], "algorithmic_bytes_per_launch": f["spmv_bytes"]}
-        roofline_fp64["frac"] = roofline_fp64["achieved"] / peak
+        m, f = results["mixed"], results["fp64"]
+        # roofline of the kernel with the largest share of an iteration's device time
+        launches_per_it = {"smoother": 2, "operator": 2, "xr_update": 1, "coarse_cycle": 2}
+        pm = prof["mixed"]
+        share = {k: pm[k][0] * n for k, n in launches_per_it.items()}
+        top = max(share, key=share.get)
+        names = {"smoother": "k_mf_post", "operator": "k_mf_v/k_mf_t", "xr_update": "k_xr_update",
+                 "coarse_cycle": "coarse cycle (k_coarse_rows_f0, k_coarse_rows, k_dense_gemv)"}
+        ms_top, by_top = pm[top]
+        achieved = by_top / (ms_top * 1e-3) / 1e9
+        tr = measured_traffic(names[top], args.case, knod, f"mixed/{args.smoother}")
+        roofline = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_kind": peak_kind,
+                    "traffic": tr["dram_bytes_per_element"] * n_el if tr else None,
+                    "traffic_source": tr["source"] if tr else None,
+                    "launch_ms": ms_top, "algorithmic_bytes_per_launch": by_top,
+                    "timing": "CUDA events between launches on the handle's stream, 30 BiCGSTAB iterations "
+                              "on the state after the timed steps (no graph)",
+                    "iteration_share": share[top] / sum(share.values()),
+                    "kernels": {k: {"ms": v[0], "bytes": v[1], "gbs": v[1] / (v[0] * 1e-3) / 1e9,
+                                    "frac": v[1] / (v[0] * 1e-3) / 1e9 / peak} for k, v in pm.items()}}
+        for key, r_, mixed in (("mixed", m, True), ("fp64", f, False)):
+            sb = step_bytes(prof[key], r_["iters_per_step"], r_["sweeps_per_step"], r_["solves_per_step"], n_dof,
+                            knod, n_el, mixed)
+            r_["step_level"] = {"algorithmic_bytes_per_step": sb,
+                                "achieved_gbs": sb / (r_["ms_per_step"] * 1e-3) / 1e9,
+                                "frac": sb / (r_["ms_per_step"] * 1e-3) / 1e9 / peak}
+        fk = prof["fp64"]
+        roofline_fp64 = {k: {"ms": v[0], "bytes": v[1], "frac": v[1] / (v[0] * 1e-3) / 1e9 / peak}
+                         for k, v in fk.items()}
         cb = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            cb = cpu_baseline(inp, args.cpu_stages, args.t0)
+            cb = reference_sample(args.case, knod, 1, args.t0, tmp)
+        secondary = None
+        if rank == 0 and world == 1 and not args.no_secondary and args.case == "cyl256x512":
+            secondary = secondary_workloads(args, tmp)
         if rank == 0:
+            def mode_out(r_):
+                return {k: r_[k] for k in ("value", "ms_per_step", "poisson_ms_per_step", "iters_per_step",
+                                           "sweeps_per_step", "iters_last_solve", "launches")
+                        } | {"step_level": r_.get("step_level")}
+
             line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                     "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
                     "data": "synthetic (seeded mesh of the stated shape)",
-                    "config": {"workload": workload_name(args), "dof": n_dof, "n_el": s0.N_el,
-                               "parallelism": f"replicas x{world}", "l2": "L2 flushed between timed steps (256 MiB device "
-                               "write outside the per-step CUDA events)",
-                               "poisson_tol": 1e-12, "t0": args.t0, "omega0": 0.0},
+                    "config": {"workload": workload_name(args.case, knod, args.t0), "dof": n_dof, "n_el": n_el,
+                               "parallelism": f"replicas x{world}",
+                               "l2": "L2 flushed between timed steps (256 MiB device write outside the per-step "
+                                     "CUDA events); working set larger than L2",
+                               "poisson_tol": 1e-12, "t0": args.t0, "omega0": 0.0,
+                               "smoother": args.smoother},
                     "poisson_ms_per_step": m["poisson_ms_per_step"],
-                    "poisson_iterations_last_solve": m["iters"],
-                    "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"],
-                             "poisson_ms_per_step": f["poisson_ms_per_step"], "roofline": roofline_fp64,
-                             "poisson_iterations_last_solve": f["iters"]},
                     "precision": "HO2D_MIXED_KRYLOV: FP64 FR stage and RK update, FP32 BiCGSTAB with FP32 "
-                                 "preconditioner inside FP64 iterative refinement of the Poisson solve",
-                    "mixed_fp32_stage": {"precision": "HO2D_MIXED: FR stage also in FP32",
-                                         "value": results["mixed_fp32_stage"]["value"],
-                                         "ms_per_step": results["mixed_fp32_stage"]["ms_per_step"],
-                                         "poisson_ms_per_step": results["mixed_fp32_stage"]["poisson_ms_per_step"],
-                                         "poisson_iterations_last_solve": results["mixed_fp32_stage"]["iters"],
-                                         "l2_rel_vorticity_vs_fp64": l2_f32},
+                                 f"preconditioner ({args.smoother} smoother) inside FP64 iterative refinement of the "
+                                 "Poisson solve, refinement loop on the device",
+                    "mixed": mode_out(m),
+                    "fp64": mode_out(f) | {"kernels": roofline_fp64},
+                    "mixed_fp32_stage": mode_out(results["mixed_fp32_stage"]) | {
+                        "precision": "HO2D_MIXED: FR stage also in FP32 (velocity from FP64 psi)",
+                        "l2_rel_vorticity_vs_fp64": rel_l2(w["mixed_fp32_stage"], w["fp64"])},
                     "mixed_over_fp64": m["value"] / f["value"],
-                    "l2_rel_vorticity_mixed_vs_fp64": l2,
+                    "l2_rel_vorticity_mixed_vs_fp64": rel_l2(w["mixed"], w["fp64"]),
                     "l2_after_steps": args.warmup + args.steps,
                     "l2_rel_vorticity_vs_fp64_long": l2_long,
                     "body_force": forces,
-                    "clocks": clocks, "e2e": e2e, "gpu_launches": m["launches"], "roofline": roofline,
-                    "cpu_baseline": cb}
+                    "clocks": m["clocks"], "e2e": e2e, "gpu_launches": m["launches"], "roofline": roofline,
+                    "cpu_baseline": cb, "secondary": secondary}
             print(json.dumps(line))
     dist.close()
 
@@ -409,14 +544,15 @@ def run_adjoint(args, rank):
 
     if rank != 0:
         return
+    knod = 5 if args.knod is None else args.knod
     with tempfile.TemporaryDirectory() as tmp:
-        r = adjoint_case.run(tmp, n=args.adj_n, knod=args.knod, steps=args.adj_steps, ckpt=args.adj_ckpt,
+        r = adjoint_case.run(tmp, n=args.adj_n, knod=knod, steps=args.adj_steps, ckpt=args.adj_ckpt,
                              ndir=args.adj_dirs)
     f = r["fp64"]
     line = {"metric": "adjoint gradient relative error vs central differences (h=1e-6)",
             "value": f["max_rel_error"], "unit": "relative error", "n_gpus": 1, "higher_is_better": False,
             "dtype": "f64", "data": "synthetic (seeded sine-mode vorticity, seeded lid profile)",
-            "config": {"workload": f"lid-driven cavity {args.adj_n}x{args.adj_n}, K={args.knod}, Re=1000, RK4, "
+            "config": {"workload": f"lid-driven cavity {args.adj_n}x{args.adj_n}, K={knod}, Re=1000, RK4, "
                                    f"{args.adj_steps} steps, checkpoints every {args.adj_ckpt}, "
                                    f"{args.adj_dirs} directions in (omega0, lid coefficients)",
                        "n_el": r["n_el"], "dof": r["dof"], "dt": r["dt"]},
@@ -457,17 +593,14 @@ def main():
                                                      f"t_end={args.t_end}", **r["case"]},
                               "fp64": r["fp64"], "mixed": r["mixed"], "difference": r["difference"]}))
         return
-    if args.adjoint:
-        visible = os.environ.get("CUDA_VISIBLE_DEVICES")
-        devs = [d for d in visible.split(",") if d.strip()] if visible else None
-        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local % len(devs)] if devs else str(local)
-        run_adjoint(args, rank)
-        return
     # one GPU per rank: each replica sees only its own device
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     devs = [d for d in visible.split(",") if d.strip()] if visible else None
     phys = devs[local % len(devs)] if devs else str(local)
     os.environ["CUDA_VISIBLE_DEVICES"] = phys
+    if args.adjoint:
+        run_adjoint(args, rank)
+        return
     run_ours(args, rank, world, local, phys)
 
 
