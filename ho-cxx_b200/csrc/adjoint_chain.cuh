@@ -80,8 +80,9 @@ struct LapAdjScratch {
     T lbcv[NF];          // result: lam of the boundary values (Dirichlet value or Neumann flux)
 };
 
-// Reverse of face_common + contravariant_gradient (+ the Laplacian of lap_element when
-// use_lap) for one element, with boundary switches sw. Result in s.lf, s.ntv, s.ntg,
+// Reverse of the forward method-2 common values and fluxes, the contravariant gradient
+// and (when use_lap) the Laplacian of one element (row_face_common, row_contravariant and
+// residual_rows in stage_rows.cuh; src/HO_2D.cpp:2666-2927), with boundary switches sw. Result in s.lf, s.ntv, s.ntg,
 // s.lbcv. Boundary values do not enter the transposed map (it is linear in f); their
 // adjoints come out in s.lbcv.
 template <int K, typename T, class C>

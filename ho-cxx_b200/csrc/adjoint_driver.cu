@@ -321,11 +321,10 @@ Error Solver::stage_adjoint_dev(double coeff, double* out) {
     return {0, ""};
 }
 
-// The element bodies also reverse advection type 2 (residual_adjoint_continuous), checked
-// on the host against complex-step derivatives of the oracle; the device path accepts
-// type 1 only until its type-2 kernels have been run against the same checks on a GPU.
+// Advection types 1 and 2 (residual_adjoint_continuous for type 2); both are checked on the
+// host and on the GPU against complex-step derivatives of the oracle.
 static Error adjoint_supported(const Input& in, bool stage32) {
-    if (in.adv_type != 1) return {4, "the adjoint is implemented for advection type 1"};
+    if (in.adv_type != 1 && in.adv_type != 2) return {4, "the adjoint covers advection types 1 and 2"};
     if (in.problem_type == 11) return {4, "the adjoint does not cover hybrid runs (problem type 11)"};
     if (stage32) return {4, "the adjoint needs the FP64 stage: precision HO2D_FP64 or HO2D_MIXED_KRYLOV"};
     return {0, ""};

@@ -10,13 +10,14 @@
 //   downs    f_{l+1} = M_l f_l              l = 0 .. d-1   (k_coarse_rows)
 //   coarsest u_d = A_d^{-1} f_d                             (k_dense_gemv)
 //   ups      u_l = S_l f_l + Q_l u_{l+1}    l = d-1 .. 1   (k_coarse_rows)
-// Level 0's own up step is not launched here: the fine smoothing kernel evaluates
-// u0 = S0 f0 + Q0 u1 for the five elements each element needs (krylov.cu, k_mf_post).
-// For the meshes this solver targets the coarsest level has a few thousand rows, so a
-// cycle is two launches over the whole GPU: one restriction and one dense product.
+// The cycle ends with level 0's own up step u0 = S0 f0 + Q0 u1, one value per element,
+// which the fine smoothing kernel (krylov.cu, k_mf_post) reads for each element and its
+// four face neighbours.
 //
 // Every kernel spans all SMs and sums in a fixed order (fixed lane-to-entry assignment
 // and xor-shuffle trees), so results are bitwise reproducible.
+#include <type_traits>
+
 #include "device.cuh"
 #include "fr_launch.hpp"
 
@@ -154,11 +155,81 @@ __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv(DevEll<T> W, con
     if (lane == 0 && !skip) u[row] = acc;
 }
 
+// u = W f for the dense coarsest inverse stored as BF16 (FP32 preconditioner): one warp per
+// row, lanes stream the row in 16-byte pieces of 8 values with kGemvUnroll loads in flight;
+// f is read as two float4 per piece (its buffer is zero-padded past n to a multiple of 8).
+__global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv16(DevEll<float> W, const float* __restrict__ f,
+                                                                   float* __restrict__ u, const KrylovScalars* sc) {
+    const bool skip = sc->done;
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * kGemvWarps + (threadIdx.x >> 5);
+    if (row >= W.n) return;
+    const int nvec = (W.n + 7) / 8;
+    const int tail = W.n - (nvec - 1) * 8;  // values of the last piece inside the vector
+    const uint4* wr = reinterpret_cast<const uint4*>(W.val16 + (size_t)row * W.w);
+    const float4* fv = reinterpret_cast<const float4*>(f);
+    float acc = 0.f;
+    for (int c0 = lane; c0 < nvec; c0 += 32 * kGemvUnroll) {
+        uint4 a[kGemvUnroll];
+        float4 b0[kGemvUnroll], b1[kGemvUnroll];
+#pragma unroll
+        for (int q = 0; q < kGemvUnroll; ++q) {
+            const int c = c0 + 32 * q;
+            if (c < nvec) {
+                a[q] = __ldg(wr + c);
+                b0[q] = __ldg(fv + 2 * c);
+                b1[q] = __ldg(fv + 2 * c + 1);
+                if (c == nvec - 1) {  // a buffer shared by both precisions may hold other bytes there
+                    Vec16<float>::keep_first(b0[q], tail);
+                    Vec16<float>::keep_first(b1[q], tail - 4);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kGemvUnroll; ++q) {
+            if (c0 + 32 * q >= nvec) continue;
+            const unsigned w4[4] = {a[q].x, a[q].y, a[q].z, a[q].w};
+            const float fx[8] = {b0[q].x, b0[q].y, b0[q].z, b0[q].w, b1[q].x, b1[q].y, b1[q].z, b1[q].w};
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                acc += __uint_as_float(w4[h] << 16) * fx[2 * h];
+                acc += __uint_as_float(w4[h] & 0xffff0000u) * fx[2 * h + 1];
+            }
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0 && !skip) u[row] = acc;
+}
+
+template <typename T>
+void dense_gemv(const DevEll<T>& W, const T* f, T* u, const KrylovScalars* sc, cudaStream_t s) {
+    const unsigned gd = (unsigned)((W.n + kGemvWarps - 1) / kGemvWarps);
+    if constexpr (std::is_same<T, float>::value) {
+        if (W.val16) {
+            k_dense_gemv16<<<gd, 32 * kGemvWarps, 0, s>>>(W, f, u, sc);
+            return;
+        }
+    }
+    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(W, f, u, sc);
+}
+
+// u0 of element c into every block slot that reads it (Precond::u0dst)
+template <typename T>
+__device__ __forceinline__ void scatter_u0(const int* __restrict__ u0dst, T* __restrict__ ue5, int c, T a) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int d = u0dst[c * 5 + k];
+        if (d >= 0) ue5[d] = a;
+    }
+}
+
 // u0 = W f0 when the P0 level itself is the dense one (small meshes): f0 is formed from
 // the element sums as it is read, one warp per row, scalar loads
 template <typename T>
 __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv_f0(DevEll<T> W, BicgVectors<T> v,
-                                                                    T* __restrict__ u, const KrylovScalars* sc,
+                                                                    const int* __restrict__ u0dst,
+                                                                    T* __restrict__ ue5, const KrylovScalars* sc,
                                                                     int mode) {
     const bool skip = sc->done;
     const F0<T> f = f0_of(v, sc, mode);
@@ -170,7 +241,7 @@ __global__ void __launch_bounds__(32 * kGemvWarps) k_dense_gemv_f0(DevEll<T> W, 
     for (int k = lane; k < W.n; k += 32) acc += __ldg(wr + k) * f[k];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (lane == 0 && !skip) u[row] = acc;
+    if (lane == 0 && !skip) scatter_u0(u0dst, ue5, row, acc);
 }
 
 // level-0 restriction with the right-hand side formed from the element sums
@@ -216,6 +287,39 @@ __global__ void __launch_bounds__(256) k_coarse_rows_f0(DevEll<T> M, BicgVectors
     }
 }
 
+// level-0 up step u0 = S0 f0 + Q0 u1 with the right-hand side formed from the element sums;
+// each row's value goes to the block slots that read it (scatter_u0)
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_up0(DevEll<T> S, DevEll<T> Q, BicgVectors<T> v,
+                                                     const T* __restrict__ u1, const int* __restrict__ u0dst,
+                                                     T* __restrict__ ue5, const KrylovScalars* sc, int mode) {
+    const bool skip = sc->done;
+    const F0<T> xa = f0_of(v, sc, mode);
+    const int G = S.g;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int group = gid / G, sub = gid % G, ngroups = (int)(gridDim.x * blockDim.x) / G;
+    const int iters = (S.n + ngroups - 1) / ngroups;
+    for (int it = 0; it < iters; it += kRowBatch) {
+        T acc[kRowBatch];
+        int row[kRowBatch];
+        bool ok[kRowBatch];
+#pragma unroll
+        for (int r = 0; r < kRowBatch; ++r) {
+            acc[r] = T(0);
+            row[r] = group + (it + r) * ngroups;
+            ok[r] = it + r < iters && row[r] < S.n;
+        }
+        ell_accumulate<T>(S, xa, row, ok, G, sub, acc);
+        ell_accumulate<T>(Q, u1, row, ok, G, sub, acc);
+#pragma unroll
+        for (int r = 0; r < kRowBatch; ++r) {
+            T a = acc[r];
+            for (int off = G >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+            if (sub == 0 && ok[r] && !skip) scatter_u0(u0dst, ue5, row[r], a);
+        }
+    }
+}
+
 }  // namespace
 
 template <typename T>
@@ -224,7 +328,7 @@ cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const Kr
     const int d = pc.nlev - 1;
     const unsigned gd = (unsigned)((pc.dense.n + kGemvWarps - 1) / kGemvWarps);
     if (d == 0) {
-        k_dense_gemv_f0<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, v, pc.lev[0].u, sc, mode);
+        k_dense_gemv_f0<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, v, pc.u0dst, pc.ue5, sc, mode);
         return cudaGetLastError();
     }
     k_coarse_rows_f0<T><<<rows_grid(pc.lev[0].M), 256, 0, s>>>(pc.lev[0].M, v, pc.lev[1].f, sc, mode);
@@ -233,11 +337,13 @@ cudaError_t coarse_cycle(const Precond<T>& pc, const BicgVectors<T>& v, const Kr
         k_coarse_rows<T, const T*><<<rows_grid(L.M), 256, 0, s>>>(L.M, L.f, DevEll<T>(), nullptr, 0,
                                                                    pc.lev[l + 1].f, sc);
     }
-    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc);
+    dense_gemv<T>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc, s);
     for (int l = d - 1; l >= 1; --l) {
         const CoarseLevel<T>& L = pc.lev[l];
         k_coarse_rows<T, const T*><<<rows_grid(L.S), 256, 0, s>>>(L.S, L.f, L.Q, pc.lev[l + 1].u, 1, L.u, sc);
     }
+    const CoarseLevel<T>& L0 = pc.lev[0];
+    k_coarse_up0<T><<<rows_grid(L0.S), 256, 0, s>>>(L0.S, L0.Q, v, pc.lev[1].u, pc.u0dst, pc.ue5, sc, mode);
     return cudaGetLastError();
 }
 
@@ -250,7 +356,7 @@ cudaError_t coarse_cycle_vec(const Precond<T>& pc, const T* f0, const KrylovScal
     if (d < 0) return cudaSuccess;
     const unsigned gd = (unsigned)((pc.dense.n + kGemvWarps - 1) / kGemvWarps);
     if (d == 0) {
-        k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, f0, pc.lev[0].u, sc);
+        dense_gemv<T>(pc.dense, f0, pc.lev[0].u, sc, s);
         return cudaGetLastError();
     }
     k_coarse_rows<T, const T*><<<rows_grid(pc.lev[0].M), 256, 0, s>>>(pc.lev[0].M, f0, DevEll<T>(), nullptr, 0,
@@ -260,7 +366,7 @@ cudaError_t coarse_cycle_vec(const Precond<T>& pc, const T* f0, const KrylovScal
         k_coarse_rows<T, const T*><<<rows_grid(L.M), 256, 0, s>>>(L.M, L.f, DevEll<T>(), nullptr, 0,
                                                                    pc.lev[l + 1].f, sc);
     }
-    k_dense_gemv<T><<<gd, 32 * kGemvWarps, 0, s>>>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc);
+    dense_gemv<T>(pc.dense, pc.lev[d].f, pc.lev[d].u, sc, s);
     for (int l = d - 1; l >= 1; --l) {
         const CoarseLevel<T>& L = pc.lev[l];
         k_coarse_rows<T, const T*><<<rows_grid(L.S), 256, 0, s>>>(L.S, L.f, L.Q, pc.lev[l + 1].u, 1, L.u, sc);
@@ -281,7 +387,7 @@ template <typename T>
 int coarse_launches(const Precond<T>& pc) {
     if (pc.nlev <= 0) return 0;
     const int d = pc.nlev - 1;
-    return d + 1 + (d > 1 ? d - 1 : 0);
+    return d == 0 ? 1 : d + 1 + (d - 1) + 1;
 }
 
 // Algorithmic bytes of one coarse cycle as coarse_cycle launches it: every row-padded
@@ -293,25 +399,21 @@ int coarse_cycle_bytes(const Precond<T>& pc) {
     if (pc.nlev <= 0) return 0;
     const int d = pc.nlev - 1;
     auto ell = [](const DevEll<T>& A) { return (double)A.n * A.w * (sizeof(T) + (A.col ? 4 : 0)); };
-    double b = (double)pc.dense.n * pc.dense.w * sizeof(T) + 2.0 * pc.dense.n * sizeof(T);
+    const double dsz = pc.dense.val16 ? 2.0 : (double)sizeof(T);
+    double b = (double)pc.dense.n * pc.dense.w * dsz + 2.0 * pc.dense.n * sizeof(T);
     if (d == 0) return (int)(b + 3.0 * pc.dense.n * sizeof(T));
     b += ell(pc.lev[0].M) + 3.0 * pc.lev[0].n * sizeof(T) + pc.lev[1].n * sizeof(T);
     for (int l = 1; l < d; ++l) b += ell(pc.lev[l].M) + (double)(pc.lev[l].n + pc.lev[l + 1].n) * sizeof(T);
     for (int l = d - 1; l >= 1; --l)
         b += ell(pc.lev[l].S) + ell(pc.lev[l].Q) + (double)(2 * pc.lev[l].n + pc.lev[l + 1].n) * sizeof(T);
+    b += ell(pc.lev[0].S) + ell(pc.lev[0].Q) + (double)(4 * pc.lev[0].n + pc.lev[1].n) * sizeof(T);
     return (int)b;
 }
 
 template <typename T>
 CoarseOut<T> coarse_out(const Precond<T>& pc) {
     CoarseOut<T> c;
-    if (pc.nlev == 1) {
-        c.u0 = pc.lev[0].u;
-    } else {
-        c.S = pc.lev[0].S;
-        c.Q = pc.lev[0].Q;
-        c.u1 = pc.lev[1].u;
-    }
+    c.ue5 = pc.ue5;
     return c;
 }
 

@@ -56,6 +56,9 @@ struct FrGeom {
     const int* sw_p;        // [N_eb]
     const int* sw_d;        // [N_eb]
     const int* noslip;      // [n_groups]
+    // [N_eb][K][K] inverse of the Neumann common-value system of every boundary edge with a
+    // Neumann psi or vorticity condition, rows scaled by 1/J_f (zero elsewhere)
+    const T* nminv;
 };
 
 // Boundary-edge arrays, always double (they carry the 1/(dt Re^-1) wall flux).

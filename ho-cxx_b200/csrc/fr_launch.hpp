@@ -48,13 +48,19 @@ struct ResidualArgs {
 
 template <typename T>
 cudaError_t launch_trace(int K, int N, const T* f, T* tv, T* tg, const DevBases<T>& b, cudaStream_t s);
-// g and bp in the precision of psi (TP), bw in that of omega (T)
-template <typename T, typename TP>
-cudaError_t launch_velocity(int K, const FrGeom<TP>& g, const DevBases<TP>& bp, const DevBases<T>& bw,
-                            const BcArrays& bc, const VelocityArgs<T, TP>& a, cudaStream_t s);
+// The metric coefficients g11, g12, g22 of the contravariant gradient ([N][K][K], the
+// Poisson operator's PoisGeom G11/G12/G22) in the stage kernels' precision.
 template <typename T>
-cudaError_t launch_residual(int K, const FrGeom<T>& g, const DevBases<T>& b, const BcArrays& bc,
-                            const ResidualArgs<T>& a, cudaStream_t s);
+struct StageCoef {
+    const T *G11, *G12, *G22;
+};
+// g, c and bp in the precision of psi (TP), bw in that of omega (T)
+template <typename T, typename TP>
+cudaError_t launch_velocity(int K, const FrGeom<TP>& g, const StageCoef<TP>& c, const DevBases<TP>& bp,
+                            const DevBases<T>& bw, const BcArrays& bc, const VelocityArgs<T, TP>& a, cudaStream_t s);
+template <typename T>
+cudaError_t launch_residual(int K, const FrGeom<T>& g, const StageCoef<T>& c, const DevBases<T>& b,
+                            const BcArrays& bc, const ResidualArgs<T>& a, cudaStream_t s);
 template <typename T>
 cudaError_t launch_poisson_rhs(int K, int N, const int* face_nb, const T* w, const T* J, const double* bsrc,
                                const double* bc_p, double* rhs, cudaStream_t s);
@@ -116,6 +122,12 @@ struct MfOp {
     const T* kron_f = nullptr;
     const int* kron_x = nullptr;
     const T* kron_exact = nullptr;
+    // [N][5][K2] the smoother's element inverse applied to each block row sum (k_make_w)
+    const T* W = nullptr;
+    // host side: a second stream and two events; when set, each coarse cycle runs on the
+    // second stream beside the fine part of the smoothing step (k_post_a)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 template <typename T>
@@ -128,6 +140,7 @@ struct BicgVectors {
     // alternate with the iteration count: the coarse right-hand sides P^T p and P^T s are
     // linear combinations of them, formed wherever they are read
     T *er, *ev, *ep[2];
+    T* zf;  // the fine part M f of the current preconditioner application (k_post_a)
 };
 
 // The level-0 coarse right-hand side of one preconditioner application, formed where it
@@ -175,6 +188,9 @@ struct DevEll {
     int g = 1;  // lanes that cooperate on one row (a power of two <= 32)
     const int* col = nullptr;
     const T* val = nullptr;
+    // the dense coarsest inverse of the FP32 preconditioner is stored as BF16 bit patterns
+    // (rows padded to a multiple of 8 values); val is then null
+    const unsigned short* val16 = nullptr;
 };
 
 // One level of the coarse hierarchy (level 0 = one value per element). Its V(1,1) cycle
@@ -196,16 +212,18 @@ struct Precond {
     double omega = 1.0;  // weight of the block-Jacobi smoothing step
     CoarseLevel<T> lev[kMaxLevels];
     DevEll<T> dense;  // row-major inverse of the coarsest operator (col == nullptr)
+    // level-0 result delivered per element: ue5[5 el + s] = u0 of the element in block slot s
+    // of element el (s = 0 itself, 1 + ijp its face neighbours; 0 where there is none);
+    // u0dst[5 c + k] lists the slots element c's value goes to (-1: unused)
+    T* ue5 = nullptr;
+    const int* u0dst = nullptr;
 };
 
-// What the fine smoothing step needs of the coarse result: u0 directly (one level), or
-// the level-0 up step u0 = S0 f0 + Q0 u1 evaluated per element where it is used (f0 is
-// formed from the element sums, F0 above).
+// What the fine smoothing step needs of the coarse result: u0 at each element's five block
+// slots (the whole cycle, level 0's up step included, ran before it).
 template <typename T>
 struct CoarseOut {
-    const T* u0 = nullptr;
-    DevEll<T> S, Q;
-    const T* u1 = nullptr;
+    const T* ue5 = nullptr;  // [N][5]: u0 of each element's five block slots (Precond::ue5)
 };
 
 // enqueues the coarse part of one preconditioner application (mode 0: on P^T p, mode 1:
@@ -232,8 +250,9 @@ cudaError_t krylov_iteration(const MfOp<T>& op, const BicgVectors<T>& v, const R
                              const Precond<T>& pc, cudaStream_t s);
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc);
-// one iteration as krylov_iteration, with the boundaries between its launches recorded on
-// 8 events (coarse, smoothing, operator, coarse, smoothing, operator, update)
+// one iteration as krylov_iteration, in order on s, with the boundaries between its
+// launches recorded on 10 events (coarse, fine smoothing part, combination, operator,
+// coarse, fine smoothing part, combination, operator, update)
 template <typename T>
 cudaError_t krylov_iteration_timed(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                                    const Precond<T>& pc, cudaEvent_t* ev, cudaStream_t s);
@@ -263,6 +282,10 @@ int krylov_max_blocks(int K, int N);
 // per-device set-up of the Krylov kernels for order K (krylov.cu): before the first launch
 // or graph capture on the device
 cudaError_t krylov_configure(int K);
+// W = M rowsum for the 5 block slots of every element ([N][5][K2], T), with the smoother
+// op selects (its element inverse M: exact blocks, BF16 blocks or Kronecker-sum factors)
+template <typename T>
+cudaError_t krylov_make_w(const MfOp<T>& op, T* W, KrylovScalars* sc, cudaStream_t s);
 
 // out[0..1] = FP64 force on a body from its boundary points' precomputed coefficients
 // (forces.cu): coef [npts][4], idx = index of each point in the boundary arrays

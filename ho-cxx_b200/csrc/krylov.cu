@@ -4,8 +4,8 @@
 // 5 K^4 entries per element (src/HO_2D.cpp:1533-1804, 3011-3062) and hands it to AMGCL.
 // That matrix is exactly the method-2 FR Laplacian of calc_RHS_diffusion applied with
 // homogeneous Poisson boundary values, so here A x is evaluated matrix-free from face
-// traces (lap_element in fr_device.cuh): per DOF it reads x, 5 volume metrics and a
-// share of the face data instead of 5 K^2 matrix entries. Every kernel that produces
+// traces (row_apply in rows.cuh): per DOF it reads x, 3 metric coefficients and a share
+// of the face data instead of 5 K^2 matrix entries. Every kernel that produces
 // a vector the operator is applied to next also writes that vector's face traces, so
 // one operator application is one launch.
 //
@@ -33,6 +33,15 @@ namespace ho2d {
 
 namespace {
 
+// Deterministic grid-wide sum of NV values per thread, in two levels so no CTA reads more
+// than a few hundred partials: every CTA stores its sums; the last CTA to finish within
+// each group of kReduceGroup consecutive CTAs adds the group's sums (fixed order) and
+// stores the group total; the last group to finish adds the group totals (fixed order)
+// and gets `out`, returning true in that CTA only. Counters: counter[0] for the groups,
+// counter[1 + g] for group g; every one is back to zero when the kernel ends. partials
+// holds NV x (gridDim.x + the number of groups) doubles. Collective (all threads).
+constexpr int kReduceGroup = 64;
+
 template <int NV>
 __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* counter,
                                             double (&out)[NV]) {
@@ -40,6 +49,10 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     __shared__ double fin[NV];
     __shared__ bool s_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int G = (int)gridDim.x, ng = (G + kReduceGroup - 1) / kReduceGroup;
+    const int grp = (int)blockIdx.x / kReduceGroup;
+    const int g0 = grp * kReduceGroup, gs = min(kReduceGroup, G - g0);
+    double* gpart = partials + (size_t)NV * G;
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         double x = v[j];
@@ -54,21 +67,38 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
             double x = lane < nw ? red[j][lane] : 0.0;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-            if (lane == 0) partials[j * gridDim.x + blockIdx.x] = x;
+            if (lane == 0) partials[j * G + blockIdx.x] = x;
         }
         __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x == 0) s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) s_last = (atomicAdd(&counter[1 + grp], 1u) == (unsigned)gs - 1);
+    __syncthreads();
+    if (!s_last) return false;
+    // the group's total: warp 0 adds its <= 64 CTA sums (lanes l and l + 32, then a tree)
+    __threadfence();
+    if (warp == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double x = lane < gs ? __ldcg(&partials[j * G + g0 + lane]) : 0.0;
+            if (lane + 32 < gs) x += __ldcg(&partials[j * G + g0 + lane + 32]);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+            if (lane == 0) gpart[j * ng + grp] = x;
+        }
+        if (lane == 0) counter[1 + grp] = 0u;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(&counter[0], 1u) == (unsigned)ng - 1);
     __syncthreads();
     if (!s_last) return false;
     __threadfence();
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
-        // the partial loads are independent: unrolled, a thread keeps up to 8 in flight
         double x = 0.0;
-#pragma unroll 8
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) x += __ldcg(&partials[j * gridDim.x + i]);
+#pragma unroll 4
+        for (int i = threadIdx.x; i < ng; i += blockDim.x) x += __ldcg(&gpart[j * ng + i]);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
         if (lane == 0) red[j][warp] = x;
@@ -86,38 +116,8 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < NV; ++j) out[j] = fin[j];
-    if (threadIdx.x == 0) *counter = 0u;
+    if (threadIdx.x == 0) counter[0] = 0u;
     return true;
-}
-
-// Scatter destinations of the face points thread ij emits (prefetched at kernel start).
-template <int K>
-struct TraceDst {
-    static constexpr int K2 = K * K, NF = 4 * K, NO = (NF + K2 - 1) / K2;
-    int dst[NO];
-    __device__ __forceinline__ void load(const int* scat, bool active, int el, int ij) {
-#pragma unroll
-        for (int q = 0; q < NO; ++q) {
-            const int o = ij + q * K2;
-            dst[q] = (active && o < NF) ? scat[el * NF + o] : -1;
-        }
-    }
-};
-
-// face traces of an element vector held in shared memory, written to the neighbours'
-// incoming slots
-template <int K, typename T>
-__device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, const TraceDst<K>& td, T* tv, T* tg,
-                                            int ij) {
-    constexpr int K2 = K * K;
-#pragma unroll
-    for (int q = 0; q < TraceDst<K>::NO; ++q) {
-        if (td.dst[q] < 0) continue;
-        T v, d;
-        face_trace<K, T>(sy, b, ij + q * K2, v, d);
-        tv[td.dst[q]] = v;
-        tg[td.dst[q]] = d;
-    }
 }
 
 }  // namespace
@@ -128,6 +128,21 @@ __device__ __forceinline__ void emit_traces(const T* sy, const DevBases<T>& b, c
 template <int K>
 static __host__ __device__ constexpr unsigned rgrid_of(int N) {
     return (unsigned)((N + Rows<K>::EPC - 1) / Rows<K>::EPC);
+}
+
+// CTAs of one full wave of each reducing row kernel (resident CTAs per SM x SMs), per K and
+// precision ([K][0] FP64, [K][1] FP32): those kernels loop over element tiles, so one wave
+// covers any mesh and each CTA reduces once. Set by krylov_configure.
+struct WaveSizes {
+    unsigned init = 0, v = 0, t = 0, xr = 0, res = 0;
+};
+static WaveSizes g_wave[9][2];
+
+template <int K, typename T>
+static unsigned wave_of(unsigned WaveSizes::*which, int N) {
+    const unsigned w = g_wave[K][std::is_same<T, float>::value ? 1 : 0].*which;
+    const unsigned nt = rgrid_of<K>(N);
+    return w == 0 || w > nt ? nt : w;
 }
 
 // incoming face traces of x (the operand of an operator application that no Krylov
@@ -141,37 +156,49 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_trace_in(MfOp<T> op, const
     int dst[4];
     if (ix.active) {
         load_row<K, T>(x + (size_t)ix.el * K * K + ix.t * K, row);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) dst[f] = op.g.scat[(size_t)ix.el * 4 * K + f * K + ix.t];
+        load4i(op.g.scat + ((size_t)ix.el * K + ix.t) * 4, dst);
     }
     row_emit_traces<K, T>(op.b, buf[ix.warp][ix.lw], row, dst, tv, tg, ix.t, ix.active);
 }
 
-// r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2; element sums of r
+// r = b - A x (x's traces in xtv/xtg), rhat = r; ||r||^2, ||b||^2; element sums of r. Like
+// every reducing row kernel it runs as one wave of CTAs, each taking element tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... and reducing once.
 template <int K, typename T>
 __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_init(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
-    const RowIdx<K> ix(op.g.N, blockIdx.x);
-    T y[K];
-    row_apply<K, T>(op, v.x, v.xtv, v.xtg, sm[ix.warp], ix, y);
+    const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[2] = {0.0, 0.0};
-    T rsum = T(0);
-    if (ix.active) {
-        const size_t p = (size_t)ix.el * K * K + ix.t * K;
-        T bb[K], r[K];
-        load_row<K, T>(v.b + p, bb);
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, v.x, v.xtv, v.xtg, sm[ix.warp], ix, y);
+        T rsum = T(0);
+        if (ix.active) {
+            const size_t p = (size_t)ix.el * K * K + ix.t * K;
+            T bb[K], r[K];
+            load_row<K, T>(v.b + p, bb);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            r[i] = bb[i] - y[i];
-            rsum += r[i];
-            part[0] += double(r[i]) * double(r[i]);
-            part[1] += double(bb[i]) * double(bb[i]);
+            for (int i = 0; i < K; ++i) {
+                r[i] = bb[i] - y[i];
+                rsum += r[i];
+                part[0] += double(r[i]) * double(r[i]);
+                part[1] += double(bb[i]) * double(bb[i]);
+            }
+            store_row<K, T>(v.r + p, r);
+            store_row<K, T>(v.rhat + p, r);
         }
-        store_row<K, T>(v.r + p, r);
-        store_row<K, T>(v.rhat + p, r);
+        const T tot = element_total<K, T>(rsum, ix.lw);
+        if (ix.active && ix.t == 0) v.er[ix.el] = tot;
+    };
+    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
+    // push the operator past the register file)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll 1
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+    } else {
+        if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }
-    const T tot = element_total<K, T>(rsum, ix.lw);
-    if (ix.active && ix.t == 0) v.er[ix.el] = tot;
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         KrylovScalars* sc = rs.sc;
@@ -197,47 +224,26 @@ __global__ void k_zero_if(T* x, size_t n, const KrylovScalars* sc) {
 }
 
 
-// Part `part` (0..4) of u0 at element c = S0_c . f0 + Q0_c . u1 (a row of the level-0
-// up step): the row entries part, part + 5, ... The first two of each row are loaded
-// before any gather, so a part costs two dependent rounds of loads.
-template <typename T>
-__device__ __forceinline__ T up0_part(const CoarseOut<T>& co, const F0<T>& f0, int c, int part) {
-    const size_t rs = (size_t)c * co.S.w, rq = (size_t)c * co.Q.w;
-    T sv[2], qv[2];
-    int sj[2], qj[2];
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        const int k = part + 5 * m;
-        const bool ins = k < co.S.w, inq = k < co.Q.w;
-        sv[m] = ins ? co.S.val[rs + k] : T(0);
-        sj[m] = ins ? co.S.col[rs + k] : 0;
-        qv[m] = inq ? co.Q.val[rq + k] : T(0);
-        qj[m] = inq ? co.Q.col[rq + k] : 0;
-    }
-    T u = sv[0] * f0[sj[0]] + qv[0] * co.u1[qj[0]] + sv[1] * f0[sj[1]] + qv[1] * co.u1[qj[1]];
-    for (int k = part + 10; k < co.S.w; k += 5) u += co.S.val[rs + k] * f0[co.S.col[rs + k]];
-    for (int k = part + 10; k < co.Q.w; k += 5) u += co.Q.val[rq + k] * co.u1[co.Q.col[rq + k]];
-    return u;
-}
-
 // The smoother's element data (BS): 0 = inverse blocks in T; 1 = inverse blocks as BF16 bit
 // patterns (FP32 smoother); 2 = Kronecker-sum factors, with the exact blocks only for the
 // elements the fit does not approximate well (FP32 smoother). Each element's data starts on
-// a 16-byte boundary (padded_count). For BS 0 and 1 a warp's EPW blocks are one contiguous
-// span, copied into shared memory by one bulk copy when the span is at most 26 KB (so a
-// CTA's four spans leave room for two CTAs per SM); larger blocks are read from global
-// memory directly.
+// a 16-byte boundary (padded_count). A warp's EPW blocks (or factor sets) are one
+// contiguous span, copied into shared memory by one bulk copy when the span is at most
+// 26 KB (so a CTA's four spans leave room for two CTAs per SM); larger blocks are read
+// from global memory directly.
 template <int K, typename T, int BS>
 struct PostRows {
     using DT = typename std::conditional<BS == 1, unsigned short, T>::type;
     static constexpr int K2 = K * K, K4 = K2 * K2;
     static constexpr int STRIDE = padded_count(K4, (int)sizeof(DT));  // values of DT per element
-    static constexpr int SPAN = Rows<K>::EPW * STRIDE * (int)sizeof(DT);  // bytes per warp
-    static constexpr bool kStage = BS != 2 && SPAN <= 26 * 1024;
-    static constexpr int SMEM = kStage ? Rows<K>::WARPS * SPAN : 0;  // dynamic shared memory
     static constexpr int KF = 4 * K2 + 2 * K;                      // Kronecker factors per element
     static constexpr int KFS = padded_count(KF, (int)sizeof(T));
     static constexpr int XSTRIDE = padded_count(K4, (int)sizeof(T));  // compact exact blocks (BS 2)
+    // bytes of one element's staged data: its inverse block, or (BS 2) its factors
+    static constexpr int ELEM = BS == 2 ? KFS * (int)sizeof(T) : STRIDE * (int)sizeof(DT);
+    static constexpr int SPAN = Rows<K>::EPW * ELEM;  // bytes per warp
+    static constexpr bool kStage = SPAN <= 26 * 1024;
+    static constexpr int SMEM = kStage ? Rows<K>::WARPS * SPAN : 0;  // dynamic shared memory
 };
 
 __device__ __forceinline__ float block_value(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
@@ -310,84 +316,161 @@ __device__ __forceinline__ void block_rows(const DT* blk, const T* sr, int t, T 
     }
 }
 
-// Preconditioner application, with the BiCGSTAB vector update that produces its operand:
-//   mode 0:  p = r + beta (p - omega v)  (p = r on the first iteration),  f = p -> ph
-//   mode 1:  s = r - alpha v, ||s||^2 (s_exit test),                      f = s -> sh
-// then the two-level smoothing step z = e + w D^{-1} (f - A e), e = P u0 element-wise
-// constant, with z's face traces. u0 of the element and of its four face neighbours comes
-// straight from the coarse cycle (one-level hierarchy), or from the level-0 up step
-// u0 = S0 f0 + Q0 u1 evaluated here as 25 partial sums (five per slot) spread over the
-// element's threads, or is zero (block-Jacobi, no coarse level). Mode 0 also stores the
-// element sums of the new p for the next iteration. Row-parallel (rows.cuh): thread t of
-// an element owns row t. The warp's inverse blocks are requested first, by one bulk copy
-// into shared memory (PostRows::kStage), so the copy overlaps the up step's dependent
-// loads and the vector loads.
-template <int K, typename T, int BS = 0>
-__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_post(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
-                                                               int has_coarse, double w, ReduceScratch rs, int mode) {
-    using R = Rows<K>;
+// The smoother's element inverse M (exact block, BF16 block or Kronecker-sum factors)
+// applied to one element vector held in shared memory (srow, K^2 values, [j][i]): row t of
+// M srow into acc. For BS 2 the transposes are warp-collective, so every lane runs them;
+// zb is a K x K scratch of the element. Warp-collective.
+template <int K, typename T, int BS>
+__device__ __forceinline__ void smoother_rows(const MfOp<T>& op, const typename PostRows<K, T, BS>::DT* blk,
+                                              const T* fk, int kx, const T* srow, T (&zb)[K][K], int t, bool act,
+                                              T (&acc)[K]) {
     using PS = PostRows<K, T, BS>;
-    using DT = typename PS::DT;
+    constexpr int K2 = K * K;
+    if constexpr (BS == 2) {
+        // exact block where the fit falls back, Kronecker-sum step (fast diagonalisation,
+        // the element body of kron_apply.cuh by rows) for the others
+        const bool kr = act && kx < 0;
+        if (act && kx >= 0) block_rows<K, T, T>(op.kron_exact + (size_t)kx * PS::XSTRIDE, srow, t, acc);
+        const T *vx = fk, *vxi = fk + K2, *vy = fk + 2 * K2, *vyi = fk + 3 * K2, *lx = fk + 4 * K2, *ly = lx + K;
+        T c1[K], r1[K], r2[K], c2[K], c3[K], r3[K];
+        // column t of Vy^-1 R
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) s += vyi[j * K + l] * srow[l * K + t];
+            }
+            c1[j] = s;
+        }
+        col_to_row<K, T>(zb, c1, r1, t, kr);
+        // row t of (Vy^-1 R Vx^-T) ./ (ly_t + lx_i)
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) s += r1[k] * vxi[i * K + k];
+                s = s / (ly[t] + lx[i]);
+            }
+            r2[i] = s;
+        }
+        __syncwarp();  // zb is rewritten next
+        rows_to_col<K, T>(zb, r2, c2, t, kr);
+        // column t of Vy (that), then row t of the product with Vx^T
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            T s = T(0);
+            if (kr) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) s += vy[j * K + l] * c2[l];
+            }
+            c3[j] = s;
+        }
+        __syncwarp();
+        col_to_row<K, T>(zb, c3, r3, t, kr);
+        if (kr) {
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                T s = T(0);
+#pragma unroll
+                for (int k = 0; k < K; ++k) s += r3[k] * vx[i * K + k];
+                acc[i] = s;
+            }
+        }
+        __syncwarp();  // zb may be reused by the caller
+    } else {
+        if (act) block_rows<K, T, typename PS::DT>(blk, srow, t, acc);
+    }
+}
+
+// The warp's smoother element data: one bulk copy of its EPW inverse blocks (or factor
+// sets) into its slice of the dynamic shared memory when PostRows::kStage, issued by lane 0
+// on barrier bar; blk/fk point at this element's data (staged or global).
+template <int K, typename T, int BS>
+struct SmootherData {
+    const typename PostRows<K, T, BS>::DT* blk = nullptr;
+    const T* fk = nullptr;
+    int kx = -1;
+    int wn = 0;
+    __device__ __forceinline__ void start(const MfOp<T>& op, const RowIdx<K>& ix, unsigned char* dyn, uint64_t* bar,
+                                          bool issue) {
+        using PS = PostRows<K, T, BS>;
+        using DT = typename PS::DT;
+        constexpr int EPW = Rows<K>::EPW;
+        const DT* dsrc;
+        if constexpr (BS == 1) dsrc = op.dinv_bf16;
+        else dsrc = op.dinv;
+        const int wel0 = (blockIdx.x * Rows<K>::WARPS + ix.warp) * EPW;
+        wn = min(EPW, op.g.N - wel0);
+        blk = dsrc + (size_t)(ix.active ? ix.el : 0) * PS::STRIDE;
+        fk = BS == 2 ? op.kron_f + (size_t)(ix.active ? ix.el : 0) * PS::KFS : nullptr;
+        if constexpr (BS == 2) {
+            if (ix.active) kx = op.kron_x[ix.el];
+        }
+        if constexpr (PS::kStage) {
+            unsigned char* stage = dyn + (size_t)ix.warp * PS::SPAN;
+            if (issue && wn > 0 && ix.lane == 0) {
+                const unsigned char* src = BS == 2 ? reinterpret_cast<const unsigned char*>(op.kron_f)
+                                                   : reinterpret_cast<const unsigned char*>(dsrc);
+                mbar_init(bar);
+                const unsigned bytes = (unsigned)(wn * PS::ELEM);
+                mbar_arrive_expect(bar, bytes);
+                bulk_load(stage, src + (size_t)wel0 * PS::ELEM, bytes, bar);
+            }
+            if constexpr (BS == 2) fk = reinterpret_cast<const T*>(stage + (size_t)ix.lw * PS::ELEM);
+            else blk = reinterpret_cast<const DT*>(stage + (size_t)ix.lw * PS::ELEM);
+        }
+    }
+    // wait for the copy; a wait that runs out is recorded for the host, the copy gets a
+    // second bounded wait, and the kernel runs on so its reductions stay consistent
+    __device__ __forceinline__ void wait(uint64_t* bar, KrylovScalars* sc, int lane) {
+        if constexpr (PostRows<K, T, BS>::kStage) {
+            if (wn > 0 && !mbar_wait_bounded(bar, 0, kBulkWaitPolls)) {
+                if (lane == 0) atomicExch(&sc->dev_error, 1);
+                mbar_wait_bounded(bar, 0, kBulkWaitPolls);
+            }
+        }
+    }
+};
+
+// Fine part of one preconditioner application, with the BiCGSTAB vector update that
+// produces its operand:
+//   mode 0:  p = r + beta (p - omega v)  (p = r on the first iteration),  f = p
+//   mode 1:  s = r - alpha v, ||s||^2 (s_exit test),                      f = s
+// then zf = M f with the smoother's element inverse M (exact FP32/FP64 block, BF16 block or
+// Kronecker-sum factors). It needs nothing of the coarse cycle, which runs beside it on a
+// second stream; k_post_b combines the two. Mode 0 also stores the element sums of the new
+// p for the next iteration. Row-parallel (rows.cuh): thread t of an element owns row t. The
+// warp's element data are requested first, by one bulk copy into shared memory
+// (PostRows::kStage), so the copy overlaps the vector loads.
+template <int K, typename T, int BS = 0>
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_post_a(MfOp<T> op, BicgVectors<T> v, int has_coarse,
+                                                              ReduceScratch rs, int mode) {
+    using R = Rows<K>;
     constexpr int K2 = R::K2, EPW = R::EPW;
     KrylovScalars* sc = rs.sc;
     const int done = sc->done;  // uniform; read early so the round trip overlaps the loads
     extern __shared__ __align__(128) unsigned char post_dyn[];
     __shared__ __align__(8) uint64_t bar[R::WARPS];
-    __shared__ T pu[R::WARPS][EPW][25];
     __shared__ __align__(16) T sr[R::WARPS][EPW][K2];
     __shared__ T zb[R::WARPS][EPW][K][K];
-    __shared__ __align__(16) T kf[BS == 2 ? R::WARPS : 1][BS == 2 ? EPW : 1][BS == 2 ? PS::KFS : 1];
     const RowIdx<K> ix(op.g.N, blockIdx.x);
     const int t = ix.t, lw = ix.lw, el = ix.el;
     const bool act = ix.active;
-    const DT* dsrc;
-    if constexpr (BS == 1) dsrc = op.dinv_bf16;
-    else dsrc = op.dinv;
-    // this warp's blocks: one bulk copy, issued before anything else
-    const int wel0 = (blockIdx.x * R::WARPS + ix.warp) * EPW;
-    const int wn = min(EPW, op.g.N - wel0);  // elements of this warp (<= 0: none)
-    const DT* blk = dsrc + (size_t)el * PS::STRIDE;
-    if constexpr (PS::kStage) {
-        DT* stage = reinterpret_cast<DT*>(post_dyn + (size_t)ix.warp * PS::SPAN);
-        if (!done && wn > 0 && ix.lane == 0) {
-            mbar_init(&bar[ix.warp]);
-            const unsigned bytes = (unsigned)(wn * PS::STRIDE * (int)sizeof(DT));
-            mbar_arrive_expect(&bar[ix.warp], bytes);
-            bulk_load(stage, dsrc + (size_t)wel0 * PS::STRIDE, bytes, &bar[ix.warp]);
-        }
-        blk = stage + (size_t)lw * PS::STRIDE;
-    }
-    // this thread's rows of the vectors and block row sums, its face points' destinations
+    SmootherData<K, T, BS> sd;
+    sd.start(op, ix, post_dyn, &bar[ix.warp], !done);
     const size_t p = (size_t)el * K2 + t * K;
-    T rr[K], vv[K], pp[K], rsum[5][K];
-    int dst[4];
+    T rr[K], vv[K], pp[K];
     if (act) {
         load_row<K, T>(v.r + p, rr);
         load_row<K, T>(v.v + p, vv);
         if (mode == 0) load_row<K, T>(v.p + p, pp);
-#pragma unroll
-        for (int s = 0; s < 5; ++s) load_row<K, T>(op.rowsum + ((size_t)el * 5 + s) * K2 + t * K, rsum[s]);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) dst[f] = op.g.scat[(size_t)el * 4 * K + f * K + t];
     }
-    int kx = -1;  // BS 2: this element's exact block, or -1 for its Kronecker factors
-    if constexpr (BS == 2) {
-        if (act) {
-            kx = op.kron_x[el];
-            for (int q = t; q < PS::KF; q += K) kf[ix.warp][lw][q] = op.kron_f[(size_t)el * PS::KFS + q];
-        }
+    if (mode == 0 && has_coarse && act && t == 0) {
+        const F0<T> f0 = f0_of(v, sc, mode);
+        v.ep[(sc->it + 1) & 1][el] = f0[el];
     }
-    const F0<T> f0 = f0_of(v, sc, mode);
-    // u0 of block slot s (element bcol[5 el + s]) as five partial sums pu[s][part]
-    if (act)
-        for (int q = t; q < 25; q += K) {
-            const int slot = q / 5, part = q % 5;
-            const int c = op.bcol[el * 5 + slot];
-            T u = T(0);
-            if (c >= 0 && has_coarse) u = co.u0 ? (part == 0 ? co.u0[c] : T(0)) : up0_part(co, f0, c, part);
-            pu[ix.warp][lw][q] = u;
-        }
-    if (mode == 0 && has_coarse && act && t == 0) v.ep[(sc->it + 1) & 1][el] = f0[el];
     // the operand: p or s
     T f[K];
     if (mode == 0) {
@@ -406,102 +489,16 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_post(MfOp<T> op, BicgVe
         for (int i = 0; i < K; ++i) f[i] = rr[i] - al * vv[i];
     }
     if (done) return;  // uniform over the grid: no copy was issued
-    if (act) store_row<K, T>((mode == 0 ? v.p : v.s) + p, f);
-    __syncwarp();
-    // the five slot values, each the sum of its five parts (part 0..4 in order), and the
-    // smoother's residual row f - A e
-    T ue[5];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-        const T* pq = pu[ix.warp][lw] + 5 * q;
-        ue[q] = pq[0] + pq[1] + pq[2] + pq[3] + pq[4];
-    }
     if (act) {
+        store_row<K, T>((mode == 0 ? v.p : v.s) + p, f);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            T ae = T(0);
-#pragma unroll
-            for (int s = 0; s < 5; ++s) ae += rsum[s][i] * ue[s];
-            sr[ix.warp][lw][t * K + i] = f[i] - ae;
-        }
+        for (int i = 0; i < K; ++i) sr[ix.warp][lw][t * K + i] = f[i];
     }
     __syncwarp();
-    if constexpr (PS::kStage) {
-        if (wn > 0 && !mbar_wait_bounded(&bar[ix.warp], 0, kBulkWaitPolls)) {
-            // record the failure for the host and give the copy a second bounded wait; the
-            // kernel then runs to its end so the grid-wide reduction stays consistent
-            if (ix.lane == 0) atomicExch(&sc->dev_error, 1);
-            mbar_wait_bounded(&bar[ix.warp], 0, kBulkWaitPolls);
-        }
-    }
-    T* z = mode == 0 ? v.ph : v.sh;
-    const T* srow = sr[ix.warp][lw];
+    sd.wait(&bar[ix.warp], sc, ix.lane);
     T acc[K];
-    if constexpr (BS == 2) {
-        // exact block where the fit falls back, Kronecker-sum step (fast diagonalisation,
-        // the element body of kron_apply.cuh by rows) for the others; the transposes are
-        // warp-collective, so every lane runs them
-        const bool kr = act && kx < 0;
-        if (act && kx >= 0) block_rows<K, T, T>(op.kron_exact + (size_t)kx * PS::XSTRIDE, srow, t, acc);
-        const T* fk = kf[ix.warp][lw];
-        const T *vx = fk, *vxi = fk + K2, *vy = fk + 2 * K2, *vyi = fk + 3 * K2, *lx = fk + 4 * K2, *ly = lx + K;
-        T c1[K], r1[K], r2[K], c2[K], c3[K], r3[K];
-        // column t of Vy^-1 R
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            T s = T(0);
-            if (kr) {
-#pragma unroll
-                for (int l = 0; l < K; ++l) s += vyi[j * K + l] * srow[l * K + t];
-            }
-            c1[j] = s;
-        }
-        col_to_row<K, T>(zb[ix.warp][lw], c1, r1, t, kr);
-        // row t of (Vy^-1 R Vx^-T) ./ (ly_t + lx_i)
-#pragma unroll
-        for (int i = 0; i < K; ++i) {
-            T s = T(0);
-            if (kr) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) s += r1[k] * vxi[i * K + k];
-                s = s / (ly[t] + lx[i]);
-            }
-            r2[i] = s;
-        }
-        __syncwarp();  // zb is rewritten next
-        rows_to_col<K, T>(zb[ix.warp][lw], r2, c2, t, kr);
-        // column t of Vy (that), then row t of the product with Vx^T
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            T s = T(0);
-            if (kr) {
-#pragma unroll
-                for (int l = 0; l < K; ++l) s += vy[j * K + l] * c2[l];
-            }
-            c3[j] = s;
-        }
-        __syncwarp();
-        col_to_row<K, T>(zb[ix.warp][lw], c3, r3, t, kr);
-        if (kr) {
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                T s = T(0);
-#pragma unroll
-                for (int k = 0; k < K; ++k) s += r3[k] * vx[i * K + k];
-                acc[i] = s;
-            }
-        }
-        __syncwarp();  // zb is the trace buffer below
-    } else {
-        if (act) block_rows<K, T, DT>(blk, srow, t, acc);
-    }
-    T zz[K];
-    if (act) {
-#pragma unroll
-        for (int i = 0; i < K; ++i) zz[i] = ue[0] + T(w) * acc[i];
-        store_row<K, T>(z + p, zz);
-    }
-    row_emit_traces<K, T>(op.b, zb[ix.warp][lw], zz, dst, v.tv, v.tg, t, act);
+    smoother_rows<K, T, BS>(op, sd.blk, sd.fk, sd.kx, sr[ix.warp][lw], zb[ix.warp][lw], t, act, acc);
+    if (act) store_row<K, T>(v.zf + p, acc);
     if (mode == 1) {
         double part[1] = {0.0};
         if (act) {
@@ -516,33 +513,120 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_post(MfOp<T> op, BicgVe
     }
 }
 
+// Coarse part of the preconditioner application and the result: the two-level smoothing
+// step z = e + w M (f - A e), e = P u0 element-wise constant, as
+//   z = u0_self + w (zf - sum_s W_s u0_s),   W_s = M rowsum_s  (k_make_w, at setup),
+// where A e = sum over the element's 5 block slots s (itself, its face neighbours) of the
+// block row sums times u0 of the slot's element; then z's face traces. Without a coarse
+// level (block-Jacobi) z = w zf.
+template <int K, typename T>
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_post_b(MfOp<T> op, BicgVectors<T> v, CoarseOut<T> co,
+                                                              int has_coarse, double w, const KrylovScalars* sc,
+                                                              int mode) {
+    using R = Rows<K>;
+    constexpr int K2 = R::K2;
+    if (sc->done) return;  // uniform
+    __shared__ T zb[R::WARPS][R::EPW][K][K];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    const int t = ix.t, el = ix.el;
+    const bool act = ix.active;
+    const size_t p = (size_t)el * K2 + t * K;
+    T zz[K];
+    int dst[4];
+    if (act) {
+        T zf[K];
+        load_row<K, T>(v.zf + p, zf);
+        load4i(op.g.scat + ((size_t)el * K + t) * 4, dst);
+        T ue[5], ws[5][K];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            ue[q] = has_coarse ? co.ue5[(size_t)el * 5 + q] : T(0);
+            if (has_coarse) load_row<K, T>(op.W + ((size_t)el * 5 + q) * K2 + t * K, ws[q]);
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            T ae = T(0);
+            if (has_coarse) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) ae += ws[q][i] * ue[q];
+            }
+            zz[i] = ue[0] + T(w) * (zf[i] - ae);
+        }
+        store_row<K, T>((mode == 0 ? v.ph : v.sh) + p, zz);
+    }
+    row_emit_traces<K, T>(op.b, zb[ix.warp][ix.lw], zz, dst, v.tv, v.tg, t, act);
+}
+
+// Setup: W_s = M rowsum_s for the 5 block slots of every element, with the smoother's own
+// element inverse M (so the split application k_post_a + k_post_b is exactly the smoothing
+// step of the stored smoother).
+template <int K, typename T, int BS>
+__global__ void __launch_bounds__(Rows<K>::THREADS) k_make_w(MfOp<T> op, T* __restrict__ W, KrylovScalars* sc) {
+    using R = Rows<K>;
+    constexpr int K2 = R::K2, EPW = R::EPW;
+    extern __shared__ __align__(128) unsigned char post_dyn[];
+    __shared__ __align__(8) uint64_t bar[R::WARPS];
+    __shared__ __align__(16) T sr[R::WARPS][EPW][K2];
+    __shared__ T zb[R::WARPS][EPW][K][K];
+    const RowIdx<K> ix(op.g.N, blockIdx.x);
+    const int t = ix.t, lw = ix.lw, el = ix.el;
+    const bool act = ix.active;
+    SmootherData<K, T, BS> sd;
+    sd.start(op, ix, post_dyn, &bar[ix.warp], true);
+    sd.wait(&bar[ix.warp], sc, ix.lane);
+    for (int q = 0; q < 5; ++q) {
+        const size_t rq = ((size_t)el * 5 + q) * K2 + t * K;
+        if (act) {
+            T r[K];
+            load_row<K, T>(op.rowsum + rq, r);
+#pragma unroll
+            for (int i = 0; i < K; ++i) sr[ix.warp][lw][t * K + i] = r[i];
+        }
+        __syncwarp();
+        T acc[K];
+        smoother_rows<K, T, BS>(op, sd.blk, sd.fk, sd.kx, sr[ix.warp][lw], zb[ix.warp][lw], t, act, acc);
+        if (act) store_row<K, T>(W + rq, acc);
+        __syncwarp();  // sr is rewritten for the next slot
+    }
+}
+
 // v = A ph; alpha = rho / (rhat, v); element sums of v
 template <int K, typename T>
 __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
-    // read before the operator's loads so the round trips overlap; the flag is uniform
-    // over the grid (only this kernel's last CTA writes it, after every CTA has read it)
-    const int done = sc->done;
+    // the flag is uniform over the grid (only this kernel's last CTA writes it, after every
+    // CTA has read it)
+    if (sc->done) return;
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
-    const RowIdx<K> ix(op.g.N, blockIdx.x);
-    T y[K];
-    row_apply<K, T>(op, v.ph, v.tv, v.tg, sm[ix.warp], ix, y);
-    if (done) return;
+    const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[1] = {0.0};
-    T ysum = T(0);
-    if (ix.active) {
-        const size_t p = (size_t)ix.el * K * K + ix.t * K;
-        T rh[K];
-        load_row<K, T>(v.rhat + p, rh);
-        store_row<K, T>(v.v + p, y);
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, v.ph, v.tv, v.tg, sm[ix.warp], ix, y);
+        T ysum = T(0);
+        if (ix.active) {
+            const size_t p = (size_t)ix.el * K * K + ix.t * K;
+            T rh[K];
+            load_row<K, T>(v.rhat + p, rh);
+            store_row<K, T>(v.v + p, y);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            ysum += y[i];
-            part[0] += double(rh[i]) * double(y[i]);
+            for (int i = 0; i < K; ++i) {
+                ysum += y[i];
+                part[0] += double(rh[i]) * double(y[i]);
+            }
         }
+        const T tot = element_total<K, T>(ysum, ix.lw);
+        if (ix.active && ix.t == 0) v.ev[ix.el] = tot;
+    };
+    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
+    // push the operator past the register file)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll 1
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+    } else {
+        if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }
-    const T tot = element_total<K, T>(ysum, ix.lw);
-    if (ix.active && ix.t == 0) v.ev[ix.el] = tot;
     double out[1];
     if (grid_reduce<1>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
         if (out[0] == 0.0 || sc->rho == 0.0) {
@@ -558,23 +642,33 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVecto
 template <int K, typename T>
 __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
-    const bool skip = sc->done || sc->s_exit;  // read early: the round trip overlaps the operator's loads
+    if (sc->done || sc->s_exit) return;  // uniform
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
-    const RowIdx<K> ix(op.g.N, blockIdx.x);
-    T y[K];
-    row_apply<K, T>(op, v.sh, v.tv, v.tg, sm[ix.warp], ix, y);
-    if (skip) return;
+    const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[2] = {0.0, 0.0};
-    if (ix.active) {
-        const size_t p = (size_t)ix.el * K * K + ix.t * K;
-        T sv[K];
-        load_row<K, T>(v.s + p, sv);
-        store_row<K, T>(v.t + p, y);
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, v.sh, v.tv, v.tg, sm[ix.warp], ix, y);
+        if (ix.active) {
+            const size_t p = (size_t)ix.el * K * K + ix.t * K;
+            T sv[K];
+            load_row<K, T>(v.s + p, sv);
+            store_row<K, T>(v.t + p, y);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            part[0] += double(y[i]) * double(sv[i]);
-            part[1] += double(y[i]) * double(y[i]);
+            for (int i = 0; i < K; ++i) {
+                part[0] += double(y[i]) * double(sv[i]);
+                part[1] += double(y[i]) * double(y[i]);
+            }
         }
+    };
+    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
+    // push the operator past the register file)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll 1
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+    } else {
+        if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0)
@@ -588,23 +682,12 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_t(MfOp<T> op, BicgVecto
 // not done). Every CTA reads `done` and `s_exit` before any CTA arrives at the counter,
 // so the last CTA may change them. Every body execution either increments `it` (capped at
 // max_iter) or finds `done` set and clears the condition, so the device loop always ends.
-// Each thread updates one element row; its loads are issued before the flag is read.
+// Each thread updates element rows.
 template <int K, typename T>
 __global__ void __launch_bounds__(Rows<K>::THREADS) k_xr_update(int N, BicgVectors<T> v, ReduceScratch rs,
                                                                  int max_iter, cudaGraphConditionalHandle h,
                                                                  int has_handle) {
     KrylovScalars* sc = rs.sc;
-    const RowIdx<K> ix(N, blockIdx.x);
-    const size_t p = (size_t)ix.el * K * K + ix.t * K;
-    T x[K], ph[K], sh[K], sv[K], tv[K], rh[K];
-    if (ix.active) {
-        load_row<K, T>(v.x + p, x);
-        load_row<K, T>(v.ph + p, ph);
-        load_row<K, T>(v.sh + p, sh);
-        load_row<K, T>(v.s + p, sv);
-        load_row<K, T>(v.t + p, tv);
-        load_row<K, T>(v.rhat + p, rh);
-    }
     if (sc->done) {  // the solve ended earlier in this body (breakdown)
         if (has_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
         return;
@@ -612,30 +695,43 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_xr_update(int N, BicgVecto
     const T alpha = T(sc->alpha);
     const bool s_exit = sc->s_exit;
     const double omega = sc->omega;
+    const int ntiles = (int)rgrid_of<K>(N);
     double part[2] = {0.0, 0.0};
-    T rsum = T(0);
-    if (ix.active) {
-        if (s_exit) {
+#pragma unroll 1
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const RowIdx<K> ix(N, tile);
+        const size_t p = (size_t)ix.el * K * K + ix.t * K;
+        T rsum = T(0);
+        if (ix.active) {
+            T x[K], ph[K];
+            load_row<K, T>(v.x + p, x);
+            load_row<K, T>(v.ph + p, ph);
+            if (s_exit) {
 #pragma unroll
-            for (int i = 0; i < K; ++i) x[i] = x[i] + alpha * ph[i];
-            store_row<K, T>(v.x + p, x);
-        } else {
-            T r[K];
+                for (int i = 0; i < K; ++i) x[i] = x[i] + alpha * ph[i];
+                store_row<K, T>(v.x + p, x);
+            } else {
+                T sh[K], sv[K], tv[K], rh[K], r[K];
+                load_row<K, T>(v.sh + p, sh);
+                load_row<K, T>(v.s + p, sv);
+                load_row<K, T>(v.t + p, tv);
+                load_row<K, T>(v.rhat + p, rh);
 #pragma unroll
-            for (int i = 0; i < K; ++i) {
-                x[i] = x[i] + (alpha * ph[i] + T(omega) * sh[i]);
-                r[i] = sv[i] - T(omega) * tv[i];
-                rsum += r[i];
-                part[0] += double(r[i]) * double(r[i]);
-                part[1] += double(rh[i]) * double(r[i]);
+                for (int i = 0; i < K; ++i) {
+                    x[i] = x[i] + (alpha * ph[i] + T(omega) * sh[i]);
+                    r[i] = sv[i] - T(omega) * tv[i];
+                    rsum += r[i];
+                    part[0] += double(r[i]) * double(r[i]);
+                    part[1] += double(rh[i]) * double(r[i]);
+                }
+                store_row<K, T>(v.x + p, x);
+                store_row<K, T>(v.r + p, r);
             }
-            store_row<K, T>(v.x + p, x);
-            store_row<K, T>(v.r + p, r);
         }
-    }
-    if (!s_exit) {
-        const T tot = element_total<K, T>(rsum, ix.lw);
-        if (ix.active && ix.t == 0) v.er[ix.el] = tot;
+        if (!s_exit) {
+            const T tot = element_total<K, T>(rsum, ix.lw);
+            if (ix.active && ix.t == 0) v.er[ix.el] = tot;
+        }
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -664,21 +760,32 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_residual(MfOp<T> op, co
                                                                    const T* __restrict__ xtg, double* __restrict__ r,
                                                                    ReduceScratch rs) {
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
-    const RowIdx<K> ix(op.g.N, blockIdx.x);
-    T y[K];
-    row_apply<K, T>(op, x, xtv, xtg, sm[ix.warp], ix, y);
+    const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[2] = {0.0, 0.0};
-    if (ix.active) {
-        const size_t p = (size_t)ix.el * K * K + ix.t * K;
-        double bb[K], rr[K];
-        load_row<K, double>(b + p, bb);
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, x, xtv, xtg, sm[ix.warp], ix, y);
+        if (ix.active) {
+            const size_t p = (size_t)ix.el * K * K + ix.t * K;
+            double bb[K], rr[K];
+            load_row<K, double>(b + p, bb);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            rr[i] = bb[i] - double(y[i]);
-            part[0] += rr[i] * rr[i];
-            part[1] += bb[i] * bb[i];
+            for (int i = 0; i < K; ++i) {
+                rr[i] = bb[i] - double(y[i]);
+                part[0] += rr[i] * rr[i];
+                part[1] += bb[i] * bb[i];
+            }
+            store_row<K, double>(r + p, rr);
         }
-        store_row<K, double>(r + p, rr);
+    };
+    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
+    // push the operator past the register file)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll 1
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+    } else {
+        if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }
     double out[2];
     if (grid_reduce<2>(part, rs.partials, rs.counter, out) && threadIdx.x == 0) {
@@ -793,7 +900,7 @@ cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const Reduce
                         cudaStream_t s) {
     const int N = op.g.N;
     HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<rgrid_of<KK>(N), Rows<KK>::THREADS, 0, s>>>(op, v.x, v.xtv, v.xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<rgrid_of<KK>(N), Rows<KK>::THREADS, 0, s>>>(op, v, rs)));
+    HO2D_KSWITCH(op.K, (k_mf_init<KK, T><<<wave_of<KK, T>(&WaveSizes::init, N), Rows<KK>::THREADS, 0, s>>>(op, v, rs)));
     const size_t n = (size_t)N * op.K * op.K;
     k_zero_if<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v.x, n, rs.sc);
     return cudaGetLastError();
@@ -802,9 +909,11 @@ cudaError_t krylov_init(const MfOp<T>& op, const BicgVectors<T>& v, const Reduce
 // One BiCGSTAB iteration: [coarse cycle on P^T p] -> p update + smoothing (ph) -> v = A ph
 // -> [coarse cycle on P^T s] -> s update + smoothing (sh) -> t = A sh -> x, r update and
 // loop control.
-// With ev (8 events) the boundaries between the launches are recorded on the stream:
-// ev[0] coarse ev[1] smoothing ev[2] operator ev[3] coarse ev[4] smoothing ev[5] operator
-// ev[6] update ev[7].
+// A preconditioner application is its coarse cycle (on the side stream when op.side is
+// set) beside the fine smoothing part k_post_a, then the combination k_post_b. With ev
+// (10 events) everything runs in order on s with the boundaries recorded: ev[0] coarse
+// ev[1] fine part ev[2] combination ev[3] operator ev[4] coarse ev[5] fine part ev[6]
+// combination ev[7] operator ev[8] update ev[9].
 template <int K, typename T>
 static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const ReduceScratch& rs, int max_iter,
                            const Precond<T>& pc, cudaGraphConditionalHandle h, int has_handle, cudaStream_t s,
@@ -817,35 +926,70 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
     const CoarseOut<T> co = mg ? coarse_out(pc) : CoarseOut<T>();
     const unsigned gp = rgrid_of<K>(N);
     constexpr int tp = Rows<K>::THREADS;
-    auto post = [&](int mode) {
+    auto post_a = [&](int mode) {
         if constexpr (std::is_same<T, float>::value) {
             if (op.kron_f) {
-                k_mf_post<K, T, 2><<<gp, tp, PostRows<K, T, 2>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                k_post_a<K, T, 2><<<gp, tp, PostRows<K, T, 2>::SMEM, s>>>(op, v, mg, rs, mode);
                 return;
             }
             if (op.dinv_bf16) {
-                k_mf_post<K, T, 1><<<gp, tp, PostRows<K, T, 1>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
+                k_post_a<K, T, 1><<<gp, tp, PostRows<K, T, 1>::SMEM, s>>>(op, v, mg, rs, mode);
                 return;
             }
         }
-        k_mf_post<K, T, 0><<<gp, tp, PostRows<K, T, 0>::SMEM, s>>>(op, v, co, mg, pc.omega, rs, mode);
+        k_post_a<K, T, 0><<<gp, tp, PostRows<K, T, 0>::SMEM, s>>>(op, v, mg, rs, mode);
     };
-    const unsigned gr = rgrid_of<K>(N);
-    mark(0);
-    if (mg) coarse_cycle<T>(pc, v, rs.sc, 0, s);
-    mark(1);
-    post(0);
-    mark(2);
-    k_mf_v<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    // one preconditioner application: the coarse cycle beside the fine part (on the side
+    // stream, joined before the combination), or after it without a side stream
+    auto precond = [&](int mode, int m0) {
+        const bool fork = mg && op.side && !ev;  // a profiled iteration runs everything in order
+        mark(m0);
+        if (fork) {
+            cudaEventRecord(op.ev_fork, s);
+            cudaStreamWaitEvent(op.side, op.ev_fork, 0);
+            coarse_cycle<T>(pc, v, rs.sc, mode, op.side);
+            cudaEventRecord(op.ev_join, op.side);
+        } else if (mg) {
+            coarse_cycle<T>(pc, v, rs.sc, mode, s);
+        }
+        mark(m0 + 1);
+        post_a(mode);
+        if (fork) cudaStreamWaitEvent(s, op.ev_join, 0);
+        mark(m0 + 2);
+        k_post_b<K, T><<<gp, tp, 0, s>>>(op, v, co, mg, pc.omega, rs.sc, mode);
+    };
+    const unsigned gwv = wave_of<K, T>(&WaveSizes::v, N), gwt = wave_of<K, T>(&WaveSizes::t, N),
+                   gwx = wave_of<K, T>(&WaveSizes::xr, N);
+    precond(0, 0);
     mark(3);
-    if (mg) coarse_cycle<T>(pc, v, rs.sc, 1, s);
-    mark(4);
-    post(1);
-    mark(5);
-    k_mf_t<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(op, v, rs);
-    mark(6);
-    k_xr_update<K, T><<<gr, Rows<K>::THREADS, 0, s>>>(N, v, rs, max_iter, h, has_handle);
+    k_mf_v<K, T><<<gwv, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    precond(1, 4);
     mark(7);
+    k_mf_t<K, T><<<gwt, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    mark(8);
+    k_xr_update<K, T><<<gwx, Rows<K>::THREADS, 0, s>>>(N, v, rs, max_iter, h, has_handle);
+    mark(9);
+}
+
+template <int K, typename T>
+static cudaError_t configure_waves() {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    WaveSizes& ws = g_wave[K][std::is_same<T, float>::value ? 1 : 0];
+    auto w = [&](auto kern, unsigned& out) {
+        int nb = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, Rows<K>::THREADS, 0);
+        out = (unsigned)(nb > 0 ? nb : 1) * (unsigned)sms;
+    };
+    w(k_xr_update<K, T>, ws.xr);
+    if constexpr (sizeof(T) == 4) {  // the FP64 operator kernels take one tile per CTA
+        w(k_mf_init<K, T>, ws.init);
+        w(k_mf_v<K, T>, ws.v);
+        w(k_mf_t<K, T>, ws.t);
+        w(k_mf_residual<K, T>, ws.res);
+    }
+    return e;
 }
 
 // Dynamic shared memory of the smoothing kernels that stage their blocks (above the
@@ -857,22 +1001,53 @@ static cudaError_t configure_post() {
         if (e == cudaSuccess && bytes > 0)
             e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     };
-    one(k_mf_post<K, double, 0>, PostRows<K, double, 0>::SMEM);
-    one(k_mf_post<K, float, 0>, PostRows<K, float, 0>::SMEM);
-    one(k_mf_post<K, float, 1>, PostRows<K, float, 1>::SMEM);
-    one(k_mf_post<K, float, 2>, PostRows<K, float, 2>::SMEM);
+    one(k_post_a<K, double, 0>, PostRows<K, double, 0>::SMEM);
+    one(k_post_a<K, float, 0>, PostRows<K, float, 0>::SMEM);
+    one(k_post_a<K, float, 1>, PostRows<K, float, 1>::SMEM);
+    one(k_post_a<K, float, 2>, PostRows<K, float, 2>::SMEM);
+    one(k_make_w<K, double, 0>, PostRows<K, double, 0>::SMEM);
+    one(k_make_w<K, float, 0>, PostRows<K, float, 0>::SMEM);
+    one(k_make_w<K, float, 1>, PostRows<K, float, 1>::SMEM);
+    one(k_make_w<K, float, 2>, PostRows<K, float, 2>::SMEM);
     return e;
 }
 
 cudaError_t krylov_configure(int K) {
     cudaError_t e = cudaSuccess;
     HO2D_KSWITCH(K, (e = configure_post<KK>()));
+    if (e == cudaSuccess) HO2D_KSWITCH(K, (e = configure_waves<KK, double>()));
+    if (e == cudaSuccess) HO2D_KSWITCH(K, (e = configure_waves<KK, float>()));
     return e;
 }
 
 template <typename T>
 int krylov_launches_per_iteration(const Precond<T>& pc) {
-    return 5 + 2 * coarse_launches(pc);
+    return 7 + 2 * coarse_launches(pc);
+}
+
+template <int K, typename T>
+static cudaError_t make_w_impl(const MfOp<T>& op, T* W, KrylovScalars* sc, cudaStream_t s) {
+    const unsigned g = rgrid_of<K>(op.g.N);
+    constexpr int tp = Rows<K>::THREADS;
+    if constexpr (std::is_same<T, float>::value) {
+        if (op.kron_f) {
+            k_make_w<K, T, 2><<<g, tp, PostRows<K, T, 2>::SMEM, s>>>(op, W, sc);
+            return cudaGetLastError();
+        }
+        if (op.dinv_bf16) {
+            k_make_w<K, T, 1><<<g, tp, PostRows<K, T, 1>::SMEM, s>>>(op, W, sc);
+            return cudaGetLastError();
+        }
+    }
+    k_make_w<K, T, 0><<<g, tp, PostRows<K, T, 0>::SMEM, s>>>(op, W, sc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t krylov_make_w(const MfOp<T>& op, T* W, KrylovScalars* sc, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    HO2D_KSWITCH(op.K, (e = make_w_impl<KK, T>(op, W, sc, s)));
+    return e;
 }
 
 template <typename T>
@@ -1014,7 +1189,7 @@ template <typename T>
 cudaError_t mf_residual(const MfOp<T>& op, const double* b, const T* x, T* xtv, T* xtg, double* r,
                         const ReduceScratch& rs, cudaStream_t s) {
     HO2D_KSWITCH(op.K, (k_trace_in<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, x, xtv, xtg)));
-    HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<rgrid_of<KK>(op.g.N), Rows<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
+    HO2D_KSWITCH(op.K, (k_mf_residual<KK, T><<<wave_of<KK, T>(&WaveSizes::res, op.g.N), Rows<KK>::THREADS, 0, s>>>(op, b, x, xtv, xtg, r,
                                                                                                   rs)));
     return cudaGetLastError();
 }
@@ -1048,6 +1223,7 @@ cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s)
     template cudaError_t krylov_iteration<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&, int,    \
                                              const Precond<T>&, cudaStream_t);                                    \
     template int krylov_launches_per_iteration<T>(const Precond<T>&);                                             \
+    template cudaError_t krylov_make_w<T>(const MfOp<T>&, T*, KrylovScalars*, cudaStream_t);                      \
     template cudaError_t krylov_iteration_timed<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,   \
                                                    int, const Precond<T>&, cudaEvent_t*, cudaStream_t);           \
     template cudaError_t krylov_capture_solve<T>(const MfOp<T>&, const BicgVectors<T>&, const ReduceScratch&,     \

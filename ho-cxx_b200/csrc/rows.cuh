@@ -100,6 +100,34 @@ __device__ __forceinline__ void store_row(T* __restrict__ p, const T (&v)[K]) {
     }
 }
 
+// The four faces' values of one face point ([N][K][4] layout), one 16-byte (float) or two
+// 16-byte (double) loads.
+template <typename T>
+__device__ __forceinline__ void load4(const T* __restrict__ p, T (&v)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = q.x;
+        v[1] = q.y;
+        v[2] = q.z;
+        v[3] = q.w;
+    } else {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 c = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = c.x;
+        v[3] = c.y;
+    }
+}
+
+__device__ __forceinline__ void load4i(const int* __restrict__ p, int (&v)[4]) {
+    const int4 q = __ldg(reinterpret_cast<const int4*>(p));
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+}
+
 // Stride-K column of an element block.
 template <int K, typename T>
 __device__ __forceinline__ void load_col(const T* __restrict__ p, T (&v)[K]) {
@@ -175,13 +203,13 @@ __device__ __forceinline__ T element_total(T v, int lw) {
 // that the reference assembles in form_Laplace_operator_matrix, src/HO_2D.cpp:1533-1804)
 // of element `el`, row t, from the element's own rows of x, its metric coefficients, its
 // face coefficients and the incoming face traces of x that its neighbours' producers
-// wrote (tvin/tgin, [N][4][K]). Every global read is the element's own data. Warp-
+// wrote (tvin/tgin, [N][K][4]). Every global read is the element's own data. Warp-
 // collective: every lane of the warp calls it.
 template <int K, typename T>
 __device__ __forceinline__ void row_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tvin,
                                           const T* __restrict__ tgin, RowScratch<K, T>& sm, const RowIdx<K>& ix,
                                           T (&y)[K]) {
-    constexpr int K2 = K * K, NF = 4 * K;
+    constexpr int K2 = K * K;
     const PoisGeom<T>& g = op.g;
     const DevBases<T>& b = op.b;
     const int t = ix.t, lw = ix.lw, el = ix.el;
@@ -203,17 +231,14 @@ __device__ __forceinline__ void row_apply(const MfOp<T>& op, const T* __restrict
         load_row<K, T>(g.G12 + e2 + t * K, g12r);
         load_col<K, T>(g.G22 + e2 + t, g22);
         load_col<K, T>(g.G12 + e2 + t, g12c);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const size_t q = (size_t)el * NF + f * K + t;
-            fa[f] = __ldg(g.fa + q);
-            fb[f] = __ldg(g.fb + q);
-            nfa[f] = __ldg(g.nfa + q);
-            nfb[f] = __ldg(g.nfb + q);
-            ntv[f] = tvin[q];
-            ntg[f] = tgin[q];
-            code[f] = __ldg(g.code + el * 4 + f);
-        }
+        const size_t q4 = ((size_t)el * K + t) * 4;  // face point t of the 4 faces ([N][K][4])
+        load4<T>(g.fa + q4, fa);
+        load4<T>(g.fb + q4, fb);
+        load4<T>(g.nfa + q4, nfa);
+        load4<T>(g.nfb + q4, nfb);
+        load4<T>(tvin + q4, ntv);
+        load4<T>(tgin + q4, ntg);
+        load4i(g.code + el * 4, code);
     } else {
 #pragma unroll
         for (int i = 0; i < K; ++i) xr[i] = xc[i] = g11[i] = g12r[i] = g22[i] = g12c[i] = T(0);

@@ -114,6 +114,9 @@ Error Solver::setup_from_mesh() {
     DeviceState& d = *d_;
     HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
     if (!d.stream) HO2D_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!d.side) HO2D_CUDA(cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* e : {&d.ev_fork, &d.ev_join})
+        if (!*e) HO2D_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
     for (cudaEvent_t* e : {&d.ev0, &d.ev1, &d.evp0, &d.evp1})
         if (!*e) HO2D_CUDA(cudaEventCreate(e), "cudaEventCreate");
     if (!d.h_sc) HO2D_CUDA(cudaMallocHost(&d.h_sc, sizeof(KrylovScalars)), "cudaMallocHost");
@@ -174,7 +177,24 @@ Error Solver::setup_from_mesh() {
     const int K4 = K2 * K2;
     HO2D_CUDA(upload(d.dinv64, padded_rows<double>(op_.dinv, N, K4, padded_count(K4, 8))), "upload block-Jacobi");
     HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
+    HO2D_CUDA(d.W64.alloc(op_.rowsum.size() * sizeof(double)), "alloc smoothed row sums");
+    HO2D_CUDA(d.W32.alloc(op_.rowsum.size() * sizeof(float)), "alloc smoothed row sums");
+    HO2D_CUDA(d.zf.alloc((size_t)N * K2 * sizeof(double)), "alloc smoother vector");
     HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
+    {
+        // where the coarse cycle delivers each element's level-0 value: every block slot
+        // (el, s) with block_col[5 el + s] = c reads u0 of element c
+        std::vector<int> dst((size_t)N * 5, -1), cnt(N, 0);
+        for (int el = 0; el < N; ++el)
+            for (int sl = 0; sl < 5; ++sl) {
+                const int c = op_.block_col[(size_t)el * 5 + sl];
+                if (c < 0) continue;
+                if (cnt[c] >= 5) return {3, "an element is a block neighbour of more than four elements"};
+                dst[(size_t)c * 5 + cnt[c]++] = el * 5 + sl;
+            }
+        HO2D_CUDA(upload(d.u0dst, dst), "upload coarse slot table");
+        HO2D_CUDA(upload(d.ue5, std::vector<double>((size_t)N * 5, 0.0)), "alloc coarse slot values");
+    }
     HO2D_TRY(build_poisson_geometry(fnb, fnijp));
     HO2D_TRY(setup_forces());
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
@@ -188,9 +208,14 @@ Error Solver::setup_from_mesh() {
     for (auto& b : d.esum) HO2D_CUDA(upload(b, std::vector<double>((size_t)N + 4, 0.0)), "alloc element sums");
     const int mb = krylov_max_blocks(K, N);
     HO2D_CUDA(upload(d.partials, std::vector<double>((size_t)4 * mb, 0.0)), "alloc partials");
-    HO2D_CUDA(upload(d.counter, std::vector<unsigned>(1, 0u)), "alloc counter");
+    // the grid reductions' counters: one for the groups of 64 CTAs, one per group
+    HO2D_CUDA(upload(d.counter, std::vector<unsigned>(2 + mb / 64, 0u)), "alloc counter");
     HO2D_CUDA(d.scalars.alloc(sizeof(KrylovScalars)), "alloc scalars");
     HO2D_CUDA(cudaMemset(d.scalars.get(), 0, sizeof(KrylovScalars)), "memset");
+    // the FP64 smoother applied to the block row sums (the split smoothing step)
+    HO2D_CUDA(krylov_make_w<double>(make_op<double>(d, mesh_, K, false), d.W64.as<double>(),
+                                    d.scalars.as<KrylovScalars>(), d.stream),
+              "smoothed row sums");
     time_ = 0.0;
     t_start_ = t_end_ = 0.0;
     hist_count_ = 0;
@@ -241,11 +266,10 @@ Error Solver::build_poisson_geometry(const std::vector<int>& fnb, const std::vec
                 continue;
             }
             const int e = -nb - 1;
-            if (bc_.sw_p[e] != kNeumann) {
-                code[(size_t)el * 4 + ijp] = -1;
-                continue;
-            }
-            code[(size_t)el * 4 + ijp] = -2 - e;
+            code[(size_t)el * 4 + ijp] = bc_.sw_p[e] == kNeumann ? -2 - e : -1;
+            // the inverse serves the operator (Neumann psi) and the stage kernels (Neumann
+            // psi or vorticity): the system depends on the face geometry only
+            if (bc_.sw_p[e] != kNeumann && bc_.sw_d[e] != kNeumann) continue;
             // M[k][c] = -fb_k l_c'(x_k) + fa_k g'(+-1) delta_kc (rows scaled by 1/J_f)
             const int lr = ijp & 1;
             std::vector<double> A((size_t)K * K), I((size_t)K * K, 0.0);
@@ -280,9 +304,24 @@ Error Solver::build_poisson_geometry(const std::vector<int>& fnb, const std::vec
             }
             std::copy(I.begin(), I.end(), h[7].begin() + (size_t)e * K * K);
         }
+    // device layout of the face data and of the trace slots: [N][K][4], the four faces of
+    // one face-point index together, so the thread that owns face point k of every face
+    // (row-parallel operator) reads them as one vector
+    auto perm = [K, NF](size_t q) {
+        const size_t el = q / NF, r = q % NF;
+        return (el * K + r % K) * 4 + r / K;
+    };
+    for (int a = 3; a < 7; ++a) {
+        std::vector<double> t(nf);
+        for (size_t q = 0; q < nf; ++q) t[perm(q)] = h[a][q];
+        h[a].swap(t);
+    }
+    std::vector<int> scat_p(nf, -1);
+    for (size_t q = 0; q < nf; ++q)
+        if (scat[q] >= 0) scat_p[perm(q)] = (int)perm((size_t)scat[q]);
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload(d.pg64[a], h[a]), "upload Poisson operator data");
     HO2D_CUDA(upload(d.pcode, code), "upload Poisson face codes");
-    HO2D_CUDA(upload(d.pscat, scat), "upload trace scatter table");
+    HO2D_CUDA(upload(d.pscat, scat_p), "upload trace scatter table");
     return {0, ""};
 }
 
@@ -381,7 +420,7 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
             HO2D_CUDA(upload_ell(b->S, eS[l]), "upload coarse S");
             HO2D_CUDA(upload_ell(b->Q, eQ[l]), "upload coarse Q");
         }
-        const std::vector<double> z((size_t)L.A.n + 4, 0.0);  // zero padding for 16-byte reads
+        const std::vector<double> z((size_t)L.A.n + 8, 0.0);  // zero padding for 16-byte reads
         for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
         lev.push_back(std::move(b));
     }
@@ -392,7 +431,19 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
         std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
                   dpad.begin() + (size_t)i * wd);
     HO2D_CUDA(upload(dense64, dpad), "upload dense");
-    HO2D_CUDA(upload_as<float>(dense32, dpad), "upload dense");
+    // the FP32 preconditioner's coarsest inverse in BF16 (half the bytes of the largest
+    // coarse read; the preconditioner's precision changes only the iteration count) when
+    // it is a level below the element level
+    const bool dense16 = nl > 1;
+    const int w16 = (nd + 7) / 8 * 8;
+    if (dense16) {
+        std::vector<uint16_t> d16((size_t)nd * w16 + 8, 0);
+        for (int i = 0; i < nd; ++i)
+            for (int c = 0; c < nd; ++c) d16[(size_t)i * w16 + c] = bf16_bits((float)H.dense_inv[(size_t)i * nd + c]);
+        HO2D_CUDA(upload(dense32, d16), "upload dense");
+    } else {
+        HO2D_CUDA(upload_as<float>(dense32, dpad), "upload dense");
+    }
     auto fill = [&](auto& pc, bool f32) {
         using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
         pc.nlev = nl;
@@ -402,6 +453,11 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
         pc.dense.g = 32;
         pc.dense.col = nullptr;
         pc.dense.val = f32 ? (const T*)dense32.get() : (const T*)dense64.get();
+        if (f32 && dense16) {
+            pc.dense.val = nullptr;
+            pc.dense.val16 = dense32.as<unsigned short>();
+            pc.dense.w = w16;
+        }
         for (int l = 0; l < nl; ++l) {
             auto& b = *lev[l];
             auto& c = pc.lev[l];
@@ -415,6 +471,8 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
             c.f = b.f.as<T>();
             c.u = b.u.as<T>();
         }
+        pc.ue5 = d_->ue5.as<T>();
+        pc.u0dst = d_->u0dst.as<int>();
     };
     fill(pc64, false);
     fill(pc32, true);
@@ -483,6 +541,11 @@ Error Solver::upload_precision_arrays() {
     }
     HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");
+    // the FP32 smoother (exact, BF16 or Kronecker-sum) applied to the block row sums
+    HO2D_CUDA(krylov_make_w<float>(make_op<float>(d, mesh_, K, true), d.W32.as<float>(), d.scalars.as<KrylovScalars>(),
+                                   d.stream),
+              "smoothed row sums");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "smoothed row sums");
     d.have32 = true;
     return {0, ""};
 }
@@ -742,7 +805,7 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     HO2D_CUDA(launch_trace<double>(K, N, psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.b64, d.stream), "trace");
     VelocityArgs<T, double> va{psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.w_stage.as<T>(), d.u.as<T>(),
                                d.v.as<T>(), d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
-    HO2D_CUDA((launch_velocity<T, double>(K, g64, d.b64, b, bc, va, d.stream)), "velocity");
+    HO2D_CUDA((launch_velocity<T, double>(K, g64, stage_coef<double>(d, false), d.b64, b, bc, va, d.stream)), "velocity");
     ResidualArgs<T> ra;
     ra.w = d.w_stage.as<T>();
     ra.u = d.u.as<T>();
@@ -765,7 +828,7 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     ra.rhs_diff = keep_rhs ? d.rhs_diff.as<T>() : nullptr;
     ra.rhs_adv = keep_rhs ? d.rhs_adv.as<T>() : nullptr;
     ra.k_out = update ? nullptr : d.kout.as<T>();
-    HO2D_CUDA(launch_residual<T>(K, g, b, bc, ra, d.stream), "residual");
+    HO2D_CUDA(launch_residual<T>(K, g, stage_coef<T>(d, f32), b, bc, ra, d.stream), "residual");
     launches_ += 3;
     return {0, ""};
 }
@@ -791,7 +854,7 @@ Error Solver::velocity_only_t() {
     HO2D_CUDA(launch_trace<double>(K, N, psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.b64, d.stream), "trace");
     VelocityArgs<T, double> va{psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.w_stage.as<T>(), d.u.as<T>(),
                                d.v.as<T>(), d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
-    HO2D_CUDA((launch_velocity<T, double>(K, g64, d.b64, b, bc, va, d.stream)), "velocity");
+    HO2D_CUDA((launch_velocity<T, double>(K, g64, stage_coef<double>(d, false), d.b64, b, bc, va, d.stream)), "velocity");
     launches_ += 4;
     return {0, ""};
 }
@@ -968,13 +1031,15 @@ Error Solver::profile_spmv(int reps, double* avg_ms, double* bytes) {
 }
 
 // Per-launch device time of the Krylov kernels inside BiCGSTAB iterations of the active
-// precision's solve, and their algorithmic bytes per launch: [0] the smoothing kernel
-// (vector update + two-level smoothing step + traces), [1] the operator kernels (v = A ph,
-// t = A sh), [2] the x/r update, [3] one coarse cycle. The iterations run on the current
-// state without a CUDA graph, with events between the launches on the handle's stream: the
-// FP32 solve of a refinement sweep on the FP64 residual of the current psi (mixed modes),
-// or the FP64 solve of the last right-hand side from a zero guess (FP64). Their tolerance
-// is zero, so none of them ends early; psi is not changed.
+// precision's solve, and their algorithmic bytes per launch: [0] the fine part of the
+// smoothing step (vector update + the smoother's element inverse), [1] the operator kernels
+// (v = A ph, t = A sh), [2] the x/r update, [3] one coarse cycle, [4] the combination of
+// the smoothing step (coarse correction + face traces). The iterations run on the current
+// state without a CUDA graph and in order on the handle's stream (the coarse cycle does not
+// run beside the fine part here), with events between the launches: the FP32 solve of a
+// refinement sweep on the FP64 residual of the current psi (mixed modes), or the FP64 solve
+// of the last right-hand side from a zero guess (FP64). Their tolerance is zero, so none of
+// them ends early; psi is not changed.
 Error Solver::profile_krylov(int reps, double* ms, double* bytes) {
     if (!setup_done_) return {1, "not set up"};
     if (reps <= 0 || reps > 1000) return {1, "reps must be in 1..1000"};
@@ -990,18 +1055,19 @@ Error Solver::profile_krylov(int reps, double* ms, double* bytes) {
     HO2D_CUDA(cudaMemcpyAsync(&d.scalars.as<KrylovScalars>()->tol, &d.h_sc->tol, sizeof(double),
                               cudaMemcpyHostToDevice, d.stream),
               "tolerance");
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     auto run = [&](auto A, auto v, const auto& pc) -> Error {
         HO2D_CUDA(krylov_init(A, v, rs, d.stream), "krylov init");
         for (int r = 0; r < reps; ++r) {
             HO2D_CUDA(krylov_iteration_timed(A, v, rs, 1 << 30, pc, d.prof_ev, d.stream), "krylov iteration");
-            HO2D_CUDA(cudaEventSynchronize(d.prof_ev[7]), "event");
-            float t[7];
-            for (int i = 0; i < 7; ++i) HO2D_CUDA(cudaEventElapsedTime(&t[i], d.prof_ev[i], d.prof_ev[i + 1]), "event");
-            acc[3] += t[0] + t[3];
-            acc[0] += t[1] + t[4];
-            acc[1] += t[2] + t[5];
-            acc[2] += t[6];
+            HO2D_CUDA(cudaEventSynchronize(d.prof_ev[9]), "event");
+            float t[9];
+            for (int i = 0; i < 9; ++i) HO2D_CUDA(cudaEventElapsedTime(&t[i], d.prof_ev[i], d.prof_ev[i + 1]), "event");
+            acc[3] += t[0] + t[4];
+            acc[0] += t[1] + t[5];
+            acc[4] += t[2] + t[6];
+            acc[1] += t[3] + t[7];
+            acc[2] += t[8];
         }
         return {0, ""};
     };
@@ -1035,24 +1101,26 @@ Error Solver::profile_krylov(int reps, double* ms, double* bytes) {
         ms[1] = acc[1] / (2.0 * reps);
         ms[2] = acc[2] / reps;
         ms[3] = acc[3] / (2.0 * reps);
+        ms[4] = acc[4] / (2.0 * reps);
     }
     if (bytes) {
-        // smoother element data: the inverse block in its storage, or the Kronecker factors
-        // plus the exact blocks of the elements that keep them
+        // fine part, per element: the smoother's element data (inverse block in its storage,
+        // or the Kronecker factors plus the exact blocks of the elements that keep them), r
+        // and v (and p in mode 0: half the launches) read, p or s and M f written
         const double K4 = (double)K2 * K2;
         double blk = K4 * bw;
         if (krylov32_ && smoother_kind_ == 1) blk = K4 * 2;
         if (krylov32_ && smoother_kind_ == 2) blk = (4.0 * K2 + 2 * K) * 4 + (double)smoother_exact_ / N * K4 * 4;
-        // per element: block, 5 block row sums, r and v (and p in mode 0: half the
-        // launches) read, p or s and z written, z's 4K face traces (value and derivative)
-        // written, 4K trace destinations and 5 coarse-slot indices read
-        bytes[0] = (double)N * (blk + 5.0 * K2 * bw + 4.5 * K2 * bw + 8.0 * K * bw + 16.0 * K + 20.0);
+        bytes[0] = (double)N * (blk + 4.5 * K2 * bw);
         // per element: operand, 3 metric coefficients, rhat or s, result; 4 face coefficients
         // and 2 incoming traces per face point; 4 face codes; the element sum
         bytes[1] = (double)N * ((6.0 * K2 + 24.0 * K) * bw + 16.0 + bw);
         // x, ph, sh, s, t, rhat read; x and r written; the element sum of r
         bytes[2] = (double)N * (8.0 * K2 * bw + bw);
         bytes[3] = coarse_bytes;
+        // combination, per element: M f, the 5 smoothed row sums and the 5 coarse values
+        // read, z and its 4K face traces (value, derivative) written, 4K destinations read
+        bytes[4] = (double)N * ((7.0 * K2 + 8.0 * K) * bw + 5.0 * bw + 16.0 * K);
     }
     return {0, ""};
 }

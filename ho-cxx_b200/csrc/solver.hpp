@@ -52,7 +52,7 @@ class Solver {
     Error set_precision(int mode);
     Error time_steps(int nsteps, double* total_ms, double* poisson_ms);
     Error profile_spmv(int reps, double* avg_ms, double* bytes);
-    Error profile_krylov(int reps, double* ms, double* bytes);  // [4] each
+    Error profile_krylov(int reps, double* ms, double* bytes);  // [5] each
     Error apply_poisson(const double* x, double* y);
     Error apply_poisson_noalloc(const double* dx, double* dy);
 

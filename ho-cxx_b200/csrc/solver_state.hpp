@@ -56,7 +56,10 @@ struct DeviceState {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
-    cudaEvent_t prof_ev[8] = {};  // launch boundaries of a profiled Krylov iteration
+    cudaEvent_t prof_ev[10] = {};  // launch boundaries of a profiled Krylov iteration
+    // the coarse cycle's stream beside the fine smoothing part, and its fork/join events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // connectivity and boundary tables
     DeviceBuffer face_nb, face_nijp, be_group, sw_p, sw_d, noslip, role, be_ijp;
     DevBases<double> b64;
@@ -72,6 +75,8 @@ struct DeviceState {
     // Poisson operator and Krylov workspace
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
     DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
+    DeviceBuffer W64, W32, zf;  // smoother applied to the block row sums; fine part of z
+    DeviceBuffer ue5, u0dst;  // level-0 coarse values per element slot, and where each goes
     DeviceBuffer dinv_bf16;  // BF16 copy of dinv for the FP32 smoother (HO2D_SMOOTHER_BF16=1)
     // Kronecker-sum smoother for the FP32 solve (HO2D_SMOOTHER_KRON=1): factors, exact-block
     // index per element, compact exact blocks
@@ -110,6 +115,9 @@ struct DeviceState {
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : prof_ev)
             if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : {ev_fork, ev_join})
+            if (e) cudaEventDestroy(e);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -232,7 +240,14 @@ FrGeom<T> geom_of(DeviceState& d, const Mesh& m, bool f32) {
     g.sw_p = d.sw_p.as<int>();
     g.sw_d = d.sw_d.as<int>();
     g.noslip = d.noslip.as<int>();
+    g.nminv = (f32 ? d.pg32[7] : d.pg64[7]).as<T>();
     return g;
+}
+
+template <typename T>
+StageCoef<T> stage_coef(DeviceState& d, bool f32) {
+    const DeviceBuffer* pg = f32 ? d.pg32 : d.pg64;
+    return {pg[0].as<T>(), pg[1].as<T>(), pg[2].as<T>()};
 }
 
 template <typename T>
@@ -260,6 +275,10 @@ MfOp<T> make_op(DeviceState& d, const Mesh& m, int K, bool f32) {
     op.kron_exact = kron ? (const T*)d.kron_exact.get() : nullptr;
     op.rowsum = f32 ? (const T*)d.rowsum32.get() : (const T*)d.rowsum64.get();
     op.bcol = d.bcol.as<int>();
+    op.W = f32 ? (const T*)d.W32.get() : (const T*)d.W64.get();
+    op.side = d.side;
+    op.ev_fork = d.ev_fork;
+    op.ev_join = d.ev_join;
     return op;
 }
 
@@ -284,6 +303,7 @@ BicgVectors<T> krylov_vectors(DeviceState& d, T* x, const T* b) {
     v.ev = d.esum[1].as<T>();
     v.ep[0] = d.esum[2].as<T>();
     v.ep[1] = d.esum[3].as<T>();
+    v.zf = d.zf.as<T>();
     return v;
 }
 

@@ -279,12 +279,13 @@ class HO_2D:
 
     def profile_krylov(self, iterations: int = 20):
         """Per-launch device ms and algorithmic bytes of the Krylov kernels inside BiCGSTAB
-        iterations on the current state: dict kernel -> (ms, bytes) for "smoother",
-        "operator", "xr_update" and "coarse_cycle"."""
-        ms = (ctypes.c_double * 4)()
-        by = (ctypes.c_double * 4)()
+        iterations on the current state: dict kernel -> (ms, bytes) for "smoother" (the fine
+        part of the smoothing step), "operator", "xr_update", "coarse_cycle" and
+        "smoother_combine" (the coarse correction and the face traces)."""
+        ms = (ctypes.c_double * 5)()
+        by = (ctypes.c_double * 5)()
         self._check(self._lib.ho2d_profile_krylov(self._h, int(iterations), ms, by))
-        names = ("smoother", "operator", "xr_update", "coarse_cycle")
+        names = ("smoother", "operator", "xr_update", "coarse_cycle", "smoother_combine")
         return {n: (ms[i], by[i]) for i, n in enumerate(names)}
 
     def apply_poisson(self, x) -> np.ndarray:

@@ -104,6 +104,8 @@ class HO_2D {
         setup_ = false;
     }
     void set_precision(int mode) { check(ho2d_set_precision(h_, mode)); }
+    // smoother of the FP32 preconditioner (enum ho2d_smoother) for the next setup
+    void set_smoother(int kind) { check(ho2d_set_smoother(h_, kind)); }
     ho2d_solver* handle() { return h_; }
 
   private:

@@ -173,9 +173,10 @@ int ho2d_time_steps(ho2d_solver* handle, int32_t nsteps, double* total_ms, doubl
 int ho2d_profile_spmv(ho2d_solver* handle, int32_t reps, double* avg_ms, double* bytes_per_launch);
 /* No counterpart in the reference. Device time of the Krylov kernels inside `iterations`
  * BiCGSTAB iterations of the active precision's Poisson solve on the current state (run
- * without a CUDA graph, CUDA events between the launches on the handle's stream; psi is
- * not changed), and their algorithmic bytes per launch. ms[4] and bytes[4]: [0] smoothing
- * kernel, [1] operator kernel, [2] x/r update, [3] one coarse cycle; per launch averages. */
+ * without a CUDA graph and in order, CUDA events between the launches on the handle's
+ * stream; psi is not changed), and their algorithmic bytes per launch. ms[5] and
+ * bytes[5]: [0] fine part of the smoothing step, [1] operator kernel, [2] x/r update,
+ * [3] one coarse cycle, [4] combination of the smoothing step; per launch averages. */
 int ho2d_profile_krylov(ho2d_solver* handle, int32_t iterations, double* ms, double* bytes);
 /* y = A x in FP64 with the device's Poisson operator: the matrix the reference assembles
  * in form_Laplace_operator_matrix (src/HO_2D.cpp:1533-1804), applied matrix-free;

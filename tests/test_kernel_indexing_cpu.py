@@ -77,6 +77,29 @@ def test_block_staging_stays_in_bounds(K, size):
         assert WARPS * span <= 104 * 1024
 
 
+@pytest.mark.parametrize("K", range(1, 9))
+def test_kronecker_factor_staging_stays_in_bounds(K):
+    """The Kronecker-sum smoother stages each warp's factor sets (4K^2 + 2K FP32 values per
+    element, stride padded to 16 bytes) the same way: always within the 26 KB per warp."""
+    epw = 32 // K
+    stride = padded_count(4 * K * K + 2 * K, 4)
+    elem = stride * 4
+    span = epw * elem
+    assert elem % 16 == 0 and span <= 26 * 1024
+    for N in list(range(1, 3 * WARPS * epw + 2)) + [4096, 131072 + 3]:
+        alloc = (N * stride + 1) * 4
+        for b in range((N + WARPS * epw - 1) // (WARPS * epw)):
+            for w in range(WARPS):
+                wel0 = (b * WARPS + w) * epw
+                wn = min(epw, N - wel0)
+                if wn <= 0:
+                    continue
+                src, nbytes = wel0 * elem, wn * elem
+                assert src % 16 == 0 and nbytes % 16 == 0 and src + nbytes <= alloc
+                for lw in range(wn):
+                    assert lw * elem + (4 * K * K + 2 * K) * 4 <= nbytes
+
+
 def test_staging_choice():
     """Which storages are staged by bulk copies: all of K <= 5, FP32 and BF16 at K = 6, BF16
     at K = 7; FP64 from K = 5 on and everything at K = 8 read from global memory."""
