@@ -109,6 +109,7 @@ Error Solver::adjoint_prepare() {
     // column sums of A's blocks: (A^T P u)(el, ij) = sum over the 5 block slots of el of
     // u[c] * sum_r A[(c, r), (el, ij)], c = the slot's element: the column sums (over rows
     // r, ascending) of block (c, s2), the slot of c whose column element is el
+    HO2D_TRY(ensure_host_colsum());
     std::vector<double> rsT((size_t)N * 5 * K2, 0.0);
     for (int el = 0; el < N; ++el)
         for (int s = 0; s < 5; ++s) {
@@ -135,7 +136,8 @@ Error Solver::adjoint_prepare() {
         const char* dm = std::getenv("HO2D_DENSE_MAX");
         const int dmax = dm ? std::max(1, std::atoi(dm)) : kDenseMax;
         CoarseHierarchy H;
-        HO2D_TRY(build_coarse_hierarchy(transpose_csr(p0_coarse_operator(op_, N)), H, dmax, dm ? dmax : kDenseMaxFirst));
+        HO2D_TRY(build_coarse_hierarchy(transpose_csr(p0_coarse_operator(op_, N)), H, dmax, dm ? dmax : kDenseMaxFirst,
+                                        !device_setup_));
         HO2D_TRY(upload_hierarchy(H, omega, a.lev, a.dense64, a.dense32, a.pc64, a.pc32, nullptr));
     }
     HO2D_CUDA(cudaDeviceSynchronize(), "adjoint setup");

@@ -193,6 +193,22 @@ int ho2d_get_smoother(ho2d_solver* h, int32_t* kind, int32_t* exact_blocks) {
     });
 }
 
+int ho2d_set_device_setup(ho2d_solver* h, int32_t on) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (on != 0 && on != 1) return {HO2D_ERR_ARG, "on must be 0 or 1"};
+        h->s.set_device_setup(on == 1);
+        return {0, ""};
+    });
+}
+
+int ho2d_get_poisson_setup(ho2d_solver* h, int32_t which, int64_t len, double* buf) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!h->s.is_setup()) return {HO2D_ERR_ARG, "call ho2d_setup first"};
+        if (!buf) return {HO2D_ERR_ARG, "null buffer"};
+        return h->s.get_poisson_setup(which, len, buf);
+    });
+}
+
 int ho2d_set_poisson_tolerance(ho2d_solver* h, double rel_tol, int32_t max_iter) {
     return guarded(h, [&]() -> ho2d::Error {
         if (!(rel_tol > 0.0) || max_iter <= 0) return {HO2D_ERR_ARG, "tolerance and iteration cap must be positive"};

@@ -282,6 +282,15 @@ int krylov_max_blocks(int K, int N);
 // per-device set-up of the Krylov kernels for order K (krylov.cu): before the first launch
 // or graph capture on the device
 cudaError_t krylov_configure(int K);
+
+// setup_device.cu: rows x cols values between row-strided arrays (idx, optional, gives the
+// source row of each destination row), to FP32 or to BF16 (round to nearest even); the
+// in-place dense inverse (row stride w) of the coarsest level
+cudaError_t rows_to_f32(const double* src, long long ss, const int* idx, float* dst, long long ds, int rows, int cols,
+                        cudaStream_t s);
+cudaError_t rows_to_bf16(const double* src, long long ss, unsigned short* dst, long long ds, int rows, int cols,
+                         cudaStream_t s);
+cudaError_t dense_invert_device(double* a, int n, int w, cudaStream_t s, bool* singular);
 // W = M rowsum for the 5 block slots of every element ([N][5][K2], T), with the smoother
 // op selects (its element inverse M: exact blocks, BF16 blocks or Kronecker-sum factors)
 template <typename T>

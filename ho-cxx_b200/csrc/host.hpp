@@ -15,6 +15,9 @@
 #include <thread>
 #include <vector>
 
+#include "assemble_element.hpp"
+#include "vtk_nodes.hpp"
+
 namespace ho2d {
 
 constexpr int kMaxK = 8;
@@ -152,11 +155,32 @@ void kron_store(const KronFit* f, double defect, int el, KronSmoother& ks);
 // eigenvalues [N][4K^2 + 2K] (zero where the exact block is used), the index of its exact
 // inverse block in the compact array, or -1 [N], and those blocks [n_exact][K^2][K^2]
 // taken from dinv (same [rs][ij] layout).
+// The fit of every element's filtered diagonal block diag [N][K2][K2] (row ij, column rs),
+// as assemble_poisson makes it while the blocks stream by.
+void kron_fit_blocks(int K, int N, const double* diag, KronSmoother& ks);
+// The packed factors [N][4 K2 + 2 K] (zero for exact elements) and the exact-block index
+// (-1 for fitted elements, else the element's rank among the exact ones).
+void kron_factor_arrays(const KronSmoother& ks, std::vector<double>& factors, std::vector<int>& exact_index);
 void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv, std::vector<double>& factors,
                         std::vector<int>& exact_index, std::vector<double>& exact_blocks);
 
 void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const BoundaryConditions& bc,
                       PoissonOperator& op, bool keep_blocks = false, KronSmoother* kron = nullptr);
+// The coefficient lists of the block assembly (one entry per (row, metric slot)): volume
+// rows ij * K2 + rs, face (d, t) rows ij * K + q at index d * 2 + t.
+struct AsmCoefficients {
+    std::vector<AsmEntry> vol, fw[4];
+    AsmTables tables() const {
+        AsmTables t{vol.data(), (int)vol.size(), {}, {}};
+        for (int f = 0; f < 4; ++f) {
+            t.fw[f] = fw[f].data();
+            t.nfw[f] = (int)fw[f].size();
+        }
+        return t;
+    }
+};
+AsmCoefficients assembly_coefficients(const Bases& B);
+AsmBases asm_bases(const Bases& B);
 int tensor2fem(int i, int j, int lnod_in);
 
 // Fields written by the VTK output: volume arrays [N][K][K] (vorticity, streamfunction,
@@ -165,6 +189,19 @@ int tensor2fem(int i, int j, int lnod_in);
 struct VtkFields {
     const double *w, *psi, *u, *v, *rhs_diff, *rhs_adv;
     const double *bc_w, *bc_nv, *bc_pv;
+    // the smooth file's node averages [nodes] and sample values [n][3] when already made
+    // (on the device); null: made on the host from the fields above
+    const double *nw = nullptr, *np = nullptr, *nux = nullptr, *nuy = nullptr, *samp = nullptr;
+};
+// Tables of the node interpolation (vtk_nodes.hpp) for a mesh: sgb [K][L], the Gmsh slot of
+// each (ly, lx) and the element node slots flattened [N][L^2].
+struct VtkGeoHost {
+    VtkGeoHost(const Mesh& m, const Bases& B);
+    VtkGeo geo() const;
+    const Mesh& mesh;
+    const Bases& bases;
+    std::vector<double> sgb;
+    std::vector<int> t2f, nodes;
 };
 // Points of the input's sample-points file (read_process_sample_points, host_samples.cpp):
 // coordinates [n][2], the element that holds each point, and the Lnod^2 geometry shape
@@ -194,6 +231,12 @@ class VtkQueue {
   public:
     struct Job {
         std::vector<double> w, psi, u, v, rhs_diff, rhs_adv, bc_w, bc_nv, bc_pv;
+        std::vector<double> nw, np, nux, nuy, samp;  // node averages and sample values (device-made)
+        VtkFields fields() const {
+            auto p = [](const std::vector<double>& v) { return v.empty() ? nullptr : v.data(); };
+            return VtkFields{p(w),     p(psi),   p(u),     p(v),   p(rhs_diff), p(rhs_adv), p(bc_w),
+                             p(bc_nv), p(bc_pv), p(nw),    p(np),  p(nux),      p(nuy),     p(samp)};
+        }
         int problem_type = 0, indx = 0, subidx = -1;
         std::string dir;
     };

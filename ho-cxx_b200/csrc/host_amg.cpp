@@ -320,7 +320,7 @@ Csr p0_coarse_operator(const PoissonOperator& op, int N) {
     return A;
 }
 
-Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max, int dense_max_first) {
+Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max, int dense_max_first, bool invert_dense) {
     H = CoarseHierarchy();
     H.levels.emplace_back();
     H.levels[0].A = A1;
@@ -352,7 +352,7 @@ Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max, i
     if (Ab.n > 2 * std::max(dense_max, kDenseMax))
         return {4, "coarse Poisson problem did not coarsen below the dense-solve size"};
     H.n_dense = Ab.n;
-    if (!dense_inverse(Ab.n, Ab, H.dense_inv)) return {3, "singular coarsest Poisson operator"};
+    if (invert_dense && !dense_inverse(Ab.n, Ab, H.dense_inv)) return {3, "singular coarsest Poisson operator"};
     return {0, ""};
 }
 

@@ -50,7 +50,8 @@ struct CoarseHierarchy {
 Csr p0_coarse_operator(const PoissonOperator& op, int N);
 // Coarsens A1 until a level has at most dense_max rows (level 0 itself: at most
 // dense_max_first rows) and inverts that level densely.
+// invert_dense = false leaves H.dense_inv empty (the caller inverts the last level).
 Error build_coarse_hierarchy(const Csr& A1, CoarseHierarchy& H, int dense_max = kDenseMax,
-                             int dense_max_first = kDenseMaxFirst);
+                             int dense_max_first = kDenseMaxFirst, bool invert_dense = true);
 
 }  // namespace ho2d

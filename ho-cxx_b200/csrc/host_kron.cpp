@@ -298,18 +298,31 @@ void kron_store(const KronFit* f, double defect, int el, KronSmoother& ks) {
     std::copy(f->ly.begin(), f->ly.end(), ks.lam.begin() + ((size_t)el * 2 + 1) * K);
 }
 
-void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv, std::vector<double>& factors,
-                        std::vector<int>& exact_index, std::vector<double>& exact_blocks) {
-    const int K = ks.K, K2 = K * K, K4 = K2 * K2, per = 4 * K2 + 2 * K;
+void kron_fit_blocks(int K, int N, const double* diag, KronSmoother& ks) {
+    const size_t K4 = (size_t)K * K * K * K;
+    ks.K = K;
+    ks.v.assign((size_t)N * 4 * K * K, 0.0);
+    ks.lam.assign((size_t)N * 2 * K, 0.0);
+    ks.exact.assign(N, 1);
+    ks.defect.assign(N, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int el = 0; el < N; ++el) {
+        const double* D = diag + (size_t)el * K4;
+        KronFit f;
+        const bool ok = kron_fit(K, D, f);
+        kron_store(ok ? &f : nullptr, ok ? kron_defect(f, D) : 0.0, el, ks);
+    }
+}
+
+void kron_factor_arrays(const KronSmoother& ks, std::vector<double>& factors, std::vector<int>& exact_index) {
+    const int K = ks.K, K2 = K * K, per = 4 * K2 + 2 * K;
     const int N = (int)ks.exact.size();
     factors.assign((size_t)N * per, 0.0);
     exact_index.assign(N, -1);
-    exact_blocks.clear();
     int n_exact = 0;
     for (int el = 0; el < N; ++el) {
         if (ks.exact[el]) {
             exact_index[el] = n_exact++;
-            exact_blocks.insert(exact_blocks.end(), dinv.begin() + (size_t)el * K4, dinv.begin() + (size_t)(el + 1) * K4);
             continue;
         }
         std::copy(ks.v.begin() + (size_t)el * 4 * K2, ks.v.begin() + (size_t)(el + 1) * 4 * K2,
@@ -317,6 +330,16 @@ void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv,
         std::copy(ks.lam.begin() + (size_t)el * 2 * K, ks.lam.begin() + (size_t)(el + 1) * 2 * K,
                   factors.begin() + (size_t)el * per + 4 * K2);
     }
+}
+
+void kron_device_arrays(const KronSmoother& ks, const std::vector<double>& dinv, std::vector<double>& factors,
+                        std::vector<int>& exact_index, std::vector<double>& exact_blocks) {
+    const size_t K4 = (size_t)ks.K * ks.K * ks.K * ks.K;
+    kron_factor_arrays(ks, factors, exact_index);
+    exact_blocks.clear();
+    for (size_t el = 0; el < exact_index.size(); ++el)
+        if (exact_index[el] >= 0)
+            exact_blocks.insert(exact_blocks.end(), dinv.begin() + el * K4, dinv.begin() + (el + 1) * K4);
 }
 
 }  // namespace ho2d

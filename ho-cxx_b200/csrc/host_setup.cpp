@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "assemble_element.hpp"
 #include "host.hpp"
 
 namespace ho2d {
@@ -57,12 +58,11 @@ void lagrange_at(const std::vector<double>& nodes, double x, double* V, double* 
 // swaps at the end: n^3 multiply-adds and no scratch beyond two rows. The row update is
 // compiled twice, for AVX2 and for the baseline, and picked at load time; neither contracts
 // to FMA, so both give the same bits as the textbook two-matrix form.
-__attribute__((target_clones("avx2", "default"))) bool invert(int n, std::vector<double>& a) {
+__attribute__((target_clones("avx2", "default"))) bool invert(int n, double* m) {
     constexpr int kMax = kMaxK * kMaxK;
-    if (n < 1 || n > kMax || a.size() < (size_t)n * n) return false;
+    if (n < 1 || n > kMax) return false;
     int piv[kMax];
     double rk[kMax];  // the scaled pivot row, kept apart so the row updates vectorise
-    double* m = a.data();
     for (int k = 0; k < n; ++k) {
         int p = k;
         for (int i = k + 1; i < n; ++i)
@@ -467,15 +467,10 @@ Error setup_bcs(const Input& in, const Mesh& m, const Bases& B, BoundaryConditio
 
 namespace {
 
-struct Entry {
-    int row, g;
-    double c;
-};
-
 // Element-interior coupling: Lc[ij][rs] += c * G[el][b][a][r][d] (src/HO_2D.cpp:1567-1596).
-std::vector<Entry> volume_entries(const Bases& B) {
+std::vector<AsmEntry> volume_entries(const Bases& B) {
     const int K = B.K, K2 = K * K;
-    std::vector<Entry> out;
+    std::vector<AsmEntry> out;
     for (int j = 0; j < K; ++j)
         for (int i = 0; i < K; ++i)
             for (int m = 0; m < K; ++m)
@@ -498,9 +493,9 @@ std::vector<Entry> volume_entries(const Bases& B) {
 }
 
 // Face weights W[ij][q] = sum c * G[el][b][a][r][d] for face (d, t) (src/HO_2D.cpp:1614-1637).
-std::vector<Entry> face_entries(const Bases& B, int d, int t) {
+std::vector<AsmEntry> face_entries(const Bases& B, int d, int t) {
     const int K = B.K;
-    std::vector<Entry> out;
+    std::vector<AsmEntry> out;
     for (int j = 0; j < K; ++j)
         for (int i = 0; i < K; ++i)
             for (int m = 0; m < K; ++m)
@@ -516,8 +511,6 @@ std::vector<Entry> face_entries(const Bases& B, int d, int t) {
     return out;
 }
 
-inline int rs_of(int p, int q, int d, int K) { return (p * d + q * (1 - d)) * K + (p * (1 - d) + q * d); }
-inline int bf_of(int side, int k, int K) { return (side / 2) * (K - 2 * k - 1) + k; }
 
 }  // namespace
 
@@ -539,153 +532,46 @@ void assemble_poisson(const Mesh& mesh, const Bases& B, const Metrics& M, const 
         kron->exact.assign(N, 1);
         kron->defect.assign(N, 0.0);
     }
-    const std::vector<Entry> vol = volume_entries(B);
-    std::vector<Entry> fw[2][2];
-    for (int d = 0; d < 2; ++d)
-        for (int t = 0; t < 2; ++t) fw[d][t] = face_entries(B, d, t);
-    const double* gp = B.gp;
+    const AsmCoefficients co = assembly_coefficients(B);
+    const AsmBases ab = asm_bases(B);
+    const AsmTables tb = co.tables();
+    const AsmMesh am{M.G.data(), M.GB.data(), M.fJ.data(), mesh.bidx.data(), mesh.nbr.data(), mesh.nbr_side.data(),
+                     bc.sw_p.data()};
+    const AsmOut ao{op.bsrc.data(), op.rowsum.data(), op.colsum.data(), op.bsum.data(),
+                    keep_blocks ? op.blocks.data() : nullptr, op.block_col.data()};
     int64_t nnz = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nnz)
-    for (int el = 0; el < N; ++el) {
-        std::vector<double> Lc(K4, 0.0), Ln(4 * (size_t)K4, 0.0), W(K2 * K), WN(K2 * K), Nm(K * K), T(K4);
-        const double* G = &M.G[(size_t)el * K2 * 4];
-        for (const Entry& e : vol) Lc[e.row] += e.c * G[e.g];
-        for (int ijp = 0; ijp < 4; ++ijp) {
-            const int d = ijp / 2, t = ijp % 2, side = kI2F[ijp];
-            std::fill(W.begin(), W.end(), 0.0);
-            for (const Entry& e : fw[d][t]) W[e.row] += e.c * G[e.g];
-            const double* GBe = &M.GB[(((size_t)el * 2 + d) * 2 + t) * K * 2];
-            const int eb = mesh.bidx[(size_t)el * 4 + side];
-            if (eb >= 0) {
-                double* bs = &op.bsrc[(size_t)eb * K2 * K];
-                for (int ij = 0; ij < K2; ++ij)
-                    for (int q = 0; q < K; ++q)
-                        for (int p = 0; p < K; ++p) Lc[ij * K2 + rs_of(p, q, d, K)] -= 0.5 * W[ij * K + q] * B.sbb[p * 2 + t];
-                if (bc.sw_p[eb] == DIRICHLET) {
-                    for (int ij = 0; ij < K2; ++ij) {
-                        const int j = ij / K, i = ij % K;
-                        for (int q = 0; q < K; ++q) bs[ij * K + bf_of(side, q, K)] += W[ij * K + q];
-                        const int alpha = i * d + j * (1 - d);
-                        const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
-                        const double A = GBe[alpha * 2 + d], Bc = GBe[alpha * 2 + 1 - d];
-                        for (int mm = 0; mm < K; ++mm)
-                            Lc[ij * K2 + rs_of(mm, alpha, d, K)] += A * (B.sbgb[mm * 2 + t] - gp[t] * B.sbb[mm * 2 + t]) * ngr;
-                        bs[ij * K + bf_of(side, alpha, K)] += A * gp[t] * ngr;
-                        for (int mm = 0; mm < K; ++mm) bs[ij * K + bf_of(side, mm, K)] += Bc * B.D[mm * K + alpha] * ngr;
-                    }
-                } else {  // Neumann face (src/HO_2D.cpp:1660-1714)
-                    for (int r = 0; r < K; ++r) {
-                        for (int c = 0; c < K; ++c) Nm[r * K + c] = -GBe[r * 2 + 1 - d] * B.D[c * K + r];
-                        Nm[r * K + r] += -GBe[r * 2 + d] * gp[t];
-                    }
-                    invert(K, Nm);
-                    const double sign = t ? 1.0 : -1.0;
-                    double s[kMaxK];
-                    for (int p = 0; p < K; ++p) s[p] = std::sqrt(GBe[p * 2 + d] * M.fJ[((size_t)el * 4 + ijp) * K + p]);
-                    for (int ij = 0; ij < K2; ++ij)
-                        for (int c = 0; c < K; ++c) {
-                            double acc = 0.0;
-                            for (int q = 0; q < K; ++q) acc += W[ij * K + q] * Nm[q * K + c];
-                            WN[ij * K + c] = acc;
-                        }
-                    for (int ij = 0; ij < K2; ++ij) {
-                        const int j = ij / K, i = ij % K;
-                        const int alpha = i * d + j * (1 - d);
-                        const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
-                        bs[ij * K + bf_of(side, alpha, K)] += sign * ngr * s[alpha];
-                        for (int p = 0; p < K; ++p) {
-                            bs[ij * K + bf_of(side, p, K)] -= sign * WN[ij * K + p] * s[p];
-                            const double tmp4 = B.sbgb[p * 2 + t] - gp[t] * B.sbb[p * 2 + t];
-                            for (int c = 0; c < K; ++c)
-                                Lc[ij * K2 + rs_of(p, c, d, K)] += WN[ij * K + c] * tmp4 * GBe[c * 2 + d];
-                        }
-                    }
-                }
-            } else {  // interior face (src/HO_2D.cpp:1716-1792)
-                const int eln = mesh.nbr[(size_t)el * 4 + side];
-                const int ijpm = kF2I[mesh.nbr_side[(size_t)el * 4 + side]];
-                const int dn = ijpm / 2, tn = ijpm % 2;
-                const int rev = (d + t + dn + tn + 1) % 2;
-                double* L = &Ln[(size_t)ijp * K4];
-                for (int ij = 0; ij < K2; ++ij)
-                    for (int q = 0; q < K; ++q) {
-                        const int Mq = rev * (K - 2 * q - 1) + q;
-                        for (int p = 0; p < K; ++p) L[ij * K2 + rs_of(p, Mq, dn, K)] += 0.5 * W[ij * K + q] * B.sbb[p * 2 + tn];
-                    }
-                const double* GBn = &M.GB[(((size_t)eln * 2 + dn) * 2 + tn) * K * 2];
-                const double sign = (t == tn) ? -1.0 : 1.0;
-                for (int ij = 0; ij < K2; ++ij) {
-                    const int j = ij / K, i = ij % K;
-                    const int alpha = i * d + j * (1 - d);
-                    const int Ma = rev * (K - 2 * alpha - 1) + alpha;
-                    const double A = GBe[alpha * 2 + d], Bc = GBe[alpha * 2 + 1 - d];
-                    const double An = GBn[Ma * 2 + dn], Bn = GBn[Ma * 2 + 1 - dn];
-                    const double ngr = B.gR[(j * d + i * (1 - d)) * 2 + t];
-                    for (int mm = 0; mm < K; ++mm) {
-                        const int Mm = rev * (K - 2 * mm - 1) + mm;
-                        Lc[ij * K2 + rs_of(mm, alpha, d, K)] +=
-                            (0.5 * A * B.sbgb[mm * 2 + t] - 0.25 * gp[t] * A * B.sbb[mm * 2 + t] +
-                             0.25 * sign * gp[tn] * An * B.sbb[mm * 2 + t]) * ngr;
-                        L[ij * K2 + rs_of(mm, Ma, dn, K)] +=
-                            (0.5 * sign * An * B.sbgb[mm * 2 + tn] - 0.25 * sign * gp[tn] * An * B.sbb[mm * 2 + tn] +
-                             0.25 * gp[t] * A * B.sbb[mm * 2 + tn]) * ngr;
-                        const double coeff = 0.25 * (Bc * B.D[mm * K + alpha] + sign * Bn * B.D[Mm * K + Ma]) * ngr;
-                        for (int p = 0; p < K; ++p) {
-                            Lc[ij * K2 + rs_of(p, mm, d, K)] += coeff * B.sbb[p * 2 + t];
-                            L[ij * K2 + rs_of(p, Mm, dn, K)] += coeff * B.sbb[p * 2 + tn];
-                        }
-                    }
-                }
-                op.block_col[(size_t)el * 5 + 1 + ijp] = eln;
+#pragma omp parallel reduction(+ : nnz)
+    {
+        std::vector<double> Lc(K4), L(K4), W((size_t)K2 * K), WN((size_t)K2 * K), Nm((size_t)K * K);
+        const AsmScratch sc{{Lc.data(), 1}, {L.data(), 1}, {W.data(), 1}, {WN.data(), 1}, {Nm.data(), 1}};
+#pragma omp for schedule(dynamic, 16)
+        for (int el = 0; el < N; ++el) {
+            nnz += assemble_element(el, ab, tb, am, ao, sc, [](int n, Str<double> a) { return invert(n, a.p); });
+            if (kron) {  // the Kronecker-sum fit of the filtered diagonal block ([ij][rs])
+                KronFit f;
+                const bool ok = kron_fit(K, Lc.data(), f);
+                kron_store(ok ? &f : nullptr, ok ? kron_defect(f, Lc.data()) : 0.0, el, *kron);
             }
-        }
-        op.block_col[(size_t)el * 5] = el;
-        // filter, transpose (T[rs][ij]) and reduce each block: row sums over rs, column sums
-        // over ij and the block sum in the stored order
-        std::vector<double> Dm(K4);
-        auto store = [&](const double* src, int slot) {
-            int64_t cnt = 0;
+            // inverse of the filtered diagonal block, stored transposed like the blocks
+            invert(K2, Lc.data());
+            double* di = &op.dinv[(size_t)el * K4];
             for (int ij = 0; ij < K2; ++ij)
-                for (int rs = 0; rs < K2; ++rs) {
-                    double v = src[ij * K2 + rs];
-                    if (!(std::fabs(v) > 1e-14)) v = 0.0;
-                    else ++cnt;
-                    T[rs * K2 + ij] = v;
-                    if (slot == 0) Dm[ij * K2 + rs] = v;
-                }
-            const size_t eb = (size_t)el * 5 + slot;
-            double* rsum = &op.rowsum[eb * K2];
-            double* csum = &op.colsum[eb * K2];
-            double tot = 0.0;
-            for (int rs = 0; rs < K2; ++rs)
-                for (int ij = 0; ij < K2; ++ij) {
-                    rsum[ij] += T[rs * K2 + ij];
-                    tot += T[rs * K2 + ij];
-                }
-            for (int rs = 0; rs < K2; ++rs) {
-                double acc = 0.0;
-                for (int ij = 0; ij < K2; ++ij) acc += T[rs * K2 + ij];
-                csum[rs] = acc;
-            }
-            op.bsum[eb] = tot;
-            if (keep_blocks) std::copy(T.begin(), T.end(), op.blocks.begin() + eb * K4);
-            return cnt;
-        };
-        nnz += store(Lc.data(), 0);
-        for (int ijp = 0; ijp < 4; ++ijp)
-            if (op.block_col[(size_t)el * 5 + 1 + ijp] >= 0) nnz += store(&Ln[(size_t)ijp * K4], 1 + ijp);
-        if (kron) {  // the Kronecker-sum fit of the filtered diagonal block ([ij][rs])
-            KronFit f;
-            const bool ok = kron_fit(K, Dm.data(), f);
-            kron_store(ok ? &f : nullptr, ok ? kron_defect(f, Dm.data()) : 0.0, el, *kron);
+                for (int rs = 0; rs < K2; ++rs) di[rs * K2 + ij] = Lc[ij * K2 + rs];
         }
-        // inverse of the filtered diagonal block, stored transposed like the blocks
-        invert(K2, Dm);
-        double* di = &op.dinv[(size_t)el * K4];
-        for (int ij = 0; ij < K2; ++ij)
-            for (int rs = 0; rs < K2; ++rs) di[rs * K2 + ij] = Dm[ij * K2 + rs];
     }
     op.nnz = nnz;
+}
+
+AsmBases asm_bases(const Bases& B) {
+    return AsmBases{B.K, B.sbb.data(), B.sbgb.data(), B.gR.data(), B.D.data(), {B.gp[0], B.gp[1]}};
+}
+
+AsmCoefficients assembly_coefficients(const Bases& B) {
+    AsmCoefficients c;
+    c.vol = volume_entries(B);
+    for (int d = 0; d < 2; ++d)
+        for (int t = 0; t < 2; ++t) c.fw[d * 2 + t] = face_entries(B, d, t);
+    return c;
 }
 
 }  // namespace ho2d

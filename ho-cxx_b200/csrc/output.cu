@@ -1,8 +1,11 @@
 // output.cu -- the reference's VTK output (src/HO_2D.cpp:3369-3692) of the device fields:
-// the fields are copied to the host and written by write_vtk_files (output_host.cpp), on
-// the caller's thread for trigger_write and on VtkQueue's thread for the time loop's dumps.
+// the smooth file's node averages and sample values are made on the device
+// (output_device.cu), the solution-point fields and those are copied to the host and
+// written by write_vtk_files (output_host.cpp), on the caller's thread for trigger_write
+// and on VtkQueue's thread for the time loop's dumps.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -29,8 +32,13 @@ Error Solver::vtk_job(int indx, int subidx, const std::string& dir, VtkQueue::Jo
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
     const int K = in_.knod;
     const size_t nv = (size_t)mesh_.n_el * K * K;
+    // the smooth file's node values are made on the device unless HO2D_HOST_OUTPUT=1; then
+    // only the vorticity file's fields come back
+    const char* ho = std::getenv("HO2D_HOST_OUTPUT");
+    const bool on_device = !(ho && std::string(ho) == "1");
+    if (on_device) HO2D_TRY(vtk_nodes_device(j));
     HO2D_CUDA(fetch<double>(j.w, d.omega, nv), "copy");
-    HO2D_CUDA(fetch<double>(j.psi, d.psi64, nv), "copy");
+    if (!on_device) HO2D_CUDA(fetch<double>(j.psi, d.psi64, nv), "copy");
     if (stage32_) {
         HO2D_CUDA(fetch<float>(j.u, d.u, nv), "copy");
         HO2D_CUDA(fetch<float>(j.v, d.v, nv), "copy");
@@ -43,9 +51,11 @@ Error Solver::vtk_job(int indx, int subidx, const std::string& dir, VtkQueue::Jo
         HO2D_CUDA(fetch<double>(j.rhs_adv, d.rhs_adv, nv), "copy");
     }
     const size_t nb = (size_t)mesh_.n_eb * K;
-    HO2D_CUDA(fetch<double>(j.bc_w, d.bc_w, nb), "copy");
-    HO2D_CUDA(fetch<double>(j.bc_nv, d.bc_nv, nb), "copy");
-    HO2D_CUDA(fetch<double>(j.bc_pv, d.bc_pv, nb), "copy");
+    if (!on_device) {
+        HO2D_CUDA(fetch<double>(j.bc_w, d.bc_w, nb), "copy");
+        HO2D_CUDA(fetch<double>(j.bc_nv, d.bc_nv, nb), "copy");
+        HO2D_CUDA(fetch<double>(j.bc_pv, d.bc_pv, nb), "copy");
+    }
     j.problem_type = in_.problem_type;
     j.indx = indx;
     j.subidx = subidx;
@@ -60,9 +70,7 @@ Error Solver::write_vtk(int indx, int subidx, const std::string& dir) {
     HO2D_TRY(vtk_queue_.wait());
     VtkQueue::Job j;
     HO2D_TRY(vtk_job(indx, subidx, dir, j));
-    VtkFields fl{j.w.data(),       j.psi.data(),  j.u.data(),     j.v.data(),    j.rhs_diff.data(),
-                 j.rhs_adv.data(), j.bc_w.data(), j.bc_nv.data(), j.bc_pv.data()};
-    return write_vtk_files(mesh_, B_, in_.problem_type, fl, indx, subidx, dir, &samples_);
+    return write_vtk_files(mesh_, B_, in_.problem_type, j.fields(), indx, subidx, dir, &samples_);
 }
 
 // a dump of the time loop: written on the queue's thread while the loop goes on

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "host.hpp"
+#include "vtk_nodes.hpp"
 
 namespace ho2d {
 
@@ -31,6 +32,31 @@ struct File {
 };
 
 }  // namespace
+
+VtkGeoHost::VtkGeoHost(const Mesh& m, const Bases& B) : mesh(m), bases(B) {
+    const int K = B.K, L = m.lnod, L2 = L * L;
+    sgb.resize((size_t)K * L);
+    for (int k = 0; k < K; ++k)
+        for (int l = 0; l < L; ++l) {
+            const double x = L > 1 ? -1.0 + 2.0 * l / (L - 1) : 0.0;
+            double p = 1.0;
+            for (int q = 0; q < K; ++q)
+                if (q != k) p *= (x - B.xs[q]) / (B.xs[k] - B.xs[q]);
+            sgb[(size_t)k * L + l] = p;
+        }
+    t2f.resize(L2);
+    for (int ly = 0; ly < L; ++ly)
+        for (int lx = 0; lx < L; ++lx) t2f[ly * L + lx] = tensor2fem(lx, ly, L - 1);
+    nodes.resize((size_t)m.n_el * L2);
+    for (int el = 0; el < m.n_el; ++el)
+        for (int l = 0; l < L2; ++l) nodes[(size_t)el * L2 + l] = m.elem_nodes[el][l];
+}
+
+VtkGeo VtkGeoHost::geo() const {
+    return VtkGeo{mesh.n_el,       bases.K,          mesh.lnod,         mesh.n_eb,          sgb.data(),
+                  t2f.data(),      nodes.data(),     mesh.node_xy.data(), mesh.be_el.data(), mesh.be_side.data(),
+                  bases.gbgb.data(), bases.gbb.data(), bases.gsb.data(),   bases.gsgb.data()};
+}
 
 Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, const VtkFields& fl, int indx, int subidx,
                       const std::string& dir, const SamplePoints* samples) {
@@ -82,112 +108,50 @@ Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, cons
     }
 
     // ---- save_smooth_vtk: values at the geometry nodes, averaged over the elements
-    // sharing a node. sgb[k][l]: solution basis k at geometry node l (equispaced in [-1, 1]).
-    std::vector<double> sgb((size_t)K * L);
-    for (int k = 0; k < K; ++k)
-        for (int l = 0; l < L; ++l) {
-            const double x = L > 1 ? -1.0 + 2.0 * l / (L - 1) : 0.0;
-            double p = 1.0;
-            for (int m = 0; m < K; ++m)
-                if (m != k) p *= (x - B_.xs[m]) / (B_.xs[k] - B_.xs[m]);
-            sgb[(size_t)k * L + l] = p;
-        }
-    std::vector<double> om((size_t)N * L2, 0.0), ps((size_t)N * L2, 0.0), vx((size_t)N * L2, 0.0),
-        vy((size_t)N * L2, 0.0);
-    for (int el = 0; el < N; ++el)
-        for (int ly = 0; ly < L; ++ly)
-            for (int lx = 0; lx < L; ++lx) {
-                const size_t g = (size_t)el * L2 + tensor2fem(lx, ly, lin);
-                double a = 0, b = 0, c = 0, e = 0;
-                for (int ky = 0; ky < K; ++ky)
-                    for (int kx = 0; kx < K; ++kx) {
-                        const double coeff = sgb[(size_t)ky * L + ly] * sgb[(size_t)kx * L + lx];
-                        const size_t p = (size_t)el * K2 + ky * K + kx;
-                        a += coeff * w[p];
-                        b += coeff * psi[p];
-                        c += coeff * u[p];
-                        e += coeff * v[p];
-                    }
-                om[g] = a;
-                ps[g] = b;
-                vx[g] = c;
-                vy[g] = e;
-            }
-    // boundary nodes: BC_vorticity, and the Cartesian velocity from the normal (local h
-    // direction) and counter-clockwise tangential components (src/HO_2D.cpp:3440-3513)
-    std::vector<double> cvx(nb, 0.0), cvy(nb, 0.0);
-    for (int e = 0; e < mesh_.n_eb; ++e) {
-        const int el = mesh_.be_el[e], side = mesh_.be_side[e], ijp = kF2I[side], dd = ijp / 2, t = ijp % 2;
-        const double parl_sign = -1.0 + 2.0 * (side / 2);
-        for (int k = 0; k < K; ++k) {
-            double xx = 0, xe = 0, yx = 0, ye = 0;  // d(x, y)/d(xi, eta) at face point k
-            for (int j = 0; j < L; ++j)
-                for (int i = 0; i < L; ++i) {
-                    const int nd = mesh_.elem_nodes[el][tensor2fem(i, j, lin)];
-                    const double X = mesh_.node_xy[2 * nd], Y = mesh_.node_xy[2 * nd + 1];
-                    double wx, we;
-                    if (dd == 0) {  // W/E face: xi = -+1, eta = x_k
-                        wx = B_.gbgb[i * 2 + t] * B_.gsb[j * K + k];
-                        we = B_.gbb[i * 2 + t] * B_.gsgb[j * K + k];
-                    } else {  // S/N face: eta = -+1, xi = x_k
-                        wx = B_.gsgb[i * K + k] * B_.gbb[j * 2 + t];
-                        we = B_.gsb[i * K + k] * B_.gbgb[j * 2 + t];
-                    }
-                    xx += wx * X;
-                    yx += wx * Y;
-                    xe += we * X;
-                    ye += we * Y;
-                }
-            const size_t q = (size_t)e * K + (side / 2) * (K - 2 * k - 1) + k;
-            if (dd == 0) {
-                const double g2 = std::sqrt(xe * xe + ye * ye), un = bnv[q], ut = parl_sign * bpv[q];
-                cvx[q] = (1.0 / g2) * (un * ye + ut * xe);
-                cvy[q] = (1.0 / g2) * (-un * xe + ut * ye);
-            } else {
-                const double g1 = std::sqrt(xx * xx + yx * yx), un = bnv[q], ut = parl_sign * bpv[q];
-                cvx[q] = (1.0 / g1) * (-un * yx + ut * xx);
-                cvy[q] = (1.0 / g1) * (un * xx + ut * yx);
-            }
-        }
-    }
-    for (int e = 0; e < mesh_.n_eb; ++e) {
-        const int el = mesh_.be_el[e], side = mesh_.be_side[e], ijp = kF2I[side], dd = ijp / 2, t = ijp % 2;
-        for (int l = 0; l < L; ++l) {
-            const int su2pv = l * ((1 - dd) * L + dd) + t * (L - 1) * (dd * (L - 1) + 1);
-            const size_t g = (size_t)el * L2 + tensor2fem(su2pv % L, su2pv / L, lin);
-            double a = 0, c = 0, f2 = 0;
-            for (int m = 0; m < K; ++m) {
-                const double coeff = sgb[(size_t)m * L + l];
-                const size_t q = (size_t)e * K + (side / 2) * (K - 2 * m - 1) + m;
-                a += coeff * bw[q];
-                c += coeff * cvx[q];
-                f2 += coeff * cvy[q];
-            }
-            om[g] = a;
-            vx[g] = c;
-            vy[g] = f2;
-        }
-    }
-    // nodes in the compact numbering of the mesh reader (first use: edges, then elements),
-    // which is the reference's numbering (src/Mesh.cpp:296-333)
+    // sharing a node (vtk_nodes.hpp), unless the caller brings them (the device's)
     const size_t nn = mesh_.node_xy.size() / 2;
-    std::vector<double> nw(nn, 0.0), np(nn, 0.0), nux(nn, 0.0), nuy(nn, 0.0);
-    std::vector<int> rep(nn, 0);
-    for (int el = 0; el < N; ++el)
-        for (int l = 0; l < L2; ++l) {
-            const size_t g = (size_t)el * L2 + l;
-            const int nd = mesh_.elem_nodes[el][l];
-            nux[nd] += vx[g];
-            nuy[nd] += vy[g];
-            nw[nd] += om[g];
-            np[nd] += ps[g];
-            ++rep[nd];
+    std::vector<double> hw, hp, hux, huy, hs;
+    const double *nw = fl.nw, *np = fl.np, *nux = fl.nux, *nuy = fl.nuy, *samp = fl.samp;
+    if (!nw) {
+        const VtkGeoHost gh(mesh_, B_);
+        const VtkGeo g = gh.geo();
+        std::vector<double> om((size_t)N * L2, 0.0), ps((size_t)N * L2, 0.0), vx((size_t)N * L2, 0.0),
+            vy((size_t)N * L2, 0.0);
+        for (int el = 0; el < N; ++el)
+            vtk_element_nodes(g, el, w, psi, u, v, om.data(), ps.data(), vx.data(), vy.data());
+        std::vector<double> cvx(nb, 0.0), cvy(nb, 0.0);
+        for (int e = 0; e < mesh_.n_eb; ++e) vtk_edge_velocity(g, e, bnv, bpv, cvx.data(), cvy.data());
+        for (int e = 0; e < mesh_.n_eb; ++e) vtk_edge_nodes(g, e, bw, cvx.data(), cvy.data(), om.data(), vx.data(), vy.data());
+        // nodes in the compact numbering of the mesh reader (first use: edges, then
+        // elements), which is the reference's numbering (src/Mesh.cpp:296-333)
+        hw.assign(nn, 0.0);
+        hp.assign(nn, 0.0);
+        hux.assign(nn, 0.0);
+        huy.assign(nn, 0.0);
+        std::vector<int> rep(nn, 0);
+        for (int el = 0; el < N; ++el)
+            for (int l = 0; l < L2; ++l) {
+                const size_t q = (size_t)el * L2 + l;
+                const int nd = mesh_.elem_nodes[el][l];
+                hux[nd] += vx[q];
+                huy[nd] += vy[q];
+                hw[nd] += om[q];
+                hp[nd] += ps[q];
+                ++rep[nd];
+            }
+        for (size_t n = 0; n < nn; ++n) vtk_node_average(rep[n], hw[n], hp[n], hux[n], huy[n]);
+        nw = hw.data();
+        np = hp.data();
+        nux = hux.data();
+        nuy = huy.data();
+        if (samples && samples->size() > 0) {
+            hs.assign(3 * samples->size(), 0.0);
+            for (size_t si = 0; si < samples->size(); ++si) {
+                const int el = samples->elem[si];
+                vtk_sample(L2, mesh_.elem_nodes[el].data(), &samples->shape[si * L2], nw, nux, nuy, &hs[3 * si]);
+            }
+            samp = hs.data();
         }
-    for (size_t n = 0; n < nn; ++n) {
-        nw[n] /= rep[n];
-        np[n] /= rep[n];
-        nux[n] *= 1.0 / rep[n];
-        nuy[n] *= 1.0 / rep[n];
     }
     File fh(pre + "problem" + tag);
     if (!fh.f) return {2, "cannot write " + pre + "problem" + tag};
@@ -215,18 +179,9 @@ Error write_vtk_files(const Mesh& mesh_, const Bases& B_, int problem_type, cons
     std::snprintf(sname, sizeof(sname), "sampling_points%d_K%d_L%d_%05d.dat", problem_type, K, L, indx);
     File sh(pre + sname);
     if (!sh.f) return {2, "cannot write " + pre + sname};
-    for (size_t s = 0; s < samples->size(); ++s) {
-        const int el = samples->elem[s];
-        const double* sf = &samples->shape[s * L2];
-        double om_s = 0.0, ux = 0.0, uy = 0.0;
-        for (int l = 0; l < L2; ++l) {
-            const int nd = mesh_.elem_nodes[el][l];
-            om_s += sf[l] * nw[nd];
-            ux += sf[l] * nux[nd];
-            uy += sf[l] * nuy[nd];
-        }
-        std::fprintf(sh.f, "%g %g %g %g %g\n", samples->xy[2 * s], samples->xy[2 * s + 1], om_s, ux, uy);
-    }
+    for (size_t si = 0; si < samples->size(); ++si)
+        std::fprintf(sh.f, "%g %g %g %g %g\n", samples->xy[2 * si], samples->xy[2 * si + 1], samp[3 * si],
+                     samp[3 * si + 1], samp[3 * si + 2]);
     return {0, ""};
 }
 
@@ -236,8 +191,7 @@ Error VtkQueue::submit(const Mesh& mesh, const Bases& B, const SamplePoints* sam
     auto owned = std::make_shared<Job>(std::move(job));
     auto work = [this, &mesh, &B, samples, owned]() {
         const Job& j = *owned;
-        const VtkFields f{j.w.data(),       j.psi.data(),  j.u.data(),     j.v.data(),    j.rhs_diff.data(),
-                          j.rhs_adv.data(), j.bc_w.data(), j.bc_nv.data(), j.bc_pv.data()};
+        const VtkFields f = j.fields();
         // nothing may leave the writer thread: every exception becomes an error status, and
         // building the message (which allocates) may itself throw, so it has a fixed fallback
         try {

@@ -105,11 +105,15 @@ Error Solver::setup_from_mesh() {
         };
         smoother_kind_ = on("HO2D_SMOOTHER_KRON") ? 2 : (on("HO2D_SMOOTHER_BF16") ? 1 : 0);
     }
-    // kind 2: the Kronecker-sum fit of every diagonal block, made while the blocks stream by
+    // the Poisson operator: assembled on the device unless the host is asked for
+    // (set_device_setup(false) or HO2D_HOST_SETUP=1); smoother kind 2 adds the Kronecker-sum
+    // fit of every diagonal block
+    device_setup_ = device_setup_req_ >= 0 ? device_setup_req_ == 1 : [] {
+        const char* e = std::getenv("HO2D_HOST_SETUP");
+        return !(e && std::string(e) == "1");
+    }();
     kron_ = KronSmoother();
-    assemble_poisson(mesh_, B_, M_, bc_, op_, false, smoother_kind_ == 2 ? &kron_ : nullptr);
-    smoother_exact_ = 0;
-    for (unsigned char x : kron_.exact) smoother_exact_ += x ? 1 : 0;
+    if (!device_setup_) assemble_poisson(mesh_, B_, M_, bc_, op_, false, smoother_kind_ == 2 ? &kron_ : nullptr);
 
     DeviceState& d = *d_;
     HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
@@ -158,7 +162,6 @@ Error Solver::setup_from_mesh() {
     HO2D_CUDA(upload(d.bc_pv, bc_.bc_pv), "upload");
     HO2D_CUDA(upload(d.bc_d, bc_.bc_d), "upload");
     HO2D_CUDA(upload(d.edge_y, bc_.edge_y), "upload");
-    HO2D_CUDA(upload(d.bsrc, op_.bsrc), "upload");
     const std::vector<double> zb((size_t)neb * K, 0.0);
     HO2D_CUDA(upload(d.bc_w, zb), "upload");
     HO2D_CUDA(upload(d.vjump, zb), "upload");
@@ -175,12 +178,23 @@ Error Solver::setup_from_mesh() {
     // every element's block starts on a 16-byte boundary (padded_count): the smoothing
     // kernel stages blocks with bulk copies
     const int K4 = K2 * K2;
-    HO2D_CUDA(upload(d.dinv64, padded_rows<double>(op_.dinv, N, K4, padded_count(K4, 8))), "upload block-Jacobi");
-    HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
-    HO2D_CUDA(d.W64.alloc(op_.rowsum.size() * sizeof(double)), "alloc smoothed row sums");
-    HO2D_CUDA(d.W32.alloc(op_.rowsum.size() * sizeof(float)), "alloc smoothed row sums");
+    d.vtk.ready = false;  // the VTK node tables follow the mesh
+    d.colsum64.reset();
+    if (device_setup_) {
+        std::vector<double> diag;
+        HO2D_TRY(assemble_device(smoother_kind_ == 2 ? &diag : nullptr));
+        if (smoother_kind_ == 2) kron_fit_blocks(K, N, diag.data(), kron_);
+    } else {
+        HO2D_CUDA(upload(d.bsrc, op_.bsrc.empty() ? std::vector<double>{0.0} : op_.bsrc), "upload");
+        HO2D_CUDA(upload(d.dinv64, padded_rows<double>(op_.dinv, N, K4, padded_count(K4, 8))), "upload block-Jacobi");
+        HO2D_CUDA(upload(d.rowsum64, op_.rowsum), "upload block row sums");
+        HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
+    }
+    smoother_exact_ = 0;
+    for (unsigned char x : kron_.exact) smoother_exact_ += x ? 1 : 0;
+    HO2D_CUDA(d.W64.alloc((size_t)N * 5 * K2 * sizeof(double)), "alloc smoothed row sums");
+    HO2D_CUDA(d.W32.alloc((size_t)N * 5 * K2 * sizeof(float)), "alloc smoothed row sums");
     HO2D_CUDA(d.zf.alloc((size_t)N * K2 * sizeof(double)), "alloc smoother vector");
-    HO2D_CUDA(upload(d.bcol, op_.block_col), "upload block columns");
     {
         // where the coarse cycle delivers each element's level-0 value: every block slot
         // (el, s) with block_col[5 el + s] = c reads u0 of element c
@@ -424,26 +438,41 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
         for (DeviceBuffer* v : {&b->f, &b->u}) HO2D_CUDA(upload(*v, z), "alloc coarse vectors");
         lev.push_back(std::move(b));
     }
-    // coarsest inverse, rows padded to a multiple of 4 entries (16-byte row starts)
+    // coarsest inverse, rows padded to a multiple of 4 entries (16-byte row starts): the
+    // host's, or inverted on the device in place when the hierarchy comes without it
     const int nd = H.n_dense, wd = (nd + 3) / 4 * 4;
     std::vector<double> dpad((size_t)nd * wd, 0.0);
-    for (int i = 0; i < nd; ++i)
-        std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
-                  dpad.begin() + (size_t)i * wd);
+    const bool on_device = H.dense_inv.empty();
+    if (on_device) {
+        const Csr& Ab = H.levels.back().A;
+        for (int i = 0; i < nd; ++i)
+            for (int k = Ab.ptr[i]; k < Ab.ptr[i + 1]; ++k) dpad[(size_t)i * wd + Ab.col[k]] += Ab.val[k];
+    } else {
+        for (int i = 0; i < nd; ++i)
+            std::copy(H.dense_inv.begin() + (size_t)i * nd, H.dense_inv.begin() + (size_t)(i + 1) * nd,
+                      dpad.begin() + (size_t)i * wd);
+    }
     HO2D_CUDA(upload(dense64, dpad), "upload dense");
+    if (on_device) {
+        bool singular = false;
+        HO2D_CUDA(dense_invert_device(dense64.as<double>(), nd, wd, d_->stream, &singular), "dense inverse");
+        if (singular) return {3, "singular coarsest Poisson operator"};
+    }
     // the FP32 preconditioner's coarsest inverse in BF16 (half the bytes of the largest
     // coarse read; the preconditioner's precision changes only the iteration count) when
     // it is a level below the element level
     const bool dense16 = nl > 1;
     const int w16 = (nd + 7) / 8 * 8;
     if (dense16) {
-        std::vector<uint16_t> d16((size_t)nd * w16 + 8, 0);
-        for (int i = 0; i < nd; ++i)
-            for (int c = 0; c < nd; ++c) d16[(size_t)i * w16 + c] = bf16_bits((float)H.dense_inv[(size_t)i * nd + c]);
-        HO2D_CUDA(upload(dense32, d16), "upload dense");
+        HO2D_CUDA(dense32.alloc(((size_t)nd * w16 + 8) * sizeof(uint16_t)), "alloc dense");
+        HO2D_CUDA(cudaMemsetAsync(dense32.get(), 0, dense32.bytes(), d_->stream), "memset");
+        HO2D_CUDA(rows_to_bf16(dense64.as<double>(), wd, dense32.as<uint16_t>(), w16, nd, nd, d_->stream), "dense");
     } else {
-        HO2D_CUDA(upload_as<float>(dense32, dpad), "upload dense");
+        HO2D_CUDA(dense32.alloc(((size_t)nd * wd + 1) * sizeof(float)), "alloc dense");
+        HO2D_CUDA(cudaMemsetAsync(dense32.get(), 0, dense32.bytes(), d_->stream), "memset");
+        HO2D_CUDA(rows_to_f32(dense64.as<double>(), wd, nullptr, dense32.as<float>(), wd, nd, nd, d_->stream), "dense");
     }
+    HO2D_CUDA(cudaStreamSynchronize(d_->stream), "dense");
     auto fill = [&](auto& pc, bool f32) {
         using T = typename std::remove_const<typename std::remove_pointer<decltype(pc.dense.val)>::type>::type;
         pc.nlev = nl;
@@ -486,6 +515,18 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
 // Builds the P0 coarse hierarchy on the host and the device views of both precisions.
 // HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight;
 // HO2D_DENSE_MAX bounds the dense coarsest level (a test hook for other hierarchy shapes).
+// The block column sums on the host: kept by the host assembly, downloaded once after the
+// device assembly.
+Error Solver::ensure_host_colsum() {
+    if (!op_.colsum.empty()) return {0, ""};
+    DeviceState& d = *d_;
+    if (!d.colsum64.get()) return {3, "block column sums unavailable"};
+    op_.colsum.resize(d.colsum64.bytes() / sizeof(double));
+    HO2D_CUDA(cudaMemcpy(op_.colsum.data(), d.colsum64.get(), d.colsum64.bytes(), cudaMemcpyDeviceToHost),
+              "download block column sums");
+    return {0, ""};
+}
+
 Error Solver::setup_preconditioner() {
     DeviceState& d = *d_;
     const int N = mesh_.n_el;
@@ -502,7 +543,8 @@ Error Solver::setup_preconditioner() {
     const char* dm = std::getenv("HO2D_DENSE_MAX");
     const int dmax = dm ? std::max(1, std::atoi(dm)) : kDenseMax;
     CoarseHierarchy H;
-    HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H, dmax, dm ? dmax : kDenseMaxFirst));
+    HO2D_TRY(build_coarse_hierarchy(p0_coarse_operator(op_, N), H, dmax, dm ? dmax : kDenseMaxFirst,
+                                    !device_setup_));
     HO2D_TRY(upload_hierarchy(H, omega, d.lev, d.dense64, d.dense32, d.pc64, d.pc32, &coarse_sizes_));
     coarse_levels_ = (int)coarse_sizes_.size();
     if (verbose_) {
@@ -519,27 +561,42 @@ Error Solver::upload_precision_arrays() {
     const std::vector<double>* mets[9] = {&M_.xxi, &M_.xeta, &M_.yxi, &M_.yeta, &M_.J, &M_.fA, &M_.fB, &M_.fJ, &M_.fAn};
     for (int i = 0; i < 9; ++i) HO2D_CUDA(upload_as<float>(d.m32[i], *mets[i]), "upload fp32 metrics");
     const int N = mesh_.n_el, K = in_.knod, K2 = K * K, K4 = K2 * K2;
-    HO2D_CUDA(upload(d.dinv32, padded_rows<float>(op_.dinv, N, K4, padded_count(K4, 4))), "upload fp32 block-Jacobi");
+    // the FP32 (and BF16) copies are made on the device from the FP64 arrays
+    const long long s8 = padded_count(K4, 8), s4 = padded_count(K4, 4);
+    HO2D_CUDA(d.dinv32.alloc(((size_t)N * s4 + 1) * sizeof(float)), "alloc fp32 block-Jacobi");
+    HO2D_CUDA(cudaMemsetAsync(d.dinv32.get(), 0, d.dinv32.bytes(), d.stream), "memset");
+    HO2D_CUDA(rows_to_f32(d.dinv64.as<double>(), s8, nullptr, d.dinv32.as<float>(), s4, N, K4, d.stream),
+              "fp32 block-Jacobi");
     // smoother kind 1: the FP32 smoother reads a BF16 copy of the inverse blocks (half the
     // bytes; the preconditioner's precision changes only the inner iteration count)
     if (smoother_kind_ == 1) {
-        const int st = padded_count(K4, 2);
-        std::vector<uint16_t> h((size_t)N * st + 1, 0);
-        for (size_t e = 0; e < (size_t)N; ++e)
-            for (int i = 0; i < K4; ++i) h[e * st + i] = bf16_bits((float)op_.dinv[e * K4 + i]);
-        HO2D_CUDA(upload(d.dinv_bf16, h), "upload bf16 block-Jacobi");
+        const long long st = padded_count(K4, 2);
+        HO2D_CUDA(d.dinv_bf16.alloc(((size_t)N * st + 1) * sizeof(uint16_t)), "alloc bf16 block-Jacobi");
+        HO2D_CUDA(cudaMemsetAsync(d.dinv_bf16.get(), 0, d.dinv_bf16.bytes(), d.stream), "memset");
+        HO2D_CUDA(rows_to_bf16(d.dinv64.as<double>(), s8, d.dinv_bf16.as<uint16_t>(), st, N, K4, d.stream),
+                  "bf16 block-Jacobi");
     }
     if (kron_.K > 0) {  // the Kronecker-sum smoother's arrays (FP32), smoother kind 2
-        std::vector<double> f, ex;
-        std::vector<int> xi;
-        kron_device_arrays(kron_, op_.dinv, f, xi, ex);
+        std::vector<double> f;
+        std::vector<int> xi, rows;
+        kron_factor_arrays(kron_, f, xi);
+        for (int el = 0; el < N; ++el)
+            if (xi[el] >= 0) rows.push_back(el);
         const int per = 4 * K2 + 2 * K;
         HO2D_CUDA(upload(d.kron_f, padded_rows<float>(f, N, per, padded_count(per, 4))), "upload Kronecker factors");
         HO2D_CUDA(upload(d.kron_x, xi), "upload Kronecker exact-block index");
-        HO2D_CUDA(upload(d.kron_exact, padded_rows<float>(ex, ex.size() / K4, K4, padded_count(K4, 4))),
-                  "upload Kronecker exact blocks");
+        DeviceBuffer drows;
+        HO2D_CUDA(upload(drows, rows.empty() ? std::vector<int>{0} : rows), "upload exact rows");
+        HO2D_CUDA(d.kron_exact.alloc(((size_t)rows.size() * s4 + 1) * sizeof(float)), "alloc Kronecker exact blocks");
+        HO2D_CUDA(cudaMemsetAsync(d.kron_exact.get(), 0, d.kron_exact.bytes(), d.stream), "memset");
+        HO2D_CUDA(rows_to_f32(d.dinv64.as<double>(), s8, drows.as<int>(), d.kron_exact.as<float>(), s4,
+                              (int)rows.size(), K4, d.stream),
+                  "Kronecker exact blocks");
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "Kronecker exact blocks");
     }
-    HO2D_CUDA(upload_as<float>(d.rowsum32, op_.rowsum), "upload fp32 block row sums");
+    HO2D_CUDA(d.rowsum32.alloc((size_t)N * 5 * K2 * sizeof(float)), "alloc fp32 block row sums");
+    HO2D_CUDA(rows_to_f32(d.rowsum64.as<double>(), K2, nullptr, d.rowsum32.as<float>(), K2, N * 5, K2, d.stream),
+              "fp32 block row sums");
     for (int a = 0; a < 8; ++a) HO2D_CUDA(upload_as<float>(d.pg32[a], d.pg_host[a]), "upload fp32 operator data");
     // the FP32 smoother (exact, BF16 or Kronecker-sum) applied to the block row sums
     HO2D_CUDA(krylov_make_w<float>(make_op<float>(d, mesh_, K, true), d.W32.as<float>(), d.scalars.as<KrylovScalars>(),

@@ -125,6 +125,13 @@ class Solver {
     // in BF16, 2 Kronecker-sum factors with exact blocks where the fit is poor; -1 = from the
     // environment (HO2D_SMOOTHER_KRON=1, HO2D_SMOOTHER_BF16=1). Takes effect at setup.
     Error set_smoother(int kind);
+    // where the Poisson operator is assembled and its diagonal blocks inverted: on the
+    // device (true, the default) or on the host (false, or HO2D_HOST_SETUP=1); both give the
+    // same bits. Takes effect at setup.
+    void set_device_setup(bool on) { device_setup_req_ = on ? 1 : 0; }
+    bool device_setup() const { return device_setup_; }
+    // one assembled array (ho2d_get_poisson_setup's which), len values into out
+    Error get_poisson_setup(int which, int64_t len, double* out);
     int smoother() const { return smoother_kind_; }
     int smoother_exact_blocks() const { return smoother_exact_; }
     int last_poisson_iterations() const { return last_iters_; }
@@ -146,6 +153,8 @@ class Solver {
     Error poisson_solve();
     Error vtk_job(int indx, int subidx, const std::string& dir, VtkQueue::Job& j);  // output.cu
     Error queue_vtk(int indx, const std::string& dir);
+    Error vtk_device_tables();                  // output_device.cu
+    Error vtk_nodes_device(VtkQueue::Job& j);   // node averages and sample values on the device
     template <typename T>
     Error stage_t(double coeff, int rk_stage, bool update, bool solve = true);
     template <typename T>
@@ -153,6 +162,8 @@ class Solver {
     template <typename T>
     Error update_bcs(double t, bool into_stage);
     Error setup_from_mesh();
+    Error assemble_device(std::vector<double>* diag_out);  // setup_device.cu
+    Error ensure_host_colsum();  // block column sums on the host (the adjoint's coarse problem)
     Error hybrid_upload();
     Error upload_precision_arrays();
     Error setup_preconditioner();
@@ -192,6 +203,8 @@ class Solver {
     int smoother_req_ = -1;                   // requested smoother kind (-1: environment)
     int smoother_kind_ = 0;                   // kind in use since the last setup
     int smoother_exact_ = 0;                  // kind 2: elements that keep their exact block
+    int device_setup_req_ = -1;               // requested setup place (-1: environment)
+    bool device_setup_ = true;                // Poisson assembly on the device since the last setup
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

@@ -52,6 +52,15 @@ struct SolveGraph {
     ~SolveGraph() { reset(); }
 };
 
+// Device tables and scratch of the VTK node values (output_device.cu), built at the first
+// dump after a setup.
+struct VtkDevice {
+    bool ready = false;
+    int nbel = 0, nn = 0;
+    DeviceBuffer sgb, t2f, nodes, node_xy, be_el, be_side, bases, bptr, bedges, nptr, nslot, sel, shape;
+    DeviceBuffer om, ps, vx, vy, cvx, cvy, avg, samp, u64, v64;
+};
+
 struct DeviceState {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -75,6 +84,8 @@ struct DeviceState {
     // Poisson operator and Krylov workspace
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
     DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;
+    DeviceBuffer colsum64;  // block column sums (device assembly only)
+    VtkDevice vtk;
     DeviceBuffer W64, W32, zf;  // smoother applied to the block row sums; fine part of z
     DeviceBuffer ue5, u0dst;  // level-0 coarse values per element slot, and where each goes
     DeviceBuffer dinv_bf16;  // BF16 copy of dinv for the FP32 smoother (HO2D_SMOOTHER_BF16=1)

@@ -243,6 +243,21 @@ class HO_2D:
         self._check(self._lib.ho2d_get_smoother(self._h, ctypes.byref(k), ctypes.byref(n)))
         return k.value, n.value
 
+    def set_device_setup(self, on: bool) -> None:
+        """Assemble the Poisson operator on the device (True, the default) or the host, at the
+        next setup."""
+        self._check(self._lib.ho2d_set_device_setup(self._h, 1 if on else 0))
+
+    def get_poisson_setup(self, which: int) -> np.ndarray:
+        """One assembled Poisson array (capi.SETUP_*), shaped as ho2d.h describes it."""
+        N, K, neb = self.N_el, self.Knod, self.N_edges_boundary
+        K2 = K * K
+        shape = {capi.SETUP_DINV: (N, K2, K2), capi.SETUP_ROWSUM: (N, 5, K2), capi.SETUP_COLSUM: (N, 5, K2),
+                 capi.SETUP_BSUM: (N, 5), capi.SETUP_BSRC: (neb, K2, K), capi.SETUP_BCOL: (N, 5)}[which]
+        out = np.zeros(shape)
+        self._check(self._lib.ho2d_get_poisson_setup(self._h, int(which), out.size, capi.dptr(out)))
+        return out
+
     def set_poisson_tolerance(self, rel_tol: float, max_iter: int) -> None:
         self._check(self._lib.ho2d_set_poisson_tolerance(self._h, float(rel_tol), int(max_iter)))
 

@@ -32,11 +32,16 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+NO_FMAD = {"setup_device.cu", "output_device.cu"}
+
+
 def _flags(src: str) -> list[str]:
     common = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC,-fopenmp", "-I", CSRC,
               "-I", os.path.join(REPO, "include")]
     if src.endswith(".cu"):
-        return common + ["--expt-relaxed-constexpr", "-Xptxas", "-O3"]
+        # the device setup reproduces the host assembly bit for bit: no contraction to FMA
+        extra = ["-fmad=false"] if os.path.basename(src) in NO_FMAD else []
+        return common + ["--expt-relaxed-constexpr", "-Xptxas", "-O3"] + extra
     return common + ["-x", "c++"]
 
 

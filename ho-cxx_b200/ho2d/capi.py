@@ -18,6 +18,7 @@ STATUS = {0: "HO2D_OK", 1: "HO2D_ERR_ARG", 2: "HO2D_ERR_IO", 3: "HO2D_ERR_MESH",
 FP64, MIXED, MIXED_KRYLOV = 0, 1, 2
 BC_POISSON, BC_NORMAL_VEL, BC_PARL_VEL, BC_DIFFUSION, BC_VORTICITY, BC_VELOCITY_JUMP, BC_ADVECTION = range(7)
 SMOOTHER_BLOCKS, SMOOTHER_BF16, SMOOTHER_KRON = range(3)
+SETUP_DINV, SETUP_ROWSUM, SETUP_COLSUM, SETUP_BSUM, SETUP_BSRC, SETUP_BCOL = range(6)
 FIELD_VORTICITY, FIELD_STREAMFUNCTION, FIELD_RHS_DIFFUSIVE, FIELD_RHS_ADVECTIVE, FIELD_STAGE_K, FIELD_JACOBIAN = range(6)
 
 # exported symbol -> (restype, argtypes); every name declared in include/ho2d.h
@@ -47,6 +48,8 @@ SIGNATURES = {
     "ho2d_set_precision": (ctypes.c_int, [_P, _I]),
     "ho2d_set_smoother": (ctypes.c_int, [_P, _I]),
     "ho2d_get_smoother": (ctypes.c_int, [_P, _IP, _IP]),
+    "ho2d_set_device_setup": (ctypes.c_int, [_P, _I]),
+    "ho2d_get_poisson_setup": (ctypes.c_int, [_P, _I, ctypes.c_int64, _DP]),
     "ho2d_set_poisson_tolerance": (ctypes.c_int, [_P, _D, _I]),
     "ho2d_poisson_stats": (ctypes.c_int, [_P, _IP, _DP]),
     "ho2d_get_time": (ctypes.c_int, [_P, _DP, _DP]),

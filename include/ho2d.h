@@ -145,6 +145,30 @@ int ho2d_set_smoother(ho2d_solver* handle, int32_t kind);
 /* The smoother in use since the last ho2d_setup and, for HO2D_SMOOTHER_KRON, how many
  * elements keep their exact inverse block (0 otherwise). */
 int ho2d_get_smoother(ho2d_solver* handle, int32_t* kind, int32_t* exact_blocks);
+/* Where the next ho2d_setup assembles the Poisson operator (src/HO_2D.cpp:1533-1804),
+ * inverts its diagonal blocks and the coarsest level's dense matrix: 1 = on the device
+ * (the default), 0 = on the host (also HO2D_HOST_SETUP=1 in the environment). Both give
+ * the same bits for the assembled arrays. No counterpart in the reference. */
+int ho2d_set_device_setup(ho2d_solver* handle, int32_t on);
+/* One array of the assembled Poisson operator after ho2d_setup, as doubles:
+ * HO2D_SETUP_DINV   inverse diagonal blocks [N_el][K^2 (rs)][K^2 (ij)] (the inverse's
+ *                   transpose, the layout the smoother reads);
+ * HO2D_SETUP_ROWSUM sums over rs of each block row [N_el][5][K^2] (slot 0 = the element,
+ *                   1..4 = its neighbour across face ijp 0..3, zero for boundary faces);
+ * HO2D_SETUP_COLSUM sums over ij of each block column [N_el][5][K^2];
+ * HO2D_SETUP_BSUM   each block's entry sum [N_el][5];
+ * HO2D_SETUP_BSRC   the boundary source [N_eb][K^2][K] (src/HO_2D.cpp:1640-1714);
+ * HO2D_SETUP_BCOL   each slot's column element (-1 = none) [N_el][5].
+ * len must equal the array's length. */
+enum ho2d_setup_array {
+    HO2D_SETUP_DINV = 0,
+    HO2D_SETUP_ROWSUM = 1,
+    HO2D_SETUP_COLSUM = 2,
+    HO2D_SETUP_BSUM = 3,
+    HO2D_SETUP_BSRC = 4,
+    HO2D_SETUP_BCOL = 5
+};
+int ho2d_get_poisson_setup(ho2d_solver* handle, int32_t which, int64_t len, double* buf);
 /* Poisson solve controls: relative tolerance on ||b - A psi|| / ||b|| (default 1e-12)
  * and iteration cap (default 500). */
 int ho2d_set_poisson_tolerance(ho2d_solver* handle, double rel_tol, int32_t max_iter);

@@ -255,3 +255,40 @@ def test_sample_points_of_the_shipped_cavity(tmp_path, vtk_harness):
     assert len(open(ours / names[0]).read().split()) == 5 * 14  # 14 points, 5 values each
     for vtk in (f"problem{ptype}_K{knod}_00002.vtk", f"vorticity{ptype}_K{knod}_00002.vtk"):  # 9-node quads
         compare_vtk(str(ours / vtk), str(d / vtk))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cavq3_rk4", "bfs2_rk4", "cyl4x8_rk4"])
+def test_device_node_values_write_the_host_files(tmp_path, case, monkeypatch):
+    """The smooth file's node averages and sample values made on the device (the default)
+    give byte-identical files to the host writer's (HO2D_HOST_OUTPUT=1), sample points
+    included; the vorticity file is written from the same fields either way."""
+    from ho2d import HO_2D
+
+    d = tmp_path / "case"
+    shutil.copytree(os.path.join(GOLDEN, case), d)
+    lines = open(d / "input.dat").read().split("\n")
+    idx = next(i for i, ln in enumerate(lines) if ln.startswith("sample_points file"))
+    lines[idx + 1] = "samples.dat"
+    open(d / "input.dat", "w").write("\n".join(lines))
+    rng = np.random.Generator(np.random.PCG64(9))
+    pts = rng.uniform(-0.2, 1.2, size=(12, 2))  # some outside the domain: the nearest-node fallback
+    np.savetxt(d / "samples.dat", pts)
+    out = {}
+    for host in ("0", "1"):
+        monkeypatch.setenv("HO2D_HOST_OUTPUT", host)
+        o = tmp_path / f"out{host}"
+        o.mkdir()
+        s = HO_2D()
+        s.read_input_file(str(d / "input.dat"))
+        s.setup()
+        s.set_output_dir(str(o))
+        s.solve_vorticity_streamfunction()
+        s.trigger_write(99, 1, str(o))
+        s.close()
+        out[host] = o
+    names = sorted(os.listdir(out["0"]))
+    assert names == sorted(os.listdir(out["1"]))
+    assert any(n.startswith("sampling_points") for n in names) and any(n.startswith("problem") for n in names)
+    for n in names:
+        assert open(out["0"] / n, "rb").read() == open(out["1"] / n, "rb").read(), n
