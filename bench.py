@@ -7,12 +7,13 @@ the stated shape (no dataset is involved). Each rank is an independent replica (
 has no data-path collective); `value` sums DOF updates over ranks and divides by the
 slowest rank's device time.
 
-The headline precision is HO2D_MIXED_KRYLOV: FP64 FR stage and RK update, FP32 BiCGSTAB
-with the FP32 preconditioner inside FP64 iterative refinement of the Poisson solve (the
-device-resident refinement loop). The FP64 plain path (every array and operation in
-FP64, exact FP64 inverse blocks) is timed on the same workload under "fp64", and the
-all-FP32-stage mode (HO2D_MIXED) under "mixed_fp32_stage", each with its relative L2
-vorticity difference from FP64 after the same steps and after --l2-steps steps.
+The headline precision is HO2D_MIXED: the FR stage kernels in FP32 (velocity from the FP64
+streamfunction, RK accumulation in FP64) and FP32 BiCGSTAB with the FP32 preconditioner
+inside FP64 iterative refinement of the Poisson solve (the device-resident refinement
+loop). The FP64 plain path (every array and operation in FP64, exact FP64 inverse blocks)
+is timed on the same workload under "fp64", and HO2D_MIXED_KRYLOV (FP64 FR stage, the same
+mixed Poisson solve) under "mixed_fp64_stage", each with its relative L2 vorticity
+difference from FP64 after the same steps and after --l2-steps steps.
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -52,7 +53,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="cyl256x512")
     ap.add_argument("--knod", type=int, default=None, help="K = P + 1 (default 6 for cylinders, 5 for the step)")
-    ap.add_argument("--smoother", default="bf16", choices=sorted(SMOOTHERS),
+    ap.add_argument("--smoother", default="kron", choices=sorted(SMOOTHERS),
                     help="smoother of the FP32 preconditioner in the mixed modes")
     ap.add_argument("--t0", type=float, default=None, help="start time (default 1.5 for the step's pulsatile inlet)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -74,9 +75,14 @@ def parse():
     ap.add_argument("--large-n", type=int, default=512)
     ap.add_argument("--large-steps", type=int, default=200)
     ap.add_argument("--strouhal", action="store_true",
-                    help="vortex shedding behind the cylinder (problem type 3, Re=100, 48x96 O-grid, K=4): "
+                    help="vortex shedding behind the cylinder (problem type 3, Re=100, 48x96 O-grid to the box "
+                         "[-15, 15]^2, K=4): "
                          "Strouhal number, mean drag and lift amplitude in FP64 and mixed, and their differences")
-    ap.add_argument("--t-end", type=float, default=80.0, help="time units simulated for --strouhal")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="one solver of the headline precision on --case: --warmup steps, then --steps graph-free "
+                         "BiCGSTAB iterations with per-kernel CUDA-event times (the command of the ncu captures "
+                         "summarised in profiles/)")
+    ap.add_argument("--t-end", type=float, default=120.0, help="time units simulated for --strouhal")
     ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
     a = ap.parse_args()
     if a.knod is None:
@@ -331,17 +337,19 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def step_bytes(prof, iters_per_step, sweeps_per_step, solves_per_step, dof, knod, n_el, mixed):
+def step_bytes(prof, iters_per_step, sweeps_per_step, solves_per_step, dof, knod, n_el, mixed, stage32=False):
     """Algorithmic bytes of one time step: the Krylov iterations (two smoothing steps, two
     operator applications, the x/r update and two coarse cycles each), the per-sweep FP64
-    residual and FP32 restart of the mixed modes (or the FP64 initial residual), and the FP64
-    stage kernels."""
+    residual and FP32 restart of the mixed modes (or the FP64 initial residual), and the
+    stage kernels: FP64, or with FP32 stage arrays (stage32) the FP64 count scaled by 0.58 --
+    of the ~24 eight-byte values a stage moves per DOF, the streamfunction, the vorticity,
+    the stage-start vorticity and the RK accumulator stay FP64 and the rest become FP32."""
     it = (2 * prof["smoother"][1] + 2 * prof["smoother_combine"][1] + 2 * prof["operator"][1] + prof["xr_update"][1]
           + 2 * prof["coarse_cycle"][1])
     op64 = n_el * ((6 * knod * knod + 24 * knod) * 8 + 24)  # one FP64 operator launch
     per_sweep = (op64 + prof["operator"][1] + 4 * dof * 4) if mixed else 0.0
     per_solve = op64 if not mixed else 0.0
-    stage = STAGE_BYTES_PER_DOF_UPDATE.get(knod, 775) * dof
+    stage = STAGE_BYTES_PER_DOF_UPDATE.get(knod, 775) * dof * (0.58 if stage32 else 1.0)
     return iters_per_step * it + sweeps_per_step * per_sweep + solves_per_step * per_solve + stage
 
 
@@ -376,13 +384,13 @@ def secondary_workloads(args, tmp):
     out = {}
     inp = meshgen.make_case("bfs", os.path.join(tmp, "bfs"), knod=5, steps=10)
     sv = {m: make_solver(inp, mode, SMOOTHERS[args.smoother], 1.5)
-          for m, mode in (("fp64", ho2d.FP64), ("mixed", ho2d.MIXED_KRYLOV), ("mixed_fp32_stage", ho2d.MIXED))}
+          for m, mode in (("fp64", ho2d.FP64), ("mixed", ho2d.MIXED), ("mixed_fp64_stage", ho2d.MIXED_KRYLOV))}
     for s in sv.values():
         s.solve_advection_diffusion(1000)
     wf = sv["fp64"].get_vorticity()
     out["bfs14625_k5_l2_after_1000_steps"] = {"workload": workload_name("bfs", 5, 1.5),
                                               "mixed": rel_l2(sv["mixed"].get_vorticity(), wf),
-                                              "mixed_fp32_stage": rel_l2(sv["mixed_fp32_stage"].get_vorticity(), wf)}
+                                              "mixed_fp64_stage": rel_l2(sv["mixed_fp64_stage"].get_vorticity(), wf)}
     del sv
     from ho2d.adjoint_case import cavity_dt
 
@@ -390,7 +398,7 @@ def secondary_workloads(args, tmp):
     inp = meshgen.make_case("cavityj512", os.path.join(tmp, "cav512"), knod=7, steps=10, dt=dt, reyn=5000.0,
                             jitter=0.1, seed=5)
     res = {}
-    for m, mode in (("mixed", ho2d.MIXED_KRYLOV), ("fp64", ho2d.FP64)):
+    for m, mode in (("mixed", ho2d.MIXED), ("fp64", ho2d.FP64)):
         s = make_solver(inp, mode, SMOOTHERS[args.smoother], 0.0)
         s.set_vorticity(meshgen.sine_spectrum(s.getsolnpts_d(), seed=3))
         s.solve_advection_diffusion(2)
@@ -416,7 +424,7 @@ def run_ours(args, rank, world, local, phys):
     with tempfile.TemporaryDirectory() as tmp:
         inp = meshgen.make_case(args.case, tmp, knod=args.knod, steps=args.steps)
         sm = SMOOTHERS[args.smoother]
-        modes = {"mixed": ho2d.MIXED_KRYLOV, "fp64": ho2d.FP64, "mixed_fp32_stage": ho2d.MIXED}
+        modes = {"mixed": ho2d.MIXED, "fp64": ho2d.FP64, "mixed_fp64_stage": ho2d.MIXED_KRYLOV}
         solvers = {m: make_solver(inp, mode, sm, args.t0) for m, mode in modes.items()}
         s0 = solvers["mixed"]
         n_el, knod = s0.N_el, s0.Knod
@@ -461,16 +469,17 @@ def run_ours(args, rank, world, local, phys):
                 s_.solve_advection_diffusion(args.l2_steps - done)
             wf = solvers["fp64"].get_vorticity()
             l2_long = {"steps": args.l2_steps, "mixed": rel_l2(solvers["mixed"].get_vorticity(), wf),
-                       "mixed_fp32_stage": rel_l2(solvers["mixed_fp32_stage"].get_vorticity(), wf),
+                       "mixed_fp64_stage": rel_l2(solvers["mixed_fp64_stage"].get_vorticity(), wf),
                        "note": "mixed restarted from its own state after the e2e steps, at the FP64 run's time"}
         del solvers, s
         peak, peak_kind = measured_peaks()
         m, f = results["mixed"], results["fp64"]
-        # roofline of the kernel with the largest share of an iteration's device time
+        # roofline of the kernel with the largest share of an iteration's main-stream time (the
+        # coarse cycle runs on a second stream beside the fine smoothing, in the timed solves)
         launches_per_it = {"smoother": 2, "smoother_combine": 2, "operator": 2, "xr_update": 1, "coarse_cycle": 2}
         pm = prof["mixed"]
         share = {k: pm[k][0] * n for k, n in launches_per_it.items()}
-        top = max(share, key=share.get)
+        top = max((k for k in share if k != "coarse_cycle"), key=share.get)
         names = {"smoother": "k_post_a", "smoother_combine": "k_post_b", "operator": "k_mf_v/k_mf_t",
                  "xr_update": "k_xr_update",
                  "coarse_cycle": "coarse cycle (k_coarse_rows_f0, k_coarse_rows, k_dense_gemv16, k_coarse_up0)"}
@@ -490,7 +499,7 @@ def run_ours(args, rank, world, local, phys):
                                     "frac": v[1] / (v[0] * 1e-3) / 1e9 / peak} for k, v in pm.items()}}
         for key, r_, mixed in (("mixed", m, True), ("fp64", f, False)):
             sb = step_bytes(prof[key], r_["iters_per_step"], r_["sweeps_per_step"], r_["solves_per_step"], n_dof,
-                            knod, n_el, mixed)
+                            knod, n_el, mixed, stage32=mixed)
             r_["step_level"] = {"algorithmic_bytes_per_step": sb,
                                 "achieved_gbs": sb / (r_["ms_per_step"] * 1e-3) / 1e9,
                                 "frac": sb / (r_["ms_per_step"] * 1e-3) / 1e9 / peak}
@@ -520,14 +529,15 @@ def run_ours(args, rank, world, local, phys):
                                "poisson_tol": 1e-12, "t0": args.t0, "omega0": 0.0,
                                "smoother": args.smoother},
                     "poisson_ms_per_step": m["poisson_ms_per_step"],
-                    "precision": "HO2D_MIXED_KRYLOV: FP64 FR stage and RK update, FP32 BiCGSTAB with FP32 "
-                                 f"preconditioner ({args.smoother} smoother) inside FP64 iterative refinement of the "
-                                 "Poisson solve, refinement loop on the device",
+                    "precision": "HO2D_MIXED: FR stage kernels in FP32 (velocity from the FP64 streamfunction, "
+                                 "RK accumulation in FP64), FP32 BiCGSTAB with FP32 preconditioner "
+                                 f"({args.smoother} smoother) inside FP64 iterative refinement of the Poisson solve, "
+                                 "refinement loop on the device",
                     "mixed": mode_out(m),
                     "fp64": mode_out(f) | {"kernels": roofline_fp64},
-                    "mixed_fp32_stage": mode_out(results["mixed_fp32_stage"]) | {
-                        "precision": "HO2D_MIXED: FR stage also in FP32 (velocity from FP64 psi)",
-                        "l2_rel_vorticity_vs_fp64": rel_l2(w["mixed_fp32_stage"], w["fp64"])},
+                    "mixed_fp64_stage": mode_out(results["mixed_fp64_stage"]) | {
+                        "precision": "HO2D_MIXED_KRYLOV: FR stage in FP64, the same mixed Poisson solve",
+                        "l2_rel_vorticity_vs_fp64": rel_l2(w["mixed_fp64_stage"], w["fp64"])},
                     "mixed_over_fp64": m["value"] / f["value"],
                     "l2_rel_vorticity_mixed_vs_fp64": rel_l2(w["mixed"], w["fp64"]),
                     "l2_after_steps": args.warmup + args.steps,
@@ -537,6 +547,26 @@ def run_ours(args, rank, world, local, phys):
                     "cpu_baseline": cb, "secondary": secondary}
             print(json.dumps(line))
     dist.close()
+
+
+def run_profile(args, rank):
+    """The headline solver alone on --case: --warmup time steps (CUDA graphs), then --steps
+    BiCGSTAB iterations launched in order without a graph, timed per kernel with CUDA events
+    (Solver::profile_krylov). Kernels inside CUDA graphs with conditional nodes are not
+    visible to ncu; these in-order iterations run the same kernels on the same state."""
+    if rank != 0:
+        return
+    import ho2d
+    from ho2d import meshgen
+
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = meshgen.make_case(args.case, tmp, knod=args.knod, steps=args.warmup)
+        s = make_solver(inp, ho2d.MIXED, SMOOTHERS[args.smoother], args.t0)
+        s.solve_advection_diffusion(args.warmup)
+        prof = s.profile_krylov(max(1, args.steps))
+        print(json.dumps({"profile": "BiCGSTAB iterations in order, no graph", "case": args.case,
+                          "knod": s.Knod, "n_el": s.N_el, "smoother": args.smoother, "iterations": args.steps,
+                          "kernels": {k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()}}))
 
 
 def run_adjoint(args, rank):
@@ -592,7 +622,7 @@ def main():
             print(json.dumps({"metric": "Strouhal number of the cylinder wake (lift frequency x D / U)",
                               "value": r["fp64"]["St"], "unit": "St", "higher_is_better": None, "n_gpus": 1,
                               "dtype": "f64", "data": "synthetic (generated O-grid; Gaussian-vortex start)",
-                              "config": {"workload": "cylinder wake, Re=100, O-grid r in [0.5, 15], "
+                              "config": {"workload": "cylinder wake, Re=100, O-grid from r=0.5 to the box [-15, 15]^2, "
                                                      f"t_end={args.t_end}", **r["case"]},
                               "fp64": r["fp64"], "mixed": r["mixed"], "difference": r["difference"]}))
         return
@@ -603,6 +633,9 @@ def main():
     os.environ["CUDA_VISIBLE_DEVICES"] = phys
     if args.adjoint:
         run_adjoint(args, rank)
+        return
+    if args.profile_solve:
+        run_profile(args, rank)
         return
     run_ours(args, rank, world, local, phys)
 

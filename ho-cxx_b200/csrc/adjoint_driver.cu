@@ -324,16 +324,17 @@ Error Solver::stage_adjoint_dev(double coeff, double* out) {
 }
 
 // Advection types 1 and 2 (residual_adjoint_continuous for type 2); both are checked on the
-// host and on the GPU against complex-step derivatives of the oracle.
-static Error adjoint_supported(const Input& in, bool stage32) {
+// host and on the GPU against complex-step derivatives of the oracle. Every precision: with
+// the FP32 stage (HO2D_MIXED) the forward sweep and the segment recomputation follow the
+// mixed trajectory, and each stage is linearised in FP64 at its states.
+static Error adjoint_supported(const Input& in) {
     if (in.adv_type != 1 && in.adv_type != 2) return {4, "the adjoint covers advection types 1 and 2"};
     if (in.problem_type == 11) return {4, "the adjoint does not cover hybrid runs (problem type 11)"};
-    if (stage32) return {4, "the adjoint needs the FP64 stage: precision HO2D_FP64 or HO2D_MIXED_KRYLOV"};
     return {0, ""};
 }
 
 Error Solver::stage_adjoint(double coeff, const double* lam_k, double* lam_w, double* lam_pv) {
-    HO2D_TRY(adjoint_supported(in_, stage32_));
+    HO2D_TRY(adjoint_supported(in_));
     HO2D_TRY(adjoint_prepare());
     DeviceState& d = *d_;
     AdjointState& a = *adj_;
@@ -387,7 +388,7 @@ Error Solver::load_state(double* dst, const void* src) {
 
 Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     const NvtxRange nvtx_range("ho2d.adjoint_forward");
-    HO2D_TRY(adjoint_supported(in_, stage32_));
+    HO2D_TRY(adjoint_supported(in_));
     if (nsteps < 0 || ckpt_every < 1) return {1, "adjoint_forward needs nsteps >= 0 and ckpt_every >= 1"};
     HO2D_TRY(adjoint_prepare());
     DeviceState& d = *d_;
@@ -424,7 +425,7 @@ Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
 
 Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* grad_pv) {
     const NvtxRange nvtx_range("ho2d.adjoint_backward");
-    HO2D_TRY(adjoint_supported(in_, stage32_));
+    HO2D_TRY(adjoint_supported(in_));
     if (!adj_ || adj_->nsteps < 0) return {1, "ho2d_adjoint_backward needs a completed ho2d_adjoint_forward"};
     HO2D_TRY(adjoint_prepare());
     DeviceState& d = *d_;

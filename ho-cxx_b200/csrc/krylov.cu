@@ -591,8 +591,10 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_make_w(MfOp<T> op, T* __re
 }
 
 // v = A ph; alpha = rho / (rhat, v); element sums of v
+// (FP32: at most 128 registers, four CTAs per SM)
 template <int K, typename T>
-__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
+__global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
+    k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
     // the flag is uniform over the grid (only this kernel's last CTA writes it, after every
     // CTA has read it)
@@ -623,7 +625,11 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVecto
     // push the operator past the register file)
     if constexpr (sizeof(T) == 4) {
 #pragma unroll 1
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (tile + (int)gridDim.x < ntiles)
+                prefetch_apply_rows<K, T>(op.g, v.ph, v.tv, v.tg, v.rhat, tile + gridDim.x);
+            tile_body(tile);
+        }
     } else {
         if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }
@@ -639,8 +645,10 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_v(MfOp<T> op, BicgVecto
 }
 
 // t = A sh; omega = (t, s) / (t, t)
+// (FP32: at most 128 registers, four CTAs per SM)
 template <int K, typename T>
-__global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
+__global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
+    k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
     if (sc->done || sc->s_exit) return;  // uniform
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
@@ -666,7 +674,11 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_t(MfOp<T> op, BicgVecto
     // push the operator past the register file)
     if constexpr (sizeof(T) == 4) {
 #pragma unroll 1
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) tile_body(tile);
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (tile + (int)gridDim.x < ntiles)
+                prefetch_apply_rows<K, T>(op.g, v.sh, v.tv, v.tg, v.s, tile + gridDim.x);
+            tile_body(tile);
+        }
     } else {
         if ((int)blockIdx.x < ntiles) tile_body(blockIdx.x);
     }

@@ -42,6 +42,32 @@ struct RowIdx {
     }
 };
 
+// Non-binding prefetch of one address's line into L2 (PTX prefetch.global.L2).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// The lines an operator tile will read for this thread's row (operand row, the three metric
+// rows, the face point's coefficients and incoming traces, and the row of the dot product's
+// second vector), prefetched into L2 one tile ahead so that the tile's loads do not wait on
+// DRAM.
+template <int K, typename T>
+__device__ __forceinline__ void prefetch_apply_rows(const PoisGeom<T>& g, const T* x, const T* tvin, const T* tgin,
+                                                    const T* second, int tile) {
+    const RowIdx<K> ix(g.N, tile);
+    if (!ix.active) return;
+    const size_t r = (size_t)ix.el * K * K + ix.t * K, q4 = ((size_t)ix.el * K + ix.t) * 4;
+    prefetch_l2(x + r);
+    prefetch_l2(g.G11 + r);
+    prefetch_l2(g.G12 + r);
+    prefetch_l2(g.G22 + r);
+    prefetch_l2(second + r);
+    prefetch_l2(g.fa + q4);
+    prefetch_l2(g.fb + q4);
+    prefetch_l2(g.nfa + q4);
+    prefetch_l2(g.nfb + q4);
+    prefetch_l2(tvin + q4);
+    prefetch_l2(tgin + q4);
+}
+
 // Per-warp shared scratch of the operator: the common values of the four faces, the
 // Neumann right-hand sides and two K x K transpose buffers for each element of the warp.
 template <int K, typename T>

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "assemble_element.hpp"
+#include "kron_fit.hpp"
 #include "device.cuh"
 #include "fr_launch.hpp"
 #include "host_amg.hpp"
@@ -60,6 +61,36 @@ __global__ void __launch_bounds__(128) k_assemble(int el0, int n, AsmBases B, As
     for (int ij = 0; ij < K2; ++ij)
         for (int rs = 0; rs < K2; ++rs) di[rs * K2 + ij] = sc.Lc[(long long)ij * K2 + rs];
     atomicAdd(nnz, (unsigned long long)cnt);
+}
+
+// ---------------------------------------------------------------- Kronecker-sum fit
+// One thread per element: the fit of its filtered diagonal block (diag [N][K4]) and its
+// defect ||I - M D||_2 (E: K4 interleaved scratch); the FP32 factors [vx vxi vy vyi lx ly]
+// of a kept fit at el * fstride, zeros and exact[el] = 1 where the exact block stays.
+__global__ void __launch_bounds__(128) k_kron_fit(int el0, int n, int K, const double* __restrict__ diag,
+                                                  double* __restrict__ scratch, float* __restrict__ factors,
+                                                  long long fstride, unsigned char* __restrict__ exact) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int el = el0 + t, K2 = K * K, K4 = K2 * K2, per = 4 * K2 + 2 * K;
+    const Str<double> D{const_cast<double*>(diag) + (size_t)el * K4, 1};
+    KronFitHD f;
+    const bool ok = kf_fit(K, D, f);
+    const double defect = ok ? kf_defect(f, D, Str<double>{scratch + t, n}) : 0.0;
+    const bool ex = !ok || !(defect <= kKronDefectMax);
+    exact[el] = ex ? 1 : 0;
+    float* fo = factors + (size_t)el * fstride;
+    if (ex) {
+        for (int i = 0; i < per; ++i) fo[i] = 0.f;
+        return;
+    }
+    const double* src[4] = {f.vx, f.vxi, f.vy, f.vyi};
+    for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < K2; ++i) fo[a * K2 + i] = (float)src[a][i];
+    for (int i = 0; i < K; ++i) {
+        fo[4 * K2 + i] = (float)f.lx[i];
+        fo[4 * K2 + K + i] = (float)f.ly[i];
+    }
 }
 
 // ---------------------------------------------------------------- dense Gauss-Jordan
@@ -179,8 +210,9 @@ __global__ void k_rows_f32(const double* __restrict__ src, long long ss, const i
 }
 
 // BF16 of the FP32 rounding, to nearest with ties to even (finite values)
-__global__ void k_rows_bf16(const double* __restrict__ src, long long ss, unsigned short* __restrict__ dst,
-                            long long ds, int rows, int cols) {
+template <typename S>
+__global__ void k_rows_bf16(const S* __restrict__ src, long long ss, unsigned short* __restrict__ dst, long long ds,
+                            int rows, int cols) {
     const size_t total = (size_t)rows * cols;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
         const size_t r = q / cols, c = q % cols;
@@ -204,7 +236,7 @@ cudaError_t rows_to_f32(const double* src, long long ss, const int* idx, float* 
 cudaError_t rows_to_bf16(const double* src, long long ss, unsigned short* dst, long long ds, int rows, int cols,
                          cudaStream_t s) {
     if (rows <= 0 || cols <= 0) return cudaSuccess;
-    k_rows_bf16<<<conv_grid((size_t)rows * cols), 256, 0, s>>>(src, ss, dst, ds, rows, cols);
+    k_rows_bf16<double><<<conv_grid((size_t)rows * cols), 256, 0, s>>>(src, ss, dst, ds, rows, cols);
     return cudaGetLastError();
 }
 
@@ -238,9 +270,10 @@ cudaError_t dense_invert_device(double* a, int n, int w, cudaStream_t s, bool* s
 // Poisson assembly on the device into the solver's buffers: inverse diagonal blocks
 // (dinv64, padded rows), block row sums (rowsum64), column sums (colsum64), the boundary
 // source (bsrc) and the block columns (bcol); the block sums, block columns and entry count
-// come back to op_ for the coarse hierarchy. diag_out (optional) receives the filtered
-// diagonal blocks [N][K2][K2] for the Kronecker-sum fit.
-Error Solver::assemble_device(std::vector<double>* diag_out) {
+// come back to op_ for the coarse hierarchy. With kron_fit, the Kronecker-sum fit of every
+// filtered diagonal block runs on the device too: its FP32 factors go to kron_f and the
+// per-element exact-block flags to kron_ on the host.
+Error Solver::assemble_device(bool kron_fit) {
     DeviceState& d = *d_;
     const int N = mesh_.n_el, K = in_.knod, K2 = K * K, K4 = K2 * K2, neb = mesh_.n_eb;
     op_ = PoissonOperator();
@@ -285,7 +318,7 @@ Error Solver::assemble_device(std::vector<double>* diag_out) {
     HO2D_CUDA(dbsum.alloc((size_t)N * 5 * sizeof(double)), "alloc block sums");
     HO2D_CUDA(dnnz.alloc(sizeof(unsigned long long)), "alloc");
     HO2D_CUDA(cudaMemsetAsync(dnnz.get(), 0, sizeof(unsigned long long), d.stream), "memset");
-    if (diag_out) HO2D_CUDA(ddiag.alloc((size_t)N * K4 * sizeof(double)), "alloc diagonal blocks");
+    if (kron_fit) HO2D_CUDA(ddiag.alloc((size_t)N * K4 * sizeof(double)), "alloc diagonal blocks");
     const AsmOut ao{d.bsrc.as<double>(), d.rowsum64.as<double>(), d.colsum64.as<double>(), dbsum.as<double>(), nullptr,
                     d.bcol.as<int>()};
     // chunks of at most ~2 GB of scratch, a multiple of the CTA size
@@ -296,7 +329,7 @@ Error Solver::assemble_device(std::vector<double>* diag_out) {
     for (int el0 = 0; el0 < N; el0 += chunk) {
         const int n = std::min(chunk, N - el0);
         k_assemble<<<(n + 127) / 128, 128, 0, d.stream>>>(el0, n, ab, tb, am, ao, d.dinv64.as<double>(), dstride,
-                                                          diag_out ? ddiag.as<double>() : nullptr,
+                                                          kron_fit ? ddiag.as<double>() : nullptr,
                                                           scratch.as<double>(), dnnz.as<unsigned long long>());
         HO2D_CUDA(cudaGetLastError(), "block assembly");
     }
@@ -311,10 +344,29 @@ Error Solver::assemble_device(std::vector<double>* diag_out) {
               "download block columns");
     HO2D_CUDA(cudaMemcpy(&nnz, dnnz.get(), sizeof(nnz), cudaMemcpyDeviceToHost), "download entry count");
     op_.nnz = (int64_t)nnz;
-    if (diag_out) {
-        diag_out->resize((size_t)N * K4);
-        HO2D_CUDA(cudaMemcpy(diag_out->data(), ddiag.get(), diag_out->size() * sizeof(double), cudaMemcpyDeviceToHost),
-                  "download diagonal blocks");
+    if (kron_fit) {
+        const int per = 4 * K2 + 2 * K;
+        const long long fstride = padded_count(per, 4);
+        HO2D_CUDA(d.kron_f.alloc(((size_t)N * fstride + 1) * sizeof(float)), "alloc Kronecker factors");
+        HO2D_CUDA(cudaMemsetAsync(d.kron_f.get(), 0, d.kron_f.bytes(), d.stream), "memset");
+        DeviceBuffer dex, kscr;
+        HO2D_CUDA(dex.alloc((size_t)N), "alloc exact flags");
+        int kchunk = (int)std::min<size_t>((size_t)N, std::max<size_t>(128, ((size_t)2 << 30) / ((size_t)K4 * 8)));
+        kchunk = (kchunk + 127) / 128 * 128;
+        HO2D_CUDA(kscr.alloc((size_t)kchunk * K4 * sizeof(double)), "alloc fit scratch");
+        for (int el0 = 0; el0 < N; el0 += kchunk) {
+            const int n = std::min(kchunk, N - el0);
+            k_kron_fit<<<(n + 127) / 128, 128, 0, d.stream>>>(el0, n, K, ddiag.as<double>(), kscr.as<double>(),
+                                                              d.kron_f.as<float>(), fstride, dex.as<unsigned char>());
+            HO2D_CUDA(cudaGetLastError(), "Kronecker-sum fit");
+        }
+        kron_ = KronSmoother();
+        kron_.K = K;
+        kron_.exact.resize(N);
+        // (the handle's stream does not synchronise with the legacy stream's copies)
+        HO2D_CUDA(cudaStreamSynchronize(d.stream), "Kronecker-sum fit");
+        HO2D_CUDA(cudaMemcpy(kron_.exact.data(), dex.get(), (size_t)N, cudaMemcpyDeviceToHost), "download exact flags");
+        kron_on_device_ = true;
     }
     return {0, ""};
 }

@@ -180,10 +180,10 @@ Error Solver::setup_from_mesh() {
     const int K4 = K2 * K2;
     d.vtk.ready = false;  // the VTK node tables follow the mesh
     d.colsum64.reset();
+    kron_on_device_ = false;
     if (device_setup_) {
-        std::vector<double> diag;
-        HO2D_TRY(assemble_device(smoother_kind_ == 2 ? &diag : nullptr));
-        if (smoother_kind_ == 2) kron_fit_blocks(K, N, diag.data(), kron_);
+        // kind 2: the Kronecker-sum fit on the device from the assembled diagonal blocks
+        HO2D_TRY(assemble_device(smoother_kind_ == 2));
     } else {
         HO2D_CUDA(upload(d.bsrc, op_.bsrc.empty() ? std::vector<double>{0.0} : op_.bsrc), "upload");
         HO2D_CUDA(upload(d.dinv64, padded_rows<double>(op_.dinv, N, K4, padded_count(K4, 8))), "upload block-Jacobi");
@@ -214,7 +214,8 @@ Error Solver::setup_from_mesh() {
     for (DeviceBuffer* b : {&d.ktv, &d.ktg, &d.kxtv, &d.kxtg}) HO2D_CUDA(upload(*b, zf), "alloc Krylov traces");
     d.dinv32.reset();
     d.dinv_bf16.reset();
-    for (DeviceBuffer* b : {&d.kron_f, &d.kron_x, &d.kron_exact}) b->reset();
+    for (DeviceBuffer* b : {&d.kron_x, &d.kron_exact}) b->reset();
+    if (!kron_on_device_) d.kron_f.reset();
     d.rowsum32.reset();
     for (auto& b : d.pg32) b.reset();
     HO2D_TRY(setup_preconditioner());
@@ -583,7 +584,9 @@ Error Solver::upload_precision_arrays() {
         for (int el = 0; el < N; ++el)
             if (xi[el] >= 0) rows.push_back(el);
         const int per = 4 * K2 + 2 * K;
-        HO2D_CUDA(upload(d.kron_f, padded_rows<float>(f, N, per, padded_count(per, 4))), "upload Kronecker factors");
+        if (!kron_on_device_)  // (the device fit wrote its factors in place)
+            HO2D_CUDA(upload(d.kron_f, padded_rows<float>(f, N, per, padded_count(per, 4))),
+                      "upload Kronecker factors");
         HO2D_CUDA(upload(d.kron_x, xi), "upload Kronecker exact-block index");
         DeviceBuffer drows;
         HO2D_CUDA(upload(drows, rows.empty() ? std::vector<int>{0} : rows), "upload exact rows");

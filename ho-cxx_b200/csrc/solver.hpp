@@ -162,7 +162,7 @@ class Solver {
     template <typename T>
     Error update_bcs(double t, bool into_stage);
     Error setup_from_mesh();
-    Error assemble_device(std::vector<double>* diag_out);  // setup_device.cu
+    Error assemble_device(bool kron_fit);  // setup_device.cu
     Error ensure_host_colsum();  // block column sums on the host (the adjoint's coarse problem)
     Error hybrid_upload();
     Error upload_precision_arrays();
@@ -205,6 +205,7 @@ class Solver {
     int smoother_exact_ = 0;                  // kind 2: elements that keep their exact block
     int device_setup_req_ = -1;               // requested setup place (-1: environment)
     bool device_setup_ = true;                // Poisson assembly on the device since the last setup
+    bool kron_on_device_ = false;             // the Kronecker-sum factors were fitted on the device
     // initial guess of each stage's Poisson solve: 0/1 = the last psi; 2, 3 = the same RK
     // stage of the last 2 or 3 steps extrapolated in time (HO2D_PSI_EXTRAP)
     int psi_extrap_ = 3;

@@ -162,12 +162,20 @@ def backward_facing_step(h: float = 1.0 / 15.0, jitter: float = 0.15, seed: int 
 
 
 def cylinder_ogrid(n_r: int = 256, n_theta: int = 512, r0: float = 0.5, r1: float = 20.0,
-                   stretch: float = 1.02) -> QuadMesh:
+                   stretch: float = 1.02, square: bool = False) -> QuadMesh:
     """O-grid around a cylinder: radial spacing dr_k = dr0 * stretch**k from r0 to r1.
 
     Names follow problem_type 3: ``object`` (r = r0), ``inlet`` (outer arc, edge
     midpoint x < 0) and ``outlet`` (outer arc, x >= 0).
+
+    With ``square`` the rings blend from the circle at r0 to the square of half-width r1
+    (weight ((r - r0) / (r1 - r0))^2 on the square's radial scaling), so the outer boundary
+    is the box [-r1, r1]^2 with its sides named as problem type 3's channel expects:
+    ``inlet`` (x = -r1), ``outlet`` (x = r1), ``top`` and ``bottom``. n_theta must be a
+    multiple of 8 (box corners on nodes).
     """
+    if square and n_theta % 8:
+        raise ValueError("square outer boundary needs n_theta divisible by 8")
     if abs(stretch - 1.0) < 1e-14:
         radii = np.linspace(r0, r1, n_r + 1)
     else:
@@ -178,7 +186,11 @@ def cylinder_ogrid(n_r: int = 256, n_theta: int = 512, r0: float = 0.5, r1: floa
     # ids[j, i]: j radial ring, i azimuth (periodic)
     ids = np.arange((n_r + 1) * n_theta).reshape(n_r + 1, n_theta)
     rr, tt = np.meshgrid(radii, theta, indexing="ij")
-    xy = np.stack([rr * np.cos(tt), rr * np.sin(tt)], axis=-1).reshape(-1, 2)
+    scale = np.ones_like(rr)
+    if square:
+        w = ((rr - r0) / (r1 - r0)) ** 2
+        scale = (1.0 - w) + w / np.maximum(np.abs(np.cos(tt)), np.abs(np.sin(tt)))
+    xy = np.stack([rr * scale * np.cos(tt), rr * scale * np.sin(tt)], axis=-1).reshape(-1, 2)
     idsp = np.concatenate([ids, ids[:, :1]], axis=1)  # wrap in azimuth
     # azimuth increases CCW: (i along theta) x (j along r) would be clockwise, so use
     # xi = radial, eta = azimuthal: SW=(j,i), SE=(j+1,i), NE=(j+1,i+1), NW=(j,i+1)
@@ -190,7 +202,13 @@ def cylinder_ogrid(n_r: int = 256, n_theta: int = 512, r0: float = 0.5, r1: floa
     inner = np.stack([idsp[0, 1:], idsp[0, :-1]], axis=1)      # domain on the left when walking
     outer = np.stack([idsp[-1, :-1], idsp[-1, 1:]], axis=1)
     mid_x = 0.5 * (xy[outer[:, 0], 0] + xy[outer[:, 1], 0])
-    bnd = {"object": inner, "inlet": outer[mid_x < 0.0], "outlet": outer[mid_x >= 0.0]}
+    if not square:
+        bnd = {"object": inner, "inlet": outer[mid_x < 0.0], "outlet": outer[mid_x >= 0.0]}
+        return QuadMesh(xy, quads, bnd)
+    mid_y = 0.5 * (xy[outer[:, 0], 1] + xy[outer[:, 1], 1])
+    side = np.abs(mid_x) >= np.abs(mid_y)
+    bnd = {"object": inner, "inlet": outer[side & (mid_x < 0.0)], "outlet": outer[side & (mid_x >= 0.0)],
+           "top": outer[~side & (mid_y > 0.0)], "bottom": outer[~side & (mid_y <= 0.0)]}
     return QuadMesh(xy, quads, bnd)
 
 

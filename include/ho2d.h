@@ -281,9 +281,11 @@ int ho2d_clean_up(ho2d_solver* handle);
  * vorticity and to BC_parl_vel (the wall velocity of no-slip walls, constant in time),
  * by the transpose of the discrete time loop of solve_advection_diffusion
  * (src/HO_2D.cpp:1465-1531): stage kernels run backwards, a transposed Poisson solve per
- * stage. Advection type 1; precision HO2D_FP64, or HO2D_MIXED_KRYLOV, whose forward and
- * transposed Poisson solves are FP32 Krylov inside FP64 refinement (HO2D_MIXED is
- * rejected with HO2D_ERR_UNSUPPORTED). */
+ * stage. Advection types 1 and 2, every precision: with HO2D_MIXED_KRYLOV the forward and
+ * transposed Poisson solves are FP32 Krylov inside FP64 refinement; with HO2D_MIXED the
+ * forward sweep and its recomputation follow the FP32-stage trajectory and each stage is
+ * linearised in FP64 at its states. Hybrid runs (problem type 11) are rejected with
+ * HO2D_ERR_UNSUPPORTED. */
 /* Storage of the adjoint's checkpoints and recomputed stage states: 0 = FP64 (default),
  * 1 = FP32 (half the memory; the backward sweep then linearises about a trajectory
  * recomputed from FP32-rounded states). Takes effect at the next ho2d_adjoint_forward. */

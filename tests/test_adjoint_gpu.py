@@ -123,17 +123,20 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     del rng
 
 
-def test_mixed_krylov_adjoint_matches_fp64():
+# HO2D_MIXED_KRYLOV: the same FP64 stages, Poisson round-off only; HO2D_MIXED: the FP32
+# stage's trajectory (about 1e-8 from FP64 after 4 steps) as the linearisation point
+@pytest.mark.parametrize("prec,tol", [(MIXED_KRYLOV, 1e-8), (MIXED, 1e-6)])
+def test_mixed_adjoint_matches_fp64(prec, tol):
     inp = golden_input("bfs2_rk4")
     res = {}
-    for prec in (FP64, MIXED_KRYLOV):
-        s = solver_for(inp, precision=prec, tol=1e-12)
+    for p in (FP64, prec):
+        s = solver_for(inp, precision=p, tol=1e-12)
         w0 = rng_of(40).standard_normal((s.N_el, s.Knod, s.Knod))
         s.setsolnvort_d(w0)
         s.adjoint_forward(4, 2)
-        res[prec] = s.adjoint_backward(rng_of(41).standard_normal(w0.shape))
-    for a, b in zip(res[MIXED_KRYLOV], res[FP64]):
-        assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
+        res[p] = s.adjoint_backward(rng_of(41).standard_normal(w0.shape))
+    for a, b in zip(res[prec], res[FP64]):
+        assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b)
 
 
 def test_fp32_state_storage_is_close_to_fp64():
@@ -225,7 +228,6 @@ def test_adjoint_rejects_what_it_does_not_cover(tmp_path):
     with pytest.raises(HO2DError) as e:
         s.adjoint_backward(np.zeros((s.N_el, s.Knod, s.Knod)))
     assert e.value.code == 1
-    s.set_precision(MIXED)
     with pytest.raises(HO2DError) as e:
-        s.adjoint_forward(1, 1)
-    assert e.value.code == 4
+        s.adjoint_forward(-1, 1)
+    assert e.value.code == 1
