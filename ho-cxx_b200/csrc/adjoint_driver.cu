@@ -339,12 +339,21 @@ Error Solver::stage_adjoint(double coeff, const double* lam_k, double* lam_w, do
     DeviceState& d = *d_;
     AdjointState& a = *adj_;
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod, nb = (size_t)mesh_.n_eb * in_.knod;
+    if (stage32_) {  // the FP32 stage input kept, and widened in place for the FP64 stage
+        if (a.w32_save.bytes() < nv * 4) HO2D_CUDA(a.w32_save.alloc(nv * 4), "alloc");
+        HO2D_CUDA(cudaMemcpyAsync(a.w32_save.get(), d.w_stage.get(), nv * 4, cudaMemcpyDeviceToDevice, d.stream),
+                  "copy");
+        HO2D_CUDA(launch_copy_f2d(a.w32_save.as<float>(), d.w_stage.as<double>(), nv, d.stream), "f2d");
+    }
     HO2D_TRY(stage_t<double>(coeff, 0, false, true));  // the stage at the current state: psi of this input
     HO2D_CUDA(cudaMemcpyAsync(a.lam_k.get(), lam_k, nv * 8, cudaMemcpyHostToDevice, d.stream), "copy");
     HO2D_CUDA(cudaMemsetAsync(a.lpv.get(), 0, a.lpv.bytes(), d.stream), "memset");
     HO2D_TRY(stage_adjoint_dev(coeff, a.lw_out.as<double>()));
     HO2D_CUDA(cudaMemcpyAsync(lam_w, a.lw_out.get(), nv * 8, cudaMemcpyDeviceToHost, d.stream), "copy");
     if (lam_pv && nb) HO2D_CUDA(cudaMemcpyAsync(lam_pv, a.lpv.get(), nb * 8, cudaMemcpyDeviceToHost, d.stream), "copy");
+    if (stage32_)  // the FP32 stage input back
+        HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), a.w32_save.get(), nv * 4, cudaMemcpyDeviceToDevice, d.stream),
+                  "copy");
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "stage adjoint");
     return {0, ""};
 }
@@ -386,6 +395,12 @@ Error Solver::load_state(double* dst, const void* src) {
     return {0, ""};
 }
 
+// The stage input d.w_stage from omega, in the stage precision (FP32 under HO2D_MIXED).
+static cudaError_t stage_input_from(const DeviceState& d, bool stage32, const double* w, size_t nv) {
+    if (stage32) return launch_copy_d2f(w, d.w_stage.as<float>(), nv, d.stream);
+    return cudaMemcpyAsync(d.w_stage.get(), w, nv * 8, cudaMemcpyDeviceToDevice, d.stream);
+}
+
 Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     const NvtxRange nvtx_range("ho2d.adjoint_forward");
     HO2D_TRY(adjoint_supported(in_));
@@ -411,7 +426,7 @@ Error Solver::adjoint_forward(int nsteps, int ckpt_every) {
     a.t0 = time_;
     a.every = ckpt_every;
     // the stage input of a step is omega itself
-    HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
+    HO2D_CUDA(stage_input_from(d, stage32_, d.omega.as<double>(), nv), "copy");
     for (int n = 0; n < nsteps; ++n) {
         if (n % ckpt_every == 0) HO2D_TRY(store_state(a.ckpt[n / ckpt_every]->get(), d.omega.as<double>()));
         HO2D_TRY(step(1));
@@ -453,7 +468,9 @@ Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* gra
     const int nseg = (nsteps + every - 1) / every;
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int n0 = seg * every, n1 = std::min(nsteps, n0 + every);
-        // recompute the segment from its checkpoint, keeping every stage input and psi
+        // recompute the segment from its checkpoint, keeping every stage input and psi; the
+        // stages are the FP64 ones the adjoint linearises (under HO2D_MIXED the checkpoints
+        // come from the FP32-stage trajectory and each segment is recomputed in FP64 from them)
         HO2D_TRY(load_state(d.omega.as<double>(), a.ckpt[seg]->get()));
         HO2D_TRY(copy(d.w_stage.get(), d.omega.get()));
         for (int n = n0; n < n1; ++n) {
@@ -461,7 +478,7 @@ Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* gra
             for (int s = 0; s < ns; ++s) {
                 const size_t off = ((size_t)(n - n0) * ns + s) * nv * wb;
                 HO2D_TRY(store_state(seg_w + off, d.w_stage.as<double>()));
-                HO2D_TRY(stage_impl(tb.c[s], s, true));
+                HO2D_TRY(stage_t<double>(tb.c[s], s, true));
                 HO2D_TRY(store_state(seg_psi + off, d.psi64.as<double>()));
             }
         }
@@ -485,7 +502,7 @@ Error Solver::adjoint_backward(const double* dJ_dw, double* grad_w0, double* gra
     if (grad_pv && nb) HO2D_CUDA(cudaMemcpyAsync(grad_pv, a.lpv.get(), nb * 8, cudaMemcpyDeviceToHost, d.stream), "copy");
     // back to the state at T
     HO2D_TRY(copy(d.omega.get(), a.wT.get()));
-    HO2D_TRY(copy(d.w_stage.get(), a.wT.get()));
+    HO2D_CUDA(stage_input_from(d, stage32_, a.wT.as<double>(), nv), "copy");
     HO2D_TRY(copy(d.psi64.get(), a.psiT.get()));
     time_ = a.t0 + nsteps * in_.dt;
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "adjoint backward");

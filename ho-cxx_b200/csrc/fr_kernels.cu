@@ -19,6 +19,8 @@
 //   bc_update_kernel  time-dependent BC refresh and h-direction flip (1979-2217)
 #include <cmath>
 
+#include <algorithm>
+
 #include "device.cuh"
 #include "fr_device.cuh"
 #include "fr_launch.hpp"
@@ -193,6 +195,26 @@ cudaError_t launch_poisson_rhs(int K, int N, const int* face_nb, const T* w, con
                                const double* bc_p, double* rhs, cudaStream_t s) {
     HO2D_DISPATCH_K(K, (poisson_rhs_kernel<KK, T><<<grid_for<KK>(N), Shape<KK>::THREADS, 0, s>>>(
                            N, face_nb, w, J, bsrc, bc_p, rhs)));
+    return cudaGetLastError();
+}
+
+// A vorticity handed in from the host (staged in `in`) against the device's current one:
+// flags[0] = some value is not finite, flags[1] = some value differs bitwise from `cur`.
+__global__ void k_vort_check(const double* __restrict__ in, const double* __restrict__ cur, size_t n,
+                             int* __restrict__ flags) {
+    bool bad = false, diff = false;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double x = in[i];
+        bad |= !isfinite(x);
+        diff |= __double_as_longlong(x) != __double_as_longlong(cur[i]);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&flags[0], 1);
+    if (__any_sync(0xffffffffu, diff) && (threadIdx.x & 31) == 0) atomicOr(&flags[1], 1);
+}
+
+cudaError_t launch_vort_check(const double* in, const double* cur, size_t n, int* flags, cudaStream_t s) {
+    const unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+    k_vort_check<<<g ? g : 1, 256, 0, s>>>(in, cur, n, flags);
     return cudaGetLastError();
 }
 

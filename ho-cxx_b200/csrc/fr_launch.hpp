@@ -303,6 +303,8 @@ cudaError_t launch_body_force(int npts, const double* coef, const int* idx, cons
 
 // elementwise helpers
 cudaError_t launch_copy_d2f(const double* a, float* b, size_t n, cudaStream_t s);
+// flags[0] |= some in[i] is not finite; flags[1] |= some in[i] differs bitwise from cur[i]
+cudaError_t launch_vort_check(const double* in, const double* cur, size_t n, int* flags, cudaStream_t s);
 cudaError_t launch_axpy_f2d(const float* e, double* x, size_t n, cudaStream_t s);  // x += e
 
 }  // namespace ho2d

@@ -1280,9 +1280,20 @@ Error Solver::set_vorticity(const double* in) {
     if (!setup_done_) return {1, "not set up"};
     DeviceState& d = *d_;
     const size_t nv = (size_t)mesh_.n_el * in_.knod * in_.knod;
-    for (size_t i = 0; i < nv; ++i)
-        if (!std::isfinite(in[i])) return {7, "non-finite value in the vorticity passed in"};
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    // staged on the device and checked there: finite everywhere, and whether it differs from
+    // the current vorticity at all (a caller handing back the state it read continues the
+    // trajectory, so the streamfunction history stays valid)
+    if (d.vort_in.bytes() < nv * 8) HO2D_CUDA(d.vort_in.alloc(nv * 8), "alloc");
+    if (!d.vort_flags.get()) HO2D_CUDA(d.vort_flags.alloc(2 * sizeof(int)), "alloc");
+    HO2D_CUDA(cudaMemsetAsync(d.vort_flags.get(), 0, 2 * sizeof(int), d.stream), "memset");
+    HO2D_CUDA(cudaMemcpyAsync(d.vort_in.get(), in, nv * 8, cudaMemcpyHostToDevice, d.stream), "copy");
+    HO2D_CUDA(launch_vort_check(d.vort_in.as<double>(), d.omega.as<double>(), nv, d.vort_flags.as<int>(), d.stream),
+              "check");
+    int flags[2] = {0, 0};
+    HO2D_CUDA(cudaMemcpyAsync(flags, d.vort_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, d.stream), "copy");
+    HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");
+    if (flags[0]) return {7, "non-finite value in the vorticity passed in"};
     if (hybrid_ && d.hvort[1].get()) {
         // hybrid operation (setsolnvort_d, src/HO_2D.cpp:4148-4170): the vorticity to blend
         // in at the end of the outer step; the previous one becomes the start value
@@ -1290,8 +1301,11 @@ Error Solver::set_vorticity(const double* in) {
         HO2D_CUDA(cudaMemcpy(d.hvort[1].get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
         return {0, ""};
     }
-    hist_count_ = 0;  // the trajectory restarts: no psi history to extrapolate from
-    HO2D_CUDA(cudaMemcpy(d.omega.get(), in, nv * 8, cudaMemcpyHostToDevice), "copy");
+    if (flags[1]) {  // a new state: the trajectory restarts, no psi history to extrapolate from
+        hist_count_ = 0;
+        HO2D_CUDA(cudaMemcpyAsync(d.omega.get(), d.vort_in.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
+    }
+    // the stage input is the vorticity either way (a single ho2d_stage starts from it)
     if (stage32_) HO2D_CUDA(launch_copy_d2f(d.omega.as<double>(), d.w_stage.as<float>(), nv, d.stream), "d2f");
     else HO2D_CUDA(cudaMemcpyAsync(d.w_stage.get(), d.omega.get(), nv * 8, cudaMemcpyDeviceToDevice, d.stream), "copy");
     HO2D_CUDA(cudaStreamSynchronize(d.stream), "sync");

@@ -80,6 +80,7 @@ struct DeviceState {
     DeviceBuffer bc_p, bc_nv, bc_pv, bc_d, bc_w, vjump, bc_adv, edge_y, bsrc;
     // fields
     DeviceBuffer omega, acc, psi64, rhs, rres;
+    DeviceBuffer vort_in, vort_flags;  // set_vorticity: the staged field and its check flags
     DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
     // Poisson operator and Krylov workspace
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
@@ -157,6 +158,7 @@ struct AdjointState {
     DeviceBuffer lam, mus[4];
     std::vector<std::unique_ptr<DeviceBuffer>> ckpt;
     DeviceBuffer seg_w, seg_psi, wT, psiT;
+    DeviceBuffer w32_save;  // the FP32 stage input kept across a single-stage adjoint (HO2D_MIXED)
     int nsteps = -1, every = 1;
     double t0 = 0.0;
     size_t state_bytes = 8;  // 8: FP64 state storage, 4: FP32
