@@ -130,7 +130,7 @@ Error Solver::adjoint_prepare() {
     a.lev.clear();
     const char* mode = std::getenv("HO2D_PRECOND");
     const char* om = std::getenv("HO2D_MG_OMEGA");
-    const double omega = om ? std::atof(om) : 1.0;
+    const double omega = om ? std::atof(om) : kSmoothingWeight;
     a.pc64.omega = a.pc32.omega = omega;
     if (!(mode && std::string(mode) == "bj")) {
         const char* dm = std::getenv("HO2D_DENSE_MAX");

@@ -107,6 +107,12 @@ struct PoisGeom {
 };
 
 // Matrix-free FR Laplacian (the Poisson operator) plus the preconditioner's element data.
+// Weight of the preconditioner's block smoothing step, z = e + w M (f - A e). Under-relaxing
+// the exact (or fitted) block inverse pays: on the 256 x 512 cylinder O-grid at K = 6 the
+// inner iterations per step fell by 18% (mixed) and 14% (FP64) from w = 1 to 0.7, and on
+// the backward-facing step by 5%.
+constexpr double kSmoothingWeight = 0.7;
+
 template <typename T>
 struct MfOp {
     int K;

@@ -513,9 +513,6 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
     return {0, ""};
 }
 
-// Builds the P0 coarse hierarchy on the host and the device views of both precisions.
-// HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight;
-// HO2D_DENSE_MAX bounds the dense coarsest level (a test hook for other hierarchy shapes).
 // The block column sums on the host: kept by the host assembly, downloaded once after the
 // device assembly.
 Error Solver::ensure_host_colsum() {
@@ -528,6 +525,9 @@ Error Solver::ensure_host_colsum() {
     return {0, ""};
 }
 
+// Builds the P0 coarse hierarchy on the host and the device views of both precisions.
+// HO2D_PRECOND=bj selects plain block-Jacobi; HO2D_MG_OMEGA sets the smoother weight;
+// HO2D_DENSE_MAX bounds the dense coarsest level (a test hook for other hierarchy shapes).
 Error Solver::setup_preconditioner() {
     DeviceState& d = *d_;
     const int N = mesh_.n_el;
@@ -540,7 +540,7 @@ Error Solver::setup_preconditioner() {
     const char* mode = std::getenv("HO2D_PRECOND");
     if (mode && std::string(mode) == "bj") return {0, ""};
     const char* om = std::getenv("HO2D_MG_OMEGA");
-    const double omega = om ? std::atof(om) : 1.0;
+    const double omega = om ? std::atof(om) : kSmoothingWeight;
     const char* dm = std::getenv("HO2D_DENSE_MAX");
     const int dmax = dm ? std::max(1, std::atoi(dm)) : kDenseMax;
     CoarseHierarchy H;

@@ -212,12 +212,11 @@ __device__ __forceinline__ void row_contravariant(const DevBases<T>& b, const T 
 // in T): corrected grad psi, u = dpsi/dy, v = -dpsi/dx, the boundary side outputs
 // (velocity_jump, BC_normal_vel, the no-slip diffusion BC) and the omega and
 // contravariant-flux face traces the residual kernel gathers.
+// (FP32 stage: at most 128 registers, four CTAs per SM)
 template <int K, typename T, typename TP>
-__global__ void __launch_bounds__(Rows<K>::THREADS) velocity_rows(FrGeom<TP> g, const TP* __restrict__ G11,
-                                                                   const TP* __restrict__ G12,
-                                                                   const TP* __restrict__ G22, DevBases<TP> b,
-                                                                   DevBases<T> bw, BcArrays bc,
-                                                                   VelocityArgs<T, TP> a) {
+__global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
+    velocity_rows(FrGeom<TP> g, const TP* __restrict__ G11, const TP* __restrict__ G12, const TP* __restrict__ G22,
+                  DevBases<TP> b, DevBases<T> bw, BcArrays bc, VelocityArgs<T, TP> a) {
     __shared__ StageScratch<K, TP> sm[Rows<K>::WARPS];
     __shared__ T wbuf[Rows<K>::WARPS][Rows<K>::EPW][K][K];
     const RowIdx<K> ix(g.N, blockIdx.x);
@@ -340,11 +339,11 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) velocity_rows(FrGeom<TP> g, 
 // advective divergence (type 1: discontinuous flux with the upwind switch; type 2:
 // continuous volumetric flux), k = dt (adv + diff) and the RK update
 // (src/HO_2D.cpp:1465-1531, 2219-2645, 2666-2927).
+// (FP32: at most 96 registers, five CTAs per SM)
 template <int K, typename T>
-__global__ void __launch_bounds__(Rows<K>::THREADS) residual_rows(FrGeom<T> g, const T* __restrict__ G11,
-                                                                   const T* __restrict__ G12,
-                                                                   const T* __restrict__ G22, DevBases<T> b,
-                                                                   BcArrays bc, ResidualArgs<T> a) {
+__global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 5 : 1)
+    residual_rows(FrGeom<T> g, const T* __restrict__ G11, const T* __restrict__ G12, const T* __restrict__ G22,
+                  DevBases<T> b, BcArrays bc, ResidualArgs<T> a) {
     __shared__ StageScratch<K, T> sm[Rows<K>::WARPS];
     const RowIdx<K> ix(g.N, blockIdx.x);
     const int t = ix.t, lw = ix.lw, el = ix.el;
