@@ -49,6 +49,8 @@ Solver::Solver() : d_(new DeviceState) {
     verbose_ = v && v[0] && v[0] != '0';
     const char* g = std::getenv("HO2D_GRAPHS");
     use_graphs_ = !(g && g[0] == '0');
+    const char* it = std::getenv("HO2D_INNER_TOL");
+    if (it && std::atof(it) > 0.0 && std::atof(it) < 1.0) inner_tol_ = std::atof(it);
 }
 Solver::~Solver() = default;
 

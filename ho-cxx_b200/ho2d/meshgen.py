@@ -212,6 +212,47 @@ def cylinder_ogrid(n_r: int = 256, n_theta: int = 512, r0: float = 0.5, r1: floa
     return QuadMesh(xy, quads, bnd)
 
 
+def cylinder_channel(n_r: int = 48, n_theta: int = 96, r0: float = 0.5, x_in: float = -15.0, x_out: float = 45.0,
+                     half_h: float = 15.0, stretch: float = 1.04) -> QuadMesh:
+    """O-grid from a cylinder at the origin (radius r0) out to the channel
+    [x_in, x_out] x [-half_h, half_h], at uniform azimuth (as ``cylinder_ogrid``). x_in
+    and x_out are moved to the nearest values that put the channel's corners on azimuthal
+    nodes, so every boundary edge lies on one side. Ring j sits at r_j along each ray,
+    blended from the circle to the channel boundary with weight ((r_j - r0) / (R - r0))^2,
+    R = half_h, r_j growing geometrically by ``stretch``. Names follow problem type 3's
+    channel: ``object``, ``inlet`` (x = x_in), ``outlet`` (x = x_out), ``top``,
+    ``bottom``."""
+    dth = 2.0 * np.pi / n_theta
+    k_out = max(1, int(round(math.atan2(half_h, x_out) / dth)))
+    k_in = max(1, int(round(math.atan2(half_h, -x_in) / dth)))
+    x_out = half_h / math.tan(k_out * dth)
+    x_in = -half_h / math.tan(k_in * dth)
+    theta = dth * np.arange(n_theta)
+    c, sn = np.cos(theta), np.sin(theta)
+    with np.errstate(divide="ignore"):
+        tx = np.where(c > 0, x_out / np.where(c > 0, c, 1.0), np.where(c < 0, x_in / np.where(c < 0, c, 1.0), np.inf))
+        ty = np.where(sn != 0, half_h / np.abs(np.where(sn != 0, sn, 1.0)), np.inf)
+    dist = np.minimum(tx, ty)  # distance from the centre to the channel boundary along each ray
+    R = half_h
+    dr0 = (R - r0) * (stretch - 1.0) / (stretch ** n_r - 1.0)
+    radii = r0 + dr0 * (stretch ** np.arange(n_r + 1) - 1.0) / (stretch - 1.0)
+    radii[-1] = R
+    w = ((radii - r0) / (R - r0)) ** 2
+    rr = radii[:, None] * ((1.0 - w)[:, None] + w[:, None] * (dist / R)[None, :])
+    xy = np.stack([rr * c[None, :], rr * sn[None, :]], axis=-1).reshape(-1, 2)
+    ids = np.arange((n_r + 1) * n_theta).reshape(n_r + 1, n_theta)
+    idsp = np.concatenate([ids, ids[:, :1]], axis=1)
+    quads = np.stack([idsp[:-1, :-1], idsp[1:, :-1], idsp[1:, 1:], idsp[:-1, 1:]], axis=-1).reshape(-1, 4)
+    inner = np.stack([idsp[0, 1:], idsp[0, :-1]], axis=1)
+    outer = np.stack([idsp[-1, :-1], idsp[-1, 1:]], axis=1)
+    mid = 0.5 * (xy[outer[:, 0]] + xy[outer[:, 1]])
+    tol = 1e-9 * max(abs(x_in), x_out, half_h)
+    bnd = {"object": inner, "inlet": outer[np.abs(mid[:, 0] - x_in) < tol],
+           "outlet": outer[np.abs(mid[:, 0] - x_out) < tol], "top": outer[np.abs(mid[:, 1] - half_h) < tol],
+           "bottom": outer[np.abs(mid[:, 1] + half_h) < tol]}
+    return QuadMesh(xy, quads, bnd)
+
+
 def write_msh(mesh: QuadMesh, path: str) -> None:
     """Write ``mesh`` as Gmsh 4.1 ASCII readable by the reference's reader."""
     names = list(mesh.boundaries.keys())

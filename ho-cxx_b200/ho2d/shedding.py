@@ -2,20 +2,24 @@
 Strouhal number.
 
 Problem type 3 (src/HO_2D.cpp:819-906) is a cylinder of diameter D = 1 (the "object"
-boundary at r = 0.5) in a channel: a uniform stream U = 1 enters through the straight
-inlet (psi = y - y_min, normal velocity U), the top and bottom move with the stream, and
-the outlet is a Neumann boundary. The
-force on the cylinder comes from ``HO_2D.forces()`` (FP64, density 1; no counterpart in the
-reference), so the drag and lift coefficients are C = 2 F / (U^2 D) and the Strouhal number
-St = f D / U is the lift frequency f.
+boundary at r = 0.5) in a channel: the stream enters through the straight inlet (psi =
+U (y - y_min), normal velocity U), the top and bottom move with it, and the outlet is a
+Neumann boundary. The reference's inflow is pulsatile, U(t) = 2 |sin(pi t / 40)|
+(update_BCs, src/HO_2D.cpp:1979-2217; ``inflow_speed``), so it peaks at U = 2 (Re = 200 on
+the peak speed) at t = 20. The force on the cylinder comes from ``HO_2D.forces()`` (FP64,
+density 1; no counterpart in the reference); the drag and lift coefficients use the
+instantaneous inflow speed, C = 2 F / (U(t)^2 D), and the Strouhal number St = f D / U uses
+the lift frequency f and the mean inflow speed over the analysed window. The default run
+ends at t = 28, so its last four shedding periods lie around the inflow peak.
 
 The case: an O-grid of ``n_r`` x ``n_theta`` cells from the cylinder at r = 0.5 out to the
-box [-r1, r1]^2 (radial spacing growing by ``stretch``, the rings blending from circles into
-the box), K = ``knod``, Re = 100. The step is the smaller of the CFL-0.5 step
-for |u| <= 2 and the viscous bound of explicit RK4 (meshgen.cfl_dt, meshgen.viscous_dt). A
-symmetric start sheds only after round-off grows, so the initial vorticity is a Gaussian
-vortex of circulation ``gamma`` centred off the axis behind the cylinder (below 1e-4 on the
-cylinder). All fields are synthetic: no dataset is involved.
+channel [-r1, 3 r1] x [-r1, r1] (radial spacing growing by ``stretch``, the rings blending
+from circles into the channel's rectangle), K = ``knod``, Re = 100 (on U = 1). The step is
+the smaller of the CFL-0.5 step for |u| <= 2 and the viscous bound of explicit RK4
+(meshgen.cfl_dt, meshgen.viscous_dt). A symmetric start sheds only after round-off grows,
+so the initial vorticity is a Gaussian vortex of circulation ``gamma`` centred off the axis
+behind the cylinder (below 1e-4 on the cylinder). All fields are synthetic: no dataset is
+involved.
 
 St from a lift series: the upward zero crossings of lift - mean (the mean over the analysed
 window) located by linear interpolation, with a hysteresis of a quarter of the half
@@ -33,6 +37,12 @@ import time
 import numpy as np
 
 from . import FP64, MIXED, HO_2D, meshgen
+
+
+def inflow_speed(t):
+    """Problem type 3's inflow speed at time t: 2 |sin(pi t / 40)| (the reference's
+    time-dependent inlet and channel walls, src/HO_2D.cpp:1979-2217)."""
+    return 2.0 * np.abs(np.sin(np.pi / 40.0 * np.asarray(t, dtype=float)))
 
 
 def upward_crossings(t: np.ndarray, y: np.ndarray, h: float = 0.0) -> np.ndarray:
@@ -101,9 +111,10 @@ class SheddingCase:
                  knod: int = 4, reyn: float = 100.0, gamma: float = 0.5, precision: int = FP64, tol: float = 1e-10,
                  max_iter: int = 500):
         os.makedirs(workdir, exist_ok=True)
-        # the box [-r1, r1]^2 around the cylinder: problem type 3's straight inlet (uniform
-        # inflow normal to it), top and bottom moving with the free stream, outlet
-        mesh = meshgen.cylinder_ogrid(n_r, n_theta, r0=0.5, r1=r1, stretch=stretch, square=True)
+        # the channel [-r1, 3 r1] x [-r1, r1] around the cylinder: problem type 3's straight
+        # inlet (uniform inflow normal to it), top and bottom moving with the free stream, and
+        # the outlet 3 r1 downstream, where the shed vortices have spread
+        mesh = meshgen.cylinder_channel(n_r, n_theta, r0=0.5, x_in=-r1, x_out=3.0 * r1, half_h=r1, stretch=stretch)
         self.dt = min(meshgen.cfl_dt(mesh, knod, 2.0), meshgen.viscous_dt(mesh, knod, reyn))
         meshgen.write_msh(mesh, os.path.join(workdir, "mesh.msh"))
         self.inp = os.path.join(workdir, "input.dat")
@@ -140,14 +151,20 @@ class SheddingCase:
             t[i] = s.time()[0]
             fx[i], fy[i] = s.forces()
         wall = time.perf_counter() - t0
-        cd, cl = 2.0 * fx, 2.0 * fy  # U = D = 1, density 1
-        st = strouhal(t, cl)
+        # coefficients on the instantaneous inflow speed (D = 1, density 1)
+        u2 = np.maximum(inflow_speed(t), 0.05) ** 2
+        cd, cl = 2.0 * fx / u2, 2.0 * fy / u2
+        st = strouhal(t, fy)  # crossings of the lift force itself: the frequency needs no scale
         w = (t >= st["window"][0]) & (t <= st["window"][1]) if np.isfinite(st["St"]) else t >= 0.5 * t[-1]
-        return {"t": t, "cd": cd, "cl": cl, "St": st, "cd_mean": float(cd[w].mean()),
-                "cl_amplitude": st["amplitude"], "steps": int(nsamp * every), "wall_s": wall}
+        u_mean = float(inflow_speed(t[w]).mean())
+        for key in ("St", "St_fft"):
+            st[key] = st[key] / u_mean if np.isfinite(st[key]) else st[key]
+        return {"t": t, "cd": cd, "cl": cl, "St": st, "u_mean": u_mean, "cd_mean": float(cd[w].mean()),
+                "cl_amplitude": float(0.5 * (cl[w].max() - cl[w].min())), "steps": int(nsamp * every),
+                "wall_s": wall}
 
 
-def run(workdir: str, t_end: float = 120.0, **kw) -> dict:
+def run(workdir: str, t_end: float = 28.0, **kw) -> dict:
     """St, mean drag and lift amplitude in FP64 and with the FP32 Krylov
     (HO2D_MIXED: FP32 stage kernels and FP32 BiCGSTAB inside FP64 refinement) on the same
     case, and their differences."""
@@ -169,7 +186,8 @@ def run_case(c: SheddingCase, t_end: float) -> dict:
     st = r["St"]
     k = max(1, len(r["t"]) // 240)  # about 240 samples of the series
     return {"St": st["St"], "St_fft": st["St_fft"], "period_spread": st["period_spread"], "window": st["window"],
-            "cd_mean": r["cd_mean"], "cl_amplitude": r["cl_amplitude"], "steps": r["steps"], "wall_s": r["wall_s"],
+            "u_mean": r["u_mean"], "cd_mean": r["cd_mean"], "cl_amplitude": r["cl_amplitude"], "steps": r["steps"],
+            "wall_s": r["wall_s"],
             "ms_per_step": 1e3 * r["wall_s"] / max(1, r["steps"]),
             "series": {"t": [round(float(x), 4) for x in r["t"][::k]], "cd": [float(x) for x in r["cd"][::k]],
                        "cl": [float(x) for x in r["cl"][::k]]}}

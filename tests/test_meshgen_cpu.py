@@ -113,3 +113,21 @@ def test_config_goldens_match_generated_inputs(tmp_path, name):
     inp = CG.write_case(name, str(tmp_path))
     assert CG.sha256(inp) == meta["input_sha256"]
     assert CG.sha256(os.path.join(os.path.dirname(inp), "mesh.msh")) == meta["mesh_sha256"]
+
+
+def test_cylinder_channel_mesh():
+    """The channel O-grid of the shedding case: counter-clockwise cells, every outer edge on
+    one side of the channel (corners on nodes), the cylinder resolved as in the O-grid."""
+    m = meshgen.cylinder_channel(48, 96, r0=0.5, x_in=-15.0, x_out=45.0, half_h=15.0, stretch=1.04)
+    xy = m.xy[m.quads]
+    area = 0.5 * sum(xy[:, k, 0] * xy[:, (k + 1) % 4, 1] - xy[:, (k + 1) % 4, 0] * xy[:, k, 1] for k in range(4))
+    assert area.min() > 0.0
+    outer = sum(len(m.boundaries[k]) for k in ("inlet", "outlet", "top", "bottom"))
+    assert outer == 96 and len(m.boundaries["object"]) == 96
+    x_out = m.xy[m.boundaries["outlet"].ravel(), 0]
+    assert np.allclose(m.xy[m.boundaries["inlet"].ravel(), 0], -15.0) and np.allclose(x_out, x_out[0])
+    assert 40.0 < x_out[0] < 50.0
+    assert np.allclose(m.xy[m.boundaries["top"].ravel(), 1], 15.0)
+    assert np.allclose(m.xy[m.boundaries["bottom"].ravel(), 1], -15.0)
+    r = np.hypot(m.xy[m.boundaries["object"].ravel(), 0], m.xy[m.boundaries["object"].ravel(), 1])
+    assert np.allclose(r, 0.5)
