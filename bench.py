@@ -82,7 +82,7 @@ def parse():
                     help="one solver of the headline precision on --case: --warmup steps, then --steps graph-free "
                          "BiCGSTAB iterations with per-kernel CUDA-event times (the command of the ncu captures "
                          "summarised in profiles/)")
-    ap.add_argument("--t-end", type=float, default=28.0,
+    ap.add_argument("--t-end", type=float, default=30.0,
                     help="time units simulated for --strouhal (the pulsatile inflow peaks at t = 20)")
     ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
     a = ap.parse_args()

@@ -232,6 +232,14 @@ int ho2d_solve_counters(ho2d_solver* h, int64_t* solves, int64_t* iterations, in
     });
 }
 
+int ho2d_fp64_finishes(ho2d_solver* h, int64_t* count) {
+    return guarded(h, [&]() -> ho2d::Error {
+        if (!count) return {HO2D_ERR_ARG, "null pointer"};
+        *count = h->s.fp64_finishes();
+        return {0, ""};
+    });
+}
+
 int ho2d_get_time(ho2d_solver* h, double* time, double* dt) {
     return guarded(h, [&]() -> ho2d::Error {
         if (time) *time = h->s.time();

@@ -87,6 +87,9 @@ struct KrylovScalars {
     int max_sweeps, sweeps, iters_total, finite, zero_psi;
     int dev_error;  // nonzero: a kernel's bounded wait ran out (the host reports it)
     double res;
+    // the refinement stopped because a sweep cut the FP64 residual by less than half (the
+    // FP32 solve is no longer accurate enough for this operator; the host finishes in FP64)
+    int stalled, pad2;
 };
 
 // A preconditioner application is skipped once the solve is done, and the second one of

@@ -822,14 +822,16 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_mf_apply(MfOp<T> op, const
 // The mixed-precision solve as one graph: FP64 residual, then while the refinement
 // continues { FP32 right-hand side, inner BiCGSTAB (its own while node), psi += x,
 // FP64 residual }. k_refine_ctl decides after every FP64 residual, with the rule the
-// host loop uses: stop on a non-finite or zero residual norm, at the target or at the
-// sweep cap; otherwise ask the inner solve for max(inner_tol, 0.3 target / current)
+// host loop uses: stop on a non-finite or zero residual norm, at the target, at the sweep
+// cap, or when the last sweep did not halve the residual (stalled: the host finishes the
+// solve in FP64); otherwise ask the inner solve for max(inner_tol, 0.3 target / current)
 // relative reduction (at most 0.5), so the last sweep does not overshoot.
 __global__ void k_refine_begin(KrylovScalars* sc) {
     sc->sweeps = 0;
     sc->iters_total = 0;
     sc->zero_psi = 0;
     sc->finite = 1;
+    sc->stalled = 0;
 }
 
 __global__ void k_refine_ctl(KrylovScalars* sc, cudaGraphConditionalHandle h) {
@@ -843,6 +845,12 @@ __global__ void k_refine_ctl(KrylovScalars* sc, cudaGraphConditionalHandle h) {
         stop = true;
     }
     if (!stop && (rn <= sc->tol_outer * sc->tol_outer * bn || sc->sweeps >= sc->max_sweeps)) stop = true;
+    // a sweep that did not halve the residual: iterative refinement with an FP32 inner solve
+    // needs cond(A) * eps_32 < 1, which this operator no longer meets
+    if (!stop && sc->sweeps > 0 && !(res <= 0.5 * sc->res)) {
+        stop = true;
+        sc->stalled = 1;
+    }
     sc->res = res;
     sc->finite = fin;
     if (!stop) {

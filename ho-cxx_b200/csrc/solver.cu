@@ -51,6 +51,8 @@ Solver::Solver() : d_(new DeviceState) {
     use_graphs_ = !(g && g[0] == '0');
     const char* it = std::getenv("HO2D_INNER_TOL");
     if (it && std::atof(it) > 0.0 && std::atof(it) < 1.0) inner_tol_ = std::atof(it);
+    const char* ms = std::getenv("HO2D_MAX_SWEEPS");
+    if (ms && std::atoi(ms) >= 1) max_sweeps_ = std::atoi(ms);
 }
 Solver::~Solver() = default;
 
@@ -120,7 +122,13 @@ Error Solver::setup_from_mesh() {
     DeviceState& d = *d_;
     HO2D_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
     if (!d.stream) HO2D_CUDA(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    if (!d.side) HO2D_CUDA(cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!d.side) {
+        // the coarse cycle's stream at the highest priority: its short dependent kernels get
+        // SM slots ahead of the wide fine-smoothing kernel they run beside, which has slack
+        int lo = 0, hi = 0;
+        HO2D_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi), "cudaDeviceGetStreamPriorityRange");
+        HO2D_CUDA(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, hi), "cudaStreamCreate");
+    }
     for (cudaEvent_t* e : {&d.ev_fork, &d.ev_join})
         if (!*e) HO2D_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
     for (cudaEvent_t* e : {&d.ev0, &d.ev1, &d.evp0, &d.evp1})
@@ -210,6 +218,7 @@ Error Solver::setup_from_mesh() {
             }
         HO2D_CUDA(upload(d.u0dst, dst), "upload coarse slot table");
         HO2D_CUDA(upload(d.ue5, std::vector<double>((size_t)N * 5, 0.0)), "alloc coarse slot values");
+        HO2D_CUDA(upload(d.ue5_32, std::vector<float>((size_t)N * 5, 0.f)), "alloc coarse slot values");
     }
     HO2D_TRY(build_poisson_geometry(fnb, fnijp));
     HO2D_TRY(setup_forces());
@@ -503,7 +512,7 @@ Error Solver::upload_hierarchy(const CoarseHierarchy& H, double omega, std::vect
             c.f = b.f.as<T>();
             c.u = b.u.as<T>();
         }
-        pc.ue5 = d_->ue5.as<T>();
+        pc.ue5 = f32 ? d_->ue5_32.as<T>() : d_->ue5.as<T>();
         pc.u0dst = d_->u0dst.as<int>();
     };
     fill(pc64, false);
@@ -671,7 +680,9 @@ Error Solver::poisson_solve() {
             if (!sg.exec || sg.max_iter != max_iter_) {
                 sg.reset();
                 HO2D_CUDA(krylov_capture_solve(A, v, rs, max_iter_, pc, d.stream, &sg.graph), "graph capture");
-                HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
+                // per-node priorities: the coarse cycle's nodes keep their stream's high priority
+                HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, cudaGraphInstantiateFlagUseNodePriority),
+                          "graph instantiate");
                 sg.max_iter = max_iter_;
             }
             HO2D_CUDA(cudaGraphLaunch(sg.exec, d.stream), "graph launch");
@@ -698,15 +709,21 @@ Error Solver::poisson_solve() {
     last_iters_ = 0;
     int sweeps = 0;
     bool finite = true;
-    if (!krylov32_) {
+    // the FP64 solve from the current psi (the FP64 mode, and the finish of a mixed solve
+    // whose refinement stalled)
+    auto fp64_solve = [&]() -> Error {
         const MfOp<double> A = make_op<double>(d, mesh_, K, false);
         const BicgVectors<double> v = krylov_vectors<double>(d, d.psi64.as<double>(), d.rhs.as<double>());
         int it = 0;
         HO2D_TRY(run(A, v, d.pc64, tol_, it, d.graph64));
-        last_iters_ = it;
+        last_iters_ += it;
         const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
         finite = std::isfinite(bn) && std::isfinite(rn);
         last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
+        return {0, ""};
+    };
+    if (!krylov32_) {
+        HO2D_TRY(fp64_solve());
     } else if (use_graphs_) {
         // FP64 iterative refinement around an FP32 BiCGSTAB, both loops on the device: one
         // graph launch and one read of the scalars per solve
@@ -720,14 +737,16 @@ Error Solver::poisson_solve() {
                                                    d.rhs.as<double>(), d.rres.as<double>(), d.kxtv.as<double>(),
                                                    d.kxtg.as<double>(), d.stream, &sg.graph),
                       "graph capture");
-            HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0), "graph instantiate");
+            // per-node priorities: the coarse cycle's nodes keep their stream's high priority
+            HO2D_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, cudaGraphInstantiateFlagUseNodePriority),
+                      "graph instantiate");
             sg.max_iter = max_iter_;
         }
         // the refinement's controls travel in the device scalars (the stream is idle: every
         // earlier read of h_sc was synchronised)
         d.h_sc->tol_outer = tol_;
         d.h_sc->inner_tol = inner_tol_;
-        d.h_sc->max_sweeps = 30;
+        d.h_sc->max_sweeps = max_sweeps_;
         static_assert(offsetof(KrylovScalars, inner_tol) == offsetof(KrylovScalars, tol_outer) + sizeof(double) &&
                           offsetof(KrylovScalars, max_sweeps) == offsetof(KrylovScalars, inner_tol) + sizeof(double),
                       "refinement controls are contiguous");
@@ -741,6 +760,10 @@ Error Solver::poisson_solve() {
         finite = d.h_sc->finite != 0;
         last_res_ = d.h_sc->res;
         launches_ += krylov_refined_launches(sweeps, last_iters_, d.pc32);
+        if (finite && !(last_res_ <= tol_)) {  // stalled or capped: the FP64 solve finishes
+            ++fp64_finishes_;
+            HO2D_TRY(fp64_solve());
+        }
     } else {
         // FP64 iterative refinement around an FP32 BiCGSTAB on the same operator, driven
         // from the host (HO2D_GRAPHS=0): every exit passes through an FP64 residual of the
@@ -748,6 +771,7 @@ Error Solver::poisson_solve() {
         const MfOp<double> A64 = make_op<double>(d, mesh_, K, false);
         const MfOp<float> A32 = make_op<float>(d, mesh_, K, true);
         const BicgVectors<float> v = krylov_vectors<float>(d, d.kv[8].as<float>(), d.kv[9].as<float>());
+        bool stalled = false;
         for (;; ++sweeps) {
             HO2D_CUDA(mf_residual<double>(A64, d.rhs.as<double>(), d.psi64.as<double>(), d.kxtv.as<double>(),
                                           d.kxtg.as<double>(), d.rres.as<double>(), rs, d.stream),
@@ -755,6 +779,7 @@ Error Solver::poisson_solve() {
             launches_ += 2;
             HO2D_TRY(poll());
             const double bn = d.h_sc->bnorm2, rn = d.h_sc->rnorm2;
+            const double prev = last_res_;
             finite = std::isfinite(bn) && std::isfinite(rn);
             last_res_ = bn > 0 ? std::sqrt(rn / bn) : 0.0;
             if (!finite) break;
@@ -763,7 +788,11 @@ Error Solver::poisson_solve() {
                 last_res_ = 0.0;
                 break;
             }
-            if (rn <= tol_ * tol_ * bn || sweeps >= 30) break;
+            if (rn <= tol_ * tol_ * bn || sweeps >= max_sweeps_) break;
+            if (sweeps > 0 && !(last_res_ <= 0.5 * prev)) {  // the same stall rule as the graph
+                stalled = true;
+                break;
+            }
             HO2D_CUDA(launch_copy_d2f(d.rres.as<double>(), d.kv[9].as<float>(), nv, d.stream), "d2f");
             HO2D_CUDA(cudaMemsetAsync(d.kv[8].get(), 0, nv * sizeof(float), d.stream), "memset");
             launches_ += 1;
@@ -777,13 +806,17 @@ Error Solver::poisson_solve() {
             HO2D_CUDA(launch_axpy_f2d(d.kv[8].as<float>(), d.psi64.as<double>(), nv, d.stream), "axpy");
             launches_ += 1;
         }
+        if (finite && (stalled || !(last_res_ <= tol_))) {
+            ++fp64_finishes_;
+            HO2D_TRY(fp64_solve());
+        }
     }
     ++n_solves_;
     iters_total_ += last_iters_;
     sweeps_total_ += krylov32_ ? sweeps : 0;
     if (verbose_)
-        std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e\n", n_solves_, last_iters_,
-                     sweeps, last_res_);
+        std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e (FP64 finishes so far %ld)\n",
+                     n_solves_, last_iters_, sweeps, last_res_, (long)fp64_finishes_);
     prev_iters_ = std::max(1, krylov32_ ? last_iters_ / std::max(1, sweeps) : last_iters_);
     if (timing_) {
         HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");

@@ -143,6 +143,7 @@ class Solver {
         if (iters) *iters = iters_total_;
         if (sweeps) *sweeps = sweeps_total_;
     }
+    int64_t fp64_finishes() const { return fp64_finishes_; }
     void set_poisson_tolerance(double tol, int max_iter) {
         tol_ = tol;
         max_iter_ = max_iter;
@@ -220,9 +221,11 @@ class Solver {
     int64_t launches_ = 0;
     long n_solves_ = 0;
     int64_t iters_total_ = 0, sweeps_total_ = 0;
+    int64_t fp64_finishes_ = 0;  // mixed solves whose refinement stalled and the FP64 solve finished
     int coarse_levels_ = 0;
     std::vector<int> coarse_sizes_;
     double inner_tol_ = 1e-4;        // FP32 inner solve: relative reduction per refinement sweep
+    int max_sweeps_ = 30;            // refinement sweep cap (HO2D_MAX_SWEEPS)
     bool verbose_ = false;           // HO2D_VERBOSE=1: coarse levels and one line per Poisson solve on stderr
     bool use_graphs_ = true;         // HO2D_GRAPHS=0: host-driven Krylov loop instead of a CUDA graph
     bool timing_ = false;

@@ -88,7 +88,10 @@ struct DeviceState {
     DeviceBuffer colsum64;  // block column sums (device assembly only)
     VtkDevice vtk;
     DeviceBuffer W64, W32, zf;  // smoother applied to the block row sums; fine part of z
-    DeviceBuffer ue5, u0dst;  // level-0 coarse values per element slot, and where each goes
+    // level-0 coarse values per element slot (one buffer per precision: the cycle writes only
+    // the slots that have a block neighbour, so a shared buffer would leave the other
+    // precision's bytes in the rest), and where each value goes
+    DeviceBuffer ue5, ue5_32, u0dst;
     DeviceBuffer dinv_bf16;  // BF16 copy of dinv for the FP32 smoother (HO2D_SMOOTHER_BF16=1)
     // Kronecker-sum smoother for the FP32 solve (HO2D_SMOOTHER_KRON=1): factors, exact-block
     // index per element, compact exact blocks

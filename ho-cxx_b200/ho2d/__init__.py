@@ -266,6 +266,12 @@ class HO_2D:
         self._check(self._lib.ho2d_poisson_stats(self._h, ctypes.byref(it), ctypes.byref(res)))
         return it.value, res.value
 
+    def fp64_finishes(self) -> int:
+        """Mixed solves since setup that the FP64 solve finished (stalled refinement)."""
+        n = ctypes.c_int64()
+        self._check(self._lib.ho2d_fp64_finishes(self._h, ctypes.byref(n)))
+        return n.value
+
     def solve_counters(self):
         """(Poisson solves, Krylov iterations, refinement sweeps) since setup."""
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

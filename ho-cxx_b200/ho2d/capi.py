@@ -55,6 +55,7 @@ SIGNATURES = {
     "ho2d_get_time": (ctypes.c_int, [_P, _DP, _DP]),
     "ho2d_solve_counters": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                            ctypes.POINTER(ctypes.c_int64)]),
+    "ho2d_fp64_finishes": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "ho2d_set_time": (ctypes.c_int, [_P, _D]),
     "ho2d_time_steps": (ctypes.c_int, [_P, _I, _DP, _DP]),
     "ho2d_profile_spmv": (ctypes.c_int, [_P, _I, _DP, _DP]),

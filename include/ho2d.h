@@ -179,6 +179,11 @@ int ho2d_poisson_stats(ho2d_solver* handle, int32_t* iterations, double* rel_res
  * iterations (inner iterations of all refinement sweeps in the mixed modes) and FP64
  * refinement sweeps (0 in HO2D_FP64). Any pointer may be NULL. */
 int ho2d_solve_counters(ho2d_solver* handle, int64_t* solves, int64_t* iterations, int64_t* sweeps);
+/* Mixed-precision Poisson solves since setup whose FP64 refinement stalled (a sweep that did
+ * not halve the residual: the FP32 inner solve is not accurate enough for the operator) or
+ * hit its sweep cap, and which the FP64 solve then finished from the refined iterate. No
+ * counterpart in the reference. */
+int ho2d_fp64_finishes(ho2d_solver* handle, int64_t* count);
 /* Current solver time and time-step size. */
 int ho2d_get_time(ho2d_solver* handle, double* time, double* dt);
 /* Sets the current solver time (the reference's time_start / current_time,

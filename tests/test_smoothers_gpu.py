@@ -78,3 +78,23 @@ def test_smoother_choice_validated():
     s = HO_2D()
     with pytest.raises(capi.HO2DError):
         s.set_smoother(3)
+
+
+@pytest.mark.parametrize("graphs", ["1", "0"])
+def test_stalled_refinement_is_finished_in_fp64(tmp_path, monkeypatch, graphs):
+    """A mixed solve whose refinement stops short of the tolerance (stalled, or at the sweep
+    cap) is finished by the FP64 solve: with the cap at one sweep the first solves end short,
+    the FP64 solve finishes them, and the steps still agree with the FP64 path at the
+    Poisson tolerance."""
+    monkeypatch.setenv("HO2D_MAX_SWEEPS", "1")
+    monkeypatch.setenv("HO2D_GRAPHS", graphs)
+    inp = os.path.join(GOLDEN, "cyl4x8_rk4", "input.dat")
+    ref = _solver(inp, FP64)
+    s = _solver(inp, MIXED_KRYLOV)
+    rng = np.random.Generator(np.random.PCG64(23))
+    w0 = rng.standard_normal((ref.N_el, ref.Knod, ref.Knod))
+    w_ref, p_ref, _ = _run(ref, w0, 2)
+    w, p, _ = _run(s, w0, 2)
+    assert s.fp64_finishes() > 0
+    assert np.max(np.abs(p - p_ref)) <= TOL * np.max(np.abs(p_ref))
+    assert np.max(np.abs(w - w_ref)) <= TOL * np.max(np.abs(w_ref))
