@@ -709,6 +709,7 @@ Error Solver::poisson_solve() {
     last_iters_ = 0;
     int sweeps = 0;
     bool finite = true;
+    double refined_res = -1.0;  // the refinement's residual when the FP64 solve finished it
     // the FP64 solve from the current psi (the FP64 mode, and the finish of a mixed solve
     // whose refinement stalled)
     auto fp64_solve = [&]() -> Error {
@@ -762,6 +763,7 @@ Error Solver::poisson_solve() {
         launches_ += krylov_refined_launches(sweeps, last_iters_, d.pc32);
         if (finite && !(last_res_ <= tol_)) {  // stalled or capped: the FP64 solve finishes
             ++fp64_finishes_;
+            refined_res = last_res_;
             HO2D_TRY(fp64_solve());
         }
     } else {
@@ -808,15 +810,19 @@ Error Solver::poisson_solve() {
         }
         if (finite && (stalled || !(last_res_ <= tol_))) {
             ++fp64_finishes_;
+            refined_res = last_res_;
             HO2D_TRY(fp64_solve());
         }
     }
     ++n_solves_;
     iters_total_ += last_iters_;
     sweeps_total_ += krylov32_ ? sweeps : 0;
-    if (verbose_)
-        std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e (FP64 finishes so far %ld)\n",
+    if (verbose_) {
+        std::fprintf(stderr, "  poisson solve %ld: iters %d sweeps %d rel. residual %.3e (FP64 finishes so far %ld)",
                      n_solves_, last_iters_, sweeps, last_res_, (long)fp64_finishes_);
+        if (refined_res >= 0.0) std::fprintf(stderr, "; finished in FP64 from %.3e", refined_res);
+        std::fprintf(stderr, "\n");
+    }
     prev_iters_ = std::max(1, krylov32_ ? last_iters_ / std::max(1, sweeps) : last_iters_);
     if (timing_) {
         HO2D_CUDA(cudaEventRecord(d.evp1, d.stream), "event");
