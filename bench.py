@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--t-end", type=float, default=30.0,
                     help="time units simulated for --strouhal (the pulsatile inflow peaks at t = 20)")
     ap.add_argument("--shed-knod", type=int, default=4, help="Knod of the --strouhal case")
+    ap.add_argument("--long-steps", type=int, default=0,
+                    help="run the backward-facing step (14,625 quads, K = 5) this many steps in FP64, HO2D_MIXED "
+                         "and HO2D_MIXED_KRYLOV and report the vorticity L2 differences every 1000 steps")
     a = ap.parse_args()
     if a.knod is None:
         a.knod = 6 if a.case.startswith("cyl") else (5 if a.case.startswith("bfs") else 4)
@@ -377,6 +380,39 @@ def time_mode(s, args, dist, phys, sample_clocks):
             "clocks": clocks, "start": start}
 
 
+def run_long(args, rank):
+    """The backward-facing step (14,625 jittered quads, K = 5, Re = 400, RK4 at CFL 0.5,
+    pulsatile inlet from t = 1.5) for --long-steps steps in the three modes, with the
+    relative vorticity L2 difference of both mixed modes from FP64 every 1000 steps and
+    each mode's device time per step."""
+    import ho2d
+    from ho2d import meshgen
+
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = meshgen.make_case("bfs", tmp, knod=5, steps=10)
+        modes = (("fp64", ho2d.FP64), ("mixed", ho2d.MIXED), ("mixed_fp64_stage", ho2d.MIXED_KRYLOV))
+        sv = {m: make_solver(inp, mode, SMOOTHERS[args.smoother], 1.5) for m, mode in modes}
+        hist, ms = [], {m: 0.0 for m in sv}
+        done = 0
+        while done < args.long_steps:
+            n = min(1000, args.long_steps - done)
+            for m, s in sv.items():
+                tot, _ = s.time_steps(n)
+                ms[m] += tot
+            done += n
+            wf = sv["fp64"].get_vorticity()
+            hist.append({"steps": done, "time": sv["fp64"].time()[0],
+                         "mixed": rel_l2(sv["mixed"].get_vorticity(), wf),
+                         "mixed_fp64_stage": rel_l2(sv["mixed_fp64_stage"].get_vorticity(), wf)})
+        print(json.dumps({"metric": "relative vorticity L2 difference from FP64 (backward-facing step)",
+                          "value": hist[-1]["mixed"], "unit": "relative L2", "higher_is_better": False,
+                          "n_gpus": 1, "steps": done, "dtype": "f32+f64", "data": "synthetic (seeded jitter)",
+                          "config": {"workload": workload_name("bfs", 5, 1.5)},
+                          "ms_per_step": {m: v / max(1, done) for m, v in ms.items()}, "history": hist}))
+
+
 def secondary_workloads(args, tmp):
     """Outside the timed region of the headline: the step (14,625 quads, K = 5) after 1000
     steps in both mixed modes against FP64, and the 512^2 jittered cavity at K = 7 (mixed and
@@ -647,6 +683,9 @@ def main():
         return
     if args.profile_solve:
         run_profile(args, rank)
+        return
+    if args.long_steps > 0:
+        run_long(args, rank)
         return
     run_ours(args, rank, world, local, phys)
 
