@@ -130,6 +130,9 @@ struct MfOp {
     const T* kron_exact = nullptr;
     // [N][5][K2] the smoother's element inverse applied to each block row sum (k_make_w)
     const T* W = nullptr;
+    // FP32 operator kernels stage their inputs in shared memory by bulk copies
+    // (apply_stage.cuh) instead of reading them through L2 prefetches
+    int staged = 0;
     // host side: a second stream and two events; when set, each coarse cycle runs on the
     // second stream beside the fine part of the smoothing step (k_post_a)
     cudaStream_t side = nullptr;

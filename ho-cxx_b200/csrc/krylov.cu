@@ -27,6 +27,7 @@
 #include "fr_launch.hpp"
 #include "kron_apply.cuh"
 #include "rows.cuh"
+#include "apply_stage.cuh"
 #include "bulk_copy.cuh"
 
 namespace ho2d {
@@ -134,7 +135,7 @@ static __host__ __device__ constexpr unsigned rgrid_of(int N) {
 // precision ([K][0] FP64, [K][1] FP32): those kernels loop over element tiles, so one wave
 // covers any mesh and each CTA reduces once. Set by krylov_configure.
 struct WaveSizes {
-    unsigned init = 0, v = 0, t = 0, xr = 0, res = 0;
+    unsigned init = 0, v = 0, t = 0, xr = 0, res = 0, v_st = 0, t_st = 0;
 };
 static WaveSizes g_wave[9][2];
 
@@ -590,9 +591,61 @@ __global__ void __launch_bounds__(Rows<K>::THREADS) k_make_w(MfOp<T> op, T* __re
     }
 }
 
-// v = A ph; alpha = rho / (rhat, v); element sums of v
+// The FP32 operator's tile loop with its inputs staged in shared memory (apply_stage.cuh):
+// the copies of a warp's next tile are issued as soon as the lanes have read the current
+// one, so they run under the current tile's arithmetic. body(ix, y, sec_row) finishes
+// each tile. A copy whose wait runs out is recorded for the host (dev_error) and gets a
+// second bounded wait; after that the warp issues no more copies and runs on, so the
+// grid reduction stays consistent.
+template <int K, typename Body>
+__device__ __forceinline__ void staged_apply_loop(const MfOp<float>& op, const float* x, const float* tvin,
+                                                  const float* tgin, const float* sec, RowScratch<K, float>* sm,
+                                                  KrylovScalars* sc, Body body) {
+    using S = ApplyStage<K>;
+    using R = Rows<K>;
+    extern __shared__ __align__(128) unsigned char apply_dyn[];
+    __shared__ __align__(8) uint64_t bar[R::WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int N = op.g.N, ntiles = (int)rgrid_of<K>(N);
+    float* st = reinterpret_cast<float*>(apply_dyn + (size_t)warp * S::WARP_BYTES);
+    auto count = [&](int tile) {
+        return tile < ntiles ? max(0, min(R::EPW, N - stage_first<K>(tile, warp))) : 0;
+    };
+    if (lane == 0) mbar_init(&bar[warp]);
+    __syncwarp();
+    if (lane == 0 && count(blockIdx.x) > 0)
+        stage_issue<K>(st, &bar[warp], op.g, x, tvin, tgin, sec, stage_first<K>(blockIdx.x, warp), count(blockIdx.x));
+    unsigned phase = 0;
+    bool ok = true;
+#pragma unroll 1
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const RowIdx<K> ix(N, tile);
+        if (ok && count(tile) > 0) {
+            if (!mbar_wait_bounded(&bar[warp], phase & 1u, kBulkWaitPolls)) {
+                if (lane == 0) atomicExch(&sc->dev_error, 1);
+                ok = mbar_wait_bounded(&bar[warp], phase & 1u, kBulkWaitPolls);
+            }
+            ++phase;
+        }
+        ApplyIn<K, float> in;
+        float sr[K];
+        stage_read<K>(st, op.g, x, sec, stage_first<K>(tile, warp), ix, in, sr);
+        __syncwarp();  // every lane has read the slice
+        const int next = tile + (int)gridDim.x;
+        if (lane == 0 && ok && count(next) > 0) {
+            stage_release();
+            stage_issue<K>(st, &bar[warp], op.g, x, tvin, tgin, sec, stage_first<K>(next, warp), count(next));
+        }
+        float y[K];
+        row_apply_core<K, float>(op, in, sm[warp], ix, y);
+        body(ix, y, sr);
+    }
+}
+
+// v = A ph; alpha = rho / (rhat, v); element sums of v. ST: the FP32 loop with staged
+// inputs (dynamic shared memory ApplyStage<K>::CTA_BYTES).
 // (FP32: at most 128 registers, four CTAs per SM)
-template <int K, typename T>
+template <int K, typename T, bool ST = false>
 __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
     k_mf_v(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
@@ -602,15 +655,10 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
     const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[1] = {0.0};
-    auto tile_body = [&](int tile) {
-        const RowIdx<K> ix(op.g.N, tile);
-        T y[K];
-        row_apply<K, T>(op, v.ph, v.tv, v.tg, sm[ix.warp], ix, y);
+    auto finish = [&](const RowIdx<K>& ix, const T (&y)[K], const T (&rh)[K]) {
         T ysum = T(0);
         if (ix.active) {
             const size_t p = (size_t)ix.el * K * K + ix.t * K;
-            T rh[K];
-            load_row<K, T>(v.rhat + p, rh);
             store_row<K, T>(v.v + p, y);
 #pragma unroll
             for (int i = 0; i < K; ++i) {
@@ -621,9 +669,19 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
         const T tot = element_total<K, T>(ysum, ix.lw);
         if (ix.active && ix.t == 0) v.ev[ix.el] = tot;
     };
-    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
-    // push the operator past the register file)
-    if constexpr (sizeof(T) == 4) {
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, v.ph, v.tv, v.tg, sm[ix.warp], ix, y);
+        T rh[K];
+        if (ix.active) load_row<K, T>(v.rhat + (size_t)ix.el * K * K + ix.t * K, rh);
+        finish(ix, y, rh);
+    };
+    if constexpr (ST && sizeof(T) == 4) {
+        staged_apply_loop<K>(op, v.ph, v.tv, v.tg, v.rhat, sm, sc, finish);
+    } else if constexpr (sizeof(T) == 4) {
+        // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop
+        // would push the operator past the register file)
 #pragma unroll 1
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             if (tile + (int)gridDim.x < ntiles)
@@ -644,9 +702,9 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
     }
 }
 
-// t = A sh; omega = (t, s) / (t, t)
+// t = A sh; omega = (t, s) / (t, t). ST as in k_mf_v.
 // (FP32: at most 128 registers, four CTAs per SM)
-template <int K, typename T>
+template <int K, typename T, bool ST = false>
 __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
     k_mf_t(MfOp<T> op, BicgVectors<T> v, ReduceScratch rs) {
     KrylovScalars* sc = rs.sc;
@@ -654,14 +712,9 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
     __shared__ RowScratch<K, T> sm[Rows<K>::WARPS];
     const int ntiles = (int)rgrid_of<K>(op.g.N);
     double part[2] = {0.0, 0.0};
-    auto tile_body = [&](int tile) {
-        const RowIdx<K> ix(op.g.N, tile);
-        T y[K];
-        row_apply<K, T>(op, v.sh, v.tv, v.tg, sm[ix.warp], ix, y);
+    auto finish = [&](const RowIdx<K>& ix, const T (&y)[K], const T (&sv)[K]) {
         if (ix.active) {
             const size_t p = (size_t)ix.el * K * K + ix.t * K;
-            T sv[K];
-            load_row<K, T>(v.s + p, sv);
             store_row<K, T>(v.t + p, y);
 #pragma unroll
             for (int i = 0; i < K; ++i) {
@@ -670,9 +723,19 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 4 : 1)
             }
         }
     };
-    // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop would
-    // push the operator past the register file)
-    if constexpr (sizeof(T) == 4) {
+    auto tile_body = [&](int tile) {
+        const RowIdx<K> ix(op.g.N, tile);
+        T y[K];
+        row_apply<K, T>(op, v.sh, v.tv, v.tg, sm[ix.warp], ix, y);
+        T sv[K];
+        if (ix.active) load_row<K, T>(v.s + (size_t)ix.el * K * K + ix.t * K, sv);
+        finish(ix, y, sv);
+    };
+    if constexpr (ST && sizeof(T) == 4) {
+        staged_apply_loop<K>(op, v.sh, v.tv, v.tg, v.s, sm, sc, finish);
+    } else if constexpr (sizeof(T) == 4) {
+        // FP32: one wave of CTAs over the tiles; FP64 keeps one tile per CTA (the loop
+        // would push the operator past the register file)
 #pragma unroll 1
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             if (tile + (int)gridDim.x < ntiles)
@@ -980,12 +1043,33 @@ static void iteration_impl(const MfOp<T>& op, const BicgVectors<T>& v, const Red
     };
     const unsigned gwv = wave_of<K, T>(&WaveSizes::v, N), gwt = wave_of<K, T>(&WaveSizes::t, N),
                    gwx = wave_of<K, T>(&WaveSizes::xr, N);
+    // the FP32 operator with its inputs staged by bulk copies, or read through L2 prefetches
+    auto apply_v = [&]() {
+        if constexpr (std::is_same<T, float>::value) {
+            if (op.staged) {
+                k_mf_v<K, T, true><<<wave_of<K, T>(&WaveSizes::v_st, N), Rows<K>::THREADS, ApplyStage<K>::CTA_BYTES,
+                                     s>>>(op, v, rs);
+                return;
+            }
+        }
+        k_mf_v<K, T><<<gwv, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    };
+    auto apply_t = [&]() {
+        if constexpr (std::is_same<T, float>::value) {
+            if (op.staged) {
+                k_mf_t<K, T, true><<<wave_of<K, T>(&WaveSizes::t_st, N), Rows<K>::THREADS, ApplyStage<K>::CTA_BYTES,
+                                     s>>>(op, v, rs);
+                return;
+            }
+        }
+        k_mf_t<K, T><<<gwt, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    };
     precond(0, 0);
     mark(3);
-    k_mf_v<K, T><<<gwv, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    apply_v();
     precond(1, 4);
     mark(7);
-    k_mf_t<K, T><<<gwt, Rows<K>::THREADS, 0, s>>>(op, v, rs);
+    apply_t();
     mark(8);
     k_xr_update<K, T><<<gwx, Rows<K>::THREADS, 0, s>>>(N, v, rs, max_iter, h, has_handle);
     mark(9);
@@ -997,9 +1081,9 @@ static cudaError_t configure_waves() {
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     WaveSizes& ws = g_wave[K][std::is_same<T, float>::value ? 1 : 0];
-    auto w = [&](auto kern, unsigned& out) {
+    auto w = [&](auto kern, unsigned& out, int dyn = 0) {
         int nb = 0;
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, Rows<K>::THREADS, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, Rows<K>::THREADS, dyn);
         out = (unsigned)(nb > 0 ? nb : 1) * (unsigned)sms;
     };
     w(k_xr_update<K, T>, ws.xr);
@@ -1007,6 +1091,8 @@ static cudaError_t configure_waves() {
         w(k_mf_init<K, T>, ws.init);
         w(k_mf_v<K, T>, ws.v);
         w(k_mf_t<K, T>, ws.t);
+        w(k_mf_v<K, T, true>, ws.v_st, ApplyStage<K>::CTA_BYTES);
+        w(k_mf_t<K, T, true>, ws.t_st, ApplyStage<K>::CTA_BYTES);
         w(k_mf_residual<K, T>, ws.res);
     }
     return e;

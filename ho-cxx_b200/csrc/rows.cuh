@@ -225,54 +225,81 @@ __device__ __forceinline__ T element_total(T v, int lw) {
     return s;
 }
 
+// What one thread of the operator reads for its row t of element `el`: rows and columns
+// of the operand and the metric coefficients, face point t of the four faces' coefficients
+// and incoming traces, and the element's face codes.
+template <int K, typename T>
+struct ApplyIn {
+    T xr[K], xc[K], g11[K], g12r[K], g22[K], g12c[K];
+    T fa[4], fb[4], nfa[4], nfb[4], ntv[4], ntg[4];
+    int code[4];
+};
+
+// The operator's inputs from global memory (zeros for an inactive thread).
+template <int K, typename T>
+__device__ __forceinline__ void row_apply_load(const PoisGeom<T>& g, const T* __restrict__ x,
+                                               const T* __restrict__ tvin, const T* __restrict__ tgin,
+                                               const RowIdx<K>& ix, ApplyIn<K, T>& in) {
+    constexpr int K2 = K * K;
+    const int t = ix.t, el = ix.el;
+    if (ix.active) {
+        const size_t e2 = (size_t)el * K2;
+        load_row<K, T>(x + e2 + t * K, in.xr);
+        load_col<K, T>(x + e2 + t, in.xc);
+        load_row<K, T>(g.G11 + e2 + t * K, in.g11);
+        load_row<K, T>(g.G12 + e2 + t * K, in.g12r);
+        load_col<K, T>(g.G22 + e2 + t, in.g22);
+        load_col<K, T>(g.G12 + e2 + t, in.g12c);
+        const size_t q4 = ((size_t)el * K + t) * 4;  // face point t of the 4 faces ([N][K][4])
+        load4<T>(g.fa + q4, in.fa);
+        load4<T>(g.fb + q4, in.fb);
+        load4<T>(g.nfa + q4, in.nfa);
+        load4<T>(g.nfb + q4, in.nfb);
+        load4<T>(tvin + q4, in.ntv);
+        load4<T>(tgin + q4, in.ntg);
+        load4i(g.code + el * 4, in.code);
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; ++i) in.xr[i] = in.xc[i] = in.g11[i] = in.g12r[i] = in.g22[i] = in.g12c[i] = T(0);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            in.fa[f] = in.fb[f] = in.nfa[f] = in.nfb[f] = in.ntv[f] = in.ntg[f] = T(0);
+            in.code[f] = -1;
+        }
+    }
+}
+
 // y = A x, rows: the homogeneous-boundary Poisson operator (the method-2 FR Laplacian
 // that the reference assembles in form_Laplace_operator_matrix, src/HO_2D.cpp:1533-1804)
 // of element `el`, row t, from the element's own rows of x, its metric coefficients, its
 // face coefficients and the incoming face traces of x that its neighbours' producers
-// wrote (tvin/tgin, [N][K][4]). Every global read is the element's own data. Warp-
-// collective: every lane of the warp calls it.
+// wrote (in, read by row_apply_load or from a staged copy). Warp-collective: every lane
+// of the warp calls it.
 template <int K, typename T>
-__device__ __forceinline__ void row_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tvin,
-                                          const T* __restrict__ tgin, RowScratch<K, T>& sm, const RowIdx<K>& ix,
-                                          T (&y)[K]) {
-    constexpr int K2 = K * K;
+__device__ __forceinline__ void row_apply_core(const MfOp<T>& op, const ApplyIn<K, T>& in, RowScratch<K, T>& sm,
+                                               const RowIdx<K>& ix, T (&y)[K]) {
     const PoisGeom<T>& g = op.g;
     const DevBases<T>& b = op.b;
-    const int t = ix.t, lw = ix.lw, el = ix.el;
+    const int t = ix.t, lw = ix.lw;
     const bool act = ix.active;
-    T xr[K], xc[K], g11[K], g12r[K], g22[K], g12c[K];
-    T fa[4], fb[4], nfa[4], nfb[4], ntv[4], ntg[4];
-    int code[4];
+    const T(&xr)[K] = in.xr;
+    const T(&xc)[K] = in.xc;
+    const T(&g11)[K] = in.g11;
+    const T(&g12r)[K] = in.g12r;
+    const T(&g22)[K] = in.g22;
+    const T(&g12c)[K] = in.g12c;
+    const T(&fa)[4] = in.fa;
+    const T(&fb)[4] = in.fb;
+    const T(&nfa)[4] = in.nfa;
+    const T(&nfb)[4] = in.nfb;
+    const T(&ntv)[4] = in.ntv;
+    const T(&ntg)[4] = in.ntg;
+    const int(&code)[4] = in.code;
     T Dc[K], Dr[K];  // column t and column K-1-t of D (thread-dependent basis entries)
 #pragma unroll
     for (int m = 0; m < K; ++m) {
         Dc[m] = b.D[m * K + t];
         Dr[m] = b.D[m * K + (K - 1 - t)];
-    }
-    if (act) {
-        const size_t e2 = (size_t)el * K2;
-        load_row<K, T>(x + e2 + t * K, xr);
-        load_col<K, T>(x + e2 + t, xc);
-        load_row<K, T>(g.G11 + e2 + t * K, g11);
-        load_row<K, T>(g.G12 + e2 + t * K, g12r);
-        load_col<K, T>(g.G22 + e2 + t, g22);
-        load_col<K, T>(g.G12 + e2 + t, g12c);
-        const size_t q4 = ((size_t)el * K + t) * 4;  // face point t of the 4 faces ([N][K][4])
-        load4<T>(g.fa + q4, fa);
-        load4<T>(g.fb + q4, fb);
-        load4<T>(g.nfa + q4, nfa);
-        load4<T>(g.nfb + q4, nfb);
-        load4<T>(tvin + q4, ntv);
-        load4<T>(tgin + q4, ntg);
-        load4i(g.code + el * 4, code);
-    } else {
-#pragma unroll
-        for (int i = 0; i < K; ++i) xr[i] = xc[i] = g11[i] = g12r[i] = g22[i] = g12c[i] = T(0);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            fa[f] = fb[f] = nfa[f] = nfb[f] = ntv[f] = ntg[f] = T(0);
-            code[f] = -1;
-        }
     }
     // own traces; common values on interior (average) and Dirichlet (zero) faces
     T tv[4], tg[4], com[4];
@@ -400,6 +427,16 @@ __device__ __forceinline__ void row_apply(const MfOp<T>& op, const T* __restrict
         y[i] = s + ycr[i];
     }
     __syncwarp();  // the scratch may be rewritten by the caller's next use
+}
+
+// y = A x with the inputs read from global memory (row_apply_load, row_apply_core).
+template <int K, typename T>
+__device__ __forceinline__ void row_apply(const MfOp<T>& op, const T* __restrict__ x, const T* __restrict__ tvin,
+                                          const T* __restrict__ tgin, RowScratch<K, T>& sm, const RowIdx<K>& ix,
+                                          T (&y)[K]) {
+    ApplyIn<K, T> in;
+    row_apply_load<K, T>(op.g, x, tvin, tgin, ix, in);
+    row_apply_core<K, T>(op, in, sm, ix, y);
 }
 
 // Face traces of an element block held as rows (row t in `row`), scattered to the

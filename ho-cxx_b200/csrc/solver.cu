@@ -26,10 +26,12 @@
 
 namespace ho2d {
 
+// Every buffer gets 16 bytes past its end: a bulk copy that rounds a span's end up to the
+// next 16-byte boundary (apply_stage.cuh) stays inside the allocation.
 cudaError_t DeviceBuffer::alloc(size_t bytes) {
     reset();
     if (bytes == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p_, bytes);
+    cudaError_t e = cudaMalloc(&p_, bytes + 16);
     if (e == cudaSuccess) n_ = bytes;
     else p_ = nullptr;
     return e;
@@ -45,6 +47,8 @@ void DeviceBuffer::reset() {
 Solver::Solver() : d_(new DeviceState) {
     const char* pe = std::getenv("HO2D_PSI_EXTRAP");
     if (pe) psi_extrap_ = std::atoi(pe);
+    const char* os = std::getenv("HO2D_OP_STAGE");
+    if (os && os[0]) d_->op_staged = std::atoi(os) != 0;
     const char* v = std::getenv("HO2D_VERBOSE");
     verbose_ = v && v[0] && v[0] != '0';
     const char* g = std::getenv("HO2D_GRAPHS");
