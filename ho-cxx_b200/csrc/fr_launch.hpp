@@ -41,6 +41,7 @@ struct ResidualArgs {
     double* omega;    // vorticity at time level n (FP64)
     double* acc;      // RK accumulator (FP64)
     T* w_next;        // next stage input (may alias nothing in the stage-only mode)
+    double* w_next64 = nullptr;  // optional FP64 copy of the next stage input (FP32 stage)
     T* rhs_diff;      // optional outputs (nullptr to skip)
     T* rhs_adv;
     T* k_out;

@@ -183,7 +183,7 @@ Error Solver::setup_from_mesh() {
     // fields (typed fields sized for double so either precision fits)
     const std::vector<double> zv(nv, 0.0);
     for (DeviceBuffer* b : {&d.omega, &d.acc, &d.psi64, &d.rhs, &d.rres, &d.w_stage, &d.psiT, &d.u, &d.v, &d.rhs_diff,
-                            &d.rhs_adv, &d.kout})
+                            &d.rhs_adv, &d.kout, &d.w_stage64})
         HO2D_CUDA(upload(*b, zv), "alloc fields");
     const std::vector<double> zf(nf, 0.0);
     for (DeviceBuffer* b : {&d.psi_tv, &d.psi_tg, &d.w_tv, &d.w_tg, &d.U_t}) HO2D_CUDA(upload(*b, zf), "alloc traces");
@@ -897,16 +897,29 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     BcArrays bc{d.bc_p.as<double>(), d.bc_nv.as<double>(), d.bc_pv.as<double>(), d.bc_d.as<double>(),
                 d.bc_w.as<double>(), d.vjump.as<double>(), d.bc_adv.as<double>()};
     HO2D_TRY(update_bcs<T>(time_ + coeff * in_.dt, rk_stage == 0));
+    const FrGeom<double> g64 = geom_of<double>(d, mesh_, false);
+    // Inside a time step the FP32 stage takes its Poisson right-hand side from the FP64
+    // stage input: omega for the first stage, the residual kernel's FP64 copy of the next
+    // stage input for the others. The FP32 rounding of the stage vorticity is noise that the
+    // extrapolated initial guess cannot predict, so a right-hand side built from it starts
+    // every solve at about 1e-7 relative residual.
+    const bool rhs64 = f32 && update;
     if (solve) {
-        HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
-                                        d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
-                  "poisson_rhs");
+        if (rhs64)
+            HO2D_CUDA(launch_poisson_rhs<double>(K, N, d.face_nb.as<int>(),
+                                                 rk_stage == 0 ? d.omega.as<double>() : d.w_stage64.as<double>(),
+                                                 g64.J, d.bsrc.as<double>(), d.bc_p.as<double>(),
+                                                 d.rhs.as<double>(), d.stream),
+                      "poisson_rhs");
+        else
+            HO2D_CUDA(launch_poisson_rhs<T>(K, N, d.face_nb.as<int>(), d.w_stage.as<T>(), g.J, d.bsrc.as<double>(),
+                                            d.bc_p.as<double>(), d.rhs.as<double>(), d.stream),
+                      "poisson_rhs");
         launches_ += 1;
         HO2D_TRY(poisson_solve());
     }
     // the velocity is derived from psi in FP64 in both precisions (VelocityArgs)
     const double* psi = d.psi64.as<double>();
-    const FrGeom<double> g64 = geom_of<double>(d, mesh_, false);
     HO2D_CUDA(launch_trace<double>(K, N, psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.b64, d.stream), "trace");
     VelocityArgs<T, double> va{psi, d.psi_tv.as<double>(), d.psi_tg.as<double>(), d.w_stage.as<T>(), d.u.as<T>(),
                                d.v.as<T>(), d.w_tv.as<T>(), d.w_tg.as<T>(), d.U_t.as<T>(), in_.dt, in_.reyn_inv};
@@ -926,6 +939,7 @@ Error Solver::stage_t(double coeff, int rk_stage, bool update, bool solve) {
     ra.omega = d.omega.as<double>();
     ra.acc = d.acc.as<double>();
     ra.w_next = update ? d.w_stage.as<T>() : nullptr;
+    ra.w_next64 = rhs64 ? d.w_stage64.as<double>() : nullptr;
     // the RHS terms are kept from a lone stage and from the last stage of a step (the
     // reference's RHS arrays hold the last stage computed; its VTK output writes them)
     const int ns = in_.ti_type == 4 ? 4 : (in_.ti_type == 2 ? 2 : 1);

@@ -82,6 +82,9 @@ struct DeviceState {
     DeviceBuffer omega, acc, psi64, rhs, rres;
     DeviceBuffer vort_in, vort_flags;  // set_vorticity: the staged field and its check flags
     DeviceBuffer w_stage, psiT, u, v, psi_tv, psi_tg, w_tv, w_tg, U_t, rhs_diff, rhs_adv, kout;
+    // FP64 value of the next stage input, written beside the FP32 one by the stage kernels
+    // of HO2D_MIXED; the Poisson right-hand side of the stages after the first reads it
+    DeviceBuffer w_stage64;
     // Poisson operator and Krylov workspace
     // Poisson operator: matrix-free; block-Jacobi inverses and block row sums from setup
     DeviceBuffer dinv64, dinv32, rowsum64, rowsum32, bcol;

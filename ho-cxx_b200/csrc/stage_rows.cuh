@@ -548,22 +548,20 @@ __global__ void __launch_bounds__(Rows<K>::THREADS, sizeof(T) == 4 ? 5 : 1)
         } else if (a.ti_type == 2) {
             if (a.stage == 0) {
                 a.acc[q] = k;
-                a.w_next[q] = T(om + 1.0 * k);
+                const double wn = om + 1.0 * k;
+                a.w_next[q] = T(wn);
+                if (a.w_next64) a.w_next64[q] = wn;
             } else {
                 om += 0.5 * (a.acc[q] + k);
                 a.omega[q] = om;
                 if (a.w_next) a.w_next[q] = T(om);
             }
         } else {
-            if (a.stage == 0) {
-                a.acc[q] = k;
-                a.w_next[q] = T(om + 0.5 * k);
-            } else if (a.stage == 1) {
-                a.acc[q] = a.acc[q] + 2.0 * k;
-                a.w_next[q] = T(om + 0.5 * k);
-            } else if (a.stage == 2) {
-                a.acc[q] = a.acc[q] + 2.0 * k;
-                a.w_next[q] = T(om + 1.0 * k);
+            if (a.stage < 3) {
+                a.acc[q] = a.stage == 0 ? k : a.acc[q] + 2.0 * k;
+                const double wn = om + (a.stage == 2 ? 1.0 : 0.5) * k;
+                a.w_next[q] = T(wn);
+                if (a.w_next64) a.w_next64[q] = wn;
             } else {
                 om += (a.acc[q] + k) / 6.0;
                 a.omega[q] = om;
